@@ -1,0 +1,366 @@
+#!/usr/bin/env python
+"""Throughput of the explicit central-difference stepper in element-cycles/s.
+
+Workload (default): the large elastic-plastic block -- 256x128x64 8-node
+hexahedra (2,097,152 elements, 2,154,945 nodes), J2 plasticity, seeded
+smoothed-Gaussian initial velocities, bottom face fixed.  One bench step is
+``--cycles-per-step`` cycles (default 500) of the stepper on the resident
+model; ten steps make the workload's 5000 cycles.  The per-cycle working set
+(~2.3 GB FP64) is far larger than the 126 MB L2, so no flush is needed
+between timed steps.
+
+Arms:
+  --impl ours (default)  the sm_100a stepper through the C ABI
+                         (enscdynamics_b200/_lib/libensc_b200.so)
+  --impl reference       the reference CPU stepper (compiled from its sources
+                         into oracle/_ref) on a bounded slab of the same
+                         workload, with all host threads
+
+One JSON line is printed by rank 0.  Multi-GPU (torchrun): every rank runs
+an independent replica of the workload (the stepper has no cross-instance
+exchange), so scaling is weak and ``value`` sums all ranks' element-cycles
+over the slowest rank's device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "element-cycles/s"
+CPU_SAMPLE_DIMS = (256, 128, 8)      # slab of the block workload for the CPU legs
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["block", "cantilever"], default="block")
+    ap.add_argument("--precision", choices=["fp64"], default="fp64")
+    ap.add_argument("--cycles-per-step", type=int, default=500)
+    ap.add_argument("--profile-cycles", type=int, default=40)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-cycles", type=int, default=20)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------------------
+# helpers
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str):
+        self.uuid = uuid
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.uuid}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), f[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def element_pass_bytes(ne: int, nn: int, plastic: bool) -> int:
+    """Algorithmic bytes of one element-pass launch (FP64): connectivity 32,
+    sigma r/w 96, QIA r/w 192, B0^T 192, V0 8, element-force write 192 per
+    element (+16 eps_p r/w with J2), and the x, u, v gather counted once per
+    node (72 B)."""
+    return ne * (32 + 96 + 192 + 192 + 8 + 192 + (16 if plastic else 0)) + nn * 72
+
+
+def cycle_bytes(ne: int, nn: int, plastic: bool) -> int:
+    """Canonical algorithmic bytes of one cycle (FP64): 904 B per element
+    (+16 with J2) and 185 B per node."""
+    return ne * (904 + (16 if plastic else 0)) + nn * 185
+
+
+def build_problem(name: str):
+    from enscdynamics_b200 import workloads
+    if name == "block":
+        return workloads.block()
+    return workloads.cantilever()
+
+
+# --------------------------------------------------------------------------
+# CPU legs (reference stepper compiled from its sources; checker territory)
+
+def cpu_reference_sample(cycles: int, threads: int, repeats: int = 1):
+    """Times the reference CPU stepper on a slab of the block workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from enscdynamics_b200 import workloads
+    if not pyoracle.harness_available():
+        return None
+    nx, ny, nz = CPU_SAMPLE_DIMS
+    p = workloads.block(nx, ny, nz, 1.0, 0.5, 0.25 * nz / 64, plastic=False)
+    out = []
+    with tempfile.TemporaryDirectory() as d:
+        deck = p.write_deck(d)
+        for _ in range(repeats):
+            r = pyoracle.run_reference(d, deck, "time", cycles, threads=threads)
+            out.append(r)
+    ne = p.mesh.n_elements
+    return {"elements": ne, "cycles": cycles, "runs": out,
+            "loop_s": [r["loop_s"] for r in out],
+            "value": ne * cycles * len(out) / sum(r["loop_s"] for r in out)}
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_reference_sample(max(2, args.cpu_cycles // 4), threads)
+    t0 = time.time()
+    res = cpu_reference_sample(args.cpu_cycles, threads, repeats=args.steps)
+    wall = time.time() - t0
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference harness not built (oracle/_ref)"}))
+        return 0
+    nx, ny, nz = CPU_SAMPLE_DIMS
+    sample = (f"{nx}x{ny}x{nz} slab ({res['elements']} elements) of the block workload, elastic (the reference "
+              f"has no J2), {args.cpu_cycles} cycles per step, cycle loop timed by the harness")
+    line = {"impl": "reference", "metric": METRIC, "value": res["value"], "unit": METRIC, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * sum(res["loop_s"]) / len(res["loop_s"]),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "block 256x128x64 hex8 J2 (reference sample: slab)", "elements": res["elements"],
+                       "cycles_per_step": args.cpu_cycles, "threads": threads},
+            "cpu_baseline": {"value": res["value"], "unit": METRIC, "cores": threads, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": res["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": wall}
+    print(json.dumps(line))
+    return 0
+
+
+# --------------------------------------------------------------------------
+# GPU arm
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from enscdynamics_b200 import capi
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    p = build_problem(args.workload)
+    ne, nn = p.mesh.n_elements, p.mesh.n_nodes
+    plastic = p.material.yield_stress > 0.0
+    C = args.cycles_per_step
+    stream = torch.cuda.Stream()
+    s = capi.Stepper(p.mesh.x0, p.mesh.conn, p.v0, material=p.material, controls=p.controls, device=local,
+                     stream=stream.cuda_stream)
+    s.set_bcs(p.bc_code, p.bc_value)
+    kpc = s.kernels_per_cycle
+
+    # warm-up
+    for _ in range(args.warmup):
+        s.step_async(C)
+    s.sync()
+
+    # timed region: K steps of C cycles, inputs resident in HBM
+    uuid = str(torch.cuda.get_device_properties(local).uuid)
+    if not uuid.startswith("GPU-"):
+        uuid = "GPU-" + uuid
+    sampler = ClockSampler(uuid)
+    barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        s.step_async(C)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    rep = s.sync()
+    assert rep["status"] == 0, rep
+    ms_max = max_over_ranks(ms)
+    work = sum_over_ranks(float(ne) * C * args.steps)
+    value = work / (ms_max / 1000.0)
+    launches = args.steps * (C * kpc + 1)
+
+    # per-kernel CUDA-event durations on the launching stream (roofline)
+    prof = s.profile(args.profile_cycles)
+    el = prof["element"]
+    el_ms = el["ms"] / max(el["launches"], 1)
+    nd = prof["node"]
+    nd_ms = nd["ms"] / max(nd["launches"], 1)
+    peak, peak_kind = measured_peaks()
+    el_bytes = element_pass_bytes(ne, nn, plastic)
+    achieved = el_bytes / (el_ms / 1000.0) / 1e9
+    total_ms = sum(v["ms"] for v in prof.values())
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "element_fp64_block_traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            traffic = json.load(f).get("bytes_per_launch")
+
+    # end to end through the C ABI with host buffers: each step uploads the
+    # step's input state from pinned host memory, runs C cycles, and reads
+    # back u, v and sigma into pinned host memory
+    ck = s.download()
+    clk = s.step(0)
+    pin = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for k, v in ck.items()}
+    outp = {k: torch.empty(pin[k].shape, dtype=torch.float64).pin_memory() for k in ("u", "v", "sigma")}
+    h2d = sum(int(t.numel() * 8) for t in pin.values())
+    d2h = sum(int(t.numel() * 8) for t in outp.values())
+    import ctypes as C_
+    P = C_.POINTER(C_.c_double)
+    ptr = lambda t: C_.cast(t.data_ptr(), P)  # noqa: E731
+    lib = s._lib
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        s._check(lib.ensc_upload_state(s.h, ptr(pin["x"]), ptr(pin["u"]), ptr(pin["v"]), ptr(pin["sigma"]),
+                                       ptr(pin["qia"]), ptr(pin["eps_p"]), clk["time"], clk["dt_i"], clk["dt_i_1"],
+                                       clk["dt_stable_min"]))
+        s.step_async(C)
+        s._check(lib.ensc_download(s.h, None, ptr(outp["u"]), ptr(outp["v"]), ptr(outp["sigma"]), None, None))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    e2e_work = sum_over_ranks(float(ne) * C * args.e2e_steps)
+    e2e_value = e2e_work / (e2e_ms / 1000.0)
+    s.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        res = cpu_reference_sample(args.cpu_cycles, threads)
+        if res is not None:
+            nx, ny, nz = CPU_SAMPLE_DIMS
+            cpu = {"value": res["value"], "unit": METRIC, "cores": threads, "kind": "reference",
+                   "sample": f"{nx}x{ny}x{nz} slab ({res['elements']} elements) of the block workload, elastic "
+                             f"(the reference has no J2), {args.cpu_cycles} cycles, cycle loop timed by the harness"}
+
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "block 256x128x64 hex8 (2,097,152 el, 2,154,945 nodes), J2, 5000 cycles = 10 steps"
+                   if args.workload == "block" else p.name,
+                   "elements": ne, "nodes": nn, "cycles_per_step": C, "precision": "fp64",
+                   "l2": f"inputs larger than L2 ({cycle_bytes(ne, nn, plastic) / 1e9:.2f} GB per cycle)",
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "kernel": "element pass (k_element, FP64)",
+                     "peak_source": peak_kind, "kernel_ms": el_ms, "bytes_per_launch": el_bytes},
+        # whole-cycle canonical bytes per GPU over the timed region
+        "cycle_roofline": {"bytes_per_cycle": cycle_bytes(ne, nn, plastic),
+                           "achieved_gbs": cycle_bytes(ne, nn, plastic) * C * args.steps / (ms_max / 1000.0) / 1e9,
+                           "frac": None},
+        "kernel_share": {k: v["ms"] / total_ms for k, v in prof.items()},
+        "node_pass_ms": nd_ms,
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    line["cycle_roofline"]["frac"] = line["cycle_roofline"]["achieved_gbs"] / peak
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,241 @@
+"""ctypes binding of the C ABI in include/ensc_gpu.h (libensc_b200.so).
+
+``Stepper`` owns one solver instance on one GPU.  There is no CPU fallback:
+if the library or a GPU is missing, construction raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+from typing import Dict, Optional
+
+import numpy as np
+
+from . import mesh as _mesh
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "_lib", "libensc_b200.so")
+
+FP64 = 0
+MIXED = 1
+
+_ERR = {-1: "ENSC_ERR_ARG", -2: "ENSC_ERR_OOM", -3: "ENSC_ERR_CUDA", -4: "ENSC_ERR_NONFINITE",
+        -5: "ENSC_ERR_INVERTED", -6: "ENSC_ERR_TIMEOUT", -7: "ENSC_ERR_NODEVICE"}
+
+_P = C.POINTER(C.c_double)
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("n_nodes", C.c_int64), ("n_elements", C.c_int64), ("conn", C.POINTER(C.c_uint32)),
+                ("x0", _P), ("v0", _P), ("bt", _P), ("vol0", _P), ("inv_mass", _P)]
+
+
+class MaterialDesc(C.Structure):
+    _fields_ = [("E", C.c_double), ("nu", C.c_double), ("rho", C.c_double),
+                ("yield_stress", C.c_double), ("hardening_modulus", C.c_double)]
+
+
+class Params(C.Structure):
+    _fields_ = [("c_dr", C.c_double), ("c_cr", C.c_double), ("factor_timestep", C.c_double),
+                ("cvisl", C.c_double), ("cvisq", C.c_double), ("total_time", C.c_double),
+                ("gravity_on", C.c_int32), ("gravity_value", C.c_double), ("gravity_dir", C.c_double * 3),
+                ("precision", C.c_int32), ("device", C.c_int32), ("stream", C.c_void_p),
+                ("graph_chunk", C.c_int32)]
+
+
+class StepReport(C.Structure):
+    _fields_ = [("time", C.c_double), ("dt_i", C.c_double), ("dt_i_1", C.c_double),
+                ("cycles", C.c_int64), ("total_cycles", C.c_int64), ("status", C.c_int32), ("done", C.c_int32),
+                ("dt_stable_min", C.c_double)]
+
+
+class EnergyReport(C.Structure):
+    _fields_ = [("kinetic", C.c_double), ("internal", C.c_double), ("hourglass", C.c_double),
+                ("viscous", C.c_double), ("external", C.c_double), ("kinetic0", C.c_double)]
+
+
+# every symbol include/ensc_gpu.h declares: (name, restype, argtypes)
+SIGNATURES = [
+    ("ensc_abi_version", C.c_int, []),
+    ("ensc_create", C.c_int, [C.POINTER(MeshDesc), C.POINTER(MaterialDesc), C.POINTER(Params),
+                              C.POINTER(C.c_void_p)]),
+    ("ensc_set_bcs", C.c_int, [C.c_void_p, C.POINTER(C.c_int8), _P]),
+    ("ensc_set_gravity", C.c_int, [C.c_void_p, C.c_int32, C.c_double, _P]),
+    ("ensc_step", C.c_int, [C.c_void_p, C.c_int64, C.c_double, C.POINTER(StepReport)]),
+    ("ensc_step_async", C.c_int, [C.c_void_p, C.c_int64, C.c_double]),
+    ("ensc_sync", C.c_int, [C.c_void_p, C.POINTER(StepReport)]),
+    ("ensc_download", C.c_int, [C.c_void_p, _P, _P, _P, _P, _P, _P]),
+    ("ensc_upload_state", C.c_int, [C.c_void_p, _P, _P, _P, _P, _P, _P, C.c_double, C.c_double, C.c_double,
+                                    C.c_double]),
+    ("ensc_energy", C.c_int, [C.c_void_p, C.POINTER(EnergyReport)]),
+    ("ensc_download_reactions", C.c_int, [C.c_void_p, _P]),
+    ("ensc_profile", C.c_int, [C.c_void_p, C.c_int64, C.c_double, _P, C.POINTER(C.c_int64)]),
+    ("ensc_device_bytes", C.c_int64, [C.c_void_p]),
+    ("ensc_kernels_per_cycle", C.c_int32, [C.c_void_p]),
+    ("ensc_destroy", None, [C.c_void_p]),
+    ("ensc_last_error", C.c_char_p, [C.c_void_p]),
+]
+
+_lib = None
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    """Loads the stepper library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} is missing: build it with `python -m enscdynamics_b200.build`")
+        lib = C.CDLL(path)
+        for name, res, args in SIGNATURES:
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+class EnscError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{_ERR.get(code, code)}: {msg}")
+        self.code = code
+
+
+def _dp(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(_P)
+
+
+class Stepper:
+    """One GPU solver instance behind the C ABI."""
+
+    def __init__(self, x0: np.ndarray, conn: np.ndarray, v0: Optional[np.ndarray] = None, *,
+                 material: _mesh.Material, controls: _mesh.Controls, precision: int = FP64,
+                 bt: Optional[np.ndarray] = None, vol0: Optional[np.ndarray] = None,
+                 inv_mass: Optional[np.ndarray] = None, device: int = 0, stream: Optional[int] = None,
+                 graph_chunk: int = 0):
+        lib = load()
+        self._lib = lib
+        self.h = C.c_void_p()
+        self.n_nodes = int(x0.shape[0])
+        self.n_elements = int(conn.shape[0])
+        keep = []
+
+        def arr(a, dt):
+            if a is None:
+                return None
+            b = np.ascontiguousarray(a, dtype=dt)
+            keep.append(b)
+            return b
+
+        conn_a = arr(conn, np.uint32)
+        x0_a = arr(x0, np.float64)
+        v0_a = arr(v0, np.float64)
+        m = MeshDesc(self.n_nodes, self.n_elements, conn_a.ctypes.data_as(C.POINTER(C.c_uint32)), _dp(x0_a),
+                     _dp(v0_a), _dp(arr(bt, np.float64)), _dp(arr(vol0, np.float64)), _dp(arr(inv_mass, np.float64)))
+        mt = MaterialDesc(material.E, material.nu, material.rho, material.yield_stress, material.hardening)
+        p = Params()
+        p.c_dr, p.c_cr, p.factor_timestep = controls.c_dr, controls.c_cr, controls.factor
+        p.cvisl, p.cvisq, p.total_time = controls.cvisl, controls.cvisq, controls.total_time
+        if controls.gravity is not None:
+            p.gravity_on = 1
+            p.gravity_value = controls.gravity[0]
+            for i in range(3):
+                p.gravity_dir[i] = controls.gravity[1][i]
+        p.precision = precision
+        p.device = device
+        p.stream = stream
+        p.graph_chunk = graph_chunk
+        rc = lib.ensc_create(C.byref(m), C.byref(mt), C.byref(p), C.byref(self.h))
+        if rc != 0:
+            raise EnscError(rc, lib.ensc_last_error(None).decode())
+        self.precision = precision
+
+    # -- helpers -------------------------------------------------------------
+    def _check(self, rc: int) -> None:
+        if rc != 0:
+            raise EnscError(rc, self._lib.ensc_last_error(self.h).decode())
+
+    def close(self) -> None:
+        if self.h:
+            self._lib.ensc_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- API -----------------------------------------------------------------
+    def set_bcs(self, code: Optional[np.ndarray], value: Optional[np.ndarray] = None) -> None:
+        c = None if code is None else np.ascontiguousarray(code, dtype=np.int8)
+        v = None if value is None else np.ascontiguousarray(value, dtype=np.float64)
+        self._check(self._lib.ensc_set_bcs(self.h, None if c is None else c.ctypes.data_as(C.POINTER(C.c_int8)),
+                                           _dp(v)))
+
+    def set_gravity(self, on: bool, value: float = 0.0, direction=(0.0, 0.0, 0.0)) -> None:
+        d = np.ascontiguousarray(direction, dtype=np.float64)
+        self._check(self._lib.ensc_set_gravity(self.h, int(on), float(value), _dp(d)))
+
+    def step(self, max_cycles: int, step_end: float = math.inf) -> Dict[str, float]:
+        r = StepReport()
+        self._check(self._lib.ensc_step(self.h, int(max_cycles), float(step_end), C.byref(r)))
+        return {k: getattr(r, k) for k, _ in StepReport._fields_}
+
+    def step_async(self, max_cycles: int, step_end: float = math.inf) -> None:
+        self._check(self._lib.ensc_step_async(self.h, int(max_cycles), float(step_end)))
+
+    def sync(self) -> Dict[str, float]:
+        r = StepReport()
+        self._check(self._lib.ensc_sync(self.h, C.byref(r)))
+        return {k: getattr(r, k) for k, _ in StepReport._fields_}
+
+    def download(self, out: Optional[Dict[str, np.ndarray]] = None) -> Dict[str, np.ndarray]:
+        nn, ne = self.n_nodes, self.n_elements
+        if out is None:
+            out = {"x": np.empty((nn, 3)), "u": np.empty((nn, 3)), "v": np.empty((nn, 3)),
+                   "sigma": np.empty((ne, 6)), "qia": np.empty((ne, 12)), "eps_p": np.empty(ne)}
+        g = lambda k: _dp(out.get(k))  # noqa: E731
+        self._check(self._lib.ensc_download(self.h, g("x"), g("u"), g("v"), g("sigma"), g("qia"), g("eps_p")))
+        return out
+
+    def upload_state(self, state: Dict[str, np.ndarray], time: float, dt_i: float, dt_i_1: float,
+                     dt_stable_min: float = 0.0) -> None:
+        arrays = {k: (None if state.get(k) is None else np.ascontiguousarray(state[k], dtype=np.float64))
+                  for k in ("x", "u", "v", "sigma", "qia", "eps_p")}
+        self._check(self._lib.ensc_upload_state(self.h, *[_dp(arrays[k]) for k in ("x", "u", "v", "sigma", "qia",
+                                                                                     "eps_p")],
+                                                float(time), float(dt_i), float(dt_i_1), float(dt_stable_min)))
+
+    def energy(self) -> Dict[str, float]:
+        r = EnergyReport()
+        self._check(self._lib.ensc_energy(self.h, C.byref(r)))
+        return {k: getattr(r, k) for k, _ in EnergyReport._fields_}
+
+    def reactions(self) -> np.ndarray:
+        rf = np.empty((self.n_nodes, 3))
+        self._check(self._lib.ensc_download_reactions(self.h, _dp(rf)))
+        return rf
+
+    KERNELS = ("cycle_begin", "edge_prepass", "begin_exact", "element", "node")
+
+    def profile(self, max_cycles: int, step_end: float = math.inf) -> Dict[str, Dict[str, float]]:
+        """Per-kernel CUDA-event durations (ms summed, launches) over max_cycles."""
+        ms = (C.c_double * 5)()
+        n = (C.c_int64 * 5)()
+        self._check(self._lib.ensc_profile(self.h, int(max_cycles), float(step_end), ms, n))
+        return {k: {"ms": ms[i], "launches": int(n[i])} for i, k in enumerate(self.KERNELS)}
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self._lib.ensc_device_bytes(self.h))
+
+    @property
+    def kernels_per_cycle(self) -> int:
+        return int(self._lib.ensc_kernels_per_cycle(self.h))

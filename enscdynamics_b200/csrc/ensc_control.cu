@@ -1,0 +1,279 @@
+// Cycle control and data-movement kernels.  Built with -fmad=false: the
+// stable-time-step arithmetic reproduces the reference's
+// update_minVertex_perMaterial_and_dt (Explicit3D/source/exDyna3D.cpp:663-686)
+// and run()'s last-step clamp (:90-97) operation by operation.
+#include "ensc_device.cuh"
+#include "ensc_kernels.h"
+
+#include <cfloat>
+
+namespace ensc {
+namespace {
+
+// Sums n values spaced by `stride` in a fixed order: thread t takes
+// t, t+NT, t+2NT, ... left to right, then a fixed shared-memory tree.
+__device__ double fixed_sum(const double* a, int n) {
+    __shared__ double red[kCtlThreads];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += kCtlThreads) s = s + a[i];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = kCtlThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] = red[threadIdx.x] + red[threadIdx.x + w];
+        __syncthreads();
+    }
+    const double r = red[0];
+    __syncthreads();
+    return r;
+}
+
+// Folds the energy partials of the previous cycle, then performs the first
+// half of update_minVertex_perMaterial_and_dt for the next cycle: rotate
+// dt_i_1 <- dt_i, advance time (computeSate :775-780) and fix dt_i_1 unless
+// the total-time clamp (:682-685) could fire, which needs this cycle's minimum
+// element edge first (edge_prepass + begin_exact).
+// mode 0: fold + begin, 1: fold only, 2: fold as the initial kinetic energy.
+__global__ void __launch_bounds__(kCtlThreads) k_between(Ctl* ctl, Partials P, int mode) {
+    if (ctl->energy_pending || mode == 2) {
+        const double ei = fixed_sum(P.elem + 0 * P.n_elem_blocks, P.n_elem_blocks);
+        const double eh = fixed_sum(P.elem + 1 * P.n_elem_blocks, P.n_elem_blocks);
+        const double ev = fixed_sum(P.elem + 2 * P.n_elem_blocks, P.n_elem_blocks);
+        const double kin = fixed_sum(P.node + 0 * P.n_node_blocks, P.n_node_blocks);
+        const double wx = fixed_sum(P.node + 1 * P.n_node_blocks, P.n_node_blocks);
+        if (threadIdx.x == 0) {
+            if (mode == 2) {
+                ctl->energy[0] = kin;
+                ctl->energy[5] = kin;
+            } else {
+                ctl->energy[0] = kin;
+                ctl->energy[1] += ei;
+                ctl->energy[2] += eh;
+                ctl->energy[3] += ev;
+                ctl->energy[4] += wx;
+            }
+            ctl->energy_pending = 0;
+        }
+    }
+    if (mode != 0 || threadIdx.x != 0 || ctl->done) return;
+    if (!(ctl->time < ctl->step_end) || ctl->cycles_done >= ctl->cycles_target) {
+        ctl->done = 1;
+        return;
+    }
+    ctl->dts_cur = bits_ord(ctl->dts_next);
+    ctl->dts_next = kInfBits;
+    ctl->len_min = kInfBits;
+    const double dt_prev = ctl->dt_i;
+    ctl->dt_prev = dt_prev;
+    const double time = ctl->time;
+    const double time_prev = time + dt_prev;
+    // the new dt is factor * min(edge / c, dts_cur) <= factor * dts_cur
+    const double bound = ctl->dts_cur * ctl->factor;
+    const double rem = ctl->total_time - time_prev;
+    const int exact = (rem > 0.0 && rem < bound) ? 1 : 0;
+    ctl->need_exact = exact;
+    ctl->dt_final = 0;
+    if (!exact) {
+        double dt_i_1 = dt_prev;
+        if (time + dt_i_1 > ctl->step_end) {
+            const double r = ctl->step_end - time;
+            dt_i_1 = r;
+            ctl->dt_i = r;
+            ctl->dt_final = 1;
+        }
+        ctl->dt_i_1 = dt_i_1;
+        double t = time + dt_i_1;
+        if (t > ctl->total_time) t = ctl->total_time;
+        ctl->time = t;
+    }
+}
+
+// Minimum element edge over the current coordinates (min_ele_edge,
+// exDyna3D.cpp:1173-1220), needed before the element pass only in a cycle
+// where the total-time clamp may fire.
+__global__ void __launch_bounds__(128) k_edge_prepass(ElemArrays E, NodeArrays N, Ctl* ctl) {
+    if (ctl->done || !ctl->need_exact) return;
+    __shared__ unsigned long long red[4];
+    const int64_t ep = E.ne_pad, np = N.nn_pad;
+    double m = DBL_MAX;
+    for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < E.ne;
+         e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        double xyz[8][3];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const uint32_t n = E.conn[k * ep + e];
+            xyz[k][0] = N.x[n];
+            xyz[k][1] = N.x[np + n];
+            xyz[k][2] = N.x[2 * np + n];
+        }
+        constexpr int A0[12] = {0, 1, 2, 3, 4, 5, 6, 7, 0, 1, 2, 3};
+        constexpr int A1[12] = {1, 2, 3, 0, 5, 6, 7, 4, 4, 5, 6, 7};
+        double mm = DBL_MAX;
+#pragma unroll
+        for (int k = 0; k < 12; ++k) {
+            const double dx = xyz[A1[k]][0] - xyz[A0[k]][0];
+            const double dy = xyz[A1[k]][1] - xyz[A0[k]][1];
+            const double dz = xyz[A1[k]][2] - xyz[A0[k]][2];
+            const double t = dx * dx + dy * dy + dz * dz;
+            mm = t < mm ? t : mm;
+        }
+        const double len = sqrt(mm);
+        m = len < m ? len : m;
+    }
+    unsigned long long b = ord_bits(m);
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long w = __shfl_xor_sync(0xffffffffu, b, o);
+        b = w < b ? w : b;
+    }
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = b;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long r = red[0];
+        for (int i = 1; i < 4; ++i) r = red[i] < r ? red[i] : r;
+        atomicMin(&ctl->len_min, r);
+    }
+}
+
+// Rest of update_minVertex_perMaterial_and_dt and run()'s clamp for a cycle
+// that needed the exact edge minimum.
+__global__ void k_begin_exact(Ctl* ctl) {
+    if (threadIdx.x != 0 || ctl->done || !ctl->need_exact) return;
+    const double time = ctl->time;
+    double dt_i_1 = ctl->dt_prev;
+    const double time_prev = time + dt_i_1;
+    double d = bits_ord(ctl->len_min) / ctl->wos;
+    d = d < ctl->dts_cur ? d : ctl->dts_cur;
+    double dt_i = d * ctl->factor;
+    if ((ctl->total_time - time_prev) < dt_i && (ctl->total_time - time_prev) > 0.0) {
+        dt_i = ctl->total_time - time_prev;
+        dt_i_1 = dt_i;
+    }
+    if (time + dt_i_1 > ctl->step_end) {
+        const double r = ctl->step_end - time;
+        dt_i = r;
+        dt_i_1 = r;
+    }
+    ctl->dt_i = dt_i;
+    ctl->dt_i_1 = dt_i_1;
+    ctl->dt_final = 1;
+    double t = time + dt_i_1;
+    if (t > ctl->total_time) t = ctl->total_time;
+    ctl->time = t;
+}
+
+__global__ void k_arm(Ctl* ctl, double step_end, long long max_cycles) {
+    ctl->step_end = step_end;
+    ctl->cycles_target = ctl->cycles_done + max_cycles;
+    ctl->done = 0;
+}
+
+__global__ void k_reset_init(Ctl* ctl) {
+    ctl->done = 0;
+    ctl->dts_next = kInfBits;
+    ctl->len_min = kInfBits;
+    ctl->status = 0;
+}
+
+// apply_boundary_condition_vec (exDyna3D.cpp:379-490): velocity conditions
+// first, fixed DOFs last.
+template <typename VT>
+__global__ void k_apply_bc_v(NodeArrays N) {
+    VT* V = static_cast<VT*>(N.v);
+    for (int64_t n = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; n < N.nn;
+         n += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t code = N.bc[n];
+        if (!code) continue;
+        for (int c = 0; c < 3; ++c) {
+            const uint32_t cc = (code >> (2 * c)) & 3u;
+            if (cc & 2u) V[c * N.nn_pad + n] = static_cast<VT>(N.bcv[c * N.nn_pad + n]);
+            if (cc & 1u) V[c * N.nn_pad + n] = static_cast<VT>(0.0);
+        }
+    }
+}
+
+template <typename VT>
+__global__ void __launch_bounds__(kNodeThreads) k_kinetic(NodeArrays N, Partials P) {
+    const VT* V = static_cast<const VT*>(N.v);
+    double kin = 0.0;
+    for (int64_t n = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; n < N.nn;
+         n += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const double im = N.inv_mass[n];
+        for (int c = 0; c < 3; ++c) {
+            const double v = static_cast<double>(V[c * N.nn_pad + n]);
+            kin = kin + 0.5 * (v * v) / im;
+        }
+    }
+    __shared__ double red[kNodeThreads];
+    red[threadIdx.x] = kin;
+    __syncthreads();
+    for (int w = kNodeThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] = red[threadIdx.x] + red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        P.node[blockIdx.x] = red[0];
+        P.node[P.n_node_blocks + blockIdx.x] = 0.0;
+    }
+}
+
+template <typename ST>
+__global__ void k_soa_to_aos(const ST* soa, int64_t n, int64_t pad, int comps, double* aos) {
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n * comps;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t e = i / comps;
+        const int c = static_cast<int>(i - e * comps);
+        aos[i] = static_cast<double>(soa[c * pad + e]);
+    }
+}
+
+template <typename DT>
+__global__ void k_aos_to_soa(const double* aos, int64_t n, int64_t pad, int comps, DT* soa) {
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n * comps;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t e = i / comps;
+        const int c = static_cast<int>(i - e * comps);
+        soa[c * pad + e] = static_cast<DT>(aos[i]);
+    }
+}
+
+int grid_for(int64_t work, int threads) {
+    const int64_t g = (work + threads - 1) / threads;
+    return static_cast<int>(g < 1 ? 1 : (g > 4096 ? 4096 : g));
+}
+
+}  // namespace
+
+void launch_between(Ctl* ctl, const Partials& P, int mode, cudaStream_t st) {
+    k_between<<<1, kCtlThreads, 0, st>>>(ctl, P, mode);
+}
+void launch_edge_prepass(const ElemArrays& E, const NodeArrays& N, Ctl* ctl, int grid, cudaStream_t st) {
+    k_edge_prepass<<<grid, 128, 0, st>>>(E, N, ctl);
+}
+void launch_begin_exact(Ctl* ctl, cudaStream_t st) { k_begin_exact<<<1, 32, 0, st>>>(ctl); }
+void launch_arm(Ctl* ctl, double step_end, long long max_cycles, cudaStream_t st) {
+    k_arm<<<1, 1, 0, st>>>(ctl, step_end, max_cycles);
+}
+void launch_reset_init(Ctl* ctl, cudaStream_t st) { k_reset_init<<<1, 1, 0, st>>>(ctl); }
+void launch_apply_bc_v(const NodeArrays& N, bool fp32_v, cudaStream_t st) {
+    const int g = grid_for(N.nn, 256);
+    if (fp32_v) k_apply_bc_v<float><<<g, 256, 0, st>>>(N);
+    else k_apply_bc_v<double><<<g, 256, 0, st>>>(N);
+}
+void launch_kinetic0(const NodeArrays& N, const Partials& P, Ctl* ctl, bool fp32_v, int grid, cudaStream_t st) {
+    if (fp32_v) k_kinetic<float><<<grid, kNodeThreads, 0, st>>>(N, P);
+    else k_kinetic<double><<<grid, kNodeThreads, 0, st>>>(N, P);
+    k_between<<<1, kCtlThreads, 0, st>>>(ctl, P, 2);
+}
+void launch_soa_to_aos(const void* soa, int64_t n, int64_t pad, int comps, bool src_fp32, double* aos,
+                       cudaStream_t st) {
+    const int g = grid_for(n * comps, 256);
+    if (src_fp32) k_soa_to_aos<float><<<g, 256, 0, st>>>(static_cast<const float*>(soa), n, pad, comps, aos);
+    else k_soa_to_aos<double><<<g, 256, 0, st>>>(static_cast<const double*>(soa), n, pad, comps, aos);
+}
+void launch_aos_to_soa(const double* aos, int64_t n, int64_t pad, int comps, void* soa, bool dst_fp32,
+                       cudaStream_t st) {
+    const int g = grid_for(n * comps, 256);
+    if (dst_fp32) k_aos_to_soa<float><<<g, 256, 0, st>>>(aos, n, pad, comps, static_cast<float*>(soa));
+    else k_aos_to_soa<double><<<g, 256, 0, st>>>(aos, n, pad, comps, static_cast<double*>(soa));
+}
+
+}  // namespace ensc

@@ -1,0 +1,113 @@
+// Device-side data structures shared by the stepper kernels.
+//
+// Memory layout in HBM (structure of arrays, one array per component so a
+// warp of consecutive elements / nodes reads consecutive words):
+//   element arrays, length ne (padded stride ne_pad):
+//     conn[8][ne_pad] uint32         local node k of element e at conn[k*ne_pad + e]
+//     bt[24][ne_pad]                 B0^T row-major per element: (3*k + c)
+//     vol0, cbrt_v0, cbrt_v0sq [ne]  per-element constants
+//     sigma[6][ne_pad], qia[12][ne_pad], eps_p[ne]
+//     fe[24][ne_pad]                 element nodal forces of the current cycle
+//                                    (the element -> node hand-off, scratch)
+//   node arrays, length nn (stride nn_pad):
+//     x[3][nn_pad], u[3][nn_pad] (FP64 always), v[3][nn_pad]
+//     inv_mass[nn]                   per node (equal for the 3 DOFs)
+//     bc[nn] uint8                   2 bits per DOF (bit0 fixed, bit1 velocity)
+//     bcv[3][nn_pad]                 prescribed velocities
+//     ell[8][nn_pad] uint32          element holding node n in local slot k, or
+//                                    ENSC_NONE; the gather sums slots k = 0..7
+//                                    in order, as the reference sums its 8
+//                                    slot vectors (exDyna3D.cpp:638-639)
+//     csr_ptr/csr_ent                general (slot, element)-sorted lists, used
+//                                    instead of ell when a node occupies the
+//                                    same slot in more than one element
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define ENSC_NONE 0xFFFFFFFFu
+
+namespace ensc {
+
+// Status bits raised on the device and read back by the host.
+enum : int32_t {
+    ST_NONFINITE = 1,
+    ST_INVERTED = 2,
+};
+
+// Per-instance control block: the scalar state of exDyna3D's time loop
+// (time, dt_i, dt_i_1: exDyna3D.h:175-178) plus the reductions that feed it.
+struct Ctl {
+    double time, dt_i, dt_i_1;
+    double dt_prev;            // dt_i at the start of the cycle
+    double step_end, total_time;
+    double factor, wos;
+    double dts_cur;            // min element dt of the previous force pass
+    unsigned long long dts_next;   // ordered bits of min element dt, this pass
+    unsigned long long len_min;    // ordered bits of min element edge, this pass
+    long long cycles_done, cycles_target;
+    int32_t done;
+    int32_t need_exact;        // total-time clamp possible: edge minimum needed first
+    int32_t dt_final;          // dt_i already fixed for this cycle
+    int32_t energy_pending;    // partial energy sums of the last cycle not yet folded
+    int32_t status;
+    int32_t pad;
+    double energy[6];          // kinetic, internal, hourglass, viscous, external, kinetic0
+};
+
+struct Material {
+    double E, nu, rho, G, K, lambda, wos;
+    double yield0, hardening;
+    double c_dr, c_cr, cvisl, cvisq;
+    int32_t plastic;
+    int32_t gravity_on;
+    double gravity_value, gravity_dir[3];
+};
+
+struct ElemArrays {
+    int64_t ne, ne_pad;
+    const uint32_t* conn;
+    const void* bt;            // double (FP64) or float (mixed)
+    const double* vol0;
+    const double* cbrt_v0;
+    const double* cbrt_v0sq;
+    void* sigma;
+    void* qia;
+    void* eps_p;
+    void* fe;
+};
+
+struct NodeArrays {
+    int64_t nn, nn_pad;
+    double* x;
+    double* u;
+    void* v;                   // double (FP64) or float (mixed)
+    const double* inv_mass;
+    const uint8_t* bc;
+    const double* bcv;
+    const uint32_t* ell;
+    const int64_t* csr_ptr;    // non-null: use the general lists
+    const uint32_t* csr_ent;   // (e << 3) | slot
+    double* rf;                // reactions, [3][nn_pad]
+};
+
+// Partial sums written by each block of a pass, folded in fixed block order.
+struct Partials {
+    double* elem;              // [3][n_elem_blocks]
+    double* node;              // [2][n_node_blocks]
+    int32_t n_elem_blocks, n_node_blocks;
+};
+
+// Positive doubles order like their bit patterns; min-reductions over
+// element dt / edge lengths use integer atomicMin on the bits, which is
+// exact and independent of scheduling.
+__device__ __forceinline__ unsigned long long ord_bits(double d) {
+    return static_cast<unsigned long long>(__double_as_longlong(d));
+}
+__device__ __forceinline__ double bits_ord(unsigned long long b) {
+    return __longlong_as_double(static_cast<long long>(b));
+}
+constexpr unsigned long long kInfBits = 0x7FF0000000000000ull;
+
+}  // namespace ensc

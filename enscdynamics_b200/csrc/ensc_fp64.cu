@@ -1,0 +1,561 @@
+// Plain FP64 stepper kernels.  Compiled with -fmad=false: every product and
+// sum below is rounded separately, in the order written, which is the order
+// the reference evaluates it (cited per block), so results match the
+// reference CPU stepper to round-off and the CPU restatement bit-for-bit.
+//
+// One cycle (exDyna3D::run loop body, Explicit3D/source/exDyna3D.cpp:86-100)
+// is the kernel sequence
+//   between  -> [edge_prepass -> begin_exact] -> element -> node
+// launched inside a CUDA graph; see ensc_capi.cu for the orchestration.
+#include "ensc_device.cuh"
+#include "ensc_kernels.h"
+
+#include <cfloat>
+
+namespace ensc {
+namespace {
+
+__device__ __forceinline__ double det3(const double m[3][3]) {
+    // Eigen 3.4 bruteforce_det3_helper form (Eigen/src/LU/Determinant.h),
+    // as used by all_F[e].determinant() (exDyna3D.cpp:869).
+    const double h0 = m[0][0] * (m[1][1] * m[2][2] - m[1][2] * m[2][1]);
+    const double h1 = m[0][1] * (m[1][0] * m[2][2] - m[1][2] * m[2][0]);
+    const double h2 = m[0][2] * (m[1][0] * m[2][1] - m[1][1] * m[2][0]);
+    return (h0 - h1) + h2;
+}
+
+__device__ __forceinline__ double cof3(const double m[3][3], int i, int j) {
+    const int i1 = (i + 1) % 3, i2 = (i + 2) % 3, j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+    return m[i1][j1] * m[i2][j2] - m[i1][j2] * m[i2][j1];
+}
+
+__device__ __forceinline__ void inv3(const double m[3][3], double r[3][3]) {
+    // Eigen 3.4 compute_inverse<...,3> (Eigen/src/LU/InverseImpl.h), as used
+    // by all_F[e].inverse() (exDyna3D.cpp:874).
+    const double c0 = cof3(m, 0, 0), c1 = cof3(m, 1, 0), c2 = cof3(m, 2, 0);
+    const double det = (c0 * m[0][0] + c1 * m[1][0]) + c2 * m[2][0];
+    const double invdet = 1.0 / det;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) r[i][j] = cof3(m, j, i) * invdet;
+}
+
+// Hourglass base vectors Gamma (exDyna3D.cpp:1003-1008) as signs.
+__device__ __forceinline__ constexpr int tau_sign(int k, int j) {
+    constexpr int T[4][8] = {{1, -1, 1, -1, 1, -1, 1, -1},
+                             {-1, -1, 1, 1, 1, 1, -1, -1},
+                             {-1, 1, 1, -1, 1, -1, -1, 1},
+                             {-1, 1, -1, 1, 1, -1, 1, -1}};
+    return T[k][j];
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_min(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const T w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = w < v ? w : v;
+    }
+    return v;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Fixed-shape block reduction (warp butterflies, then warp 0 over the
+// warp results): deterministic for a given block size.
+template <int NT, int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double* out_slots, int stride, int slot) {
+    __shared__ double red[NV][NT / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+        const double s = warp_sum(v[i]);
+        if (lane == 0) red[i][wid] = s;
+    }
+    __syncthreads();
+    if (wid == 0) {
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+            double s = lane < NT / 32 ? red[i][lane] : 0.0;
+            s = warp_sum(s);
+            if (lane == 0) out_slots[i * stride + slot] = s;
+        }
+    }
+    __syncthreads();
+}
+
+template <int NT>
+__device__ __forceinline__ void block_min2(double a, double b, unsigned long long* ga, unsigned long long* gb) {
+    __shared__ unsigned long long ra[NT / 32], rb[NT / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    unsigned long long x = warp_min(ord_bits(a)), y = warp_min(ord_bits(b));
+    if (lane == 0) {
+        ra[wid] = x;
+        rb[wid] = y;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        x = lane < NT / 32 ? ra[lane] : kInfBits;
+        y = lane < NT / 32 ? rb[lane] : kInfBits;
+        x = warp_min(x);
+        y = warp_min(y);
+        if (lane == 0) {
+            if (ga) atomicMin(ga, x);
+            if (gb) atomicMin(gb, y);
+        }
+    }
+    __syncthreads();
+}
+
+// Element pass: add_inForce_to_rhs's element loop body
+// (exDyna3D.cpp:556-573): kinematics, Jaumann stress (+ J2 return),
+// hourglass, bulk viscosity, element dt and min edge.  Writes the element's
+// 8x3 nodal forces to fe for the node-centric gather.
+template <bool PLASTIC, bool INIT>
+__global__ void __launch_bounds__(kElemThreads) k_element(ElemArrays E, NodeArrays N, Material M, Ctl* ctl,
+                                                          Partials P) {
+    if (ctl->done) return;
+    const double dt1 = INIT ? 0.0 : ctl->dt_i_1;
+    const int64_t ne = E.ne, ep = E.ne_pad, np = N.nn_pad;
+    const uint32_t* __restrict__ conn = E.conn;
+    const double* __restrict__ bt = static_cast<const double*>(E.bt);
+    double* __restrict__ sig = static_cast<double*>(E.sigma);
+    double* __restrict__ qia = static_cast<double*>(E.qia);
+    double* __restrict__ epsp = static_cast<double*>(E.eps_p);
+    double* __restrict__ fe = static_cast<double*>(E.fe);
+    const double* __restrict__ X = N.x;
+    const double* __restrict__ U = N.u;
+    const double* __restrict__ V = static_cast<const double*>(N.v);
+    const double G = M.G, lam = M.lambda;
+    double e_int = 0.0, e_hg = 0.0, e_vis = 0.0;
+    double dts_min = DBL_MAX, len_min = DBL_MAX;
+    int32_t bad = 0;
+
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    const int64_t e_end = (ne + blockDim.x - 1) / blockDim.x * blockDim.x;
+    for (int64_t e0 = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e0 < e_end; e0 += stride) {
+        const bool live = e0 < ne;
+        const int64_t e = live ? e0 : 0;
+        double dts = DBL_MAX, len = DBL_MAX;
+        if (live) {
+            uint32_t n[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) n[k] = __ldg(conn + k * ep + e);
+            // F = I + u_e B0^T (:862-865), summed over k = 0..7
+            double F[3][3];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const double u0 = U[n[k]], u1 = U[np + n[k]], u2 = U[2 * np + n[k]];
+                const double b0 = __ldg(bt + (3 * k) * ep + e), b1 = __ldg(bt + (3 * k + 1) * ep + e),
+                             b2 = __ldg(bt + (3 * k + 2) * ep + e);
+                const double uu[3] = {u0, u1, u2}, bb[3] = {b0, b1, b2};
+#pragma unroll
+                for (int r = 0; r < 3; ++r)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) F[r][c] = (k == 0) ? uu[r] * bb[c] : F[r][c] + uu[r] * bb[c];
+            }
+            F[0][0] = 1.0 + F[0][0];
+            F[1][1] = 1.0 + F[1][1];
+            F[2][2] = 1.0 + F[2][2];
+            F[0][1] = 0.0 + F[0][1];
+            F[0][2] = 0.0 + F[0][2];
+            F[1][0] = 0.0 + F[1][0];
+            F[1][2] = 0.0 + F[1][2];
+            F[2][0] = 0.0 + F[2][0];
+            F[2][1] = 0.0 + F[2][1];
+            const double J = det3(F);
+            double Fi[3][3];
+            inv3(F, Fi);
+            if (!(J > 0.0)) bad |= ST_INVERTED;
+            // b^T = B0^T F^-1 (:872-875); L = v_e b^T (:928); VolRate (:877-885)
+            double vel[3][8];
+            double L[3][3];
+            double q01[3], q23[3], q0123[3], q45[3];
+            double vr = 0.0;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const double b0 = __ldg(bt + (3 * k) * ep + e), b1 = __ldg(bt + (3 * k + 1) * ep + e),
+                             b2 = __ldg(bt + (3 * k + 2) * ep + e);
+                double bk[3];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) bk[c] = (b0 * Fi[0][c] + b1 * Fi[1][c]) + b2 * Fi[2][c];
+                vel[0][k] = V[n[k]];
+                vel[1][k] = V[np + n[k]];
+                vel[2][k] = V[2 * np + n[k]];
+#pragma unroll
+                for (int r = 0; r < 3; ++r)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) L[r][c] = (k == 0) ? vel[r][k] * bk[c] : L[r][c] + vel[r][k] * bk[c];
+                // pairwise dot ((q0+q1)+(q2+q3)) + ((q4+q5)+(q6+q7)) per direction
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const double q = vel[c][k] * bk[c];
+                    if (k == 0 || k == 2 || k == 4 || k == 6) {
+                        if (k == 0 || k == 4) q01[c] = q; else q23[c] = q;
+                    } else if (k == 1) {
+                        q01[c] = q01[c] + q;
+                    } else if (k == 3) {
+                        q23[c] = q23[c] + q;
+                        q0123[c] = q01[c] + q23[c];
+                    } else if (k == 5) {
+                        q45[c] = q01[c] + q;
+                    } else {  // k == 7
+                        const double q67 = q23[c] + q;
+                        const double d = q0123[c] + (q45[c] + q67);
+                        vr = (c == 0) ? d : vr + d;
+                    }
+                }
+            }
+            // Jaumann stress update (:930-973)
+            double eps[6];
+            eps[0] = L[0][0];
+            eps[1] = L[1][1];
+            eps[2] = L[2][2];
+            eps[3] = (L[0][1] + L[1][0]) / 2.0;
+            eps[4] = (L[0][2] + L[2][0]) / 2.0;
+            eps[5] = (L[1][2] + L[2][1]) / 2.0;
+#pragma unroll
+            for (int i = 0; i < 6; ++i) eps[i] = eps[i] * dt1;
+            const double w0 = (L[0][1] - L[1][0]) / 2.0;
+            const double w1 = (L[0][2] - L[2][0]) / 2.0;
+            const double w2 = (L[1][2] - L[2][1]) / 2.0;
+            const double tr = (eps[0] + eps[1]) + eps[2];
+            double s[6], so[6];
+#pragma unroll
+            for (int i = 0; i < 6; ++i) so[i] = sig[i * ep + e];
+            double inc[6];
+            inc[0] = (lam * tr + 2.0 * G * eps[0]) + 2.0 * so[3] * w0 * dt1 + 2.0 * so[4] * w1 * dt1;
+            inc[1] = (lam * tr + 2.0 * G * eps[1]) - 2.0 * so[3] * w0 * dt1 + 2.0 * so[5] * w2 * dt1;
+            inc[2] = (lam * tr + 2.0 * G * eps[2]) - 2.0 * so[4] * w1 * dt1 - 2.0 * so[5] * w2 * dt1;
+            inc[3] = (2.0 * G * eps[3]) + (so[1] - so[0]) * w0 * dt1 + so[5] * w1 * dt1;
+            inc[4] = (2.0 * G * eps[4]) + (so[2] - so[0]) * w1 * dt1 + so[5] * w0 * dt1;
+            inc[5] = (2.0 * G * eps[5]) + (so[2] - so[1]) * w2 * dt1 + so[3] * w1 * dt1 - so[4] * w0 * dt1;
+#pragma unroll
+            for (int i = 0; i < 6; ++i) s[i] = so[i] + inc[i];
+            if (PLASTIC) {
+                // J2 radial return, linear isotropic hardening (no reference
+                // counterpart; the elastic instantiation omits it).
+                const double pm = ((s[0] + s[1]) + s[2]) / 3.0;
+                const double d0 = s[0] - pm, d1 = s[1] - pm, d2 = s[2] - pm;
+                const double j2 = 0.5 * ((d0 * d0 + d1 * d1) + d2 * d2) + ((s[3] * s[3] + s[4] * s[4]) + s[5] * s[5]);
+                const double seq = sqrt(3.0 * j2);
+                const double ep_old = epsp[e];
+                const double sy = M.yield0 + M.hardening * ep_old;
+                if (seq > sy) {
+                    const double dl = (seq - sy) / (3.0 * G + M.hardening);
+                    const double r = 1.0 - 3.0 * G * dl / seq;
+                    s[0] = d0 * r + pm;
+                    s[1] = d1 * r + pm;
+                    s[2] = d2 * r + pm;
+                    s[3] = s[3] * r;
+                    s[4] = s[4] * r;
+                    s[5] = s[5] * r;
+                    if (!INIT) epsp[e] = ep_old + dl;
+                }
+            }
+            if (!INIT) {
+#pragma unroll
+                for (int i = 0; i < 6; ++i) sig[i * ep + e] = s[i];
+            }
+            const double V0 = E.vol0[e];
+            const double Vc = J * V0;
+            {
+                double w = 0.0;
+#pragma unroll
+                for (int i = 0; i < 6; ++i) {
+                    const double sm = 0.5 * (so[i] + s[i]);
+                    w = w + (i < 3 ? 1.0 : 2.0) * sm * eps[i];
+                }
+                e_int += w * Vc;
+            }
+            // hourglass (:1000-1071)
+            double xyz[8][3];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                xyz[k][0] = X[n[k]];
+                xyz[k][1] = X[np + n[k]];
+                xyz[k][2] = X[2 * np + n[k]];
+            }
+            {  // min_ele_edge (:1173-1220)
+                constexpr int A0[12] = {0, 1, 2, 3, 4, 5, 6, 7, 0, 1, 2, 3};
+                constexpr int A1[12] = {1, 2, 3, 0, 5, 6, 7, 4, 4, 5, 6, 7};
+                double m = DBL_MAX;
+#pragma unroll
+                for (int k = 0; k < 12; ++k) {
+                    const double dx = xyz[A1[k]][0] - xyz[A0[k]][0];
+                    const double dy = xyz[A1[k]][1] - xyz[A0[k]][1];
+                    const double dz = xyz[A1[k]][2] - xyz[A0[k]][2];
+                    const double t = dx * dx + dy * dy + dz * dz;
+                    m = t < m ? t : m;
+                }
+                len = sqrt(m);
+            }
+            // TAU * xyz: the Gamma entries are +-1, so each product is exact
+            double TX[4][3];
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    double t = tau_sign(kk, 0) > 0 ? xyz[0][c] : -xyz[0][c];
+#pragma unroll
+                    for (int j = 1; j < 8; ++j) t = tau_sign(kk, j) > 0 ? t + xyz[j][c] : t - xyz[j][c];
+                    TX[kk][c] = t;
+                }
+            // NX2 = ||B0^T||^2 in the reference's two-lane pairwise order
+            double nx2;
+            {
+                double l0[12], l1[12];
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+#pragma unroll
+                    for (int a = 0; a < 8; ++a) {
+                        const double b = __ldg(bt + (3 * a + c) * ep + e);
+                        const int lin = 8 * c + a;
+                        if (lin & 1) l1[lin >> 1] = b * b; else l0[lin >> 1] = b * b;
+                    }
+                const double a0 = ((l0[0] + (l0[1] + l0[2])) + (l0[3] + (l0[4] + l0[5]))) +
+                                  ((l0[6] + (l0[7] + l0[8])) + (l0[9] + (l0[10] + l0[11])));
+                const double a1 = ((l1[0] + (l1[1] + l1[2])) + (l1[3] + (l1[4] + l1[5]))) +
+                                  ((l1[6] + (l1[7] + l1[8])) + (l1[9] + (l1[10] + l1[11])));
+                nx2 = a0 + a1;
+            }
+            double AT[4][8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const double b0 = __ldg(bt + (3 * j) * ep + e), b1 = __ldg(bt + (3 * j + 1) * ep + e),
+                             b2 = __ldg(bt + (3 * j + 2) * ep + e);
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk) {
+                    const double t = (TX[kk][0] * b0 + TX[kk][1] * b1) + TX[kk][2] * b2;
+                    AT[kk][j] = static_cast<double>(tau_sign(kk, j)) - t;
+                }
+            }
+            double HIA[3][4];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk) {
+                    double t = vel[i][0] * AT[kk][0];
+#pragma unroll
+                    for (int j = 1; j < 8; ++j) t = t + vel[i][j] * AT[kk][j];
+                    HIA[i][kk] = t;
+                }
+            const double r43 = 4.0 / 3.0;
+            const double r1s8 = 1.0 / sqrt(8.0);
+            const double DR = M.c_dr * (r43 * G + M.K) * 0.1 * nx2 * Vc * r1s8 * dt1;
+            const double CR = M.c_cr * M.rho * V0 / Vc * E.cbrt_v0sq[e] * M.wos / 4.0;
+            double Q[3][4];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk) {
+                    Q[i][kk] = qia[(4 * i + kk) * ep + e] + DR * HIA[i][kk];
+                    if (!INIT) qia[(4 * i + kk) * ep + e] = Q[i][kk];
+                }
+            // bulk viscosity pressure (:1073-1109)
+            const bool visc = !(fabs(vr) < 1.0e-10);
+            double pv = 0.0;
+            if (visc) {
+                const double rho_c = M.rho / J;
+                const double l0 = E.cbrt_v0[e];
+                const double m0 = vr < 0.0 ? vr : 0.0;
+                pv = rho_c * l0 * (M.cvisq * M.cvisq * l0 * vr * m0 - M.cvisl * M.wos * vr);
+                e_vis += -(pv * Vc * vr) * dt1;
+            }
+            // nodal forces: f = ((0 - b^T sigma V) - hourglass) + viscosity
+            double hpow = 0.0;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const double b0 = __ldg(bt + (3 * j) * ep + e), b1 = __ldg(bt + (3 * j + 1) * ep + e),
+                             b2 = __ldg(bt + (3 * j + 2) * ep + e);
+                double bj[3];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) bj[c] = (b0 * Fi[0][c] + b1 * Fi[1][c]) + b2 * Fi[2][c];
+                double fj[3];
+                fj[0] = 0.0 - ((bj[0] * s[0] + bj[1] * s[3]) + bj[2] * s[4]) * Vc;
+                fj[1] = 0.0 - ((bj[0] * s[3] + bj[1] * s[1]) + bj[2] * s[5]) * Vc;
+                fj[2] = 0.0 - ((bj[0] * s[4] + bj[1] * s[5]) + bj[2] * s[2]) * Vc;
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    double hgs = 0.0;
+#pragma unroll
+                    for (int kk = 0; kk < 4; ++kk) hgs = hgs + Q[i][kk] * AT[kk][j];
+                    const double hgd = (AT[0][j] * HIA[i][0] + AT[1][j] * HIA[i][1]) +
+                                       (AT[2][j] * HIA[i][2] + AT[3][j] * HIA[i][3]);
+                    const double h = hgs + hgd * CR;
+                    fj[i] = fj[i] - h;
+                    hpow = hpow + h * vel[i][j];
+                    if (visc) fj[i] = fj[i] + pv * bj[i] * Vc;
+                    fe[(3 * j + i) * ep + e] = fj[i];
+                }
+            }
+            e_hg += hpow * dt1;
+            // compute_dtStable (:828-834)
+            {
+                const double cd = M.wos;
+                const double m0 = vr < 0.0 ? vr : 0.0;
+                const double xi = M.cvisl - M.cvisq * M.cvisq * len / cd * m0;
+                dts = (sqrt(1.0 + xi * xi) - xi) * len / cd;
+            }
+            if (!(J > 0.0) || !isfinite(dts)) bad |= (isfinite(dts) ? 0 : ST_NONFINITE);
+        }
+        dts_min = dts < dts_min ? dts : dts_min;
+        len_min = len < len_min ? len : len_min;
+    }
+    if (bad) atomicOr(&ctl->status, bad);
+    block_min2<kElemThreads>(dts_min, len_min, &ctl->dts_next, &ctl->len_min);
+    if (!INIT) {
+        double v3[3] = {e_int, e_hg, e_vis};
+        block_sum<kElemThreads, 3>(v3, P.elem, P.n_elem_blocks, blockIdx.x);
+    }
+}
+
+// Node pass: gather of the element forces in slot order (the reference's
+// ((((((a0+a1)+a2)+a3)+a4)+a5)+a6)+a7, exDyna3D.cpp:638-639), gravity
+// (:819-824), boundary conditions on a (:2029-2145), a = f M^-1 (:642-644),
+// v += (dt_i + dt_i_1) a / 2, u += dt_i v, x += dt_i v (:646-654, :688-696).
+__global__ void __launch_bounds__(kNodeThreads) k_node(ElemArrays E, NodeArrays N, Material M, Ctl* ctl, Partials P) {
+    if (ctl->done) return;
+    // stable dt of this cycle (update_minVertex_perMaterial_and_dt :673-679)
+    double dt_i;
+    const double dt_i_1 = ctl->dt_i_1;
+    if (ctl->dt_final) {
+        dt_i = ctl->dt_i;
+    } else {
+        const double lmin = bits_ord(ctl->len_min);
+        double d = lmin / ctl->wos;
+        const double tmp = ctl->dts_cur;
+        d = d < tmp ? d : tmp;
+        dt_i = d * ctl->factor;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (!ctl->dt_final) ctl->dt_i = dt_i;
+        ctl->cycles_done += 1;
+        ctl->energy_pending = 1;
+    }
+    const int64_t nn = N.nn, np = N.nn_pad, ep = E.ne_pad;
+    const double* __restrict__ fe = static_cast<const double*>(E.fe);
+    double* __restrict__ V = static_cast<double*>(N.v);
+    const double half = (dt_i + dt_i_1);
+    const double dt_avg = (dt_i + dt_i_1) / 2.0;
+    double kin = 0.0, wext = 0.0;
+    int32_t bad = 0;
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    for (int64_t n = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; n < nn; n += stride) {
+        double f[3];
+        if (N.csr_ptr == nullptr) {
+            f[0] = f[1] = f[2] = 0.0;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const uint32_t el = __ldg(N.ell + k * np + n);
+                if (el != ENSC_NONE) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) f[c] = f[c] + fe[(3 * k + c) * ep + el];
+                }
+            }
+        } else {
+            // general lists: entries sorted by (slot, element); each slot's
+            // contributions are summed first (the reference's per-slot +=
+            // in element order), then added to the running total
+            f[0] = f[1] = f[2] = 0.0;
+            const int64_t b = N.csr_ptr[n], t = N.csr_ptr[n + 1];
+            int cur = -1;
+            double sl[3] = {0.0, 0.0, 0.0};
+            for (int64_t i = b; i < t; ++i) {
+                const uint32_t ent = N.csr_ent[i];
+                const int k = static_cast<int>(ent & 7u);
+                const uint32_t el = ent >> 3;
+                if (k != cur) {
+                    if (cur >= 0) {
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) f[c] = f[c] + sl[c];
+                    }
+                    cur = k;
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) sl[c] = 0.0 + fe[(3 * k + c) * ep + el];
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) sl[c] = sl[c] + fe[(3 * k + c) * ep + el];
+                }
+            }
+            if (cur >= 0) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) f[c] = f[c] + sl[c];
+            }
+        }
+        const double im = N.inv_mass[n];
+        const uint32_t code = N.bc[n];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            double a = f[c];
+            double g = 0.0;
+            if (M.gravity_on) {
+                g = 1.0 * M.gravity_value * M.gravity_dir[c] / im;
+                a = a + g;
+            }
+            const uint32_t cc = (code >> (2 * c)) & 3u;
+            double r = 0.0, rf = 0.0;
+            if (cc & 2u) {
+                r = -a;
+                a = 0.0;
+            }
+            if ((cc & 1u) && a != 0.0) {
+                rf = -a;
+                r = -a;
+                a = 0.0;
+            }
+            if (cc) N.rf[c * np + n] = rf;
+            a = a * im;
+            const double vo = V[c * np + n];
+            const double vn = vo + half * a / 2.0;
+            V[c * np + n] = vn;
+            N.u[c * np + n] = N.u[c * np + n] + dt_i * vn;
+            N.x[c * np + n] = N.x[c * np + n] + dt_i * vn;
+            const double vb = 0.5 * (vo + vn);
+            wext = wext + (g + r) * dt_avg * vb;
+            kin = kin + 0.5 * (vn * vn) / im;
+            if (!isfinite(vn)) bad |= ST_NONFINITE;
+        }
+    }
+    if (bad) atomicOr(&ctl->status, bad);
+    double v2[2] = {kin, wext};
+    block_sum<kNodeThreads, 2>(v2, P.node, P.n_node_blocks, blockIdx.x);
+}
+
+}  // namespace
+
+void launch_element_fp64(const ElemArrays& E, const NodeArrays& N, const Material& M, Ctl* ctl, const Partials& P,
+                         int grid, bool init, cudaStream_t st) {
+    if (M.plastic) {
+        if (init) k_element<true, true><<<grid, kElemThreads, 0, st>>>(E, N, M, ctl, P);
+        else k_element<true, false><<<grid, kElemThreads, 0, st>>>(E, N, M, ctl, P);
+    } else {
+        if (init) k_element<false, true><<<grid, kElemThreads, 0, st>>>(E, N, M, ctl, P);
+        else k_element<false, false><<<grid, kElemThreads, 0, st>>>(E, N, M, ctl, P);
+    }
+}
+
+void launch_node_fp64(const ElemArrays& E, const NodeArrays& N, const Material& M, Ctl* ctl, const Partials& P,
+                      int grid, cudaStream_t st) {
+    k_node<<<grid, kNodeThreads, 0, st>>>(E, N, M, ctl, P);
+}
+
+int occupancy_element_fp64(bool plastic) {
+    int nb = 0;
+    if (plastic) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element<true, false>, kElemThreads, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element<false, false>, kElemThreads, 0);
+    return nb;
+}
+
+int occupancy_node_fp64() {
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_node, kNodeThreads, 0);
+    return nb;
+}
+
+}  // namespace ensc

@@ -1,0 +1,36 @@
+// Internal launcher declarations shared by the kernel translation units and
+// the C-ABI implementation (ensc_capi.cu).  Not installed; not part of the ABI.
+#pragma once
+
+#include "ensc_device.cuh"
+
+namespace ensc {
+
+constexpr int kElemThreads = 128;
+constexpr int kNodeThreads = 256;
+constexpr int kCtlThreads = 256;
+
+// FP64 (ensc_fp64.cu, built with -fmad=false)
+void launch_element_fp64(const ElemArrays& E, const NodeArrays& N, const Material& M, Ctl* ctl, const Partials& P,
+                         int grid, bool init, cudaStream_t st);
+void launch_node_fp64(const ElemArrays& E, const NodeArrays& N, const Material& M, Ctl* ctl, const Partials& P,
+                      int grid, cudaStream_t st);
+int occupancy_element_fp64(bool plastic);
+int occupancy_node_fp64();
+
+// control (ensc_control.cu, built with -fmad=false)
+// mode 0: fold energy partials + begin next cycle; 1: fold only; 2: fold as initial KE
+void launch_between(Ctl* ctl, const Partials& P, int mode, cudaStream_t st);
+void launch_edge_prepass(const ElemArrays& E, const NodeArrays& N, Ctl* ctl, int grid, cudaStream_t st);
+void launch_begin_exact(Ctl* ctl, cudaStream_t st);
+void launch_arm(Ctl* ctl, double step_end, long long max_cycles, cudaStream_t st);
+void launch_apply_bc_v(const NodeArrays& N, bool fp32_v, cudaStream_t st);
+void launch_reset_init(Ctl* ctl, cudaStream_t st);
+void launch_kinetic0(const NodeArrays& N, const Partials& P, Ctl* ctl, bool fp32_v, int grid, cudaStream_t st);
+// layout conversion between caller AoS arrays and device SoA arrays
+void launch_soa_to_aos(const void* soa, int64_t n, int64_t pad, int comps, bool src_fp32, double* aos,
+                       cudaStream_t st);
+void launch_aos_to_soa(const double* aos, int64_t n, int64_t pad, int comps, void* soa, bool dst_fp32,
+                       cudaStream_t st);
+
+}  // namespace ensc

@@ -1,0 +1,127 @@
+"""Synthetic solve problems with the shapes, materials and boundary conditions
+of the measured workloads (there is no public dataset for this solver; the
+reference ships only hand-run Abaqus decks).
+
+Each builder returns a ``Problem``: mesh arrays, initial velocity, per-DOF BC
+arrays, material and controls, plus the node sets needed to write the same
+model as an ``.inp`` deck for the reference CPU stepper.
+"""
+from __future__ import annotations
+
+import dataclasses
+from typing import Dict, List, Optional, Tuple
+
+import numpy as np
+
+from . import mesh as M
+
+
+@dataclasses.dataclass
+class Problem:
+    name: str
+    mesh: M.Mesh
+    v0: np.ndarray                     # (n_nodes, 3)
+    bc_code: np.ndarray                # (3*n_nodes,) int8
+    bc_value: np.ndarray               # (3*n_nodes,) float64
+    material: M.Material
+    controls: M.Controls
+    cycles: int                        # cycles of the measured run
+    end_time: Optional[float] = None   # run-to-time workloads
+    fixed_sets: List[Tuple[str, str]] = dataclasses.field(default_factory=list)
+    initial_velocity: List[Tuple[str, int, float]] = dataclasses.field(default_factory=list)
+    per_node_velocity: bool = False
+
+    def write_deck(self, dirpath: str, deck: str = "model.inp", period: Optional[float] = None) -> str:
+        """Writes deck + project.txt for the reference stepper; returns the deck name."""
+        import os
+        per = period if period is not None else (self.end_time or self.controls.total_time)
+        M.write_deck(os.path.join(dirpath, deck), self.mesh, self.material, period=per,
+                     fixed_sets=self.fixed_sets, initial_velocity=self.initial_velocity,
+                     node_velocities=self.v0 if self.per_node_velocity else None,
+                     bulk_viscosity=(self.controls.cvisl, self.controls.cvisq), gravity=self.controls.gravity)
+        M.write_project(dirpath, deck, self.controls)
+        return deck
+
+
+DEFAULT_CONTROLS = dict(c_dr=0.013, c_cr=0.1, factor=0.9, cvisl=0.06, cvisq=1.2)
+
+
+def cantilever(nx: int = 20, ny: int = 4, nz: int = 4, lx: float = 2.0, ly: float = 0.4, lz: float = 0.4,
+               vz: float = 5.0, cycles: int = 2000, E: float = 210e9, nu: float = 0.3, rho: float = 7850.0,
+               yield_stress: float = 0.0, tangent: float = 0.0) -> Problem:
+    """Cantilever block: x = 0 face fixed (PINNED), all other nodes start with
+    vz; the 20x4x4 default is the reference-runnable parity case (320
+    elements, 525 nodes, 2000 cycles, FP64)."""
+    m = M.box_mesh(nx, ny, nz, lx, ly, lz)
+    fix = M.face_nodes(m, 0, "min")
+    free = np.setdiff1d(np.arange(m.n_nodes), fix)
+    m.node_sets = {"Set-1": fix, "Set-2": free}
+    v0 = np.zeros((m.n_nodes, 3))
+    v0[free, 2] = vz
+    code, val = M.bc_arrays(m.n_nodes, fixed=[(fix, 0, 2)])
+    ctl = M.Controls(total_time=1.0, **DEFAULT_CONTROLS)
+    return Problem("cantilever_%dx%dx%d" % (nx, ny, nz), m, v0, code, val,
+                   M.Material(E, nu, rho, yield_stress, tangent), ctl, cycles,
+                   fixed_sets=[("Set-1", "PINNED")], initial_velocity=[("Set-2", 3, vz)])
+
+
+def smoothed_gaussian_velocity(dims: Tuple[int, int, int], std: float, seed: int, passes: int = 3) -> np.ndarray:
+    """Per-node, per-component N(0, std) velocities on an (nx+1, ny+1, nz+1)
+    node lattice, smoothed by ``passes`` Jacobi sweeps (each value replaced by
+    the mean over itself and its existing face neighbours)."""
+    nx, ny, nz = dims
+    rng = np.random.default_rng(seed)
+    v = rng.normal(0.0, std, size=(nz + 1, ny + 1, nx + 1, 3))
+    for _ in range(passes):
+        s = v.copy()
+        cnt = np.ones(v.shape[:3] + (1,))
+        for ax in range(3):
+            lo = [slice(None)] * 4
+            hi = [slice(None)] * 4
+            lo[ax] = slice(0, -1)
+            hi[ax] = slice(1, None)
+            s[tuple(lo)] += v[tuple(hi)]
+            s[tuple(hi)] += v[tuple(lo)]
+            cnt[tuple(lo)] += 1
+            cnt[tuple(hi)] += 1
+        v = s / cnt
+    return v.reshape(-1, 3)
+
+
+def block(nx: int = 256, ny: int = 128, nz: int = 64, lx: float = 1.0, ly: float = 0.5, lz: float = 0.25,
+          cycles: int = 5000, seed: int = 20241203, plastic: bool = True) -> Problem:
+    """Large elastic-plastic block (roofline workload): 256x128x64 hexahedra
+    (2,097,152 elements, 2,154,945 nodes) over 1.0 x 0.5 x 0.25 m, J2 with
+    E = 70 GPa, nu = 0.33, rho = 2700, yield 250 MPa and a 100 MPa tangent
+    modulus; bottom face (z = 0) fixed; seeded Gaussian nodal velocities
+    (std 2 m/s) smoothed by 3 Jacobi passes; 5000 cycles."""
+    m = M.box_mesh(nx, ny, nz, lx, ly, lz)
+    fix = M.face_nodes(m, 2, "min")
+    m.node_sets = {"Set-1": fix}
+    v0 = smoothed_gaussian_velocity((nx, ny, nz), 2.0, seed)
+    v0[fix] = 0.0
+    code, val = M.bc_arrays(m.n_nodes, fixed=[(fix, 0, 2)])
+    mat = M.Material(70e9, 0.33, 2700.0, 250e6 if plastic else 0.0, 100e6 if plastic else 0.0)
+    ctl = M.Controls(total_time=1.0, **DEFAULT_CONTROLS)
+    return Problem("block_%dx%dx%d" % (nx, ny, nz), m, v0, code, val, mat, ctl, cycles,
+                   fixed_sets=[("Set-1", "ENCASTRE")], per_node_velocity=True)
+
+
+def impact_bar(n_core: int = 12, n_ring: int = 6, n_layers: int = 120, radius: float = 3.2e-3,
+               length: float = 32.4e-3, v_impact: float = -190.0, end_time: float = 80e-6,
+               plastic: bool = True) -> Problem:
+    """Taylor-type impact bar: butterfly-meshed copper cylinder (r = 3.2 mm,
+    L = 32.4 mm) with J2 (E 117 GPa, nu 0.35, rho 8930, yield 400 MPa,
+    tangent 100 MPa), z = 0 face fixed in z only, all nodes at vz = -190 m/s,
+    run to 80 us."""
+    m = M.butterfly_cylinder(radius, length, n_core, n_ring, n_layers)
+    bot = M.face_nodes(m, 2, "min")
+    allnodes = np.arange(m.n_nodes)
+    m.node_sets = {"Set-1": bot, "Set-2": allnodes}
+    v0 = np.zeros((m.n_nodes, 3))
+    v0[:, 2] = v_impact
+    code, val = M.bc_arrays(m.n_nodes, fixed=[(bot, 2, 2)])
+    mat = M.Material(117e9, 0.35, 8930.0, 400e6 if plastic else 0.0, 100e6 if plastic else 0.0)
+    ctl = M.Controls(total_time=end_time, **DEFAULT_CONTROLS)
+    return Problem("impact_bar", m, v0, code, val, mat, ctl, cycles=0, end_time=end_time,
+                   fixed_sets=[("Set-1", "3, 3")], initial_velocity=[("Set-2", 3, v_impact)])

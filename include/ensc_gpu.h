@@ -1,0 +1,199 @@
+/* EnSCDynamics-B200: C ABI of the GPU explicit central-difference stepper.
+ *
+ * This is the drop-in boundary for the reference solver's time-step loop
+ * (EnSC::exDyna3D::run, Explicit3D/source/exDyna3D.cpp:54-102).  A host
+ * program that has read a deck with the reference reader hands the mesh,
+ * material, controls and boundary conditions to ensc_create/ensc_set_bcs and
+ * advances the solution with ensc_step; ensc_download copies the state back
+ * into the reference's own arrays.  All entry points use plain pointers and
+ * sizes; no C++ or torch types cross the boundary.
+ *
+ * Conventions
+ *   - Nodal vectors are interleaved xyz per node, float64, as the reference's
+ *     solution_u / solution_v (exDyna3D.h:159-160) and vertices
+ *     (exDyna3D.h:141, std::array<double,3> per node).
+ *   - Connectivity is 8 x uint32 per element, 0-based, in the reference's
+ *     local node order (Element_HexN8.cpp:49-91; ElementBase.h:110).
+ *   - Stress is [xx, yy, zz, xy, xz, yz] per element (all_sigma,
+ *     exDyna3D.h:146); hourglass history is 12 doubles per element (all_QIA,
+ *     exDyna3D.h:148).
+ *   - Every call returns 0 on success or a negative ENSC_ERR_* code; the
+ *     library never calls exit() and throws nothing across the ABI.
+ *   - There is no global mutable state: one handle per solve, each on its own
+ *     CUDA stream.  Calls on one handle are not thread-safe; separate handles
+ *     are independent.
+ *   - The caller owns all host arrays; the library copies them and keeps no
+ *     host pointer after a call returns.
+ */
+#ifndef ENSC_GPU_H
+#define ENSC_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ENSC_ABI_VERSION 1
+
+/* return codes */
+#define ENSC_OK 0
+#define ENSC_ERR_ARG (-1)          /* invalid argument / size */
+#define ENSC_ERR_OOM (-2)          /* device allocation failed or budget exceeded */
+#define ENSC_ERR_CUDA (-3)         /* CUDA runtime error */
+#define ENSC_ERR_NONFINITE (-4)    /* non-finite nodal state detected */
+#define ENSC_ERR_INVERTED (-5)     /* element with J <= 0 detected */
+#define ENSC_ERR_TIMEOUT (-6)      /* a bounded device wait expired */
+#define ENSC_ERR_NODEVICE (-7)     /* no usable CUDA device */
+
+/* precision of the stepper */
+#define ENSC_FP64 0     /* plain FP64, operation order of the reference */
+#define ENSC_MIXED 1    /* FP32 element work and gather; FP64 x, u, time, dt, energy */
+
+/* BC code bits per DOF, as resolved by apply_boundary_condition_vec /
+ * apply_boundary_condition_a (exDyna3D.cpp:379-490, 2029-2145) */
+#define ENSC_BC_FIXED 1      /* SPC: v := 0, a := 0, reaction recorded */
+#define ENSC_BC_VELOCITY 2   /* prescribed velocity: v := value, a := 0 */
+
+typedef struct ensc_handle ensc_handle;
+
+/* Mesh and initial state.  Replaces the reference's vertices,
+ * hexahedron_elements and solution_v after apply_initial_condition
+ * (exDyna3D.h:141-142,160; exDyna3D.cpp:338-377). */
+typedef struct {
+    int64_t n_nodes;
+    int64_t n_elements;
+    const uint32_t* conn;   /* [n_elements*8] */
+    const double* x0;       /* [n_nodes*3] reference coordinates */
+    const double* v0;       /* [n_nodes*3] initial velocity, or NULL for zero */
+    /* Optional precomputed element constants.  When NULL they are computed
+     * as compute_invMassMatrix does (exDyna3D.cpp:492-515); a drop-in caller
+     * that already ran the reference's init() passes its all_BT (row-major
+     * 8x3 per element), all_Volume and inv_mass_matrix (per DOF). */
+    const double* bt;       /* [n_elements*24] or NULL */
+    const double* vol0;     /* [n_elements] or NULL */
+    const double* inv_mass; /* [n_nodes*3] or NULL */
+} ensc_mesh_desc;
+
+/* Material_elastic (Material_elastic.h:8-21) plus J2 plasticity, which the
+ * reference does not have: yield_stress <= 0 selects the reference's
+ * hypoelastic update unchanged. */
+typedef struct {
+    double E, nu, rho;
+    double yield_stress;       /* initial yield stress; <= 0: elastic */
+    double hardening_modulus;  /* linear isotropic hardening H = E*Et/(E-Et) */
+} ensc_material;
+
+/* Solver controls: exDyna3D members c_dr, c_cr, factor_timeStep, Cvisl,
+ * Cvisq, totalTime (exDyna3D.h:176-185) and the current step's gravity
+ * (StepData::gravity, StepData.h:22; amplitude 1). */
+typedef struct {
+    double c_dr, c_cr, factor_timestep, cvisl, cvisq;
+    double total_time;
+    int32_t gravity_on;
+    double gravity_value;
+    double gravity_dir[3];
+    int32_t precision;      /* ENSC_FP64 or ENSC_MIXED */
+    int32_t device;         /* CUDA device ordinal */
+    void* stream;           /* cudaStream_t to run on, or NULL for a private stream */
+    int32_t graph_chunk;    /* cycles per captured CUDA graph; 0 = default */
+} ensc_params;
+
+typedef struct {
+    double time;            /* exDyna3D::time */
+    double dt_i;            /* exDyna3D::dt_i */
+    double dt_i_1;          /* exDyna3D::dt_i_1 */
+    int64_t cycles;         /* cycles run by this call */
+    int64_t total_cycles;   /* cycles since ensc_create */
+    int32_t status;         /* 0 or the ENSC_ERR_* that stopped stepping */
+    int32_t done;           /* 1 when time reached step_end */
+    double dt_stable_min;   /* min of dtStable (exDyna3D.h:206) over the last
+                               force pass; seeds the next cycle's dt */
+} ensc_step_report;
+
+typedef struct {
+    double kinetic;         /* 1/2 sum m v^2 at the last half step */
+    double internal;        /* accumulated stress work */
+    double hourglass;       /* accumulated hourglass work */
+    double viscous;         /* accumulated bulk-viscosity work */
+    double external;        /* accumulated work of gravity and reactions */
+    double kinetic0;        /* kinetic energy after the first ensc_set_bcs */
+} ensc_energy_report;
+
+int ensc_abi_version(void);
+
+/* Creates a solver instance: exDyna3D::init() (exDyna3D.cpp:105-142) --
+ * element constants and lumped mass, then the init force pass with dt = 0
+ * that seeds the stable time step -- on the device.  No boundary condition
+ * is active until ensc_set_bcs. */
+int ensc_create(const ensc_mesh_desc* mesh, const ensc_material* mat, const ensc_params* params,
+                ensc_handle** out);
+
+/* Activates a step's resolved boundary conditions (setCurrentStep,
+ * exDyna3D.cpp:1760-1940) and applies them to the velocity field at once, as
+ * setCurrentStep's call to apply_boundary_condition_vec does (:1911).
+ * dof_code/dof_value: [n_nodes*3]; dof_value is read where the code has
+ * ENSC_BC_VELOCITY.  NULL code clears all conditions. */
+int ensc_set_bcs(ensc_handle* h, const int8_t* dof_code, const double* dof_value);
+
+/* Changes the gravity load of the current step (apply_gravity,
+ * exDyna3D.cpp:800-826). */
+int ensc_set_gravity(ensc_handle* h, int32_t on, double value, const double dir[3]);
+
+/* Runs the body of run()'s step loop (exDyna3D.cpp:86-100) -- stable dt,
+ * last-step clamp, computeSate -- while time < step_end_time, at most
+ * max_cycles cycles.  Blocks until done; report may be NULL. */
+int ensc_step(ensc_handle* h, int64_t max_cycles, double step_end_time, ensc_step_report* report);
+
+/* Enqueues the same work without waiting (for callers that time the stream
+ * themselves); finish with ensc_sync. */
+int ensc_step_async(ensc_handle* h, int64_t max_cycles, double step_end_time);
+int ensc_sync(ensc_handle* h, ensc_step_report* report);
+
+/* Copies state to host arrays (any pointer may be NULL): x = vertices,
+ * u = solution_u, v = solution_v ([n_nodes*3]), sigma = all_sigma
+ * ([n_elements*6]), qia = all_QIA ([n_elements*12]), eps_p = equivalent
+ * plastic strain ([n_elements]). */
+int ensc_download(ensc_handle* h, double* x, double* u, double* v, double* sigma, double* qia,
+                  double* eps_p);
+
+/* Replaces the evolving state from host arrays (all [..] as in
+ * ensc_download; NULL leaves a field unchanged) and the clock.  Used to
+ * restart from a checkpoint: time, dt_i, dt_i_1 and dt_stable_min as reported
+ * by ensc_step at the checkpoint (dt_stable_min <= 0 keeps the current
+ * value). */
+int ensc_upload_state(ensc_handle* h, const double* x, const double* u, const double* v,
+                      const double* sigma, const double* qia, const double* eps_p, double time,
+                      double dt_i, double dt_i_1, double dt_stable_min);
+
+/* Energy sums (no counterpart in the reference). */
+int ensc_energy(ensc_handle* h, ensc_energy_report* out);
+
+/* Reaction forces at fixed DOFs of the last cycle (solution_rf,
+ * exDyna3D.h:164), [n_nodes*3]. */
+int ensc_download_reactions(ensc_handle* h, double* rf);
+
+/* Runs up to max_cycles cycles (same work as ensc_step, launched kernel by
+ * kernel instead of as a graph) with CUDA events around every kernel on the
+ * handle's stream, and returns each kernel's summed duration in milliseconds
+ * and launch count.  Kernel order: [0] cycle begin, [1] edge prepass,
+ * [2] exact-dt begin, [3] element pass, [4] node pass.  For measurement. */
+int ensc_profile(ensc_handle* h, int64_t max_cycles, double step_end_time, double ms[5], int64_t launches[5]);
+
+/* Device bytes held by the handle. */
+int64_t ensc_device_bytes(const ensc_handle* h);
+
+/* Number of kernel launches one cycle issues (for launch accounting). */
+int32_t ensc_kernels_per_cycle(const ensc_handle* h);
+
+void ensc_destroy(ensc_handle* h);
+
+/* Message of the last error on h (or of the last failed ensc_create on this
+ * thread when h is NULL). */
+const char* ensc_last_error(const ensc_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ENSC_GPU_H */

@@ -1,0 +1,63 @@
+"""Shared helpers for the tests: golden fixtures and solver construction."""
+import glob
+import json
+import os
+
+import numpy as np
+
+from enscdynamics_b200 import mesh as M
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+# FP64 parity bar against the reference CPU stepper (relative to the field's
+# max magnitude), as stated for the plain path.
+REL_TOL_REFERENCE = 1e-9
+
+
+def golden_names():
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
+
+
+def load_golden(name):
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    d = {k: z[k] for k in z.files}
+    d["meta"] = json.loads(str(d["meta"]))
+    return d
+
+
+def rel(a, b):
+    a = np.asarray(a, dtype=np.float64).reshape(-1)
+    b = np.asarray(b, dtype=np.float64).reshape(-1)
+    scale = np.abs(b).max()
+    if scale == 0.0:
+        return float(np.abs(a).max())
+    return float(np.abs(a - b).max() / scale)
+
+
+def material_controls(meta):
+    mat = M.Material(meta["E"], meta["nu"], meta["rho"], meta.get("yield", 0.0), meta.get("tangent", 0.0))
+    g = meta.get("gravity")
+    ctl = M.Controls(c_dr=meta["c_dr"], c_cr=meta["c_cr"], factor=meta["factor"], cvisl=meta["cvisl"],
+                     cvisq=meta["cvisq"], total_time=meta["total_time"],
+                     gravity=None if g is None else (g[0], tuple(g[1])))
+    return mat, ctl
+
+
+def oracle_for(g, setup_from_reference=False, **overrides):
+    import pyoracle
+    meta = dict(g["meta"])
+    meta.update(overrides)
+    setup = dict(bt=g["bt"], vol0=g["vol0"], inv_mass=g["inv_mass"]) if setup_from_reference else None
+    return pyoracle.Oracle(g["x0"], g["conn"], g["v0"], g["bc_code"], g["bc_value"], E=meta["E"], nu=meta["nu"],
+                           rho=meta["rho"], c_dr=meta["c_dr"], c_cr=meta["c_cr"], factor=meta["factor"],
+                           cvisl=meta["cvisl"], cvisq=meta["cvisq"], total_time=meta["total_time"],
+                           yield0=meta.get("yield", 0.0), hardening=meta.get("hardening", 0.0),
+                           gravity=None if meta.get("gravity") is None else (meta["gravity"][0], meta["gravity"][1]),
+                           setup=setup)
+
+
+def run_len(g):
+    meta = g["meta"]
+    if meta["mode"] == "full":
+        return 10 ** 9, meta["step_end"]
+    return meta["cycles"], float("inf")

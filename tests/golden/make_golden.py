@@ -1,0 +1,156 @@
+"""Generates the golden fixtures in this directory by running the reference
+CPU stepper (compiled from the reference sources into oracle/_ref by
+oracle/Makefile) on decks written by enscdynamics_b200.mesh.
+
+Run in a container that has the reference checkout (REF, default
+/root/reference):
+
+    make -C oracle && python tests/golden/make_golden.py
+
+Each fixture stores the model in array form (x0, conn, v0, BC arrays,
+material, controls) and the reference's state after the run (u, v, x, sigma,
+QIA, time, dt_i, dt_i_1, reactions).  Fixtures are small (<= a few hundred
+elements) so the CPU restatement and the GPU stepper can be checked against
+them anywhere, without the reference.
+"""
+from __future__ import annotations
+
+import itertools
+import json
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+from enscdynamics_b200 import mesh as M  # noqa: E402
+from enscdynamics_b200 import workloads as W  # noqa: E402
+import pyoracle  # noqa: E402
+
+
+def cases():
+    out = []
+    # 1. the reference-runnable cantilever, 2000 cycles
+    p = W.cantilever()
+    out.append(("cantilever_20x4x4", p, "cycles", 2000))
+    # 2. single element: bottom fixed, prescribed velocity on the top face
+    m = M.box_mesh(1, 1, 1, 0.1, 0.1, 0.1)
+    bot = M.face_nodes(m, 2, "min")
+    top = M.face_nodes(m, 2, "max")
+    m.node_sets = {"Set-1": bot, "Set-2": top}
+    code, val = M.bc_arrays(m.n_nodes, fixed=[(bot, 0, 2)], velocity=[(top, 2, 2, -2.0)])
+    p = W.Problem("single_element_velbc", m, np.zeros((m.n_nodes, 3)), code, val,
+                  M.Material(200e9, 0.3, 7800.0), M.Controls(total_time=1.0, **W.DEFAULT_CONTROLS), 400,
+                  fixed_sets=[("Set-1", "ENCASTRE")])
+    p.velocity_sets = [("Set-2", 3, 3, -2.0)]
+    out.append(("single_element_velbc", p, "cycles", 400))
+    # 3. gravity-loaded cantilever with an initial velocity field
+    p = W.cantilever(6, 2, 2, 0.6, 0.2, 0.2, vz=0.5)
+    p.controls = M.Controls(total_time=1.0, gravity=(9.81, (0.0, 0.0, -1.0)), **W.DEFAULT_CONTROLS)
+    out.append(("gravity_6x2x2", p, "cycles", 600))
+    # 4. run to end time through exDyna3D::run() itself (last-step and
+    #    total-time clamps fire in the final cycles)
+    p = W.cantilever(4, 2, 2, 0.4, 0.2, 0.2, vz=3.0)
+    p.controls = M.Controls(total_time=3.3e-4, **W.DEFAULT_CONTROLS)
+    p.end_time = 3.3e-4
+    out.append(("run_to_time_4x2x2", p, "full", None))
+    # 5. slot clashes: elements with rotated local numbering so a node sits
+    #    in the same local slot of two elements
+    out.append(("slot_clash_2x2x1", clash_problem(), "cycles", 300))
+    return out
+
+
+def _rotations():
+    """The 24 proper rotations of the reference hexahedron as node permutations."""
+    xi = np.array([[-1, -1, -1], [1, -1, -1], [1, 1, -1], [-1, 1, -1],
+                   [-1, -1, 1], [1, -1, 1], [1, 1, 1], [-1, 1, 1]])
+    perms = []
+    for P in itertools.permutations(range(3)):
+        for s in itertools.product((-1, 1), repeat=3):
+            R = np.zeros((3, 3), dtype=int)
+            for i in range(3):
+                R[i, P[i]] = s[i]
+            if round(np.linalg.det(R)) != 1:
+                continue
+            img = xi @ R.T
+            perm = [int(np.nonzero((xi == img[k]).all(axis=1))[0][0]) for k in range(8)]
+            perms.append(perm)
+    return perms
+
+
+def clash_problem():
+    m = M.box_mesh(2, 2, 1, 0.2, 0.2, 0.1)
+    rots = _rotations()
+    rng = np.random.default_rng(7)
+    base = m.conn.copy()
+    for _ in range(1000):
+        conn = np.stack([base[e][rots[rng.integers(len(rots))]] for e in range(base.shape[0])]).astype(np.uint32)
+        if M.check_slot_clashes(conn, m.n_nodes) > 0:
+            break
+    m.conn = conn
+    bot = M.face_nodes(m, 2, "min")
+    free = np.setdiff1d(np.arange(m.n_nodes), bot)
+    m.node_sets = {"Set-1": bot, "Set-2": free}
+    v0 = np.zeros((m.n_nodes, 3))
+    v0[free, 0] = 1.5
+    code, val = M.bc_arrays(m.n_nodes, fixed=[(bot, 0, 2)])
+    return W.Problem("slot_clash_2x2x1", m, v0, code, val, M.Material(70e9, 0.33, 2700.0),
+                     M.Controls(total_time=1.0, **W.DEFAULT_CONTROLS), 300,
+                     fixed_sets=[("Set-1", "PINNED")], initial_velocity=[("Set-2", 1, 1.5)])
+
+
+def write_case_deck(p, d):
+    deck = "model.inp"
+    per = p.end_time if p.end_time else p.controls.total_time
+    M.write_deck(os.path.join(d, deck), p.mesh, p.material, period=per, fixed_sets=p.fixed_sets,
+                 initial_velocity=p.initial_velocity, bulk_viscosity=(p.controls.cvisl, p.controls.cvisq),
+                 gravity=p.controls.gravity)
+    vel = getattr(p, "velocity_sets", [])
+    if vel:  # velocity conditions go inside the step: the reference does not
+        # carry Initial-step velocity conditions into step 1 (exDyna3D.cpp:1859-1880)
+        txt = open(os.path.join(d, deck)).read()
+        block = "".join(f"*Boundary, type=VELOCITY\n{n}, {a}, {b}, {v!r}\n" for n, a, b, v in vel)
+        txt = txt.replace("*End Step", block + "*End Step", 1)
+        open(os.path.join(d, deck), "w").write(txt)
+    M.write_project(d, deck, p.controls)
+    return deck
+
+
+def main():
+    assert pyoracle.harness_available(), "build the reference harness first: make -C oracle"
+    index = {}
+    for name, p, mode, cycles in cases():
+        with tempfile.TemporaryDirectory() as d:
+            deck = write_case_deck(p, d)
+            pyoracle.run_reference(d, deck, "setup", dump=os.path.join(d, "s.bin"))
+            s = pyoracle.read_dump(os.path.join(d, "s.bin"))
+            assert np.array_equal(s["conn"], p.mesh.conn), name
+            assert np.array_equal(s["x"], p.mesh.x0), name
+            assert np.array_equal(s["bc_code"], p.bc_code), name
+            assert np.array_equal(s["bc_value"], p.bc_value), name
+            info = pyoracle.run_reference(d, deck, mode, cycles, dump=os.path.join(d, "o.bin"))
+            r = pyoracle.read_dump(os.path.join(d, "o.bin"))
+        c = p.controls
+        meta = dict(E=p.material.E, nu=p.material.nu, rho=p.material.rho, c_dr=c.c_dr, c_cr=c.c_cr,
+                    factor=c.factor, cvisl=c.cvisl, cvisq=c.cvisq, total_time=c.total_time,
+                    gravity=c.gravity, mode=mode, cycles=int(r["cycles"]),
+                    step_end=(p.end_time if mode == "full" else None))
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), x0=p.mesh.x0, conn=p.mesh.conn, v0=p.v0,
+                            bc_code=p.bc_code, bc_value=p.bc_value, bt=s["bt"], vol0=s["vol0"],
+                            inv_mass=s["inv_mass"], u=r["u"], v=r["v"], x=r["x"], sigma=r["sigma"],
+                            qia=r["qia"], rf=r["rf"],
+                            clock=np.array([r["time"], r["dt_i"], r["dt_i_1"]]),
+                            meta=np.array(json.dumps(meta)))
+        index[name] = meta
+        print(name, info)
+    with open(os.path.join(HERE, "index.json"), "w") as f:
+        json.dump(index, f, indent=1, sort_keys=True)
+
+
+if __name__ == "__main__":
+    main()
