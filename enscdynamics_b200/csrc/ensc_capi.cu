@@ -192,6 +192,7 @@ int read_ctl(ensc_handle* h) {
 int status_code(ensc_handle* h, int32_t st) {
     if (st & ensc::ST_NONFINITE) return set_err(h, ENSC_ERR_NONFINITE, "non-finite nodal state detected");
     if (st & ensc::ST_INVERTED) return set_err(h, ENSC_ERR_INVERTED, "element with J <= 0 detected");
+    if (st & ensc::ST_BAD_DT) return set_err(h, ENSC_ERR_NONFINITE, "stable time step is not positive");
     return ENSC_OK;
 }
 
@@ -203,7 +204,7 @@ void fill_report(const ensc_handle* h, int64_t before, ensc_step_report* r) {
     r->dt_i_1 = c.dt_i_1;
     r->cycles = c.cycles_done - before;
     r->total_cycles = c.cycles_done;
-    r->status = c.status ? (c.status & ensc::ST_NONFINITE ? ENSC_ERR_NONFINITE : ENSC_ERR_INVERTED) : 0;
+    r->status = c.status ? ((c.status & ensc::ST_INVERTED) ? ENSC_ERR_INVERTED : ENSC_ERR_NONFINITE) : 0;
     r->done = c.time < c.step_end ? 0 : 1;
     std::memcpy(&r->dt_stable_min, &c.dts_next, sizeof(double));
 }

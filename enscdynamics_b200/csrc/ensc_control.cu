@@ -55,7 +55,7 @@ __global__ void __launch_bounds__(kCtlThreads) k_between(Ctl* ctl, Partials P, i
         }
     }
     if (mode != 0 || threadIdx.x != 0 || ctl->done) return;
-    if (!(ctl->time < ctl->step_end) || ctl->cycles_done >= ctl->cycles_target) {
+    if (ctl->status || !(ctl->time < ctl->step_end) || ctl->cycles_done >= ctl->cycles_target) {
         ctl->done = 1;
         return;
     }

@@ -34,6 +34,7 @@ namespace ensc {
 enum : int32_t {
     ST_NONFINITE = 1,
     ST_INVERTED = 2,
+    ST_BAD_DT = 4,       // stable dt not positive and finite
 };
 
 // Per-instance control block: the scalar state of exDyna3D's time loop

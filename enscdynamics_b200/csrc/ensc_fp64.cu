@@ -434,6 +434,7 @@ __global__ void __launch_bounds__(kNodeThreads) k_node(ElemArrays E, NodeArrays 
         dt_i = d * ctl->factor;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (!(dt_i > 0.0) || !isfinite(dt_i)) atomicOr(&ctl->status, ST_BAD_DT);
         if (!ctl->dt_final) ctl->dt_i = dt_i;
         ctl->cycles_done += 1;
         ctl->energy_pending = 1;

@@ -59,5 +59,5 @@ def oracle_for(g, setup_from_reference=False, **overrides):
 def run_len(g):
     meta = g["meta"]
     if meta["mode"] == "full":
-        return 10 ** 9, meta["step_end"]
+        return 10 ** 6, meta["step_end"]
     return meta["cycles"], float("inf")
