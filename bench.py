@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["block", "cantilever"], default="block")
-    ap.add_argument("--precision", choices=["fp64"], default="fp64")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--cycles-per-step", type=int, default=500)
     ap.add_argument("--profile-cycles", type=int, default=40)
     ap.add_argument("--e2e-steps", type=int, default=3)
@@ -116,17 +116,24 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def element_pass_bytes(ne: int, nn: int, plastic: bool) -> int:
-    """Algorithmic bytes of one element-pass launch (FP64): connectivity 32,
-    sigma r/w 96, QIA r/w 192, B0^T 192, V0 8, element-force write 192 per
-    element (+16 eps_p r/w with J2), and the x, u, v gather counted once per
-    node (72 B)."""
+def element_pass_bytes(ne: int, nn: int, plastic: bool, mixed: bool = False) -> int:
+    """Algorithmic bytes of one element-pass launch.
+    FP64: connectivity 32, sigma r/w 96, QIA r/w 192, B0^T 192, V0 8,
+    element-force write 192 per element (+16 eps_p r/w with J2); x, u, v
+    gathered once per node (72 B).
+    Mixed: connectivity 32, sigma r/w 48, QIA r/w 96, B0^T 96, V0 4, force
+    write 96 (+8 eps_p); x, u FP64 and v FP32 per node (60 B)."""
+    if mixed:
+        return ne * (32 + 48 + 96 + 96 + 4 + 96 + (8 if plastic else 0)) + nn * 60
     return ne * (32 + 96 + 192 + 192 + 8 + 192 + (16 if plastic else 0)) + nn * 72
 
 
-def cycle_bytes(ne: int, nn: int, plastic: bool) -> int:
-    """Canonical algorithmic bytes of one cycle (FP64): 904 B per element
-    (+16 with J2) and 185 B per node."""
+def cycle_bytes(ne: int, nn: int, plastic: bool, mixed: bool = False) -> int:
+    """Canonical algorithmic bytes of one cycle: FP64 904 B per element (+16
+    with J2) and 185 B per node; mixed 468 B per element (+8) and 157 B per
+    node."""
+    if mixed:
+        return ne * (468 + (8 if plastic else 0)) + nn * 157
     return ne * (904 + (16 if plastic else 0)) + nn * 185
 
 
@@ -231,8 +238,9 @@ def run_ours(args):
     plastic = p.material.yield_stress > 0.0
     C = args.cycles_per_step
     stream = torch.cuda.Stream()
+    mixed = args.precision == "mixed"
     s = capi.Stepper(p.mesh.x0, p.mesh.conn, p.v0, material=p.material, controls=p.controls, device=local,
-                     stream=stream.cuda_stream)
+                     stream=stream.cuda_stream, precision=capi.MIXED if mixed else capi.FP64)
     s.set_bcs(p.bc_code, p.bc_value)
     kpc = s.kernels_per_cycle
 
@@ -273,11 +281,11 @@ def run_ours(args):
     nd = prof["node"]
     nd_ms = nd["ms"] / max(nd["launches"], 1)
     peak, peak_kind = measured_peaks()
-    el_bytes = element_pass_bytes(ne, nn, plastic)
+    el_bytes = element_pass_bytes(ne, nn, plastic, mixed)
     achieved = el_bytes / (el_ms / 1000.0) / 1e9
     total_ms = sum(v["ms"] for v in prof.values())
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "element_fp64_block_traffic.json")
+    tp = os.path.join(ROOT, "profiles", f"element_{args.precision}_block_traffic.json")
     if os.path.exists(tp):
         with open(tp) as f:
             traffic = json.load(f).get("bytes_per_launch")
@@ -330,18 +338,18 @@ def run_ours(args):
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "vs_baseline": None, "dtype": "f32+f64" if mixed else "f64", "data": "synthetic",
         "config": {"workload": "block 256x128x64 hex8 (2,097,152 el, 2,154,945 nodes), J2, 5000 cycles = 10 steps"
                    if args.workload == "block" else p.name,
-                   "elements": ne, "nodes": nn, "cycles_per_step": C, "precision": "fp64",
-                   "l2": f"inputs larger than L2 ({cycle_bytes(ne, nn, plastic) / 1e9:.2f} GB per cycle)",
+                   "elements": ne, "nodes": nn, "cycles_per_step": C, "precision": args.precision,
+                   "l2": f"inputs larger than L2 ({cycle_bytes(ne, nn, plastic, mixed) / 1e9:.2f} GB per cycle)",
                    "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "kernel": "element pass (k_element, FP64)",
+                     "traffic": traffic, "kernel": "element pass (%s)" % ("k_element_mixed" if mixed else "k_element, FP64"),
                      "peak_source": peak_kind, "kernel_ms": el_ms, "bytes_per_launch": el_bytes},
         # whole-cycle canonical bytes per GPU over the timed region
-        "cycle_roofline": {"bytes_per_cycle": cycle_bytes(ne, nn, plastic),
-                           "achieved_gbs": cycle_bytes(ne, nn, plastic) * C * args.steps / (ms_max / 1000.0) / 1e9,
+        "cycle_roofline": {"bytes_per_cycle": cycle_bytes(ne, nn, plastic, mixed),
+                           "achieved_gbs": cycle_bytes(ne, nn, plastic, mixed) * C * args.steps / (ms_max / 1000.0) / 1e9,
                            "frac": None},
         "kernel_share": {k: v["ms"] / total_ms for k, v in prof.items()},
         "node_pass_ms": nd_ms,

@@ -30,6 +30,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + INCLUD
 UNITS = [
     ("ensc_fp64.cu", ["-fmad=false"]),
     ("ensc_control.cu", ["-fmad=false"]),
+    ("ensc_mixed.cu", []),
     ("ensc_capi.cu", []),
 ]
 HEADERS = ["ensc_device.cuh", "ensc_kernels.h"]

@@ -161,6 +161,18 @@ std::vector<T> to_soa(const double* aos, int64_t n, int64_t pad, int comps) {
     return out;
 }
 
+bool mixed(const ensc_handle* h) { return h->precision == ENSC_MIXED; }
+
+void launch_element(ensc_handle* h, bool init, cudaStream_t st) {
+    if (mixed(h)) ensc::launch_element_mixed(h->E, h->N, h->M, h->ctl, h->P, h->grid_e, init, st);
+    else ensc::launch_element_fp64(h->E, h->N, h->M, h->ctl, h->P, h->grid_e, init, st);
+}
+
+void launch_node(ensc_handle* h, cudaStream_t st) {
+    if (mixed(h)) ensc::launch_node_mixed(h->E, h->N, h->M, h->ctl, h->P, h->grid_n, st);
+    else ensc::launch_node_fp64(h->E, h->N, h->M, h->ctl, h->P, h->grid_n, st);
+}
+
 int build_graph(ensc_handle* h) {
     if (h->graph) {
         cudaGraphExecDestroy(h->graph);
@@ -172,8 +184,8 @@ int build_graph(ensc_handle* h) {
         ensc::launch_between(h->ctl, h->P, 0, h->cap_stream);
         ensc::launch_edge_prepass(h->E, h->N, h->ctl, h->grid_e, h->cap_stream);
         ensc::launch_begin_exact(h->ctl, h->cap_stream);
-        ensc::launch_element_fp64(h->E, h->N, h->M, h->ctl, h->P, h->grid_e, false, h->cap_stream);
-        ensc::launch_node_fp64(h->E, h->N, h->M, h->ctl, h->P, h->grid_n, h->cap_stream);
+        launch_element(h, false, h->cap_stream);
+        launch_node(h, h->cap_stream);
     }
     cudaError_t e = cudaStreamEndCapture(h->cap_stream, &g);
     if (e != cudaSuccess) return cuda_err(h, "cudaStreamEndCapture", e);
@@ -226,7 +238,7 @@ int ensc_create(const ensc_mesh_desc* mesh, const ensc_material* mat, const ensc
         return set_err(nullptr, ENSC_ERR_ARG, "empty mesh or missing conn/x0");
     if (mesh->n_nodes >= (int64_t(1) << 32) - 1 || mesh->n_elements >= (int64_t(1) << 29))
         return set_err(nullptr, ENSC_ERR_ARG, "mesh too large for 32-bit node / 29-bit element indices");
-    if (params->precision != ENSC_FP64)
+    if (params->precision != ENSC_FP64 && params->precision != ENSC_MIXED)
         return set_err(nullptr, ENSC_ERR_ARG, "unsupported precision");
     if (!(mat->rho > 0.0) || !(mat->E > 0.0) || !(mat->nu < 0.5))
         return set_err(nullptr, ENSC_ERR_ARG, "invalid material");
@@ -304,8 +316,9 @@ int ensc_create(const ensc_mesh_desc* mesh, const ensc_material* mat, const ensc
         set_err(h, ENSC_ERR_CUDA, "cudaGetDeviceProperties failed");
         return fail(ENSC_ERR_CUDA);
     }
-    const int occ_e = std::max(1, ensc::occupancy_element_fp64(h->plastic));
-    const int occ_n = std::max(1, ensc::occupancy_node_fp64());
+    const bool mx = h->precision == ENSC_MIXED;
+    const int occ_e = std::max(1, mx ? ensc::occupancy_element_mixed(h->plastic) : ensc::occupancy_element_fp64(h->plastic));
+    const int occ_n = std::max(1, mx ? ensc::occupancy_node_mixed() : ensc::occupancy_node_fp64());
     const int64_t ge = (ne + ensc::kElemThreads - 1) / ensc::kElemThreads;
     const int64_t gn = (nn + ensc::kNodeThreads - 1) / ensc::kNodeThreads;
     h->grid_e = static_cast<int>(std::min<int64_t>(ge, static_cast<int64_t>(occ_e) * prop.multiProcessorCount));
@@ -313,7 +326,7 @@ int ensc_create(const ensc_mesh_desc* mesh, const ensc_material* mat, const ensc
 
     // ---- one device arena, every array 256-byte aligned ----
     const int64_t ep = h->ne_pad, np = h->nn_pad;
-    const size_t real = 8;
+    const size_t real = mx ? 4 : 8;   // storage width of element state, forces and velocity
     struct Piece {
         void** dst;
         size_t bytes;
@@ -407,14 +420,24 @@ int ensc_create(const ensc_mesh_desc* mesh, const ensc_material* mat, const ensc
             for (int k = 0; k < 8; ++k) conn_soa[k * ep + e] = mesh->conn[8 * e + k];
         int rc = upload(h, p_conn, conn_soa);
         if (rc) return fail(rc);
-        rc = upload(h, p_bt, to_soa<double>(bt.data(), ne, ep, 24));
+        if (mx) {
+            rc = upload(h, p_bt, to_soa<float>(bt.data(), ne, ep, 24));
+            std::vector<float> v0f(vol0.begin(), vol0.end()), cbf(cb.begin(), cb.end());
+            if (!rc) rc = upload(h, p_vol0, v0f);
+            if (!rc) rc = upload(h, p_cb, cbf);
+        } else {
+            rc = upload(h, p_bt, to_soa<double>(bt.data(), ne, ep, 24));
+            if (!rc) rc = upload(h, p_vol0, vol0);
+            if (!rc) rc = upload(h, p_cb, cb);
+            if (!rc) rc = upload(h, p_cb2, cb2);
+        }
         if (rc) return fail(rc);
-        rc = upload(h, p_vol0, vol0);
-        if (!rc) rc = upload(h, p_cb, cb);
-        if (!rc) rc = upload(h, p_cb2, cb2);
         if (!rc) rc = upload(h, p_im, im);
         if (!rc) rc = upload(h, p_x, to_soa<double>(mesh->x0, nn, np, 3));
-        if (!rc && mesh->v0) rc = upload(h, p_v, to_soa<double>(mesh->v0, nn, np, 3));
+        if (!rc && mesh->v0) {
+            rc = mx ? upload(h, p_v, to_soa<float>(mesh->v0, nn, np, 3))
+                    : upload(h, p_v, to_soa<double>(mesh->v0, nn, np, 3));
+        }
         if (!rc) rc = upload(h, p_ell, ell);
         if (!rc && clash) rc = upload(h, p_cptr, csr_ptr);
         if (!rc && clash) rc = upload(h, p_cent, csr_ent);
@@ -476,7 +499,7 @@ int ensc_create(const ensc_mesh_desc* mesh, const ensc_material* mat, const ensc
     }
     // init(): the force pass with dt = 0 and no boundary conditions, which
     // leaves the minimum element dt for the first cycle in ctl->dts_next
-    ensc::launch_element_fp64(h->E, h->N, h->M, h->ctl, h->P, h->grid_e, true, h->stream);
+    launch_element(h, true, h->stream);
     ce = cudaGetLastError();
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->stream);
     if (ce != cudaSuccess) {
@@ -508,9 +531,9 @@ int ensc_set_bcs(ensc_handle* h, const int8_t* dof_code, const double* dof_value
     int rc = upload(h, const_cast<uint8_t*>(h->N.bc), bc);
     if (!rc) rc = upload(h, const_cast<double*>(h->N.bcv), bcv);
     if (rc) return rc;
-    ensc::launch_apply_bc_v(h->N, false, h->stream);
+    ensc::launch_apply_bc_v(h->N, mixed(h), h->stream);
     if (!h->kinetic0_done) {
-        ensc::launch_kinetic0(h->N, h->P, h->ctl, false, h->grid_n, h->stream);
+        ensc::launch_kinetic0(h->N, h->P, h->ctl, mixed(h), h->grid_n, h->stream);
         h->kinetic0_done = true;
     }
     CK(h, cudaGetLastError());
@@ -586,13 +609,15 @@ int ensc_download(ensc_handle* h, double* x, double* u, double* v, double* sigma
         const void* src;
         int64_t n, pad;
         int comps;
+        bool f32;
     };
-    const Item items[] = {{x, h->N.x, h->nn, h->nn_pad, 3},       {u, h->N.u, h->nn, h->nn_pad, 3},
-                          {v, h->N.v, h->nn, h->nn_pad, 3},       {sigma, h->E.sigma, h->ne, h->ne_pad, 6},
-                          {qia, h->E.qia, h->ne, h->ne_pad, 12},  {eps_p, h->E.eps_p, h->ne, h->ne_pad, 1}};
+    const bool mx = mixed(h);
+    const Item items[] = {{x, h->N.x, h->nn, h->nn_pad, 3, false},        {u, h->N.u, h->nn, h->nn_pad, 3, false},
+                          {v, h->N.v, h->nn, h->nn_pad, 3, mx},           {sigma, h->E.sigma, h->ne, h->ne_pad, 6, mx},
+                          {qia, h->E.qia, h->ne, h->ne_pad, 12, mx},      {eps_p, h->E.eps_p, h->ne, h->ne_pad, 1, mx}};
     for (const Item& it : items) {
         if (!it.dst) continue;
-        ensc::launch_soa_to_aos(it.src, it.n, it.pad, it.comps, false, h->staging, h->stream);
+        ensc::launch_soa_to_aos(it.src, it.n, it.pad, it.comps, it.f32, h->staging, h->stream);
         CK(h, cudaGetLastError());
         CK(h, cudaMemcpyAsync(it.dst, h->staging, it.n * it.comps * sizeof(double), cudaMemcpyDeviceToHost,
                               h->stream));
@@ -621,15 +646,17 @@ int ensc_upload_state(ensc_handle* h, const double* x, const double* u, const do
         void* dst;
         int64_t n, pad;
         int comps;
+        bool f32;
     };
-    const Item items[] = {{x, h->N.x, h->nn, h->nn_pad, 3},       {u, h->N.u, h->nn, h->nn_pad, 3},
-                          {v, h->N.v, h->nn, h->nn_pad, 3},       {sigma, h->E.sigma, h->ne, h->ne_pad, 6},
-                          {qia, h->E.qia, h->ne, h->ne_pad, 12},  {eps_p, h->E.eps_p, h->ne, h->ne_pad, 1}};
+    const bool mx = mixed(h);
+    const Item items[] = {{x, h->N.x, h->nn, h->nn_pad, 3, false},        {u, h->N.u, h->nn, h->nn_pad, 3, false},
+                          {v, h->N.v, h->nn, h->nn_pad, 3, mx},           {sigma, h->E.sigma, h->ne, h->ne_pad, 6, mx},
+                          {qia, h->E.qia, h->ne, h->ne_pad, 12, mx},      {eps_p, h->E.eps_p, h->ne, h->ne_pad, 1, mx}};
     for (const Item& it : items) {
         if (!it.src) continue;
         CK(h, cudaMemcpyAsync(h->staging, it.src, it.n * it.comps * sizeof(double), cudaMemcpyHostToDevice,
                               h->stream));
-        ensc::launch_aos_to_soa(h->staging, it.n, it.pad, it.comps, it.dst, false, h->stream);
+        ensc::launch_aos_to_soa(h->staging, it.n, it.pad, it.comps, it.dst, it.f32, h->stream);
         CK(h, cudaGetLastError());
     }
     int rc = read_ctl(h);
@@ -683,9 +710,9 @@ int ensc_profile(ensc_handle* h, int64_t max_cycles, double step_end_time, doubl
         cudaEventRecord(ev[2], h->stream);
         ensc::launch_begin_exact(h->ctl, h->stream);
         cudaEventRecord(ev[3], h->stream);
-        ensc::launch_element_fp64(h->E, h->N, h->M, h->ctl, h->P, h->grid_e, false, h->stream);
+        launch_element(h, false, h->stream);
         cudaEventRecord(ev[4], h->stream);
-        ensc::launch_node_fp64(h->E, h->N, h->M, h->ctl, h->P, h->grid_n, h->stream);
+        launch_node(h, h->stream);
         cudaEventRecord(ev[5], h->stream);
         cudaError_t e = cudaEventSynchronize(ev[5]);
         if (e != cudaSuccess) {

@@ -18,6 +18,14 @@ void launch_node_fp64(const ElemArrays& E, const NodeArrays& N, const Material& 
 int occupancy_element_fp64(bool plastic);
 int occupancy_node_fp64();
 
+// mixed precision (ensc_mixed.cu)
+void launch_element_mixed(const ElemArrays& E, const NodeArrays& N, const Material& M, Ctl* ctl, const Partials& P,
+                          int grid, bool init, cudaStream_t st);
+void launch_node_mixed(const ElemArrays& E, const NodeArrays& N, const Material& M, Ctl* ctl, const Partials& P,
+                       int grid, cudaStream_t st);
+int occupancy_element_mixed(bool plastic);
+int occupancy_node_mixed();
+
 // control (ensc_control.cu, built with -fmad=false)
 // mode 0: fold energy partials + begin next cycle; 1: fold only; 2: fold as initial KE
 void launch_between(Ctl* ctl, const Partials& P, int mode, cudaStream_t st);

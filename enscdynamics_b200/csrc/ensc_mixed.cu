@@ -1,0 +1,445 @@
+// Mixed-precision stepper kernels: the element pass (kinematics, Jaumann /
+// J2 stress, hourglass, bulk viscosity) and the force gather run in FP32;
+// nodal position and displacement accumulation (x += dt v, u += dt v), the
+// clock, the stable-dt reduction and the energy sums stay FP64.
+//
+// Same algorithm and data flow as the FP64 path (ensc_fp64.cu); operation
+// order is free here (FMA contraction on), accuracy is checked against the
+// FP64 path by relative displacement error and energy drift.
+//
+// Element arrays: bt, sigma, qia, eps_p, fe are float; vol0 and cbrt_v0 are
+// float copies (stored in the first ne words of the FP64 arrays' storage).
+// Node arrays: x, u double; v float.
+#include "ensc_device.cuh"
+#include "ensc_kernels.h"
+
+#include <cfloat>
+
+namespace ensc {
+namespace {
+
+__device__ __forceinline__ float det3f(const float m[3][3]) {
+    return m[0][0] * (m[1][1] * m[2][2] - m[1][2] * m[2][1]) - m[0][1] * (m[1][0] * m[2][2] - m[1][2] * m[2][0]) +
+           m[0][2] * (m[1][0] * m[2][1] - m[1][1] * m[2][0]);
+}
+
+__device__ __forceinline__ float cof3f(const float m[3][3], int i, int j) {
+    const int i1 = (i + 1) % 3, i2 = (i + 2) % 3, j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+    return m[i1][j1] * m[i2][j2] - m[i1][j2] * m[i2][j1];
+}
+
+__device__ __forceinline__ constexpr int tau_s(int k, int j) {
+    constexpr int T[4][8] = {{1, -1, 1, -1, 1, -1, 1, -1},
+                             {-1, -1, 1, 1, 1, 1, -1, -1},
+                             {-1, 1, 1, -1, 1, -1, -1, 1},
+                             {-1, 1, -1, 1, 1, -1, 1, -1}};
+    return T[k][j];
+}
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <int NT, int NV>
+__device__ __forceinline__ void block_sum_d(double (&v)[NV], double* out_slots, int stride, int slot) {
+    __shared__ double red[NV][NT / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+        const double s = warp_sum_d(v[i]);
+        if (lane == 0) red[i][wid] = s;
+    }
+    __syncthreads();
+    if (wid == 0) {
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+            double s = lane < NT / 32 ? red[i][lane] : 0.0;
+            s = warp_sum_d(s);
+            if (lane == 0) out_slots[i * stride + slot] = s;
+        }
+    }
+    __syncthreads();
+}
+
+template <int NT>
+__device__ __forceinline__ void block_min2_d(double a, double b, unsigned long long* ga, unsigned long long* gb) {
+    __shared__ unsigned long long ra[NT / 32], rb[NT / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    unsigned long long x = ord_bits(a), y = ord_bits(b);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long wx = __shfl_xor_sync(0xffffffffu, x, o);
+        const unsigned long long wy = __shfl_xor_sync(0xffffffffu, y, o);
+        x = wx < x ? wx : x;
+        y = wy < y ? wy : y;
+    }
+    if (lane == 0) {
+        ra[wid] = x;
+        rb[wid] = y;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int i = 1; i < NT / 32; ++i) {
+            x = ra[i] < x ? ra[i] : x;
+            y = rb[i] < y ? rb[i] : y;
+        }
+        atomicMin(ga, x);
+        atomicMin(gb, y);
+    }
+    __syncthreads();
+}
+
+// Element pass (add_inForce_to_rhs element loop body, exDyna3D.cpp:556-573)
+// in FP32.  Node coordinates enter as offsets from the element's node 0,
+// formed in FP64 before rounding, so hourglass projections and edge lengths
+// keep their precision far from the origin.
+template <bool PLASTIC, bool INIT>
+__global__ void __launch_bounds__(kElemThreads) k_element_mixed(ElemArrays E, NodeArrays N, Material M, Ctl* ctl,
+                                                                Partials P) {
+    if (ctl->done) return;
+    const float dt1 = INIT ? 0.f : static_cast<float>(ctl->dt_i_1);
+    const double dt1d = INIT ? 0.0 : ctl->dt_i_1;
+    const int64_t ne = E.ne, ep = E.ne_pad, np = N.nn_pad;
+    const uint32_t* __restrict__ conn = E.conn;
+    const float* __restrict__ bt = static_cast<const float*>(E.bt);
+    const float* __restrict__ vol0 = reinterpret_cast<const float*>(E.vol0);
+    const float* __restrict__ cb = reinterpret_cast<const float*>(E.cbrt_v0);
+    float* __restrict__ sig = static_cast<float*>(E.sigma);
+    float* __restrict__ qia = static_cast<float*>(E.qia);
+    float* __restrict__ epsp = static_cast<float*>(E.eps_p);
+    float* __restrict__ fe = static_cast<float*>(E.fe);
+    const double* __restrict__ X = N.x;
+    const double* __restrict__ U = N.u;
+    const float* __restrict__ V = static_cast<const float*>(N.v);
+    const float G = static_cast<float>(M.G), lam = static_cast<float>(M.lambda), K = static_cast<float>(M.K);
+    const float rho = static_cast<float>(M.rho), wos = static_cast<float>(M.wos);
+    const float cvisl = static_cast<float>(M.cvisl), cvisq = static_cast<float>(M.cvisq);
+    const float y0 = static_cast<float>(M.yield0), H = static_cast<float>(M.hardening);
+    const float DRc = static_cast<float>(M.c_dr * (4.0 / 3.0 * M.G + M.K) * 0.1 / sqrt(8.0));
+    const float CRc = static_cast<float>(M.c_cr * M.rho * M.wos / 4.0);
+    double e_int = 0.0, e_hg = 0.0, e_vis = 0.0;
+    double dts_min = DBL_MAX, len_min = DBL_MAX;
+    int32_t bad = 0;
+
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < ne; e += stride) {
+        uint32_t n[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) n[k] = __ldg(conn + k * ep + e);
+        float b[8][3];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) b[k][c] = __ldg(bt + (3 * k + c) * ep + e);
+        // F = I + u_e B0^T
+        float F[3][3] = {{1.f, 0.f, 0.f}, {0.f, 1.f, 0.f}, {0.f, 0.f, 1.f}};
+        float vel[3][8];
+        float xr[8][3];
+        const double x00 = X[n[0]], x01 = X[np + n[0]], x02 = X[2 * np + n[0]];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const float u0 = static_cast<float>(U[n[k]]), u1 = static_cast<float>(U[np + n[k]]),
+                        u2 = static_cast<float>(U[2 * np + n[k]]);
+            const float uu[3] = {u0, u1, u2};
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) F[r][c] = fmaf(uu[r], b[k][c], F[r][c]);
+            vel[0][k] = V[n[k]];
+            vel[1][k] = V[np + n[k]];
+            vel[2][k] = V[2 * np + n[k]];
+            xr[k][0] = static_cast<float>(X[n[k]] - x00);
+            xr[k][1] = static_cast<float>(X[np + n[k]] - x01);
+            xr[k][2] = static_cast<float>(X[2 * np + n[k]] - x02);
+        }
+        const float J = det3f(F);
+        if (!(J > 0.f)) bad |= ST_INVERTED;
+        const float invdet = 1.f / J;
+        float Fi[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) Fi[i][j] = cof3f(F, j, i) * invdet;
+        // b^T = B0^T F^-1, L = v_e b^T
+        float L[3][3] = {};
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            float bk[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) bk[c] = b[k][0] * Fi[0][c] + b[k][1] * Fi[1][c] + b[k][2] * Fi[2][c];
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) L[r][c] = fmaf(vel[r][k], bk[c], L[r][c]);
+        }
+        const float vr = L[0][0] + L[1][1] + L[2][2];
+        // Jaumann stress update
+        float eps[6] = {L[0][0] * dt1, L[1][1] * dt1, L[2][2] * dt1, 0.5f * (L[0][1] + L[1][0]) * dt1,
+                        0.5f * (L[0][2] + L[2][0]) * dt1, 0.5f * (L[1][2] + L[2][1]) * dt1};
+        const float w0 = 0.5f * (L[0][1] - L[1][0]) * dt1;
+        const float w1 = 0.5f * (L[0][2] - L[2][0]) * dt1;
+        const float w2 = 0.5f * (L[1][2] - L[2][1]) * dt1;
+        const float tr = eps[0] + eps[1] + eps[2];
+        float so[6], s[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) so[i] = sig[i * ep + e];
+        const float g2 = 2.f * G;
+        s[0] = so[0] + lam * tr + g2 * eps[0] + 2.f * so[3] * w0 + 2.f * so[4] * w1;
+        s[1] = so[1] + lam * tr + g2 * eps[1] - 2.f * so[3] * w0 + 2.f * so[5] * w2;
+        s[2] = so[2] + lam * tr + g2 * eps[2] - 2.f * so[4] * w1 - 2.f * so[5] * w2;
+        s[3] = so[3] + g2 * eps[3] + (so[1] - so[0]) * w0 + so[5] * w1;
+        s[4] = so[4] + g2 * eps[4] + (so[2] - so[0]) * w1 + so[5] * w0;
+        s[5] = so[5] + g2 * eps[5] + (so[2] - so[1]) * w2 + so[3] * w1 - so[4] * w0;
+        if (PLASTIC) {
+            const float pm = (s[0] + s[1] + s[2]) * (1.f / 3.f);
+            const float d0 = s[0] - pm, d1 = s[1] - pm, d2 = s[2] - pm;
+            const float j2 = 0.5f * (d0 * d0 + d1 * d1 + d2 * d2) + s[3] * s[3] + s[4] * s[4] + s[5] * s[5];
+            const float seq = sqrtf(3.f * j2);
+            const float ep_old = epsp[e];
+            const float sy = y0 + H * ep_old;
+            if (seq > sy) {
+                const float dl = (seq - sy) / (3.f * G + H);
+                const float r = 1.f - 3.f * G * dl / seq;
+                s[0] = d0 * r + pm;
+                s[1] = d1 * r + pm;
+                s[2] = d2 * r + pm;
+                s[3] *= r;
+                s[4] *= r;
+                s[5] *= r;
+                if (!INIT) epsp[e] = ep_old + dl;
+            }
+        }
+        if (!INIT) {
+#pragma unroll
+            for (int i = 0; i < 6; ++i) sig[i * ep + e] = s[i];
+        }
+        const float V0 = vol0[e];
+        const float Vc = J * V0;
+        {
+            float w = 0.f;
+#pragma unroll
+            for (int i = 0; i < 6; ++i) w += (i < 3 ? 0.5f : 1.0f) * (so[i] + s[i]) * eps[i];
+            e_int += static_cast<double>(w * Vc);
+        }
+        // min edge
+        float len;
+        {
+            constexpr int A0[12] = {0, 1, 2, 3, 4, 5, 6, 7, 0, 1, 2, 3};
+            constexpr int A1[12] = {1, 2, 3, 0, 5, 6, 7, 4, 4, 5, 6, 7};
+            float m = FLT_MAX;
+#pragma unroll
+            for (int k = 0; k < 12; ++k) {
+                const float dx = xr[A1[k]][0] - xr[A0[k]][0];
+                const float dy = xr[A1[k]][1] - xr[A0[k]][1];
+                const float dz = xr[A1[k]][2] - xr[A0[k]][2];
+                m = fminf(m, dx * dx + dy * dy + dz * dz);
+            }
+            len = sqrtf(m);
+        }
+        // hourglass: the Gamma vectors sum to zero, so TAU x = TAU (x - x0)
+        float TX[4][3];
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                float t = 0.f;
+#pragma unroll
+                for (int j = 1; j < 8; ++j) t += tau_s(kk, j) > 0 ? xr[j][c] : -xr[j][c];
+                TX[kk][c] = t;
+            }
+        float nx2 = 0.f;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) nx2 += b[k][0] * b[k][0] + b[k][1] * b[k][1] + b[k][2] * b[k][2];
+        float AT[4][8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk)
+                AT[kk][j] = static_cast<float>(tau_s(kk, j)) - (TX[kk][0] * b[j][0] + TX[kk][1] * b[j][1] +
+                                                                TX[kk][2] * b[j][2]);
+        float HIA[3][4];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) {
+                float t = 0.f;
+#pragma unroll
+                for (int j = 0; j < 8; ++j) t = fmaf(vel[i][j], AT[kk][j], t);
+                HIA[i][kk] = t;
+            }
+        const float DR = DRc * nx2 * Vc * dt1;
+        const float CR = CRc * V0 / Vc * (cb[e] * cb[e]);
+        float Q[3][4];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) {
+                Q[i][kk] = qia[(4 * i + kk) * ep + e] + DR * HIA[i][kk];
+                if (!INIT) qia[(4 * i + kk) * ep + e] = Q[i][kk];
+            }
+        const bool visc = !(fabsf(vr) < 1.0e-10f);
+        float pv = 0.f;
+        if (visc) {
+            const float l0 = cb[e];
+            const float m0 = fminf(vr, 0.f);
+            pv = rho / J * l0 * (cvisq * cvisq * l0 * vr * m0 - cvisl * wos * vr);
+            e_vis += -static_cast<double>(pv * Vc * vr) * dt1d;
+        }
+        float hpow = 0.f;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            float bj[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) bj[c] = b[j][0] * Fi[0][c] + b[j][1] * Fi[1][c] + b[j][2] * Fi[2][c];
+            float fj[3];
+            fj[0] = -(bj[0] * s[0] + bj[1] * s[3] + bj[2] * s[4]) * Vc;
+            fj[1] = -(bj[0] * s[3] + bj[1] * s[1] + bj[2] * s[5]) * Vc;
+            fj[2] = -(bj[0] * s[4] + bj[1] * s[5] + bj[2] * s[2]) * Vc;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const float hgs = Q[i][0] * AT[0][j] + Q[i][1] * AT[1][j] + Q[i][2] * AT[2][j] + Q[i][3] * AT[3][j];
+                const float hgd = AT[0][j] * HIA[i][0] + AT[1][j] * HIA[i][1] + AT[2][j] * HIA[i][2] +
+                                  AT[3][j] * HIA[i][3];
+                const float h = hgs + hgd * CR;
+                hpow = fmaf(h, vel[i][j], hpow);
+                fe[(3 * j + i) * ep + e] = fj[i] - h + pv * bj[i] * Vc;
+            }
+        }
+        e_hg += static_cast<double>(hpow) * dt1d;
+        // element dt (compute_dtStable, exDyna3D.cpp:828-834)
+        const float m0 = fminf(vr, 0.f);
+        const float xi = cvisl - cvisq * cvisq * len / wos * m0;
+        const float dts = (sqrtf(1.f + xi * xi) - xi) * len / wos;
+        if (!isfinite(dts)) bad |= ST_NONFINITE;
+        dts_min = fmin(dts_min, static_cast<double>(dts));
+        len_min = fmin(len_min, static_cast<double>(len));
+    }
+    if (bad) atomicOr(&ctl->status, bad);
+    block_min2_d<kElemThreads>(dts_min, len_min, &ctl->dts_next, &ctl->len_min);
+    if (!INIT) {
+        double v3[3] = {e_int, e_hg, e_vis};
+        block_sum_d<kElemThreads, 3>(v3, P.elem, P.n_elem_blocks, blockIdx.x);
+    }
+}
+
+// Node pass in mixed precision: FP32 slot-ordered gather and acceleration,
+// FP32 velocity, FP64 displacement / position accumulation and energy.
+__global__ void __launch_bounds__(kNodeThreads) k_node_mixed(ElemArrays E, NodeArrays N, Material M, Ctl* ctl,
+                                                             Partials P) {
+    if (ctl->done) return;
+    double dt_i;
+    const double dt_i_1 = ctl->dt_i_1;
+    if (ctl->dt_final) {
+        dt_i = ctl->dt_i;
+    } else {
+        double d = bits_ord(ctl->len_min) / ctl->wos;
+        d = d < ctl->dts_cur ? d : ctl->dts_cur;
+        dt_i = d * ctl->factor;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (!(dt_i > 0.0) || !isfinite(dt_i)) atomicOr(&ctl->status, ST_BAD_DT);
+        if (!ctl->dt_final) ctl->dt_i = dt_i;
+        ctl->cycles_done += 1;
+        ctl->energy_pending = 1;
+    }
+    const int64_t nn = N.nn, np = N.nn_pad, ep = E.ne_pad;
+    const float* __restrict__ fe = static_cast<const float*>(E.fe);
+    float* __restrict__ V = static_cast<float*>(N.v);
+    const float hdt = static_cast<float>(0.5 * (dt_i + dt_i_1));
+    const double dt_avg = 0.5 * (dt_i + dt_i_1);
+    double kin = 0.0, wext = 0.0;
+    int32_t bad = 0;
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    for (int64_t n = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; n < nn; n += stride) {
+        float f[3] = {0.f, 0.f, 0.f};
+        if (N.csr_ptr == nullptr) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const uint32_t el = __ldg(N.ell + k * np + n);
+                if (el != ENSC_NONE) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) f[c] += fe[(3 * k + c) * ep + el];
+                }
+            }
+        } else {
+            for (int64_t i = N.csr_ptr[n]; i < N.csr_ptr[n + 1]; ++i) {
+                const uint32_t ent = N.csr_ent[i];
+                const int k = static_cast<int>(ent & 7u);
+                const uint32_t el = ent >> 3;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) f[c] += fe[(3 * k + c) * ep + el];
+            }
+        }
+        const double im = N.inv_mass[n];
+        const float imf = static_cast<float>(im);
+        const uint32_t code = N.bc[n];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            float a = f[c];
+            float g = 0.f;
+            if (M.gravity_on) {
+                g = static_cast<float>(M.gravity_value * M.gravity_dir[c] / im);
+                a += g;
+            }
+            const uint32_t cc = (code >> (2 * c)) & 3u;
+            float r = 0.f, rf = 0.f;
+            if (cc & 2u) {
+                r = -a;
+                a = 0.f;
+            }
+            if ((cc & 1u) && a != 0.f) {
+                rf = -a;
+                r = -a;
+                a = 0.f;
+            }
+            if (cc) N.rf[c * np + n] = static_cast<double>(rf);
+            const float vo = V[c * np + n];
+            const float vn = fmaf(hdt, a * imf, vo);
+            V[c * np + n] = vn;
+            const double vnd = static_cast<double>(vn);
+            N.u[c * np + n] += dt_i * vnd;
+            N.x[c * np + n] += dt_i * vnd;
+            wext += static_cast<double>(g + r) * dt_avg * 0.5 * (static_cast<double>(vo) + vnd);
+            kin += 0.5 * (vnd * vnd) / im;
+            if (!isfinite(vn)) bad |= ST_NONFINITE;
+        }
+    }
+    if (bad) atomicOr(&ctl->status, bad);
+    double v2[2] = {kin, wext};
+    block_sum_d<kNodeThreads, 2>(v2, P.node, P.n_node_blocks, blockIdx.x);
+}
+
+}  // namespace
+
+void launch_element_mixed(const ElemArrays& E, const NodeArrays& N, const Material& M, Ctl* ctl, const Partials& P,
+                          int grid, bool init, cudaStream_t st) {
+    if (M.plastic) {
+        if (init) k_element_mixed<true, true><<<grid, kElemThreads, 0, st>>>(E, N, M, ctl, P);
+        else k_element_mixed<true, false><<<grid, kElemThreads, 0, st>>>(E, N, M, ctl, P);
+    } else {
+        if (init) k_element_mixed<false, true><<<grid, kElemThreads, 0, st>>>(E, N, M, ctl, P);
+        else k_element_mixed<false, false><<<grid, kElemThreads, 0, st>>>(E, N, M, ctl, P);
+    }
+}
+
+void launch_node_mixed(const ElemArrays& E, const NodeArrays& N, const Material& M, Ctl* ctl, const Partials& P,
+                       int grid, cudaStream_t st) {
+    k_node_mixed<<<grid, kNodeThreads, 0, st>>>(E, N, M, ctl, P);
+}
+
+int occupancy_element_mixed(bool plastic) {
+    int nb = 0;
+    if (plastic) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_mixed<true, false>, kElemThreads, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_mixed<false, false>, kElemThreads, 0);
+    return nb;
+}
+
+int occupancy_node_mixed() {
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_node_mixed, kNodeThreads, 0);
+    return nb;
+}
+
+}  // namespace ensc

@@ -94,7 +94,13 @@ def block(nx: int = 256, ny: int = 128, nz: int = 64, lx: float = 1.0, ly: float
     (2,097,152 elements, 2,154,945 nodes) over 1.0 x 0.5 x 0.25 m, J2 with
     E = 70 GPa, nu = 0.33, rho = 2700, yield 250 MPa and a 100 MPa tangent
     modulus; bottom face (z = 0) fixed; seeded Gaussian nodal velocities
-    (std 2 m/s) smoothed by 3 Jacobi passes; 5000 cycles."""
+    (std 2 m/s) smoothed by 3 Jacobi passes; 5000 cycles.
+
+    Hourglass viscosity is the reference's default c_cr = 0.05
+    (exDyna3D.cpp:701) with dt factor 0.9: the random field excites the
+    hourglass modes strongly, and with c_cr = 0.1 the reference algorithm's
+    stable-dt estimate (which ignores hourglass viscosity) lets the solution
+    grow without bound within ~200 cycles, on the CPU as on the GPU."""
     m = M.box_mesh(nx, ny, nz, lx, ly, lz)
     fix = M.face_nodes(m, 2, "min")
     m.node_sets = {"Set-1": fix}
@@ -102,7 +108,7 @@ def block(nx: int = 256, ny: int = 128, nz: int = 64, lx: float = 1.0, ly: float
     v0[fix] = 0.0
     code, val = M.bc_arrays(m.n_nodes, fixed=[(fix, 0, 2)])
     mat = M.Material(70e9, 0.33, 2700.0, 250e6 if plastic else 0.0, 100e6 if plastic else 0.0)
-    ctl = M.Controls(total_time=1.0, **DEFAULT_CONTROLS)
+    ctl = M.Controls(total_time=1.0, **dict(DEFAULT_CONTROLS, c_cr=0.05))
     return Problem("block_%dx%dx%d" % (nx, ny, nz), m, v0, code, val, mat, ctl, cycles,
                    fixed_sets=[("Set-1", "ENCASTRE")], per_node_velocity=True)
 

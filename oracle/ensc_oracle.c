@@ -107,6 +107,13 @@ void ensc_oracle_setup(int64_t nn, int64_t ne, const uint32_t* conn, const doubl
     for (int64_t i = 0; i < 3 * nn; ++i) inv_mass[i] = 1.0 / inv_mass[i];
 }
 
+void ensc_oracle_cbrt_pair(int64_t ne, const double* vol0, double* cbrt_v0, double* cbrt_v0sq) {
+    for (int64_t e = 0; e < ne; ++e) {
+        cbrt_v0[e] = cbrt(vol0[e]);
+        cbrt_v0sq[e] = cbrt(vol0[e] * vol0[e]);
+    }
+}
+
 /* min_ele_edge (exDyna3D.cpp:1173-1220): 12 edges, squared lengths compared in
  * the order bottom ring, top ring, verticals; sqrt of the minimum. */
 static double min_edge(const double xyz[8][3]) {

@@ -79,6 +79,10 @@ void ensc_oracle_setup(int64_t nn, int64_t ne, const uint32_t* conn, const doubl
                        double* bt, double* vol0, double* cbrt_v0, double* cbrt_v0sq,
                        double* inv_mass);
 
+/* cbrt(V0) and cbrt(V0^2) with the C library, as the reference's std::cbrt
+ * (exDyna3D.cpp:1040, 1081). */
+void ensc_oracle_cbrt_pair(int64_t ne, const double* vol0, double* cbrt_v0, double* cbrt_v0sq);
+
 /* The force pass that exDyna3D::init() runs with dt = 0 and no boundary
  * conditions (exDyna3D.cpp:126-141): fills len[] and dtstable[]. */
 void ensc_oracle_init_pass(const ensc_oracle_params* p, ensc_oracle_state* s);

@@ -65,6 +65,7 @@ def _load():
         lib.ensc_oracle_material_update.argtypes = [C.POINTER(_Params)]
         lib.ensc_oracle_setup.argtypes = [C.c_int64, C.c_int64, C.POINTER(C.c_uint32), _P, C.c_double,
                                           _P, _P, _P, _P, _P]
+        lib.ensc_oracle_cbrt_pair.argtypes = [C.c_int64, _P, _P, _P]
         lib.ensc_oracle_init_pass.argtypes = [C.POINTER(_Params), C.POINTER(_State)]
         lib.ensc_oracle_apply_bc_v.argtypes = [C.POINTER(_State)]
         lib.ensc_oracle_kinetic.argtypes = [C.POINTER(_State)]
@@ -122,8 +123,8 @@ class Oracle:
             self.bt[:] = setup["bt"].reshape(-1)
             self.vol0[:] = setup["vol0"]
             self.inv_mass[:] = setup["inv_mass"].reshape(-1)
-            self.cbrt_v0[:] = np.cbrt(self.vol0) if "cbrt_v0" not in setup else setup["cbrt_v0"]
-            self.cbrt_v0sq[:] = np.cbrt(self.vol0 * self.vol0) if "cbrt_v0sq" not in setup else setup["cbrt_v0sq"]
+            # the C library's cbrt, as the reference (NumPy's cbrt can differ in the last bit)
+            lib.ensc_oracle_cbrt_pair(ne, _ptr(self.vol0), _ptr(self.cbrt_v0), _ptr(self.cbrt_v0sq))
         s = _State()
         s.nn, s.ne = nn, ne
         s.conn = _ptr(self.conn, C.c_uint32)

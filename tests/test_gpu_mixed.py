@@ -1,0 +1,86 @@
+"""Mixed-precision stepper (FP32 element work and gather, FP64 x/u/clock/dt/
+energy) against the FP64 oracle.
+
+Bars (per workload, after the stated cycles):
+  * max relative displacement error  max|u_mixed - u_fp64| / max|u_fp64| <= 1e-5
+  * energy-balance drift: |E_bal_mixed - E_bal_fp64| / KE0 <= 0.5 %, where
+    E_bal = kinetic + internal + hourglass + viscous - external work
+"""
+import numpy as np
+import pytest
+
+from _common import load_golden, material_controls, oracle_for, run_len
+from enscdynamics_b200 import capi
+from enscdynamics_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+DISP_TOL = 1e-5
+ENERGY_TOL = 5e-3
+
+
+def energy_balance(e):
+    return e["kinetic"] + e["internal"] + e["hourglass"] + e["viscous"] - e["external"]
+
+
+def oracle_energy(o):
+    k, i, h, v, x = o.energy
+    return dict(kinetic=k, internal=i, hourglass=h, viscous=v, external=x)
+
+
+def compare(problem, cycles):
+    import pyoracle
+    m, c = problem.material, problem.controls
+    o = pyoracle.Oracle(problem.mesh.x0, problem.mesh.conn, problem.v0, problem.bc_code, problem.bc_value,
+                        E=m.E, nu=m.nu, rho=m.rho, c_dr=c.c_dr, c_cr=c.c_cr, factor=c.factor, cvisl=c.cvisl,
+                        cvisq=c.cvisq, total_time=c.total_time, yield0=m.yield_stress, hardening=m.hardening,
+                        gravity=c.gravity)
+    o.run(cycles)
+    with capi.Stepper(problem.mesh.x0, problem.mesh.conn, problem.v0, material=m, controls=c,
+                      precision=capi.MIXED) as s:
+        s.set_bcs(problem.bc_code, problem.bc_value)
+        rep = s.step(cycles)
+        st = s.download()
+        e = s.energy()
+    assert rep["cycles"] == cycles and rep["status"] == 0
+    u_ref = o.u.reshape(-1, 3)
+    disp_err = np.abs(st["u"] - u_ref).max() / np.abs(u_ref).max()
+    oe = oracle_energy(o)
+    drift = abs(energy_balance(e) - energy_balance(oe)) / o.kinetic0
+    return disp_err, drift, e, oe
+
+
+def test_mixed_cantilever():
+    err, drift, e, oe = compare(W.cantilever(), 2000)
+    assert err <= DISP_TOL, err
+    assert drift <= ENERGY_TOL, drift
+
+
+def test_mixed_block_j2():
+    p = W.block(32, 16, 8, 0.32, 0.16, 0.08, plastic=True)
+    err, drift, e, oe = compare(p, 1500)
+    assert err <= DISP_TOL, err
+    assert drift <= ENERGY_TOL, drift
+
+
+def test_mixed_gravity_golden_case():
+    g = load_golden("gravity_6x2x2")
+    mat, ctl = material_controls(g["meta"])
+    p = W.Problem("gravity", None, g["v0"], g["bc_code"], g["bc_value"], mat, ctl, 600)
+    from enscdynamics_b200 import mesh as M
+    p.mesh = M.Mesh(x0=g["x0"], conn=g["conn"])
+    err, drift, e, oe = compare(p, 600)
+    assert err <= DISP_TOL, err
+
+
+def test_mixed_deterministic():
+    p = W.block(24, 12, 8, 0.24, 0.12, 0.08, plastic=True)
+    outs = []
+    for _ in range(2):
+        with capi.Stepper(p.mesh.x0, p.mesh.conn, p.v0, material=p.material, controls=p.controls,
+                          precision=capi.MIXED) as s:
+            s.set_bcs(p.bc_code, p.bc_value)
+            s.step(200)
+            outs.append(s.download())
+    for k in outs[0]:
+        assert np.array_equal(outs[0][k], outs[1][k]), k
