@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--workload", choices=["block", "cantilever"], default="block")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--cycles-per-step", type=int, default=500)
+    ap.add_argument("--block-dims", default="256,128,64", help="block workload cells nx,ny,nz")
     ap.add_argument("--profile-cycles", type=int, default=40)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-cycles", type=int, default=20)
@@ -137,10 +138,11 @@ def cycle_bytes(ne: int, nn: int, plastic: bool, mixed: bool = False) -> int:
     return ne * (904 + (16 if plastic else 0)) + nn * 185
 
 
-def build_problem(name: str):
+def build_problem(name: str, dims: str = "256,128,64"):
     from enscdynamics_b200 import workloads
     if name == "block":
-        return workloads.block()
+        nx, ny, nz = (int(v) for v in dims.split(","))
+        return workloads.block(nx, ny, nz, 1.0 * nx / 256, 0.5 * ny / 128, 0.25 * nz / 64)
     return workloads.cantilever()
 
 
@@ -233,7 +235,7 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.SUM)
         return float(t.item())
 
-    p = build_problem(args.workload)
+    p = build_problem(args.workload, args.block_dims)
     ne, nn = p.mesh.n_elements, p.mesh.n_nodes
     plastic = p.material.yield_stress > 0.0
     C = args.cycles_per_step
@@ -339,8 +341,8 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64" if mixed else "f64", "data": "synthetic",
-        "config": {"workload": "block 256x128x64 hex8 (2,097,152 el, 2,154,945 nodes), J2, 5000 cycles = 10 steps"
-                   if args.workload == "block" else p.name,
+        "config": {"workload": ("block 256x128x64 hex8 (2,097,152 el, 2,154,945 nodes), J2, 5000 cycles = 10 steps"
+                                if args.block_dims == "256,128,64" else p.name) if args.workload == "block" else p.name,
                    "elements": ne, "nodes": nn, "cycles_per_step": C, "precision": args.precision,
                    "l2": f"inputs larger than L2 ({cycle_bytes(ne, nn, plastic, mixed) / 1e9:.2f} GB per cycle)",
                    "parallelism": f"replicas x{world}"},
