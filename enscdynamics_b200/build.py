@@ -31,6 +31,7 @@ UNITS = [
     ("ensc_fp64.cu", ["-fmad=false"]),
     ("ensc_control.cu", ["-fmad=false"]),
     ("ensc_mixed.cu", []),
+    ("ensc_noalloc.cu", []),
     ("ensc_capi.cu", []),
 ]
 HEADERS = ["ensc_device.cuh", "ensc_kernels.h"]

@@ -55,6 +55,24 @@ class EnergyReport(C.Structure):
                 ("viscous", C.c_double), ("external", C.c_double), ("kinetic0", C.c_double)]
 
 
+class DeviceModel(C.Structure):
+    """ensc_device_model: caller-owned device arrays for ensc_step_noalloc."""
+    _fields_ = [("n_nodes", C.c_int64), ("n_elements", C.c_int64), ("conn", C.c_void_p), ("bt", C.c_void_p),
+                ("vol0", C.c_void_p), ("cbrt_v0", C.c_void_p), ("cbrt_v0sq", C.c_void_p),
+                ("inv_mass", C.c_void_p), ("bc", C.c_void_p), ("bc_value", C.c_void_p), ("node_elem", C.c_void_p),
+                ("x", C.c_void_p), ("u", C.c_void_p), ("v", C.c_void_p), ("sigma", C.c_void_p),
+                ("qia", C.c_void_p), ("eps_p", C.c_void_p), ("rf", C.c_void_p)]
+
+
+class NoallocClock(C.Structure):
+    _fields_ = [("time", C.c_double), ("dt_i", C.c_double), ("dt_i_1", C.c_double),
+                ("dt_stable_min", C.c_double), ("init_pass", C.c_int32), ("cycles", C.c_int64)]
+
+
+NOALLOC_MAX_ELEMENTS = 32768
+NOALLOC_MAX_NODES = 262144
+
+
 # every symbol include/ensc_gpu.h declares: (name, restype, argtypes)
 SIGNATURES = [
     ("ensc_abi_version", C.c_int, []),
@@ -74,6 +92,8 @@ SIGNATURES = [
     ("ensc_device_bytes", C.c_int64, [C.c_void_p]),
     ("ensc_kernels_per_cycle", C.c_int32, [C.c_void_p]),
     ("ensc_destroy", None, [C.c_void_p]),
+    ("ensc_step_noalloc", C.c_int, [C.POINTER(DeviceModel), C.POINTER(MaterialDesc), C.POINTER(Params),
+                                    C.POINTER(NoallocClock), C.c_int64, C.c_double]),
     ("ensc_last_error", C.c_char_p, [C.c_void_p]),
 ]
 

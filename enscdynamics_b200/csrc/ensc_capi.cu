@@ -223,6 +223,10 @@ void fill_report(const ensc_handle* h, int64_t before, ensc_step_report* r) {
 
 }  // namespace
 
+namespace ensc {
+void set_thread_error(const std::string& msg) { g_create_error = msg; }
+}  // namespace ensc
+
 extern "C" {
 
 int ensc_abi_version(void) { return ENSC_ABI_VERSION; }

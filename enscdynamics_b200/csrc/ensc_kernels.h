@@ -4,6 +4,8 @@
 
 #include "ensc_device.cuh"
 
+#include <string>
+
 namespace ensc {
 
 constexpr int kElemThreads = 128;
@@ -40,5 +42,8 @@ void launch_soa_to_aos(const void* soa, int64_t n, int64_t pad, int comps, bool 
                        cudaStream_t st);
 void launch_aos_to_soa(const double* aos, int64_t n, int64_t pad, int comps, void* soa, bool dst_fp32,
                        cudaStream_t st);
+
+// thread-local message returned by ensc_last_error(NULL) (ensc_capi.cu)
+void set_thread_error(const std::string& msg);
 
 }  // namespace ensc

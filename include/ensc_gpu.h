@@ -188,6 +188,61 @@ int32_t ensc_kernels_per_cycle(const ensc_handle* h);
 
 void ensc_destroy(ensc_handle* h);
 
+/* ---- stepping without device allocation --------------------------------
+ * No counterpart in the reference: the reference stepper never allocates on
+ * a GPU.  For callers that cannot call cudaMalloc -- code running inside a
+ * stream capture it does not own, plug-ins whose host application owns all
+ * device memory, loops with a budget fixed at start-up -- ensc_step_noalloc
+ * runs the FP64 cycle on device arrays the caller already owns and keeps its
+ * scratch (element-force hand-off, energy partials, control block) in one
+ * fixed file-scope device array of about 6.3 MiB that every GPU loading this
+ * library holds until exit.  It allocates nothing.  Meshes above the limits
+ * below are rejected with ENSC_ERR_ARG; meshes where a node sits in the same
+ * local slot of two elements are not supported (node_elem holds one element
+ * per slot).  All calls share the scratch and it keeps the last call's
+ * contents: each call re-initialises it, but calls that overlap on the GPU
+ * race on it.  The first call on a device looks up the scratch address
+ * (once per device); make it before any stream capture that should contain
+ * later calls.  Messages: ensc_last_error(NULL). */
+#define ENSC_NOALLOC_MAX_ELEMENTS 32768
+#define ENSC_NOALLOC_MAX_NODES 262144
+
+/* Caller-owned device arrays, structure of arrays with component stride
+ * n_elements (element arrays) or n_nodes (node arrays), no padding. */
+typedef struct {
+    int64_t n_nodes, n_elements;
+    const uint32_t* conn;       /* [8][n_elements] local node k of element e */
+    const double* bt;           /* [24][n_elements] component 3k+c = B0^T(k, c) */
+    const double* vol0;         /* [n_elements] V0 */
+    const double* cbrt_v0;      /* [n_elements] cbrt(V0) */
+    const double* cbrt_v0sq;    /* [n_elements] cbrt(V0 * V0) */
+    const double* inv_mass;     /* [n_nodes] inverse lumped mass */
+    const uint8_t* bc;          /* [n_nodes] bits 2c / 2c+1: DOF c fixed / velocity */
+    const double* bc_value;     /* [3][n_nodes] prescribed velocities */
+    const uint32_t* node_elem;  /* [8][n_nodes] element holding node n in slot k, or 0xFFFFFFFF */
+    double* x;                  /* [3][n_nodes] current coordinates, in/out */
+    double* u;                  /* [3][n_nodes] displacement, in/out */
+    double* v;                  /* [3][n_nodes] velocity, in/out */
+    double* sigma;              /* [6][n_elements] in/out */
+    double* qia;                /* [12][n_elements] in/out */
+    double* eps_p;              /* [n_elements] in/out */
+    double* rf;                 /* [3][n_nodes] reactions, out */
+} ensc_device_model;
+
+/* Clock carried between calls (in/out). */
+typedef struct {
+    double time, dt_i, dt_i_1;
+    double dt_stable_min;       /* min element dt of the last force pass */
+    int32_t init_pass;          /* 1 on the first call: run init()'s dt = 0 pass */
+    int64_t cycles;             /* out: cycles run by the call */
+} ensc_noalloc_clock;
+
+/* Runs up to max_cycles FP64 cycles while time < step_end_time, on
+ * params->stream (NULL: the legacy default stream) of params->device, and
+ * waits for them.  params->precision must be ENSC_FP64. */
+int ensc_step_noalloc(const ensc_device_model* m, const ensc_material* mat, const ensc_params* params,
+                      ensc_noalloc_clock* clk, int64_t max_cycles, double step_end_time);
+
 /* Message of the last error on h (or of the last failed ensc_create on this
  * thread when h is NULL). */
 const char* ensc_last_error(const ensc_handle* h);
