@@ -400,6 +400,7 @@ int ensc_create(const ensc_mesh_desc* mesh, const ensc_material* mat, const ensc
     h->E.qia = p_qia;
     h->E.eps_p = p_eps;
     h->E.fe = p_fe;
+    h->E.tiles_aligned = 1;  // arena pieces are 256-byte aligned, ne_pad % 32 == 0
     h->N.nn = nn;
     h->N.nn_pad = np;
     h->N.x = static_cast<double*>(p_x);

@@ -50,6 +50,12 @@ __device__ __forceinline__ constexpr int tau_sign(int k, int j) {
     return T[k][j];
 }
 
+// Gamma row k as a bit mask: bit j set where the entry is +1.
+__device__ __forceinline__ double tau_of(int k, int j) {
+    constexpr unsigned kMask = 0x55u | (0x3Cu << 8) | (0x96u << 16) | (0x5Au << 24);
+    return ((kMask >> (8 * k + j)) & 1u) ? 1.0 : -1.0;
+}
+
 template <typename T>
 __device__ __forceinline__ T warp_min(T v) {
 #pragma unroll
@@ -116,9 +122,15 @@ __device__ __forceinline__ void block_min2(double a, double b, unsigned long lon
 // (exDyna3D.cpp:556-573): kinematics, Jaumann stress (+ J2 return),
 // hourglass, bulk viscosity, element dt and min edge.  Writes the element's
 // 8x3 nodal forces to fe for the node-centric gather.
+//
+// Register-lean structure: the element's nodes are streamed once for the
+// kinematics (b^T, L, hourglass vectors, HIA) and once more for the forces;
+// per-node rows of b^T and ATAU are recomputed from B0^T (L1-resident) rather
+// than held, so no 8x3 / 4x8 array stays live.  Every value is the same
+// expression, in the same order, as the CPU restatement (explicit fma only).
 template <bool PLASTIC, bool INIT>
-__global__ void __launch_bounds__(kElemThreads) k_element(ElemArrays E, NodeArrays N, Material M, Ctl* ctl,
-                                                          Partials P) {
+__global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_FP64) k_element(ElemArrays E, NodeArrays N, Material M, Ctl* ctl,
+                                                             Partials P) {
     if (ctl->done) return;
     const double dt1 = INIT ? 0.0 : ctl->dt_i_1;
     const int64_t ne = E.ne, ep = E.ne_pad, np = N.nn_pad;
@@ -142,85 +154,120 @@ __global__ void __launch_bounds__(kElemThreads) k_element(ElemArrays E, NodeArra
         const bool live = e0 < ne;
         const int64_t e = live ? e0 : 0;
         double dts = DBL_MAX, len = DBL_MAX;
+        if (ENSC_PREFETCH && E.tiles_aligned) {
+            // this warp's next tile (32 elements, 32-element aligned, inside ne_pad)
+            const int lane = threadIdx.x & 31;
+            const int64_t tn = e0 - lane + stride;
+            if (tn < ne) {
+                prefetch_tile(conn, ep, 8, tn, lane);
+                prefetch_tile(bt, ep, 24, tn, lane);
+                prefetch_tile(sig, ep, 6, tn, lane);
+                prefetch_tile(qia, ep, 12, tn, lane);
+                if (lane == 0) {
+                    prefetch_l2(E.vol0 + tn, 256);
+                    prefetch_l2(E.cbrt_v0 + tn, 256);
+                    prefetch_l2(E.cbrt_v0sq + tn, 256);
+                    if (PLASTIC) prefetch_l2(epsp + tn, 256);
+                }
+            }
+        }
         if (live) {
+            const double* __restrict__ bte = bt + e;
             uint32_t n[8];
 #pragma unroll
             for (int k = 0; k < 8; ++k) n[k] = __ldg(conn + k * ep + e);
-            // F = I + u_e B0^T (:862-865), summed over k = 0..7
-            double F[3][3];
+            // current coordinates: hourglass projections TAU x (exact, the
+            // Gamma entries are +-1) and the minimum edge (min_ele_edge :1173-1220)
+            double TX[4][3];
+            {
+                double xyz[8][3];
 #pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    xyz[k][0] = X[n[k]];
+                    xyz[k][1] = X[np + n[k]];
+                    xyz[k][2] = X[2 * np + n[k]];
+                }
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        double t = tau_sign(kk, 0) > 0 ? xyz[0][c] : -xyz[0][c];
+#pragma unroll
+                        for (int j = 1; j < 8; ++j) t = tau_sign(kk, j) > 0 ? t + xyz[j][c] : t - xyz[j][c];
+                        TX[kk][c] = t;
+                    }
+                constexpr int A0[12] = {0, 1, 2, 3, 4, 5, 6, 7, 0, 1, 2, 3};
+                constexpr int A1[12] = {1, 2, 3, 0, 5, 6, 7, 4, 4, 5, 6, 7};
+                double m = DBL_MAX;
+#pragma unroll
+                for (int k = 0; k < 12; ++k) {
+                    const double dx = xyz[A1[k]][0] - xyz[A0[k]][0];
+                    const double dy = xyz[A1[k]][1] - xyz[A0[k]][1];
+                    const double dz = xyz[A1[k]][2] - xyz[A0[k]][2];
+                    const double t = __fma_rn(dz, dz, __fma_rn(dy, dy, dx * dx));
+                    m = t < m ? t : m;
+                }
+                len = sqrt(m);
+            }
+            // F = I + u_e B0^T (:862-865)
+            double F[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+#pragma unroll ENSC_NODE_UNROLL_FP64
             for (int k = 0; k < 8; ++k) {
-                const double u0 = U[n[k]], u1 = U[np + n[k]], u2 = U[2 * np + n[k]];
-                const double b0 = __ldg(bt + (3 * k) * ep + e), b1 = __ldg(bt + (3 * k + 1) * ep + e),
-                             b2 = __ldg(bt + (3 * k + 2) * ep + e);
-                const double uu[3] = {u0, u1, u2}, bb[3] = {b0, b1, b2};
+                const uint32_t nk = __ldg(conn + k * ep + e);
+                const double uu[3] = {U[nk], U[np + nk], U[2 * np + nk]};
+                const double* bk = bte + 3 * k * ep;
+                const double bb[3] = {__ldg(bk), __ldg(bk + ep), __ldg(bk + 2 * ep)};
 #pragma unroll
                 for (int r = 0; r < 3; ++r)
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) F[r][c] = (k == 0) ? uu[r] * bb[c] : F[r][c] + uu[r] * bb[c];
+                    for (int c = 0; c < 3; ++c) F[r][c] = __fma_rn(uu[r], bb[c], F[r][c]);
             }
             F[0][0] = 1.0 + F[0][0];
             F[1][1] = 1.0 + F[1][1];
             F[2][2] = 1.0 + F[2][2];
-            F[0][1] = 0.0 + F[0][1];
-            F[0][2] = 0.0 + F[0][2];
-            F[1][0] = 0.0 + F[1][0];
-            F[1][2] = 0.0 + F[1][2];
-            F[2][0] = 0.0 + F[2][0];
-            F[2][1] = 0.0 + F[2][1];
             const double J = det3(F);
             double Fi[3][3];
             inv3(F, Fi);
             if (!(J > 0.0)) bad |= ST_INVERTED;
-            // b^T = B0^T F^-1 (:872-875); L = v_e b^T (:928); VolRate (:877-885)
-            double vel[3][8];
-            double L[3][3];
-            double q01[3], q23[3], q0123[3], q45[3];
-            double vr = 0.0;
+            // per node: L0 = v_e B0^T, VT = v_e Gamma^T (signed sums), NX2 (:1024)
+            double L0[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+            double VT[3][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
+            double nx2 = 0.0;
+#pragma unroll ENSC_NODE_UNROLL_FP64
+            for (int j = 0; j < 8; ++j) {
+                const uint32_t nj = __ldg(conn + j * ep + e);
+                const double* bk = bte + 3 * j * ep;
+                const double bb[3] = {__ldg(bk), __ldg(bk + ep), __ldg(bk + 2 * ep)};
+                const double vj[3] = {V[nj], V[np + nj], V[2 * np + nj]};
 #pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const double b0 = __ldg(bt + (3 * k) * ep + e), b1 = __ldg(bt + (3 * k + 1) * ep + e),
-                             b2 = __ldg(bt + (3 * k + 2) * ep + e);
-                double bk[3];
+                for (int r = 0; r < 3; ++r) {
 #pragma unroll
-                for (int c = 0; c < 3; ++c) bk[c] = (b0 * Fi[0][c] + b1 * Fi[1][c]) + b2 * Fi[2][c];
-                vel[0][k] = V[n[k]];
-                vel[1][k] = V[np + n[k]];
-                vel[2][k] = V[2 * np + n[k]];
+                    for (int c = 0; c < 3; ++c) L0[r][c] = __fma_rn(vj[r], bb[c], L0[r][c]);
 #pragma unroll
-                for (int r = 0; r < 3; ++r)
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) L[r][c] = (k == 0) ? vel[r][k] * bk[c] : L[r][c] + vel[r][k] * bk[c];
-                // pairwise dot ((q0+q1)+(q2+q3)) + ((q4+q5)+(q6+q7)) per direction
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    const double q = vel[c][k] * bk[c];
-                    if (k == 0 || k == 2 || k == 4 || k == 6) {
-                        if (k == 0 || k == 4) q01[c] = q; else q23[c] = q;
-                    } else if (k == 1) {
-                        q01[c] = q01[c] + q;
-                    } else if (k == 3) {
-                        q23[c] = q23[c] + q;
-                        q0123[c] = q01[c] + q23[c];
-                    } else if (k == 5) {
-                        q45[c] = q01[c] + q;
-                    } else {  // k == 7
-                        const double q67 = q23[c] + q;
-                        const double d = q0123[c] + (q45[c] + q67);
-                        vr = (c == 0) ? d : vr + d;
-                    }
+                    for (int kk = 0; kk < 4; ++kk) VT[r][kk] = tau_of(kk, j) > 0.0 ? VT[r][kk] + vj[r] : VT[r][kk] - vj[r];
                 }
+                nx2 = nx2 + __fma_rn(bb[2], bb[2], __fma_rn(bb[1], bb[1], bb[0] * bb[0]));
             }
+            // L = L0 F^-1 (= v_e b^T, :928); HIA = VT - L0 TX^T (= v_e ATAU^T, :1020-1021)
+            double L[3][3], HIA[3][4];
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    L[r][c] = __fma_rn(L0[r][2], Fi[2][c], __fma_rn(L0[r][1], Fi[1][c], L0[r][0] * Fi[0][c]));
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk)
+                    HIA[r][kk] = VT[r][kk] - __fma_rn(L0[r][2], TX[kk][2], __fma_rn(L0[r][1], TX[kk][1], L0[r][0] * TX[kk][0]));
+            }
+            const double vr = (L[0][0] + L[1][1]) + L[2][2];
             // Jaumann stress update (:930-973)
             double eps[6];
-            eps[0] = L[0][0];
-            eps[1] = L[1][1];
-            eps[2] = L[2][2];
-            eps[3] = (L[0][1] + L[1][0]) / 2.0;
-            eps[4] = (L[0][2] + L[2][0]) / 2.0;
-            eps[5] = (L[1][2] + L[2][1]) / 2.0;
-#pragma unroll
-            for (int i = 0; i < 6; ++i) eps[i] = eps[i] * dt1;
+            eps[0] = L[0][0] * dt1;
+            eps[1] = L[1][1] * dt1;
+            eps[2] = L[2][2] * dt1;
+            eps[3] = (L[0][1] + L[1][0]) / 2.0 * dt1;
+            eps[4] = (L[0][2] + L[2][0]) / 2.0 * dt1;
+            eps[5] = (L[1][2] + L[2][1]) / 2.0 * dt1;
             const double w0 = (L[0][1] - L[1][0]) / 2.0;
             const double w1 = (L[0][2] - L[2][0]) / 2.0;
             const double w2 = (L[1][2] - L[2][1]) / 2.0;
@@ -273,89 +320,19 @@ __global__ void __launch_bounds__(kElemThreads) k_element(ElemArrays E, NodeArra
                 }
                 e_int += w * Vc;
             }
-            // hourglass (:1000-1071)
-            double xyz[8][3];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                xyz[k][0] = X[n[k]];
-                xyz[k][1] = X[np + n[k]];
-                xyz[k][2] = X[2 * np + n[k]];
-            }
-            {  // min_ele_edge (:1173-1220)
-                constexpr int A0[12] = {0, 1, 2, 3, 4, 5, 6, 7, 0, 1, 2, 3};
-                constexpr int A1[12] = {1, 2, 3, 0, 5, 6, 7, 4, 4, 5, 6, 7};
-                double m = DBL_MAX;
-#pragma unroll
-                for (int k = 0; k < 12; ++k) {
-                    const double dx = xyz[A1[k]][0] - xyz[A0[k]][0];
-                    const double dy = xyz[A1[k]][1] - xyz[A0[k]][1];
-                    const double dz = xyz[A1[k]][2] - xyz[A0[k]][2];
-                    const double t = dx * dx + dy * dy + dz * dz;
-                    m = t < m ? t : m;
-                }
-                len = sqrt(m);
-            }
-            // TAU * xyz: the Gamma entries are +-1, so each product is exact
-            double TX[4][3];
-#pragma unroll
-            for (int kk = 0; kk < 4; ++kk)
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    double t = tau_sign(kk, 0) > 0 ? xyz[0][c] : -xyz[0][c];
-#pragma unroll
-                    for (int j = 1; j < 8; ++j) t = tau_sign(kk, j) > 0 ? t + xyz[j][c] : t - xyz[j][c];
-                    TX[kk][c] = t;
-                }
-            // NX2 = ||B0^T||^2 in the reference's two-lane pairwise order
-            double nx2;
-            {
-                double l0[12], l1[12];
-#pragma unroll
-                for (int c = 0; c < 3; ++c)
-#pragma unroll
-                    for (int a = 0; a < 8; ++a) {
-                        const double b = __ldg(bt + (3 * a + c) * ep + e);
-                        const int lin = 8 * c + a;
-                        if (lin & 1) l1[lin >> 1] = b * b; else l0[lin >> 1] = b * b;
-                    }
-                const double a0 = ((l0[0] + (l0[1] + l0[2])) + (l0[3] + (l0[4] + l0[5]))) +
-                                  ((l0[6] + (l0[7] + l0[8])) + (l0[9] + (l0[10] + l0[11])));
-                const double a1 = ((l1[0] + (l1[1] + l1[2])) + (l1[3] + (l1[4] + l1[5]))) +
-                                  ((l1[6] + (l1[7] + l1[8])) + (l1[9] + (l1[10] + l1[11])));
-                nx2 = a0 + a1;
-            }
-            double AT[4][8];
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const double b0 = __ldg(bt + (3 * j) * ep + e), b1 = __ldg(bt + (3 * j + 1) * ep + e),
-                             b2 = __ldg(bt + (3 * j + 2) * ep + e);
-#pragma unroll
-                for (int kk = 0; kk < 4; ++kk) {
-                    const double t = (TX[kk][0] * b0 + TX[kk][1] * b1) + TX[kk][2] * b2;
-                    AT[kk][j] = static_cast<double>(tau_sign(kk, j)) - t;
-                }
-            }
-            double HIA[3][4];
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int kk = 0; kk < 4; ++kk) {
-                    double t = vel[i][0] * AT[kk][0];
-#pragma unroll
-                    for (int j = 1; j < 8; ++j) t = t + vel[i][j] * AT[kk][j];
-                    HIA[i][kk] = t;
-                }
+            // hourglass coefficients and history (:1038-1050); Gq = QIA + CR HIA
             const double r43 = 4.0 / 3.0;
             const double r1s8 = 1.0 / sqrt(8.0);
             const double DR = M.c_dr * (r43 * G + M.K) * 0.1 * nx2 * Vc * r1s8 * dt1;
             const double CR = M.c_cr * M.rho * V0 / Vc * E.cbrt_v0sq[e] * M.wos / 4.0;
-            double Q[3][4];
+            double Gq[3][4];
 #pragma unroll
             for (int i = 0; i < 3; ++i)
 #pragma unroll
                 for (int kk = 0; kk < 4; ++kk) {
-                    Q[i][kk] = qia[(4 * i + kk) * ep + e] + DR * HIA[i][kk];
-                    if (!INIT) qia[(4 * i + kk) * ep + e] = Q[i][kk];
+                    const double q = __fma_rn(DR, HIA[i][kk], qia[(4 * i + kk) * ep + e]);
+                    if (!INIT) qia[(4 * i + kk) * ep + e] = q;
+                    Gq[i][kk] = __fma_rn(CR, HIA[i][kk], q);
                 }
             // bulk viscosity pressure (:1073-1109)
             const bool visc = !(fabs(vr) < 1.0e-10);
@@ -367,34 +344,48 @@ __global__ void __launch_bounds__(kElemThreads) k_element(ElemArrays E, NodeArra
                 pv = rho_c * l0 * (M.cvisq * M.cvisq * l0 * vr * m0 - M.cvisl * M.wos * vr);
                 e_vis += -(pv * Vc * vr) * dt1;
             }
-            // nodal forces: f = ((0 - b^T sigma V) - hourglass) + viscosity
-            double hpow = 0.0;
+            // Z = Vc F^-1 (sigma - p I) - W^T, W = Gq TX
+            const double Sp[3][3] = {{s[0] - pv, s[3], s[4]}, {s[3], s[1] - pv, s[5]}, {s[4], s[5], s[2] - pv}};
+            double W[3][3], Z[3][3];
 #pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    W[i][c] = __fma_rn(Gq[i][3], TX[3][c],
+                                       __fma_rn(Gq[i][2], TX[2][c], __fma_rn(Gq[i][1], TX[1][c], Gq[i][0] * TX[0][c])));
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+                    Z[c][i] = Vc * __fma_rn(Fi[c][2], Sp[2][i], __fma_rn(Fi[c][1], Sp[1][i], Fi[c][0] * Sp[0][i])) - W[i][c];
+            // hourglass power sum_j h_j . v_j = Gq : VT - W : L0
+            {
+                double hp = 0.0, wl = 0.0;
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int kk = 0; kk < 4; ++kk) hp = __fma_rn(Gq[i][kk], VT[i][kk], hp);
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) wl = __fma_rn(W[i][c], L0[i][c], wl);
+                e_hg += (hp - wl) * dt1;
+            }
+            // nodal forces f_j = -(B0_j Z) - Gamma_j Gq^T
+            // (= -b_j sigma V - h_j + p b_j V: :985-997, :1070, :1106)
+#pragma unroll ENSC_NODE_UNROLL_FP64
             for (int j = 0; j < 8; ++j) {
-                const double b0 = __ldg(bt + (3 * j) * ep + e), b1 = __ldg(bt + (3 * j + 1) * ep + e),
-                             b2 = __ldg(bt + (3 * j + 2) * ep + e);
-                double bj[3];
-#pragma unroll
-                for (int c = 0; c < 3; ++c) bj[c] = (b0 * Fi[0][c] + b1 * Fi[1][c]) + b2 * Fi[2][c];
-                double fj[3];
-                fj[0] = 0.0 - ((bj[0] * s[0] + bj[1] * s[3]) + bj[2] * s[4]) * Vc;
-                fj[1] = 0.0 - ((bj[0] * s[3] + bj[1] * s[1]) + bj[2] * s[5]) * Vc;
-                fj[2] = 0.0 - ((bj[0] * s[4] + bj[1] * s[5]) + bj[2] * s[2]) * Vc;
+                const double* bk = bte + 3 * j * ep;
+                const double b0 = __ldg(bk), b1 = __ldg(bk + ep), b2 = __ldg(bk + 2 * ep);
+                double* fej = fe + 3 * j * ep + e;
 #pragma unroll
                 for (int i = 0; i < 3; ++i) {
-                    double hgs = 0.0;
+                    double tg = tau_of(0, j) > 0.0 ? Gq[i][0] : -Gq[i][0];
 #pragma unroll
-                    for (int kk = 0; kk < 4; ++kk) hgs = hgs + Q[i][kk] * AT[kk][j];
-                    const double hgd = (AT[0][j] * HIA[i][0] + AT[1][j] * HIA[i][1]) +
-                                       (AT[2][j] * HIA[i][2] + AT[3][j] * HIA[i][3]);
-                    const double h = hgs + hgd * CR;
-                    fj[i] = fj[i] - h;
-                    hpow = hpow + h * vel[i][j];
-                    if (visc) fj[i] = fj[i] + pv * bj[i] * Vc;
-                    fe[(3 * j + i) * ep + e] = fj[i];
+                    for (int kk = 1; kk < 4; ++kk) tg = tau_of(kk, j) > 0.0 ? tg + Gq[i][kk] : tg - Gq[i][kk];
+                    fej[i * ep] = -__fma_rn(b2, Z[2][i], __fma_rn(b1, Z[1][i], b0 * Z[0][i])) - tg;
                 }
             }
-            e_hg += hpow * dt1;
             // compute_dtStable (:828-834)
             {
                 const double cd = M.wos;
@@ -402,7 +393,7 @@ __global__ void __launch_bounds__(kElemThreads) k_element(ElemArrays E, NodeArra
                 const double xi = M.cvisl - M.cvisq * M.cvisq * len / cd * m0;
                 dts = (sqrt(1.0 + xi * xi) - xi) * len / cd;
             }
-            if (!(J > 0.0) || !isfinite(dts)) bad |= (isfinite(dts) ? 0 : ST_NONFINITE);
+            if (!isfinite(dts)) bad |= ST_NONFINITE;
         }
         dts_min = dts < dts_min ? dts : dts_min;
         len_min = len < len_min ? len : len_min;

@@ -9,6 +9,27 @@
 namespace ensc {
 
 constexpr int kElemThreads = 128;
+
+// Minimum resident blocks per SM requested from the compiler for the element
+// passes (register budget = 65536 / (128 * minb)); tuned on B200.
+#ifndef ENSC_ELEM_MINB_FP64
+#define ENSC_ELEM_MINB_FP64 3
+#endif
+#ifndef ENSC_ELEM_MINB_MIXED
+#define ENSC_ELEM_MINB_MIXED 6
+#endif
+// Unroll factor of the element passes' loops over the 8 nodes: more in-flight
+// gathers per thread against more live registers.
+#ifndef ENSC_NODE_UNROLL_FP64
+#define ENSC_NODE_UNROLL_FP64 8
+#endif
+#ifndef ENSC_NODE_UNROLL_MIXED
+#define ENSC_NODE_UNROLL_MIXED 4
+#endif
+// L2 bulk prefetch of the next grid-stride tile in the element passes.
+#ifndef ENSC_PREFETCH
+#define ENSC_PREFETCH 0
+#endif
 constexpr int kNodeThreads = 256;
 constexpr int kCtlThreads = 256;
 

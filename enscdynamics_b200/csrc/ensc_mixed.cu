@@ -28,14 +28,6 @@ __device__ __forceinline__ float cof3f(const float m[3][3], int i, int j) {
     return m[i1][j1] * m[i2][j2] - m[i1][j2] * m[i2][j1];
 }
 
-__device__ __forceinline__ constexpr int tau_s(int k, int j) {
-    constexpr int T[4][8] = {{1, -1, 1, -1, 1, -1, 1, -1},
-                             {-1, -1, 1, 1, 1, 1, -1, -1},
-                             {-1, 1, 1, -1, 1, -1, -1, 1},
-                             {-1, 1, -1, 1, 1, -1, 1, -1}};
-    return T[k][j];
-}
-
 __device__ __forceinline__ double warp_sum_d(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -94,10 +86,18 @@ __device__ __forceinline__ void block_min2_d(double a, double b, unsigned long l
 // Element pass (add_inForce_to_rhs element loop body, exDyna3D.cpp:556-573)
 // in FP32.  Node coordinates enter as offsets from the element's node 0,
 // formed in FP64 before rounding, so hourglass projections and edge lengths
-// keep their precision far from the origin.
+// keep their precision far from the origin.  The nodes are streamed twice
+// (kinematics, then forces) with per-node rows of b^T and ATAU recomputed, so
+// only accumulators stay live.  The hourglass force uses the reassociated
+// sum  sum_k ATAU(k,j) (QIA(i,k) + CR HIA(i,k))  (exDyna3D.cpp:1053-1070).
+__device__ __forceinline__ float tau_f(int k, int j) {
+    constexpr unsigned kMask = 0x55u | (0x3Cu << 8) | (0x96u << 16) | (0x5Au << 24);
+    return ((kMask >> (8 * k + j)) & 1u) ? 1.f : -1.f;
+}
+
 template <bool PLASTIC, bool INIT>
-__global__ void __launch_bounds__(kElemThreads) k_element_mixed(ElemArrays E, NodeArrays N, Material M, Ctl* ctl,
-                                                                Partials P) {
+__global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_MIXED)
+    k_element_mixed(ElemArrays E, NodeArrays N, Material M, Ctl* ctl, Partials P) {
     if (ctl->done) return;
     const float dt1 = INIT ? 0.f : static_cast<float>(ctl->dt_i_1);
     const double dt1d = INIT ? 0.0 : ctl->dt_i_1;
@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(kElemThreads) k_element_mixed(ElemArrays E, No
     const double* __restrict__ X = N.x;
     const double* __restrict__ U = N.u;
     const float* __restrict__ V = static_cast<const float*>(N.v);
-    const float G = static_cast<float>(M.G), lam = static_cast<float>(M.lambda), K = static_cast<float>(M.K);
+    const float G = static_cast<float>(M.G), lam = static_cast<float>(M.lambda);
     const float rho = static_cast<float>(M.rho), wos = static_cast<float>(M.wos);
     const float cvisl = static_cast<float>(M.cvisl), cvisq = static_cast<float>(M.cvisq);
     const float y0 = static_cast<float>(M.yield0), H = static_cast<float>(M.hardening);
@@ -125,34 +125,72 @@ __global__ void __launch_bounds__(kElemThreads) k_element_mixed(ElemArrays E, No
 
     const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
     for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < ne; e += stride) {
-        uint32_t n[8];
+        if (ENSC_PREFETCH && E.tiles_aligned) {
+            const int lane = threadIdx.x & 31;
+            const int64_t tn = e - lane + stride;
+            if (tn < ne) {
+                prefetch_tile(conn, ep, 8, tn, lane);
+                prefetch_tile(bt, ep, 24, tn, lane);
+                prefetch_tile(sig, ep, 6, tn, lane);
+                prefetch_tile(qia, ep, 12, tn, lane);
+                if (lane == 0) {
+                    prefetch_l2(vol0 + tn, 128);
+                    prefetch_l2(cb + tn, 128);
+                    if (PLASTIC) prefetch_l2(epsp + tn, 128);
+                }
+            }
+        }
+        const float* __restrict__ bte = bt + e;
+        const uint32_t n0 = __ldg(conn + e);
+        const double x00 = X[n0], x01 = X[np + n0], x02 = X[2 * np + n0];
+        // hourglass projections (TAU x = TAU (x - x0): the Gamma rows sum to
+        // zero) and minimum edge from coordinates relative to node 0
+        float TX[4][3];
+        float len;
+        {
+            float xr[8][3];
+            xr[0][0] = xr[0][1] = xr[0][2] = 0.f;
 #pragma unroll
-        for (int k = 0; k < 8; ++k) n[k] = __ldg(conn + k * ep + e);
-        float b[8][3];
+            for (int k = 1; k < 8; ++k) {
+                const uint32_t nk = __ldg(conn + k * ep + e);
+                xr[k][0] = static_cast<float>(X[nk] - x00);
+                xr[k][1] = static_cast<float>(X[np + nk] - x01);
+                xr[k][2] = static_cast<float>(X[2 * np + nk] - x02);
+            }
 #pragma unroll
-        for (int k = 0; k < 8; ++k)
+            for (int kk = 0; kk < 4; ++kk)
 #pragma unroll
-            for (int c = 0; c < 3; ++c) b[k][c] = __ldg(bt + (3 * k + c) * ep + e);
-        // F = I + u_e B0^T
+                for (int c = 0; c < 3; ++c) {
+                    float t = 0.f;
+#pragma unroll
+                    for (int j = 1; j < 8; ++j) t += tau_f(kk, j) * xr[j][c];
+                    TX[kk][c] = t;
+                }
+            constexpr int A0[12] = {0, 1, 2, 3, 4, 5, 6, 7, 0, 1, 2, 3};
+            constexpr int A1[12] = {1, 2, 3, 0, 5, 6, 7, 4, 4, 5, 6, 7};
+            float m = FLT_MAX;
+#pragma unroll
+            for (int k = 0; k < 12; ++k) {
+                const float dx = xr[A1[k]][0] - xr[A0[k]][0];
+                const float dy = xr[A1[k]][1] - xr[A0[k]][1];
+                const float dz = xr[A1[k]][2] - xr[A0[k]][2];
+                m = fminf(m, fmaf(dz, dz, fmaf(dy, dy, dx * dx)));
+            }
+            len = sqrtf(m);
+        }
+        // F = I + u_e B0^T (B0^T rows are re-read per pass; they stay in L1)
         float F[3][3] = {{1.f, 0.f, 0.f}, {0.f, 1.f, 0.f}, {0.f, 0.f, 1.f}};
-        float vel[3][8];
-        float xr[8][3];
-        const double x00 = X[n[0]], x01 = X[np + n[0]], x02 = X[2 * np + n[0]];
-#pragma unroll
+#pragma unroll ENSC_NODE_UNROLL_MIXED
         for (int k = 0; k < 8; ++k) {
-            const float u0 = static_cast<float>(U[n[k]]), u1 = static_cast<float>(U[np + n[k]]),
-                        u2 = static_cast<float>(U[2 * np + n[k]]);
-            const float uu[3] = {u0, u1, u2};
+            const uint32_t nk = __ldg(conn + k * ep + e);
+            const float uu[3] = {static_cast<float>(U[nk]), static_cast<float>(U[np + nk]),
+                                 static_cast<float>(U[2 * np + nk])};
+            const float* bk = bte + 3 * k * ep;
+            const float bb[3] = {__ldg(bk), __ldg(bk + ep), __ldg(bk + 2 * ep)};
 #pragma unroll
             for (int r = 0; r < 3; ++r)
 #pragma unroll
-                for (int c = 0; c < 3; ++c) F[r][c] = fmaf(uu[r], b[k][c], F[r][c]);
-            vel[0][k] = V[n[k]];
-            vel[1][k] = V[np + n[k]];
-            vel[2][k] = V[2 * np + n[k]];
-            xr[k][0] = static_cast<float>(X[n[k]] - x00);
-            xr[k][1] = static_cast<float>(X[np + n[k]] - x01);
-            xr[k][2] = static_cast<float>(X[2 * np + n[k]] - x02);
+                for (int c = 0; c < 3; ++c) F[r][c] = fmaf(uu[r], bb[c], F[r][c]);
         }
         const float J = det3f(F);
         if (!(J > 0.f)) bad |= ST_INVERTED;
@@ -162,17 +200,32 @@ __global__ void __launch_bounds__(kElemThreads) k_element_mixed(ElemArrays E, No
         for (int i = 0; i < 3; ++i)
 #pragma unroll
             for (int j = 0; j < 3; ++j) Fi[i][j] = cof3f(F, j, i) * invdet;
-        // b^T = B0^T F^-1, L = v_e b^T
-        float L[3][3] = {};
+        // L0 = v_e B0^T, VT = v_e Gamma^T, NX2
+        float L0[3][3] = {}, VT[3][4] = {}, nx2 = 0.f;
+#pragma unroll ENSC_NODE_UNROLL_MIXED
+        for (int j = 0; j < 8; ++j) {
+            const uint32_t nj = __ldg(conn + j * ep + e);
+            const float vj[3] = {V[nj], V[np + nj], V[2 * np + nj]};
+            const float* bk = bte + 3 * j * ep;
+            const float bb[3] = {__ldg(bk), __ldg(bk + ep), __ldg(bk + 2 * ep)};
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            float bk[3];
+            for (int r = 0; r < 3; ++r) {
 #pragma unroll
-            for (int c = 0; c < 3; ++c) bk[c] = b[k][0] * Fi[0][c] + b[k][1] * Fi[1][c] + b[k][2] * Fi[2][c];
+                for (int c = 0; c < 3; ++c) L0[r][c] = fmaf(vj[r], bb[c], L0[r][c]);
 #pragma unroll
-            for (int r = 0; r < 3; ++r)
+                for (int kk = 0; kk < 4; ++kk) VT[r][kk] += tau_f(kk, j) * vj[r];
+            }
+            nx2 += fmaf(bb[2], bb[2], fmaf(bb[1], bb[1], bb[0] * bb[0]));
+        }
+        // L = L0 F^-1, HIA = VT - L0 TX^T
+        float L[3][3], HIA[3][4];
 #pragma unroll
-                for (int c = 0; c < 3; ++c) L[r][c] = fmaf(vel[r][k], bk[c], L[r][c]);
+        for (int r = 0; r < 3; ++r) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) L[r][c] = fmaf(L0[r][2], Fi[2][c], fmaf(L0[r][1], Fi[1][c], L0[r][0] * Fi[0][c]));
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk)
+                HIA[r][kk] = VT[r][kk] - fmaf(L0[r][2], TX[kk][2], fmaf(L0[r][1], TX[kk][1], L0[r][0] * TX[kk][0]));
         }
         const float vr = L[0][0] + L[1][1] + L[2][2];
         // Jaumann stress update
@@ -223,91 +276,63 @@ __global__ void __launch_bounds__(kElemThreads) k_element_mixed(ElemArrays E, No
             for (int i = 0; i < 6; ++i) w += (i < 3 ? 0.5f : 1.0f) * (so[i] + s[i]) * eps[i];
             e_int += static_cast<double>(w * Vc);
         }
-        // min edge
-        float len;
-        {
-            constexpr int A0[12] = {0, 1, 2, 3, 4, 5, 6, 7, 0, 1, 2, 3};
-            constexpr int A1[12] = {1, 2, 3, 0, 5, 6, 7, 4, 4, 5, 6, 7};
-            float m = FLT_MAX;
-#pragma unroll
-            for (int k = 0; k < 12; ++k) {
-                const float dx = xr[A1[k]][0] - xr[A0[k]][0];
-                const float dy = xr[A1[k]][1] - xr[A0[k]][1];
-                const float dz = xr[A1[k]][2] - xr[A0[k]][2];
-                m = fminf(m, dx * dx + dy * dy + dz * dz);
-            }
-            len = sqrtf(m);
-        }
-        // hourglass: the Gamma vectors sum to zero, so TAU x = TAU (x - x0)
-        float TX[4][3];
-#pragma unroll
-        for (int kk = 0; kk < 4; ++kk)
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                float t = 0.f;
-#pragma unroll
-                for (int j = 1; j < 8; ++j) t += tau_s(kk, j) > 0 ? xr[j][c] : -xr[j][c];
-                TX[kk][c] = t;
-            }
-        float nx2 = 0.f;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) nx2 += b[k][0] * b[k][0] + b[k][1] * b[k][1] + b[k][2] * b[k][2];
-        float AT[4][8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j)
-#pragma unroll
-            for (int kk = 0; kk < 4; ++kk)
-                AT[kk][j] = static_cast<float>(tau_s(kk, j)) - (TX[kk][0] * b[j][0] + TX[kk][1] * b[j][1] +
-                                                                TX[kk][2] * b[j][2]);
-        float HIA[3][4];
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int kk = 0; kk < 4; ++kk) {
-                float t = 0.f;
-#pragma unroll
-                for (int j = 0; j < 8; ++j) t = fmaf(vel[i][j], AT[kk][j], t);
-                HIA[i][kk] = t;
-            }
         const float DR = DRc * nx2 * Vc * dt1;
-        const float CR = CRc * V0 / Vc * (cb[e] * cb[e]);
-        float Q[3][4];
+        const float cbe = cb[e];
+        const float CR = CRc * V0 / Vc * (cbe * cbe);
+        float Gq[3][4];
 #pragma unroll
         for (int i = 0; i < 3; ++i)
 #pragma unroll
             for (int kk = 0; kk < 4; ++kk) {
-                Q[i][kk] = qia[(4 * i + kk) * ep + e] + DR * HIA[i][kk];
-                if (!INIT) qia[(4 * i + kk) * ep + e] = Q[i][kk];
+                const float q = fmaf(DR, HIA[i][kk], qia[(4 * i + kk) * ep + e]);
+                if (!INIT) qia[(4 * i + kk) * ep + e] = q;
+                Gq[i][kk] = fmaf(CR, HIA[i][kk], q);
             }
         const bool visc = !(fabsf(vr) < 1.0e-10f);
         float pv = 0.f;
         if (visc) {
-            const float l0 = cb[e];
             const float m0 = fminf(vr, 0.f);
-            pv = rho / J * l0 * (cvisq * cvisq * l0 * vr * m0 - cvisl * wos * vr);
+            pv = rho / J * cbe * (cvisq * cvisq * cbe * vr * m0 - cvisl * wos * vr);
             e_vis += -static_cast<double>(pv * Vc * vr) * dt1d;
         }
-        float hpow = 0.f;
+        // Z = Vc F^-1 (sigma - p I) - W^T, W = Gq TX
+        const float Sp[3][3] = {{s[0] - pv, s[3], s[4]}, {s[3], s[1] - pv, s[5]}, {s[4], s[5], s[2] - pv}};
+        float W[3][3], Z[3][3];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            float bj[3];
+        for (int i = 0; i < 3; ++i)
 #pragma unroll
-            for (int c = 0; c < 3; ++c) bj[c] = b[j][0] * Fi[0][c] + b[j][1] * Fi[1][c] + b[j][2] * Fi[2][c];
-            float fj[3];
-            fj[0] = -(bj[0] * s[0] + bj[1] * s[3] + bj[2] * s[4]) * Vc;
-            fj[1] = -(bj[0] * s[3] + bj[1] * s[1] + bj[2] * s[5]) * Vc;
-            fj[2] = -(bj[0] * s[4] + bj[1] * s[5] + bj[2] * s[2]) * Vc;
+            for (int c = 0; c < 3; ++c)
+                W[i][c] = fmaf(Gq[i][3], TX[3][c], fmaf(Gq[i][2], TX[2][c], fmaf(Gq[i][1], TX[1][c], Gq[i][0] * TX[0][c])));
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+                Z[c][i] = Vc * fmaf(Fi[c][2], Sp[2][i], fmaf(Fi[c][1], Sp[1][i], Fi[c][0] * Sp[0][i])) - W[i][c];
+        {
+            float hp = 0.f;
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
-                const float hgs = Q[i][0] * AT[0][j] + Q[i][1] * AT[1][j] + Q[i][2] * AT[2][j] + Q[i][3] * AT[3][j];
-                const float hgd = AT[0][j] * HIA[i][0] + AT[1][j] * HIA[i][1] + AT[2][j] * HIA[i][2] +
-                                  AT[3][j] * HIA[i][3];
-                const float h = hgs + hgd * CR;
-                hpow = fmaf(h, vel[i][j], hpow);
-                fe[(3 * j + i) * ep + e] = fj[i] - h + pv * bj[i] * Vc;
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk) hp = fmaf(Gq[i][kk], VT[i][kk], hp);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) hp = fmaf(-W[i][c], L0[i][c], hp);
+            }
+            e_hg += static_cast<double>(hp) * dt1d;
+        }
+        // nodal forces f_j = -(B0_j Z) - Gamma_j Gq^T
+#pragma unroll ENSC_NODE_UNROLL_MIXED
+        for (int j = 0; j < 8; ++j) {
+            const float* bk = bte + 3 * j * ep;
+            const float b0 = __ldg(bk), b1 = __ldg(bk + ep), b2 = __ldg(bk + 2 * ep);
+            float* fej = fe + 3 * j * ep + e;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                float tg = 0.f;
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk) tg += tau_f(kk, j) * Gq[i][kk];
+                fej[i * ep] = -fmaf(b2, Z[2][i], fmaf(b1, Z[1][i], b0 * Z[0][i])) - tg;
             }
         }
-        e_hg += static_cast<double>(hpow) * dt1d;
         // element dt (compute_dtStable, exDyna3D.cpp:828-834)
         const float m0 = fminf(vr, 0.f);
         const float xi = cvisl - cvisq * cvisq * len / wos * m0;

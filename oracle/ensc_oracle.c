@@ -4,16 +4,15 @@
  * cites the reference function it follows (paths relative to the reference
  * project).  Floating-point evaluation order is fixed and documented here;
  * the product's FP64 CUDA kernel evaluates the same expressions in the same
- * order (without FMA contraction), so the two agree bit-for-bit:
- *   - sums over the 8 element nodes or over the 3/4-long inner dimensions of
- *     the small matrix products run left to right (k = 0, 1, ...), except the
- *     ones where the reference's Eigen evaluation was pinned to a different
- *     fixed order (noted at each site);
+ * order (explicit fused multiply-adds only, no contraction), so the two
+ * agree bit-for-bit:
+ *   - sums over the 8 element nodes run node by node with fma; the 3- and
+ *     4-term dot products are spelled out with fma at each site;
  *   - 3x3 determinant and inverse follow Eigen 3.4's closed forms
  *     (Eigen/src/LU/Determinant.h bruteforce_det3_helper and
  *     Eigen/src/LU/InverseImpl.h compute_inverse<...,3>), the library the
  *     reference links.
- * Compiled with -ffp-contract=off so no multiply-add is fused.
+ * Compiled with -ffp-contract=off so only the explicit fma() calls fuse.
  */
 #include "ensc_oracle.h"
 
@@ -124,7 +123,7 @@ static double min_edge(const double xyz[8][3]) {
         const double dx = xyz[E1[k]][0] - xyz[E0[k]][0];
         const double dy = xyz[E1[k]][1] - xyz[E0[k]][1];
         const double dz = xyz[E1[k]][2] - xyz[E0[k]][2];
-        const double t = dx * dx + dy * dy + dz * dz;
+        const double t = fma(dz, dz, fma(dy, dy, dx * dx));
         if (t < m) m = t;
     }
     return sqrt(m);
@@ -139,7 +138,20 @@ static void gather_xyz(const ensc_oracle_state* s, int64_t e, double xyz[8][3]) 
  * (reinit_some_CellData :888-918), Jaumann stress (:920-998) with the optional
  * J2 return, hourglass (:1000-1071), bulk viscosity (:1073-1109) and the
  * element dt (:828-834).  Writes the 8x3 element force f; returns dtStable.
- * de[0..2] receive the element's internal/hourglass/viscous work increments. */
+ * de[0..2] receive the element's internal/hourglass/viscous work increments.
+ *
+ * The same quantities as the reference, regrouped so the per-node work is
+ * a few accumulations (shared with the GPU kernel, operation for operation):
+ *   L0  = v_e B0^T                 (3x3, sum over nodes)
+ *   VT  = v_e Gamma^T              (3x4, signed sums, exact)
+ *   L   = L0 F^-1                  (= v_e b^T, :928)
+ *   HIA = VT - L0 TX^T             (= v_e ATAU^T with ATAU = Gamma - TX B0, :1020-1021)
+ *   Gq  = QIA + CR HIA             (hourglass force h_j = ATAU_j^T Gq, :1053-1067)
+ *   W   = Gq TX                    (3x3)
+ *   Z   = Vc F^-1 (sigma - p I) - W^T
+ *   f_j = -(B0_j Z) - Gamma_j Gq^T (= -b_j sigma V - h_j + p b_j V, :985-997, :1070, :1106)
+ * Sums over the 8 nodes run node by node from 0.0 with fma (one rounding per
+ * term); short dot products are spelled out with fma at each site. */
 static double element(const ensc_oracle_params* p, ensc_oracle_state* s, int64_t e, double dt1,
                       double f[8][3], double de[3]) {
     const uint32_t* cn = s->conn + 8 * e;
@@ -153,40 +165,44 @@ static double element(const ensc_oracle_params* p, ensc_oracle_state* s, int64_t
             ue[c][a] = s->u[3 * n + c];
         }
     }
+    /* hourglass base projections TX = Gamma xyz (exact: entries are +-1) */
+    double TX[4][3];
+    for (int k = 0; k < 4; ++k)
+        for (int c = 0; c < 3; ++c) {
+            double t = TAU[k][0] > 0 ? xyz[0][c] : -xyz[0][c];
+            for (int j = 1; j < 8; ++j) t = TAU[k][j] > 0 ? t + xyz[j][c] : t - xyz[j][c];
+            TX[k][c] = t;
+        }
     /* F = I + u_e B0^T (:862-865) */
     double F[3][3];
     for (int r = 0; r < 3; ++r)
         for (int c = 0; c < 3; ++c) {
-            double t = ue[r][0] * BT[c];
-            for (int k = 1; k < 8; ++k) t += ue[r][k] * BT[3 * k + c];
-            F[r][c] = (r == c ? 1.0 : 0.0) + t;
+            double t = 0.0;
+            for (int k = 0; k < 8; ++k) t = fma(ue[r][k], BT[3 * k + c], t);
+            F[r][c] = (r == c) ? 1.0 + t : t;
         }
     const double J = det3(F); /* :867-870 */
     double Fi[3][3];
     inv3(F, Fi);
-    /* b^T = B0^T F^-1 (:872-875) */
-    double bT[8][3];
-    for (int a = 0; a < 8; ++a)
-        for (int c = 0; c < 3; ++c)
-            bT[a][c] = (BT[3 * a] * Fi[0][c] + BT[3 * a + 1] * Fi[1][c]) + BT[3 * a + 2] * Fi[2][c];
-    /* VolRate (:877-885): three dot products over the 8 nodes.  The reference's
-     * Eigen dot of a strided row with a contiguous column is a pairwise tree
-     * ((n0+n1)+(n2+n3)) + ((n4+n5)+(n6+n7)); restated in that order. */
-    double vr = 0.0;
-    for (int c = 0; c < 3; ++c) {
-        double q[8];
-        for (int a = 0; a < 8; ++a) q[a] = vel[c][a] * bT[a][c];
-        const double d = ((q[0] + q[1]) + (q[2] + q[3])) + ((q[4] + q[5]) + (q[6] + q[7]));
-        vr = (c == 0) ? d : vr + d;
-    }
-    /* L = v_e b^T (:928) */
-    double L[3][3];
-    for (int r = 0; r < 3; ++r)
-        for (int c = 0; c < 3; ++c) {
-            double t = vel[r][0] * bT[0][c];
-            for (int k = 1; k < 8; ++k) t += vel[r][k] * bT[k][c];
-            L[r][c] = t;
+    /* per-node accumulations */
+    double L0[3][3] = {{0.0}}, VT[3][4] = {{0.0}}, nx2 = 0.0;
+    for (int j = 0; j < 8; ++j) {
+        const double b0 = BT[3 * j], b1 = BT[3 * j + 1], b2 = BT[3 * j + 2];
+        const double bb[3] = {b0, b1, b2};
+        for (int r = 0; r < 3; ++r) {
+            for (int c = 0; c < 3; ++c) L0[r][c] = fma(vel[r][j], bb[c], L0[r][c]);
+            for (int k = 0; k < 4; ++k) VT[r][k] = TAU[k][j] > 0 ? VT[r][k] + vel[r][j] : VT[r][k] - vel[r][j];
         }
+        nx2 = nx2 + fma(b2, b2, fma(b1, b1, b0 * b0));
+    }
+    double L[3][3], HIA[3][4];
+    for (int r = 0; r < 3; ++r) {
+        for (int c = 0; c < 3; ++c) L[r][c] = fma(L0[r][2], Fi[2][c], fma(L0[r][1], Fi[1][c], L0[r][0] * Fi[0][c]));
+        for (int k = 0; k < 4; ++k)
+            HIA[r][k] = VT[r][k] - fma(L0[r][2], TX[k][2], fma(L0[r][1], TX[k][1], L0[r][0] * TX[k][0]));
+    }
+    /* VolRate = tr L (:877-885) */
+    const double vr = (L[0][0] + L[1][1]) + L[2][2];
     double eps[6];
     eps[0] = L[0][0];
     eps[1] = L[1][1];
@@ -252,92 +268,57 @@ static double element(const ensc_oracle_params* p, ensc_oracle_state* s, int64_t
         }
         de[0] = w * Vc;
     }
-    /* f -= b^T sigma V (:985-997) */
-    for (int a = 0; a < 8; ++a) {
-        const double fx = (bT[a][0] * sg[0] + bT[a][1] * sg[3] + bT[a][2] * sg[4]) * Vc;
-        const double fy = (bT[a][0] * sg[3] + bT[a][1] * sg[1] + bT[a][2] * sg[5]) * Vc;
-        const double fz = (bT[a][0] * sg[4] + bT[a][1] * sg[5] + bT[a][2] * sg[2]) * Vc;
-        f[a][0] = 0.0 - fx;
-        f[a][1] = 0.0 - fy;
-        f[a][2] = 0.0 - fz;
-    }
-    /* hourglass (:1000-1071) */
-    {
-        const double C2 = 0.1;
-        const double r43 = 4.0 / 3.0;
-        const double r1s8 = 1.0 / sqrt(8.0);
-        double TX[4][3]; /* TAU * xyz */
-        for (int k = 0; k < 4; ++k)
-            for (int c = 0; c < 3; ++c) {
-                double t = TAU[k][0] * xyz[0][c];
-                for (int j = 1; j < 8; ++j) t += TAU[k][j] * xyz[j][c];
-                TX[k][c] = t;
-            }
-        double AT[4][8]; /* ATAU = TAU - TX * B0 */
-        for (int k = 0; k < 4; ++k)
-            for (int j = 0; j < 8; ++j)
-                AT[k][j] = TAU[k][j] - ((TX[k][0] * BT[3 * j] + TX[k][1] * BT[3 * j + 1]) + TX[k][2] * BT[3 * j + 2]);
-        double HIA[3][4]; /* v_e ATAU^T */
-        for (int i = 0; i < 3; ++i)
-            for (int k = 0; k < 4; ++k) {
-                double t = vel[i][0] * AT[k][0];
-                for (int j = 1; j < 8; ++j) t += vel[i][j] * AT[k][j];
-                HIA[i][k] = t;
-            }
-        /* NX2 = ||B0^T||_F^2.  Pinned to the reference's vectorised Eigen
-         * reduction: the 24 squares in column-major order split into two
-         * interleaved lanes (even / odd index), each lane summed as a pairwise
-         * tree, then lane0 + lane1. */
-        double nx2;
-        {
-            double sq[24];
-            for (int c = 0; c < 3; ++c)
-                for (int a = 0; a < 8; ++a) sq[8 * c + a] = BT[3 * a + c] * BT[3 * a + c];
-            double l0[12], l1[12];
-            for (int i = 0; i < 12; ++i) {
-                l0[i] = sq[2 * i];
-                l1[i] = sq[2 * i + 1];
-            }
-            /* pairwise tree over 12: (6)+(6), 6 = (3)+(3), 3 = a + (b + c) */
-#define PW3(q, o) ((q)[(o)] + ((q)[(o) + 1] + (q)[(o) + 2]))
-#define PW6(q, o) (PW3(q, o) + PW3(q, (o) + 3))
-            const double a0 = PW6(l0, 0) + PW6(l0, 6);
-            const double a1 = PW6(l1, 0) + PW6(l1, 6);
-#undef PW6
-#undef PW3
-            nx2 = a0 + a1;
+    /* hourglass coefficients and history (:1038-1050) */
+    const double C2 = 0.1;
+    const double r43 = 4.0 / 3.0;
+    const double r1s8 = 1.0 / sqrt(8.0);
+    const double DR = p->c_dr * (r43 * G + p->K) * C2 * nx2 * Vc * r1s8 * dt1;
+    const double CR = p->c_cr * p->rho * V0 / Vc * s->cbrt_v0sq[e] * p->wos / 4.0;
+    double* Q = s->qia + 12 * e;
+    double Gq[3][4];
+    for (int i = 0; i < 3; ++i)
+        for (int k = 0; k < 4; ++k) {
+            Q[4 * i + k] = fma(DR, HIA[i][k], Q[4 * i + k]);
+            Gq[i][k] = fma(CR, HIA[i][k], Q[4 * i + k]);
         }
-        const double Kb = p->K, rho = p->rho, wos = p->wos;
-        const double DR = p->c_dr * (r43 * G + Kb) * C2 * nx2 * Vc * r1s8 * dt1;
-        const double CR = p->c_cr * rho * V0 / Vc * s->cbrt_v0sq[e] * wos / 4.0;
-        double* Q = s->qia + 12 * e;
-        for (int i = 0; i < 3; ++i)
-            for (int k = 0; k < 4; ++k) Q[4 * i + k] += DR * HIA[i][k];
-        double hpow = 0.0;
-        for (int j = 0; j < 8; ++j)
-            for (int i = 0; i < 3; ++i) {
-                double hgs = 0.0;
-                for (int k = 0; k < 4; ++k) hgs += Q[4 * i + k] * AT[k][j];
-                /* HGD = ATAU^T HIA^T: the reference's Eigen product sums the
-                 * 4 terms pairwise, (k0 + k1) + (k2 + k3). */
-                const double hgd = (AT[0][j] * HIA[i][0] + AT[1][j] * HIA[i][1]) +
-                                   (AT[2][j] * HIA[i][2] + AT[3][j] * HIA[i][3]);
-                const double h = hgs + hgd * CR;
-                f[j][i] -= h;
-                hpow += h * vel[i][j];
-            }
-        de[1] = hpow * dt1;
-    }
-    /* bulk viscosity (:1073-1109) */
+    /* bulk viscosity pressure (:1073-1109) */
+    const int visc = !(fabs(vr) < 1.0e-10);
+    double pv = 0.0;
     de[2] = 0.0;
-    if (!(fabs(vr) < 1.0e-10)) {
+    if (visc) {
         const double rho_c = p->rho / J;
         const double len0 = s->cbrt_v0[e];
         const double m0 = vr < 0.0 ? vr : 0.0; /* std::min(zero, VolRate) */
-        const double pv = rho_c * len0 * (p->cvisq * p->cvisq * len0 * vr * m0 - p->cvisl * p->wos * vr);
-        for (int a = 0; a < 8; ++a)
-            for (int c = 0; c < 3; ++c) f[a][c] += pv * bT[a][c] * Vc;
+        pv = rho_c * len0 * (p->cvisq * p->cvisq * len0 * vr * m0 - p->cvisl * p->wos * vr);
         de[2] = -(pv * Vc * vr) * dt1;
+    }
+    /* Z = Vc F^-1 (sigma - p I) - W^T,  W = Gq TX */
+    const double Sp[3][3] = {{sg[0] - pv, sg[3], sg[4]}, {sg[3], sg[1] - pv, sg[5]}, {sg[4], sg[5], sg[2] - pv}};
+    double Z[3][3], W[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int c = 0; c < 3; ++c)
+            W[i][c] = fma(Gq[i][3], TX[3][c], fma(Gq[i][2], TX[2][c], fma(Gq[i][1], TX[1][c], Gq[i][0] * TX[0][c])));
+    for (int c = 0; c < 3; ++c)
+        for (int i = 0; i < 3; ++i)
+            Z[c][i] = Vc * fma(Fi[c][2], Sp[2][i], fma(Fi[c][1], Sp[1][i], Fi[c][0] * Sp[0][i])) - W[i][c];
+    /* nodal forces f_j = -(B0_j Z) - Gamma_j Gq^T */
+    for (int j = 0; j < 8; ++j) {
+        const double b0 = BT[3 * j], b1 = BT[3 * j + 1], b2 = BT[3 * j + 2];
+        for (int i = 0; i < 3; ++i) {
+            double tg = TAU[0][j] > 0 ? Gq[i][0] : -Gq[i][0];
+            for (int k = 1; k < 4; ++k) tg = TAU[k][j] > 0 ? tg + Gq[i][k] : tg - Gq[i][k];
+            f[j][i] = -fma(b2, Z[2][i], fma(b1, Z[1][i], b0 * Z[0][i])) - tg;
+        }
+    }
+    /* hourglass power sum_j h_j . v_j = Gq : VT - W : L0 */
+    {
+        double hp = 0.0;
+        for (int i = 0; i < 3; ++i)
+            for (int k = 0; k < 4; ++k) hp = fma(Gq[i][k], VT[i][k], hp);
+        double wl = 0.0;
+        for (int i = 0; i < 3; ++i)
+            for (int c = 0; c < 3; ++c) wl = fma(W[i][c], L0[i][c], wl);
+        de[1] = (hp - wl) * dt1;
     }
     /* compute_dtStable (:828-834) with this cycle's min edge */
     {
