@@ -123,9 +123,10 @@ def element_pass_bytes(ne: int, nn: int, plastic: bool, mixed: bool = False) -> 
     element-force write 192 per element (+16 eps_p r/w with J2); x, u, v
     gathered once per node (72 B).
     Mixed: connectivity 32, sigma r/w 48, QIA r/w 96, B0^T 96, V0 4, force
-    write 96 (+8 eps_p); x, u FP64 and v FP32 per node (60 B)."""
+    write 96 (+8 eps_p); x FP64 and v FP32 per node (36 B: the mixed pass
+    forms F from current coordinates and does not read u)."""
     if mixed:
-        return ne * (32 + 48 + 96 + 96 + 4 + 96 + (8 if plastic else 0)) + nn * 60
+        return ne * (32 + 48 + 96 + 96 + 4 + 96 + (8 if plastic else 0)) + nn * 36
     return ne * (32 + 96 + 192 + 192 + 8 + 192 + (16 if plastic else 0)) + nn * 72
 
 

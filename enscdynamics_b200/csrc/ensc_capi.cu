@@ -299,6 +299,14 @@ int ensc_create(const ensc_mesh_desc* mesh, const ensc_material* mat, const ensc
             }
             slot = static_cast<uint32_t>(e);
         }
+    // per-node mask of occupied local slots (slot-major force hand-off)
+    std::vector<uint8_t> slot_mask;
+    if (!clash) {
+        slot_mask.assign(static_cast<size_t>(h->nn_pad), 0);
+        for (int k = 0; k < 8; ++k)
+            for (int64_t n = 0; n < nn; ++n)
+                if (ell[k * h->nn_pad + n] != ENSC_NONE) slot_mask[n] |= static_cast<uint8_t>(1u << k);
+    }
     std::vector<int64_t> csr_ptr;
     std::vector<uint32_t> csr_ent;
     if (clash) {
@@ -336,11 +344,12 @@ int ensc_create(const ensc_mesh_desc* mesh, const ensc_material* mat, const ensc
         size_t bytes;
     };
     void *p_conn, *p_bt, *p_vol0, *p_cb, *p_cb2, *p_sig, *p_qia, *p_eps, *p_fe, *p_x, *p_u, *p_v, *p_im, *p_bc,
-        *p_bcv, *p_ell, *p_rf, *p_pe, *p_pn, *p_ctl, *p_cptr = nullptr, *p_cent = nullptr;
+        *p_bcv, *p_ell, *p_rf, *p_pe, *p_pn, *p_ctl, *p_cptr = nullptr, *p_cent = nullptr, *p_mask = nullptr;
+    const int64_t fe_rows = clash ? ep : np;   // slot-major hand-off is indexed by node
     std::vector<Piece> pieces = {
         {&p_conn, 8 * ep * sizeof(uint32_t)}, {&p_bt, 24 * ep * real}, {&p_vol0, ep * 8}, {&p_cb, ep * 8},
         {&p_cb2, ep * 8}, {&p_sig, 6 * ep * real}, {&p_qia, 12 * ep * real}, {&p_eps, ep * real},
-        {&p_fe, 24 * ep * real}, {&p_x, 3 * np * 8}, {&p_u, 3 * np * 8}, {&p_v, 3 * np * real},
+        {&p_fe, static_cast<size_t>(24 * fe_rows) * real}, {&p_x, 3 * np * 8}, {&p_u, 3 * np * 8}, {&p_v, 3 * np * real},
         {&p_im, np * 8}, {&p_bc, static_cast<size_t>(np)}, {&p_bcv, 3 * np * 8},
         {&p_ell, 8 * np * sizeof(uint32_t)}, {&p_rf, 3 * np * 8},
         {&p_pe, 3 * static_cast<size_t>(h->grid_e) * 8}, {&p_pn, 2 * static_cast<size_t>(h->grid_n) * 8},
@@ -348,6 +357,8 @@ int ensc_create(const ensc_mesh_desc* mesh, const ensc_material* mat, const ensc
     if (clash) {
         pieces.push_back({&p_cptr, (nn + 1) * sizeof(int64_t)});
         pieces.push_back({&p_cent, 8 * ne * sizeof(uint32_t)});
+    } else {
+        pieces.push_back({&p_mask, static_cast<size_t>(np)});
     }
     size_t total = 0;
     for (auto& pc : pieces) total += (pc.bytes + 255) / 256 * 256;
@@ -372,7 +383,7 @@ int ensc_create(const ensc_mesh_desc* mesh, const ensc_material* mat, const ensc
     }
     // staging for AoS up/download: reuse the element force scratch when large enough
     const size_t need_stage = std::max<size_t>(12 * ne, 3 * nn) * sizeof(double);
-    if (24 * ep * real >= need_stage) {
+    if (static_cast<size_t>(24 * fe_rows) * real >= need_stage) {
         h->staging = static_cast<double*>(p_fe);
     } else {
         ce = cudaMalloc(reinterpret_cast<void**>(&h->staging), need_stage);
@@ -401,6 +412,7 @@ int ensc_create(const ensc_mesh_desc* mesh, const ensc_material* mat, const ensc
     h->E.eps_p = p_eps;
     h->E.fe = p_fe;
     h->E.tiles_aligned = 1;  // arena pieces are 256-byte aligned, ne_pad % 32 == 0
+    h->E.slot_major = clash ? 0 : 1;
     h->N.nn = nn;
     h->N.nn_pad = np;
     h->N.x = static_cast<double*>(p_x);
@@ -413,6 +425,7 @@ int ensc_create(const ensc_mesh_desc* mesh, const ensc_material* mat, const ensc
     h->N.csr_ptr = clash ? static_cast<int64_t*>(p_cptr) : nullptr;
     h->N.csr_ent = clash ? static_cast<uint32_t*>(p_cent) : nullptr;
     h->N.rf = static_cast<double*>(p_rf);
+    h->N.slot_mask = clash ? nullptr : static_cast<uint8_t*>(p_mask);
     h->P.elem = static_cast<double*>(p_pe);
     h->P.node = static_cast<double*>(p_pn);
     h->P.n_elem_blocks = h->grid_e;
@@ -446,6 +459,7 @@ int ensc_create(const ensc_mesh_desc* mesh, const ensc_material* mat, const ensc
         if (!rc) rc = upload(h, p_ell, ell);
         if (!rc && clash) rc = upload(h, p_cptr, csr_ptr);
         if (!rc && clash) rc = upload(h, p_cent, csr_ent);
+        if (!rc && !clash) rc = upload(h, p_mask, slot_mask);
         if (rc) return fail(rc);
     }
 

@@ -7,8 +7,10 @@
 //     bt[24][ne_pad]                 B0^T row-major per element: (3*k + c)
 //     vol0, cbrt_v0, cbrt_v0sq [ne]  per-element constants
 //     sigma[6][ne_pad], qia[12][ne_pad], eps_p[ne]
-//     fe[24][ne_pad]                 element nodal forces of the current cycle
-//                                    (the element -> node hand-off, scratch)
+//     fe                             element nodal forces of the current cycle
+//                                    (the element -> node hand-off, scratch):
+//                                    [24][nn_pad] by node and local slot when
+//                                    no node repeats a slot, else [24][ne_pad]
 //   node arrays, length nn (stride nn_pad):
 //     x[3][nn_pad], u[3][nn_pad] (FP64 always), v[3][nn_pad]
 //     inv_mass[nn]                   per node (equal for the 3 DOFs)
@@ -80,6 +82,12 @@ struct ElemArrays {
     // 1 when every component array starts 256-byte aligned and ne_pad is a
     // multiple of 32, so whole 32-element tiles may be bulk-prefetched
     int32_t tiles_aligned;
+    // 1: fe is node-major, fe[(3k + c) * nn_pad + conn[k][e]] -- the
+    // reference's per-local-slot nodal vectors (exDyna3D.cpp:523-634), each
+    // entry written by the one element that holds the node in slot k;
+    // 0: fe is element-major, fe[(3k + c) * ne_pad + e], gathered through
+    // ell / csr by the node pass
+    int32_t slot_major;
 };
 
 struct NodeArrays {
@@ -93,6 +101,7 @@ struct NodeArrays {
     const uint32_t* ell;
     const int64_t* csr_ptr;    // non-null: use the general lists
     const uint32_t* csr_ent;   // (e << 3) | slot
+    const uint8_t* slot_mask;  // slot-major forces: bit k set if slot k holds an element
     double* rf;                // reactions, [3][nn_pad]
 };
 

@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_FP64) k_element(E
             }
             // F = I + u_e B0^T (:862-865)
             double F[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
-#pragma unroll ENSC_NODE_UNROLL_FP64
+#pragma unroll kNodeUnrollFp64
             for (int k = 0; k < 8; ++k) {
                 const uint32_t nk = __ldg(conn + k * ep + e);
                 const double uu[3] = {U[nk], U[np + nk], U[2 * np + nk]};
@@ -233,7 +233,7 @@ __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_FP64) k_element(E
             double L0[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
             double VT[3][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
             double nx2 = 0.0;
-#pragma unroll ENSC_NODE_UNROLL_FP64
+#pragma unroll kNodeUnrollFp64
             for (int j = 0; j < 8; ++j) {
                 const uint32_t nj = __ldg(conn + j * ep + e);
                 const double* bk = bte + 3 * j * ep;
@@ -358,32 +358,36 @@ __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_FP64) k_element(E
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
                     Z[c][i] = Vc * __fma_rn(Fi[c][2], Sp[2][i], __fma_rn(Fi[c][1], Sp[1][i], Fi[c][0] * Sp[0][i])) - W[i][c];
-            // hourglass power sum_j h_j . v_j = Gq : VT - W : L0
+            // hourglass power sum_j h_j . v_j = Gq : HIA
             {
-                double hp = 0.0, wl = 0.0;
+                double hp = 0.0;
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
 #pragma unroll
-                    for (int kk = 0; kk < 4; ++kk) hp = __fma_rn(Gq[i][kk], VT[i][kk], hp);
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) wl = __fma_rn(W[i][c], L0[i][c], wl);
-                e_hg += (hp - wl) * dt1;
+                    for (int kk = 0; kk < 4; ++kk) hp = __fma_rn(Gq[i][kk], HIA[i][kk], hp);
+                e_hg += hp * dt1;
             }
             // nodal forces f_j = -(B0_j Z) - Gamma_j Gq^T
             // (= -b_j sigma V - h_j + p b_j V: :985-997, :1070, :1106)
-#pragma unroll ENSC_NODE_UNROLL_FP64
+#pragma unroll kNodeUnrollFp64
             for (int j = 0; j < 8; ++j) {
                 const double* bk = bte + 3 * j * ep;
                 const double b0 = __ldg(bk), b1 = __ldg(bk + ep), b2 = __ldg(bk + 2 * ep);
-                double* fej = fe + 3 * j * ep + e;
+                double* fej;
+                int64_t fst;
+                if (E.slot_major) {
+                    fej = fe + 3 * j * np + __ldg(conn + j * ep + e);
+                    fst = np;
+                } else {
+                    fej = fe + 3 * j * ep + e;
+                    fst = ep;
+                }
 #pragma unroll
                 for (int i = 0; i < 3; ++i) {
                     double tg = tau_of(0, j) > 0.0 ? Gq[i][0] : -Gq[i][0];
 #pragma unroll
                     for (int kk = 1; kk < 4; ++kk) tg = tau_of(kk, j) > 0.0 ? tg + Gq[i][kk] : tg - Gq[i][kk];
-                    fej[i * ep] = -__fma_rn(b2, Z[2][i], __fma_rn(b1, Z[1][i], b0 * Z[0][i])) - tg;
+                    fej[i * fst] = -__fma_rn(b2, Z[2][i], __fma_rn(b1, Z[1][i], b0 * Z[0][i])) - tg;
                 }
             }
             // compute_dtStable (:828-834)
@@ -440,7 +444,19 @@ __global__ void __launch_bounds__(kNodeThreads) k_node(ElemArrays E, NodeArrays 
     const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
     for (int64_t n = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; n < nn; n += stride) {
         double f[3];
-        if (N.csr_ptr == nullptr) {
+        if (E.slot_major) {
+            // the reference's ((((((a0+a1)+a2)+a3)+a4)+a5)+a6)+a7 over the
+            // slots that hold an element (an absent slot adds +0.0)
+            f[0] = f[1] = f[2] = 0.0;
+            const uint32_t msk = N.slot_mask[n];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                if ((msk >> k) & 1u) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) f[c] = f[c] + fe[(3 * k + c) * np + n];
+                }
+            }
+        } else if (N.csr_ptr == nullptr) {
             f[0] = f[1] = f[2] = 0.0;
 #pragma unroll
             for (int k = 0; k < 8; ++k) {

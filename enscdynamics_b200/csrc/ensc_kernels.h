@@ -26,6 +26,8 @@ constexpr int kElemThreads = 128;
 #ifndef ENSC_NODE_UNROLL_MIXED
 #define ENSC_NODE_UNROLL_MIXED 4
 #endif
+constexpr int kNodeUnrollFp64 = ENSC_NODE_UNROLL_FP64;
+constexpr int kNodeUnrollMixed = ENSC_NODE_UNROLL_MIXED;
 // L2 bulk prefetch of the next grid-stride tile in the element passes.
 #ifndef ENSC_PREFETCH
 #define ENSC_PREFETCH 0

@@ -111,7 +111,6 @@ __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_MIXED)
     float* __restrict__ epsp = static_cast<float*>(E.eps_p);
     float* __restrict__ fe = static_cast<float*>(E.fe);
     const double* __restrict__ X = N.x;
-    const double* __restrict__ U = N.u;
     const float* __restrict__ V = static_cast<const float*>(N.v);
     const float G = static_cast<float>(M.G), lam = static_cast<float>(M.lambda);
     const float rho = static_cast<float>(M.rho), wos = static_cast<float>(M.wos);
@@ -143,9 +142,12 @@ __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_MIXED)
         const float* __restrict__ bte = bt + e;
         const uint32_t n0 = __ldg(conn + e);
         const double x00 = X[n0], x01 = X[np + n0], x02 = X[2 * np + n0];
-        // hourglass projections (TAU x = TAU (x - x0): the Gamma rows sum to
-        // zero) and minimum edge from coordinates relative to node 0
-        float TX[4][3];
+        // coordinates relative to node 0 (differences formed in FP64):
+        // hourglass projections TAU x = TAU (x - x0) (the Gamma rows sum to
+        // zero), the minimum edge, and F = sum_j (x_j - x_0) B0_j, which equals
+        // I + u_e B0^T because sum_j X0_j B0_j = I and sum_j B0_j = 0
+        float TX[4][3] = {};
+        float F[3][3] = {};
         float len;
         {
             float xr[8][3];
@@ -158,14 +160,17 @@ __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_MIXED)
                 xr[k][2] = static_cast<float>(X[2 * np + nk] - x02);
             }
 #pragma unroll
-            for (int kk = 0; kk < 4; ++kk)
+            for (int k = 1; k < 8; ++k) {
+                const float* bk = bte + 3 * k * ep;
+                const float bb[3] = {__ldg(bk), __ldg(bk + ep), __ldg(bk + 2 * ep)};
 #pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    float t = 0.f;
+                for (int r = 0; r < 3; ++r) {
 #pragma unroll
-                    for (int j = 1; j < 8; ++j) t += tau_f(kk, j) * xr[j][c];
-                    TX[kk][c] = t;
+                    for (int c = 0; c < 3; ++c) F[r][c] = fmaf(xr[k][r], bb[c], F[r][c]);
+#pragma unroll
+                    for (int kk = 0; kk < 4; ++kk) TX[kk][r] += tau_f(kk, k) * xr[k][r];
                 }
+            }
             constexpr int A0[12] = {0, 1, 2, 3, 4, 5, 6, 7, 0, 1, 2, 3};
             constexpr int A1[12] = {1, 2, 3, 0, 5, 6, 7, 4, 4, 5, 6, 7};
             float m = FLT_MAX;
@@ -178,20 +183,6 @@ __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_MIXED)
             }
             len = sqrtf(m);
         }
-        // F = I + u_e B0^T (B0^T rows are re-read per pass; they stay in L1)
-        float F[3][3] = {{1.f, 0.f, 0.f}, {0.f, 1.f, 0.f}, {0.f, 0.f, 1.f}};
-#pragma unroll ENSC_NODE_UNROLL_MIXED
-        for (int k = 0; k < 8; ++k) {
-            const uint32_t nk = __ldg(conn + k * ep + e);
-            const float uu[3] = {static_cast<float>(U[nk]), static_cast<float>(U[np + nk]),
-                                 static_cast<float>(U[2 * np + nk])};
-            const float* bk = bte + 3 * k * ep;
-            const float bb[3] = {__ldg(bk), __ldg(bk + ep), __ldg(bk + 2 * ep)};
-#pragma unroll
-            for (int r = 0; r < 3; ++r)
-#pragma unroll
-                for (int c = 0; c < 3; ++c) F[r][c] = fmaf(uu[r], bb[c], F[r][c]);
-        }
         const float J = det3f(F);
         if (!(J > 0.f)) bad |= ST_INVERTED;
         const float invdet = 1.f / J;
@@ -202,7 +193,7 @@ __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_MIXED)
             for (int j = 0; j < 3; ++j) Fi[i][j] = cof3f(F, j, i) * invdet;
         // L0 = v_e B0^T, VT = v_e Gamma^T, NX2
         float L0[3][3] = {}, VT[3][4] = {}, nx2 = 0.f;
-#pragma unroll ENSC_NODE_UNROLL_MIXED
+#pragma unroll kNodeUnrollMixed
         for (int j = 0; j < 8; ++j) {
             const uint32_t nj = __ldg(conn + j * ep + e);
             const float vj[3] = {V[nj], V[np + nj], V[2 * np + nj]};
@@ -309,28 +300,34 @@ __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_MIXED)
             for (int i = 0; i < 3; ++i)
                 Z[c][i] = Vc * fmaf(Fi[c][2], Sp[2][i], fmaf(Fi[c][1], Sp[1][i], Fi[c][0] * Sp[0][i])) - W[i][c];
         {
+            // hourglass power sum_j h_j . v_j = Gq : HIA
             float hp = 0.f;
 #pragma unroll
-            for (int i = 0; i < 3; ++i) {
+            for (int i = 0; i < 3; ++i)
 #pragma unroll
-                for (int kk = 0; kk < 4; ++kk) hp = fmaf(Gq[i][kk], VT[i][kk], hp);
-#pragma unroll
-                for (int c = 0; c < 3; ++c) hp = fmaf(-W[i][c], L0[i][c], hp);
-            }
+                for (int kk = 0; kk < 4; ++kk) hp = fmaf(Gq[i][kk], HIA[i][kk], hp);
             e_hg += static_cast<double>(hp) * dt1d;
         }
         // nodal forces f_j = -(B0_j Z) - Gamma_j Gq^T
-#pragma unroll ENSC_NODE_UNROLL_MIXED
+#pragma unroll kNodeUnrollMixed
         for (int j = 0; j < 8; ++j) {
             const float* bk = bte + 3 * j * ep;
             const float b0 = __ldg(bk), b1 = __ldg(bk + ep), b2 = __ldg(bk + 2 * ep);
-            float* fej = fe + 3 * j * ep + e;
+            float* fej;
+            int64_t fst;
+            if (E.slot_major) {
+                fej = fe + 3 * j * np + __ldg(conn + j * ep + e);
+                fst = np;
+            } else {
+                fej = fe + 3 * j * ep + e;
+                fst = ep;
+            }
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
                 float tg = 0.f;
 #pragma unroll
                 for (int kk = 0; kk < 4; ++kk) tg += tau_f(kk, j) * Gq[i][kk];
-                fej[i * ep] = -fmaf(b2, Z[2][i], fmaf(b1, Z[1][i], b0 * Z[0][i])) - tg;
+                fej[i * fst] = -fmaf(b2, Z[2][i], fmaf(b1, Z[1][i], b0 * Z[0][i])) - tg;
             }
         }
         // element dt (compute_dtStable, exDyna3D.cpp:828-834)
@@ -379,7 +376,16 @@ __global__ void __launch_bounds__(kNodeThreads) k_node_mixed(ElemArrays E, NodeA
     const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
     for (int64_t n = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; n < nn; n += stride) {
         float f[3] = {0.f, 0.f, 0.f};
-        if (N.csr_ptr == nullptr) {
+        if (E.slot_major) {
+            const uint32_t msk = N.slot_mask[n];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                if ((msk >> k) & 1u) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) f[c] += fe[(3 * k + c) * np + n];
+                }
+            }
+        } else if (N.csr_ptr == nullptr) {
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
                 const uint32_t el = __ldg(N.ell + k * np + n);

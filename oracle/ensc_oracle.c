@@ -310,15 +310,12 @@ static double element(const ensc_oracle_params* p, ensc_oracle_state* s, int64_t
             f[j][i] = -fma(b2, Z[2][i], fma(b1, Z[1][i], b0 * Z[0][i])) - tg;
         }
     }
-    /* hourglass power sum_j h_j . v_j = Gq : VT - W : L0 */
+    /* hourglass power sum_j h_j . v_j = Gq : HIA */
     {
         double hp = 0.0;
         for (int i = 0; i < 3; ++i)
-            for (int k = 0; k < 4; ++k) hp = fma(Gq[i][k], VT[i][k], hp);
-        double wl = 0.0;
-        for (int i = 0; i < 3; ++i)
-            for (int c = 0; c < 3; ++c) wl = fma(W[i][c], L0[i][c], wl);
-        de[1] = (hp - wl) * dt1;
+            for (int k = 0; k < 4; ++k) hp = fma(Gq[i][k], HIA[i][k], hp);
+        de[1] = hp * dt1;
     }
     /* compute_dtStable (:828-834) with this cycle's min edge */
     {
