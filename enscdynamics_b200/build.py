@@ -32,9 +32,11 @@ UNITS = [
     ("ensc_control.cu", ["-fmad=false"]),
     ("ensc_mixed.cu", []),
     ("ensc_noalloc.cu", []),
+    ("ensc_instance.cu", []),
+    ("ensc_batch.cu", []),
     ("ensc_capi.cu", []),
 ]
-HEADERS = ["ensc_device.cuh", "ensc_kernels.h"]
+HEADERS = ["ensc_device.cuh", "ensc_kernels.h", "ensc_instance.h"]
 
 
 def nvcc() -> str:

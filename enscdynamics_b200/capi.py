@@ -95,6 +95,22 @@ SIGNATURES = [
     ("ensc_step_noalloc", C.c_int, [C.POINTER(DeviceModel), C.POINTER(MaterialDesc), C.POINTER(Params),
                                     C.POINTER(NoallocClock), C.c_int64, C.c_double]),
     ("ensc_last_error", C.c_char_p, [C.c_void_p]),
+    ("ensc_batch_create", C.c_int, [C.POINTER(Params), C.c_int32, C.c_int64, C.c_int64, C.c_int64,
+                                    C.POINTER(C.c_void_p)]),
+    ("ensc_batch_add", C.c_int, [C.c_void_p, C.POINTER(MeshDesc), C.POINTER(MaterialDesc), C.POINTER(Params),
+                                 C.POINTER(C.c_int32)]),
+    ("ensc_batch_set_bcs", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int8), _P]),
+    ("ensc_batch_arm", C.c_int, [C.c_void_p, C.c_int32, C.c_int64, C.c_double]),
+    ("ensc_batch_run", C.c_int, [C.c_void_p, C.c_int64]),
+    ("ensc_batch_sync", C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
+    ("ensc_batch_report", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(StepReport)]),
+    ("ensc_batch_energy", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(EnergyReport)]),
+    ("ensc_batch_download", C.c_int, [C.c_void_p, C.c_int32, _P, _P, _P, _P, _P, _P]),
+    ("ensc_batch_remove", C.c_int, [C.c_void_p, C.c_int32]),
+    ("ensc_batch_device_bytes", C.c_int64, [C.c_void_p]),
+    ("ensc_batch_instances", C.c_int32, [C.c_void_p]),
+    ("ensc_batch_destroy", None, [C.c_void_p]),
+    ("ensc_batch_last_error", C.c_char_p, [C.c_void_p]),
 ]
 
 _lib = None
@@ -125,6 +141,34 @@ def _dp(a: Optional[np.ndarray]):
     return None if a is None else a.ctypes.data_as(_P)
 
 
+def _descriptors(x0, conn, v0, material, controls, bt=None, vol0=None, inv_mass=None):
+    """Mesh, material and control descriptors (plus the arrays they point into)."""
+    keep = []
+
+    def arr(a, dt):
+        if a is None:
+            return None
+        b = np.ascontiguousarray(a, dtype=dt)
+        keep.append(b)
+        return b
+
+    conn_a = arr(conn, np.uint32)
+    x0_a = arr(x0, np.float64)
+    v0_a = arr(v0, np.float64)
+    m = MeshDesc(int(x0.shape[0]), int(conn.shape[0]), conn_a.ctypes.data_as(C.POINTER(C.c_uint32)), _dp(x0_a),
+                 _dp(v0_a), _dp(arr(bt, np.float64)), _dp(arr(vol0, np.float64)), _dp(arr(inv_mass, np.float64)))
+    mt = MaterialDesc(material.E, material.nu, material.rho, material.yield_stress, material.hardening)
+    p = Params()
+    p.c_dr, p.c_cr, p.factor_timestep = controls.c_dr, controls.c_cr, controls.factor
+    p.cvisl, p.cvisq, p.total_time = controls.cvisl, controls.cvisq, controls.total_time
+    if controls.gravity is not None:
+        p.gravity_on = 1
+        p.gravity_value = controls.gravity[0]
+        for i in range(3):
+            p.gravity_dir[i] = controls.gravity[1][i]
+    return keep, m, mt, p
+
+
 class Stepper:
     """One GPU solver instance behind the C ABI."""
 
@@ -138,29 +182,7 @@ class Stepper:
         self.h = C.c_void_p()
         self.n_nodes = int(x0.shape[0])
         self.n_elements = int(conn.shape[0])
-        keep = []
-
-        def arr(a, dt):
-            if a is None:
-                return None
-            b = np.ascontiguousarray(a, dtype=dt)
-            keep.append(b)
-            return b
-
-        conn_a = arr(conn, np.uint32)
-        x0_a = arr(x0, np.float64)
-        v0_a = arr(v0, np.float64)
-        m = MeshDesc(self.n_nodes, self.n_elements, conn_a.ctypes.data_as(C.POINTER(C.c_uint32)), _dp(x0_a),
-                     _dp(v0_a), _dp(arr(bt, np.float64)), _dp(arr(vol0, np.float64)), _dp(arr(inv_mass, np.float64)))
-        mt = MaterialDesc(material.E, material.nu, material.rho, material.yield_stress, material.hardening)
-        p = Params()
-        p.c_dr, p.c_cr, p.factor_timestep = controls.c_dr, controls.c_cr, controls.factor
-        p.cvisl, p.cvisq, p.total_time = controls.cvisl, controls.cvisq, controls.total_time
-        if controls.gravity is not None:
-            p.gravity_on = 1
-            p.gravity_value = controls.gravity[0]
-            for i in range(3):
-                p.gravity_dir[i] = controls.gravity[1][i]
+        self._keep, m, mt, p = _descriptors(x0, conn, v0, material, controls, bt, vol0, inv_mass)
         p.precision = precision
         p.device = device
         p.stream = stream
@@ -259,3 +281,107 @@ class Stepper:
     @property
     def kernels_per_cycle(self) -> int:
         return int(self._lib.ensc_kernels_per_cycle(self.h))
+
+
+class Batch:
+    """Many independent solver instances stepped together (ensc_batch_* ABI).
+
+    Each instance is what a Stepper over the same arguments would be; the
+    batch runs one launch per cycle phase for all of them."""
+
+    def __init__(self, *, max_instances: int, max_elements: int, max_nodes: int, budget_bytes: int,
+                 precision: int = MIXED, device: int = 0, stream: Optional[int] = None, graph_chunk: int = 0):
+        lib = load()
+        self._lib = lib
+        self.h = C.c_void_p()
+        p = Params()
+        p.precision = precision
+        p.device = device
+        p.stream = stream
+        p.graph_chunk = graph_chunk
+        p.factor_timestep = 1.0
+        rc = lib.ensc_batch_create(C.byref(p), int(max_instances), int(max_elements), int(max_nodes),
+                                   int(budget_bytes), C.byref(self.h))
+        if rc != 0:
+            raise EnscError(rc, lib.ensc_last_error(None).decode())
+        self.precision = precision
+        self.sizes: Dict[int, tuple] = {}
+
+    def _check(self, rc: int) -> None:
+        if rc != 0:
+            raise EnscError(rc, self._lib.ensc_batch_last_error(self.h).decode())
+
+    def close(self) -> None:
+        if self.h:
+            self._lib.ensc_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def add(self, x0: np.ndarray, conn: np.ndarray, v0: Optional[np.ndarray] = None, *,
+            material: _mesh.Material, controls: _mesh.Controls, bt: Optional[np.ndarray] = None,
+            vol0: Optional[np.ndarray] = None, inv_mass: Optional[np.ndarray] = None) -> int:
+        keep, m, mt, p = _descriptors(x0, conn, v0, material, controls, bt, vol0, inv_mass)
+        slot = C.c_int32(-1)
+        self._check(self._lib.ensc_batch_add(self.h, C.byref(m), C.byref(mt), C.byref(p), C.byref(slot)))
+        del keep
+        self.sizes[slot.value] = (int(x0.shape[0]), int(conn.shape[0]))
+        return slot.value
+
+    def set_bcs(self, slot: int, code: Optional[np.ndarray], value: Optional[np.ndarray] = None) -> None:
+        c = None if code is None else np.ascontiguousarray(code, dtype=np.int8)
+        v = None if value is None else np.ascontiguousarray(value, dtype=np.float64)
+        self._check(self._lib.ensc_batch_set_bcs(
+            self.h, int(slot), None if c is None else c.ctypes.data_as(C.POINTER(C.c_int8)), _dp(v)))
+
+    def arm(self, slot: int, max_cycles: int, step_end: float = math.inf) -> None:
+        self._check(self._lib.ensc_batch_arm(self.h, int(slot), int(max_cycles), float(step_end)))
+
+    def run(self, cycles: int) -> None:
+        self._check(self._lib.ensc_batch_run(self.h, int(cycles)))
+
+    def sync(self) -> int:
+        n = C.c_int32(0)
+        self._check(self._lib.ensc_batch_sync(self.h, C.byref(n)))
+        return n.value
+
+    def report(self, slot: int) -> Dict[str, float]:
+        r = StepReport()
+        self._check(self._lib.ensc_batch_report(self.h, int(slot), C.byref(r)))
+        return {k: getattr(r, k) for k, _ in StepReport._fields_}
+
+    def energy(self, slot: int) -> Dict[str, float]:
+        r = EnergyReport()
+        self._check(self._lib.ensc_batch_energy(self.h, int(slot), C.byref(r)))
+        return {k: getattr(r, k) for k, _ in EnergyReport._fields_}
+
+    def download(self, slot: int, fields=("x", "u", "v", "sigma", "qia", "eps_p")) -> Dict[str, np.ndarray]:
+        nn, ne = self.sizes[slot]
+        shapes = {"x": (nn, 3), "u": (nn, 3), "v": (nn, 3), "sigma": (ne, 6), "qia": (ne, 12), "eps_p": (ne,)}
+        out = {k: np.empty(shapes[k]) for k in fields}
+        g = lambda k: _dp(out.get(k))  # noqa: E731
+        self._check(self._lib.ensc_batch_download(self.h, int(slot), g("x"), g("u"), g("v"), g("sigma"), g("qia"),
+                                                  g("eps_p")))
+        return out
+
+    def remove(self, slot: int) -> None:
+        self._check(self._lib.ensc_batch_remove(self.h, int(slot)))
+        self.sizes.pop(slot, None)
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self._lib.ensc_batch_device_bytes(self.h))
+
+    @property
+    def instances(self) -> int:
+        return int(self._lib.ensc_batch_instances(self.h))

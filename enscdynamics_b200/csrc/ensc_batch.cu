@@ -1,0 +1,592 @@
+// Batched stepping of many independent solver instances (ensc_batch_* in
+// include/ensc_gpu.h).
+//
+// Instances are sub-allocated from a CUDA memory pool owned by the batch (the
+// arena, bounded by a byte budget); each keeps the single-instance layout of
+// ensc_instance.h in its block.  A device table of instance descriptors and
+// two tile lists (32-element and 32-node tiles, each inside one instance)
+// drive one persistent launch per phase for all instances, each with its own
+// clock, dt and material.  The cycle is captured once as a CUDA graph; adding
+// or removing instances rewrites the tables in place, so the graph stays
+// valid.  Instances advance until their own cycle budget or end time, then
+// idle (their tiles return at once) until the host retires them.
+#include "ensc_gpu.h"
+#include "ensc_device.cuh"
+#include "ensc_instance.h"
+#include "ensc_kernels.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using ensc::Ctl;
+
+namespace {
+
+struct Slot {
+    bool used = false;
+    void* block = nullptr;
+    size_t bytes = 0;
+    int64_t nn = 0, ne = 0, nn_pad = 0, ne_pad = 0;
+    bool plastic = false;
+    ensc::ElemArrays E{};
+    ensc::NodeArrays N{};
+    ensc::Material M{};
+    bool kinetic0_done = false;
+};
+
+struct Tune {
+    int mult_e = 1, mult_n = 1, chunk = 32;
+};
+
+}  // namespace
+
+struct ensc_batch {
+    int device = 0;
+    int precision = ENSC_MIXED;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    cudaStream_t cap_stream = nullptr;
+    cudaMemPool_t pool = nullptr;
+    int64_t budget = 0, used = 0;
+    int slots = 0;
+    int64_t max_etiles = 0, max_ntiles = 0;
+    // device tables (one allocation)
+    void* tables = nullptr;
+    ensc::InstanceDesc* d_desc = nullptr;
+    int32_t *d_etile_inst = nullptr, *d_etile_base = nullptr, *d_ntile_inst = nullptr, *d_ntile_base = nullptr;
+    int32_t* d_counts = nullptr;
+    double *d_etile_part = nullptr, *d_ntile_part = nullptr;
+    Ctl* d_ctl = nullptr;
+    double* d_scratch = nullptr;  // partials for init / kinetic passes of one instance
+    int scratch_blocks = 4096;
+    Ctl* h_ctl = nullptr;         // pinned mirror of d_ctl
+    std::vector<Slot> inst;
+    ensc::BatchTables T{};
+    bool dirty = true;
+    int64_t n_etiles = 0, n_ntiles = 0;
+    int sms = 148, occ_e = 1, occ_n = 1, occ_pre = 4;
+    Tune tune;
+    int fixed_chunk = 0;  // cycles per graph launch given by the caller (0: tuned)
+    bool tuned = false;
+    cudaGraphExec_t graph = nullptr;
+    int graph_chunk = 0, graph_ge = 0, graph_gn = 0;
+    std::string err;
+};
+
+namespace {
+
+int berr(ensc_batch* b, int code, const std::string& m) {
+    if (b) b->err = m;
+    ensc::set_thread_error(m);
+    return code;
+}
+
+int bcuda(ensc_batch* b, const char* what, cudaError_t e) {
+    return berr(b, e == cudaErrorMemoryAllocation ? ENSC_ERR_OOM : ENSC_ERR_CUDA,
+                std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
+}
+
+#define BCK(b, call)                                      \
+    do {                                                  \
+        cudaError_t _e = (call);                          \
+        if (_e != cudaSuccess) return bcuda((b), #call, _e); \
+    } while (0)
+
+struct DevGuard {
+    int prev = -1;
+    explicit DevGuard(int d) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != d) cudaSetDevice(d);
+    }
+    ~DevGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+bool is_mixed(const ensc_batch* b) { return b->precision == ENSC_MIXED; }
+
+// Rewrites the instance table and tile lists from the live slots.
+int rebuild_tables(ensc_batch* b) {
+    std::vector<ensc::InstanceDesc> desc(static_cast<size_t>(b->slots));
+    std::vector<int32_t> ei, eb, ni, nb;
+    int used_slots = 0;
+    for (int s = 0; s < b->slots; ++s) {
+        const Slot& sl = b->inst[s];
+        ensc::InstanceDesc& d = desc[s];
+        d = ensc::InstanceDesc{};
+        d.ctl = b->d_ctl + s;
+        if (!sl.used) continue;
+        used_slots = s + 1;
+        d.E = sl.E;
+        d.N = sl.N;
+        d.M = sl.M;
+        d.active = 1;
+        d.e_tile0 = static_cast<int32_t>(ei.size());
+        for (int64_t e = 0; e < sl.ne; e += ensc::kTile) {
+            ei.push_back(s);
+            eb.push_back(static_cast<int32_t>(e));
+        }
+        d.e_ntiles = static_cast<int32_t>(ei.size()) - d.e_tile0;
+        d.n_tile0 = static_cast<int32_t>(ni.size());
+        for (int64_t n = 0; n < sl.nn; n += ensc::kTile) {
+            ni.push_back(s);
+            nb.push_back(static_cast<int32_t>(n));
+        }
+        d.n_ntiles = static_cast<int32_t>(ni.size()) - d.n_tile0;
+    }
+    if (static_cast<int64_t>(ei.size()) > b->max_etiles || static_cast<int64_t>(ni.size()) > b->max_ntiles)
+        return berr(b, ENSC_ERR_OOM, "batch tile capacity exceeded");
+    const int32_t counts[3] = {static_cast<int32_t>(ei.size()), static_cast<int32_t>(ni.size()), used_slots};
+    BCK(b, cudaMemcpyAsync(b->d_desc, desc.data(), desc.size() * sizeof(ensc::InstanceDesc), cudaMemcpyHostToDevice,
+                           b->stream));
+    if (!ei.empty()) {
+        BCK(b, cudaMemcpyAsync(b->d_etile_inst, ei.data(), ei.size() * 4, cudaMemcpyHostToDevice, b->stream));
+        BCK(b, cudaMemcpyAsync(b->d_etile_base, eb.data(), eb.size() * 4, cudaMemcpyHostToDevice, b->stream));
+    }
+    if (!ni.empty()) {
+        BCK(b, cudaMemcpyAsync(b->d_ntile_inst, ni.data(), ni.size() * 4, cudaMemcpyHostToDevice, b->stream));
+        BCK(b, cudaMemcpyAsync(b->d_ntile_base, nb.data(), nb.size() * 4, cudaMemcpyHostToDevice, b->stream));
+    }
+    BCK(b, cudaMemcpyAsync(b->d_counts, counts, sizeof(counts), cudaMemcpyHostToDevice, b->stream));
+    BCK(b, cudaStreamSynchronize(b->stream));
+    b->n_etiles = static_cast<int64_t>(ei.size());
+    b->n_ntiles = static_cast<int64_t>(ni.size());
+    b->dirty = false;
+    return ENSC_OK;
+}
+
+void launch_cycle(ensc_batch* b, int ge, int gn, cudaStream_t st) {
+    ensc::launch_between_batch(b->T, b->slots, 0, st);
+    ensc::launch_edge_prepass_batch(b->T, b->sms * b->occ_pre, st);
+    ensc::launch_begin_exact_batch(b->T, b->slots, st);
+    if (is_mixed(b)) {
+        ensc::launch_element_batch_mixed(b->T, ge, st);
+        ensc::launch_node_batch_mixed(b->T, gn, st);
+    } else {
+        ensc::launch_element_batch_fp64(b->T, ge, st);
+        ensc::launch_node_batch_fp64(b->T, gn, st);
+    }
+}
+
+int build_graph(ensc_batch* b, const Tune& t) {
+    const int ge = b->sms * b->occ_e * t.mult_e, gn = b->sms * b->occ_n * t.mult_n;
+    if (b->graph && b->graph_chunk == t.chunk && b->graph_ge == ge && b->graph_gn == gn) return ENSC_OK;
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    BCK(b, cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal));
+    for (int c = 0; c < t.chunk; ++c) launch_cycle(b, ge, gn, b->cap_stream);
+    cudaError_t e = cudaStreamEndCapture(b->cap_stream, &g);
+    if (e != cudaSuccess) return bcuda(b, "cudaStreamEndCapture", e);
+    e = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return bcuda(b, "cudaGraphInstantiate", e);
+    b->graph_chunk = t.chunk;
+    b->graph_ge = ge;
+    b->graph_gn = gn;
+    return ENSC_OK;
+}
+
+// Picks the launch geometry and graph length with the shortest time per
+// cycle on the batch as loaded.  The candidates differ only in how work is
+// spread over the GPU, not in arithmetic, so the cycles they run are ordinary
+// cycles of the solve (results are identical whichever wins).
+int autotune(ensc_batch* b, int64_t* cycles_left) {
+    const Tune cand[] = {{1, 1, 32}, {2, 1, 32}, {1, 2, 32}, {2, 2, 32}, {1, 1, 8}};
+    cudaEvent_t e0, e1;
+    BCK(b, cudaEventCreate(&e0));
+    BCK(b, cudaEventCreate(&e1));
+    float best = 1e30f;
+    Tune bt = b->tune;
+    for (Tune t : cand) {
+        if (b->fixed_chunk > 0) t.chunk = b->fixed_chunk;
+        if (*cycles_left < 3 * t.chunk) break;
+        int rc = build_graph(b, t);
+        if (rc) return rc;
+        BCK(b, cudaGraphLaunch(b->graph, b->stream));  // warm-up
+        BCK(b, cudaEventRecord(e0, b->stream));
+        BCK(b, cudaGraphLaunch(b->graph, b->stream));
+        BCK(b, cudaGraphLaunch(b->graph, b->stream));
+        BCK(b, cudaEventRecord(e1, b->stream));
+        BCK(b, cudaEventSynchronize(e1));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        const float per = ms / (2.f * t.chunk);
+        if (per < best) {
+            best = per;
+            bt = t;
+        }
+        *cycles_left -= 3 * t.chunk;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    b->tune = bt;
+    b->tuned = true;
+    return build_graph(b, bt);
+}
+
+}  // namespace
+
+extern "C" {
+
+int ensc_batch_create(const ensc_params* params, int32_t max_instances, int64_t max_elements, int64_t max_nodes,
+                      int64_t budget_bytes, ensc_batch** out) {
+    if (!out || !params) return berr(nullptr, ENSC_ERR_ARG, "params and out are required");
+    *out = nullptr;
+    if (max_instances <= 0 || max_elements <= 0 || max_nodes <= 0 || budget_bytes <= 0)
+        return berr(nullptr, ENSC_ERR_ARG, "batch capacities and budget must be positive");
+    if (params->precision != ENSC_FP64 && params->precision != ENSC_MIXED)
+        return berr(nullptr, ENSC_ERR_ARG, "unsupported precision");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || params->device < 0 || params->device >= ndev)
+        return berr(nullptr, ENSC_ERR_NODEVICE, "no usable CUDA device");
+    ensc_batch* b = new ensc_batch();
+    b->device = params->device;
+    b->precision = params->precision;
+    b->budget = budget_bytes;
+    b->slots = max_instances;
+    // tiles: every instance rounds its element and node counts up to tiles
+    b->max_etiles = max_elements / ensc::kTile + max_instances + 1;
+    b->max_ntiles = max_nodes / ensc::kTile + max_instances + 1;
+    b->inst.resize(static_cast<size_t>(max_instances));
+    if (params->graph_chunk > 0) {
+        b->fixed_chunk = static_cast<int>(std::min<int64_t>(params->graph_chunk, 1024));
+        b->tune.chunk = b->fixed_chunk;
+    }
+    DevGuard dg(b->device);
+    auto fail = [&](int code) {
+        ensc_batch_destroy(b);
+        return code;
+    };
+    cudaDeviceProp prop{};
+    if (cudaGetDeviceProperties(&prop, b->device) != cudaSuccess) return fail(berr(b, ENSC_ERR_CUDA, "device query"));
+    b->sms = prop.multiProcessorCount;
+    b->occ_e = std::max(1, is_mixed(b) ? ensc::occupancy_element_batch_mixed() : ensc::occupancy_element_batch_fp64());
+    b->occ_n = std::max(1, is_mixed(b) ? ensc::occupancy_node_batch_mixed() : ensc::occupancy_node_batch_fp64());
+    // arena: a memory pool that keeps released blocks for reuse
+    cudaMemPoolProps pp{};
+    pp.allocType = cudaMemAllocationTypePinned;
+    pp.location.type = cudaMemLocationTypeDevice;
+    pp.location.id = b->device;
+    cudaError_t e = cudaMemPoolCreate(&b->pool, &pp);
+    if (e != cudaSuccess) return fail(bcuda(b, "cudaMemPoolCreate", e));
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(b->pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    if (params->stream) {
+        b->stream = static_cast<cudaStream_t>(params->stream);
+    } else {
+        e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return fail(bcuda(b, "cudaStreamCreate", e));
+        b->own_stream = true;
+    }
+    e = cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return fail(bcuda(b, "cudaStreamCreate", e));
+    // tables
+    auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+    const size_t s_desc = al(sizeof(ensc::InstanceDesc) * b->slots), s_et = al(4 * b->max_etiles),
+                 s_nt = al(4 * b->max_ntiles), s_cnt = 256, s_ep = al(8 * 3 * b->max_etiles),
+                 s_np = al(8 * 2 * b->max_ntiles), s_ctl = al(sizeof(Ctl) * b->slots),
+                 s_scr = al(8 * 3 * static_cast<size_t>(b->scratch_blocks));
+    const size_t total = s_desc + 2 * s_et + 2 * s_nt + s_cnt + s_ep + s_np + s_ctl + s_scr;
+    e = cudaMalloc(&b->tables, total);
+    if (e != cudaSuccess) return fail(bcuda(b, "cudaMalloc(batch tables)", e));
+    cudaMemset(b->tables, 0, total);
+    char* p = static_cast<char*>(b->tables);
+    b->d_desc = reinterpret_cast<ensc::InstanceDesc*>(p);
+    p += s_desc;
+    b->d_etile_inst = reinterpret_cast<int32_t*>(p);
+    p += s_et;
+    b->d_etile_base = reinterpret_cast<int32_t*>(p);
+    p += s_et;
+    b->d_ntile_inst = reinterpret_cast<int32_t*>(p);
+    p += s_nt;
+    b->d_ntile_base = reinterpret_cast<int32_t*>(p);
+    p += s_nt;
+    b->d_counts = reinterpret_cast<int32_t*>(p);
+    p += s_cnt;
+    b->d_etile_part = reinterpret_cast<double*>(p);
+    p += s_ep;
+    b->d_ntile_part = reinterpret_cast<double*>(p);
+    p += s_np;
+    b->d_ctl = reinterpret_cast<Ctl*>(p);
+    p += s_ctl;
+    b->d_scratch = reinterpret_cast<double*>(p);
+    e = cudaMallocHost(reinterpret_cast<void**>(&b->h_ctl), sizeof(Ctl) * b->slots);
+    if (e != cudaSuccess) return fail(bcuda(b, "cudaMallocHost(ctl)", e));
+    std::memset(b->h_ctl, 0, sizeof(Ctl) * b->slots);
+    for (int s = 0; s < b->slots; ++s) b->h_ctl[s].done = 1;
+    e = cudaMemcpy(b->d_ctl, b->h_ctl, sizeof(Ctl) * b->slots, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return fail(bcuda(b, "ctl init", e));
+    b->T.desc = b->d_desc;
+    b->T.etile_inst = b->d_etile_inst;
+    b->T.etile_base = b->d_etile_base;
+    b->T.ntile_inst = b->d_ntile_inst;
+    b->T.ntile_base = b->d_ntile_base;
+    b->T.counts = b->d_counts;
+    b->T.etile_part = b->d_etile_part;
+    b->T.ntile_part = b->d_ntile_part;
+    int rc = rebuild_tables(b);
+    if (rc) return fail(rc);
+    *out = b;
+    return ENSC_OK;
+}
+
+int ensc_batch_add(ensc_batch* b, const ensc_mesh_desc* mesh, const ensc_material* mat, const ensc_params* controls,
+                   int32_t* slot_out) {
+    if (!b || !mesh || !mat || !controls || !slot_out) return berr(b, ENSC_ERR_ARG, "missing argument");
+    if (!(controls->factor_timestep > 0.0)) return berr(b, ENSC_ERR_ARG, "factor_timestep must be > 0");
+    DevGuard dg(b->device);
+    int s = -1;
+    for (int i = 0; i < b->slots; ++i)
+        if (!b->inst[i].used) {
+            s = i;
+            break;
+        }
+    if (s < 0) return berr(b, ENSC_ERR_OOM, "no free instance slot");
+    ensc::InstanceHost ih;
+    std::string perr;
+    int rc = ensc::instance_prepare(mesh, mat, is_mixed(b), ih, perr);
+    if (rc) return berr(b, rc, perr);
+    if (b->used + static_cast<int64_t>(ih.bytes) > b->budget)
+        return berr(b, ENSC_ERR_OOM, "instance does not fit the batch's memory budget");
+    const int64_t et = (ih.ne + ensc::kTile - 1) / ensc::kTile, nt = (ih.nn + ensc::kTile - 1) / ensc::kTile;
+    if (b->n_etiles + et > b->max_etiles || b->n_ntiles + nt > b->max_ntiles)
+        return berr(b, ENSC_ERR_OOM, "batch tile capacity exceeded");
+    Slot& sl = b->inst[s];
+    void* block = nullptr;
+    BCK(b, cudaMallocFromPoolAsync(&block, ih.bytes, b->pool, b->stream));
+    rc = ensc::instance_upload(ih, block, b->stream, sl.E, sl.N, perr);
+    if (rc) {
+        cudaFreeAsync(block, b->stream);
+        return berr(b, rc, perr);
+    }
+    sl.block = block;
+    sl.bytes = ih.bytes;
+    sl.nn = ih.nn;
+    sl.ne = ih.ne;
+    sl.nn_pad = ih.nn_pad;
+    sl.ne_pad = ih.ne_pad;
+    sl.plastic = ih.plastic;
+    sl.kinetic0_done = false;
+    ensc::material_from(mat, controls, sl.M);
+    b->h_ctl[s] = ensc::initial_ctl(controls, sl.M);
+    b->h_ctl[s].done = 1;  // idle until armed
+    BCK(b, cudaMemcpyAsync(b->d_ctl + s, b->h_ctl + s, sizeof(Ctl), cudaMemcpyHostToDevice, b->stream));
+    // init(): force pass with dt = 0 on the unconstrained velocities
+    Ctl c0 = b->h_ctl[s];
+    c0.done = 0;
+    BCK(b, cudaMemcpyAsync(b->d_ctl + s, &c0, sizeof(Ctl), cudaMemcpyHostToDevice, b->stream));
+    ensc::Partials P{};
+    P.elem = b->d_scratch;
+    P.node = b->d_scratch;
+    const int g = static_cast<int>(std::min<int64_t>((ih.ne + ensc::kElemThreads - 1) / ensc::kElemThreads,
+                                                     b->scratch_blocks));
+    P.n_elem_blocks = g;
+    if (is_mixed(b)) ensc::launch_element_mixed(sl.E, sl.N, sl.M, b->d_ctl + s, P, g, true, b->stream);
+    else ensc::launch_element_fp64(sl.E, sl.N, sl.M, b->d_ctl + s, P, g, true, b->stream);
+    BCK(b, cudaGetLastError());
+    BCK(b, cudaMemcpyAsync(b->h_ctl + s, b->d_ctl + s, sizeof(Ctl), cudaMemcpyDeviceToHost, b->stream));
+    BCK(b, cudaStreamSynchronize(b->stream));
+    b->h_ctl[s].done = 1;
+    BCK(b, cudaMemcpyAsync(b->d_ctl + s, b->h_ctl + s, sizeof(Ctl), cudaMemcpyHostToDevice, b->stream));
+    sl.used = true;
+    b->used += static_cast<int64_t>(ih.bytes);
+    rc = rebuild_tables(b);
+    if (rc) return rc;
+    *slot_out = s;
+    return ENSC_OK;
+}
+
+int ensc_batch_set_bcs(ensc_batch* b, int32_t slot, const int8_t* dof_code, const double* dof_value) {
+    if (!b || slot < 0 || slot >= b->slots || !b->inst[slot].used) return berr(b, ENSC_ERR_ARG, "bad slot");
+    DevGuard dg(b->device);
+    Slot& sl = b->inst[slot];
+    std::vector<uint8_t> bc(static_cast<size_t>(sl.nn_pad), 0);
+    std::vector<double> bcv(static_cast<size_t>(3 * sl.nn_pad), 0.0);
+    if (dof_code) {
+        for (int64_t n = 0; n < sl.nn; ++n) {
+            uint32_t packed = 0;
+            for (int c = 0; c < 3; ++c) {
+                const uint32_t cc = static_cast<uint32_t>(dof_code[3 * n + c]) & 3u;
+                packed |= cc << (2 * c);
+                if ((cc & ENSC_BC_VELOCITY) && dof_value) bcv[c * sl.nn_pad + n] = dof_value[3 * n + c];
+            }
+            bc[n] = static_cast<uint8_t>(packed);
+        }
+    }
+    BCK(b, cudaMemcpyAsync(const_cast<uint8_t*>(sl.N.bc), bc.data(), bc.size(), cudaMemcpyHostToDevice, b->stream));
+    BCK(b, cudaMemcpyAsync(const_cast<double*>(sl.N.bcv), bcv.data(), bcv.size() * 8, cudaMemcpyHostToDevice,
+                           b->stream));
+    ensc::launch_apply_bc_v(sl.N, is_mixed(b), b->stream);
+    if (!sl.kinetic0_done) {
+        ensc::Partials P{};
+        const int g = static_cast<int>(std::min<int64_t>((sl.nn + ensc::kNodeThreads - 1) / ensc::kNodeThreads,
+                                                         b->scratch_blocks));
+        P.elem = b->d_scratch;
+        P.node = b->d_scratch;
+        P.n_elem_blocks = 0;
+        P.n_node_blocks = g;
+        ensc::launch_kinetic0(sl.N, P, b->d_ctl + slot, is_mixed(b), g, b->stream);
+        sl.kinetic0_done = true;
+    }
+    BCK(b, cudaGetLastError());
+    BCK(b, cudaStreamSynchronize(b->stream));
+    return ENSC_OK;
+}
+
+int ensc_batch_arm(ensc_batch* b, int32_t slot, int64_t max_cycles, double step_end_time) {
+    if (!b || slot < 0 || slot >= b->slots || !b->inst[slot].used || max_cycles < 0)
+        return berr(b, ENSC_ERR_ARG, "bad slot or cycle count");
+    DevGuard dg(b->device);
+    ensc::launch_arm(b->d_ctl + slot, step_end_time, max_cycles, b->stream);
+    BCK(b, cudaGetLastError());
+    return ENSC_OK;
+}
+
+int ensc_batch_run(ensc_batch* b, int64_t cycles) {
+    if (!b || cycles < 0) return berr(b, ENSC_ERR_ARG, "bad cycle count");
+    if (cycles == 0) return ENSC_OK;
+    DevGuard dg(b->device);
+    if (b->dirty) {
+        int rc = rebuild_tables(b);
+        if (rc) return rc;
+    }
+    int64_t left = cycles;
+    if (!b->tuned) {
+        int rc = autotune(b, &left);
+        if (rc) return rc;
+    } else {
+        int rc = build_graph(b, b->tune);
+        if (rc) return rc;
+    }
+    const int64_t launches = (left + b->tune.chunk - 1) / b->tune.chunk;
+    for (int64_t i = 0; i < launches; ++i) BCK(b, cudaGraphLaunch(b->graph, b->stream));
+    return ENSC_OK;
+}
+
+int ensc_batch_sync(ensc_batch* b, int32_t* n_running) {
+    if (!b) return berr(b, ENSC_ERR_ARG, "batch is NULL");
+    DevGuard dg(b->device);
+    ensc::launch_between_batch(b->T, b->slots, 1, b->stream);  // fold the last cycle's energy
+    BCK(b, cudaGetLastError());
+    BCK(b, cudaMemcpyAsync(b->h_ctl, b->d_ctl, sizeof(Ctl) * b->slots, cudaMemcpyDeviceToHost, b->stream));
+    BCK(b, cudaStreamSynchronize(b->stream));
+    int running = 0;
+    for (int s = 0; s < b->slots; ++s)
+        if (b->inst[s].used && !b->h_ctl[s].done) ++running;
+    if (n_running) *n_running = running;
+    return ENSC_OK;
+}
+
+int ensc_batch_report(ensc_batch* b, int32_t slot, ensc_step_report* r) {
+    if (!b || !r || slot < 0 || slot >= b->slots || !b->inst[slot].used) return berr(b, ENSC_ERR_ARG, "bad slot");
+    const Ctl& c = b->h_ctl[slot];
+    r->time = c.time;
+    r->dt_i = c.dt_i;
+    r->dt_i_1 = c.dt_i_1;
+    r->cycles = c.cycles_done;
+    r->total_cycles = c.cycles_done;
+    r->status = (c.status & ensc::ST_INVERTED) ? ENSC_ERR_INVERTED : (c.status ? ENSC_ERR_NONFINITE : ENSC_OK);
+    r->done = c.done;
+    std::memcpy(&r->dt_stable_min, &c.dts_next, sizeof(double));
+    return ENSC_OK;
+}
+
+int ensc_batch_energy(ensc_batch* b, int32_t slot, ensc_energy_report* out) {
+    if (!b || !out || slot < 0 || slot >= b->slots || !b->inst[slot].used) return berr(b, ENSC_ERR_ARG, "bad slot");
+    const double* e = b->h_ctl[slot].energy;
+    out->kinetic = e[0];
+    out->internal = e[1];
+    out->hourglass = e[2];
+    out->viscous = e[3];
+    out->external = e[4];
+    out->kinetic0 = e[5];
+    return ENSC_OK;
+}
+
+int ensc_batch_download(ensc_batch* b, int32_t slot, double* x, double* u, double* v, double* sigma, double* qia,
+                        double* eps_p) {
+    if (!b || slot < 0 || slot >= b->slots || !b->inst[slot].used) return berr(b, ENSC_ERR_ARG, "bad slot");
+    DevGuard dg(b->device);
+    const Slot& sl = b->inst[slot];
+    const bool mx = is_mixed(b);
+    struct Item {
+        double* dst;
+        const void* src;
+        int64_t n, pad;
+        int comps;
+        bool f32;
+    };
+    const Item items[] = {{x, sl.N.x, sl.nn, sl.nn_pad, 3, false},       {u, sl.N.u, sl.nn, sl.nn_pad, 3, false},
+                          {v, sl.N.v, sl.nn, sl.nn_pad, 3, mx},          {sigma, sl.E.sigma, sl.ne, sl.ne_pad, 6, mx},
+                          {qia, sl.E.qia, sl.ne, sl.ne_pad, 12, mx},     {eps_p, sl.E.eps_p, sl.ne, sl.ne_pad, 1, mx}};
+    const size_t need = static_cast<size_t>(std::max<int64_t>(12 * sl.ne, 3 * sl.nn)) * sizeof(double);
+    double* stage = nullptr;
+    BCK(b, cudaMallocFromPoolAsync(reinterpret_cast<void**>(&stage), need, b->pool, b->stream));
+    int rc = ENSC_OK;
+    for (const Item& it : items) {
+        if (!it.dst) continue;
+        ensc::launch_soa_to_aos(it.src, it.n, it.pad, it.comps, it.f32, stage, b->stream);
+        cudaError_t e = cudaMemcpyAsync(it.dst, stage, it.n * it.comps * sizeof(double), cudaMemcpyDeviceToHost,
+                                        b->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+        if (e != cudaSuccess) {
+            rc = bcuda(b, "batch download", e);
+            break;
+        }
+    }
+    cudaFreeAsync(stage, b->stream);
+    cudaStreamSynchronize(b->stream);
+    return rc;
+}
+
+int ensc_batch_remove(ensc_batch* b, int32_t slot) {
+    if (!b || slot < 0 || slot >= b->slots || !b->inst[slot].used) return berr(b, ENSC_ERR_ARG, "bad slot");
+    DevGuard dg(b->device);
+    Slot& sl = b->inst[slot];
+    // the slot idles from now on; its block returns to the pool in stream order
+    b->h_ctl[slot] = Ctl{};
+    b->h_ctl[slot].done = 1;
+    BCK(b, cudaMemcpyAsync(b->d_ctl + slot, b->h_ctl + slot, sizeof(Ctl), cudaMemcpyHostToDevice, b->stream));
+    sl.used = false;
+    int rc = rebuild_tables(b);
+    BCK(b, cudaFreeAsync(sl.block, b->stream));
+    b->used -= static_cast<int64_t>(sl.bytes);
+    sl = Slot{};
+    return rc;
+}
+
+int64_t ensc_batch_device_bytes(const ensc_batch* b) { return b ? b->used : 0; }
+
+int32_t ensc_batch_instances(const ensc_batch* b) {
+    if (!b) return 0;
+    int n = 0;
+    for (const Slot& s : b->inst) n += s.used ? 1 : 0;
+    return n;
+}
+
+void ensc_batch_destroy(ensc_batch* b) {
+    if (!b) return;
+    DevGuard dg(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    for (Slot& s : b->inst)
+        if (s.block) cudaFreeAsync(s.block, b->stream);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
+    if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
+    if (b->pool) cudaMemPoolDestroy(b->pool);
+    if (b->tables) cudaFree(b->tables);
+    if (b->h_ctl) cudaFreeHost(b->h_ctl);
+    delete b;
+}
+
+const char* ensc_batch_last_error(const ensc_batch* b) { return b ? b->err.c_str() : ensc_last_error(nullptr); }
+
+}  // extern "C"

@@ -27,6 +27,56 @@ __device__ double fixed_sum(const double* a, int n) {
     return r;
 }
 
+// Same fixed order over n values spaced by `stride`.
+__device__ double fixed_sum_strided(const double* a, int n, int stride) {
+    __shared__ double red[kCtlThreads];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += kCtlThreads) s = s + a[static_cast<int64_t>(i) * stride];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = kCtlThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] = red[threadIdx.x] + red[threadIdx.x + w];
+        __syncthreads();
+    }
+    const double r = red[0];
+    __syncthreads();
+    return r;
+}
+
+// First half of update_minVertex_perMaterial_and_dt for the next cycle
+// (exDyna3D.cpp:663-686) and computeSate's clock advance (:775-780): rotate
+// dt_i_1 <- dt_i and advance time, unless the total-time clamp (:682-685)
+// could fire, which needs the cycle's minimum element edge first
+// (edge_prepass + begin_exact).  Caller has checked done / step end.
+__device__ __forceinline__ void cycle_begin(Ctl* ctl) {
+    ctl->dts_cur = bits_ord(ctl->dts_next);
+    ctl->dts_next = kInfBits;
+    ctl->len_min = kInfBits;
+    const double dt_prev = ctl->dt_i;
+    ctl->dt_prev = dt_prev;
+    const double time = ctl->time;
+    const double time_prev = time + dt_prev;
+    // the new dt is factor * min(edge / c, dts_cur) <= factor * dts_cur
+    const double bound = ctl->dts_cur * ctl->factor;
+    const double rem = ctl->total_time - time_prev;
+    const int exact = (rem > 0.0 && rem < bound) ? 1 : 0;
+    ctl->need_exact = exact;
+    ctl->dt_final = 0;
+    if (!exact) {
+        double dt_i_1 = dt_prev;
+        if (time + dt_i_1 > ctl->step_end) {
+            const double r = ctl->step_end - time;
+            dt_i_1 = r;
+            ctl->dt_i = r;
+            ctl->dt_final = 1;
+        }
+        ctl->dt_i_1 = dt_i_1;
+        double t = time + dt_i_1;
+        if (t > ctl->total_time) t = ctl->total_time;
+        ctl->time = t;
+    }
+}
+
 // Folds the energy partials of the previous cycle, then performs the first
 // half of update_minVertex_perMaterial_and_dt for the next cycle: rotate
 // dt_i_1 <- dt_i, advance time (computeSate :775-780) and fix dt_i_1 unless
@@ -59,32 +109,7 @@ __global__ void __launch_bounds__(kCtlThreads) k_between(Ctl* ctl, Partials P, i
         ctl->done = 1;
         return;
     }
-    ctl->dts_cur = bits_ord(ctl->dts_next);
-    ctl->dts_next = kInfBits;
-    ctl->len_min = kInfBits;
-    const double dt_prev = ctl->dt_i;
-    ctl->dt_prev = dt_prev;
-    const double time = ctl->time;
-    const double time_prev = time + dt_prev;
-    // the new dt is factor * min(edge / c, dts_cur) <= factor * dts_cur
-    const double bound = ctl->dts_cur * ctl->factor;
-    const double rem = ctl->total_time - time_prev;
-    const int exact = (rem > 0.0 && rem < bound) ? 1 : 0;
-    ctl->need_exact = exact;
-    ctl->dt_final = 0;
-    if (!exact) {
-        double dt_i_1 = dt_prev;
-        if (time + dt_i_1 > ctl->step_end) {
-            const double r = ctl->step_end - time;
-            dt_i_1 = r;
-            ctl->dt_i = r;
-            ctl->dt_final = 1;
-        }
-        ctl->dt_i_1 = dt_i_1;
-        double t = time + dt_i_1;
-        if (t > ctl->total_time) t = ctl->total_time;
-        ctl->time = t;
-    }
+    cycle_begin(ctl);
 }
 
 // Minimum element edge over the current coordinates (min_ele_edge,
@@ -113,7 +138,7 @@ __global__ void __launch_bounds__(128) k_edge_prepass(ElemArrays E, NodeArrays N
             const double dx = xyz[A1[k]][0] - xyz[A0[k]][0];
             const double dy = xyz[A1[k]][1] - xyz[A0[k]][1];
             const double dz = xyz[A1[k]][2] - xyz[A0[k]][2];
-            const double t = dx * dx + dy * dy + dz * dz;
+            const double t = __fma_rn(dz, dz, __fma_rn(dy, dy, dx * dx));  // as the element pass
             mm = t < mm ? t : mm;
         }
         const double len = sqrt(mm);
@@ -135,8 +160,7 @@ __global__ void __launch_bounds__(128) k_edge_prepass(ElemArrays E, NodeArrays N
 
 // Rest of update_minVertex_perMaterial_and_dt and run()'s clamp for a cycle
 // that needed the exact edge minimum.
-__global__ void k_begin_exact(Ctl* ctl) {
-    if (threadIdx.x != 0 || ctl->done || !ctl->need_exact) return;
+__device__ __forceinline__ void begin_exact(Ctl* ctl) {
     const double time = ctl->time;
     double dt_i_1 = ctl->dt_prev;
     const double time_prev = time + dt_i_1;
@@ -158,6 +182,11 @@ __global__ void k_begin_exact(Ctl* ctl) {
     double t = time + dt_i_1;
     if (t > ctl->total_time) t = ctl->total_time;
     ctl->time = t;
+}
+
+__global__ void k_begin_exact(Ctl* ctl) {
+    if (threadIdx.x != 0 || ctl->done || !ctl->need_exact) return;
+    begin_exact(ctl);
 }
 
 __global__ void k_arm(Ctl* ctl, double step_end, long long max_cycles) {
@@ -235,6 +264,92 @@ __global__ void k_aos_to_soa(const double* aos, int64_t n, int64_t pad, int comp
     }
 }
 
+// ---- batched instances: one block per instance slot ------------------------
+// Folds the instance's tile partials of the last cycle in tile order and, in
+// mode 0, begins its next cycle exactly as k_between does for one instance.
+__global__ void __launch_bounds__(kCtlThreads) k_between_batch(BatchTables T, int mode) {
+    const int slot = blockIdx.x;
+    if (slot >= T.counts[2]) return;
+    const InstanceDesc& d = T.desc[slot];
+    if (!d.active) return;
+    Ctl* ctl = d.ctl;
+    if (ctl->energy_pending) {
+        const double ei = fixed_sum_strided(T.etile_part + 3 * static_cast<int64_t>(d.e_tile0) + 0, d.e_ntiles, 3);
+        const double eh = fixed_sum_strided(T.etile_part + 3 * static_cast<int64_t>(d.e_tile0) + 1, d.e_ntiles, 3);
+        const double ev = fixed_sum_strided(T.etile_part + 3 * static_cast<int64_t>(d.e_tile0) + 2, d.e_ntiles, 3);
+        const double kin = fixed_sum_strided(T.ntile_part + 2 * static_cast<int64_t>(d.n_tile0) + 0, d.n_ntiles, 2);
+        const double wx = fixed_sum_strided(T.ntile_part + 2 * static_cast<int64_t>(d.n_tile0) + 1, d.n_ntiles, 2);
+        if (threadIdx.x == 0) {
+            ctl->energy[0] = kin;
+            ctl->energy[1] += ei;
+            ctl->energy[2] += eh;
+            ctl->energy[3] += ev;
+            ctl->energy[4] += wx;
+            ctl->energy_pending = 0;
+        }
+    }
+    if (mode != 0 || threadIdx.x != 0 || ctl->done) return;
+    if (ctl->status || !(ctl->time < ctl->step_end) || ctl->cycles_done >= ctl->cycles_target) {
+        ctl->done = 1;
+        return;
+    }
+    cycle_begin(ctl);
+}
+
+// Minimum element edge for the instances whose cycle may hit the total-time
+// clamp (see k_edge_prepass), one warp per element tile.
+__global__ void __launch_bounds__(128) k_edge_prepass_batch(BatchTables T) {
+    const int lane = threadIdx.x & 31;
+    const int warp = static_cast<int>((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
+    const int nwarps = static_cast<int>((static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5);
+    for (int t = warp; t < T.counts[0]; t += nwarps) {
+        const InstanceDesc& d = T.desc[T.etile_inst[t]];
+        Ctl* ctl = d.ctl;
+        if (ctl->done || !ctl->need_exact) continue;
+        const int64_t e = static_cast<int64_t>(T.etile_base[t]) + lane;
+        double m = DBL_MAX;
+        if (e < d.E.ne) {
+            const int64_t ep = d.E.ne_pad, np = d.N.nn_pad;
+            double xyz[8][3];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const uint32_t n = d.E.conn[k * ep + e];
+                xyz[k][0] = d.N.x[n];
+                xyz[k][1] = d.N.x[np + n];
+                xyz[k][2] = d.N.x[2 * np + n];
+            }
+            constexpr int A0[12] = {0, 1, 2, 3, 4, 5, 6, 7, 0, 1, 2, 3};
+            constexpr int A1[12] = {1, 2, 3, 0, 5, 6, 7, 4, 4, 5, 6, 7};
+            double mm = DBL_MAX;
+#pragma unroll
+            for (int k = 0; k < 12; ++k) {
+                const double dx = xyz[A1[k]][0] - xyz[A0[k]][0];
+                const double dy = xyz[A1[k]][1] - xyz[A0[k]][1];
+                const double dz = xyz[A1[k]][2] - xyz[A0[k]][2];
+                const double tt = __fma_rn(dz, dz, __fma_rn(dy, dy, dx * dx));  // as the element pass
+                mm = tt < mm ? tt : mm;
+            }
+            m = sqrt(mm);
+        }
+        unsigned long long b = ord_bits(m);
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long w = __shfl_xor_sync(0xffffffffu, b, o);
+            b = w < b ? w : b;
+        }
+        if (lane == 0) atomicMin(&ctl->len_min, b);
+    }
+}
+
+__global__ void k_begin_exact_batch(BatchTables T) {
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= T.counts[2]) return;
+    const InstanceDesc& d = T.desc[slot];
+    if (!d.active) return;
+    Ctl* ctl = d.ctl;
+    if (ctl->done || !ctl->need_exact) return;
+    begin_exact(ctl);
+}
+
 int grid_for(int64_t work, int threads) {
     const int64_t g = (work + threads - 1) / threads;
     return static_cast<int>(g < 1 ? 1 : (g > 4096 ? 4096 : g));
@@ -242,6 +357,15 @@ int grid_for(int64_t work, int threads) {
 
 }  // namespace
 
+void launch_between_batch(const BatchTables& T, int slots, int mode, cudaStream_t st) {
+    k_between_batch<<<slots, kCtlThreads, 0, st>>>(T, mode);
+}
+void launch_edge_prepass_batch(const BatchTables& T, int grid, cudaStream_t st) {
+    k_edge_prepass_batch<<<grid, 128, 0, st>>>(T);
+}
+void launch_begin_exact_batch(const BatchTables& T, int slots, cudaStream_t st) {
+    k_begin_exact_batch<<<(slots + 127) / 128, 128, 0, st>>>(T);
+}
 void launch_between(Ctl* ctl, const Partials& P, int mode, cudaStream_t st) {
     k_between<<<1, kCtlThreads, 0, st>>>(ctl, P, mode);
 }

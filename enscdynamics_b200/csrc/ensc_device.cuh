@@ -112,6 +112,34 @@ struct Partials {
     int32_t n_elem_blocks, n_node_blocks;
 };
 
+// ---- batched instances ------------------------------------------------------
+// Independent solver instances advanced together: each warp-sized tile (32
+// elements or 32 nodes) belongs to one instance, so instance parameters,
+// clock and reductions are warp-uniform.
+constexpr int kTile = 32;
+
+struct InstanceDesc {
+    ElemArrays E;
+    NodeArrays N;
+    Material M;
+    Ctl* ctl;
+    int32_t e_tile0, e_ntiles;   // range in the element-tile list
+    int32_t n_tile0, n_ntiles;   // range in the node-tile list
+    int32_t active;
+    int32_t pad;
+};
+
+struct BatchTables {
+    const InstanceDesc* desc;    // [slots]
+    const int32_t* etile_inst;   // [etiles] instance slot of each element tile
+    const int32_t* etile_base;   // first element of the tile within its instance
+    const int32_t* ntile_inst;   // [ntiles]
+    const int32_t* ntile_base;
+    const int32_t* counts;       // [0] element tiles, [1] node tiles, [2] slots in use
+    double* etile_part;          // [etiles][3] internal / hourglass / viscous work per tile
+    double* ntile_part;          // [ntiles][2] kinetic / external work per tile
+};
+
 // Positive doubles order like their bit patterns; min-reductions over
 // element dt / edge lengths use integer atomicMin on the bits, which is
 // exact and independent of scheduling.

@@ -118,6 +118,252 @@ __device__ __forceinline__ void block_min2(double a, double b, unsigned long lon
     __syncthreads();
 }
 
+// One element of the element pass (the kernel comment below has the
+// reference mapping); shared by the single-instance and batched kernels.
+template <bool PLASTIC, bool INIT>
+__device__ __forceinline__ void element_body(const ElemArrays& E, const NodeArrays& N, const Material& M,
+                                             const double dt1, const int64_t e, double& dts, double& len,
+                                             double& e_int, double& e_hg, double& e_vis, int32_t& bad) {
+    const int64_t ep = E.ne_pad, np = N.nn_pad;
+    const uint32_t* __restrict__ conn = E.conn;
+    const double* __restrict__ bt = static_cast<const double*>(E.bt);
+    double* __restrict__ sig = static_cast<double*>(E.sigma);
+    double* __restrict__ qia = static_cast<double*>(E.qia);
+    double* __restrict__ epsp = static_cast<double*>(E.eps_p);
+    double* __restrict__ fe = static_cast<double*>(E.fe);
+    const double* __restrict__ X = N.x;
+    const double* __restrict__ U = N.u;
+    const double* __restrict__ V = static_cast<const double*>(N.v);
+    const double G = M.G, lam = M.lambda;
+
+    const double* __restrict__ bte = bt + e;
+    uint32_t n[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) n[k] = __ldg(conn + k * ep + e);
+    // current coordinates: hourglass projections TAU x (exact, the
+    // Gamma entries are +-1) and the minimum edge (min_ele_edge :1173-1220)
+    double TX[4][3];
+    {
+        double xyz[8][3];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            xyz[k][0] = X[n[k]];
+            xyz[k][1] = X[np + n[k]];
+            xyz[k][2] = X[2 * np + n[k]];
+        }
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                double t = tau_sign(kk, 0) > 0 ? xyz[0][c] : -xyz[0][c];
+#pragma unroll
+                for (int j = 1; j < 8; ++j) t = tau_sign(kk, j) > 0 ? t + xyz[j][c] : t - xyz[j][c];
+                TX[kk][c] = t;
+            }
+        constexpr int A0[12] = {0, 1, 2, 3, 4, 5, 6, 7, 0, 1, 2, 3};
+        constexpr int A1[12] = {1, 2, 3, 0, 5, 6, 7, 4, 4, 5, 6, 7};
+        double m = DBL_MAX;
+#pragma unroll
+        for (int k = 0; k < 12; ++k) {
+            const double dx = xyz[A1[k]][0] - xyz[A0[k]][0];
+            const double dy = xyz[A1[k]][1] - xyz[A0[k]][1];
+            const double dz = xyz[A1[k]][2] - xyz[A0[k]][2];
+            const double t = __fma_rn(dz, dz, __fma_rn(dy, dy, dx * dx));
+            m = t < m ? t : m;
+        }
+        len = sqrt(m);
+    }
+    // F = I + u_e B0^T (:862-865)
+    double F[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+#pragma unroll kNodeUnrollFp64
+    for (int k = 0; k < 8; ++k) {
+        const uint32_t nk = __ldg(conn + k * ep + e);
+        const double uu[3] = {U[nk], U[np + nk], U[2 * np + nk]};
+        const double* bk = bte + 3 * k * ep;
+        const double bb[3] = {__ldg(bk), __ldg(bk + ep), __ldg(bk + 2 * ep)};
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) F[r][c] = __fma_rn(uu[r], bb[c], F[r][c]);
+    }
+    F[0][0] = 1.0 + F[0][0];
+    F[1][1] = 1.0 + F[1][1];
+    F[2][2] = 1.0 + F[2][2];
+    const double J = det3(F);
+    double Fi[3][3];
+    inv3(F, Fi);
+    if (!(J > 0.0)) bad |= ST_INVERTED;
+    // per node: L0 = v_e B0^T, VT = v_e Gamma^T (signed sums), NX2 (:1024)
+    double L0[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+    double VT[3][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
+    double nx2 = 0.0;
+#pragma unroll kNodeUnrollFp64
+    for (int j = 0; j < 8; ++j) {
+        const uint32_t nj = __ldg(conn + j * ep + e);
+        const double* bk = bte + 3 * j * ep;
+        const double bb[3] = {__ldg(bk), __ldg(bk + ep), __ldg(bk + 2 * ep)};
+        const double vj[3] = {V[nj], V[np + nj], V[2 * np + nj]};
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) L0[r][c] = __fma_rn(vj[r], bb[c], L0[r][c]);
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) VT[r][kk] = tau_of(kk, j) > 0.0 ? VT[r][kk] + vj[r] : VT[r][kk] - vj[r];
+        }
+        nx2 = nx2 + __fma_rn(bb[2], bb[2], __fma_rn(bb[1], bb[1], bb[0] * bb[0]));
+    }
+    // L = L0 F^-1 (= v_e b^T, :928); HIA = VT - L0 TX^T (= v_e ATAU^T, :1020-1021)
+    double L[3][3], HIA[3][4];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            L[r][c] = __fma_rn(L0[r][2], Fi[2][c], __fma_rn(L0[r][1], Fi[1][c], L0[r][0] * Fi[0][c]));
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk)
+            HIA[r][kk] = VT[r][kk] - __fma_rn(L0[r][2], TX[kk][2], __fma_rn(L0[r][1], TX[kk][1], L0[r][0] * TX[kk][0]));
+    }
+    const double vr = (L[0][0] + L[1][1]) + L[2][2];
+    // Jaumann stress update (:930-973)
+    double eps[6];
+    eps[0] = L[0][0] * dt1;
+    eps[1] = L[1][1] * dt1;
+    eps[2] = L[2][2] * dt1;
+    eps[3] = (L[0][1] + L[1][0]) / 2.0 * dt1;
+    eps[4] = (L[0][2] + L[2][0]) / 2.0 * dt1;
+    eps[5] = (L[1][2] + L[2][1]) / 2.0 * dt1;
+    const double w0 = (L[0][1] - L[1][0]) / 2.0;
+    const double w1 = (L[0][2] - L[2][0]) / 2.0;
+    const double w2 = (L[1][2] - L[2][1]) / 2.0;
+    const double tr = (eps[0] + eps[1]) + eps[2];
+    double s[6], so[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) so[i] = sig[i * ep + e];
+    double inc[6];
+    inc[0] = (lam * tr + 2.0 * G * eps[0]) + 2.0 * so[3] * w0 * dt1 + 2.0 * so[4] * w1 * dt1;
+    inc[1] = (lam * tr + 2.0 * G * eps[1]) - 2.0 * so[3] * w0 * dt1 + 2.0 * so[5] * w2 * dt1;
+    inc[2] = (lam * tr + 2.0 * G * eps[2]) - 2.0 * so[4] * w1 * dt1 - 2.0 * so[5] * w2 * dt1;
+    inc[3] = (2.0 * G * eps[3]) + (so[1] - so[0]) * w0 * dt1 + so[5] * w1 * dt1;
+    inc[4] = (2.0 * G * eps[4]) + (so[2] - so[0]) * w1 * dt1 + so[5] * w0 * dt1;
+    inc[5] = (2.0 * G * eps[5]) + (so[2] - so[1]) * w2 * dt1 + so[3] * w1 * dt1 - so[4] * w0 * dt1;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) s[i] = so[i] + inc[i];
+    if (PLASTIC) {
+        // J2 radial return, linear isotropic hardening (no reference
+        // counterpart; the elastic instantiation omits it).
+        const double pm = ((s[0] + s[1]) + s[2]) / 3.0;
+        const double d0 = s[0] - pm, d1 = s[1] - pm, d2 = s[2] - pm;
+        const double j2 = 0.5 * ((d0 * d0 + d1 * d1) + d2 * d2) + ((s[3] * s[3] + s[4] * s[4]) + s[5] * s[5]);
+        const double seq = sqrt(3.0 * j2);
+        const double ep_old = epsp[e];
+        const double sy = M.yield0 + M.hardening * ep_old;
+        if (seq > sy) {
+            const double dl = (seq - sy) / (3.0 * G + M.hardening);
+            const double r = 1.0 - 3.0 * G * dl / seq;
+            s[0] = d0 * r + pm;
+            s[1] = d1 * r + pm;
+            s[2] = d2 * r + pm;
+            s[3] = s[3] * r;
+            s[4] = s[4] * r;
+            s[5] = s[5] * r;
+            if (!INIT) epsp[e] = ep_old + dl;
+        }
+    }
+    if (!INIT) {
+#pragma unroll
+        for (int i = 0; i < 6; ++i) sig[i * ep + e] = s[i];
+    }
+    const double V0 = E.vol0[e];
+    const double Vc = J * V0;
+    {
+        double w = 0.0;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            const double sm = 0.5 * (so[i] + s[i]);
+            w = w + (i < 3 ? 1.0 : 2.0) * sm * eps[i];
+        }
+        e_int += w * Vc;
+    }
+    // hourglass coefficients and history (:1038-1050); Gq = QIA + CR HIA
+    const double r43 = 4.0 / 3.0;
+    const double r1s8 = 1.0 / sqrt(8.0);
+    const double DR = M.c_dr * (r43 * G + M.K) * 0.1 * nx2 * Vc * r1s8 * dt1;
+    const double CR = M.c_cr * M.rho * V0 / Vc * E.cbrt_v0sq[e] * M.wos / 4.0;
+    double Gq[3][4];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+            const double q = __fma_rn(DR, HIA[i][kk], qia[(4 * i + kk) * ep + e]);
+            if (!INIT) qia[(4 * i + kk) * ep + e] = q;
+            Gq[i][kk] = __fma_rn(CR, HIA[i][kk], q);
+        }
+    // bulk viscosity pressure (:1073-1109)
+    const bool visc = !(fabs(vr) < 1.0e-10);
+    double pv = 0.0;
+    if (visc) {
+        const double rho_c = M.rho / J;
+        const double l0 = E.cbrt_v0[e];
+        const double m0 = vr < 0.0 ? vr : 0.0;
+        pv = rho_c * l0 * (M.cvisq * M.cvisq * l0 * vr * m0 - M.cvisl * M.wos * vr);
+        e_vis += -(pv * Vc * vr) * dt1;
+    }
+    // Z = Vc F^-1 (sigma - p I) - W^T, W = Gq TX
+    const double Sp[3][3] = {{s[0] - pv, s[3], s[4]}, {s[3], s[1] - pv, s[5]}, {s[4], s[5], s[2] - pv}};
+    double W[3][3], Z[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            W[i][c] = __fma_rn(Gq[i][3], TX[3][c],
+                               __fma_rn(Gq[i][2], TX[2][c], __fma_rn(Gq[i][1], TX[1][c], Gq[i][0] * TX[0][c])));
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+            Z[c][i] = Vc * __fma_rn(Fi[c][2], Sp[2][i], __fma_rn(Fi[c][1], Sp[1][i], Fi[c][0] * Sp[0][i])) - W[i][c];
+    // hourglass power sum_j h_j . v_j = Gq : HIA
+    {
+        double hp = 0.0;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) hp = __fma_rn(Gq[i][kk], HIA[i][kk], hp);
+        e_hg += hp * dt1;
+    }
+    // nodal forces f_j = -(B0_j Z) - Gamma_j Gq^T
+    // (= -b_j sigma V - h_j + p b_j V: :985-997, :1070, :1106)
+#pragma unroll kNodeUnrollFp64
+    for (int j = 0; j < 8; ++j) {
+        const double* bk = bte + 3 * j * ep;
+        const double b0 = __ldg(bk), b1 = __ldg(bk + ep), b2 = __ldg(bk + 2 * ep);
+        double* fej;
+        int64_t fst;
+        if (E.slot_major) {
+            fej = fe + 3 * j * np + __ldg(conn + j * ep + e);
+            fst = np;
+        } else {
+            fej = fe + 3 * j * ep + e;
+            fst = ep;
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            double tg = tau_of(0, j) > 0.0 ? Gq[i][0] : -Gq[i][0];
+#pragma unroll
+            for (int kk = 1; kk < 4; ++kk) tg = tau_of(kk, j) > 0.0 ? tg + Gq[i][kk] : tg - Gq[i][kk];
+            fej[i * fst] = -__fma_rn(b2, Z[2][i], __fma_rn(b1, Z[1][i], b0 * Z[0][i])) - tg;
+        }
+    }
+    // compute_dtStable (:828-834)
+    {
+        const double cd = M.wos;
+        const double m0 = vr < 0.0 ? vr : 0.0;
+        const double xi = M.cvisl - M.cvisq * M.cvisq * len / cd * m0;
+        dts = (sqrt(1.0 + xi * xi) - xi) * len / cd;
+    }
+    if (!isfinite(dts)) bad |= ST_NONFINITE;
+}
+
 // Element pass: add_inForce_to_rhs's element loop body
 // (exDyna3D.cpp:556-573): kinematics, Jaumann stress (+ J2 return),
 // hourglass, bulk viscosity, element dt and min edge.  Writes the element's
@@ -171,234 +417,7 @@ __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_FP64) k_element(E
                 }
             }
         }
-        if (live) {
-            const double* __restrict__ bte = bt + e;
-            uint32_t n[8];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) n[k] = __ldg(conn + k * ep + e);
-            // current coordinates: hourglass projections TAU x (exact, the
-            // Gamma entries are +-1) and the minimum edge (min_ele_edge :1173-1220)
-            double TX[4][3];
-            {
-                double xyz[8][3];
-#pragma unroll
-                for (int k = 0; k < 8; ++k) {
-                    xyz[k][0] = X[n[k]];
-                    xyz[k][1] = X[np + n[k]];
-                    xyz[k][2] = X[2 * np + n[k]];
-                }
-#pragma unroll
-                for (int kk = 0; kk < 4; ++kk)
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        double t = tau_sign(kk, 0) > 0 ? xyz[0][c] : -xyz[0][c];
-#pragma unroll
-                        for (int j = 1; j < 8; ++j) t = tau_sign(kk, j) > 0 ? t + xyz[j][c] : t - xyz[j][c];
-                        TX[kk][c] = t;
-                    }
-                constexpr int A0[12] = {0, 1, 2, 3, 4, 5, 6, 7, 0, 1, 2, 3};
-                constexpr int A1[12] = {1, 2, 3, 0, 5, 6, 7, 4, 4, 5, 6, 7};
-                double m = DBL_MAX;
-#pragma unroll
-                for (int k = 0; k < 12; ++k) {
-                    const double dx = xyz[A1[k]][0] - xyz[A0[k]][0];
-                    const double dy = xyz[A1[k]][1] - xyz[A0[k]][1];
-                    const double dz = xyz[A1[k]][2] - xyz[A0[k]][2];
-                    const double t = __fma_rn(dz, dz, __fma_rn(dy, dy, dx * dx));
-                    m = t < m ? t : m;
-                }
-                len = sqrt(m);
-            }
-            // F = I + u_e B0^T (:862-865)
-            double F[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
-#pragma unroll kNodeUnrollFp64
-            for (int k = 0; k < 8; ++k) {
-                const uint32_t nk = __ldg(conn + k * ep + e);
-                const double uu[3] = {U[nk], U[np + nk], U[2 * np + nk]};
-                const double* bk = bte + 3 * k * ep;
-                const double bb[3] = {__ldg(bk), __ldg(bk + ep), __ldg(bk + 2 * ep)};
-#pragma unroll
-                for (int r = 0; r < 3; ++r)
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) F[r][c] = __fma_rn(uu[r], bb[c], F[r][c]);
-            }
-            F[0][0] = 1.0 + F[0][0];
-            F[1][1] = 1.0 + F[1][1];
-            F[2][2] = 1.0 + F[2][2];
-            const double J = det3(F);
-            double Fi[3][3];
-            inv3(F, Fi);
-            if (!(J > 0.0)) bad |= ST_INVERTED;
-            // per node: L0 = v_e B0^T, VT = v_e Gamma^T (signed sums), NX2 (:1024)
-            double L0[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
-            double VT[3][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
-            double nx2 = 0.0;
-#pragma unroll kNodeUnrollFp64
-            for (int j = 0; j < 8; ++j) {
-                const uint32_t nj = __ldg(conn + j * ep + e);
-                const double* bk = bte + 3 * j * ep;
-                const double bb[3] = {__ldg(bk), __ldg(bk + ep), __ldg(bk + 2 * ep)};
-                const double vj[3] = {V[nj], V[np + nj], V[2 * np + nj]};
-#pragma unroll
-                for (int r = 0; r < 3; ++r) {
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) L0[r][c] = __fma_rn(vj[r], bb[c], L0[r][c]);
-#pragma unroll
-                    for (int kk = 0; kk < 4; ++kk) VT[r][kk] = tau_of(kk, j) > 0.0 ? VT[r][kk] + vj[r] : VT[r][kk] - vj[r];
-                }
-                nx2 = nx2 + __fma_rn(bb[2], bb[2], __fma_rn(bb[1], bb[1], bb[0] * bb[0]));
-            }
-            // L = L0 F^-1 (= v_e b^T, :928); HIA = VT - L0 TX^T (= v_e ATAU^T, :1020-1021)
-            double L[3][3], HIA[3][4];
-#pragma unroll
-            for (int r = 0; r < 3; ++r) {
-#pragma unroll
-                for (int c = 0; c < 3; ++c)
-                    L[r][c] = __fma_rn(L0[r][2], Fi[2][c], __fma_rn(L0[r][1], Fi[1][c], L0[r][0] * Fi[0][c]));
-#pragma unroll
-                for (int kk = 0; kk < 4; ++kk)
-                    HIA[r][kk] = VT[r][kk] - __fma_rn(L0[r][2], TX[kk][2], __fma_rn(L0[r][1], TX[kk][1], L0[r][0] * TX[kk][0]));
-            }
-            const double vr = (L[0][0] + L[1][1]) + L[2][2];
-            // Jaumann stress update (:930-973)
-            double eps[6];
-            eps[0] = L[0][0] * dt1;
-            eps[1] = L[1][1] * dt1;
-            eps[2] = L[2][2] * dt1;
-            eps[3] = (L[0][1] + L[1][0]) / 2.0 * dt1;
-            eps[4] = (L[0][2] + L[2][0]) / 2.0 * dt1;
-            eps[5] = (L[1][2] + L[2][1]) / 2.0 * dt1;
-            const double w0 = (L[0][1] - L[1][0]) / 2.0;
-            const double w1 = (L[0][2] - L[2][0]) / 2.0;
-            const double w2 = (L[1][2] - L[2][1]) / 2.0;
-            const double tr = (eps[0] + eps[1]) + eps[2];
-            double s[6], so[6];
-#pragma unroll
-            for (int i = 0; i < 6; ++i) so[i] = sig[i * ep + e];
-            double inc[6];
-            inc[0] = (lam * tr + 2.0 * G * eps[0]) + 2.0 * so[3] * w0 * dt1 + 2.0 * so[4] * w1 * dt1;
-            inc[1] = (lam * tr + 2.0 * G * eps[1]) - 2.0 * so[3] * w0 * dt1 + 2.0 * so[5] * w2 * dt1;
-            inc[2] = (lam * tr + 2.0 * G * eps[2]) - 2.0 * so[4] * w1 * dt1 - 2.0 * so[5] * w2 * dt1;
-            inc[3] = (2.0 * G * eps[3]) + (so[1] - so[0]) * w0 * dt1 + so[5] * w1 * dt1;
-            inc[4] = (2.0 * G * eps[4]) + (so[2] - so[0]) * w1 * dt1 + so[5] * w0 * dt1;
-            inc[5] = (2.0 * G * eps[5]) + (so[2] - so[1]) * w2 * dt1 + so[3] * w1 * dt1 - so[4] * w0 * dt1;
-#pragma unroll
-            for (int i = 0; i < 6; ++i) s[i] = so[i] + inc[i];
-            if (PLASTIC) {
-                // J2 radial return, linear isotropic hardening (no reference
-                // counterpart; the elastic instantiation omits it).
-                const double pm = ((s[0] + s[1]) + s[2]) / 3.0;
-                const double d0 = s[0] - pm, d1 = s[1] - pm, d2 = s[2] - pm;
-                const double j2 = 0.5 * ((d0 * d0 + d1 * d1) + d2 * d2) + ((s[3] * s[3] + s[4] * s[4]) + s[5] * s[5]);
-                const double seq = sqrt(3.0 * j2);
-                const double ep_old = epsp[e];
-                const double sy = M.yield0 + M.hardening * ep_old;
-                if (seq > sy) {
-                    const double dl = (seq - sy) / (3.0 * G + M.hardening);
-                    const double r = 1.0 - 3.0 * G * dl / seq;
-                    s[0] = d0 * r + pm;
-                    s[1] = d1 * r + pm;
-                    s[2] = d2 * r + pm;
-                    s[3] = s[3] * r;
-                    s[4] = s[4] * r;
-                    s[5] = s[5] * r;
-                    if (!INIT) epsp[e] = ep_old + dl;
-                }
-            }
-            if (!INIT) {
-#pragma unroll
-                for (int i = 0; i < 6; ++i) sig[i * ep + e] = s[i];
-            }
-            const double V0 = E.vol0[e];
-            const double Vc = J * V0;
-            {
-                double w = 0.0;
-#pragma unroll
-                for (int i = 0; i < 6; ++i) {
-                    const double sm = 0.5 * (so[i] + s[i]);
-                    w = w + (i < 3 ? 1.0 : 2.0) * sm * eps[i];
-                }
-                e_int += w * Vc;
-            }
-            // hourglass coefficients and history (:1038-1050); Gq = QIA + CR HIA
-            const double r43 = 4.0 / 3.0;
-            const double r1s8 = 1.0 / sqrt(8.0);
-            const double DR = M.c_dr * (r43 * G + M.K) * 0.1 * nx2 * Vc * r1s8 * dt1;
-            const double CR = M.c_cr * M.rho * V0 / Vc * E.cbrt_v0sq[e] * M.wos / 4.0;
-            double Gq[3][4];
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int kk = 0; kk < 4; ++kk) {
-                    const double q = __fma_rn(DR, HIA[i][kk], qia[(4 * i + kk) * ep + e]);
-                    if (!INIT) qia[(4 * i + kk) * ep + e] = q;
-                    Gq[i][kk] = __fma_rn(CR, HIA[i][kk], q);
-                }
-            // bulk viscosity pressure (:1073-1109)
-            const bool visc = !(fabs(vr) < 1.0e-10);
-            double pv = 0.0;
-            if (visc) {
-                const double rho_c = M.rho / J;
-                const double l0 = E.cbrt_v0[e];
-                const double m0 = vr < 0.0 ? vr : 0.0;
-                pv = rho_c * l0 * (M.cvisq * M.cvisq * l0 * vr * m0 - M.cvisl * M.wos * vr);
-                e_vis += -(pv * Vc * vr) * dt1;
-            }
-            // Z = Vc F^-1 (sigma - p I) - W^T, W = Gq TX
-            const double Sp[3][3] = {{s[0] - pv, s[3], s[4]}, {s[3], s[1] - pv, s[5]}, {s[4], s[5], s[2] - pv}};
-            double W[3][3], Z[3][3];
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int c = 0; c < 3; ++c)
-                    W[i][c] = __fma_rn(Gq[i][3], TX[3][c],
-                                       __fma_rn(Gq[i][2], TX[2][c], __fma_rn(Gq[i][1], TX[1][c], Gq[i][0] * TX[0][c])));
-#pragma unroll
-            for (int c = 0; c < 3; ++c)
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-                    Z[c][i] = Vc * __fma_rn(Fi[c][2], Sp[2][i], __fma_rn(Fi[c][1], Sp[1][i], Fi[c][0] * Sp[0][i])) - W[i][c];
-            // hourglass power sum_j h_j . v_j = Gq : HIA
-            {
-                double hp = 0.0;
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int kk = 0; kk < 4; ++kk) hp = __fma_rn(Gq[i][kk], HIA[i][kk], hp);
-                e_hg += hp * dt1;
-            }
-            // nodal forces f_j = -(B0_j Z) - Gamma_j Gq^T
-            // (= -b_j sigma V - h_j + p b_j V: :985-997, :1070, :1106)
-#pragma unroll kNodeUnrollFp64
-            for (int j = 0; j < 8; ++j) {
-                const double* bk = bte + 3 * j * ep;
-                const double b0 = __ldg(bk), b1 = __ldg(bk + ep), b2 = __ldg(bk + 2 * ep);
-                double* fej;
-                int64_t fst;
-                if (E.slot_major) {
-                    fej = fe + 3 * j * np + __ldg(conn + j * ep + e);
-                    fst = np;
-                } else {
-                    fej = fe + 3 * j * ep + e;
-                    fst = ep;
-                }
-#pragma unroll
-                for (int i = 0; i < 3; ++i) {
-                    double tg = tau_of(0, j) > 0.0 ? Gq[i][0] : -Gq[i][0];
-#pragma unroll
-                    for (int kk = 1; kk < 4; ++kk) tg = tau_of(kk, j) > 0.0 ? tg + Gq[i][kk] : tg - Gq[i][kk];
-                    fej[i * fst] = -__fma_rn(b2, Z[2][i], __fma_rn(b1, Z[1][i], b0 * Z[0][i])) - tg;
-                }
-            }
-            // compute_dtStable (:828-834)
-            {
-                const double cd = M.wos;
-                const double m0 = vr < 0.0 ? vr : 0.0;
-                const double xi = M.cvisl - M.cvisq * M.cvisq * len / cd * m0;
-                dts = (sqrt(1.0 + xi * xi) - xi) * len / cd;
-            }
-            if (!isfinite(dts)) bad |= ST_NONFINITE;
-        }
+        if (live) element_body<PLASTIC, INIT>(E, N, M, dt1, e, dts, len, e_int, e_hg, e_vis, bad);
         dts_min = dts < dts_min ? dts : dts_min;
         len_min = len < len_min ? len : len_min;
     }
@@ -407,6 +426,105 @@ __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_FP64) k_element(E
     if (!INIT) {
         double v3[3] = {e_int, e_hg, e_vis};
         block_sum<kElemThreads, 3>(v3, P.elem, P.n_elem_blocks, blockIdx.x);
+    }
+}
+
+// One node of the node pass (see the kernel comment below); shared by the
+// single-instance and batched kernels.
+__device__ __forceinline__ void node_body(const ElemArrays& E, const NodeArrays& N, const Material& M,
+                                          const double dt_i, const double dt_i_1, const int64_t n, double& kin,
+                                          double& wext, int32_t& bad) {
+    const int64_t np = N.nn_pad, ep = E.ne_pad;
+    const double* __restrict__ fe = static_cast<const double*>(E.fe);
+    double* __restrict__ V = static_cast<double*>(N.v);
+    const double half = (dt_i + dt_i_1);
+    const double dt_avg = (dt_i + dt_i_1) / 2.0;
+
+    double f[3];
+    if (E.slot_major) {
+        // the reference's ((((((a0+a1)+a2)+a3)+a4)+a5)+a6)+a7 over the
+        // slots that hold an element (an absent slot adds +0.0)
+        f[0] = f[1] = f[2] = 0.0;
+        const uint32_t msk = N.slot_mask[n];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if ((msk >> k) & 1u) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) f[c] = f[c] + fe[(3 * k + c) * np + n];
+            }
+        }
+    } else if (N.csr_ptr == nullptr) {
+        f[0] = f[1] = f[2] = 0.0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const uint32_t el = __ldg(N.ell + k * np + n);
+            if (el != ENSC_NONE) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) f[c] = f[c] + fe[(3 * k + c) * ep + el];
+            }
+        }
+    } else {
+        // general lists: entries sorted by (slot, element); each slot's
+        // contributions are summed first (the reference's per-slot +=
+        // in element order), then added to the running total
+        f[0] = f[1] = f[2] = 0.0;
+        const int64_t b = N.csr_ptr[n], t = N.csr_ptr[n + 1];
+        int cur = -1;
+        double sl[3] = {0.0, 0.0, 0.0};
+        for (int64_t i = b; i < t; ++i) {
+            const uint32_t ent = N.csr_ent[i];
+            const int k = static_cast<int>(ent & 7u);
+            const uint32_t el = ent >> 3;
+            if (k != cur) {
+                if (cur >= 0) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) f[c] = f[c] + sl[c];
+                }
+                cur = k;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) sl[c] = 0.0 + fe[(3 * k + c) * ep + el];
+            } else {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) sl[c] = sl[c] + fe[(3 * k + c) * ep + el];
+            }
+        }
+        if (cur >= 0) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) f[c] = f[c] + sl[c];
+        }
+    }
+    const double im = N.inv_mass[n];
+    const uint32_t code = N.bc[n];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        double a = f[c];
+        double g = 0.0;
+        if (M.gravity_on) {
+            g = 1.0 * M.gravity_value * M.gravity_dir[c] / im;
+            a = a + g;
+        }
+        const uint32_t cc = (code >> (2 * c)) & 3u;
+        double r = 0.0, rf = 0.0;
+        if (cc & 2u) {
+            r = -a;
+            a = 0.0;
+        }
+        if ((cc & 1u) && a != 0.0) {
+            rf = -a;
+            r = -a;
+            a = 0.0;
+        }
+        if (cc) N.rf[c * np + n] = rf;
+        a = a * im;
+        const double vo = V[c * np + n];
+        const double vn = vo + half * a / 2.0;
+        V[c * np + n] = vn;
+        N.u[c * np + n] = N.u[c * np + n] + dt_i * vn;
+        N.x[c * np + n] = N.x[c * np + n] + dt_i * vn;
+        const double vb = 0.5 * (vo + vn);
+        wext = wext + (g + r) * dt_avg * vb;
+        kin = kin + 0.5 * (vn * vn) / im;
+        if (!isfinite(vn)) bad |= ST_NONFINITE;
     }
 }
 
@@ -443,96 +561,120 @@ __global__ void __launch_bounds__(kNodeThreads) k_node(ElemArrays E, NodeArrays 
     int32_t bad = 0;
     const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
     for (int64_t n = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; n < nn; n += stride) {
-        double f[3];
-        if (E.slot_major) {
-            // the reference's ((((((a0+a1)+a2)+a3)+a4)+a5)+a6)+a7 over the
-            // slots that hold an element (an absent slot adds +0.0)
-            f[0] = f[1] = f[2] = 0.0;
-            const uint32_t msk = N.slot_mask[n];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                if ((msk >> k) & 1u) {
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) f[c] = f[c] + fe[(3 * k + c) * np + n];
-                }
-            }
-        } else if (N.csr_ptr == nullptr) {
-            f[0] = f[1] = f[2] = 0.0;
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const uint32_t el = __ldg(N.ell + k * np + n);
-                if (el != ENSC_NONE) {
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) f[c] = f[c] + fe[(3 * k + c) * ep + el];
-                }
-            }
-        } else {
-            // general lists: entries sorted by (slot, element); each slot's
-            // contributions are summed first (the reference's per-slot +=
-            // in element order), then added to the running total
-            f[0] = f[1] = f[2] = 0.0;
-            const int64_t b = N.csr_ptr[n], t = N.csr_ptr[n + 1];
-            int cur = -1;
-            double sl[3] = {0.0, 0.0, 0.0};
-            for (int64_t i = b; i < t; ++i) {
-                const uint32_t ent = N.csr_ent[i];
-                const int k = static_cast<int>(ent & 7u);
-                const uint32_t el = ent >> 3;
-                if (k != cur) {
-                    if (cur >= 0) {
-#pragma unroll
-                        for (int c = 0; c < 3; ++c) f[c] = f[c] + sl[c];
-                    }
-                    cur = k;
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) sl[c] = 0.0 + fe[(3 * k + c) * ep + el];
-                } else {
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) sl[c] = sl[c] + fe[(3 * k + c) * ep + el];
-                }
-            }
-            if (cur >= 0) {
-#pragma unroll
-                for (int c = 0; c < 3; ++c) f[c] = f[c] + sl[c];
-            }
-        }
-        const double im = N.inv_mass[n];
-        const uint32_t code = N.bc[n];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            double a = f[c];
-            double g = 0.0;
-            if (M.gravity_on) {
-                g = 1.0 * M.gravity_value * M.gravity_dir[c] / im;
-                a = a + g;
-            }
-            const uint32_t cc = (code >> (2 * c)) & 3u;
-            double r = 0.0, rf = 0.0;
-            if (cc & 2u) {
-                r = -a;
-                a = 0.0;
-            }
-            if ((cc & 1u) && a != 0.0) {
-                rf = -a;
-                r = -a;
-                a = 0.0;
-            }
-            if (cc) N.rf[c * np + n] = rf;
-            a = a * im;
-            const double vo = V[c * np + n];
-            const double vn = vo + half * a / 2.0;
-            V[c * np + n] = vn;
-            N.u[c * np + n] = N.u[c * np + n] + dt_i * vn;
-            N.x[c * np + n] = N.x[c * np + n] + dt_i * vn;
-            const double vb = 0.5 * (vo + vn);
-            wext = wext + (g + r) * dt_avg * vb;
-            kin = kin + 0.5 * (vn * vn) / im;
-            if (!isfinite(vn)) bad |= ST_NONFINITE;
-        }
+        node_body(E, N, M, dt_i, dt_i_1, n, kin, wext, bad);
     }
     if (bad) atomicOr(&ctl->status, bad);
     double v2[2] = {kin, wext};
     block_sum<kNodeThreads, 2>(v2, P.node, P.n_node_blocks, blockIdx.x);
+}
+
+
+// ---- batched instances --------------------------------------------------------
+// One warp per 32-element (32-node) tile; each tile belongs to one instance,
+// whose arrays, material and control block come from the instance table.
+// Per-tile work sums are written to a tile-indexed buffer and folded per
+// instance in tile order, so the totals do not depend on scheduling.
+__device__ __forceinline__ double warp_sum_b(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = w < v ? w : v;
+    }
+    return v;
+}
+
+__global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_FP64) k_element_batch_fp64(BatchTables T) {
+    const int lane = threadIdx.x & 31;
+    const int warp = static_cast<int>((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
+    const int nwarps = static_cast<int>((static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5);
+    const int ntiles = T.counts[0];
+    for (int t = warp; t < ntiles; t += nwarps) {
+        const int slot = T.etile_inst[t];
+        const InstanceDesc& d = T.desc[slot];
+        Ctl* ctl = d.ctl;
+        double* part = T.etile_part + 3 * static_cast<int64_t>(t);
+        if (ctl->done) {
+            if (lane < 3) part[lane] = 0.0;
+            continue;
+        }
+        const double dt1 = ctl->dt_i_1;
+        const int64_t e = static_cast<int64_t>(T.etile_base[t]) + lane;
+        double dts = DBL_MAX, len = DBL_MAX;
+        double ei = 0.0, eh = 0.0, ev = 0.0;
+        int32_t bad = 0;
+        if (e < d.E.ne) {
+            if (d.M.plastic) element_body<true, false>(d.E, d.N, d.M, dt1, e, dts, len, ei, eh, ev, bad);
+            else element_body<false, false>(d.E, d.N, d.M, dt1, e, dts, len, ei, eh, ev, bad);
+        }
+        const unsigned long long dmin = warp_min_u64(ord_bits(static_cast<double>(dts)));
+        const unsigned long long lmin = warp_min_u64(ord_bits(static_cast<double>(len)));
+        ei = warp_sum_b(ei);
+        eh = warp_sum_b(eh);
+        ev = warp_sum_b(ev);
+        bad = static_cast<int32_t>(__reduce_or_sync(0xffffffffu, static_cast<unsigned>(bad)));
+        if (lane == 0) {
+            atomicMin(&ctl->dts_next, dmin);
+            atomicMin(&ctl->len_min, lmin);
+            if (bad) atomicOr(&ctl->status, bad);
+            part[0] = ei;
+            part[1] = eh;
+            part[2] = ev;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kNodeThreads) k_node_batch_fp64(BatchTables T) {
+    const int lane = threadIdx.x & 31;
+    const int warp = static_cast<int>((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
+    const int nwarps = static_cast<int>((static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5);
+    const int ntiles = T.counts[1];
+    for (int t = warp; t < ntiles; t += nwarps) {
+        const int slot = T.ntile_inst[t];
+        const InstanceDesc& d = T.desc[slot];
+        Ctl* ctl = d.ctl;
+        double* part = T.ntile_part + 2 * static_cast<int64_t>(t);
+        if (ctl->done) {
+            if (lane < 2) part[lane] = 0.0;
+            continue;
+        }
+        // stable dt of this cycle, identically on every tile of the instance
+        // (update_minVertex_perMaterial_and_dt, exDyna3D.cpp:673-679)
+        double dt_i;
+        const double dt_i_1 = ctl->dt_i_1;
+        const int dt_final = ctl->dt_final;
+        if (dt_final) {
+            dt_i = ctl->dt_i;
+        } else {
+            double dd = bits_ord(ctl->len_min) / ctl->wos;
+            const double tmp = ctl->dts_cur;
+            dd = dd < tmp ? dd : tmp;
+            dt_i = dd * ctl->factor;
+        }
+        if (t == d.n_tile0 && lane == 0) {
+            if (!(dt_i > 0.0) || !isfinite(dt_i)) atomicOr(&ctl->status, ST_BAD_DT);
+            if (!dt_final) ctl->dt_i = dt_i;
+            ctl->cycles_done += 1;
+            ctl->energy_pending = 1;
+        }
+        const int64_t n = static_cast<int64_t>(T.ntile_base[t]) + lane;
+        double kin = 0.0, wext = 0.0;
+        int32_t bad = 0;
+        if (n < d.N.nn) node_body(d.E, d.N, d.M, dt_i, dt_i_1, n, kin, wext, bad);
+        kin = warp_sum_b(kin);
+        wext = warp_sum_b(wext);
+        bad = static_cast<int32_t>(__reduce_or_sync(0xffffffffu, static_cast<unsigned>(bad)));
+        if (lane == 0) {
+            if (bad) atomicOr(&ctl->status, bad);
+            part[0] = kin;
+            part[1] = wext;
+        }
+    }
 }
 
 }  // namespace
@@ -563,6 +705,24 @@ int occupancy_element_fp64(bool plastic) {
 int occupancy_node_fp64() {
     int nb = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_node, kNodeThreads, 0);
+    return nb;
+}
+
+
+void launch_element_batch_fp64(const BatchTables& T, int grid, cudaStream_t st) {
+    k_element_batch_fp64<<<grid, kElemThreads, 0, st>>>(T);
+}
+void launch_node_batch_fp64(const BatchTables& T, int grid, cudaStream_t st) {
+    k_node_batch_fp64<<<grid, kNodeThreads, 0, st>>>(T);
+}
+int occupancy_element_batch_fp64() {
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_batch_fp64, kElemThreads, 0);
+    return nb;
+}
+int occupancy_node_batch_fp64() {
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_node_batch_fp64, kNodeThreads, 0);
     return nb;
 }
 

@@ -1,0 +1,324 @@
+// Host-side preparation and device layout of one solver instance.
+#include "ensc_instance.h"
+#include "ensc_kernels.h"
+
+#include <cmath>
+#include <cstring>
+
+namespace ensc {
+namespace {
+
+int64_t pad32(int64_t n) { return (n + 31) / 32 * 32; }
+
+// Restatement of compute_invMassMatrix (exDyna3D.cpp:492-515) with
+// FEValues::reinit at the single Gauss point (fevalues.h:232-265): J = dN X,
+// B = J^-1 dN, V0 = det(J) * 8, node mass += rho V0 / 8 in element order.
+// The 3x3 determinant and inverse are Eigen 3.4's closed forms, the library
+// the reference uses.
+double det3h(const double m[3][3]) {
+    const double h0 = m[0][0] * (m[1][1] * m[2][2] - m[1][2] * m[2][1]);
+    const double h1 = m[0][1] * (m[1][0] * m[2][2] - m[1][2] * m[2][0]);
+    const double h2 = m[0][2] * (m[1][0] * m[2][1] - m[1][1] * m[2][0]);
+    return (h0 - h1) + h2;
+}
+double cof3h(const double m[3][3], int i, int j) {
+    const int i1 = (i + 1) % 3, i2 = (i + 2) % 3, j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+    return m[i1][j1] * m[i2][j2] - m[i1][j2] * m[i2][j1];
+}
+void inv3h(const double m[3][3], double r[3][3]) {
+    const double c0 = cof3h(m, 0, 0), c1 = cof3h(m, 1, 0), c2 = cof3h(m, 2, 0);
+    const double det = (c0 * m[0][0] + c1 * m[1][0]) + c2 * m[2][0];
+    const double invdet = 1.0 / det;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) r[i][j] = cof3h(m, j, i) * invdet;
+}
+
+void element_constants(int64_t nn, int64_t ne, const uint32_t* conn, const double* x0, double rho,
+                       std::vector<double>& bt, std::vector<double>& vol0, std::vector<double>& inv_mass) {
+    static const double XI[8][3] = {{-1., -1., -1.}, {1., -1., -1.}, {1., 1., -1.}, {-1., 1., -1.},
+                                    {-1., -1., 1.},  {1., -1., 1.},  {1., 1., 1.},  {-1., 1., 1.}};
+    double dn[3][8];
+    for (int a = 0; a < 8; ++a)
+        for (int d = 0; d < 3; ++d) dn[d][a] = 1.0 / 8.0 * XI[a][d];
+    bt.assign(static_cast<size_t>(24 * ne), 0.0);
+    vol0.assign(static_cast<size_t>(ne), 0.0);
+    std::vector<double> mass(static_cast<size_t>(3 * nn), 0.0);
+    for (int64_t e = 0; e < ne; ++e) {
+        double xyz[8][3];
+        for (int a = 0; a < 8; ++a)
+            for (int c = 0; c < 3; ++c) xyz[a][c] = x0[3 * static_cast<int64_t>(conn[8 * e + a]) + c];
+        double jac[3][3];
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) {
+                double s = dn[r][0] * xyz[0][c];
+                for (int k = 1; k < 8; ++k) s += dn[r][k] * xyz[k][c];
+                jac[r][c] = s;
+            }
+        double ij[3][3];
+        inv3h(jac, ij);
+        const double detj = det3h(jac);
+        for (int a = 0; a < 8; ++a)
+            for (int r = 0; r < 3; ++r)
+                bt[24 * e + 3 * a + r] = (ij[r][0] * dn[0][a] + ij[r][1] * dn[1][a]) + ij[r][2] * dn[2][a];
+        const double v0 = detj * 8.0;
+        vol0[e] = v0;
+        const double nm = rho * v0 / 8.0;
+        for (int a = 0; a < 8; ++a)
+            for (int c = 0; c < 3; ++c) mass[3 * static_cast<int64_t>(conn[8 * e + a]) + c] += nm;
+    }
+    inv_mass.resize(static_cast<size_t>(3 * nn));
+    for (int64_t i = 0; i < 3 * nn; ++i) inv_mass[i] = 1.0 / mass[i];
+}
+
+// Converts an AoS host array [n][comps] into SoA [comps][pad] of type T.
+template <typename T>
+std::vector<T> to_soa(const double* aos, int64_t n, int64_t pad, int comps) {
+    std::vector<T> out(static_cast<size_t>(comps * pad), T(0));
+    for (int64_t i = 0; i < n; ++i)
+        for (int c = 0; c < comps; ++c) out[c * pad + i] = static_cast<T>(aos[i * comps + c]);
+    return out;
+}
+
+template <typename T>
+cudaError_t put(void* block, size_t off, const std::vector<T>& v, cudaStream_t st) {
+    if (v.empty()) return cudaSuccess;
+    return cudaMemcpyAsync(static_cast<char*>(block) + off, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice,
+                           st);
+}
+
+}  // namespace
+
+int instance_prepare(const ensc_mesh_desc* mesh, const ensc_material* mat, bool mixed, InstanceHost& h,
+                     std::string& err) {
+    if (!mesh || !mat) {
+        err = "mesh and material are required";
+        return ENSC_ERR_ARG;
+    }
+    if (mesh->n_nodes <= 0 || mesh->n_elements <= 0 || !mesh->conn || !mesh->x0) {
+        err = "empty mesh or missing conn/x0";
+        return ENSC_ERR_ARG;
+    }
+    if (mesh->n_nodes >= (int64_t(1) << 32) - 1 || mesh->n_elements >= (int64_t(1) << 29)) {
+        err = "mesh too large for 32-bit node / 29-bit element indices";
+        return ENSC_ERR_ARG;
+    }
+    if (!(mat->rho > 0.0) || !(mat->E > 0.0) || !(mat->nu < 0.5)) {
+        err = "invalid material";
+        return ENSC_ERR_ARG;
+    }
+    const int64_t nn = mesh->n_nodes, ne = mesh->n_elements;
+    for (int64_t i = 0; i < 8 * ne; ++i)
+        if (static_cast<int64_t>(mesh->conn[i]) >= nn) {
+            err = "connectivity index out of range";
+            return ENSC_ERR_ARG;
+        }
+    h.nn = nn;
+    h.ne = ne;
+    h.nn_pad = pad32(nn);
+    h.ne_pad = pad32(ne);
+    h.mixed = mixed;
+    h.plastic = mat->yield_stress > 0.0;
+    h.x0 = mesh->x0;
+    h.v0 = mesh->v0;
+    const int64_t ep = h.ne_pad, np = h.nn_pad;
+
+    // element constants and lumped mass
+    std::vector<double> inv_mass_dof;
+    if (mesh->bt && mesh->vol0 && mesh->inv_mass) {
+        h.bt.assign(mesh->bt, mesh->bt + 24 * ne);
+        h.vol0.assign(mesh->vol0, mesh->vol0 + ne);
+        inv_mass_dof.assign(mesh->inv_mass, mesh->inv_mass + 3 * nn);
+    } else {
+        element_constants(nn, ne, mesh->conn, mesh->x0, mat->rho, h.bt, h.vol0, inv_mass_dof);
+    }
+    h.cb.resize(ne);
+    h.cb2.resize(ne);
+    for (int64_t e = 0; e < ne; ++e) {
+        h.cb[e] = std::cbrt(h.vol0[e]);
+        h.cb2[e] = std::cbrt(h.vol0[e] * h.vol0[e]);
+    }
+    h.im.assign(static_cast<size_t>(np), 1.0);
+    for (int64_t n = 0; n < nn; ++n) h.im[n] = inv_mass_dof[3 * n];
+    h.conn_soa.assign(static_cast<size_t>(8 * ep), 0);
+    for (int64_t e = 0; e < ne; ++e)
+        for (int k = 0; k < 8; ++k) h.conn_soa[k * ep + e] = mesh->conn[8 * e + k];
+
+    // node-to-element tables: slot-major when no node repeats a local slot
+    h.ell.assign(static_cast<size_t>(8 * np), ENSC_NONE);
+    h.clash = false;
+    for (int k = 0; k < 8 && !h.clash; ++k)
+        for (int64_t e = 0; e < ne; ++e) {
+            uint32_t& slot = h.ell[k * np + mesh->conn[8 * e + k]];
+            if (slot != ENSC_NONE) {
+                h.clash = true;
+                break;
+            }
+            slot = static_cast<uint32_t>(e);
+        }
+    if (!h.clash) {
+        h.slot_mask.assign(static_cast<size_t>(np), 0);
+        for (int k = 0; k < 8; ++k)
+            for (int64_t n = 0; n < nn; ++n)
+                if (h.ell[k * np + n] != ENSC_NONE) h.slot_mask[n] |= static_cast<uint8_t>(1u << k);
+    } else {
+        h.csr_ptr.assign(static_cast<size_t>(nn + 1), 0);
+        for (int64_t i = 0; i < 8 * ne; ++i) h.csr_ptr[mesh->conn[i] + 1] += 1;
+        for (int64_t n = 0; n < nn; ++n) h.csr_ptr[n + 1] += h.csr_ptr[n];
+        h.csr_ent.resize(static_cast<size_t>(8 * ne));
+        std::vector<int64_t> fill(h.csr_ptr.begin(), h.csr_ptr.end() - 1);
+        for (int k = 0; k < 8; ++k)
+            for (int64_t e = 0; e < ne; ++e) {
+                const uint32_t n = mesh->conn[8 * e + k];
+                h.csr_ent[fill[n]++] = (static_cast<uint32_t>(e) << 3) | static_cast<uint32_t>(k);
+            }
+    }
+
+    // device layout
+    const size_t real = mixed ? 4 : 8;  // element state, forces and velocity
+    const size_t E8 = static_cast<size_t>(ep), N8 = static_cast<size_t>(np);
+    const size_t fe_rows = h.clash ? E8 : N8;
+    using P = InstanceHost::Piece;
+    h.size[P::CONN] = 8 * E8 * sizeof(uint32_t);
+    h.size[P::BT] = 24 * E8 * real;
+    h.size[P::VOL0] = E8 * 8;
+    h.size[P::CB] = E8 * 8;
+    h.size[P::CB2] = E8 * 8;
+    h.size[P::SIG] = 6 * E8 * real;
+    h.size[P::QIA] = 12 * E8 * real;
+    h.size[P::EPS] = E8 * real;
+    h.size[P::FE] = 24 * fe_rows * real;
+    h.size[P::X] = 3 * N8 * 8;
+    h.size[P::U] = 3 * N8 * 8;
+    h.size[P::V] = 3 * N8 * real;
+    h.size[P::IM] = N8 * 8;
+    h.size[P::BC] = N8;
+    h.size[P::BCV] = 3 * N8 * 8;
+    h.size[P::ELL] = 8 * N8 * sizeof(uint32_t);
+    h.size[P::RF] = 3 * N8 * 8;
+    h.size[P::CPTR] = h.clash ? static_cast<size_t>(nn + 1) * sizeof(int64_t) : 0;
+    h.size[P::CENT] = h.clash ? static_cast<size_t>(8 * ne) * sizeof(uint32_t) : 0;
+    h.size[P::MASK] = h.clash ? 0 : N8;
+    size_t total = 0;
+    for (int i = 0; i < P::NPIECE; ++i) {
+        h.off[i] = total;
+        total += (h.size[i] + 255) / 256 * 256;
+    }
+    h.bytes = total;
+    return ENSC_OK;
+}
+
+int instance_upload(const InstanceHost& h, void* block, cudaStream_t st, ElemArrays& E, NodeArrays& N,
+                    std::string& err) {
+    using P = InstanceHost::Piece;
+    const int64_t ep = h.ne_pad, np = h.nn_pad;
+    char* b = static_cast<char*>(block);
+    cudaError_t e = cudaMemsetAsync(block, 0, h.bytes, st);
+    std::vector<uint8_t> bc(static_cast<size_t>(np), 0);
+    if (h.mixed) {
+        if (e == cudaSuccess) e = put(block, h.off[P::BT], to_soa<float>(h.bt.data(), h.ne, ep, 24), st);
+        std::vector<float> v0f(h.vol0.begin(), h.vol0.end()), cbf(h.cb.begin(), h.cb.end());
+        if (e == cudaSuccess) e = put(block, h.off[P::VOL0], v0f, st);
+        if (e == cudaSuccess) e = put(block, h.off[P::CB], cbf, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // temporaries above die here
+    } else {
+        std::vector<double> btsoa = to_soa<double>(h.bt.data(), h.ne, ep, 24);
+        if (e == cudaSuccess) e = put(block, h.off[P::BT], btsoa, st);
+        if (e == cudaSuccess) e = put(block, h.off[P::VOL0], h.vol0, st);
+        if (e == cudaSuccess) e = put(block, h.off[P::CB], h.cb, st);
+        if (e == cudaSuccess) e = put(block, h.off[P::CB2], h.cb2, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    }
+    if (e == cudaSuccess) e = put(block, h.off[P::CONN], h.conn_soa, st);
+    if (e == cudaSuccess) e = put(block, h.off[P::IM], h.im, st);
+    std::vector<double> xs = to_soa<double>(h.x0, h.nn, np, 3);
+    if (e == cudaSuccess) e = put(block, h.off[P::X], xs, st);
+    std::vector<double> vd;
+    std::vector<float> vf;
+    if (h.v0) {
+        if (h.mixed) {
+            vf = to_soa<float>(h.v0, h.nn, np, 3);
+            if (e == cudaSuccess) e = put(block, h.off[P::V], vf, st);
+        } else {
+            vd = to_soa<double>(h.v0, h.nn, np, 3);
+            if (e == cudaSuccess) e = put(block, h.off[P::V], vd, st);
+        }
+    }
+    if (e == cudaSuccess) e = put(block, h.off[P::ELL], h.ell, st);
+    if (h.clash) {
+        if (e == cudaSuccess) e = put(block, h.off[P::CPTR], h.csr_ptr, st);
+        if (e == cudaSuccess) e = put(block, h.off[P::CENT], h.csr_ent, st);
+    } else {
+        if (e == cudaSuccess) e = put(block, h.off[P::MASK], h.slot_mask, st);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        err = std::string("instance upload: ") + cudaGetErrorString(e);
+        return ENSC_ERR_CUDA;
+    }
+    E = ElemArrays{};
+    E.ne = h.ne;
+    E.ne_pad = ep;
+    E.conn = reinterpret_cast<uint32_t*>(b + h.off[P::CONN]);
+    E.bt = b + h.off[P::BT];
+    E.vol0 = reinterpret_cast<double*>(b + h.off[P::VOL0]);
+    E.cbrt_v0 = reinterpret_cast<double*>(b + h.off[P::CB]);
+    E.cbrt_v0sq = reinterpret_cast<double*>(b + h.off[P::CB2]);
+    E.sigma = b + h.off[P::SIG];
+    E.qia = b + h.off[P::QIA];
+    E.eps_p = b + h.off[P::EPS];
+    E.fe = b + h.off[P::FE];
+    E.tiles_aligned = 1;  // pieces are 256-byte aligned, ne_pad % 32 == 0
+    E.slot_major = h.clash ? 0 : 1;
+    N = NodeArrays{};
+    N.nn = h.nn;
+    N.nn_pad = np;
+    N.x = reinterpret_cast<double*>(b + h.off[P::X]);
+    N.u = reinterpret_cast<double*>(b + h.off[P::U]);
+    N.v = b + h.off[P::V];
+    N.inv_mass = reinterpret_cast<double*>(b + h.off[P::IM]);
+    N.bc = reinterpret_cast<uint8_t*>(b + h.off[P::BC]);
+    N.bcv = reinterpret_cast<double*>(b + h.off[P::BCV]);
+    N.ell = reinterpret_cast<uint32_t*>(b + h.off[P::ELL]);
+    N.csr_ptr = h.clash ? reinterpret_cast<int64_t*>(b + h.off[P::CPTR]) : nullptr;
+    N.csr_ent = h.clash ? reinterpret_cast<uint32_t*>(b + h.off[P::CENT]) : nullptr;
+    N.rf = reinterpret_cast<double*>(b + h.off[P::RF]);
+    N.slot_mask = h.clash ? nullptr : reinterpret_cast<uint8_t*>(b + h.off[P::MASK]);
+    return ENSC_OK;
+}
+
+void material_from(const ensc_material* mat, const ensc_params* p, Material& M) {
+    M = Material{};
+    M.E = mat->E;
+    M.nu = mat->nu;
+    M.rho = mat->rho;
+    M.G = M.E / ((1.0 + M.nu) * 2.0);
+    M.K = M.E / (1.0 - 2.0 * M.nu) / 3.0;
+    M.lambda = 2.0 * M.G * M.nu / (1.0 - 2.0 * M.nu);
+    M.wos = std::sqrt((M.lambda + 2.0 * M.G) / M.rho);
+    M.yield0 = mat->yield_stress;
+    M.hardening = mat->hardening_modulus;
+    M.plastic = mat->yield_stress > 0.0 ? 1 : 0;
+    M.c_dr = p->c_dr;
+    M.c_cr = p->c_cr;
+    M.cvisl = p->cvisl;
+    M.cvisq = p->cvisq;
+    M.gravity_on = p->gravity_on;
+    M.gravity_value = p->gravity_value;
+    for (int i = 0; i < 3; ++i) M.gravity_dir[i] = p->gravity_dir[i];
+}
+
+Ctl initial_ctl(const ensc_params* p, const Material& M) {
+    Ctl c{};
+    c.time = 0.0;
+    c.dt_i = 0.0;
+    c.dt_i_1 = 0.0;
+    c.step_end = HUGE_VAL;
+    c.total_time = p->total_time;
+    c.factor = p->factor_timestep;
+    c.wos = M.wos;
+    c.dts_next = kInfBits;
+    c.len_min = kInfBits;
+    return c;
+}
+
+}  // namespace ensc

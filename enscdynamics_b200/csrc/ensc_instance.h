@@ -1,0 +1,55 @@
+// Host-side preparation and device layout of one solver instance, shared by
+// the single-instance handle (ensc_capi.cu) and the batch (ensc_batch.cu).
+// Internal; not part of the ABI.
+#pragma once
+
+#include "ensc_gpu.h"
+#include "ensc_device.cuh"
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+namespace ensc {
+
+// Everything exDyna3D::init() derives from the deck before stepping
+// (Explicit3D/source/exDyna3D.cpp:105-142) that the device needs, in host
+// memory, plus the byte layout of the instance's device block.
+struct InstanceHost {
+    int64_t nn = 0, ne = 0, nn_pad = 0, ne_pad = 0;
+    bool mixed = false, plastic = false, clash = false;
+    std::vector<uint32_t> conn_soa;   // [8][ne_pad]
+    std::vector<double> bt;           // [ne][24] row-major B0^T
+    std::vector<double> vol0, cb, cb2;  // [ne] V0, cbrt(V0), cbrt(V0^2)
+    std::vector<double> im;           // [nn_pad] inverse lumped mass per node
+    std::vector<uint32_t> ell;        // [8][nn_pad] element in slot k, or ENSC_NONE
+    std::vector<uint8_t> slot_mask;   // [nn_pad] occupied slots (clash-free meshes)
+    std::vector<int64_t> csr_ptr;     // clash meshes: (slot, element)-sorted lists
+    std::vector<uint32_t> csr_ent;
+    const double* x0 = nullptr;       // caller arrays, read during upload
+    const double* v0 = nullptr;
+    // device layout: byte offsets of the pieces in one 256-byte-aligned block
+    enum Piece { CONN, BT, VOL0, CB, CB2, SIG, QIA, EPS, FE, X, U, V, IM, BC, BCV, ELL, RF, CPTR, CENT, MASK, NPIECE };
+    size_t off[NPIECE] = {};
+    size_t size[NPIECE] = {};
+    size_t bytes = 0;
+};
+
+// Validates the mesh and fills `h` (element constants computed as
+// compute_invMassMatrix does unless the caller supplies them).
+int instance_prepare(const ensc_mesh_desc* mesh, const ensc_material* mat, bool mixed, InstanceHost& h,
+                     std::string& err);
+
+// Copies the instance into `block` (h.bytes bytes, 256-byte aligned) on
+// stream `st`, waits for the copies, and fills the array descriptors.
+int instance_upload(const InstanceHost& h, void* block, cudaStream_t st, ElemArrays& E, NodeArrays& N,
+                    std::string& err);
+
+// Material_elastic::update (Material_elastic.cpp:9-14) plus the controls.
+void material_from(const ensc_material* mat, const ensc_params* p, Material& M);
+
+// Initial control block for time 0.
+Ctl initial_ctl(const ensc_params* p, const Material& M);
+
+}  // namespace ensc

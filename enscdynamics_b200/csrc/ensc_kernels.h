@@ -51,6 +51,19 @@ void launch_node_mixed(const ElemArrays& E, const NodeArrays& N, const Material&
 int occupancy_element_mixed(bool plastic);
 int occupancy_node_mixed();
 
+// batched instances (one launch per phase for all instances of a batch)
+void launch_element_batch_fp64(const BatchTables& T, int grid, cudaStream_t st);
+void launch_node_batch_fp64(const BatchTables& T, int grid, cudaStream_t st);
+int occupancy_element_batch_fp64();
+int occupancy_node_batch_fp64();
+void launch_element_batch_mixed(const BatchTables& T, int grid, cudaStream_t st);
+void launch_node_batch_mixed(const BatchTables& T, int grid, cudaStream_t st);
+int occupancy_element_batch_mixed();
+int occupancy_node_batch_mixed();
+void launch_between_batch(const BatchTables& T, int slots, int mode, cudaStream_t st);
+void launch_edge_prepass_batch(const BatchTables& T, int grid, cudaStream_t st);
+void launch_begin_exact_batch(const BatchTables& T, int slots, cudaStream_t st);
+
 // control (ensc_control.cu, built with -fmad=false)
 // mode 0: fold energy partials + begin next cycle; 1: fold only; 2: fold as initial KE
 void launch_between(Ctl* ctl, const Partials& P, int mode, cudaStream_t st);

@@ -95,6 +95,227 @@ __device__ __forceinline__ float tau_f(int k, int j) {
     return ((kMask >> (8 * k + j)) & 1u) ? 1.f : -1.f;
 }
 
+// One element of the mixed element pass (see the kernel comment below);
+// shared by the single-instance and batched kernels.
+template <bool PLASTIC, bool INIT>
+__device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const NodeArrays& N, const Material& M,
+                                                   const float dt1, const double dt1d, const int64_t e, float& dts,
+                                                   float& len, double& e_int, double& e_hg, double& e_vis,
+                                                   int32_t& bad) {
+    const int64_t ep = E.ne_pad, np = N.nn_pad;
+    const uint32_t* __restrict__ conn = E.conn;
+    const float* __restrict__ bt = static_cast<const float*>(E.bt);
+    const float* __restrict__ vol0 = reinterpret_cast<const float*>(E.vol0);
+    const float* __restrict__ cb = reinterpret_cast<const float*>(E.cbrt_v0);
+    float* __restrict__ sig = static_cast<float*>(E.sigma);
+    float* __restrict__ qia = static_cast<float*>(E.qia);
+    float* __restrict__ epsp = static_cast<float*>(E.eps_p);
+    float* __restrict__ fe = static_cast<float*>(E.fe);
+    const double* __restrict__ X = N.x;
+    const float* __restrict__ V = static_cast<const float*>(N.v);
+    const float G = static_cast<float>(M.G), lam = static_cast<float>(M.lambda);
+    const float rho = static_cast<float>(M.rho), wos = static_cast<float>(M.wos);
+    const float cvisl = static_cast<float>(M.cvisl), cvisq = static_cast<float>(M.cvisq);
+    const float y0 = static_cast<float>(M.yield0), H = static_cast<float>(M.hardening);
+    const float DRc = static_cast<float>(M.c_dr * (4.0 / 3.0 * M.G + M.K) * 0.1 / sqrt(8.0));
+    const float CRc = static_cast<float>(M.c_cr * M.rho * M.wos / 4.0);
+    const float* __restrict__ bte = bt + e;
+    const uint32_t n0 = __ldg(conn + e);
+    const double x00 = X[n0], x01 = X[np + n0], x02 = X[2 * np + n0];
+    // coordinates relative to node 0 (differences formed in FP64):
+    // hourglass projections TAU x = TAU (x - x0) (the Gamma rows sum to
+    // zero), the minimum edge, and F = sum_j (x_j - x_0) B0_j, which equals
+    // I + u_e B0^T because sum_j X0_j B0_j = I and sum_j B0_j = 0
+    float TX[4][3] = {};
+    float F[3][3] = {};
+    {
+        float xr[8][3];
+        xr[0][0] = xr[0][1] = xr[0][2] = 0.f;
+#pragma unroll
+        for (int k = 1; k < 8; ++k) {
+            const uint32_t nk = __ldg(conn + k * ep + e);
+            xr[k][0] = static_cast<float>(X[nk] - x00);
+            xr[k][1] = static_cast<float>(X[np + nk] - x01);
+            xr[k][2] = static_cast<float>(X[2 * np + nk] - x02);
+        }
+#pragma unroll
+        for (int k = 1; k < 8; ++k) {
+            const float* bk = bte + 3 * k * ep;
+            const float bb[3] = {__ldg(bk), __ldg(bk + ep), __ldg(bk + 2 * ep)};
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) F[r][c] = fmaf(xr[k][r], bb[c], F[r][c]);
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk) TX[kk][r] += tau_f(kk, k) * xr[k][r];
+            }
+        }
+        constexpr int A0[12] = {0, 1, 2, 3, 4, 5, 6, 7, 0, 1, 2, 3};
+        constexpr int A1[12] = {1, 2, 3, 0, 5, 6, 7, 4, 4, 5, 6, 7};
+        float m = FLT_MAX;
+#pragma unroll
+        for (int k = 0; k < 12; ++k) {
+            const float dx = xr[A1[k]][0] - xr[A0[k]][0];
+            const float dy = xr[A1[k]][1] - xr[A0[k]][1];
+            const float dz = xr[A1[k]][2] - xr[A0[k]][2];
+            m = fminf(m, fmaf(dz, dz, fmaf(dy, dy, dx * dx)));
+        }
+        len = sqrtf(m);
+    }
+    const float J = det3f(F);
+    if (!(J > 0.f)) bad |= ST_INVERTED;
+    const float invdet = 1.f / J;
+    float Fi[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) Fi[i][j] = cof3f(F, j, i) * invdet;
+    // L0 = v_e B0^T, VT = v_e Gamma^T, NX2
+    float L0[3][3] = {}, VT[3][4] = {}, nx2 = 0.f;
+#pragma unroll kNodeUnrollMixed
+    for (int j = 0; j < 8; ++j) {
+        const uint32_t nj = __ldg(conn + j * ep + e);
+        const float vj[3] = {V[nj], V[np + nj], V[2 * np + nj]};
+        const float* bk = bte + 3 * j * ep;
+        const float bb[3] = {__ldg(bk), __ldg(bk + ep), __ldg(bk + 2 * ep)};
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) L0[r][c] = fmaf(vj[r], bb[c], L0[r][c]);
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) VT[r][kk] += tau_f(kk, j) * vj[r];
+        }
+        nx2 += fmaf(bb[2], bb[2], fmaf(bb[1], bb[1], bb[0] * bb[0]));
+    }
+    // L = L0 F^-1, HIA = VT - L0 TX^T
+    float L[3][3], HIA[3][4];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) L[r][c] = fmaf(L0[r][2], Fi[2][c], fmaf(L0[r][1], Fi[1][c], L0[r][0] * Fi[0][c]));
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk)
+            HIA[r][kk] = VT[r][kk] - fmaf(L0[r][2], TX[kk][2], fmaf(L0[r][1], TX[kk][1], L0[r][0] * TX[kk][0]));
+    }
+    const float vr = L[0][0] + L[1][1] + L[2][2];
+    // Jaumann stress update
+    float eps[6] = {L[0][0] * dt1, L[1][1] * dt1, L[2][2] * dt1, 0.5f * (L[0][1] + L[1][0]) * dt1,
+                    0.5f * (L[0][2] + L[2][0]) * dt1, 0.5f * (L[1][2] + L[2][1]) * dt1};
+    const float w0 = 0.5f * (L[0][1] - L[1][0]) * dt1;
+    const float w1 = 0.5f * (L[0][2] - L[2][0]) * dt1;
+    const float w2 = 0.5f * (L[1][2] - L[2][1]) * dt1;
+    const float tr = eps[0] + eps[1] + eps[2];
+    float so[6], s[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) so[i] = sig[i * ep + e];
+    const float g2 = 2.f * G;
+    s[0] = so[0] + lam * tr + g2 * eps[0] + 2.f * so[3] * w0 + 2.f * so[4] * w1;
+    s[1] = so[1] + lam * tr + g2 * eps[1] - 2.f * so[3] * w0 + 2.f * so[5] * w2;
+    s[2] = so[2] + lam * tr + g2 * eps[2] - 2.f * so[4] * w1 - 2.f * so[5] * w2;
+    s[3] = so[3] + g2 * eps[3] + (so[1] - so[0]) * w0 + so[5] * w1;
+    s[4] = so[4] + g2 * eps[4] + (so[2] - so[0]) * w1 + so[5] * w0;
+    s[5] = so[5] + g2 * eps[5] + (so[2] - so[1]) * w2 + so[3] * w1 - so[4] * w0;
+    if (PLASTIC) {
+        const float pm = (s[0] + s[1] + s[2]) * (1.f / 3.f);
+        const float d0 = s[0] - pm, d1 = s[1] - pm, d2 = s[2] - pm;
+        const float j2 = 0.5f * (d0 * d0 + d1 * d1 + d2 * d2) + s[3] * s[3] + s[4] * s[4] + s[5] * s[5];
+        const float seq = sqrtf(3.f * j2);
+        const float ep_old = epsp[e];
+        const float sy = y0 + H * ep_old;
+        if (seq > sy) {
+            const float dl = (seq - sy) / (3.f * G + H);
+            const float r = 1.f - 3.f * G * dl / seq;
+            s[0] = d0 * r + pm;
+            s[1] = d1 * r + pm;
+            s[2] = d2 * r + pm;
+            s[3] *= r;
+            s[4] *= r;
+            s[5] *= r;
+            if (!INIT) epsp[e] = ep_old + dl;
+        }
+    }
+    if (!INIT) {
+#pragma unroll
+        for (int i = 0; i < 6; ++i) sig[i * ep + e] = s[i];
+    }
+    const float V0 = vol0[e];
+    const float Vc = J * V0;
+    {
+        float w = 0.f;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) w += (i < 3 ? 0.5f : 1.0f) * (so[i] + s[i]) * eps[i];
+        e_int += static_cast<double>(w * Vc);
+    }
+    const float DR = DRc * nx2 * Vc * dt1;
+    const float cbe = cb[e];
+    const float CR = CRc * V0 / Vc * (cbe * cbe);
+    float Gq[3][4];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+            const float q = fmaf(DR, HIA[i][kk], qia[(4 * i + kk) * ep + e]);
+            if (!INIT) qia[(4 * i + kk) * ep + e] = q;
+            Gq[i][kk] = fmaf(CR, HIA[i][kk], q);
+        }
+    const bool visc = !(fabsf(vr) < 1.0e-10f);
+    float pv = 0.f;
+    if (visc) {
+        const float m0 = fminf(vr, 0.f);
+        pv = rho / J * cbe * (cvisq * cvisq * cbe * vr * m0 - cvisl * wos * vr);
+        e_vis += -static_cast<double>(pv * Vc * vr) * dt1d;
+    }
+    // Z = Vc F^-1 (sigma - p I) - W^T, W = Gq TX
+    const float Sp[3][3] = {{s[0] - pv, s[3], s[4]}, {s[3], s[1] - pv, s[5]}, {s[4], s[5], s[2] - pv}};
+    float W[3][3], Z[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            W[i][c] = fmaf(Gq[i][3], TX[3][c], fmaf(Gq[i][2], TX[2][c], fmaf(Gq[i][1], TX[1][c], Gq[i][0] * TX[0][c])));
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+            Z[c][i] = Vc * fmaf(Fi[c][2], Sp[2][i], fmaf(Fi[c][1], Sp[1][i], Fi[c][0] * Sp[0][i])) - W[i][c];
+    {
+        // hourglass power sum_j h_j . v_j = Gq : HIA
+        float hp = 0.f;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) hp = fmaf(Gq[i][kk], HIA[i][kk], hp);
+        e_hg += static_cast<double>(hp) * dt1d;
+    }
+    // nodal forces f_j = -(B0_j Z) - Gamma_j Gq^T
+#pragma unroll kNodeUnrollMixed
+    for (int j = 0; j < 8; ++j) {
+        const float* bk = bte + 3 * j * ep;
+        const float b0 = __ldg(bk), b1 = __ldg(bk + ep), b2 = __ldg(bk + 2 * ep);
+        float* fej;
+        int64_t fst;
+        if (E.slot_major) {
+            fej = fe + 3 * j * np + __ldg(conn + j * ep + e);
+            fst = np;
+        } else {
+            fej = fe + 3 * j * ep + e;
+            fst = ep;
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            float tg = 0.f;
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) tg += tau_f(kk, j) * Gq[i][kk];
+            fej[i * fst] = -fmaf(b2, Z[2][i], fmaf(b1, Z[1][i], b0 * Z[0][i])) - tg;
+        }
+    }
+    // element dt (compute_dtStable, exDyna3D.cpp:828-834)
+    const float m0 = fminf(vr, 0.f);
+    const float xi = cvisl - cvisq * cvisq * len / wos * m0;
+    dts = (sqrtf(1.f + xi * xi) - xi) * len / wos;
+    if (!isfinite(dts)) bad |= ST_NONFINITE;
+}
+
 template <bool PLASTIC, bool INIT>
 __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_MIXED)
     k_element_mixed(ElemArrays E, NodeArrays N, Material M, Ctl* ctl, Partials P) {
@@ -139,202 +360,8 @@ __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_MIXED)
                 }
             }
         }
-        const float* __restrict__ bte = bt + e;
-        const uint32_t n0 = __ldg(conn + e);
-        const double x00 = X[n0], x01 = X[np + n0], x02 = X[2 * np + n0];
-        // coordinates relative to node 0 (differences formed in FP64):
-        // hourglass projections TAU x = TAU (x - x0) (the Gamma rows sum to
-        // zero), the minimum edge, and F = sum_j (x_j - x_0) B0_j, which equals
-        // I + u_e B0^T because sum_j X0_j B0_j = I and sum_j B0_j = 0
-        float TX[4][3] = {};
-        float F[3][3] = {};
-        float len;
-        {
-            float xr[8][3];
-            xr[0][0] = xr[0][1] = xr[0][2] = 0.f;
-#pragma unroll
-            for (int k = 1; k < 8; ++k) {
-                const uint32_t nk = __ldg(conn + k * ep + e);
-                xr[k][0] = static_cast<float>(X[nk] - x00);
-                xr[k][1] = static_cast<float>(X[np + nk] - x01);
-                xr[k][2] = static_cast<float>(X[2 * np + nk] - x02);
-            }
-#pragma unroll
-            for (int k = 1; k < 8; ++k) {
-                const float* bk = bte + 3 * k * ep;
-                const float bb[3] = {__ldg(bk), __ldg(bk + ep), __ldg(bk + 2 * ep)};
-#pragma unroll
-                for (int r = 0; r < 3; ++r) {
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) F[r][c] = fmaf(xr[k][r], bb[c], F[r][c]);
-#pragma unroll
-                    for (int kk = 0; kk < 4; ++kk) TX[kk][r] += tau_f(kk, k) * xr[k][r];
-                }
-            }
-            constexpr int A0[12] = {0, 1, 2, 3, 4, 5, 6, 7, 0, 1, 2, 3};
-            constexpr int A1[12] = {1, 2, 3, 0, 5, 6, 7, 4, 4, 5, 6, 7};
-            float m = FLT_MAX;
-#pragma unroll
-            for (int k = 0; k < 12; ++k) {
-                const float dx = xr[A1[k]][0] - xr[A0[k]][0];
-                const float dy = xr[A1[k]][1] - xr[A0[k]][1];
-                const float dz = xr[A1[k]][2] - xr[A0[k]][2];
-                m = fminf(m, fmaf(dz, dz, fmaf(dy, dy, dx * dx)));
-            }
-            len = sqrtf(m);
-        }
-        const float J = det3f(F);
-        if (!(J > 0.f)) bad |= ST_INVERTED;
-        const float invdet = 1.f / J;
-        float Fi[3][3];
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int j = 0; j < 3; ++j) Fi[i][j] = cof3f(F, j, i) * invdet;
-        // L0 = v_e B0^T, VT = v_e Gamma^T, NX2
-        float L0[3][3] = {}, VT[3][4] = {}, nx2 = 0.f;
-#pragma unroll kNodeUnrollMixed
-        for (int j = 0; j < 8; ++j) {
-            const uint32_t nj = __ldg(conn + j * ep + e);
-            const float vj[3] = {V[nj], V[np + nj], V[2 * np + nj]};
-            const float* bk = bte + 3 * j * ep;
-            const float bb[3] = {__ldg(bk), __ldg(bk + ep), __ldg(bk + 2 * ep)};
-#pragma unroll
-            for (int r = 0; r < 3; ++r) {
-#pragma unroll
-                for (int c = 0; c < 3; ++c) L0[r][c] = fmaf(vj[r], bb[c], L0[r][c]);
-#pragma unroll
-                for (int kk = 0; kk < 4; ++kk) VT[r][kk] += tau_f(kk, j) * vj[r];
-            }
-            nx2 += fmaf(bb[2], bb[2], fmaf(bb[1], bb[1], bb[0] * bb[0]));
-        }
-        // L = L0 F^-1, HIA = VT - L0 TX^T
-        float L[3][3], HIA[3][4];
-#pragma unroll
-        for (int r = 0; r < 3; ++r) {
-#pragma unroll
-            for (int c = 0; c < 3; ++c) L[r][c] = fmaf(L0[r][2], Fi[2][c], fmaf(L0[r][1], Fi[1][c], L0[r][0] * Fi[0][c]));
-#pragma unroll
-            for (int kk = 0; kk < 4; ++kk)
-                HIA[r][kk] = VT[r][kk] - fmaf(L0[r][2], TX[kk][2], fmaf(L0[r][1], TX[kk][1], L0[r][0] * TX[kk][0]));
-        }
-        const float vr = L[0][0] + L[1][1] + L[2][2];
-        // Jaumann stress update
-        float eps[6] = {L[0][0] * dt1, L[1][1] * dt1, L[2][2] * dt1, 0.5f * (L[0][1] + L[1][0]) * dt1,
-                        0.5f * (L[0][2] + L[2][0]) * dt1, 0.5f * (L[1][2] + L[2][1]) * dt1};
-        const float w0 = 0.5f * (L[0][1] - L[1][0]) * dt1;
-        const float w1 = 0.5f * (L[0][2] - L[2][0]) * dt1;
-        const float w2 = 0.5f * (L[1][2] - L[2][1]) * dt1;
-        const float tr = eps[0] + eps[1] + eps[2];
-        float so[6], s[6];
-#pragma unroll
-        for (int i = 0; i < 6; ++i) so[i] = sig[i * ep + e];
-        const float g2 = 2.f * G;
-        s[0] = so[0] + lam * tr + g2 * eps[0] + 2.f * so[3] * w0 + 2.f * so[4] * w1;
-        s[1] = so[1] + lam * tr + g2 * eps[1] - 2.f * so[3] * w0 + 2.f * so[5] * w2;
-        s[2] = so[2] + lam * tr + g2 * eps[2] - 2.f * so[4] * w1 - 2.f * so[5] * w2;
-        s[3] = so[3] + g2 * eps[3] + (so[1] - so[0]) * w0 + so[5] * w1;
-        s[4] = so[4] + g2 * eps[4] + (so[2] - so[0]) * w1 + so[5] * w0;
-        s[5] = so[5] + g2 * eps[5] + (so[2] - so[1]) * w2 + so[3] * w1 - so[4] * w0;
-        if (PLASTIC) {
-            const float pm = (s[0] + s[1] + s[2]) * (1.f / 3.f);
-            const float d0 = s[0] - pm, d1 = s[1] - pm, d2 = s[2] - pm;
-            const float j2 = 0.5f * (d0 * d0 + d1 * d1 + d2 * d2) + s[3] * s[3] + s[4] * s[4] + s[5] * s[5];
-            const float seq = sqrtf(3.f * j2);
-            const float ep_old = epsp[e];
-            const float sy = y0 + H * ep_old;
-            if (seq > sy) {
-                const float dl = (seq - sy) / (3.f * G + H);
-                const float r = 1.f - 3.f * G * dl / seq;
-                s[0] = d0 * r + pm;
-                s[1] = d1 * r + pm;
-                s[2] = d2 * r + pm;
-                s[3] *= r;
-                s[4] *= r;
-                s[5] *= r;
-                if (!INIT) epsp[e] = ep_old + dl;
-            }
-        }
-        if (!INIT) {
-#pragma unroll
-            for (int i = 0; i < 6; ++i) sig[i * ep + e] = s[i];
-        }
-        const float V0 = vol0[e];
-        const float Vc = J * V0;
-        {
-            float w = 0.f;
-#pragma unroll
-            for (int i = 0; i < 6; ++i) w += (i < 3 ? 0.5f : 1.0f) * (so[i] + s[i]) * eps[i];
-            e_int += static_cast<double>(w * Vc);
-        }
-        const float DR = DRc * nx2 * Vc * dt1;
-        const float cbe = cb[e];
-        const float CR = CRc * V0 / Vc * (cbe * cbe);
-        float Gq[3][4];
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int kk = 0; kk < 4; ++kk) {
-                const float q = fmaf(DR, HIA[i][kk], qia[(4 * i + kk) * ep + e]);
-                if (!INIT) qia[(4 * i + kk) * ep + e] = q;
-                Gq[i][kk] = fmaf(CR, HIA[i][kk], q);
-            }
-        const bool visc = !(fabsf(vr) < 1.0e-10f);
-        float pv = 0.f;
-        if (visc) {
-            const float m0 = fminf(vr, 0.f);
-            pv = rho / J * cbe * (cvisq * cvisq * cbe * vr * m0 - cvisl * wos * vr);
-            e_vis += -static_cast<double>(pv * Vc * vr) * dt1d;
-        }
-        // Z = Vc F^-1 (sigma - p I) - W^T, W = Gq TX
-        const float Sp[3][3] = {{s[0] - pv, s[3], s[4]}, {s[3], s[1] - pv, s[5]}, {s[4], s[5], s[2] - pv}};
-        float W[3][3], Z[3][3];
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int c = 0; c < 3; ++c)
-                W[i][c] = fmaf(Gq[i][3], TX[3][c], fmaf(Gq[i][2], TX[2][c], fmaf(Gq[i][1], TX[1][c], Gq[i][0] * TX[0][c])));
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-                Z[c][i] = Vc * fmaf(Fi[c][2], Sp[2][i], fmaf(Fi[c][1], Sp[1][i], Fi[c][0] * Sp[0][i])) - W[i][c];
-        {
-            // hourglass power sum_j h_j . v_j = Gq : HIA
-            float hp = 0.f;
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int kk = 0; kk < 4; ++kk) hp = fmaf(Gq[i][kk], HIA[i][kk], hp);
-            e_hg += static_cast<double>(hp) * dt1d;
-        }
-        // nodal forces f_j = -(B0_j Z) - Gamma_j Gq^T
-#pragma unroll kNodeUnrollMixed
-        for (int j = 0; j < 8; ++j) {
-            const float* bk = bte + 3 * j * ep;
-            const float b0 = __ldg(bk), b1 = __ldg(bk + ep), b2 = __ldg(bk + 2 * ep);
-            float* fej;
-            int64_t fst;
-            if (E.slot_major) {
-                fej = fe + 3 * j * np + __ldg(conn + j * ep + e);
-                fst = np;
-            } else {
-                fej = fe + 3 * j * ep + e;
-                fst = ep;
-            }
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                float tg = 0.f;
-#pragma unroll
-                for (int kk = 0; kk < 4; ++kk) tg += tau_f(kk, j) * Gq[i][kk];
-                fej[i * fst] = -fmaf(b2, Z[2][i], fmaf(b1, Z[1][i], b0 * Z[0][i])) - tg;
-            }
-        }
-        // element dt (compute_dtStable, exDyna3D.cpp:828-834)
-        const float m0 = fminf(vr, 0.f);
-        const float xi = cvisl - cvisq * cvisq * len / wos * m0;
-        const float dts = (sqrtf(1.f + xi * xi) - xi) * len / wos;
-        if (!isfinite(dts)) bad |= ST_NONFINITE;
+        float dts, len;
+        element_body_mixed<PLASTIC, INIT>(E, N, M, dt1, dt1d, e, dts, len, e_int, e_hg, e_vis, bad);
         dts_min = fmin(dts_min, static_cast<double>(dts));
         len_min = fmin(len_min, static_cast<double>(len));
     }
@@ -343,6 +370,80 @@ __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_MIXED)
     if (!INIT) {
         double v3[3] = {e_int, e_hg, e_vis};
         block_sum_d<kElemThreads, 3>(v3, P.elem, P.n_elem_blocks, blockIdx.x);
+    }
+}
+
+// One node of the mixed node pass; shared by the single-instance and
+// batched kernels.
+__device__ __forceinline__ void node_body_mixed(const ElemArrays& E, const NodeArrays& N, const Material& M,
+                                                const double dt_i, const double dt_i_1, const int64_t n,
+                                                double& kin, double& wext, int32_t& bad) {
+    const int64_t np = N.nn_pad, ep = E.ne_pad;
+    const float* __restrict__ fe = static_cast<const float*>(E.fe);
+    float* __restrict__ V = static_cast<float*>(N.v);
+    const float hdt = static_cast<float>(0.5 * (dt_i + dt_i_1));
+    const double dt_avg = 0.5 * (dt_i + dt_i_1);
+
+    float f[3] = {0.f, 0.f, 0.f};
+    if (E.slot_major) {
+        const uint32_t msk = N.slot_mask[n];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if ((msk >> k) & 1u) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) f[c] += fe[(3 * k + c) * np + n];
+            }
+        }
+    } else if (N.csr_ptr == nullptr) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const uint32_t el = __ldg(N.ell + k * np + n);
+            if (el != ENSC_NONE) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) f[c] += fe[(3 * k + c) * ep + el];
+            }
+        }
+    } else {
+        for (int64_t i = N.csr_ptr[n]; i < N.csr_ptr[n + 1]; ++i) {
+            const uint32_t ent = N.csr_ent[i];
+            const int k = static_cast<int>(ent & 7u);
+            const uint32_t el = ent >> 3;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) f[c] += fe[(3 * k + c) * ep + el];
+        }
+    }
+    const double im = N.inv_mass[n];
+    const float imf = static_cast<float>(im);
+    const uint32_t code = N.bc[n];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        float a = f[c];
+        float g = 0.f;
+        if (M.gravity_on) {
+            g = static_cast<float>(M.gravity_value * M.gravity_dir[c] / im);
+            a += g;
+        }
+        const uint32_t cc = (code >> (2 * c)) & 3u;
+        float r = 0.f, rf = 0.f;
+        if (cc & 2u) {
+            r = -a;
+            a = 0.f;
+        }
+        if ((cc & 1u) && a != 0.f) {
+            rf = -a;
+            r = -a;
+            a = 0.f;
+        }
+        if (cc) N.rf[c * np + n] = static_cast<double>(rf);
+        const float vo = V[c * np + n];
+        const float vn = fmaf(hdt, a * imf, vo);
+        V[c * np + n] = vn;
+        const double vnd = static_cast<double>(vn);
+        N.u[c * np + n] += dt_i * vnd;
+        N.x[c * np + n] += dt_i * vnd;
+        wext += static_cast<double>(g + r) * dt_avg * 0.5 * (static_cast<double>(vo) + vnd);
+        kin += 0.5 * (vnd * vnd) / im;
+        if (!isfinite(vn)) bad |= ST_NONFINITE;
     }
 }
 
@@ -375,71 +476,121 @@ __global__ void __launch_bounds__(kNodeThreads) k_node_mixed(ElemArrays E, NodeA
     int32_t bad = 0;
     const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
     for (int64_t n = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; n < nn; n += stride) {
-        float f[3] = {0.f, 0.f, 0.f};
-        if (E.slot_major) {
-            const uint32_t msk = N.slot_mask[n];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                if ((msk >> k) & 1u) {
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) f[c] += fe[(3 * k + c) * np + n];
-                }
-            }
-        } else if (N.csr_ptr == nullptr) {
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const uint32_t el = __ldg(N.ell + k * np + n);
-                if (el != ENSC_NONE) {
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) f[c] += fe[(3 * k + c) * ep + el];
-                }
-            }
-        } else {
-            for (int64_t i = N.csr_ptr[n]; i < N.csr_ptr[n + 1]; ++i) {
-                const uint32_t ent = N.csr_ent[i];
-                const int k = static_cast<int>(ent & 7u);
-                const uint32_t el = ent >> 3;
-#pragma unroll
-                for (int c = 0; c < 3; ++c) f[c] += fe[(3 * k + c) * ep + el];
-            }
-        }
-        const double im = N.inv_mass[n];
-        const float imf = static_cast<float>(im);
-        const uint32_t code = N.bc[n];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            float a = f[c];
-            float g = 0.f;
-            if (M.gravity_on) {
-                g = static_cast<float>(M.gravity_value * M.gravity_dir[c] / im);
-                a += g;
-            }
-            const uint32_t cc = (code >> (2 * c)) & 3u;
-            float r = 0.f, rf = 0.f;
-            if (cc & 2u) {
-                r = -a;
-                a = 0.f;
-            }
-            if ((cc & 1u) && a != 0.f) {
-                rf = -a;
-                r = -a;
-                a = 0.f;
-            }
-            if (cc) N.rf[c * np + n] = static_cast<double>(rf);
-            const float vo = V[c * np + n];
-            const float vn = fmaf(hdt, a * imf, vo);
-            V[c * np + n] = vn;
-            const double vnd = static_cast<double>(vn);
-            N.u[c * np + n] += dt_i * vnd;
-            N.x[c * np + n] += dt_i * vnd;
-            wext += static_cast<double>(g + r) * dt_avg * 0.5 * (static_cast<double>(vo) + vnd);
-            kin += 0.5 * (vnd * vnd) / im;
-            if (!isfinite(vn)) bad |= ST_NONFINITE;
-        }
+        node_body_mixed(E, N, M, dt_i, dt_i_1, n, kin, wext, bad);
     }
     if (bad) atomicOr(&ctl->status, bad);
     double v2[2] = {kin, wext};
     block_sum_d<kNodeThreads, 2>(v2, P.node, P.n_node_blocks, blockIdx.x);
+}
+
+
+// ---- batched instances --------------------------------------------------------
+// One warp per 32-element (32-node) tile; each tile belongs to one instance,
+// whose arrays, material and control block come from the instance table.
+// Per-tile work sums are written to a tile-indexed buffer and folded per
+// instance in tile order, so the totals do not depend on scheduling.
+__device__ __forceinline__ double warp_sum_b(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = w < v ? w : v;
+    }
+    return v;
+}
+
+__global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_MIXED) k_element_batch_mixed(BatchTables T) {
+    const int lane = threadIdx.x & 31;
+    const int warp = static_cast<int>((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
+    const int nwarps = static_cast<int>((static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5);
+    const int ntiles = T.counts[0];
+    for (int t = warp; t < ntiles; t += nwarps) {
+        const int slot = T.etile_inst[t];
+        const InstanceDesc& d = T.desc[slot];
+        Ctl* ctl = d.ctl;
+        double* part = T.etile_part + 3 * static_cast<int64_t>(t);
+        if (ctl->done) {
+            if (lane < 3) part[lane] = 0.0;
+            continue;
+        }
+        const double dt1d = ctl->dt_i_1;
+        const float dt1 = static_cast<float>(dt1d);
+        const int64_t e = static_cast<int64_t>(T.etile_base[t]) + lane;
+        float dts = FLT_MAX, len = FLT_MAX;
+        double ei = 0.0, eh = 0.0, ev = 0.0;
+        int32_t bad = 0;
+        if (e < d.E.ne) {
+            if (d.M.plastic) element_body_mixed<true, false>(d.E, d.N, d.M, dt1, dt1d, e, dts, len, ei, eh, ev, bad);
+            else element_body_mixed<false, false>(d.E, d.N, d.M, dt1, dt1d, e, dts, len, ei, eh, ev, bad);
+        }
+        const unsigned long long dmin = warp_min_u64(ord_bits(static_cast<double>(dts)));
+        const unsigned long long lmin = warp_min_u64(ord_bits(static_cast<double>(len)));
+        ei = warp_sum_b(ei);
+        eh = warp_sum_b(eh);
+        ev = warp_sum_b(ev);
+        bad = static_cast<int32_t>(__reduce_or_sync(0xffffffffu, static_cast<unsigned>(bad)));
+        if (lane == 0) {
+            atomicMin(&ctl->dts_next, dmin);
+            atomicMin(&ctl->len_min, lmin);
+            if (bad) atomicOr(&ctl->status, bad);
+            part[0] = ei;
+            part[1] = eh;
+            part[2] = ev;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kNodeThreads) k_node_batch_mixed(BatchTables T) {
+    const int lane = threadIdx.x & 31;
+    const int warp = static_cast<int>((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
+    const int nwarps = static_cast<int>((static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5);
+    const int ntiles = T.counts[1];
+    for (int t = warp; t < ntiles; t += nwarps) {
+        const int slot = T.ntile_inst[t];
+        const InstanceDesc& d = T.desc[slot];
+        Ctl* ctl = d.ctl;
+        double* part = T.ntile_part + 2 * static_cast<int64_t>(t);
+        if (ctl->done) {
+            if (lane < 2) part[lane] = 0.0;
+            continue;
+        }
+        // stable dt of this cycle, identically on every tile of the instance
+        // (update_minVertex_perMaterial_and_dt, exDyna3D.cpp:673-679)
+        double dt_i;
+        const double dt_i_1 = ctl->dt_i_1;
+        const int dt_final = ctl->dt_final;
+        if (dt_final) {
+            dt_i = ctl->dt_i;
+        } else {
+            double dd = bits_ord(ctl->len_min) / ctl->wos;
+            const double tmp = ctl->dts_cur;
+            dd = dd < tmp ? dd : tmp;
+            dt_i = dd * ctl->factor;
+        }
+        if (t == d.n_tile0 && lane == 0) {
+            if (!(dt_i > 0.0) || !isfinite(dt_i)) atomicOr(&ctl->status, ST_BAD_DT);
+            if (!dt_final) ctl->dt_i = dt_i;
+            ctl->cycles_done += 1;
+            ctl->energy_pending = 1;
+        }
+        const int64_t n = static_cast<int64_t>(T.ntile_base[t]) + lane;
+        double kin = 0.0, wext = 0.0;
+        int32_t bad = 0;
+        if (n < d.N.nn) node_body_mixed(d.E, d.N, d.M, dt_i, dt_i_1, n, kin, wext, bad);
+        kin = warp_sum_b(kin);
+        wext = warp_sum_b(wext);
+        bad = static_cast<int32_t>(__reduce_or_sync(0xffffffffu, static_cast<unsigned>(bad)));
+        if (lane == 0) {
+            if (bad) atomicOr(&ctl->status, bad);
+            part[0] = kin;
+            part[1] = wext;
+        }
+    }
 }
 
 }  // namespace
@@ -470,6 +621,24 @@ int occupancy_element_mixed(bool plastic) {
 int occupancy_node_mixed() {
     int nb = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_node_mixed, kNodeThreads, 0);
+    return nb;
+}
+
+
+void launch_element_batch_mixed(const BatchTables& T, int grid, cudaStream_t st) {
+    k_element_batch_mixed<<<grid, kElemThreads, 0, st>>>(T);
+}
+void launch_node_batch_mixed(const BatchTables& T, int grid, cudaStream_t st) {
+    k_node_batch_mixed<<<grid, kNodeThreads, 0, st>>>(T);
+}
+int occupancy_element_batch_mixed() {
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_batch_mixed, kElemThreads, 0);
+    return nb;
+}
+int occupancy_node_batch_mixed() {
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_node_batch_mixed, kNodeThreads, 0);
     return nb;
 }
 

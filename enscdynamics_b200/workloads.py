@@ -131,3 +131,105 @@ def impact_bar(n_core: int = 12, n_ring: int = 6, n_layers: int = 120, radius: f
     ctl = M.Controls(total_time=end_time, **DEFAULT_CONTROLS)
     return Problem("impact_bar", m, v0, code, val, mat, ctl, cycles=0, end_time=end_time,
                    fixed_sets=[("Set-1", "3, 3")], initial_velocity=[("Set-2", 3, v_impact)])
+
+
+# dt factor of the sweep and serving problems (stable over nu in [0.25, 0.4])
+SWEEP_DT_FACTOR = 0.8
+
+
+def _tip_ramp(m: M.Mesh, free: np.ndarray, v_tip: float, length: float) -> np.ndarray:
+    """Initial vz growing linearly from 0 at the clamp (x = 0) to v_tip at x = length."""
+    v0 = np.zeros((m.n_nodes, 3))
+    v0[free, 2] = v_tip * m.x0[free, 0] / length
+    return v0
+
+
+def sweep_instance(index: int, seed: int = 7, ne_min: int = 2000, ne_max: int = 60000, cycles: int = 3000,
+                   tangent: float = 100e6) -> Problem:
+    """Member ``index`` of the batched parameter sweep: a cantilever (even
+    index; aspect 5:1:1, nx = 5k, ny = nz = k) or a plate (odd index; 1 x 1 m,
+    k x k x 4 cells) clamped at x = 0, with its element count drawn
+    log-uniform in [ne_min, ne_max] and, per instance and seeded, E in
+    [50, 250] GPa, nu in [0.25, 0.4], rho in [2000, 9000] kg/m^3, J2 yield in
+    [150, 600] MPa (tangent modulus ``tangent``) and a tip velocity in [1, 50]
+    m/s: vz ramps linearly from 0 at the clamp to the tip value.
+
+    Elements are cubes (the plate's thickness is 4 of its k in-plane cells)
+    and the dt factor is SWEEP_DT_FACTOR: the reference's stable-dt estimate
+    (exDyna3D.cpp:663-686) ignores the hourglass stiffness and viscosity, and
+    with dt = 0.9 CFL its own algorithm diverges within ~100 cycles for
+    Poisson ratios above ~0.33 or flat elements, on the CPU as on the GPU."""
+    rng = np.random.default_rng([seed, index])
+    target = float(np.exp(rng.uniform(np.log(ne_min), np.log(ne_max))))
+    E = rng.uniform(50e9, 250e9)
+    nu = rng.uniform(0.25, 0.4)
+    rho = rng.uniform(2000.0, 9000.0)
+    ys = rng.uniform(150e6, 600e6)
+    v_tip = rng.uniform(1.0, 50.0)
+    if index % 2 == 0:
+        k = max(2, int(round((target / 5.0) ** (1.0 / 3.0))))
+        nx, ny, nz = 5 * k, k, k
+        lx, ly, lz = 2.0, 0.4, 0.4
+    else:
+        k = max(2, int(round(np.sqrt(target / 4.0))))
+        nx, ny, nz = k, k, 4
+        lx, ly, lz = 1.0, 1.0, 4.0 / k
+    m = M.box_mesh(nx, ny, nz, lx, ly, lz)
+    fix = M.face_nodes(m, 0, "min")
+    free = np.setdiff1d(np.arange(m.n_nodes), fix)
+    m.node_sets = {"Set-1": fix}
+    v0 = _tip_ramp(m, free, v_tip, lx)
+    code, val = M.bc_arrays(m.n_nodes, fixed=[(fix, 0, 2)])
+    ctl = M.Controls(total_time=1.0, **dict(DEFAULT_CONTROLS, factor=SWEEP_DT_FACTOR))
+    return Problem("sweep_%d" % index, m, v0, code, val, M.Material(E, nu, rho, ys, tangent), ctl, cycles,
+                   fixed_sets=[("Set-1", "ENCASTRE")], per_node_velocity=True)
+
+
+@dataclasses.dataclass
+class Request:
+    """One solve request of the serving stream."""
+
+    index: int
+    arrival: float        # seconds after the stream starts
+    problem: Problem
+
+
+def serving_requests(n: int, rate: float = 50.0, seed: int = 11, ne_min: int = 1000, ne_max: int = 500000,
+                     steps: Tuple[int, int] = (1000, 10000)) -> List[Request]:
+    """The serving stream: ``n`` requests arriving as a Poisson process of
+    ``rate`` per second, each a structured block (cantilever aspect 5:1:1 or
+    a 1 x 1 m plate of k x k x 4 cubes, chosen by a seeded draw) with its element
+    count log-uniform in [ne_min, ne_max], elastic or J2 (seeded, half each),
+    material and tip velocity drawn as in the batched sweep, and a cycle
+    count uniform in ``steps``; dt factor SWEEP_DT_FACTOR as in the sweep."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for i in range(n):
+        t += float(rng.exponential(1.0 / rate))
+        target = float(np.exp(rng.uniform(np.log(ne_min), np.log(ne_max))))
+        plate = bool(rng.integers(0, 2))
+        plastic = bool(rng.integers(0, 2))
+        E = rng.uniform(50e9, 250e9)
+        nu = rng.uniform(0.25, 0.4)
+        rho = rng.uniform(2000.0, 9000.0)
+        ys = rng.uniform(150e6, 600e6)
+        v_tip = rng.uniform(1.0, 50.0)
+        cycles = int(rng.integers(steps[0], steps[1] + 1))
+        if plate:
+            k = max(2, int(round(np.sqrt(target / 4.0))))
+            nx, ny, nz, lx, ly, lz = k, k, 4, 1.0, 1.0, 4.0 / k
+        else:
+            k = max(2, int(round((target / 5.0) ** (1.0 / 3.0))))
+            nx, ny, nz, lx, ly, lz = 5 * k, k, k, 2.0, 0.4, 0.4
+        m = M.box_mesh(nx, ny, nz, lx, ly, lz)
+        fix = M.face_nodes(m, 0, "min")
+        free = np.setdiff1d(np.arange(m.n_nodes), fix)
+        m.node_sets = {"Set-1": fix}
+        v0 = _tip_ramp(m, free, v_tip, lx)
+        code, val = M.bc_arrays(m.n_nodes, fixed=[(fix, 0, 2)])
+        mat = M.Material(E, nu, rho, ys if plastic else 0.0, 100e6 if plastic else 0.0)
+        ctl = M.Controls(total_time=1.0, **dict(DEFAULT_CONTROLS, factor=SWEEP_DT_FACTOR))
+        out.append(Request(i, t, Problem("request_%d" % i, m, v0, code, val, mat, ctl, cycles,
+                                         fixed_sets=[("Set-1", "ENCASTRE")], per_node_velocity=True)))
+    return out

@@ -188,6 +188,69 @@ int32_t ensc_kernels_per_cycle(const ensc_handle* h);
 
 void ensc_destroy(ensc_handle* h);
 
+/* ---- batches of independent solves --------------------------------------
+ * No counterpart in the reference, which runs one exDyna3D per process
+ * (main.cpp).  A batch steps many independent instances -- each its own
+ * mesh, material, controls, boundary conditions and clock, exactly what
+ * ensc_create/ensc_set_bcs/ensc_step would do for it alone -- with one
+ * launch per cycle phase for all of them.  Instances are sub-allocated from
+ * a device memory pool bounded by budget_bytes and can be added and removed
+ * between runs.  An armed instance advances until its own cycle budget or
+ * step end, then idles while the others continue.  All instances of a batch
+ * share its precision and stream.  Results of an instance do not depend on
+ * the other instances in the batch: its state and energies are those of the
+ * same solve with ensc_create (state bit-identical; energy sums may differ in
+ * the last bits, being summed per 32-element tile). */
+typedef struct ensc_batch ensc_batch;
+
+/* params: precision, device, stream (NULL: own stream) and graph_chunk
+ * (cycles per graph launch, 0: tuned) are used; the solve controls come per
+ * instance.  Capacities bound the instances and their total elements and
+ * nodes; budget_bytes bounds the instances' device memory. */
+int ensc_batch_create(const ensc_params* params, int32_t max_instances, int64_t max_elements, int64_t max_nodes,
+                      int64_t budget_bytes, ensc_batch** out);
+
+/* Adds an instance (ensc_create's work for it, controls from `controls`);
+ * *slot receives its index.  ENSC_ERR_OOM when the budget, the slots or the
+ * tile capacity would be exceeded. */
+int ensc_batch_add(ensc_batch* b, const ensc_mesh_desc* mesh, const ensc_material* mat, const ensc_params* controls,
+                   int32_t* slot);
+
+/* ensc_set_bcs for one instance. */
+int ensc_batch_set_bcs(ensc_batch* b, int32_t slot, const int8_t* dof_code, const double* dof_value);
+
+/* Lets the instance run up to max_cycles more cycles while its time is below
+ * step_end_time (ensc_step's limits), starting with the next run. */
+int ensc_batch_arm(ensc_batch* b, int32_t slot, int64_t max_cycles, double step_end_time);
+
+/* Enqueues `cycles` cycles of the whole batch (instances that are done skip
+ * them) on the batch's stream and returns without waiting. */
+int ensc_batch_run(ensc_batch* b, int64_t cycles);
+
+/* Waits for the batch's stream and refreshes every instance's report;
+ * *n_running (may be NULL) receives the number of armed instances not done. */
+int ensc_batch_sync(ensc_batch* b, int32_t* n_running);
+
+/* Report and energies of an instance as of the last ensc_batch_sync. */
+int ensc_batch_report(ensc_batch* b, int32_t slot, ensc_step_report* report);
+int ensc_batch_energy(ensc_batch* b, int32_t slot, ensc_energy_report* out);
+
+/* ensc_download for one instance (waits for the batch's stream). */
+int ensc_batch_download(ensc_batch* b, int32_t slot, double* x, double* u, double* v, double* sigma, double* qia,
+                        double* eps_p);
+
+/* Removes an instance; its memory returns to the batch's pool. */
+int ensc_batch_remove(ensc_batch* b, int32_t slot);
+
+/* Device bytes held by the batch's instances, and their number. */
+int64_t ensc_batch_device_bytes(const ensc_batch* b);
+int32_t ensc_batch_instances(const ensc_batch* b);
+
+void ensc_batch_destroy(ensc_batch* b);
+
+/* Message of the last error on b (NULL: as ensc_last_error(NULL)). */
+const char* ensc_batch_last_error(const ensc_batch* b);
+
 /* ---- stepping without device allocation --------------------------------
  * No counterpart in the reference: the reference stepper never allocates on
  * a GPU.  For callers that cannot call cudaMalloc -- code running inside a
