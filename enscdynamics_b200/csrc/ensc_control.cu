@@ -266,7 +266,8 @@ __global__ void k_aos_to_soa(const double* aos, int64_t n, int64_t pad, int comp
 
 // ---- batched instances: one block per instance slot ------------------------
 // Folds the instance's tile partials of the last cycle in tile order and, in
-// mode 0, begins its next cycle exactly as k_between does for one instance.
+// mode 0, begins its next cycle exactly as k_between does for one instance;
+// mode 1 folds and marks instances that have reached their limits as done.
 __global__ void __launch_bounds__(kCtlThreads) k_between_batch(BatchTables T, int mode) {
     const int slot = blockIdx.x;
     if (slot >= T.counts[2]) return;
@@ -288,12 +289,14 @@ __global__ void __launch_bounds__(kCtlThreads) k_between_batch(BatchTables T, in
             ctl->energy_pending = 0;
         }
     }
-    if (mode != 0 || threadIdx.x != 0 || ctl->done) return;
+    if (threadIdx.x != 0 || ctl->done) return;
+    // an instance that has reached its limits is marked done here in both
+    // modes, so that a sync right after its last cycle reports it finished
     if (ctl->status || !(ctl->time < ctl->step_end) || ctl->cycles_done >= ctl->cycles_target) {
         ctl->done = 1;
         return;
     }
-    cycle_begin(ctl);
+    if (mode == 0) cycle_begin(ctl);
 }
 
 // Minimum element edge for the instances whose cycle may hit the total-time

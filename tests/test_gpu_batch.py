@@ -173,3 +173,16 @@ def test_budget_and_capacity_are_enforced():
             b.add(c.x0, c.conn, c.v0, material=c.mat, controls=c.ctl)
         assert e.value.code == -2
         assert b.device_bytes > 0
+
+
+def test_instance_reports_done_right_after_its_last_cycle():
+    """A run that ends exactly on an instance's last cycle leaves it
+    reported as finished by the next sync."""
+    c = sweep_case(17, 100)
+    with make_batch(capi.FP64, graph_chunk=10) as b:
+        s = add(b, c)
+        b.arm(s, 100)
+        b.run(100)
+        assert b.sync() == 0
+        rep = b.report(s)
+        assert rep["done"] == 1 and rep["cycles"] == 100

@@ -1,0 +1,78 @@
+"""The request loop's scheduling on a host-only backend with the batch's
+admission rules: every request completes, the byte budget and slot count
+are never exceeded, requests run concurrently and finished ones release
+their memory, and a request larger than the whole budget is rejected without
+stopping the others."""
+import numpy as np
+
+from enscdynamics_b200 import serving as S
+from enscdynamics_b200 import workloads as W
+
+
+class _Mesh:
+    def __init__(self, ne):
+        self.n_elements = ne
+
+
+class _Problem:
+    def __init__(self, ne, cycles):
+        self.mesh = _Mesh(ne)
+        self.cycles = cycles
+
+
+def stream(n, rate=50.0, seed=5):
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for i in range(n):
+        t += rng.exponential(1.0 / rate)
+        ne = int(np.exp(rng.uniform(np.log(1000), np.log(500000))))
+        out.append(W.Request(i, t, _Problem(ne, int(rng.integers(1000, 10001)))))
+    return out
+
+
+def run(reqs, **kw):
+    be = S.FakeBackend(**kw)
+    srv = S.Server(be, clock=be.now, sleep=be.sleep)
+    return be, srv.serve(reqs)
+
+
+def test_all_complete_within_budget_and_slots():
+    reqs = stream(200)
+    budget = 200_000 * 400 * 3   # about three large requests at a time
+    be, out = run(reqs, budget_bytes=budget, max_instances=16)
+    assert all(o.status == 0 and o.cycles == r.problem.cycles for o, r in zip(out, reqs))
+    assert be.peak <= budget and be.peak_instances <= 16
+    assert be.peak_instances > 1          # requests overlap on the device
+    assert be.used == 0 and not be.slots  # everything retired and freed
+    for o in out:
+        assert o.arrival <= o.admitted <= o.finished
+    s = S.summarize(out)
+    assert s["requests"] == 200 and s["failed"] == 0
+    assert s["p99_latency_s"] >= s["p50_latency_s"] > 0
+
+
+def test_backfill_admits_small_requests_past_a_blocked_large_one():
+    reqs = [W.Request(0, 0.0, _Problem(900, 5000)), W.Request(1, 0.001, _Problem(900, 100)),
+            W.Request(2, 0.002, _Problem(100, 100))]
+    be, out = run(reqs, budget_bytes=1000 * 400, max_instances=8)
+    # request 1 waits for request 0; request 2 fits beside request 0 and finishes first
+    assert out[2].admitted < out[1].admitted
+    assert out[2].finished < out[0].finished
+    assert out[1].admitted >= out[0].finished
+
+
+def test_oversized_request_is_rejected_and_others_finish():
+    reqs = [W.Request(0, 0.0, _Problem(10_000, 100)), W.Request(1, 0.5, _Problem(10, 100)),
+            W.Request(2, 0.6, _Problem(20, 200))]
+    be, out = run(reqs, budget_bytes=1000 * 400, max_instances=8)
+    assert out[0].status == S.ERR_OOM
+    assert out[1].status == 0 and out[2].status == 0 and out[2].cycles == 200
+
+
+def test_quantum_follows_the_earliest_finishing_instance():
+    reqs = [W.Request(0, 0.0, _Problem(100, 1000)), W.Request(1, 0.0, _Problem(100, 70))]
+    be, out = run(reqs, budget_bytes=10 ** 9, max_instances=8)
+    # the short request retires after one 70-cycle quantum, not after 1024
+    assert out[1].finished <= out[0].finished
+    assert be.cycles_run < 1000 + 64
