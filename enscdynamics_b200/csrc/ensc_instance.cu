@@ -1,6 +1,5 @@
 // Host-side preparation and device layout of one solver instance.
 #include "ensc_instance.h"
-#include "ensc_kernels.h"
 
 #include <cmath>
 #include <cstring>

@@ -99,8 +99,8 @@ __device__ __forceinline__ float tau_f(int k, int j) {
 // shared by the single-instance and batched kernels.
 template <bool PLASTIC, bool INIT>
 __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const NodeArrays& N, const Material& M,
-                                                   const float dt1, const double dt1d, const int64_t e, float& dts,
-                                                   float& len, double& e_int, double& e_hg, double& e_vis,
+                                                   const float dt1, const double dt1d, const int64_t e, double& dts,
+                                                   double& len, double& e_int, double& e_hg, double& e_vis,
                                                    int32_t& bad) {
     const int64_t ep = E.ne_pad, np = N.nn_pad;
     const uint32_t* __restrict__ conn = E.conn;
@@ -113,7 +113,11 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
     float* __restrict__ fe = static_cast<float*>(E.fe);
     const double* __restrict__ X = N.x;
     const float* __restrict__ V = static_cast<const float*>(N.v);
-    const float G = static_cast<float>(M.G), lam = static_cast<float>(M.lambda);
+    const float G = static_cast<float>(M.G);
+    const float lam_hi = static_cast<float>(M.lambda);
+    const float lam_lo = static_cast<float>(M.lambda - static_cast<double>(lam_hi));
+    const float g2_hi = static_cast<float>(2.0 * M.G);
+    const float g2_lo = static_cast<float>(2.0 * M.G - static_cast<double>(g2_hi));
     const float rho = static_cast<float>(M.rho), wos = static_cast<float>(M.wos);
     const float cvisl = static_cast<float>(M.cvisl), cvisq = static_cast<float>(M.cvisq);
     const float y0 = static_cast<float>(M.yield0), H = static_cast<float>(M.hardening);
@@ -134,9 +138,10 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
 #pragma unroll
         for (int k = 1; k < 8; ++k) {
             const uint32_t nk = __ldg(conn + k * ep + e);
-            xr[k][0] = static_cast<float>(X[nk] - x00);
-            xr[k][1] = static_cast<float>(X[np + nk] - x01);
-            xr[k][2] = static_cast<float>(X[2 * np + nk] - x02);
+            const double d0 = X[nk] - x00, d1 = X[np + nk] - x01, d2 = X[2 * np + nk] - x02;
+            xr[k][0] = static_cast<float>(d0);
+            xr[k][1] = static_cast<float>(d1);
+            xr[k][2] = static_cast<float>(d2);
         }
 #pragma unroll
         for (int k = 1; k < 8; ++k) {
@@ -199,22 +204,31 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
     }
     const float vr = L[0][0] + L[1][1] + L[2][2];
     // Jaumann stress update
-    float eps[6] = {L[0][0] * dt1, L[1][1] * dt1, L[2][2] * dt1, 0.5f * (L[0][1] + L[1][0]) * dt1,
-                    0.5f * (L[0][2] + L[2][0]) * dt1, 0.5f * (L[1][2] + L[2][1]) * dt1};
-    const float w0 = 0.5f * (L[0][1] - L[1][0]) * dt1;
-    const float w1 = 0.5f * (L[0][2] - L[2][0]) * dt1;
-    const float w2 = 0.5f * (L[1][2] - L[2][1]) * dt1;
-    const float tr = eps[0] + eps[1] + eps[2];
     float so[6], s[6];
 #pragma unroll
     for (int i = 0; i < 6; ++i) so[i] = sig[i * ep + e];
-    const float g2 = 2.f * G;
-    s[0] = so[0] + lam * tr + g2 * eps[0] + 2.f * so[3] * w0 + 2.f * so[4] * w1;
-    s[1] = so[1] + lam * tr + g2 * eps[1] - 2.f * so[3] * w0 + 2.f * so[5] * w2;
-    s[2] = so[2] + lam * tr + g2 * eps[2] - 2.f * so[4] * w1 - 2.f * so[5] * w2;
-    s[3] = so[3] + g2 * eps[3] + (so[1] - so[0]) * w0 + so[5] * w1;
-    s[4] = so[4] + g2 * eps[4] + (so[2] - so[0]) * w1 + so[5] * w0;
-    s[5] = so[5] + g2 * eps[5] + (so[2] - so[1]) * w2 + so[3] * w1 - so[4] * w0;
+    float eps[6] = {L[0][0] * dt1, L[1][1] * dt1, L[2][2] * dt1, 0.5f * (L[0][1] + L[1][0]) * dt1,
+                    0.5f * (L[0][2] + L[2][0]) * dt1, 0.5f * (L[1][2] + L[2][1]) * dt1};
+    {
+        const float w0 = 0.5f * (L[0][1] - L[1][0]) * dt1;
+        const float w1 = 0.5f * (L[0][2] - L[2][0]) * dt1;
+        const float w2 = 0.5f * (L[1][2] - L[2][1]) * dt1;
+        const float tr = eps[0] + eps[1] + eps[2];
+        // lambda and 2G enter as unevaluated pairs hi + lo of floats: a
+        // stiffness rounded to FP32 is off by up to 6e-8 for every element
+        // and cycle alike, which shifts all wave speeds and accumulates as
+        // phase error; the pair carries the FP64 constants to ~1e-15
+        const float lt = fmaf(lam_hi, tr, lam_lo * tr);
+        float ge[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) ge[i] = fmaf(g2_hi, eps[i], g2_lo * eps[i]);
+        s[0] = so[0] + lt + ge[0] + 2.f * so[3] * w0 + 2.f * so[4] * w1;
+        s[1] = so[1] + lt + ge[1] - 2.f * so[3] * w0 + 2.f * so[5] * w2;
+        s[2] = so[2] + lt + ge[2] - 2.f * so[4] * w1 - 2.f * so[5] * w2;
+        s[3] = so[3] + ge[3] + (so[1] - so[0]) * w0 + so[5] * w1;
+        s[4] = so[4] + ge[4] + (so[2] - so[0]) * w1 + so[5] * w0;
+        s[5] = so[5] + ge[5] + (so[2] - so[1]) * w2 + so[3] * w1 - so[4] * w0;
+    }
     if (PLASTIC) {
         const float pm = (s[0] + s[1] + s[2]) * (1.f / 3.f);
         const float d0 = s[0] - pm, d1 = s[1] - pm, d2 = s[2] - pm;
@@ -310,9 +324,12 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
         }
     }
     // element dt (compute_dtStable, exDyna3D.cpp:828-834)
-    const float m0 = fminf(vr, 0.f);
-    const float xi = cvisl - cvisq * cvisq * len / wos * m0;
-    dts = (sqrtf(1.f + xi * xi) - xi) * len / wos;
+    {
+        const float lf = static_cast<float>(len);
+        const float m0 = fminf(vr, 0.f);
+        const float xi = cvisl - cvisq * cvisq * lf / wos * m0;
+        dts = (sqrtf(1.f + xi * xi) - xi) * lf / wos;
+    }
     if (!isfinite(dts)) bad |= ST_NONFINITE;
 }
 
@@ -360,10 +377,10 @@ __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_MIXED)
                 }
             }
         }
-        float dts, len;
+        double dts, len;
         element_body_mixed<PLASTIC, INIT>(E, N, M, dt1, dt1d, e, dts, len, e_int, e_hg, e_vis, bad);
-        dts_min = fmin(dts_min, static_cast<double>(dts));
-        len_min = fmin(len_min, static_cast<double>(len));
+        dts_min = fmin(dts_min, dts);
+        len_min = fmin(len_min, len);
     }
     if (bad) atomicOr(&ctl->status, bad);
     block_min2_d<kElemThreads>(dts_min, len_min, &ctl->dts_next, &ctl->len_min);
@@ -467,11 +484,7 @@ __global__ void __launch_bounds__(kNodeThreads) k_node_mixed(ElemArrays E, NodeA
         ctl->cycles_done += 1;
         ctl->energy_pending = 1;
     }
-    const int64_t nn = N.nn, np = N.nn_pad, ep = E.ne_pad;
-    const float* __restrict__ fe = static_cast<const float*>(E.fe);
-    float* __restrict__ V = static_cast<float*>(N.v);
-    const float hdt = static_cast<float>(0.5 * (dt_i + dt_i_1));
-    const double dt_avg = 0.5 * (dt_i + dt_i_1);
+    const int64_t nn = N.nn;
     double kin = 0.0, wext = 0.0;
     int32_t bad = 0;
     const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
@@ -521,15 +534,15 @@ __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_MIXED) k_element_
         const double dt1d = ctl->dt_i_1;
         const float dt1 = static_cast<float>(dt1d);
         const int64_t e = static_cast<int64_t>(T.etile_base[t]) + lane;
-        float dts = FLT_MAX, len = FLT_MAX;
+        double dts = DBL_MAX, len = DBL_MAX;
         double ei = 0.0, eh = 0.0, ev = 0.0;
         int32_t bad = 0;
         if (e < d.E.ne) {
             if (d.M.plastic) element_body_mixed<true, false>(d.E, d.N, d.M, dt1, dt1d, e, dts, len, ei, eh, ev, bad);
             else element_body_mixed<false, false>(d.E, d.N, d.M, dt1, dt1d, e, dts, len, ei, eh, ev, bad);
         }
-        const unsigned long long dmin = warp_min_u64(ord_bits(static_cast<double>(dts)));
-        const unsigned long long lmin = warp_min_u64(ord_bits(static_cast<double>(len)));
+        const unsigned long long dmin = warp_min_u64(ord_bits(dts));
+        const unsigned long long lmin = warp_min_u64(ord_bits(len));
         ei = warp_sum_b(ei);
         eh = warp_sum_b(eh);
         ev = warp_sum_b(ev);
