@@ -80,6 +80,7 @@ SIGNATURES = [
                               C.POINTER(C.c_void_p)]),
     ("ensc_set_bcs", C.c_int, [C.c_void_p, C.POINTER(C.c_int8), _P]),
     ("ensc_set_gravity", C.c_int, [C.c_void_p, C.c_int32, C.c_double, _P]),
+    ("ensc_set_gravity_amplitude", C.c_int, [C.c_void_p, C.c_int32, _P]),
     ("ensc_step", C.c_int, [C.c_void_p, C.c_int64, C.c_double, C.POINTER(StepReport)]),
     ("ensc_step_async", C.c_int, [C.c_void_p, C.c_int64, C.c_double]),
     ("ensc_sync", C.c_int, [C.c_void_p, C.POINTER(StepReport)]),
@@ -100,6 +101,7 @@ SIGNATURES = [
     ("ensc_batch_add", C.c_int, [C.c_void_p, C.POINTER(MeshDesc), C.POINTER(MaterialDesc), C.POINTER(Params),
                                  C.POINTER(C.c_int32)]),
     ("ensc_batch_set_bcs", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int8), _P]),
+    ("ensc_batch_set_gravity_amplitude", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, _P]),
     ("ensc_batch_arm", C.c_int, [C.c_void_p, C.c_int32, C.c_int64, C.c_double]),
     ("ensc_batch_run", C.c_int, [C.c_void_p, C.c_int64]),
     ("ensc_batch_sync", C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
@@ -191,6 +193,8 @@ class Stepper:
         if rc != 0:
             raise EnscError(rc, lib.ensc_last_error(None).decode())
         self.precision = precision
+        if controls.gravity_amplitude:
+            self.set_gravity_amplitude(controls.gravity_amplitude)
 
     # -- helpers -------------------------------------------------------------
     def _check(self, rc: int) -> None:
@@ -224,6 +228,11 @@ class Stepper:
     def set_gravity(self, on: bool, value: float = 0.0, direction=(0.0, 0.0, 0.0)) -> None:
         d = np.ascontiguousarray(direction, dtype=np.float64)
         self._check(self._lib.ensc_set_gravity(self.h, int(on), float(value), _dp(d)))
+
+    def set_gravity_amplitude(self, points) -> None:
+        """(time, value) points of the gravity amplitude; empty removes it."""
+        a = np.ascontiguousarray(points if points is not None else [], dtype=np.float64).reshape(-1)
+        self._check(self._lib.ensc_set_gravity_amplitude(self.h, a.size // 2, _dp(a) if a.size else None))
 
     def step(self, max_cycles: int, step_end: float = math.inf) -> Dict[str, float]:
         r = StepReport()
@@ -336,7 +345,14 @@ class Batch:
         self._check(self._lib.ensc_batch_add(self.h, C.byref(m), C.byref(mt), C.byref(p), C.byref(slot)))
         del keep
         self.sizes[slot.value] = (int(x0.shape[0]), int(conn.shape[0]))
+        if controls.gravity_amplitude:
+            self.set_gravity_amplitude(slot.value, controls.gravity_amplitude)
         return slot.value
+
+    def set_gravity_amplitude(self, slot: int, points) -> None:
+        a = np.ascontiguousarray(points if points is not None else [], dtype=np.float64).reshape(-1)
+        self._check(self._lib.ensc_batch_set_gravity_amplitude(self.h, int(slot), a.size // 2,
+                                                               _dp(a) if a.size else None))
 
     def set_bcs(self, slot: int, code: Optional[np.ndarray], value: Optional[np.ndarray] = None) -> None:
         c = None if code is None else np.ascontiguousarray(code, dtype=np.int8)

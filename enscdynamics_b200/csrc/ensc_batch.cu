@@ -36,6 +36,7 @@ struct Slot {
     ensc::NodeArrays N{};
     ensc::Material M{};
     bool kinetic0_done = false;
+    double* amp = nullptr;  // gravity amplitude table (from the pool)
 };
 
 struct Tune {
@@ -440,6 +441,23 @@ int ensc_batch_set_bcs(ensc_batch* b, int32_t slot, const int8_t* dof_code, cons
     return ENSC_OK;
 }
 
+int ensc_batch_set_gravity_amplitude(ensc_batch* b, int32_t slot, int32_t n_points, const double* time_value) {
+    if (!b || slot < 0 || slot >= b->slots || !b->inst[slot].used) return berr(b, ENSC_ERR_ARG, "bad slot");
+    if (n_points < 0 || n_points > ENSC_MAX_AMPLITUDE_POINTS || (n_points > 0 && !time_value))
+        return berr(b, ENSC_ERR_ARG, "amplitude: 0 to ENSC_MAX_AMPLITUDE_POINTS (time, value) pairs");
+    DevGuard dg(b->device);
+    Slot& sl = b->inst[slot];
+    if (n_points > 0 && !sl.amp)
+        BCK(b, cudaMallocFromPoolAsync(reinterpret_cast<void**>(&sl.amp),
+                                       2 * sizeof(double) * ENSC_MAX_AMPLITUDE_POINTS, b->pool, b->stream));
+    if (n_points > 0)
+        BCK(b, cudaMemcpyAsync(sl.amp, time_value, 2 * sizeof(double) * n_points, cudaMemcpyHostToDevice,
+                               b->stream));
+    sl.M.amp = n_points > 0 ? sl.amp : nullptr;
+    sl.M.amp_n = n_points;
+    return rebuild_tables(b);  // the instance table carries the material by value
+}
+
 int ensc_batch_arm(ensc_batch* b, int32_t slot, int64_t max_cycles, double step_end_time) {
     if (!b || slot < 0 || slot >= b->slots || !b->inst[slot].used || max_cycles < 0)
         return berr(b, ENSC_ERR_ARG, "bad slot or cycle count");
@@ -556,6 +574,7 @@ int ensc_batch_remove(ensc_batch* b, int32_t slot) {
     BCK(b, cudaMemcpyAsync(b->d_ctl + slot, b->h_ctl + slot, sizeof(Ctl), cudaMemcpyHostToDevice, b->stream));
     sl.used = false;
     int rc = rebuild_tables(b);
+    if (sl.amp) BCK(b, cudaFreeAsync(sl.amp, b->stream));
     BCK(b, cudaFreeAsync(sl.block, b->stream));
     b->used -= static_cast<int64_t>(sl.bytes);
     sl = Slot{};
@@ -576,8 +595,10 @@ void ensc_batch_destroy(ensc_batch* b) {
     DevGuard dg(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
     if (b->graph) cudaGraphExecDestroy(b->graph);
-    for (Slot& s : b->inst)
+    for (Slot& s : b->inst) {
         if (s.block) cudaFreeAsync(s.block, b->stream);
+        if (s.amp) cudaFreeAsync(s.amp, b->stream);
+    }
     if (b->stream) cudaStreamSynchronize(b->stream);
     if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
     if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);

@@ -49,6 +49,7 @@ struct ensc_handle {
     int chunk = 32;
     cudaGraphExec_t graph = nullptr;
     bool kinetic0_done = false;
+    double* amp = nullptr;         // device gravity amplitude table
     std::string err;
 };
 
@@ -329,6 +330,31 @@ int ensc_set_gravity(ensc_handle* h, int32_t on, double value, const double dir[
     return build_graph(h);
 }
 
+int ensc_set_gravity_amplitude(ensc_handle* h, int32_t n_points, const double* time_value) {
+    if (!h) return ENSC_ERR_ARG;
+    if (n_points < 0 || n_points > ENSC_MAX_AMPLITUDE_POINTS || (n_points > 0 && !time_value))
+        return set_err(h, ENSC_ERR_ARG, "amplitude: 0 to ENSC_MAX_AMPLITUDE_POINTS (time, value) pairs");
+    DevGuard dg(h->device);
+    if (n_points == 0) {
+        h->M.amp = nullptr;
+        h->M.amp_n = 0;
+        return build_graph(h);
+    }
+    if (!h->amp) {
+        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&h->amp), 2 * sizeof(double) * ENSC_MAX_AMPLITUDE_POINTS);
+        if (e != cudaSuccess) {
+            h->amp = nullptr;
+            return cuda_err(h, "cudaMalloc(amplitude)", e);
+        }
+    }
+    // stream order: cycles already enqueued finish with the previous table
+    CK(h, cudaMemcpyAsync(h->amp, time_value, 2 * sizeof(double) * n_points, cudaMemcpyHostToDevice, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    h->M.amp = h->amp;
+    h->M.amp_n = n_points;
+    return build_graph(h);
+}
+
 int ensc_step_async(ensc_handle* h, int64_t max_cycles, double step_end_time) {
     if (!h || max_cycles < 0) return ENSC_ERR_ARG;
     if (max_cycles == 0) return ENSC_OK;
@@ -527,6 +553,7 @@ void ensc_destroy(ensc_handle* h) {
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
     if (h->staging_owned && h->staging) cudaFree(h->staging);
     if (h->arena) cudaFree(h->arena);
+    if (h->amp) cudaFree(h->amp);
     if (h->ctl_host) cudaFreeHost(h->ctl_host);
     delete h;
 }

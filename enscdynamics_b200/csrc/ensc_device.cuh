@@ -66,6 +66,9 @@ struct Material {
     int32_t plastic;
     int32_t gravity_on;
     double gravity_value, gravity_dir[3];
+    // gravity amplitude table: amp_n (time, value) pairs in device memory
+    const double* amp;
+    int32_t amp_n;
 };
 
 struct ElemArrays {
@@ -139,6 +142,52 @@ struct BatchTables {
     double* etile_part;          // [etiles][3] internal / hourglass / viscous work per tile
     double* ntile_part;          // [ntiles][2] kinetic / external work per tile
 };
+
+// Amplitude factor of gravity in a cycle at `time` with step dt, as
+// exDyna3D::deal_amp computes it (exDyna3D.cpp:1222-1278), behaviour kept as
+// is: the scan stops at the first segment that ends before `time` (factor
+// 1); a cycle inside one segment takes the segment's value at mid-cycle; a
+// cycle that crosses segment ends takes the mean of the curve over the cycle,
+// where the partial last segment's intercept uses the first segment's slope
+// (:1257) and time past the last point counts with value 1.  n < 2: 1.
+__host__ __device__ inline double gravity_amplitude(const double* amp, int n, double time, double dt) {
+    double y = 1.0;
+    for (int i = 0; i + 1 < n; ++i) {
+        const double x1 = amp[2 * i], y1 = amp[2 * i + 1];
+        const double x2 = amp[2 * i + 2], y2 = amp[2 * i + 3];
+        if (time > x2) break;
+        const double m = (y2 - y1) / (x2 - x1);
+        const double c = y1 - m * x1;
+        const double x = time + dt / 2.0;
+        if ((x + dt / 2.0) < x2) {
+            y = m * x + c;
+            break;
+        }
+        const double dt1 = x2 - time;
+        const double xm = time + dt1 / 2.0;
+        const double ym = m * xm + c;
+        const double a1 = ym * dt1;
+        double a2 = 0.0;
+        for (int j = 2; j + i < n; ++j) {
+            const double xj = amp[2 * (i + j)], yj = amp[2 * (i + j) + 1];
+            const double xp = amp[2 * (i + j - 1)], yp = amp[2 * (i + j - 1) + 1];
+            if ((x + dt / 2.0) > xj) {
+                a2 += (xj - xp) * (yj + yp) / 2.0;
+            } else {
+                const double mj = (yj - yp) / (xj - xp);
+                const double cj = yp - m * xp;
+                const double yend = mj * (x + dt / 2.0) + cj;
+                a2 += (x + dt / 2.0 - xp) * (yp + yend) / 2.0;
+                break;
+            }
+        }
+        const double x_end = amp[2 * (n - 1)];
+        if (x + dt / 2.0 > x_end) a2 += (x + dt / 2.0 - x_end) * 1.0;
+        y = (a1 + a2) / dt;
+        break;
+    }
+    return y;
+}
 
 // Positive doubles order like their bit patterns; min-reductions over
 // element dt / edge lengths use integer atomicMin on the bits, which is

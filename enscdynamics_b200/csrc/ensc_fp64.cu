@@ -432,7 +432,7 @@ __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_FP64) k_element(E
 // One node of the node pass (see the kernel comment below); shared by the
 // single-instance and batched kernels.
 __device__ __forceinline__ void node_body(const ElemArrays& E, const NodeArrays& N, const Material& M,
-                                          const double dt_i, const double dt_i_1, const int64_t n, double& kin,
+                                          const double dt_i, const double dt_i_1, const double amp, const int64_t n, double& kin,
                                           double& wext, int32_t& bad) {
     const int64_t np = N.nn_pad, ep = E.ne_pad;
     const double* __restrict__ fe = static_cast<const double*>(E.fe);
@@ -500,7 +500,7 @@ __device__ __forceinline__ void node_body(const ElemArrays& E, const NodeArrays&
         double a = f[c];
         double g = 0.0;
         if (M.gravity_on) {
-            g = 1.0 * M.gravity_value * M.gravity_dir[c] / im;
+            g = amp * M.gravity_value * M.gravity_dir[c] / im;  // apply_gravity (:809-824)
             a = a + g;
         }
         const uint32_t cc = (code >> (2 * c)) & 3u;
@@ -553,6 +553,7 @@ __global__ void __launch_bounds__(kNodeThreads) k_node(ElemArrays E, NodeArrays 
         ctl->energy_pending = 1;
     }
     const int64_t nn = N.nn, np = N.nn_pad, ep = E.ne_pad;
+    const double amp = (M.gravity_on && M.amp_n > 0) ? gravity_amplitude(M.amp, M.amp_n, ctl->time, dt_i) : 1.0;
     const double* __restrict__ fe = static_cast<const double*>(E.fe);
     double* __restrict__ V = static_cast<double*>(N.v);
     const double half = (dt_i + dt_i_1);
@@ -561,7 +562,7 @@ __global__ void __launch_bounds__(kNodeThreads) k_node(ElemArrays E, NodeArrays 
     int32_t bad = 0;
     const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
     for (int64_t n = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; n < nn; n += stride) {
-        node_body(E, N, M, dt_i, dt_i_1, n, kin, wext, bad);
+        node_body(E, N, M, dt_i, dt_i_1, amp, n, kin, wext, bad);
     }
     if (bad) atomicOr(&ctl->status, bad);
     double v2[2] = {kin, wext};
@@ -663,9 +664,11 @@ __global__ void __launch_bounds__(kNodeThreads) k_node_batch_fp64(BatchTables T)
             ctl->energy_pending = 1;
         }
         const int64_t n = static_cast<int64_t>(T.ntile_base[t]) + lane;
+        const double amp =
+            (d.M.gravity_on && d.M.amp_n > 0) ? gravity_amplitude(d.M.amp, d.M.amp_n, ctl->time, dt_i) : 1.0;
         double kin = 0.0, wext = 0.0;
         int32_t bad = 0;
-        if (n < d.N.nn) node_body(d.E, d.N, d.M, dt_i, dt_i_1, n, kin, wext, bad);
+        if (n < d.N.nn) node_body(d.E, d.N, d.M, dt_i, dt_i_1, amp, n, kin, wext, bad);
         kin = warp_sum_b(kin);
         wext = warp_sum_b(wext);
         bad = static_cast<int32_t>(__reduce_or_sync(0xffffffffu, static_cast<unsigned>(bad)));

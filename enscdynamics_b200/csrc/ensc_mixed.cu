@@ -393,7 +393,7 @@ __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_MIXED)
 // One node of the mixed node pass; shared by the single-instance and
 // batched kernels.
 __device__ __forceinline__ void node_body_mixed(const ElemArrays& E, const NodeArrays& N, const Material& M,
-                                                const double dt_i, const double dt_i_1, const int64_t n,
+                                                const double dt_i, const double dt_i_1, const double amp, const int64_t n,
                                                 double& kin, double& wext, int32_t& bad) {
     const int64_t np = N.nn_pad, ep = E.ne_pad;
     const float* __restrict__ fe = static_cast<const float*>(E.fe);
@@ -437,7 +437,7 @@ __device__ __forceinline__ void node_body_mixed(const ElemArrays& E, const NodeA
         float a = f[c];
         float g = 0.f;
         if (M.gravity_on) {
-            g = static_cast<float>(M.gravity_value * M.gravity_dir[c] / im);
+            g = static_cast<float>(amp * M.gravity_value * M.gravity_dir[c] / im);
             a += g;
         }
         const uint32_t cc = (code >> (2 * c)) & 3u;
@@ -485,11 +485,12 @@ __global__ void __launch_bounds__(kNodeThreads) k_node_mixed(ElemArrays E, NodeA
         ctl->energy_pending = 1;
     }
     const int64_t nn = N.nn;
+    const double amp = (M.gravity_on && M.amp_n > 0) ? gravity_amplitude(M.amp, M.amp_n, ctl->time, dt_i) : 1.0;
     double kin = 0.0, wext = 0.0;
     int32_t bad = 0;
     const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
     for (int64_t n = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; n < nn; n += stride) {
-        node_body_mixed(E, N, M, dt_i, dt_i_1, n, kin, wext, bad);
+        node_body_mixed(E, N, M, dt_i, dt_i_1, amp, n, kin, wext, bad);
     }
     if (bad) atomicOr(&ctl->status, bad);
     double v2[2] = {kin, wext};
@@ -592,9 +593,11 @@ __global__ void __launch_bounds__(kNodeThreads) k_node_batch_mixed(BatchTables T
             ctl->energy_pending = 1;
         }
         const int64_t n = static_cast<int64_t>(T.ntile_base[t]) + lane;
+        const double amp =
+            (d.M.gravity_on && d.M.amp_n > 0) ? gravity_amplitude(d.M.amp, d.M.amp_n, ctl->time, dt_i) : 1.0;
         double kin = 0.0, wext = 0.0;
         int32_t bad = 0;
-        if (n < d.N.nn) node_body_mixed(d.E, d.N, d.M, dt_i, dt_i_1, n, kin, wext, bad);
+        if (n < d.N.nn) node_body_mixed(d.E, d.N, d.M, dt_i, dt_i_1, amp, n, kin, wext, bad);
         kin = warp_sum_b(kin);
         wext = warp_sum_b(wext);
         bad = static_cast<int32_t>(__reduce_or_sync(0xffffffffu, static_cast<unsigned>(bad)));

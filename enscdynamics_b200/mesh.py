@@ -86,6 +86,8 @@ class Controls:
     cvisq: float = 1.2
     total_time: float = 1.0
     gravity: Optional[Tuple[float, Tuple[float, float, float]]] = None  # (value, dir)
+    # gravity amplitude: (time, value) points of the *Amplitude the *Dload names
+    gravity_amplitude: Optional[Sequence[Tuple[float, float]]] = None
 
 
 def box_mesh(nx: int, ny: int, nz: int, lx: float, ly: float, lz: float,
@@ -255,7 +257,8 @@ def write_deck(path: str, mesh: Mesh, material: Material, *, period: float,
                initial_velocity: Sequence[Tuple[str, int, float]] = (),
                node_velocities: Optional[np.ndarray] = None,
                bulk_viscosity: Tuple[float, float] = (0.06, 1.2),
-               gravity: Optional[Tuple[float, Tuple[float, float, float]]] = None) -> None:
+               gravity: Optional[Tuple[float, Tuple[float, float, float]]] = None,
+               amplitude: Optional[Sequence[Tuple[float, float]]] = None) -> None:
     """Writes an ``.inp`` deck of the model for the reference reader.
 
     ``fixed_sets``: (set name, spec) with spec e.g. ``"PINNED"`` or ``"3, 3"``.
@@ -264,6 +267,9 @@ def write_deck(path: str, mesh: Mesh, material: Material, *, period: float,
     initial-condition lines (node id, dof, value); zeros are skipped.
     Sets referenced must be present in ``mesh.node_sets`` (names contain
     ``Set-``).
+    ``amplitude``: (time, value) points of the gravity load's amplitude,
+    written on one line because DataIn::AMP keeps only the last data line of
+    an *Amplitude block (dataIn.cpp:1249-1268).
     """
     with open(path, "w") as f:
         f.write("*Heading\n** generated by enscdynamics_b200.mesh\n")
@@ -291,12 +297,16 @@ def write_deck(path: str, mesh: Mesh, material: Material, *, period: float,
                         val = node_velocities[i, d]
                         if val != 0.0:
                             f.write(f"{i + 1}, {d + 1}, {_fmt(val)}\n")
+        if amplitude:
+            f.write("*Amplitude, name=Amp-1\n")
+            f.write(", ".join(f"{_fmt(t)}, {_fmt(a)}" for t, a in amplitude) + "\n")
         f.write("*Step, name=Step-1, nlgeom=YES\n*Dynamic, Explicit\n")
         f.write(f", {_fmt(period)}\n")
         f.write(f"*Bulk Viscosity\n{_fmt(bulk_viscosity[0])}, {_fmt(bulk_viscosity[1])}\n")
         if gravity is not None:
             g, d = gravity
-            f.write(f"*Dload\n, GRAV, {_fmt(g)}, {_fmt(d[0])}, {_fmt(d[1])}, {_fmt(d[2])}\n")
+            f.write("*Dload, amplitude=Amp-1\n" if amplitude else "*Dload\n")
+            f.write(f", GRAV, {_fmt(g)}, {_fmt(d[0])}, {_fmt(d[1])}, {_fmt(d[2])}\n")
         f.write("*End Step\n")
 
 

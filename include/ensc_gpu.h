@@ -86,7 +86,8 @@ typedef struct {
 
 /* Solver controls: exDyna3D members c_dr, c_cr, factor_timeStep, Cvisl,
  * Cvisq, totalTime (exDyna3D.h:176-185) and the current step's gravity
- * (StepData::gravity, StepData.h:22; amplitude 1). */
+ * (StepData::gravity, StepData.h:22; its amplitude is set with
+ * ensc_set_gravity_amplitude). */
 typedef struct {
     double c_dr, c_cr, factor_timestep, cvisl, cvisq;
     double total_time;
@@ -139,6 +140,14 @@ int ensc_set_bcs(ensc_handle* h, const int8_t* dof_code, const double* dof_value
 /* Changes the gravity load of the current step (apply_gravity,
  * exDyna3D.cpp:800-826). */
 int ensc_set_gravity(ensc_handle* h, int32_t on, double value, const double dir[3]);
+
+/* Gravity amplitude of the current step (the *Amplitude named by the step's
+ * *Dload, map_amp_list / deal_amp, exDyna3D.cpp:809-813, 1222-1278): n_points
+ * (time, value) pairs interleaved in time_value; each cycle scales gravity by
+ * the factor deal_amp gives for the cycle's time and dt.  n_points = 0
+ * removes the amplitude (factor 1). */
+#define ENSC_MAX_AMPLITUDE_POINTS 4096
+int ensc_set_gravity_amplitude(ensc_handle* h, int32_t n_points, const double* time_value);
 
 /* Runs the body of run()'s step loop (exDyna3D.cpp:86-100) -- stable dt,
  * last-step clamp, computeSate -- while time < step_end_time, at most
@@ -218,6 +227,9 @@ int ensc_batch_add(ensc_batch* b, const ensc_mesh_desc* mesh, const ensc_materia
 
 /* ensc_set_bcs for one instance. */
 int ensc_batch_set_bcs(ensc_batch* b, int32_t slot, const int8_t* dof_code, const double* dof_value);
+
+/* ensc_set_gravity_amplitude for one instance. */
+int ensc_batch_set_gravity_amplitude(ensc_batch* b, int32_t slot, int32_t n_points, const double* time_value);
 
 /* Lets the instance run up to max_cycles more cycles while its time is below
  * step_end_time (ensc_step's limits), starting with the next run. */

@@ -44,6 +44,53 @@ void ensc_oracle_material_update(ensc_oracle_params* p) {
 
 /* Eigen 3.4 bruteforce 3x3 determinant: h(0,1,2) - h(1,0,2) + h(2,0,1),
  * h(a,b,c) = m(0,a) * (m(1,b)*m(2,c) - m(1,c)*m(2,b)). */
+double ensc_oracle_amplitude(const double* amp, int32_t n, double time, double dt) {
+    /* Restated from deal_amp with its behaviour kept as is: the scan stops at
+     * the first segment whose end lies before `time` (the factor is then 1),
+     * a cycle inside one segment takes the segment's value at mid-cycle,
+     * and a cycle that crosses segment ends takes the mean of the piecewise
+     * linear curve over [time, time + dt], where the partial last segment
+     * uses the first segment's slope in its intercept (exDyna3D.cpp:1257)
+     * and time beyond the last point counts with value 1 (:1266-1270).
+     * n < 2: factor 1. */
+    double y = 1.0;
+    for (int32_t i = 0; i + 1 < n; ++i) {
+        const double x1 = amp[2 * i], y1 = amp[2 * i + 1];
+        const double x2 = amp[2 * i + 2], y2 = amp[2 * i + 3];
+        if (time > x2) break;
+        const double m = (y2 - y1) / (x2 - x1);
+        const double c = y1 - m * x1;
+        const double x = time + dt / 2.0;
+        if ((x + dt / 2.0) < x2) {
+            y = m * x + c;
+            break;
+        }
+        const double dt1 = x2 - time;
+        const double xm = time + dt1 / 2.0;
+        const double ym = m * xm + c;
+        const double a1 = ym * dt1;
+        double a2 = 0.0;
+        for (int32_t j = 2; j + i < n; ++j) {
+            const double xj = amp[2 * (i + j)], yj = amp[2 * (i + j) + 1];
+            const double xp = amp[2 * (i + j - 1)], yp = amp[2 * (i + j - 1) + 1];
+            if ((x + dt / 2.0) > xj) {
+                a2 += (xj - xp) * (yj + yp) / 2.0;
+            } else {
+                const double mj = (yj - yp) / (xj - xp);
+                const double cj = yp - m * xp;
+                const double yend = mj * (x + dt / 2.0) + cj;
+                a2 += (x + dt / 2.0 - xp) * (yp + yend) / 2.0;
+                break;
+            }
+        }
+        const double x_end = amp[2 * (n - 1)];
+        if (x + dt / 2.0 > x_end) a2 += (x + dt / 2.0 - x_end) * 1.0;
+        y = (a1 + a2) / dt;
+        break;
+    }
+    return y;
+}
+
 static double det3(const double m[3][3]) {
     const double h0 = m[0][0] * (m[1][1] * m[2][2] - m[1][2] * m[2][1]);
     const double h1 = m[0][1] * (m[1][0] * m[2][2] - m[1][2] * m[2][0]);
@@ -419,11 +466,13 @@ int64_t ensc_oracle_cycles(const ensc_oracle_params* p, ensc_oracle_state* s, in
         s->energy[3] += de[2];
         const double dt_avg = (s->dt_i + s->dt_i_1) / 2.0;
         double wext = 0.0, kin = 0.0;
+        const double ampv = (p->gravity_on && p->amp_n > 0) ? ensc_oracle_amplitude(p->amp, p->amp_n, s->time, s->dt_i)
+                                                            : 1.0;
         for (int64_t i = 0; i < ndof; ++i) {
             double a = s->force[i];
             double g = 0.0;
-            if (p->gravity_on) { /* apply_gravity (:819-824), amplitude 1 */
-                g = 1.0 * p->gravity_value * p->gravity_dir[i % 3] / s->inv_mass[i];
+            if (p->gravity_on) { /* apply_gravity (:809-824) */
+                g = ampv * p->gravity_value * p->gravity_dir[i % 3] / s->inv_mass[i];
                 a += g;
             }
             /* apply_boundary_condition_a (:2029-2145) */

@@ -37,9 +37,13 @@ typedef struct {
     /* solver controls (exDyna3D.h:176-185, read_project_txt exDyna3D.cpp:698) */
     double c_dr, c_cr, factor, cvisl, cvisq;
     double total_time;
-    /* gravity (StepData::gravity, apply_gravity exDyna3D.cpp:800-826), amp = 1 */
+    /* gravity (StepData::gravity, apply_gravity exDyna3D.cpp:800-826) with
+     * an optional amplitude table (map_amp_list, read by DataIn::AMP
+     * dataIn.cpp:1244-1270): amp_n (time, value) pairs, none when amp_n = 0 */
     int32_t gravity_on;
     double gravity_value, gravity_dir[3];
+    int32_t amp_n;
+    const double* amp;
 } ensc_oracle_params;
 
 typedef struct {
@@ -71,6 +75,10 @@ typedef struct {
 } ensc_oracle_state;
 
 void ensc_oracle_material_update(ensc_oracle_params* p);
+
+/* exDyna3D::deal_amp (exDyna3D.cpp:1222-1278): the amplitude factor applied
+ * to gravity in a cycle at `time` with step dt, from n (time, value) pairs. */
+double ensc_oracle_amplitude(const double* amp, int32_t n, double time, double dt);
 
 /* compute_invMassMatrix (exDyna3D.cpp:492-515) with FEValues::reinit at the
  * single Gauss point (fevalues.h:232-265): B0^T, V0 and the inverse lumped

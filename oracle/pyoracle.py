@@ -36,7 +36,8 @@ class _Params(C.Structure):
                 ("yield0", C.c_double), ("hardening", C.c_double),
                 ("c_dr", C.c_double), ("c_cr", C.c_double), ("factor", C.c_double),
                 ("cvisl", C.c_double), ("cvisq", C.c_double), ("total_time", C.c_double),
-                ("gravity_on", C.c_int32), ("gravity_value", C.c_double), ("gravity_dir", C.c_double * 3)]
+                ("gravity_on", C.c_int32), ("gravity_value", C.c_double), ("gravity_dir", C.c_double * 3),
+                ("amp_n", C.c_int32), ("amp", C.POINTER(C.c_double))]
 
 
 _P = C.POINTER(C.c_double)
@@ -85,7 +86,7 @@ class Oracle:
 
     def __init__(self, x0, conn, v0, bc_code, bc_value, *, E, nu, rho, c_dr=0.013, c_cr=0.05,
                  factor=0.71, cvisl=0.06, cvisq=1.2, total_time=1.0, yield0=0.0, hardening=0.0,
-                 gravity=None, setup: Optional[Dict[str, np.ndarray]] = None):
+                 gravity=None, amplitude=None, setup: Optional[Dict[str, np.ndarray]] = None):
         lib = _load()
         self.nn = int(x0.shape[0])
         self.ne = int(conn.shape[0])
@@ -111,6 +112,10 @@ class Oracle:
             self.p.gravity_value = gravity[0]
             for i in range(3):
                 self.p.gravity_dir[i] = gravity[1][i]
+        if amplitude is not None and len(amplitude) > 0:
+            self.amp = np.ascontiguousarray(amplitude, dtype=np.float64).reshape(-1).copy()
+            self.p.amp_n = self.amp.size // 2
+            self.p.amp = _ptr(self.amp)
         lib.ensc_oracle_material_update(C.byref(self.p))
         self.bt = np.zeros(24 * ne)
         self.vol0 = np.zeros(ne)

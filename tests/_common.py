@@ -39,7 +39,8 @@ def material_controls(meta):
     g = meta.get("gravity")
     ctl = M.Controls(c_dr=meta["c_dr"], c_cr=meta["c_cr"], factor=meta["factor"], cvisl=meta["cvisl"],
                      cvisq=meta["cvisq"], total_time=meta["total_time"],
-                     gravity=None if g is None else (g[0], tuple(g[1])))
+                     gravity=None if g is None else (g[0], tuple(g[1])),
+                     gravity_amplitude=meta.get("amplitude"))
     return mat, ctl
 
 
@@ -53,7 +54,7 @@ def oracle_for(g, setup_from_reference=False, **overrides):
                            cvisl=meta["cvisl"], cvisq=meta["cvisq"], total_time=meta["total_time"],
                            yield0=meta.get("yield", 0.0), hardening=meta.get("hardening", 0.0),
                            gravity=None if meta.get("gravity") is None else (meta["gravity"][0], meta["gravity"][1]),
-                           setup=setup)
+                           amplitude=meta.get("amplitude"), setup=setup)
 
 
 def run_len(g):

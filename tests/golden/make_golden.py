@@ -62,6 +62,14 @@ def cases():
     # 5. slot clashes: elements with rotated local numbering so a node sits
     #    in the same local slot of two elements
     out.append(("slot_clash_2x2x1", clash_problem(), "cycles", 300))
+    # 6. gravity under an amplitude: a ramp over the first segment, a cycle
+    #    that crosses its end (the averaging branch of deal_amp) and factor 1
+    #    after it, as deal_amp gives
+    p = W.cantilever(6, 2, 2, 0.6, 0.2, 0.2, vz=0.5)
+    p.controls = M.Controls(total_time=1.0, gravity=(9.81e3, (0.0, 0.0, -1.0)),
+                            gravity_amplitude=[(0.0, 0.0), (3.0e-3, 1.0), (6.0e-3, 0.25), (1.0e-2, 0.8)],
+                            **W.DEFAULT_CONTROLS)
+    out.append(("gravity_amp_6x2x2", p, "cycles", 600))
     return out
 
 
@@ -109,7 +117,7 @@ def write_case_deck(p, d):
     per = p.end_time if p.end_time else p.controls.total_time
     M.write_deck(os.path.join(d, deck), p.mesh, p.material, period=per, fixed_sets=p.fixed_sets,
                  initial_velocity=p.initial_velocity, bulk_viscosity=(p.controls.cvisl, p.controls.cvisq),
-                 gravity=p.controls.gravity)
+                 gravity=p.controls.gravity, amplitude=p.controls.gravity_amplitude)
     vel = getattr(p, "velocity_sets", [])
     if vel:  # velocity conditions go inside the step: the reference does not
         # carry Initial-step velocity conditions into step 1 (exDyna3D.cpp:1859-1880)
@@ -121,10 +129,17 @@ def write_case_deck(p, d):
     return deck
 
 
-def main():
+def main(only=()):
+    """Regenerates every fixture, or only the named ones (index.json keeps the others)."""
     assert pyoracle.harness_available(), "build the reference harness first: make -C oracle"
     index = {}
+    ipath = os.path.join(HERE, "index.json")
+    if only and os.path.exists(ipath):
+        with open(ipath) as f:
+            index = json.load(f)
     for name, p, mode, cycles in cases():
+        if only and name not in only:
+            continue
         with tempfile.TemporaryDirectory() as d:
             deck = write_case_deck(p, d)
             pyoracle.run_reference(d, deck, "setup", dump=os.path.join(d, "s.bin"))
@@ -139,6 +154,7 @@ def main():
         meta = dict(E=p.material.E, nu=p.material.nu, rho=p.material.rho, c_dr=c.c_dr, c_cr=c.c_cr,
                     factor=c.factor, cvisl=c.cvisl, cvisq=c.cvisq, total_time=c.total_time,
                     gravity=c.gravity, mode=mode, cycles=int(r["cycles"]),
+                    amplitude=[list(t) for t in c.gravity_amplitude] if c.gravity_amplitude else None,
                     step_end=(p.end_time if mode == "full" else None))
         np.savez_compressed(os.path.join(HERE, name + ".npz"), x0=p.mesh.x0, conn=p.mesh.conn, v0=p.v0,
                             bc_code=p.bc_code, bc_value=p.bc_value, bt=s["bt"], vol0=s["vol0"],
@@ -153,4 +169,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(tuple(sys.argv[1:]))
