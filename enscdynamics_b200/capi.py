@@ -82,6 +82,7 @@ SIGNATURES = [
     ("ensc_set_gravity", C.c_int, [C.c_void_p, C.c_int32, C.c_double, _P]),
     ("ensc_set_gravity_amplitude", C.c_int, [C.c_void_p, C.c_int32, _P]),
     ("ensc_step", C.c_int, [C.c_void_p, C.c_int64, C.c_double, C.POINTER(StepReport)]),
+    ("ensc_step_until", C.c_int, [C.c_void_p, C.c_int64, C.c_double, C.c_double, C.POINTER(StepReport)]),
     ("ensc_step_async", C.c_int, [C.c_void_p, C.c_int64, C.c_double]),
     ("ensc_sync", C.c_int, [C.c_void_p, C.POINTER(StepReport)]),
     ("ensc_download", C.c_int, [C.c_void_p, _P, _P, _P, _P, _P, _P]),
@@ -237,6 +238,11 @@ class Stepper:
     def step(self, max_cycles: int, step_end: float = math.inf) -> Dict[str, float]:
         r = StepReport()
         self._check(self._lib.ensc_step(self.h, int(max_cycles), float(step_end), C.byref(r)))
+        return {k: getattr(r, k) for k, _ in StepReport._fields_}
+
+    def step_until(self, max_cycles: int, step_end: float, pause: float) -> Dict[str, float]:
+        r = StepReport()
+        self._check(self._lib.ensc_step_until(self.h, int(max_cycles), float(step_end), float(pause), C.byref(r)))
         return {k: getattr(r, k) for k, _ in StepReport._fields_}
 
     def step_async(self, max_cycles: int, step_end: float = math.inf) -> None:

@@ -379,11 +379,16 @@ int ensc_sync(ensc_handle* h, ensc_step_report* report) {
 }
 
 int ensc_step(ensc_handle* h, int64_t max_cycles, double step_end_time, ensc_step_report* report) {
+    return ensc_step_until(h, max_cycles, step_end_time, HUGE_VAL, report);
+}
+
+int ensc_step_until(ensc_handle* h, int64_t max_cycles, double step_end_time, double pause_time,
+                    ensc_step_report* report) {
     if (!h || max_cycles < 0) return ENSC_ERR_ARG;
     DevGuard dg(h->device);
     const int64_t before = h->ctl_host->cycles_done;
     if (max_cycles > 0) {
-        ensc::launch_arm(h->ctl, step_end_time, max_cycles, h->stream);
+        ensc::launch_arm(h->ctl, step_end_time, max_cycles, h->stream, pause_time);
         // launch graphs in batches; between batches read the control block
         // to stop once time reached step_end
         const int64_t batch = std::max<int64_t>(1, 4096 / h->chunk);

@@ -105,7 +105,8 @@ __global__ void __launch_bounds__(kCtlThreads) k_between(Ctl* ctl, Partials P, i
         }
     }
     if (mode != 0 || threadIdx.x != 0 || ctl->done) return;
-    if (ctl->status || !(ctl->time < ctl->step_end) || ctl->cycles_done >= ctl->cycles_target) {
+    if (ctl->status || !(ctl->time < ctl->step_end) || ctl->cycles_done >= ctl->cycles_target ||
+        !(ctl->time < ctl->pause_time)) {
         ctl->done = 1;
         return;
     }
@@ -189,8 +190,9 @@ __global__ void k_begin_exact(Ctl* ctl) {
     begin_exact(ctl);
 }
 
-__global__ void k_arm(Ctl* ctl, double step_end, long long max_cycles) {
+__global__ void k_arm(Ctl* ctl, double step_end, long long max_cycles, double pause) {
     ctl->step_end = step_end;
+    ctl->pause_time = pause;
     ctl->cycles_target = ctl->cycles_done + max_cycles;
     ctl->done = 0;
 }
@@ -292,7 +294,8 @@ __global__ void __launch_bounds__(kCtlThreads) k_between_batch(BatchTables T, in
     if (threadIdx.x != 0 || ctl->done) return;
     // an instance that has reached its limits is marked done here in both
     // modes, so that a sync right after its last cycle reports it finished
-    if (ctl->status || !(ctl->time < ctl->step_end) || ctl->cycles_done >= ctl->cycles_target) {
+    if (ctl->status || !(ctl->time < ctl->step_end) || ctl->cycles_done >= ctl->cycles_target ||
+        !(ctl->time < ctl->pause_time)) {
         ctl->done = 1;
         return;
     }
@@ -376,8 +379,8 @@ void launch_edge_prepass(const ElemArrays& E, const NodeArrays& N, Ctl* ctl, int
     k_edge_prepass<<<grid, 128, 0, st>>>(E, N, ctl);
 }
 void launch_begin_exact(Ctl* ctl, cudaStream_t st) { k_begin_exact<<<1, 32, 0, st>>>(ctl); }
-void launch_arm(Ctl* ctl, double step_end, long long max_cycles, cudaStream_t st) {
-    k_arm<<<1, 1, 0, st>>>(ctl, step_end, max_cycles);
+void launch_arm(Ctl* ctl, double step_end, long long max_cycles, cudaStream_t st, double pause) {
+    k_arm<<<1, 1, 0, st>>>(ctl, step_end, max_cycles, pause);
 }
 void launch_reset_init(Ctl* ctl, cudaStream_t st) { k_reset_init<<<1, 1, 0, st>>>(ctl); }
 void launch_apply_bc_v(const NodeArrays& N, bool fp32_v, cudaStream_t st) {

@@ -45,6 +45,7 @@ struct Ctl {
     double time, dt_i, dt_i_1;
     double dt_prev;            // dt_i at the start of the cycle
     double step_end, total_time;
+    double pause_time;         // stop after the cycle in which time reaches it (no dt clamp)
     double factor, wos;
     double dts_cur;            // min element dt of the previous force pass
     unsigned long long dts_next;   // ordered bits of min element dt, this pass

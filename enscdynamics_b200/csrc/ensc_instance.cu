@@ -312,6 +312,7 @@ Ctl initial_ctl(const ensc_params* p, const Material& M) {
     c.dt_i = 0.0;
     c.dt_i_1 = 0.0;
     c.step_end = HUGE_VAL;
+    c.pause_time = HUGE_VAL;
     c.total_time = p->total_time;
     c.factor = p->factor_timestep;
     c.wos = M.wos;

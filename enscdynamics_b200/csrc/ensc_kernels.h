@@ -69,7 +69,9 @@ void launch_begin_exact_batch(const BatchTables& T, int slots, cudaStream_t st);
 void launch_between(Ctl* ctl, const Partials& P, int mode, cudaStream_t st);
 void launch_edge_prepass(const ElemArrays& E, const NodeArrays& N, Ctl* ctl, int grid, cudaStream_t st);
 void launch_begin_exact(Ctl* ctl, cudaStream_t st);
-void launch_arm(Ctl* ctl, double step_end, long long max_cycles, cudaStream_t st);
+// pause: the instance stops after the cycle in which its time reaches pause
+// (dt is not clamped to it)
+void launch_arm(Ctl* ctl, double step_end, long long max_cycles, cudaStream_t st, double pause = HUGE_VAL);
 void launch_apply_bc_v(const NodeArrays& N, bool fp32_v, cudaStream_t st);
 void launch_reset_init(Ctl* ctl, cudaStream_t st);
 void launch_kinetic0(const NodeArrays& N, const Partials& P, Ctl* ctl, bool fp32_v, int grid, cudaStream_t st);

@@ -170,6 +170,7 @@ int ensc_step_noalloc(const ensc_device_model* m, const ensc_material* mat, cons
     c.dt_i = clk->dt_i;
     c.dt_i_1 = clk->dt_i_1;
     c.step_end = step_end_time;
+    c.pause_time = HUGE_VAL;
     c.total_time = params->total_time;
     c.factor = params->factor_timestep;
     c.wos = M.wos;

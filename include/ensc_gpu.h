@@ -154,6 +154,15 @@ int ensc_set_gravity_amplitude(ensc_handle* h, int32_t n_points, const double* t
  * max_cycles cycles.  Blocks until done; report may be NULL. */
 int ensc_step(ensc_handle* h, int64_t max_cycles, double step_end_time, ensc_step_report* report);
 
+/* ensc_step that also stops after the cycle in which time first reaches
+ * pause_time, without shortening any dt: the reference writes results from
+ * inside the cycle in which time reaches the next output time
+ * (output_results, exDyna3D.cpp:207-219, called from computeSate :788), so
+ * a caller that writes output pauses there and continues with the same
+ * trajectory. */
+int ensc_step_until(ensc_handle* h, int64_t max_cycles, double step_end_time, double pause_time,
+                    ensc_step_report* report);
+
 /* Enqueues the same work without waiting (for callers that time the stream
  * themselves); finish with ensc_sync. */
 int ensc_step_async(ensc_handle* h, int64_t max_cycles, double step_end_time);

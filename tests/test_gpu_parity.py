@@ -175,3 +175,28 @@ def test_errors_are_reported_not_fatal():
             s.step(-1)
         rep = s.step(10)
         assert rep["cycles"] == 10 and rep["status"] == 0
+
+
+def test_pause_at_output_times_keeps_the_trajectory():
+    """ensc_step_until stops after the cycle in which time reaches the pause
+    time without shortening dt, so a run paused for output ends bit-identical
+    to an uninterrupted one."""
+    g = load_golden("cantilever_20x4x4")
+    n = g["meta"]["cycles"]
+    with stepper_for(g) as s:
+        full = s.step(n)
+        ref = s.download()
+    t_end = full["time"]
+    done = 0
+    with stepper_for(g) as s:
+        for frac in (0.1, 0.37, 0.8):
+            pause = frac * t_end
+            r = s.step_until(n - done, math.inf, pause)
+            done += r["cycles"]
+            assert r["time"] >= pause and r["time"] - r["dt_i_1"] < pause, (r, pause)
+        r = s.step(n - done)
+        assert done + r["cycles"] == n
+        st = s.download()
+    for k in ("x", "u", "v", "sigma", "qia"):
+        assert np.array_equal(st[k], ref[k]), k
+    assert r["time"] == full["time"]
