@@ -208,7 +208,8 @@ int ensc_create(const ensc_mesh_desc* mesh, const ensc_material* mat, const ensc
     const int occ_e = std::max(1, mx ? ensc::occupancy_element_mixed(h->plastic) : ensc::occupancy_element_fp64(h->plastic));
     const int occ_n = std::max(1, mx ? ensc::occupancy_node_mixed() : ensc::occupancy_node_fp64());
     const int64_t ge = (h->ne + ensc::kElemThreads - 1) / ensc::kElemThreads;
-    const int64_t gn = (h->nn + ensc::kNodeThreads - 1) / ensc::kNodeThreads;
+    const int64_t node_threads = static_cast<int64_t>(ensc::kNodeThreads) * ensc::node_group_width(mx);
+    const int64_t gn = (h->nn + node_threads - 1) / node_threads;
     h->grid_e = static_cast<int>(std::min<int64_t>(ge, static_cast<int64_t>(occ_e) * prop.multiProcessorCount));
     h->grid_n = static_cast<int>(std::min<int64_t>(gn, static_cast<int64_t>(occ_n) * prop.multiProcessorCount));
 

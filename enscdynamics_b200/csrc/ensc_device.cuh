@@ -25,6 +25,8 @@
 //                                    same slot in more than one element
 #pragma once
 
+#include <cstring>
+
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -188,6 +190,36 @@ __host__ __device__ inline double gravity_amplitude(const double* amp, int n, do
         break;
     }
     return y;
+}
+
+// 16-byte vector access to W consecutive entries of a padded SoA row (rows
+// start 256-byte aligned, the row stride is a multiple of 32 entries and the
+// first index a multiple of W, so every chunk is 16-byte aligned).
+template <int W, typename T>
+__device__ __forceinline__ void ld_row(const T* p, T (&o)[W]) {
+    static_assert((W * sizeof(T)) % 16 == 0, "whole 16-byte chunks");
+#pragma unroll
+    for (int i = 0; i < static_cast<int>(W * sizeof(T) / 16); ++i) {
+        const uint4 q = reinterpret_cast<const uint4*>(p)[i];
+        memcpy(reinterpret_cast<char*>(o) + 16 * i, &q, 16);
+    }
+}
+template <int W, typename T>
+__device__ __forceinline__ void st_row(T* p, const T (&v)[W]) {
+    static_assert((W * sizeof(T)) % 16 == 0, "whole 16-byte chunks");
+#pragma unroll
+    for (int i = 0; i < static_cast<int>(W * sizeof(T) / 16); ++i) {
+        uint4 q;
+        memcpy(&q, reinterpret_cast<const char*>(v) + 16 * i, 16);
+        reinterpret_cast<uint4*>(p)[i] = q;
+    }
+}
+// W (2 or 4) consecutive bytes as one word, byte j of node j in bits 8j..8j+7.
+template <int W>
+__device__ __forceinline__ uint32_t ld_bytes(const uint8_t* p) {
+    static_assert(W == 2 || W == 4, "2 or 4 bytes");
+    if (W == 4) return *reinterpret_cast<const uint32_t*>(p);
+    return *reinterpret_cast<const uint16_t*>(p);
 }
 
 // Positive doubles order like their bit patterns; min-reductions over

@@ -528,6 +528,90 @@ __device__ __forceinline__ void node_body(const ElemArrays& E, const NodeArrays&
     }
 }
 
+// W consecutive nodes of the node pass with 16-byte row accesses: the same
+// arithmetic per node as node_body on the slot-major layout, in the same
+// order.  Nodes at or past nn (row padding) are loaded and stored back
+// unchanged.
+
+template <int W>
+__device__ __forceinline__ void node_group(const ElemArrays& E, const NodeArrays& N, const Material& M,
+                                           const double dt_i, const double dt_i_1, const double amp, const int64_t n0,
+                                           const int64_t nn, double& kin, double& wext, int32_t& bad) {
+    const int64_t np = N.nn_pad;
+    const double* __restrict__ fe = static_cast<const double*>(E.fe);
+    double* __restrict__ V = static_cast<double*>(N.v);
+    const double half = (dt_i + dt_i_1);
+    const double dt_avg = (dt_i + dt_i_1) / 2.0;
+    const uint32_t msk = ld_bytes<W>(N.slot_mask + n0);
+    double f[3][W];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int j = 0; j < W; ++j) f[c][j] = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        uint32_t sel = 0;
+#pragma unroll
+        for (int j = 0; j < W; ++j) sel |= ((msk >> (8 * j + k)) & 1u) << j;
+        if (sel) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                double r[W];
+                ld_row<W>(fe + (3 * k + c) * np + n0, r);
+#pragma unroll
+                for (int j = 0; j < W; ++j)
+                    if ((sel >> j) & 1u) f[c][j] = f[c][j] + r[j];
+            }
+        }
+    }
+    double im[W];
+    ld_row<W>(N.inv_mass + n0, im);
+    const uint32_t code = ld_bytes<W>(N.bc + n0);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        double vo[W], uo[W], xo[W], vn[W], un[W], xn[W];
+        ld_row<W>(V + c * np + n0, vo);
+        ld_row<W>(N.u + c * np + n0, uo);
+        ld_row<W>(N.x + c * np + n0, xo);
+#pragma unroll
+        for (int j = 0; j < W; ++j) {
+            vn[j] = vo[j];
+            un[j] = uo[j];
+            xn[j] = xo[j];
+            if (n0 + j >= nn) continue;
+            double a = f[c][j];
+            double g = 0.0;
+            if (M.gravity_on) {
+                g = amp * M.gravity_value * M.gravity_dir[c] / im[j];
+                a = a + g;
+            }
+            const uint32_t cc = (code >> (8 * j + 2 * c)) & 3u;
+            double r = 0.0, rf = 0.0;
+            if (cc & 2u) {
+                r = -a;
+                a = 0.0;
+            }
+            if ((cc & 1u) && a != 0.0) {
+                rf = -a;
+                r = -a;
+                a = 0.0;
+            }
+            if (cc) N.rf[c * np + n0 + j] = rf;
+            a = a * im[j];
+            vn[j] = vo[j] + half * a / 2.0;
+            un[j] = uo[j] + dt_i * vn[j];
+            xn[j] = xo[j] + dt_i * vn[j];
+            const double vb = 0.5 * (vo[j] + vn[j]);
+            wext = wext + (g + r) * dt_avg * vb;
+            kin = kin + 0.5 * (vn[j] * vn[j]) / im[j];
+            if (!isfinite(vn[j])) bad |= ST_NONFINITE;
+        }
+        st_row<W>(V + c * np + n0, vn);
+        st_row<W>(N.u + c * np + n0, un);
+        st_row<W>(N.x + c * np + n0, xn);
+    }
+}
+
 // Node pass: gather of the element forces in slot order (the reference's
 // ((((((a0+a1)+a2)+a3)+a4)+a5)+a6)+a7, exDyna3D.cpp:638-639), gravity
 // (:819-824), boundary conditions on a (:2029-2145), a = f M^-1 (:642-644),
@@ -552,17 +636,17 @@ __global__ void __launch_bounds__(kNodeThreads) k_node(ElemArrays E, NodeArrays 
         ctl->cycles_done += 1;
         ctl->energy_pending = 1;
     }
-    const int64_t nn = N.nn, np = N.nn_pad, ep = E.ne_pad;
+    const int64_t nn = N.nn;
     const double amp = (M.gravity_on && M.amp_n > 0) ? gravity_amplitude(M.amp, M.amp_n, ctl->time, dt_i) : 1.0;
-    const double* __restrict__ fe = static_cast<const double*>(E.fe);
-    double* __restrict__ V = static_cast<double*>(N.v);
-    const double half = (dt_i + dt_i_1);
-    const double dt_avg = (dt_i + dt_i_1) / 2.0;
     double kin = 0.0, wext = 0.0;
     int32_t bad = 0;
     const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-    for (int64_t n = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; n < nn; n += stride) {
-        node_body(E, N, M, dt_i, dt_i_1, amp, n, kin, wext, bad);
+    const int64_t t0 = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (E.slot_major && E.tiles_aligned) {
+        constexpr int W = kNodeGroupFp64;
+        for (int64_t g = t0; g * W < nn; g += stride) node_group<W>(E, N, M, dt_i, dt_i_1, amp, g * W, nn, kin, wext, bad);
+    } else {
+        for (int64_t n = t0; n < nn; n += stride) node_body(E, N, M, dt_i, dt_i_1, amp, n, kin, wext, bad);
     }
     if (bad) atomicOr(&ctl->status, bad);
     double v2[2] = {kin, wext};
@@ -704,6 +788,8 @@ int occupancy_element_fp64(bool plastic) {
     else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element<false, false>, kElemThreads, 0);
     return nb;
 }
+
+int node_group_width(bool mixed_precision) { return mixed_precision ? kNodeGroupMixed : kNodeGroupFp64; }
 
 int occupancy_node_fp64() {
     int nb = 0;

@@ -41,6 +41,10 @@ void launch_element_fp64(const ElemArrays& E, const NodeArrays& N, const Materia
 void launch_node_fp64(const ElemArrays& E, const NodeArrays& N, const Material& M, Ctl* ctl, const Partials& P,
                       int grid, cudaStream_t st);
 int occupancy_element_fp64(bool plastic);
+// nodes per thread of the node pass on the padded slot-major layout
+constexpr int kNodeGroupFp64 = 2;
+constexpr int kNodeGroupMixed = 4;
+int node_group_width(bool mixed_precision);
 int occupancy_node_fp64();
 
 // mixed precision (ensc_mixed.cu)

@@ -464,6 +464,90 @@ __device__ __forceinline__ void node_body_mixed(const ElemArrays& E, const NodeA
     }
 }
 
+// W consecutive nodes of the mixed node pass with 16-byte row accesses
+// (float4 force slots and velocities, pairs of doubles for x, u and the
+// inverse mass); per node the arithmetic of node_body_mixed.  Nodes at or
+// past nn (row padding) are loaded and stored back unchanged.
+template <int W>
+__device__ __forceinline__ void node_group_mixed(const ElemArrays& E, const NodeArrays& N, const Material& M,
+                                                 const double dt_i, const double dt_i_1, const double amp,
+                                                 const int64_t n0, const int64_t nn, double& kin, double& wext,
+                                                 int32_t& bad) {
+    const int64_t np = N.nn_pad;
+    const float* __restrict__ fe = static_cast<const float*>(E.fe);
+    float* __restrict__ V = static_cast<float*>(N.v);
+    const float hdt = static_cast<float>(0.5 * (dt_i + dt_i_1));
+    const double dt_avg = 0.5 * (dt_i + dt_i_1);
+    const uint32_t msk = ld_bytes<W>(N.slot_mask + n0);
+    float f[3][W];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int j = 0; j < W; ++j) f[c][j] = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        uint32_t sel = 0;
+#pragma unroll
+        for (int j = 0; j < W; ++j) sel |= ((msk >> (8 * j + k)) & 1u) << j;
+        if (sel) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                float r[W];
+                ld_row<W>(fe + (3 * k + c) * np + n0, r);
+#pragma unroll
+                for (int j = 0; j < W; ++j)
+                    if ((sel >> j) & 1u) f[c][j] += r[j];
+            }
+        }
+    }
+    double im[W];
+    ld_row<W>(N.inv_mass + n0, im);
+    const uint32_t code = ld_bytes<W>(N.bc + n0);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        float vo[W], vn[W];
+        double uo[W], xo[W], un[W], xn[W];
+        ld_row<W>(V + c * np + n0, vo);
+        ld_row<W>(N.u + c * np + n0, uo);
+        ld_row<W>(N.x + c * np + n0, xo);
+#pragma unroll
+        for (int j = 0; j < W; ++j) {
+            vn[j] = vo[j];
+            un[j] = uo[j];
+            xn[j] = xo[j];
+            if (n0 + j >= nn) continue;
+            float a = f[c][j];
+            float g = 0.f;
+            if (M.gravity_on) {
+                g = static_cast<float>(amp * M.gravity_value * M.gravity_dir[c] / im[j]);
+                a += g;
+            }
+            const uint32_t cc = (code >> (8 * j + 2 * c)) & 3u;
+            float r = 0.f, rf = 0.f;
+            if (cc & 2u) {
+                r = -a;
+                a = 0.f;
+            }
+            if ((cc & 1u) && a != 0.f) {
+                rf = -a;
+                r = -a;
+                a = 0.f;
+            }
+            if (cc) N.rf[c * np + n0 + j] = static_cast<double>(rf);
+            vn[j] = fmaf(hdt, a * static_cast<float>(im[j]), vo[j]);
+            const double vnd = static_cast<double>(vn[j]);
+            un[j] = uo[j] + dt_i * vnd;
+            xn[j] = xo[j] + dt_i * vnd;
+            wext += static_cast<double>(g + r) * dt_avg * 0.5 * (static_cast<double>(vo[j]) + vnd);
+            kin += 0.5 * (vnd * vnd) / im[j];
+            if (!isfinite(vn[j])) bad |= ST_NONFINITE;
+        }
+        st_row<W>(V + c * np + n0, vn);
+        st_row<W>(N.u + c * np + n0, un);
+        st_row<W>(N.x + c * np + n0, xn);
+    }
+}
+
 // Node pass in mixed precision: FP32 slot-ordered gather and acceleration,
 // FP32 velocity, FP64 displacement / position accumulation and energy.
 __global__ void __launch_bounds__(kNodeThreads) k_node_mixed(ElemArrays E, NodeArrays N, Material M, Ctl* ctl,
@@ -489,8 +573,13 @@ __global__ void __launch_bounds__(kNodeThreads) k_node_mixed(ElemArrays E, NodeA
     double kin = 0.0, wext = 0.0;
     int32_t bad = 0;
     const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-    for (int64_t n = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; n < nn; n += stride) {
-        node_body_mixed(E, N, M, dt_i, dt_i_1, amp, n, kin, wext, bad);
+    const int64_t t0 = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (E.slot_major && E.tiles_aligned) {
+        constexpr int W = kNodeGroupMixed;
+        for (int64_t g = t0; g * W < nn; g += stride)
+            node_group_mixed<W>(E, N, M, dt_i, dt_i_1, amp, g * W, nn, kin, wext, bad);
+    } else {
+        for (int64_t n = t0; n < nn; n += stride) node_body_mixed(E, N, M, dt_i, dt_i_1, amp, n, kin, wext, bad);
     }
     if (bad) atomicOr(&ctl->status, bad);
     double v2[2] = {kin, wext};
