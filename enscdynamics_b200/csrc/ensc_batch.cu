@@ -510,7 +510,9 @@ int ensc_batch_report(ensc_batch* b, int32_t slot, ensc_step_report* r) {
     r->dt_i_1 = c.dt_i_1;
     r->cycles = c.cycles_done;
     r->total_cycles = c.cycles_done;
-    r->status = (c.status & ensc::ST_INVERTED) ? ENSC_ERR_INVERTED : (c.status ? ENSC_ERR_NONFINITE : ENSC_OK);
+    r->status = (c.status & ensc::ST_TIMEOUT) ? ENSC_ERR_TIMEOUT
+                : (c.status & ensc::ST_INVERTED) ? ENSC_ERR_INVERTED
+                : c.status ? ENSC_ERR_NONFINITE : ENSC_OK;
     r->done = c.done;
     std::memcpy(&r->dt_stable_min, &c.dts_next, sizeof(double));
     return ENSC_OK;

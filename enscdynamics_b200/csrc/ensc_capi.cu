@@ -138,6 +138,7 @@ int status_code(ensc_handle* h, int32_t st) {
     if (st & ensc::ST_NONFINITE) return set_err(h, ENSC_ERR_NONFINITE, "non-finite nodal state detected");
     if (st & ensc::ST_INVERTED) return set_err(h, ENSC_ERR_INVERTED, "element with J <= 0 detected");
     if (st & ensc::ST_BAD_DT) return set_err(h, ENSC_ERR_NONFINITE, "stable time step is not positive");
+    if (st & ensc::ST_TIMEOUT) return set_err(h, ENSC_ERR_TIMEOUT, "a bounded wait for staged element data expired");
     return ENSC_OK;
 }
 
@@ -149,7 +150,9 @@ void fill_report(const ensc_handle* h, int64_t before, ensc_step_report* r) {
     r->dt_i_1 = c.dt_i_1;
     r->cycles = c.cycles_done - before;
     r->total_cycles = c.cycles_done;
-    r->status = c.status ? ((c.status & ensc::ST_INVERTED) ? ENSC_ERR_INVERTED : ENSC_ERR_NONFINITE) : 0;
+    r->status = (c.status & ensc::ST_TIMEOUT) ? ENSC_ERR_TIMEOUT
+                : (c.status & ensc::ST_INVERTED) ? ENSC_ERR_INVERTED
+                : c.status ? ENSC_ERR_NONFINITE : ENSC_OK;
     r->done = c.time < c.step_end ? 0 : 1;
     std::memcpy(&r->dt_stable_min, &c.dts_next, sizeof(double));
 }

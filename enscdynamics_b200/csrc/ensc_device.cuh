@@ -39,6 +39,7 @@ enum : int32_t {
     ST_NONFINITE = 1,
     ST_INVERTED = 2,
     ST_BAD_DT = 4,       // stable dt not positive and finite
+    ST_TIMEOUT = 8,      // a bounded wait for staged data expired; the pass stopped early
 };
 
 // Per-instance control block: the scalar state of exDyna3D's time loop

@@ -28,6 +28,11 @@ constexpr int kElemThreads = 128;
 #endif
 constexpr int kNodeUnrollFp64 = ENSC_NODE_UNROLL_FP64;
 constexpr int kNodeUnrollMixed = ENSC_NODE_UNROLL_MIXED;
+// Mixed element pass with its streamed inputs staged in shared memory by
+// bulk copies (k_element_mixed_staged) instead of per-thread loads.
+#ifndef ENSC_STAGED_MIXED
+#define ENSC_STAGED_MIXED 1
+#endif
 // L2 bulk prefetch of the next grid-stride tile in the element passes.
 #ifndef ENSC_PREFETCH
 #define ENSC_PREFETCH 0

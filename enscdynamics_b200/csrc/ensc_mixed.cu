@@ -12,6 +12,7 @@
 // Node arrays: x, u double; v float.
 #include "ensc_device.cuh"
 #include "ensc_kernels.h"
+#include "ensc_stage.cuh"
 
 #include <cfloat>
 
@@ -95,21 +96,52 @@ __device__ __forceinline__ float tau_f(int k, int j) {
     return ((kMask >> (8 * k + j)) & 1u) ? 1.f : -1.f;
 }
 
+// Where one element's inputs are read from: rows of `stride` entries with the
+// element at `i` -- the instance's own arrays in global memory, or a
+// shared-memory stage that holds a tile of them.
+struct MixedSrc {
+    const uint32_t* conn;   // [8] rows
+    const float* bt;        // [24] rows
+    const float* vol0;
+    const float* cb;
+    const float* sig;       // [6] rows
+    const float* qia;       // [12] rows
+    const float* eps;
+    int64_t stride, i;
+};
+
+__device__ __forceinline__ MixedSrc mixed_src_global(const ElemArrays& E, int64_t e) {
+    return MixedSrc{E.conn,
+                    static_cast<const float*>(E.bt),
+                    reinterpret_cast<const float*>(E.vol0),
+                    reinterpret_cast<const float*>(E.cbrt_v0),
+                    static_cast<const float*>(E.sigma),
+                    static_cast<const float*>(E.qia),
+                    static_cast<const float*>(E.eps_p),
+                    E.ne_pad,
+                    e};
+}
+
+// read-only loads: through the non-coherent path from global memory, plain
+// loads from a shared-memory stage
+template <bool SMEM, typename T>
+__device__ __forceinline__ T ldin(const T* p) {
+    if constexpr (SMEM) return *p;
+    else return __ldg(p);
+}
+
 // One element of the mixed element pass (see the kernel comment below);
-// shared by the single-instance and batched kernels.
-template <bool PLASTIC, bool INIT>
+// shared by the single-instance, staged and batched kernels.  Inputs come
+// from S, outputs go to the instance's arrays at element e.
+template <bool PLASTIC, bool INIT, bool SMEM = false>
 __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const NodeArrays& N, const Material& M,
-                                                   const float dt1, const double dt1d, const int64_t e, double& dts,
-                                                   double& len, double& e_int, double& e_hg, double& e_vis,
-                                                   int32_t& bad) {
-    const int64_t ep = E.ne_pad, np = N.nn_pad;
-    const uint32_t* __restrict__ conn = E.conn;
-    const float* __restrict__ bt = static_cast<const float*>(E.bt);
-    const float* __restrict__ vol0 = reinterpret_cast<const float*>(E.vol0);
-    const float* __restrict__ cb = reinterpret_cast<const float*>(E.cbrt_v0);
-    float* __restrict__ sig = static_cast<float*>(E.sigma);
-    float* __restrict__ qia = static_cast<float*>(E.qia);
-    float* __restrict__ epsp = static_cast<float*>(E.eps_p);
+                                                   const MixedSrc& S, const float dt1, const double dt1d,
+                                                   const int64_t e, double& dts, double& len, double& e_int,
+                                                   double& e_hg, double& e_vis, int32_t& bad) {
+    const int64_t ep = E.ne_pad, np = N.nn_pad, ss = S.stride, si = S.i;
+    float* sig = static_cast<float*>(E.sigma);
+    float* qia = static_cast<float*>(E.qia);
+    float* epsp = static_cast<float*>(E.eps_p);
     float* __restrict__ fe = static_cast<float*>(E.fe);
     const double* __restrict__ X = N.x;
     const float* __restrict__ V = static_cast<const float*>(N.v);
@@ -123,8 +155,8 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
     const float y0 = static_cast<float>(M.yield0), H = static_cast<float>(M.hardening);
     const float DRc = static_cast<float>(M.c_dr * (4.0 / 3.0 * M.G + M.K) * 0.1 / sqrt(8.0));
     const float CRc = static_cast<float>(M.c_cr * M.rho * M.wos / 4.0);
-    const float* __restrict__ bte = bt + e;
-    const uint32_t n0 = __ldg(conn + e);
+    const float* bte = S.bt + si;
+    const uint32_t n0 = ldin<SMEM>(S.conn + si);
     const double x00 = X[n0], x01 = X[np + n0], x02 = X[2 * np + n0];
     // coordinates relative to node 0 (differences formed in FP64):
     // hourglass projections TAU x = TAU (x - x0) (the Gamma rows sum to
@@ -137,7 +169,7 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
         xr[0][0] = xr[0][1] = xr[0][2] = 0.f;
 #pragma unroll
         for (int k = 1; k < 8; ++k) {
-            const uint32_t nk = __ldg(conn + k * ep + e);
+            const uint32_t nk = ldin<SMEM>(S.conn + k * ss + si);
             const double d0 = X[nk] - x00, d1 = X[np + nk] - x01, d2 = X[2 * np + nk] - x02;
             xr[k][0] = static_cast<float>(d0);
             xr[k][1] = static_cast<float>(d1);
@@ -145,8 +177,8 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
         }
 #pragma unroll
         for (int k = 1; k < 8; ++k) {
-            const float* bk = bte + 3 * k * ep;
-            const float bb[3] = {__ldg(bk), __ldg(bk + ep), __ldg(bk + 2 * ep)};
+            const float* bk = bte + 3 * k * ss;
+            const float bb[3] = {ldin<SMEM>(bk), ldin<SMEM>(bk + ss), ldin<SMEM>(bk + 2 * ss)};
 #pragma unroll
             for (int r = 0; r < 3; ++r) {
 #pragma unroll
@@ -179,10 +211,10 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
     float L0[3][3] = {}, VT[3][4] = {}, nx2 = 0.f;
 #pragma unroll kNodeUnrollMixed
     for (int j = 0; j < 8; ++j) {
-        const uint32_t nj = __ldg(conn + j * ep + e);
+        const uint32_t nj = ldin<SMEM>(S.conn + j * ss + si);
         const float vj[3] = {V[nj], V[np + nj], V[2 * np + nj]};
-        const float* bk = bte + 3 * j * ep;
-        const float bb[3] = {__ldg(bk), __ldg(bk + ep), __ldg(bk + 2 * ep)};
+        const float* bk = bte + 3 * j * ss;
+        const float bb[3] = {ldin<SMEM>(bk), ldin<SMEM>(bk + ss), ldin<SMEM>(bk + 2 * ss)};
 #pragma unroll
         for (int r = 0; r < 3; ++r) {
 #pragma unroll
@@ -206,7 +238,7 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
     // Jaumann stress update
     float so[6], s[6];
 #pragma unroll
-    for (int i = 0; i < 6; ++i) so[i] = sig[i * ep + e];
+    for (int i = 0; i < 6; ++i) so[i] = S.sig[i * ss + si];
     float eps[6] = {L[0][0] * dt1, L[1][1] * dt1, L[2][2] * dt1, 0.5f * (L[0][1] + L[1][0]) * dt1,
                     0.5f * (L[0][2] + L[2][0]) * dt1, 0.5f * (L[1][2] + L[2][1]) * dt1};
     {
@@ -234,7 +266,7 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
         const float d0 = s[0] - pm, d1 = s[1] - pm, d2 = s[2] - pm;
         const float j2 = 0.5f * (d0 * d0 + d1 * d1 + d2 * d2) + s[3] * s[3] + s[4] * s[4] + s[5] * s[5];
         const float seq = sqrtf(3.f * j2);
-        const float ep_old = epsp[e];
+        const float ep_old = S.eps[si];
         const float sy = y0 + H * ep_old;
         if (seq > sy) {
             const float dl = (seq - sy) / (3.f * G + H);
@@ -252,7 +284,7 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
 #pragma unroll
         for (int i = 0; i < 6; ++i) sig[i * ep + e] = s[i];
     }
-    const float V0 = vol0[e];
+    const float V0 = S.vol0[si];
     const float Vc = J * V0;
     {
         float w = 0.f;
@@ -261,14 +293,14 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
         e_int += static_cast<double>(w * Vc);
     }
     const float DR = DRc * nx2 * Vc * dt1;
-    const float cbe = cb[e];
+    const float cbe = S.cb[si];
     const float CR = CRc * V0 / Vc * (cbe * cbe);
     float Gq[3][4];
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int kk = 0; kk < 4; ++kk) {
-            const float q = fmaf(DR, HIA[i][kk], qia[(4 * i + kk) * ep + e]);
+            const float q = fmaf(DR, HIA[i][kk], S.qia[(4 * i + kk) * ss + si]);
             if (!INIT) qia[(4 * i + kk) * ep + e] = q;
             Gq[i][kk] = fmaf(CR, HIA[i][kk], q);
         }
@@ -304,12 +336,12 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
     // nodal forces f_j = -(B0_j Z) - Gamma_j Gq^T
 #pragma unroll kNodeUnrollMixed
     for (int j = 0; j < 8; ++j) {
-        const float* bk = bte + 3 * j * ep;
-        const float b0 = __ldg(bk), b1 = __ldg(bk + ep), b2 = __ldg(bk + 2 * ep);
+        const float* bk = bte + 3 * j * ss;
+        const float b0 = ldin<SMEM>(bk), b1 = ldin<SMEM>(bk + ss), b2 = ldin<SMEM>(bk + 2 * ss);
         float* fej;
         int64_t fst;
         if (E.slot_major) {
-            fej = fe + 3 * j * np + __ldg(conn + j * ep + e);
+            fej = fe + 3 * j * np + ldin<SMEM>(S.conn + j * ss + si);
             fst = np;
         } else {
             fej = fe + 3 * j * ep + e;
@@ -378,7 +410,8 @@ __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_MIXED)
             }
         }
         double dts, len;
-        element_body_mixed<PLASTIC, INIT>(E, N, M, dt1, dt1d, e, dts, len, e_int, e_hg, e_vis, bad);
+        element_body_mixed<PLASTIC, INIT>(E, N, M, mixed_src_global(E, e), dt1, dt1d, e, dts, len, e_int, e_hg, e_vis,
+                                          bad);
         dts_min = fmin(dts_min, dts);
         len_min = fmin(len_min, len);
     }
@@ -388,6 +421,118 @@ __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_MIXED)
         double v3[3] = {e_int, e_hg, e_vis};
         block_sum_d<kElemThreads, 3>(v3, P.elem, P.n_elem_blocks, blockIdx.x);
     }
+}
+
+// ---- staged element pass ------------------------------------------------
+// Each block walks tiles of kStageTile consecutive elements.  Thread 0 copies
+// a tile's streamed inputs -- connectivity, B0^T, sigma, QIA, V0, cbrt(V0)
+// and eps_p, 52 or 53 rows of kStageTile entries -- into one of two
+// shared-memory stages with bulk copies, one tile ahead of the compute; the
+// block then evaluates the tile with element_body_mixed reading those inputs
+// from the stage while the next tile's copies are in flight.  Node data are
+// gathered from global memory as in the unstaged pass, and all outputs are
+// written there.
+constexpr int kStageTile = 128;
+constexpr int kStageRows = 53;  // 8 conn + 24 B0^T + 6 sigma + 12 QIA + V0 + cbrt(V0) + eps_p
+constexpr uint32_t kStageBytes = kStageRows * kStageTile * 4;
+constexpr size_t kStageSmem = 2 * static_cast<size_t>(kStageBytes) + 16;  // two stages, two barriers
+
+// row r of the streamed inputs (stage row order) in global memory
+__device__ __forceinline__ const float* stage_row(const ElemArrays& E, int r) {
+    const int64_t ep = E.ne_pad;
+    if (r < 8) return reinterpret_cast<const float*>(E.conn + r * ep);
+    if (r < 32) return static_cast<const float*>(E.bt) + (r - 8) * ep;
+    if (r < 38) return static_cast<const float*>(E.sigma) + (r - 32) * ep;
+    if (r < 50) return static_cast<const float*>(E.qia) + (r - 38) * ep;
+    if (r == 50) return reinterpret_cast<const float*>(E.vol0);
+    if (r == 51) return reinterpret_cast<const float*>(E.cbrt_v0);
+    return static_cast<const float*>(E.eps_p);
+}
+
+// Thread 0: copies the tile starting at element `base` into the stage at
+// shared address dst, completing on bar.  The rows are padded to a multiple
+// of 32 entries and start 256-byte aligned, so every copy is 16-byte aligned
+// and a multiple of 128 bytes long.
+template <bool PLASTIC>
+__device__ __forceinline__ void stage_issue(const ElemArrays& E, uint32_t dst, uint32_t bar, int64_t base) {
+    const int64_t left = E.ne_pad - base;
+    const uint32_t bytes = static_cast<uint32_t>(left < kStageTile ? left : kStageTile) * 4u;
+    constexpr int rows = PLASTIC ? kStageRows : kStageRows - 1;
+    mbar_arrive_expect_tx(bar, rows * bytes);
+    for (int r = 0; r < rows; ++r) bulk_g2s(dst + r * (kStageTile * 4u), stage_row(E, r) + base, bytes, bar);
+}
+
+template <bool PLASTIC>
+__global__ void __launch_bounds__(kStageTile, 4)
+    k_element_mixed_staged(ElemArrays E, NodeArrays N, Material M, Ctl* ctl, Partials P) {
+    if (ctl->done) return;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const float dt1 = static_cast<float>(ctl->dt_i_1);
+    const double dt1d = ctl->dt_i_1;
+    const int tid = threadIdx.x;
+    const uint32_t stage0 = smem_addr(smem);
+    const uint32_t bar0 = stage0 + 2 * kStageBytes;
+    const int64_t ntiles = (E.ne + kStageTile - 1) / kStageTile;
+    const int64_t gstride = gridDim.x;
+    if (tid == 0) {
+        mbar_init(bar0, 1);
+        mbar_init(bar0 + 8, 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (int s = 0; s < 2; ++s) {
+            const int64_t t = blockIdx.x + s * gstride;
+            if (t < ntiles) stage_issue<PLASTIC>(E, stage0 + s * kStageBytes, bar0 + 8 * s, t * kStageTile);
+        }
+    }
+    double e_int = 0.0, e_hg = 0.0, e_vis = 0.0;
+    double dts_min = DBL_MAX, len_min = DBL_MAX;
+    int32_t bad = 0;
+    bool timed_out = false;
+    int it = 0;
+    for (int64_t t = blockIdx.x; t < ntiles; t += gstride, ++it) {
+        const int s = it & 1;
+        const uint32_t bar = bar0 + 8 * s;
+        const bool ok = mbar_wait_bounded(bar, (it >> 1) & 1);
+        if (__syncthreads_or(!ok)) {
+            timed_out = true;
+            break;
+        }
+        const int64_t e = t * kStageTile + tid;
+        if (e < E.ne) {
+            const float* st = reinterpret_cast<const float*>(smem + s * kStageBytes);
+            const MixedSrc S{reinterpret_cast<const uint32_t*>(st), st + 8 * kStageTile, st + 50 * kStageTile,
+                             st + 51 * kStageTile, st + 32 * kStageTile, st + 38 * kStageTile,
+                             st + 52 * kStageTile, kStageTile, tid};
+            double dts, len;
+            element_body_mixed<PLASTIC, false, true>(E, N, M, S, dt1, dt1d, e, dts, len, e_int, e_hg, e_vis, bad);
+            dts_min = fmin(dts_min, dts);
+            len_min = fmin(len_min, len);
+        }
+        __syncthreads();  // the block is done with stage s
+        const int64_t tn = t + 2 * gstride;
+        if (tid == 0 && tn < ntiles) {
+            fence_proxy_async_smem();
+            stage_issue<PLASTIC>(E, stage0 + s * kStageBytes, bar, tn * kStageTile);
+        }
+    }
+    if (timed_out) {
+        // record the failure and let the copies this block started land
+        // (bounded) before its shared memory is released
+        if (tid == 0) {
+            atomicOr(&ctl->status, ST_TIMEOUT);
+            for (int k = 0; k < 2; ++k) {
+                const int itk = it + k;
+                if (blockIdx.x + itk * gstride < ntiles) mbar_wait_bounded(bar0 + 8 * (itk & 1), (itk >> 1) & 1);
+            }
+        }
+        __syncthreads();
+    }
+    if (bad) atomicOr(&ctl->status, bad);
+    block_min2_d<kStageTile>(dts_min, len_min, &ctl->dts_next, &ctl->len_min);
+    double v3[3] = {e_int, e_hg, e_vis};
+    block_sum_d<kStageTile, 3>(v3, P.elem, P.n_elem_blocks, blockIdx.x);
 }
 
 // One node of the mixed node pass; shared by the single-instance and
@@ -628,8 +773,9 @@ __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_MIXED) k_element_
         double ei = 0.0, eh = 0.0, ev = 0.0;
         int32_t bad = 0;
         if (e < d.E.ne) {
-            if (d.M.plastic) element_body_mixed<true, false>(d.E, d.N, d.M, dt1, dt1d, e, dts, len, ei, eh, ev, bad);
-            else element_body_mixed<false, false>(d.E, d.N, d.M, dt1, dt1d, e, dts, len, ei, eh, ev, bad);
+            const MixedSrc S = mixed_src_global(d.E, e);
+            if (d.M.plastic) element_body_mixed<true, false>(d.E, d.N, d.M, S, dt1, dt1d, e, dts, len, ei, eh, ev, bad);
+            else element_body_mixed<false, false>(d.E, d.N, d.M, S, dt1, dt1d, e, dts, len, ei, eh, ev, bad);
         }
         const unsigned long long dmin = warp_min_u64(ord_bits(dts));
         const unsigned long long lmin = warp_min_u64(ord_bits(len));
@@ -702,6 +848,11 @@ __global__ void __launch_bounds__(kNodeThreads) k_node_batch_mixed(BatchTables T
 
 void launch_element_mixed(const ElemArrays& E, const NodeArrays& N, const Material& M, Ctl* ctl, const Partials& P,
                           int grid, bool init, cudaStream_t st) {
+    if (ENSC_STAGED_MIXED && !init && E.tiles_aligned) {
+        if (M.plastic) k_element_mixed_staged<true><<<grid, kStageTile, kStageSmem, st>>>(E, N, M, ctl, P);
+        else k_element_mixed_staged<false><<<grid, kStageTile, kStageSmem, st>>>(E, N, M, ctl, P);
+        return;
+    }
     if (M.plastic) {
         if (init) k_element_mixed<true, true><<<grid, kElemThreads, 0, st>>>(E, N, M, ctl, P);
         else k_element_mixed<true, false><<<grid, kElemThreads, 0, st>>>(E, N, M, ctl, P);
@@ -718,6 +869,20 @@ void launch_node_mixed(const ElemArrays& E, const NodeArrays& N, const Material&
 
 int occupancy_element_mixed(bool plastic) {
     int nb = 0;
+    if (ENSC_STAGED_MIXED) {
+        // the staged pass needs more than the default 48 KB of dynamic shared
+        // memory; the attribute is set here, on the current device, before
+        // any launch or capture
+        cudaFuncSetAttribute(k_element_mixed_staged<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(kStageSmem));
+        cudaFuncSetAttribute(k_element_mixed_staged<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(kStageSmem));
+        if (plastic)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_mixed_staged<true>, kStageTile, kStageSmem);
+        else
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_mixed_staged<false>, kStageTile, kStageSmem);
+        return nb;
+    }
     if (plastic) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_mixed<true, false>, kElemThreads, 0);
     else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_mixed<false, false>, kElemThreads, 0);
     return nb;
