@@ -223,6 +223,14 @@ __device__ __forceinline__ uint32_t ld_bytes(const uint8_t* p) {
     return *reinterpret_cast<const uint16_t*>(p);
 }
 
+// Read-only input loads: through the non-coherent path from global memory,
+// plain loads from a shared-memory stage.
+template <bool SMEM, typename T>
+__device__ __forceinline__ T ldin(const T* p) {
+    if constexpr (SMEM) return *p;
+    else return __ldg(p);
+}
+
 // Positive doubles order like their bit patterns; min-reductions over
 // element dt / edge lengths use integer atomicMin on the bits, which is
 // exact and independent of scheduling.

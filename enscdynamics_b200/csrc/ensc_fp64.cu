@@ -9,6 +9,7 @@
 // launched inside a CUDA graph; see ensc_capi.cu for the orchestration.
 #include "ensc_device.cuh"
 #include "ensc_kernels.h"
+#include "ensc_stage.cuh"
 
 #include <cfloat>
 
@@ -118,28 +119,54 @@ __device__ __forceinline__ void block_min2(double a, double b, unsigned long lon
     __syncthreads();
 }
 
-// One element of the element pass (the kernel comment below has the
-// reference mapping); shared by the single-instance and batched kernels.
-template <bool PLASTIC, bool INIT>
+// Where one element's inputs are read from: rows of `stride` entries with the
+// element at `i` (the instance's global arrays, or a shared-memory stage
+// holding a tile of them); B0^T has its own rows so that it can stay in
+// global memory while the rest is staged.
+struct Fp64Src {
+    const uint32_t* conn;   // [8] rows
+    const double* sig;      // [6] rows
+    const double* qia;      // [12] rows
+    const double* vol0;
+    const double* cb;       // cbrt(V0)
+    const double* cb2;      // cbrt(V0^2)
+    const double* eps;
+    int64_t stride, i;
+    const double* bt;       // [24] rows
+    int64_t bt_stride, bt_i;
+};
+
+__device__ __forceinline__ Fp64Src fp64_src_global(const ElemArrays& E, int64_t e) {
+    return Fp64Src{E.conn, static_cast<const double*>(E.sigma), static_cast<const double*>(E.qia), E.vol0,
+                   E.cbrt_v0, E.cbrt_v0sq, static_cast<const double*>(E.eps_p), E.ne_pad, e,
+                   static_cast<const double*>(E.bt), E.ne_pad, e};
+}
+
+// One element of the FP64 element pass (the kernel comment below has the
+// reference mapping), shared by the single-instance, staged and batched
+// kernels; inputs come from S, outputs go to the instance's arrays at
+// element e.  SMEM / BT_SMEM: S's rows / B0^T rows
+// are in shared memory.
+template <bool PLASTIC, bool INIT, bool SMEM = false, bool BT_SMEM = false>
 __device__ __forceinline__ void element_body(const ElemArrays& E, const NodeArrays& N, const Material& M,
-                                             const double dt1, const int64_t e, double& dts, double& len,
-                                             double& e_int, double& e_hg, double& e_vis, int32_t& bad) {
+                                             const Fp64Src& S, const double dt1, const int64_t e, double& dts,
+                                             double& len, double& e_int, double& e_hg, double& e_vis,
+                                             int32_t& bad) {
+    const int64_t ss = S.stride, si = S.i, bs = S.bt_stride;
     const int64_t ep = E.ne_pad, np = N.nn_pad;
-    const uint32_t* __restrict__ conn = E.conn;
-    const double* __restrict__ bt = static_cast<const double*>(E.bt);
-    double* __restrict__ sig = static_cast<double*>(E.sigma);
-    double* __restrict__ qia = static_cast<double*>(E.qia);
-    double* __restrict__ epsp = static_cast<double*>(E.eps_p);
+    double* sig = static_cast<double*>(E.sigma);
+    double* qia = static_cast<double*>(E.qia);
+    double* epsp = static_cast<double*>(E.eps_p);
     double* __restrict__ fe = static_cast<double*>(E.fe);
     const double* __restrict__ X = N.x;
     const double* __restrict__ U = N.u;
     const double* __restrict__ V = static_cast<const double*>(N.v);
     const double G = M.G, lam = M.lambda;
 
-    const double* __restrict__ bte = bt + e;
+    const double* bte = S.bt + S.bt_i;
     uint32_t n[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) n[k] = __ldg(conn + k * ep + e);
+    for (int k = 0; k < 8; ++k) n[k] = ldin<SMEM>(S.conn + k * ss + si);
     // current coordinates: hourglass projections TAU x (exact, the
     // Gamma entries are +-1) and the minimum edge (min_ele_edge :1173-1220)
     double TX[4][3];
@@ -177,10 +204,10 @@ __device__ __forceinline__ void element_body(const ElemArrays& E, const NodeArra
     double F[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
 #pragma unroll kNodeUnrollFp64
     for (int k = 0; k < 8; ++k) {
-        const uint32_t nk = __ldg(conn + k * ep + e);
+        const uint32_t nk = ldin<SMEM>(S.conn + k * ss + si);
         const double uu[3] = {U[nk], U[np + nk], U[2 * np + nk]};
-        const double* bk = bte + 3 * k * ep;
-        const double bb[3] = {__ldg(bk), __ldg(bk + ep), __ldg(bk + 2 * ep)};
+        const double* bk = bte + 3 * k * bs;
+        const double bb[3] = {ldin<BT_SMEM>(bk), ldin<BT_SMEM>(bk + bs), ldin<BT_SMEM>(bk + 2 * bs)};
 #pragma unroll
         for (int r = 0; r < 3; ++r)
 #pragma unroll
@@ -199,9 +226,9 @@ __device__ __forceinline__ void element_body(const ElemArrays& E, const NodeArra
     double nx2 = 0.0;
 #pragma unroll kNodeUnrollFp64
     for (int j = 0; j < 8; ++j) {
-        const uint32_t nj = __ldg(conn + j * ep + e);
-        const double* bk = bte + 3 * j * ep;
-        const double bb[3] = {__ldg(bk), __ldg(bk + ep), __ldg(bk + 2 * ep)};
+        const uint32_t nj = ldin<SMEM>(S.conn + j * ss + si);
+        const double* bk = bte + 3 * j * bs;
+        const double bb[3] = {ldin<BT_SMEM>(bk), ldin<BT_SMEM>(bk + bs), ldin<BT_SMEM>(bk + 2 * bs)};
         const double vj[3] = {V[nj], V[np + nj], V[2 * np + nj]};
 #pragma unroll
         for (int r = 0; r < 3; ++r) {
@@ -238,7 +265,7 @@ __device__ __forceinline__ void element_body(const ElemArrays& E, const NodeArra
     const double tr = (eps[0] + eps[1]) + eps[2];
     double s[6], so[6];
 #pragma unroll
-    for (int i = 0; i < 6; ++i) so[i] = sig[i * ep + e];
+    for (int i = 0; i < 6; ++i) so[i] = S.sig[i * ss + si];
     double inc[6];
     inc[0] = (lam * tr + 2.0 * G * eps[0]) + 2.0 * so[3] * w0 * dt1 + 2.0 * so[4] * w1 * dt1;
     inc[1] = (lam * tr + 2.0 * G * eps[1]) - 2.0 * so[3] * w0 * dt1 + 2.0 * so[5] * w2 * dt1;
@@ -255,7 +282,7 @@ __device__ __forceinline__ void element_body(const ElemArrays& E, const NodeArra
         const double d0 = s[0] - pm, d1 = s[1] - pm, d2 = s[2] - pm;
         const double j2 = 0.5 * ((d0 * d0 + d1 * d1) + d2 * d2) + ((s[3] * s[3] + s[4] * s[4]) + s[5] * s[5]);
         const double seq = sqrt(3.0 * j2);
-        const double ep_old = epsp[e];
+        const double ep_old = S.eps[si];
         const double sy = M.yield0 + M.hardening * ep_old;
         if (seq > sy) {
             const double dl = (seq - sy) / (3.0 * G + M.hardening);
@@ -273,7 +300,7 @@ __device__ __forceinline__ void element_body(const ElemArrays& E, const NodeArra
 #pragma unroll
         for (int i = 0; i < 6; ++i) sig[i * ep + e] = s[i];
     }
-    const double V0 = E.vol0[e];
+    const double V0 = S.vol0[si];
     const double Vc = J * V0;
     {
         double w = 0.0;
@@ -288,13 +315,13 @@ __device__ __forceinline__ void element_body(const ElemArrays& E, const NodeArra
     const double r43 = 4.0 / 3.0;
     const double r1s8 = 1.0 / sqrt(8.0);
     const double DR = M.c_dr * (r43 * G + M.K) * 0.1 * nx2 * Vc * r1s8 * dt1;
-    const double CR = M.c_cr * M.rho * V0 / Vc * E.cbrt_v0sq[e] * M.wos / 4.0;
+    const double CR = M.c_cr * M.rho * V0 / Vc * S.cb2[si] * M.wos / 4.0;
     double Gq[3][4];
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int kk = 0; kk < 4; ++kk) {
-            const double q = __fma_rn(DR, HIA[i][kk], qia[(4 * i + kk) * ep + e]);
+            const double q = __fma_rn(DR, HIA[i][kk], S.qia[(4 * i + kk) * ss + si]);
             if (!INIT) qia[(4 * i + kk) * ep + e] = q;
             Gq[i][kk] = __fma_rn(CR, HIA[i][kk], q);
         }
@@ -303,7 +330,7 @@ __device__ __forceinline__ void element_body(const ElemArrays& E, const NodeArra
     double pv = 0.0;
     if (visc) {
         const double rho_c = M.rho / J;
-        const double l0 = E.cbrt_v0[e];
+        const double l0 = S.cb[si];
         const double m0 = vr < 0.0 ? vr : 0.0;
         pv = rho_c * l0 * (M.cvisq * M.cvisq * l0 * vr * m0 - M.cvisl * M.wos * vr);
         e_vis += -(pv * Vc * vr) * dt1;
@@ -335,12 +362,12 @@ __device__ __forceinline__ void element_body(const ElemArrays& E, const NodeArra
     // (= -b_j sigma V - h_j + p b_j V: :985-997, :1070, :1106)
 #pragma unroll kNodeUnrollFp64
     for (int j = 0; j < 8; ++j) {
-        const double* bk = bte + 3 * j * ep;
-        const double b0 = __ldg(bk), b1 = __ldg(bk + ep), b2 = __ldg(bk + 2 * ep);
+        const double* bk = bte + 3 * j * bs;
+        const double b0 = ldin<BT_SMEM>(bk), b1 = ldin<BT_SMEM>(bk + bs), b2 = ldin<BT_SMEM>(bk + 2 * bs);
         double* fej;
         int64_t fst;
         if (E.slot_major) {
-            fej = fe + 3 * j * np + __ldg(conn + j * ep + e);
+            fej = fe + 3 * j * np + ldin<SMEM>(S.conn + j * ss + si);
             fst = np;
         } else {
             fej = fe + 3 * j * ep + e;
@@ -417,7 +444,7 @@ __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_FP64) k_element(E
                 }
             }
         }
-        if (live) element_body<PLASTIC, INIT>(E, N, M, dt1, e, dts, len, e_int, e_hg, e_vis, bad);
+        if (live) element_body<PLASTIC, INIT>(E, N, M, fp64_src_global(E, e), dt1, e, dts, len, e_int, e_hg, e_vis, bad);
         dts_min = dts < dts_min ? dts : dts_min;
         len_min = len < len_min ? len : len_min;
     }
@@ -526,6 +553,129 @@ __device__ __forceinline__ void node_body(const ElemArrays& E, const NodeArrays&
         kin = kin + 0.5 * (vn * vn) / im;
         if (!isfinite(vn)) bad |= ST_NONFINITE;
     }
+}
+
+// ---- staged element pass ------------------------------------------------
+// As k_element, with each block walking tiles of kStageTileF64 consecutive
+// elements whose streamed inputs -- connectivity, sigma, QIA, V0, cbrt(V0),
+// cbrt(V0^2), eps_p and, when BT, B0^T -- thread 0 copies into one of two
+// shared-memory stages with bulk copies one tile ahead of the compute.  The
+// arithmetic is element_body's, so results are bit-identical to k_element.
+constexpr int kStageTileF64 = 128;
+constexpr int kF64StageRows = 22;  // double rows before B0^T: 6 sigma, 12 QIA, V0, cbrt V0, cbrt V0^2, eps_p
+template <bool BT>
+constexpr uint32_t f64_stage_bytes() {
+    return 8u * kStageTileF64 * 4u + static_cast<uint32_t>(kF64StageRows + (BT ? 24 : 0)) * kStageTileF64 * 8u;
+}
+template <bool BT>
+constexpr size_t f64_stage_smem() {
+    return 2 * static_cast<size_t>(f64_stage_bytes<BT>()) + 16;
+}
+
+// double row r of the stage in global memory
+__device__ __forceinline__ const double* f64_stage_row(const ElemArrays& E, int r) {
+    const int64_t ep = E.ne_pad;
+    if (r < 6) return static_cast<const double*>(E.sigma) + r * ep;
+    if (r < 18) return static_cast<const double*>(E.qia) + (r - 6) * ep;
+    if (r == 18) return E.vol0;
+    if (r == 19) return E.cbrt_v0;
+    if (r == 20) return E.cbrt_v0sq;
+    if (r == 21) return static_cast<const double*>(E.eps_p);
+    return static_cast<const double*>(E.bt) + (r - kF64StageRows) * ep;
+}
+
+// Thread 0: the tile starting at element `base` into the stage at shared
+// address dst, completing on bar (rows padded to 32 entries and 256-byte
+// aligned: every copy is 16-byte aligned and a multiple of 128 bytes).
+template <bool PLASTIC, bool BT>
+__device__ __forceinline__ void f64_stage_issue(const ElemArrays& E, uint32_t dst, uint32_t bar, int64_t base) {
+    const int64_t left = E.ne_pad - base;
+    const uint32_t cnt = static_cast<uint32_t>(left < kStageTileF64 ? left : kStageTileF64);
+    constexpr int drows = kF64StageRows + (BT ? 24 : 0);
+    constexpr int dcopies = PLASTIC ? drows : drows - 1;
+    mbar_arrive_expect_tx(bar, 8u * cnt * 4u + static_cast<uint32_t>(dcopies) * cnt * 8u);
+    for (int k = 0; k < 8; ++k) bulk_g2s(dst + k * (kStageTileF64 * 4u), E.conn + k * E.ne_pad + base, cnt * 4u, bar);
+    const uint32_t dbase = dst + 8u * kStageTileF64 * 4u;
+    for (int r = 0; r < drows; ++r) {
+        if (!PLASTIC && r == 21) continue;  // eps_p is read only with J2
+        bulk_g2s(dbase + r * (kStageTileF64 * 8u), f64_stage_row(E, r) + base, cnt * 8u, bar);
+    }
+}
+
+template <bool PLASTIC, bool BT>
+__global__ void __launch_bounds__(kStageTileF64, BT ? 2 : 3)
+    k_element_staged(ElemArrays E, NodeArrays N, Material M, Ctl* ctl, Partials P) {
+    if (ctl->done) return;
+    extern __shared__ __align__(128) unsigned char smem[];
+    constexpr uint32_t SB = f64_stage_bytes<BT>();
+    constexpr int T = kStageTileF64;
+    const double dt1 = ctl->dt_i_1;
+    const int tid = threadIdx.x;
+    const uint32_t stage0 = smem_addr(smem);
+    const uint32_t bar0 = stage0 + 2 * SB;
+    const int64_t ntiles = (E.ne + T - 1) / T;
+    const int64_t gstride = gridDim.x;
+    if (tid == 0) {
+        mbar_init(bar0, 1);
+        mbar_init(bar0 + 8, 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (int s = 0; s < 2; ++s) {
+            const int64_t t = blockIdx.x + s * gstride;
+            if (t < ntiles) f64_stage_issue<PLASTIC, BT>(E, stage0 + s * SB, bar0 + 8 * s, t * T);
+        }
+    }
+    double e_int = 0.0, e_hg = 0.0, e_vis = 0.0;
+    double dts_min = DBL_MAX, len_min = DBL_MAX;
+    int32_t bad = 0;
+    bool timed_out = false;
+    int it = 0;
+    for (int64_t t = blockIdx.x; t < ntiles; t += gstride, ++it) {
+        const int s = it & 1;
+        const uint32_t bar = bar0 + 8 * s;
+        const bool ok = mbar_wait_bounded(bar, (it >> 1) & 1);
+        if (__syncthreads_or(!ok)) {
+            timed_out = true;
+            break;
+        }
+        const int64_t e = t * T + tid;
+        if (e < E.ne) {
+            const unsigned char* st = smem + s * SB;
+            const double* d = reinterpret_cast<const double*>(st + 8 * T * 4);
+            const Fp64Src S{reinterpret_cast<const uint32_t*>(st), d, d + 6 * T, d + 18 * T, d + 19 * T, d + 20 * T,
+                            d + 21 * T, T, tid,
+                            BT ? d + kF64StageRows * T : static_cast<const double*>(E.bt),
+                            BT ? static_cast<int64_t>(T) : E.ne_pad, BT ? static_cast<int64_t>(tid) : e};
+            double dts, len;
+            element_body<PLASTIC, false, true, BT>(E, N, M, S, dt1, e, dts, len, e_int, e_hg, e_vis, bad);
+            dts_min = dts < dts_min ? dts : dts_min;
+            len_min = len < len_min ? len : len_min;
+        }
+        __syncthreads();  // the block is done with stage s
+        const int64_t tn = t + 2 * gstride;
+        if (tid == 0 && tn < ntiles) {
+            fence_proxy_async_smem();
+            f64_stage_issue<PLASTIC, BT>(E, stage0 + s * SB, bar, tn * T);
+        }
+    }
+    if (timed_out) {
+        // record the failure and let the copies this block started land
+        // (bounded) before its shared memory is released
+        if (tid == 0) {
+            atomicOr(&ctl->status, ST_TIMEOUT);
+            for (int k = 0; k < 2; ++k) {
+                const int itk = it + k;
+                if (blockIdx.x + itk * gstride < ntiles) mbar_wait_bounded(bar0 + 8 * (itk & 1), (itk >> 1) & 1);
+            }
+        }
+        __syncthreads();
+    }
+    if (bad) atomicOr(&ctl->status, bad);
+    block_min2<kStageTileF64>(dts_min, len_min, &ctl->dts_next, &ctl->len_min);
+    double v3[3] = {e_int, e_hg, e_vis};
+    block_sum<kStageTileF64, 3>(v3, P.elem, P.n_elem_blocks, blockIdx.x);
 }
 
 // W consecutive nodes of the node pass with 16-byte row accesses: the same
@@ -694,8 +844,9 @@ __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_FP64) k_element_b
         double ei = 0.0, eh = 0.0, ev = 0.0;
         int32_t bad = 0;
         if (e < d.E.ne) {
-            if (d.M.plastic) element_body<true, false>(d.E, d.N, d.M, dt1, e, dts, len, ei, eh, ev, bad);
-            else element_body<false, false>(d.E, d.N, d.M, dt1, e, dts, len, ei, eh, ev, bad);
+            const Fp64Src S = fp64_src_global(d.E, e);
+            if (d.M.plastic) element_body<true, false>(d.E, d.N, d.M, S, dt1, e, dts, len, ei, eh, ev, bad);
+            else element_body<false, false>(d.E, d.N, d.M, S, dt1, e, dts, len, ei, eh, ev, bad);
         }
         const unsigned long long dmin = warp_min_u64(ord_bits(static_cast<double>(dts)));
         const unsigned long long lmin = warp_min_u64(ord_bits(static_cast<double>(len)));
@@ -766,8 +917,18 @@ __global__ void __launch_bounds__(kNodeThreads) k_node_batch_fp64(BatchTables T)
 
 }  // namespace
 
+namespace {
+constexpr bool kStagedBt = ENSC_STAGED_FP64 == 2;
+}
+
 void launch_element_fp64(const ElemArrays& E, const NodeArrays& N, const Material& M, Ctl* ctl, const Partials& P,
                          int grid, bool init, cudaStream_t st) {
+    if (ENSC_STAGED_FP64 && !init && E.tiles_aligned) {
+        constexpr size_t smem = f64_stage_smem<kStagedBt>();
+        if (M.plastic) k_element_staged<true, kStagedBt><<<grid, kStageTileF64, smem, st>>>(E, N, M, ctl, P);
+        else k_element_staged<false, kStagedBt><<<grid, kStageTileF64, smem, st>>>(E, N, M, ctl, P);
+        return;
+    }
     if (M.plastic) {
         if (init) k_element<true, true><<<grid, kElemThreads, 0, st>>>(E, N, M, ctl, P);
         else k_element<true, false><<<grid, kElemThreads, 0, st>>>(E, N, M, ctl, P);
@@ -784,6 +945,20 @@ void launch_node_fp64(const ElemArrays& E, const NodeArrays& N, const Material& 
 
 int occupancy_element_fp64(bool plastic) {
     int nb = 0;
+    if (ENSC_STAGED_FP64) {
+        // more than the default 48 KB of dynamic shared memory: set on the
+        // current device, before any launch or capture
+        constexpr size_t smem = f64_stage_smem<kStagedBt>();
+        cudaFuncSetAttribute(k_element_staged<true, kStagedBt>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem));
+        cudaFuncSetAttribute(k_element_staged<false, kStagedBt>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem));
+        if (plastic)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_staged<true, kStagedBt>, kStageTileF64, smem);
+        else
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_staged<false, kStagedBt>, kStageTileF64, smem);
+        return nb;
+    }
     if (plastic) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element<true, false>, kElemThreads, 0);
     else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element<false, false>, kElemThreads, 0);
     return nb;

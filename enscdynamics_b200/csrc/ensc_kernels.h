@@ -33,6 +33,11 @@ constexpr int kNodeUnrollMixed = ENSC_NODE_UNROLL_MIXED;
 #ifndef ENSC_STAGED_MIXED
 #define ENSC_STAGED_MIXED 1
 #endif
+// FP64 element pass staged the same way: 0 off, 1 staging all streamed
+// inputs except B0^T (read from global memory), 2 staging B0^T too.
+#ifndef ENSC_STAGED_FP64
+#define ENSC_STAGED_FP64 2
+#endif
 // L2 bulk prefetch of the next grid-stride tile in the element passes.
 #ifndef ENSC_PREFETCH
 #define ENSC_PREFETCH 0

@@ -122,14 +122,6 @@ __device__ __forceinline__ MixedSrc mixed_src_global(const ElemArrays& E, int64_
                     e};
 }
 
-// read-only loads: through the non-coherent path from global memory, plain
-// loads from a shared-memory stage
-template <bool SMEM, typename T>
-__device__ __forceinline__ T ldin(const T* p) {
-    if constexpr (SMEM) return *p;
-    else return __ldg(p);
-}
-
 // One element of the mixed element pass (see the kernel comment below);
 // shared by the single-instance, staged and batched kernels.  Inputs come
 // from S, outputs go to the instance's arrays at element e.
