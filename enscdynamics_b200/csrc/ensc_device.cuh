@@ -86,8 +86,10 @@ struct ElemArrays {
     void* qia;
     void* eps_p;
     void* fe;
-    // 1 when every component array starts 256-byte aligned and ne_pad is a
-    // multiple of 32, so whole 32-element tiles may be bulk-prefetched
+    // 1 when every element and node array starts 256-byte aligned and
+    // ne_pad / nn_pad are multiples of 32: rows of whole 32-entry tiles can be
+    // bulk-copied and read as 16-byte vectors (the staged element passes and
+    // the vectorised node passes)
     int32_t tiles_aligned;
     // 1: fe is node-major, fe[(3k + c) * nn_pad + conn[k][e]] -- the
     // reference's per-local-slot nodal vectors (exDyna3D.cpp:523-634), each
@@ -241,20 +243,5 @@ __device__ __forceinline__ double bits_ord(unsigned long long b) {
     return __longlong_as_double(static_cast<long long>(b));
 }
 constexpr unsigned long long kInfBits = 0x7FF0000000000000ull;
-
-// Bulk prefetch of [p, p + bytes) into L2 (bytes a multiple of 16, p 16-byte
-// aligned).  Used one grid-stride iteration ahead on structure-of-arrays
-// tiles, so streamed element / node data is L2-resident when a warp needs it.
-__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
-
-// A warp's lanes prefetch the tile [t0, t0 + 32) of ncomp component arrays
-// (component c at base + c * stride elements, elements of esize bytes); the
-// caller guarantees the tile lies inside the padded arrays.
-template <typename T>
-__device__ __forceinline__ void prefetch_tile(const T* base, int64_t stride, int ncomp, int64_t t0, int lane) {
-    for (int c = lane; c < ncomp; c += 32) prefetch_l2(base + c * stride + t0, 32u * sizeof(T));
-}
 
 }  // namespace ensc

@@ -427,23 +427,6 @@ __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_FP64) k_element(E
         const bool live = e0 < ne;
         const int64_t e = live ? e0 : 0;
         double dts = DBL_MAX, len = DBL_MAX;
-        if (ENSC_PREFETCH && E.tiles_aligned) {
-            // this warp's next tile (32 elements, 32-element aligned, inside ne_pad)
-            const int lane = threadIdx.x & 31;
-            const int64_t tn = e0 - lane + stride;
-            if (tn < ne) {
-                prefetch_tile(conn, ep, 8, tn, lane);
-                prefetch_tile(bt, ep, 24, tn, lane);
-                prefetch_tile(sig, ep, 6, tn, lane);
-                prefetch_tile(qia, ep, 12, tn, lane);
-                if (lane == 0) {
-                    prefetch_l2(E.vol0 + tn, 256);
-                    prefetch_l2(E.cbrt_v0 + tn, 256);
-                    prefetch_l2(E.cbrt_v0sq + tn, 256);
-                    if (PLASTIC) prefetch_l2(epsp + tn, 256);
-                }
-            }
-        }
         if (live) element_body<PLASTIC, INIT>(E, N, M, fp64_src_global(E, e), dt1, e, dts, len, e_int, e_hg, e_vis, bad);
         dts_min = dts < dts_min ? dts : dts_min;
         len_min = len < len_min ? len : len_min;

@@ -178,7 +178,9 @@ int instance_prepare(const ensc_mesh_desc* mesh, const ensc_material* mat, bool 
     const size_t fe_rows = h.clash ? E8 : N8;
     using P = InstanceHost::Piece;
     h.size[P::CONN] = 8 * E8 * sizeof(uint32_t);
-    h.size[P::BT] = 24 * E8 * real;
+    // FP64: B0^T rows as given; mixed: the 3x3 matrix A = sum_j B0_j s_j^T
+    // (B0_j = A s_j / 8) as 9 hi and 9 lo float rows
+    h.size[P::BT] = (mixed ? 18 : 24) * E8 * real;
     h.size[P::VOL0] = E8 * 8;
     h.size[P::CB] = E8 * 8;
     h.size[P::CB2] = E8 * 8;
@@ -214,9 +216,22 @@ int instance_upload(const InstanceHost& h, void* block, cudaStream_t st, ElemArr
     cudaError_t e = cudaMemsetAsync(block, 0, h.bytes, st);
     std::vector<uint8_t> bc(static_cast<size_t>(np), 0);
     if (h.mixed) {
-        if (e == cudaSuccess) e = put(block, h.off[P::BT], to_soa<float>(h.bt.data(), h.ne, ep, 24), st);
-        std::vector<float> v0f(h.vol0.begin(), h.vol0.end()), cbf(h.cb.begin(), h.cb.end());
-        if (e == cudaSuccess) e = put(block, h.off[P::VOL0], v0f, st);
+        // corner signs s_j of the reference hexahedron (Element_HexN8.cpp:49-91)
+        static const double kCorner[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
+                                             {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
+        std::vector<float> a(static_cast<size_t>(18 * ep), 0.f);
+        for (int64_t el = 0; el < h.ne; ++el)
+            for (int c = 0; c < 3; ++c)
+                for (int m = 0; m < 3; ++m) {
+                    double v = 0.0;
+                    for (int j = 0; j < 8; ++j) v += h.bt[24 * el + 3 * j + c] * kCorner[j][m];
+                    const float hi = static_cast<float>(v);
+                    a[(3 * c + m) * ep + el] = hi;
+                    a[(9 + 3 * c + m) * ep + el] = static_cast<float>(v - static_cast<double>(hi));
+                }
+        if (e == cudaSuccess) e = put(block, h.off[P::BT], a, st);
+        std::vector<float> cbf(h.cb.begin(), h.cb.end());
+        if (e == cudaSuccess) e = put(block, h.off[P::VOL0], h.vol0, st);
         if (e == cudaSuccess) e = put(block, h.off[P::CB], cbf, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // temporaries above die here
     } else {

@@ -38,10 +38,6 @@ constexpr int kNodeUnrollMixed = ENSC_NODE_UNROLL_MIXED;
 #ifndef ENSC_STAGED_FP64
 #define ENSC_STAGED_FP64 2
 #endif
-// L2 bulk prefetch of the next grid-stride tile in the element passes.
-#ifndef ENSC_PREFETCH
-#define ENSC_PREFETCH 0
-#endif
 constexpr int kNodeThreads = 256;
 constexpr int kCtlThreads = 256;
 

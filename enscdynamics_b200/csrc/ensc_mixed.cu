@@ -7,8 +7,10 @@
 // order is free here (FMA contraction on), accuracy is checked against the
 // FP64 path by relative displacement error and energy drift.
 //
-// Element arrays: bt, sigma, qia, eps_p, fe are float; vol0 and cbrt_v0 are
-// float copies (stored in the first ne words of the FP64 arrays' storage).
+// Element arrays: the bt rows hold A = sum_j B0_j s_j^T (the one-point B0
+// rows are A s_j / 8, s_j the node's reference-corner signs) as a float pair,
+// 9 hi then 9 lo rows; sigma, qia, eps_p and fe are float; vol0 is double;
+// cbrt_v0 is a float copy (in the first ne words of its FP64 storage).
 // Node arrays: x, u double; v float.
 #include "ensc_device.cuh"
 #include "ensc_kernels.h"
@@ -101,8 +103,8 @@ __device__ __forceinline__ float tau_f(int k, int j) {
 // shared-memory stage that holds a tile of them.
 struct MixedSrc {
     const uint32_t* conn;   // [8] rows
-    const float* bt;        // [24] rows
-    const float* vol0;
+    const float* a;         // [18] rows: A hi (3c+m), then A lo
+    const double* vol0;
     const float* cb;
     const float* sig;       // [6] rows
     const float* qia;       // [12] rows
@@ -113,13 +115,21 @@ struct MixedSrc {
 __device__ __forceinline__ MixedSrc mixed_src_global(const ElemArrays& E, int64_t e) {
     return MixedSrc{E.conn,
                     static_cast<const float*>(E.bt),
-                    reinterpret_cast<const float*>(E.vol0),
+                    E.vol0,
                     reinterpret_cast<const float*>(E.cbrt_v0),
                     static_cast<const float*>(E.sigma),
                     static_cast<const float*>(E.qia),
                     static_cast<const float*>(E.eps_p),
                     E.ne_pad,
                     e};
+}
+
+// sign of the reference-hexahedron corner coordinate m (xi, eta, zeta) of
+// local node j (Element_HexN8.cpp:49-91): the one-point B0 row of node j is
+// A (s_j) / 8 with A = sum_j B0_j s_j^T
+__device__ __forceinline__ float corner_sign(int m, int j) {
+    constexpr unsigned kMask = 0x66u | (0xCCu << 8) | (0xF0u << 16);
+    return ((kMask >> (8 * m + j)) & 1u) ? 1.f : -1.f;
 }
 
 // One element of the mixed element pass (see the kernel comment below);
@@ -147,49 +157,71 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
     const float y0 = static_cast<float>(M.yield0), H = static_cast<float>(M.hardening);
     const float DRc = static_cast<float>(M.c_dr * (4.0 / 3.0 * M.G + M.K) * 0.1 / sqrt(8.0));
     const float CRc = static_cast<float>(M.c_cr * M.rho * M.wos / 4.0);
-    const float* bte = S.bt + si;
+    // A = sum_j B0_j s_j^T as a float pair (hi + lo); B0 enters every
+    // product through A, so no FP32 rounding of the reference geometry is
+    // shared by all elements of a uniform mesh
+    float Ah[3][3], Al[3][3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            Ah[c][m] = ldin<SMEM>(S.a + (3 * c + m) * ss + si);
+            Al[c][m] = ldin<SMEM>(S.a + (9 + 3 * c + m) * ss + si);
+        }
     const uint32_t n0 = ldin<SMEM>(S.conn + si);
     const double x00 = X[n0], x01 = X[np + n0], x02 = X[2 * np + n0];
-    // coordinates relative to node 0 (differences formed in FP64):
-    // hourglass projections TAU x = TAU (x - x0) (the Gamma rows sum to
-    // zero), the minimum edge, and F = sum_j (x_j - x_0) B0_j, which equals
-    // I + u_e B0^T because sum_j X0_j B0_j = I and sum_j B0_j = 0
+    // coordinates relative to node 0, as FP64 differences: hourglass
+    // projections TAU x = TAU (x - x0) (the Gamma rows sum to zero) in FP32;
+    // the minimum edge and F = sum_j (x_j - x_0) B0_j
+    // = (sum_j (x_j - x_0) s_j^T) A^T / 8 (= I + u_e B0^T, as
+    // sum_j X0_j B0_j = I and sum_j B0_j = 0) in FP64, since on a uniform mesh
+    // the FP32 rounding of the spacing would be the same for every element
+    // and shift the stiffness and the stable dt of all of them alike
     float TX[4][3] = {};
     float F[3][3] = {};
     {
-        float xr[8][3];
-        xr[0][0] = xr[0][1] = xr[0][2] = 0.f;
+        double xd[8][3];
+        xd[0][0] = xd[0][1] = xd[0][2] = 0.0;
 #pragma unroll
         for (int k = 1; k < 8; ++k) {
             const uint32_t nk = ldin<SMEM>(S.conn + k * ss + si);
-            const double d0 = X[nk] - x00, d1 = X[np + nk] - x01, d2 = X[2 * np + nk] - x02;
-            xr[k][0] = static_cast<float>(d0);
-            xr[k][1] = static_cast<float>(d1);
-            xr[k][2] = static_cast<float>(d2);
+            xd[k][0] = X[nk] - x00;
+            xd[k][1] = X[np + nk] - x01;
+            xd[k][2] = X[2 * np + nk] - x02;
         }
+        double Gx[3][3] = {};
 #pragma unroll
         for (int k = 1; k < 8; ++k) {
-            const float* bk = bte + 3 * k * ss;
-            const float bb[3] = {ldin<SMEM>(bk), ldin<SMEM>(bk + ss), ldin<SMEM>(bk + 2 * ss)};
 #pragma unroll
             for (int r = 0; r < 3; ++r) {
+                const float xr = static_cast<float>(xd[k][r]);
 #pragma unroll
-                for (int c = 0; c < 3; ++c) F[r][c] = fmaf(xr[k][r], bb[c], F[r][c]);
+                for (int m = 0; m < 3; ++m) Gx[r][m] += static_cast<double>(corner_sign(m, k)) * xd[k][r];
 #pragma unroll
-                for (int kk = 0; kk < 4; ++kk) TX[kk][r] += tau_f(kk, k) * xr[k][r];
+                for (int kk = 0; kk < 4; ++kk) TX[kk][r] += tau_f(kk, k) * xr;
             }
         }
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                double t = 0.0;
+#pragma unroll
+                for (int m = 0; m < 3; ++m)
+                    t = fma(Gx[r][m], static_cast<double>(Ah[c][m]) + static_cast<double>(Al[c][m]), t);
+                F[r][c] = static_cast<float>(0.125 * t);
+            }
         constexpr int A0[12] = {0, 1, 2, 3, 4, 5, 6, 7, 0, 1, 2, 3};
         constexpr int A1[12] = {1, 2, 3, 0, 5, 6, 7, 4, 4, 5, 6, 7};
-        float m = FLT_MAX;
+        double m = DBL_MAX;
 #pragma unroll
         for (int k = 0; k < 12; ++k) {
-            const float dx = xr[A1[k]][0] - xr[A0[k]][0];
-            const float dy = xr[A1[k]][1] - xr[A0[k]][1];
-            const float dz = xr[A1[k]][2] - xr[A0[k]][2];
-            m = fminf(m, fmaf(dz, dz, fmaf(dy, dy, dx * dx)));
+            const double dx = xd[A1[k]][0] - xd[A0[k]][0];
+            const double dy = xd[A1[k]][1] - xd[A0[k]][1];
+            const double dz = xd[A1[k]][2] - xd[A0[k]][2];
+            m = fmin(m, fma(dz, dz, fma(dy, dy, dx * dx)));
         }
-        len = sqrtf(m);
+        len = sqrt(m);
     }
     const float J = det3f(F);
     if (!(J > 0.f)) bad |= ST_INVERTED;
@@ -199,22 +231,40 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
     for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int j = 0; j < 3; ++j) Fi[i][j] = cof3f(F, j, i) * invdet;
-    // L0 = v_e B0^T, VT = v_e Gamma^T, NX2
-    float L0[3][3] = {}, VT[3][4] = {}, nx2 = 0.f;
+    // L0 = v_e B0^T = (sum_j v_j s_j^T) A^T / 8, VT = v_e Gamma^T,
+    // NX2 = sum_j |B0_j|^2 = |A|^2 / 8 (sum_j s_j s_j^T = 8 I)
+    float L0[3][3], VT[3][4] = {}, nx2 = 0.f;
+    {
+        float Gv[3][3] = {};
 #pragma unroll kNodeUnrollMixed
-    for (int j = 0; j < 8; ++j) {
-        const uint32_t nj = ldin<SMEM>(S.conn + j * ss + si);
-        const float vj[3] = {V[nj], V[np + nj], V[2 * np + nj]};
-        const float* bk = bte + 3 * j * ss;
-        const float bb[3] = {ldin<SMEM>(bk), ldin<SMEM>(bk + ss), ldin<SMEM>(bk + 2 * ss)};
+        for (int j = 0; j < 8; ++j) {
+            const uint32_t nj = ldin<SMEM>(S.conn + j * ss + si);
+            const float vj[3] = {V[nj], V[np + nj], V[2 * np + nj]};
 #pragma unroll
-        for (int r = 0; r < 3; ++r) {
+            for (int r = 0; r < 3; ++r) {
 #pragma unroll
-            for (int c = 0; c < 3; ++c) L0[r][c] = fmaf(vj[r], bb[c], L0[r][c]);
+                for (int m = 0; m < 3; ++m) Gv[r][m] += corner_sign(m, j) * vj[r];
 #pragma unroll
-            for (int kk = 0; kk < 4; ++kk) VT[r][kk] += tau_f(kk, j) * vj[r];
+                for (int kk = 0; kk < 4; ++kk) VT[r][kk] += tau_f(kk, j) * vj[r];
+            }
         }
-        nx2 += fmaf(bb[2], bb[2], fmaf(bb[1], bb[1], bb[0] * bb[0]));
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                float t = Gv[r][0] * Al[c][0];
+                t = fmaf(Gv[r][1], Al[c][1], t);
+                t = fmaf(Gv[r][2], Al[c][2], t);
+                t = fmaf(Gv[r][0], Ah[c][0], t);
+                t = fmaf(Gv[r][1], Ah[c][1], t);
+                t = fmaf(Gv[r][2], Ah[c][2], t);
+                L0[r][c] = 0.125f * t;
+            }
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int m = 0; m < 3; ++m) nx2 = fmaf(Ah[c][m], Ah[c][m], nx2);
+        nx2 *= 0.125f;
     }
     // L = L0 F^-1, HIA = VT - L0 TX^T
     float L[3][3], HIA[3][4];
@@ -231,12 +281,16 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
     float so[6], s[6];
 #pragma unroll
     for (int i = 0; i < 6; ++i) so[i] = S.sig[i * ss + si];
-    float eps[6] = {L[0][0] * dt1, L[1][1] * dt1, L[2][2] * dt1, 0.5f * (L[0][1] + L[1][0]) * dt1,
-                    0.5f * (L[0][2] + L[2][0]) * dt1, 0.5f * (L[1][2] + L[2][1]) * dt1};
+    // dt enters the increments as a float pair too: it changes little from
+    // cycle to cycle, so its FP32 rounding would repeat with the same sign
+    const float dt1_lo = static_cast<float>(dt1d - static_cast<double>(dt1));
+    auto incr = [&](float g) { return fmaf(g, dt1, g * dt1_lo); };
+    float eps[6] = {incr(L[0][0]), incr(L[1][1]), incr(L[2][2]), incr(0.5f * (L[0][1] + L[1][0])),
+                    incr(0.5f * (L[0][2] + L[2][0])), incr(0.5f * (L[1][2] + L[2][1]))};
     {
-        const float w0 = 0.5f * (L[0][1] - L[1][0]) * dt1;
-        const float w1 = 0.5f * (L[0][2] - L[2][0]) * dt1;
-        const float w2 = 0.5f * (L[1][2] - L[2][1]) * dt1;
+        const float w0 = incr(0.5f * (L[0][1] - L[1][0]));
+        const float w1 = incr(0.5f * (L[0][2] - L[2][0]));
+        const float w2 = incr(0.5f * (L[1][2] - L[2][1]));
         const float tr = eps[0] + eps[1] + eps[2];
         // lambda and 2G enter as unevaluated pairs hi + lo of floats: a
         // stiffness rounded to FP32 is off by up to 6e-8 for every element
@@ -276,8 +330,7 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
 #pragma unroll
         for (int i = 0; i < 6; ++i) sig[i * ep + e] = s[i];
     }
-    const float V0 = S.vol0[si];
-    const float Vc = J * V0;
+    const float Vc = static_cast<float>(static_cast<double>(J) * S.vol0[si]);
     {
         float w = 0.f;
 #pragma unroll
@@ -286,7 +339,7 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
     }
     const float DR = DRc * nx2 * Vc * dt1;
     const float cbe = S.cb[si];
-    const float CR = CRc * V0 / Vc * (cbe * cbe);
+    const float CR = CRc / J * (cbe * cbe);  // V0 / Vc = 1 / J
     float Gq[3][4];
 #pragma unroll
     for (int i = 0; i < 3; ++i)
@@ -325,11 +378,23 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
             for (int kk = 0; kk < 4; ++kk) hp = fmaf(Gq[i][kk], HIA[i][kk], hp);
         e_hg += static_cast<double>(hp) * dt1d;
     }
-    // nodal forces f_j = -(B0_j Z) - Gamma_j Gq^T
+    // nodal forces f_j = -(B0_j Z) - Gamma_j Gq^T with B0_j Z = s_j^T Y / 8,
+    // Y = A^T Z
+    float Y[3][3];
+#pragma unroll
+    for (int m = 0; m < 3; ++m)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            float t = Al[0][m] * Z[0][i];
+            t = fmaf(Al[1][m], Z[1][i], t);
+            t = fmaf(Al[2][m], Z[2][i], t);
+            t = fmaf(Ah[0][m], Z[0][i], t);
+            t = fmaf(Ah[1][m], Z[1][i], t);
+            t = fmaf(Ah[2][m], Z[2][i], t);
+            Y[m][i] = 0.125f * t;
+        }
 #pragma unroll kNodeUnrollMixed
     for (int j = 0; j < 8; ++j) {
-        const float* bk = bte + 3 * j * ss;
-        const float b0 = ldin<SMEM>(bk), b1 = ldin<SMEM>(bk + ss), b2 = ldin<SMEM>(bk + 2 * ss);
         float* fej;
         int64_t fst;
         if (E.slot_major) {
@@ -344,15 +409,15 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
             float tg = 0.f;
 #pragma unroll
             for (int kk = 0; kk < 4; ++kk) tg += tau_f(kk, j) * Gq[i][kk];
-            fej[i * fst] = -fmaf(b2, Z[2][i], fmaf(b1, Z[1][i], b0 * Z[0][i])) - tg;
+            const float bz = corner_sign(0, j) * Y[0][i] + corner_sign(1, j) * Y[1][i] + corner_sign(2, j) * Y[2][i];
+            fej[i * fst] = -bz - tg;
         }
     }
     // element dt (compute_dtStable, exDyna3D.cpp:828-834)
     {
-        const float lf = static_cast<float>(len);
-        const float m0 = fminf(vr, 0.f);
-        const float xi = cvisl - cvisq * cvisq * lf / wos * m0;
-        dts = (sqrtf(1.f + xi * xi) - xi) * lf / wos;
+        const double m0 = fmin(static_cast<double>(vr), 0.0);
+        const double xi = M.cvisl - M.cvisq * M.cvisq * len / M.wos * m0;
+        dts = (sqrt(1.0 + xi * xi) - xi) * len / M.wos;
     }
     if (!isfinite(dts)) bad |= ST_NONFINITE;
 }
@@ -386,21 +451,6 @@ __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_MIXED)
 
     const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
     for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < ne; e += stride) {
-        if (ENSC_PREFETCH && E.tiles_aligned) {
-            const int lane = threadIdx.x & 31;
-            const int64_t tn = e - lane + stride;
-            if (tn < ne) {
-                prefetch_tile(conn, ep, 8, tn, lane);
-                prefetch_tile(bt, ep, 24, tn, lane);
-                prefetch_tile(sig, ep, 6, tn, lane);
-                prefetch_tile(qia, ep, 12, tn, lane);
-                if (lane == 0) {
-                    prefetch_l2(vol0 + tn, 128);
-                    prefetch_l2(cb + tn, 128);
-                    if (PLASTIC) prefetch_l2(epsp + tn, 128);
-                }
-            }
-        }
         double dts, len;
         element_body_mixed<PLASTIC, INIT>(E, N, M, mixed_src_global(E, e), dt1, dt1d, e, dts, len, e_int, e_hg, e_vis,
                                           bad);
@@ -417,27 +467,29 @@ __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_MIXED)
 
 // ---- staged element pass ------------------------------------------------
 // Each block walks tiles of kStageTile consecutive elements.  Thread 0 copies
-// a tile's streamed inputs -- connectivity, B0^T, sigma, QIA, V0, cbrt(V0)
-// and eps_p, 52 or 53 rows of kStageTile entries -- into one of two
+// a tile's streamed inputs -- connectivity, the B0 matrix A (hi and lo),
+// sigma, QIA, cbrt(V0), eps_p and V0 -- into one of two
 // shared-memory stages with bulk copies, one tile ahead of the compute; the
 // block then evaluates the tile with element_body_mixed reading those inputs
 // from the stage while the next tile's copies are in flight.  Node data are
 // gathered from global memory as in the unstaged pass, and all outputs are
 // written there.
 constexpr int kStageTile = 128;
-constexpr int kStageRows = 53;  // 8 conn + 24 B0^T + 6 sigma + 12 QIA + V0 + cbrt(V0) + eps_p
-constexpr uint32_t kStageBytes = kStageRows * kStageTile * 4;
+// stage: 46 rows of 4-byte words (8 conn, 18 A, 6 sigma, 12 QIA, cbrt(V0),
+// eps_p), then V0 as a row of doubles
+constexpr int kStageWordRows = 46;
+constexpr uint32_t kStageV0Off = kStageWordRows * kStageTile * 4;
+constexpr uint32_t kStageBytes = kStageV0Off + kStageTile * 8;
 constexpr size_t kStageSmem = 2 * static_cast<size_t>(kStageBytes) + 16;  // two stages, two barriers
 
-// row r of the streamed inputs (stage row order) in global memory
+// word row r of the stage in global memory
 __device__ __forceinline__ const float* stage_row(const ElemArrays& E, int r) {
     const int64_t ep = E.ne_pad;
     if (r < 8) return reinterpret_cast<const float*>(E.conn + r * ep);
-    if (r < 32) return static_cast<const float*>(E.bt) + (r - 8) * ep;
-    if (r < 38) return static_cast<const float*>(E.sigma) + (r - 32) * ep;
-    if (r < 50) return static_cast<const float*>(E.qia) + (r - 38) * ep;
-    if (r == 50) return reinterpret_cast<const float*>(E.vol0);
-    if (r == 51) return reinterpret_cast<const float*>(E.cbrt_v0);
+    if (r < 26) return static_cast<const float*>(E.bt) + (r - 8) * ep;
+    if (r < 32) return static_cast<const float*>(E.sigma) + (r - 26) * ep;
+    if (r < 44) return static_cast<const float*>(E.qia) + (r - 32) * ep;
+    if (r == 44) return reinterpret_cast<const float*>(E.cbrt_v0);
     return static_cast<const float*>(E.eps_p);
 }
 
@@ -448,10 +500,11 @@ __device__ __forceinline__ const float* stage_row(const ElemArrays& E, int r) {
 template <bool PLASTIC>
 __device__ __forceinline__ void stage_issue(const ElemArrays& E, uint32_t dst, uint32_t bar, int64_t base) {
     const int64_t left = E.ne_pad - base;
-    const uint32_t bytes = static_cast<uint32_t>(left < kStageTile ? left : kStageTile) * 4u;
-    constexpr int rows = PLASTIC ? kStageRows : kStageRows - 1;
-    mbar_arrive_expect_tx(bar, rows * bytes);
-    for (int r = 0; r < rows; ++r) bulk_g2s(dst + r * (kStageTile * 4u), stage_row(E, r) + base, bytes, bar);
+    const uint32_t cnt = static_cast<uint32_t>(left < kStageTile ? left : kStageTile);
+    constexpr int rows = PLASTIC ? kStageWordRows : kStageWordRows - 1;  // eps_p last, J2 only
+    mbar_arrive_expect_tx(bar, rows * cnt * 4u + cnt * 8u);
+    for (int r = 0; r < rows; ++r) bulk_g2s(dst + r * (kStageTile * 4u), stage_row(E, r) + base, cnt * 4u, bar);
+    bulk_g2s(dst + kStageV0Off, E.vol0 + base, cnt * 8u, bar);
 }
 
 template <bool PLASTIC>
@@ -494,9 +547,15 @@ __global__ void __launch_bounds__(kStageTile, 4)
         const int64_t e = t * kStageTile + tid;
         if (e < E.ne) {
             const float* st = reinterpret_cast<const float*>(smem + s * kStageBytes);
-            const MixedSrc S{reinterpret_cast<const uint32_t*>(st), st + 8 * kStageTile, st + 50 * kStageTile,
-                             st + 51 * kStageTile, st + 32 * kStageTile, st + 38 * kStageTile,
-                             st + 52 * kStageTile, kStageTile, tid};
+            const MixedSrc S{reinterpret_cast<const uint32_t*>(st),
+                             st + 8 * kStageTile,
+                             reinterpret_cast<const double*>(smem + s * kStageBytes + kStageV0Off),
+                             st + 44 * kStageTile,
+                             st + 26 * kStageTile,
+                             st + 32 * kStageTile,
+                             st + 45 * kStageTile,
+                             kStageTile,
+                             tid};
             double dts, len;
             element_body_mixed<PLASTIC, false, true>(E, N, M, S, dt1, dt1d, e, dts, len, e_int, e_hg, e_vis, bad);
             dts_min = fmin(dts_min, dts);
@@ -527,6 +586,16 @@ __global__ void __launch_bounds__(kStageTile, 4)
     block_sum_d<kStageTile, 3>(v3, P.elem, P.n_elem_blocks, blockIdx.x);
 }
 
+// v + (dt_i + dt_i_1) / 2 * f * M^-1 in FP32 with the half step and the
+// inverse mass as float pairs: both are the same for many nodes and cycles,
+// so their FP32 rounding would scale all accelerations alike.
+__device__ __forceinline__ float velocity_update(float vo, float f, double im, float hdt, float hdt_lo) {
+    const float im_hi = static_cast<float>(im);
+    const float im_lo = static_cast<float>(im - static_cast<double>(im_hi));
+    const float acc = fmaf(f, im_hi, f * im_lo);
+    return fmaf(hdt, acc, fmaf(hdt_lo, acc, vo));
+}
+
 // One node of the mixed node pass; shared by the single-instance and
 // batched kernels.
 __device__ __forceinline__ void node_body_mixed(const ElemArrays& E, const NodeArrays& N, const Material& M,
@@ -536,6 +605,7 @@ __device__ __forceinline__ void node_body_mixed(const ElemArrays& E, const NodeA
     const float* __restrict__ fe = static_cast<const float*>(E.fe);
     float* __restrict__ V = static_cast<float*>(N.v);
     const float hdt = static_cast<float>(0.5 * (dt_i + dt_i_1));
+    const float hdt_lo = static_cast<float>(0.5 * (dt_i + dt_i_1) - static_cast<double>(hdt));
     const double dt_avg = 0.5 * (dt_i + dt_i_1);
 
     float f[3] = {0.f, 0.f, 0.f};
@@ -567,7 +637,6 @@ __device__ __forceinline__ void node_body_mixed(const ElemArrays& E, const NodeA
         }
     }
     const double im = N.inv_mass[n];
-    const float imf = static_cast<float>(im);
     const uint32_t code = N.bc[n];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -590,7 +659,7 @@ __device__ __forceinline__ void node_body_mixed(const ElemArrays& E, const NodeA
         }
         if (cc) N.rf[c * np + n] = static_cast<double>(rf);
         const float vo = V[c * np + n];
-        const float vn = fmaf(hdt, a * imf, vo);
+        const float vn = velocity_update(vo, a, im, hdt, hdt_lo);
         V[c * np + n] = vn;
         const double vnd = static_cast<double>(vn);
         N.u[c * np + n] += dt_i * vnd;
@@ -614,6 +683,7 @@ __device__ __forceinline__ void node_group_mixed(const ElemArrays& E, const Node
     const float* __restrict__ fe = static_cast<const float*>(E.fe);
     float* __restrict__ V = static_cast<float*>(N.v);
     const float hdt = static_cast<float>(0.5 * (dt_i + dt_i_1));
+    const float hdt_lo = static_cast<float>(0.5 * (dt_i + dt_i_1) - static_cast<double>(hdt));
     const double dt_avg = 0.5 * (dt_i + dt_i_1);
     const uint32_t msk = ld_bytes<W>(N.slot_mask + n0);
     float f[3][W];
@@ -671,7 +741,7 @@ __device__ __forceinline__ void node_group_mixed(const ElemArrays& E, const Node
                 a = 0.f;
             }
             if (cc) N.rf[c * np + n0 + j] = static_cast<double>(rf);
-            vn[j] = fmaf(hdt, a * static_cast<float>(im[j]), vo[j]);
+            vn[j] = velocity_update(vo[j], a, im[j], hdt, hdt_lo);
             const double vnd = static_cast<double>(vn[j]);
             un[j] = uo[j] + dt_i * vnd;
             xn[j] = xo[j] + dt_i * vnd;
