@@ -141,11 +141,12 @@ def element_pass_bytes(ne: int, nn: int, plastic: bool, mixed: bool = False) -> 
     FP64: connectivity 32, sigma r/w 96, QIA r/w 192, B0^T 192, V0 8,
     element-force write 192 per element (+16 eps_p r/w with J2); x, u, v
     gathered once per node (72 B).
-    Mixed: connectivity 32, sigma r/w 48, QIA r/w 96, B0^T 96, V0 4, force
-    write 96 (+8 eps_p); x FP64 and v FP32 per node (36 B: the mixed pass
-    forms F from current coordinates and does not read u)."""
+    Mixed: connectivity 32, sigma r/w 48, QIA r/w 96, the B0 matrix A as a
+    float pair 72, V0 8, cbrt(V0) 4, force write 96 (+8 eps_p); x FP64 and
+    v FP32 per node (36 B: the mixed pass forms F from current coordinates
+    and does not read u)."""
     if mixed:
-        return ne * (32 + 48 + 96 + 96 + 4 + 96 + (8 if plastic else 0)) + nn * 36
+        return ne * (32 + 48 + 96 + 72 + 8 + 4 + 96 + (8 if plastic else 0)) + nn * 36
     return ne * (32 + 96 + 192 + 192 + 8 + 192 + (16 if plastic else 0)) + nn * 72
 
 
@@ -161,12 +162,10 @@ def node_pass_bytes(ne: int, nn: int, mixed: bool = False) -> int:
 
 
 def cycle_bytes(ne: int, nn: int, plastic: bool, mixed: bool = False) -> int:
-    """Canonical algorithmic bytes of one cycle: FP64 904 B per element (+16
-    with J2) and 185 B per node; mixed 468 B per element (+8) and 157 B per
-    node."""
-    if mixed:
-        return ne * (468 + (8 if plastic else 0)) + nn * 157
-    return ne * (904 + (16 if plastic else 0)) + nn * 185
+    """Canonical algorithmic bytes of one cycle (element pass + node pass):
+    FP64 904 B per element (+16 with J2) and 226 B per node; mixed 452 B per
+    element (+8) and 166 B per node."""
+    return element_pass_bytes(ne, nn, plastic, mixed) + node_pass_bytes(ne, nn, mixed)
 
 
 def build_problem(name: str, dims: str = "256,128,64"):

@@ -87,16 +87,12 @@ __device__ __forceinline__ void block_min2_d(double a, double b, unsigned long l
 }
 
 // Element pass (add_inForce_to_rhs element loop body, exDyna3D.cpp:556-573)
-// in FP32.  Node coordinates enter as offsets from the element's node 0,
-// formed in FP64 before rounding, so hourglass projections and edge lengths
-// keep their precision far from the origin.  The nodes are streamed twice
-// (kinematics, then forces) with per-node rows of b^T and ATAU recomputed, so
-// only accumulators stay live.  The hourglass force uses the reassociated
-// sum  sum_k ATAU(k,j) (QIA(i,k) + CR HIA(i,k))  (exDyna3D.cpp:1053-1070).
-__device__ __forceinline__ float tau_f(int k, int j) {
-    constexpr unsigned kMask = 0x55u | (0x3Cu << 8) | (0x96u << 16) | (0x5Au << 24);
-    return ((kMask >> (8 * k + j)) & 1u) ? 1.f : -1.f;
-}
+// in FP32.  Node coordinates enter as FP64 offsets from the element's node
+// 0; the geometry that every element of a uniform mesh shares (F, edges,
+// B0) is carried in FP64 or as float pairs.  Node data are visited twice
+// (kinematics, then forces), one component at a time, through the corner
+// transforms below.  The hourglass force uses the reassociated sum
+// sum_k ATAU(k,j) (QIA(i,k) + CR HIA(i,k))  (exDyna3D.cpp:1053-1070).
 
 // Where one element's inputs are read from: rows of `stride` entries with the
 // element at `i` -- the instance's own arrays in global memory, or a
@@ -124,12 +120,49 @@ __device__ __forceinline__ MixedSrc mixed_src_global(const ElemArrays& E, int64_
                     e};
 }
 
-// sign of the reference-hexahedron corner coordinate m (xi, eta, zeta) of
-// local node j (Element_HexN8.cpp:49-91): the one-point B0 row of node j is
-// A (s_j) / 8 with A = sum_j B0_j s_j^T
-__device__ __forceinline__ float corner_sign(int m, int j) {
-    constexpr unsigned kMask = 0x66u | (0xCCu << 8) | (0xF0u << 16);
-    return ((kMask >> (8 * m + j)) & 1u) ? 1.f : -1.f;
+// The one-point B0 row of local node j is A s_j / 8 with A = sum_j B0_j s_j^T
+// and s_j the node's reference-corner signs (xi, eta, zeta), Element_HexN8.cpp
+// :49-91.
+
+// Sums over the 8 nodes with the signs of the reference corners.  Node j sits
+// at corner bits x + 2y + 4z (x set where xi = +1, y for eta, z for zeta);
+// for a subset S of {xi, eta, zeta} (bits 0, 1, 2) the coefficient
+// c[S] = sum_j (prod_{d in S} sigma_d(j)) a_j, sigma_d(j) = +-1.  The corner
+// signs are c[1], c[2], c[4]; the hourglass vectors are
+// Gamma = (c[3], -c[6], -c[5], c[7]) (xi eta, -eta zeta, -zeta xi,
+// xi eta zeta).  One butterfly of 24 additions gives all of them.
+template <typename T>
+__device__ __forceinline__ void corner_coeffs(const T (&a)[8], T (&c)[8]) {
+    constexpr int kBits[8] = {0, 1, 3, 2, 4, 5, 7, 6};
+#pragma unroll
+    for (int j = 0; j < 8; ++j) c[kBits[j]] = a[j];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+            if (!(i & (1 << d))) {
+                const T lo = c[i], hi = c[i | (1 << d)];
+                c[i] = hi + lo;
+                c[i | (1 << d)] = hi - lo;
+            }
+}
+
+// The other direction: node values a_j = sum_S c[S] prod_{d in S} sigma_d(j)
+// (c is overwritten).
+template <typename T>
+__device__ __forceinline__ void corner_values(T (&c)[8], T (&a)[8]) {
+    constexpr int kBits[8] = {0, 1, 3, 2, 4, 5, 7, 6};
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+            if (!(i & (1 << d))) {
+                const T c0 = c[i], c1 = c[i | (1 << d)];
+                c[i | (1 << d)] = c0 + c1;
+                c[i] = c0 - c1;
+            }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) a[j] = c[kBits[j]];
 }
 
 // One element of the mixed element pass (see the kernel comment below);
@@ -168,38 +201,45 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
             Ah[c][m] = ldin<SMEM>(S.a + (3 * c + m) * ss + si);
             Al[c][m] = ldin<SMEM>(S.a + (9 + 3 * c + m) * ss + si);
         }
-    const uint32_t n0 = ldin<SMEM>(S.conn + si);
-    const double x00 = X[n0], x01 = X[np + n0], x02 = X[2 * np + n0];
-    // coordinates relative to node 0, as FP64 differences: hourglass
-    // projections TAU x = TAU (x - x0) (the Gamma rows sum to zero) in FP32;
-    // the minimum edge and F = sum_j (x_j - x_0) B0_j
+    uint32_t nk[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) nk[k] = ldin<SMEM>(S.conn + k * ss + si);
+    // coordinates relative to node 0, as FP64 differences, one component at a
+    // time: hourglass projections TAU x = TAU (x - x0) (the Gamma rows sum to
+    // zero) rounded to FP32; the minimum edge and F = sum_j (x_j - x_0) B0_j
     // = (sum_j (x_j - x_0) s_j^T) A^T / 8 (= I + u_e B0^T, as
-    // sum_j X0_j B0_j = I and sum_j B0_j = 0) in FP64, since on a uniform mesh
-    // the FP32 rounding of the spacing would be the same for every element
-    // and shift the stiffness and the stable dt of all of them alike
-    float TX[4][3] = {};
-    float F[3][3] = {};
+    // sum_j X0_j B0_j = I and sum_j B0_j = 0) kept in FP64, since on a
+    // uniform mesh the FP32 rounding of the spacing would be the same for
+    // every element and shift the stiffness and the stable dt of all of them
+    float TX[4][3];
+    float F[3][3];
     {
-        double xd[8][3];
-        xd[0][0] = xd[0][1] = xd[0][2] = 0.0;
+        constexpr int A0[12] = {0, 1, 2, 3, 4, 5, 6, 7, 0, 1, 2, 3};
+        constexpr int A1[12] = {1, 2, 3, 0, 5, 6, 7, 4, 4, 5, 6, 7};
+        double e2[12];
+        double Gx[3][3];
 #pragma unroll
-        for (int k = 1; k < 8; ++k) {
-            const uint32_t nk = ldin<SMEM>(S.conn + k * ss + si);
-            xd[k][0] = X[nk] - x00;
-            xd[k][1] = X[np + nk] - x01;
-            xd[k][2] = X[2 * np + nk] - x02;
-        }
-        double Gx[3][3] = {};
+        for (int r = 0; r < 3; ++r) {
+            const double* Xr = X + r * np;
+            const double xo = Xr[nk[0]];
+            double xd[8];
+            xd[0] = 0.0;
 #pragma unroll
-        for (int k = 1; k < 8; ++k) {
+            for (int k = 1; k < 8; ++k) xd[k] = Xr[nk[k]] - xo;
 #pragma unroll
-            for (int r = 0; r < 3; ++r) {
-                const float xr = static_cast<float>(xd[k][r]);
-#pragma unroll
-                for (int m = 0; m < 3; ++m) Gx[r][m] += static_cast<double>(corner_sign(m, k)) * xd[k][r];
-#pragma unroll
-                for (int kk = 0; kk < 4; ++kk) TX[kk][r] += tau_f(kk, k) * xr;
+            for (int q = 0; q < 12; ++q) {
+                const double d = xd[A1[q]] - xd[A0[q]];
+                e2[q] = r == 0 ? d * d : fma(d, d, e2[q]);
             }
+            double c[8];
+            corner_coeffs(xd, c);
+            Gx[r][0] = c[1];
+            Gx[r][1] = c[2];
+            Gx[r][2] = c[4];
+            TX[0][r] = static_cast<float>(c[3]);
+            TX[1][r] = static_cast<float>(-c[6]);
+            TX[2][r] = static_cast<float>(-c[5]);
+            TX[3][r] = static_cast<float>(c[7]);
         }
 #pragma unroll
         for (int r = 0; r < 3; ++r)
@@ -211,16 +251,9 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
                     t = fma(Gx[r][m], static_cast<double>(Ah[c][m]) + static_cast<double>(Al[c][m]), t);
                 F[r][c] = static_cast<float>(0.125 * t);
             }
-        constexpr int A0[12] = {0, 1, 2, 3, 4, 5, 6, 7, 0, 1, 2, 3};
-        constexpr int A1[12] = {1, 2, 3, 0, 5, 6, 7, 4, 4, 5, 6, 7};
         double m = DBL_MAX;
 #pragma unroll
-        for (int k = 0; k < 12; ++k) {
-            const double dx = xd[A1[k]][0] - xd[A0[k]][0];
-            const double dy = xd[A1[k]][1] - xd[A0[k]][1];
-            const double dz = xd[A1[k]][2] - xd[A0[k]][2];
-            m = fmin(m, fma(dz, dz, fma(dy, dy, dx * dx)));
-        }
+        for (int q = 0; q < 12; ++q) m = fmin(m, e2[q]);
         len = sqrt(m);
     }
     const float J = det3f(F);
@@ -231,22 +264,25 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
     for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int j = 0; j < 3; ++j) Fi[i][j] = cof3f(F, j, i) * invdet;
-    // L0 = v_e B0^T = (sum_j v_j s_j^T) A^T / 8, VT = v_e Gamma^T,
+    // L0 = v_e B0^T = (sum_j v_j s_j^T) A^T / 8, VT = v_e Gamma^T (both from
+    // the corner coefficients of each velocity component),
     // NX2 = sum_j |B0_j|^2 = |A|^2 / 8 (sum_j s_j s_j^T = 8 I)
-    float L0[3][3], VT[3][4] = {}, nx2 = 0.f;
+    float L0[3][3], VT[3][4], nx2 = 0.f;
     {
-        float Gv[3][3] = {};
-#pragma unroll kNodeUnrollMixed
-        for (int j = 0; j < 8; ++j) {
-            const uint32_t nj = ldin<SMEM>(S.conn + j * ss + si);
-            const float vj[3] = {V[nj], V[np + nj], V[2 * np + nj]};
+        float Gv[3][3];
 #pragma unroll
-            for (int r = 0; r < 3; ++r) {
+        for (int r = 0; r < 3; ++r) {
+            float a[8], c[8];
 #pragma unroll
-                for (int m = 0; m < 3; ++m) Gv[r][m] += corner_sign(m, j) * vj[r];
-#pragma unroll
-                for (int kk = 0; kk < 4; ++kk) VT[r][kk] += tau_f(kk, j) * vj[r];
-            }
+            for (int j = 0; j < 8; ++j) a[j] = V[r * np + nk[j]];
+            corner_coeffs(a, c);
+            Gv[r][0] = c[1];
+            Gv[r][1] = c[2];
+            Gv[r][2] = c[4];
+            VT[r][0] = c[3];
+            VT[r][1] = -c[6];
+            VT[r][2] = -c[5];
+            VT[r][3] = c[7];
         }
 #pragma unroll
         for (int r = 0; r < 3; ++r)
@@ -393,24 +429,19 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
             t = fmaf(Ah[2][m], Z[2][i], t);
             Y[m][i] = 0.125f * t;
         }
-#pragma unroll kNodeUnrollMixed
-    for (int j = 0; j < 8; ++j) {
-        float* fej;
-        int64_t fst;
-        if (E.slot_major) {
-            fej = fe + 3 * j * np + ldin<SMEM>(S.conn + j * ss + si);
-            fst = np;
-        } else {
-            fej = fe + 3 * j * ep + e;
-            fst = ep;
-        }
+    // per force component: the node values of -(B0_j Z) - Gamma_j Gq^T from
+    // their corner coefficients (-Y on xi, eta, zeta; -Gq on the hourglass
+    // vectors, signed as Gamma)
 #pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            float tg = 0.f;
+    for (int i = 0; i < 3; ++i) {
+        float c[8] = {0.f,          -Y[0][i],     -Y[1][i],     -Gq[i][0],
+                      -Y[2][i],     Gq[i][2],     Gq[i][1],     -Gq[i][3]};
+        float f[8];
+        corner_values(c, f);
 #pragma unroll
-            for (int kk = 0; kk < 4; ++kk) tg += tau_f(kk, j) * Gq[i][kk];
-            const float bz = corner_sign(0, j) * Y[0][i] + corner_sign(1, j) * Y[1][i] + corner_sign(2, j) * Y[2][i];
-            fej[i * fst] = -bz - tg;
+        for (int j = 0; j < 8; ++j) {
+            if (E.slot_major) fe[(3 * j + i) * np + nk[j]] = f[j];
+            else fe[(3 * j + i) * ep + e] = f[j];
         }
     }
     // element dt (compute_dtStable, exDyna3D.cpp:828-834)
@@ -814,7 +845,7 @@ __device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v)
     return v;
 }
 
-__global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_MIXED) k_element_batch_mixed(BatchTables T) {
+__global__ void __launch_bounds__(kElemThreads, 4) k_element_batch_mixed(BatchTables T) {
     const int lane = threadIdx.x & 31;
     const int warp = static_cast<int>((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
     const int nwarps = static_cast<int>((static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5);
