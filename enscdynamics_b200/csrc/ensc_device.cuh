@@ -195,26 +195,40 @@ __host__ __device__ inline double gravity_amplitude(const double* amp, int n, do
     return y;
 }
 
-// 16-byte vector access to W consecutive entries of a padded SoA row (rows
-// start 256-byte aligned, the row stride is a multiple of 32 entries and the
-// first index a multiple of W, so every chunk is 16-byte aligned).
+// Vector access to W consecutive entries of a padded SoA row (rows start
+// 256-byte aligned, the row stride is a multiple of 32 entries and the first
+// index a multiple of W): 16-byte chunks, or one 8-byte chunk when the W
+// entries take 8 bytes.
 template <int W, typename T>
 __device__ __forceinline__ void ld_row(const T* p, T (&o)[W]) {
-    static_assert((W * sizeof(T)) % 16 == 0, "whole 16-byte chunks");
+    constexpr int kBytes = W * static_cast<int>(sizeof(T));
+    static_assert(kBytes % 16 == 0 || kBytes == 8, "16-byte chunks or one 8-byte chunk");
+    if constexpr (kBytes == 8) {
+        const uint2 q = *reinterpret_cast<const uint2*>(p);
+        memcpy(o, &q, 8);
+    } else {
 #pragma unroll
-    for (int i = 0; i < static_cast<int>(W * sizeof(T) / 16); ++i) {
-        const uint4 q = reinterpret_cast<const uint4*>(p)[i];
-        memcpy(reinterpret_cast<char*>(o) + 16 * i, &q, 16);
+        for (int i = 0; i < kBytes / 16; ++i) {
+            const uint4 q = reinterpret_cast<const uint4*>(p)[i];
+            memcpy(reinterpret_cast<char*>(o) + 16 * i, &q, 16);
+        }
     }
 }
 template <int W, typename T>
 __device__ __forceinline__ void st_row(T* p, const T (&v)[W]) {
-    static_assert((W * sizeof(T)) % 16 == 0, "whole 16-byte chunks");
+    constexpr int kBytes = W * static_cast<int>(sizeof(T));
+    static_assert(kBytes % 16 == 0 || kBytes == 8, "16-byte chunks or one 8-byte chunk");
+    if constexpr (kBytes == 8) {
+        uint2 q;
+        memcpy(&q, v, 8);
+        *reinterpret_cast<uint2*>(p) = q;
+    } else {
 #pragma unroll
-    for (int i = 0; i < static_cast<int>(W * sizeof(T) / 16); ++i) {
-        uint4 q;
-        memcpy(&q, reinterpret_cast<const char*>(v) + 16 * i, 16);
-        reinterpret_cast<uint4*>(p)[i] = q;
+        for (int i = 0; i < kBytes / 16; ++i) {
+            uint4 q;
+            memcpy(&q, reinterpret_cast<const char*>(v) + 16 * i, 16);
+            reinterpret_cast<uint4*>(p)[i] = q;
+        }
     }
 }
 // W (2 or 4) consecutive bytes as one word, byte j of node j in bits 8j..8j+7.

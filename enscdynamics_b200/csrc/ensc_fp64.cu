@@ -749,7 +749,7 @@ __device__ __forceinline__ void node_group(const ElemArrays& E, const NodeArrays
 // ((((((a0+a1)+a2)+a3)+a4)+a5)+a6)+a7, exDyna3D.cpp:638-639), gravity
 // (:819-824), boundary conditions on a (:2029-2145), a = f M^-1 (:642-644),
 // v += (dt_i + dt_i_1) a / 2, u += dt_i v, x += dt_i v (:646-654, :688-696).
-__global__ void __launch_bounds__(kNodeThreads) k_node(ElemArrays E, NodeArrays N, Material M, Ctl* ctl, Partials P) {
+__global__ void __launch_bounds__(kNodeThreads, ENSC_NODE_MINB_FP64) k_node(ElemArrays E, NodeArrays N, Material M, Ctl* ctl, Partials P) {
     if (ctl->done) return;
     // stable dt of this cycle (update_minVertex_perMaterial_and_dt :673-679)
     double dt_i;

@@ -48,8 +48,19 @@ void launch_node_fp64(const ElemArrays& E, const NodeArrays& N, const Material& 
                       int grid, cudaStream_t st);
 int occupancy_element_fp64(bool plastic);
 // nodes per thread of the node pass on the padded slot-major layout
+#ifndef ENSC_NODE_GROUP_MIXED
+#define ENSC_NODE_GROUP_MIXED 4
+#endif
+// resident blocks per SM requested for the node passes (register budget
+// 65536 / (256 * minb)); tuned on B200
+#ifndef ENSC_NODE_MINB_MIXED
+#define ENSC_NODE_MINB_MIXED 3
+#endif
+#ifndef ENSC_NODE_MINB_FP64
+#define ENSC_NODE_MINB_FP64 4
+#endif
 constexpr int kNodeGroupFp64 = 2;
-constexpr int kNodeGroupMixed = 4;
+constexpr int kNodeGroupMixed = ENSC_NODE_GROUP_MIXED;
 int node_group_width(bool mixed_precision);
 int occupancy_node_fp64();
 

@@ -788,7 +788,7 @@ __device__ __forceinline__ void node_group_mixed(const ElemArrays& E, const Node
 
 // Node pass in mixed precision: FP32 slot-ordered gather and acceleration,
 // FP32 velocity, FP64 displacement / position accumulation and energy.
-__global__ void __launch_bounds__(kNodeThreads) k_node_mixed(ElemArrays E, NodeArrays N, Material M, Ctl* ctl,
+__global__ void __launch_bounds__(kNodeThreads, ENSC_NODE_MINB_MIXED) k_node_mixed(ElemArrays E, NodeArrays N, Material M, Ctl* ctl,
                                                              Partials P) {
     if (ctl->done) return;
     double dt_i;
