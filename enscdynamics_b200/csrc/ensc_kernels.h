@@ -33,6 +33,14 @@ constexpr int kNodeUnrollMixed = ENSC_NODE_UNROLL_MIXED;
 #ifndef ENSC_STAGED_MIXED
 #define ENSC_STAGED_MIXED 1
 #endif
+// elements per stage (= threads per block) and resident blocks per SM of
+// the staged mixed pass; tuned on B200
+#ifndef ENSC_STAGE_TILE_MIXED
+#define ENSC_STAGE_TILE_MIXED 64
+#endif
+#ifndef ENSC_STAGE_MINB_MIXED
+#define ENSC_STAGE_MINB_MIXED 8
+#endif
 // FP64 element pass staged the same way: 0 off, 1 staging all streamed
 // inputs except B0^T (read from global memory), 2 staging B0^T too.
 #ifndef ENSC_STAGED_FP64

@@ -505,7 +505,7 @@ __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_MIXED)
 // from the stage while the next tile's copies are in flight.  Node data are
 // gathered from global memory as in the unstaged pass, and all outputs are
 // written there.
-constexpr int kStageTile = 128;
+constexpr int kStageTile = ENSC_STAGE_TILE_MIXED;
 // stage: 46 rows of 4-byte words (8 conn, 18 A, 6 sigma, 12 QIA, cbrt(V0),
 // eps_p), then V0 as a row of doubles
 constexpr int kStageWordRows = 46;
@@ -539,7 +539,7 @@ __device__ __forceinline__ void stage_issue(const ElemArrays& E, uint32_t dst, u
 }
 
 template <bool PLASTIC>
-__global__ void __launch_bounds__(kStageTile, 4)
+__global__ void __launch_bounds__(kStageTile, ENSC_STAGE_MINB_MIXED)
     k_element_mixed_staged(ElemArrays E, NodeArrays N, Material M, Ctl* ctl, Partials P) {
     if (ctl->done) return;
     extern __shared__ __align__(128) unsigned char smem[];
