@@ -55,6 +55,7 @@ struct ensc_batch {
     int64_t budget = 0, used = 0;
     int slots = 0;
     int64_t max_etiles = 0, max_ntiles = 0;
+    int etile = 32, ntile = 32;   // elements / nodes per tile
     // device tables (one allocation)
     void* tables = nullptr;
     ensc::InstanceDesc* d_desc = nullptr;
@@ -127,13 +128,13 @@ int rebuild_tables(ensc_batch* b) {
         d.M = sl.M;
         d.active = 1;
         d.e_tile0 = static_cast<int32_t>(ei.size());
-        for (int64_t e = 0; e < sl.ne; e += ensc::kTile) {
+        for (int64_t e = 0; e < sl.ne; e += b->etile) {
             ei.push_back(s);
             eb.push_back(static_cast<int32_t>(e));
         }
         d.e_ntiles = static_cast<int32_t>(ei.size()) - d.e_tile0;
         d.n_tile0 = static_cast<int32_t>(ni.size());
-        for (int64_t n = 0; n < sl.nn; n += ensc::kTile) {
+        for (int64_t n = 0; n < sl.nn; n += b->ntile) {
             ni.push_back(s);
             nb.push_back(static_cast<int32_t>(n));
         }
@@ -253,8 +254,10 @@ int ensc_batch_create(const ensc_params* params, int32_t max_instances, int64_t 
     b->budget = budget_bytes;
     b->slots = max_instances;
     // tiles: every instance rounds its element and node counts up to tiles
-    b->max_etiles = max_elements / ensc::kTile + max_instances + 1;
-    b->max_ntiles = max_nodes / ensc::kTile + max_instances + 1;
+    b->etile = ensc::batch_element_tile(params->precision == ENSC_MIXED);
+    b->ntile = ensc::batch_node_tile(params->precision == ENSC_MIXED);
+    b->max_etiles = max_elements / b->etile + max_instances + 1;
+    b->max_ntiles = max_nodes / b->ntile + max_instances + 1;
     b->inst.resize(static_cast<size_t>(max_instances));
     if (params->graph_chunk > 0) {
         b->fixed_chunk = static_cast<int>(std::min<int64_t>(params->graph_chunk, 1024));
@@ -332,6 +335,8 @@ int ensc_batch_create(const ensc_params* params, int32_t max_instances, int64_t 
     b->T.counts = b->d_counts;
     b->T.etile_part = b->d_etile_part;
     b->T.ntile_part = b->d_ntile_part;
+    b->T.etile = b->etile;
+    b->T.ntile = b->ntile;
     int rc = rebuild_tables(b);
     if (rc) return fail(rc);
     *out = b;
@@ -356,7 +361,7 @@ int ensc_batch_add(ensc_batch* b, const ensc_mesh_desc* mesh, const ensc_materia
     if (rc) return berr(b, rc, perr);
     if (b->used + static_cast<int64_t>(ih.bytes) > b->budget)
         return berr(b, ENSC_ERR_OOM, "instance does not fit the batch's memory budget");
-    const int64_t et = (ih.ne + ensc::kTile - 1) / ensc::kTile, nt = (ih.nn + ensc::kTile - 1) / ensc::kTile;
+    const int64_t et = (ih.ne + b->etile - 1) / b->etile, nt = (ih.nn + b->ntile - 1) / b->ntile;
     if (b->n_etiles + et > b->max_etiles || b->n_ntiles + nt > b->max_ntiles)
         return berr(b, ENSC_ERR_OOM, "batch tile capacity exceeded");
     Slot& sl = b->inst[s];

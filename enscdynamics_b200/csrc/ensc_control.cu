@@ -303,7 +303,7 @@ __global__ void __launch_bounds__(kCtlThreads) k_between_batch(BatchTables T, in
 }
 
 // Minimum element edge for the instances whose cycle may hit the total-time
-// clamp (see k_edge_prepass), one warp per element tile.
+// clamp (see k_edge_prepass), one warp per element tile of T.etile elements.
 __global__ void __launch_bounds__(128) k_edge_prepass_batch(BatchTables T) {
     const int lane = threadIdx.x & 31;
     const int warp = static_cast<int>((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
@@ -312,9 +312,10 @@ __global__ void __launch_bounds__(128) k_edge_prepass_batch(BatchTables T) {
         const InstanceDesc& d = T.desc[T.etile_inst[t]];
         Ctl* ctl = d.ctl;
         if (ctl->done || !ctl->need_exact) continue;
-        const int64_t e = static_cast<int64_t>(T.etile_base[t]) + lane;
+        const int64_t base = T.etile_base[t];
+        const int64_t end = base + T.etile < d.E.ne ? base + T.etile : d.E.ne;
         double m = DBL_MAX;
-        if (e < d.E.ne) {
+        for (int64_t e = base + lane; e < end; e += 32) {
             const int64_t ep = d.E.ne_pad, np = d.N.nn_pad;
             double xyz[8][3];
 #pragma unroll
@@ -335,7 +336,8 @@ __global__ void __launch_bounds__(128) k_edge_prepass_batch(BatchTables T) {
                 const double tt = __fma_rn(dz, dz, __fma_rn(dy, dy, dx * dx));  // as the element pass
                 mm = tt < mm ? tt : mm;
             }
-            m = sqrt(mm);
+            const double len = sqrt(mm);
+            m = len < m ? len : m;
         }
         unsigned long long b = ord_bits(m);
         for (int o = 16; o > 0; o >>= 1) {

@@ -147,6 +147,7 @@ struct BatchTables {
     const int32_t* counts;       // [0] element tiles, [1] node tiles, [2] slots in use
     double* etile_part;          // [etiles][3] internal / hourglass / viscous work per tile
     double* ntile_part;          // [ntiles][2] kinetic / external work per tile
+    int32_t etile, ntile;        // elements / nodes per tile
 };
 
 // Amplitude factor of gravity in a cycle at `time` with step dt, as

@@ -788,10 +788,14 @@ __global__ void __launch_bounds__(kNodeThreads, ENSC_NODE_MINB_FP64) k_node(Elem
 
 
 // ---- batched instances --------------------------------------------------------
-// One warp per 32-element (32-node) tile; each tile belongs to one instance,
-// whose arrays, material and control block come from the instance table.
-// Per-tile work sums are written to a tile-indexed buffer and folded per
-// instance in tile order, so the totals do not depend on scheduling.
+// Element tiles of kStageTileF64 elements and node tiles of
+// 32 * kNodeGroupFp64 nodes, each inside one instance whose arrays, material
+// and control block come from the instance table.  The element pass runs the
+// staged pipeline over the tile list, one tile per block at a time; the node
+// pass gives each node tile to one warp.  Per-tile work sums are written to a
+// tile-indexed buffer and folded per instance in tile order, so the totals
+// do not depend on scheduling.  Arithmetic per element and node is that of
+// the single-instance kernels, so states are bit-identical to them.
 __device__ __forceinline__ double warp_sum_b(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -807,48 +811,122 @@ __device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v)
     return v;
 }
 
-__global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_FP64) k_element_batch_fp64(BatchTables T) {
-    const int lane = threadIdx.x & 31;
-    const int warp = static_cast<int>((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
-    const int nwarps = static_cast<int>((static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5);
-    const int ntiles = T.counts[0];
-    for (int t = warp; t < ntiles; t += nwarps) {
-        const int slot = T.etile_inst[t];
-        const InstanceDesc& d = T.desc[slot];
+// Tiles of instances that are done are not copied: their stage's phase is
+// completed by a plain arrival (done cannot change during the pass).
+__device__ __forceinline__ void f64_batch_stage_issue(const BatchTables& T, int64_t t, uint32_t dst, uint32_t bar) {
+    const InstanceDesc& d = T.desc[T.etile_inst[t]];
+    if (d.ctl->done) mbar_arrive(bar);
+    else if (d.M.plastic) f64_stage_issue<true, true>(d.E, dst, bar, T.etile_base[t]);
+    else f64_stage_issue<false, true>(d.E, dst, bar, T.etile_base[t]);
+}
+
+__global__ void __launch_bounds__(kStageTileF64, 2) k_element_batch_fp64(BatchTables T) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    constexpr int TT = kStageTileF64;
+    constexpr int NW = TT / 32;
+    constexpr uint32_t SB = f64_stage_bytes<true>();
+    __shared__ double red_e[3][NW];
+    __shared__ unsigned long long red_m[2][NW];
+    __shared__ int red_bad[NW];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const uint32_t stage0 = smem_addr(smem);
+    const uint32_t bar0 = stage0 + 2 * SB;
+    const int64_t ntiles = T.counts[0];
+    const int64_t gstride = gridDim.x;
+    if (tid == 0) {
+        mbar_init(bar0, 1);
+        mbar_init(bar0 + 8, 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (int s = 0; s < 2; ++s) {
+            const int64_t t = blockIdx.x + s * gstride;
+            if (t < ntiles) f64_batch_stage_issue(T, t, stage0 + s * SB, bar0 + 8 * s);
+        }
+    }
+    bool timed_out = false;
+    int it = 0;
+    int64_t t = blockIdx.x;
+    for (; t < ntiles; t += gstride, ++it) {
+        const int s = it & 1;
+        const uint32_t bar = bar0 + 8 * s;
+        const bool ok = mbar_wait_bounded(bar, (it >> 1) & 1);
+        if (__syncthreads_or(!ok)) {
+            timed_out = true;
+            break;
+        }
+        const InstanceDesc& d = T.desc[T.etile_inst[t]];
         Ctl* ctl = d.ctl;
-        double* part = T.etile_part + 3 * static_cast<int64_t>(t);
-        if (ctl->done) {
-            if (lane < 3) part[lane] = 0.0;
-            continue;
-        }
-        const double dt1 = ctl->dt_i_1;
-        const int64_t e = static_cast<int64_t>(T.etile_base[t]) + lane;
-        double dts = DBL_MAX, len = DBL_MAX;
-        double ei = 0.0, eh = 0.0, ev = 0.0;
+        const bool live = !ctl->done;
+        double ei = 0.0, eh = 0.0, ev = 0.0, dts = DBL_MAX, len = DBL_MAX;
         int32_t bad = 0;
-        if (e < d.E.ne) {
-            const Fp64Src S = fp64_src_global(d.E, e);
-            if (d.M.plastic) element_body<true, false>(d.E, d.N, d.M, S, dt1, e, dts, len, ei, eh, ev, bad);
-            else element_body<false, false>(d.E, d.N, d.M, S, dt1, e, dts, len, ei, eh, ev, bad);
+        const int64_t e = static_cast<int64_t>(T.etile_base[t]) + tid;
+        if (live && e < d.E.ne) {
+            const double dt1 = ctl->dt_i_1;
+            const unsigned char* st = smem + s * SB;
+            const double* dr = reinterpret_cast<const double*>(st + 8 * TT * 4);
+            const Fp64Src S{reinterpret_cast<const uint32_t*>(st), dr, dr + 6 * TT, dr + 18 * TT, dr + 19 * TT,
+                            dr + 20 * TT, dr + 21 * TT, TT, tid, dr + kF64StageRows * TT, TT, tid};
+            if (d.M.plastic) element_body<true, false, true, true>(d.E, d.N, d.M, S, dt1, e, dts, len, ei, eh, ev, bad);
+            else element_body<false, false, true, true>(d.E, d.N, d.M, S, dt1, e, dts, len, ei, eh, ev, bad);
         }
-        const unsigned long long dmin = warp_min_u64(ord_bits(static_cast<double>(dts)));
-        const unsigned long long lmin = warp_min_u64(ord_bits(static_cast<double>(len)));
+        // the tile's sums and minima (fixed order: lanes, then warps)
         ei = warp_sum_b(ei);
         eh = warp_sum_b(eh);
         ev = warp_sum_b(ev);
+        const unsigned long long dmin = warp_min_u64(ord_bits(dts));
+        const unsigned long long lmin = warp_min_u64(ord_bits(len));
         bad = static_cast<int32_t>(__reduce_or_sync(0xffffffffu, static_cast<unsigned>(bad)));
         if (lane == 0) {
-            atomicMin(&ctl->dts_next, dmin);
-            atomicMin(&ctl->len_min, lmin);
-            if (bad) atomicOr(&ctl->status, bad);
-            part[0] = ei;
-            part[1] = eh;
-            part[2] = ev;
+            red_e[0][wid] = ei;
+            red_e[1][wid] = eh;
+            red_e[2][wid] = ev;
+            red_m[0][wid] = dmin;
+            red_m[1][wid] = lmin;
+            red_bad[wid] = bad;
+        }
+        __syncthreads();  // also: the block is done with stage s
+        if (tid == 0) {
+            double se[3] = {0.0, 0.0, 0.0};
+            unsigned long long md = kInfBits, ml = kInfBits;
+            int32_t b = 0;
+#pragma unroll
+            for (int w = 0; w < NW; ++w) {
+#pragma unroll
+                for (int k = 0; k < 3; ++k) se[k] = se[k] + red_e[k][w];
+                md = red_m[0][w] < md ? red_m[0][w] : md;
+                ml = red_m[1][w] < ml ? red_m[1][w] : ml;
+                b |= red_bad[w];
+            }
+            double* part = T.etile_part + 3 * t;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) part[k] = se[k];
+            if (live) {
+                atomicMin(&ctl->dts_next, md);
+                atomicMin(&ctl->len_min, ml);
+                if (b) atomicOr(&ctl->status, b);
+            }
+            const int64_t tn = t + 2 * gstride;
+            if (tn < ntiles) {
+                fence_proxy_async_smem();
+                f64_batch_stage_issue(T, tn, stage0 + s * SB, bar);
+            }
+        }
+    }
+    if (timed_out && tid == 0) {
+        // record the failure on the instance whose tile could not be read and
+        // let the copies this block started land (bounded) before exiting
+        atomicOr(&T.desc[T.etile_inst[t]].ctl->status, ST_TIMEOUT);
+        for (int k = 0; k < 2; ++k) {
+            const int itk = it + k;
+            if (blockIdx.x + itk * gstride < ntiles) mbar_wait_bounded(bar0 + 8 * (itk & 1), (itk >> 1) & 1);
         }
     }
 }
 
-__global__ void __launch_bounds__(kNodeThreads) k_node_batch_fp64(BatchTables T) {
+__global__ void __launch_bounds__(kNodeThreads, ENSC_NODE_MINB_FP64) k_node_batch_fp64(BatchTables T) {
+    constexpr int W = kNodeGroupFp64;
     const int lane = threadIdx.x & 31;
     const int warp = static_cast<int>((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
     const int nwarps = static_cast<int>((static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5);
@@ -881,12 +959,20 @@ __global__ void __launch_bounds__(kNodeThreads) k_node_batch_fp64(BatchTables T)
             ctl->cycles_done += 1;
             ctl->energy_pending = 1;
         }
-        const int64_t n = static_cast<int64_t>(T.ntile_base[t]) + lane;
         const double amp =
             (d.M.gravity_on && d.M.amp_n > 0) ? gravity_amplitude(d.M.amp, d.M.amp_n, ctl->time, dt_i) : 1.0;
         double kin = 0.0, wext = 0.0;
         int32_t bad = 0;
-        if (n < d.N.nn) node_body(d.E, d.N, d.M, dt_i, dt_i_1, amp, n, kin, wext, bad);
+        const int64_t n0 = static_cast<int64_t>(T.ntile_base[t]) + static_cast<int64_t>(lane) * W;
+        const int64_t nn = d.N.nn;
+        if (n0 < nn) {
+            if (d.E.slot_major && d.E.tiles_aligned) {
+                node_group<W>(d.E, d.N, d.M, dt_i, dt_i_1, amp, n0, nn, kin, wext, bad);
+            } else {
+                for (int j = 0; j < W && n0 + j < nn; ++j)
+                    node_body(d.E, d.N, d.M, dt_i, dt_i_1, amp, n0 + j, kin, wext, bad);
+            }
+        }
         kin = warp_sum_b(kin);
         wext = warp_sum_b(wext);
         bad = static_cast<int32_t>(__reduce_or_sync(0xffffffffu, static_cast<unsigned>(bad)));
@@ -957,16 +1043,22 @@ int occupancy_node_fp64() {
 
 
 void launch_element_batch_fp64(const BatchTables& T, int grid, cudaStream_t st) {
-    k_element_batch_fp64<<<grid, kElemThreads, 0, st>>>(T);
+    k_element_batch_fp64<<<grid, kStageTileF64, f64_stage_smem<true>(), st>>>(T);
 }
 void launch_node_batch_fp64(const BatchTables& T, int grid, cudaStream_t st) {
     k_node_batch_fp64<<<grid, kNodeThreads, 0, st>>>(T);
 }
 int occupancy_element_batch_fp64() {
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_batch_fp64, kElemThreads, 0);
+    // dynamic shared memory above the default 48 KB: set on the current
+    // device before any launch or capture
+    cudaFuncSetAttribute(k_element_batch_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(f64_stage_smem<true>()));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_batch_fp64, kStageTileF64, f64_stage_smem<true>());
     return nb;
 }
+
+int batch_element_tile_fp64() { return kStageTileF64; }
 int occupancy_node_batch_fp64() {
     int nb = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_node_batch_fp64, kNodeThreads, 0);

@@ -89,6 +89,11 @@ void launch_element_batch_mixed(const BatchTables& T, int grid, cudaStream_t st)
 void launch_node_batch_mixed(const BatchTables& T, int grid, cudaStream_t st);
 int occupancy_element_batch_mixed();
 int occupancy_node_batch_mixed();
+// elements and nodes per batch tile (element tiles are the staged passes'
+// tiles; node tiles are one warp of node groups)
+int batch_element_tile(bool mixed_precision);
+int batch_element_tile_fp64();
+int batch_node_tile(bool mixed_precision);
 void launch_between_batch(const BatchTables& T, int slots, int mode, cudaStream_t st);
 void launch_edge_prepass_batch(const BatchTables& T, int grid, cudaStream_t st);
 void launch_begin_exact_batch(const BatchTables& T, int slots, cudaStream_t st);
