@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -60,10 +61,13 @@ struct ensc_batch {
     void* tables = nullptr;
     ensc::InstanceDesc* d_desc = nullptr;
     int32_t *d_etile_inst = nullptr, *d_etile_base = nullptr, *d_ntile_inst = nullptr, *d_ntile_base = nullptr;
-    int32_t* d_counts = nullptr;
+    int32_t* d_counts = nullptr;   // [0..2] tile and slot counts, [3] edge-prepass counter
     double *d_etile_part = nullptr, *d_ntile_part = nullptr;
     Ctl* d_ctl = nullptr;
     double* d_scratch = nullptr;  // partials for init / kinetic passes of one instance
+    ensc::NodeParam* d_nparam = nullptr;
+    ensc::StageHdr* d_sparam = nullptr;
+    ensc::ETileSrc* d_etile_src = nullptr;
     int scratch_blocks = 4096;
     Ctl* h_ctl = nullptr;         // pinned mirror of d_ctl
     std::vector<Slot> inst;
@@ -111,10 +115,16 @@ struct DevGuard {
 
 bool is_mixed(const ensc_batch* b) { return b->precision == ENSC_MIXED; }
 
-// Rewrites the instance table and tile lists from the live slots.
+// Rewrites the instance table and tile lists from the live slots.  The tile
+// energy accumulators are folded into the instances first (tile indices
+// change) and cleared after.
 int rebuild_tables(ensc_batch* b) {
+    ensc::launch_between_batch(b->T, b->slots, 1, b->stream);
+    BCK(b, cudaGetLastError());
     std::vector<ensc::InstanceDesc> desc(static_cast<size_t>(b->slots));
     std::vector<int32_t> ei, eb, ni, nb;
+    std::vector<ensc::ETileSrc> es;
+    const int64_t real = is_mixed(b) ? 4 : 8;
     int used_slots = 0;
     for (int s = 0; s < b->slots; ++s) {
         const Slot& sl = b->inst[s];
@@ -126,11 +136,34 @@ int rebuild_tables(ensc_batch* b) {
         d.E = sl.E;
         d.N = sl.N;
         d.M = sl.M;
+        // the batched element passes run the J2 update for every instance; an
+        // infinite yield stress leaves the elastic update bit-for-bit unchanged
+        if (!d.M.plastic) {
+            d.M.yield0 = HUGE_VAL;
+            d.M.hardening = 0.0;
+            ensc::set_mixed_consts(d.M);
+        }
         d.active = 1;
         d.e_tile0 = static_cast<int32_t>(ei.size());
         for (int64_t e = 0; e < sl.ne; e += b->etile) {
             ei.push_back(s);
             eb.push_back(static_cast<int32_t>(e));
+            const ensc::ElemArrays& E = sl.E;
+            auto at = [e](const void* p, int64_t size) { return static_cast<const void*>(static_cast<const char*>(p) + e * size); };
+            ensc::ETileSrc t{};
+            t.conn = at(E.conn, 4);
+            t.bt = at(E.bt, real);
+            t.vol0 = at(E.vol0, 8);
+            t.cbrt_v0 = at(E.cbrt_v0, real);  // mixed: a float copy in the first words
+            t.cbrt_v0sq = at(E.cbrt_v0sq, 8);
+            t.sigma = at(E.sigma, real);
+            t.qia = at(E.qia, real);
+            t.eps_p = at(E.eps_p, real);
+            t.ne_pad = static_cast<int32_t>(E.ne_pad);
+            t.cnt = static_cast<int32_t>(std::min<int64_t>(E.ne_pad - e, b->etile));
+            t.slot = s;
+            t.base = static_cast<int32_t>(e);
+            es.push_back(t);
         }
         d.e_ntiles = static_cast<int32_t>(ei.size()) - d.e_tile0;
         d.n_tile0 = static_cast<int32_t>(ni.size());
@@ -148,12 +181,16 @@ int rebuild_tables(ensc_batch* b) {
     if (!ei.empty()) {
         BCK(b, cudaMemcpyAsync(b->d_etile_inst, ei.data(), ei.size() * 4, cudaMemcpyHostToDevice, b->stream));
         BCK(b, cudaMemcpyAsync(b->d_etile_base, eb.data(), eb.size() * 4, cudaMemcpyHostToDevice, b->stream));
+        BCK(b, cudaMemcpyAsync(b->d_etile_src, es.data(), es.size() * sizeof(ensc::ETileSrc), cudaMemcpyHostToDevice,
+                               b->stream));
     }
     if (!ni.empty()) {
         BCK(b, cudaMemcpyAsync(b->d_ntile_inst, ni.data(), ni.size() * 4, cudaMemcpyHostToDevice, b->stream));
         BCK(b, cudaMemcpyAsync(b->d_ntile_base, nb.data(), nb.size() * 4, cudaMemcpyHostToDevice, b->stream));
     }
     BCK(b, cudaMemcpyAsync(b->d_counts, counts, sizeof(counts), cudaMemcpyHostToDevice, b->stream));
+    BCK(b, cudaMemsetAsync(b->d_etile_part, 0, sizeof(double) * 3 * b->max_etiles * (b->etile / 32), b->stream));
+    BCK(b, cudaMemsetAsync(b->d_ntile_part, 0, sizeof(double) * 2 * b->max_ntiles, b->stream));
     BCK(b, cudaStreamSynchronize(b->stream));
     b->n_etiles = static_cast<int64_t>(ei.size());
     b->n_ntiles = static_cast<int64_t>(ni.size());
@@ -167,9 +204,11 @@ void launch_cycle(ensc_batch* b, int ge, int gn, cudaStream_t st) {
     ensc::launch_begin_exact_batch(b->T, b->slots, st);
     if (is_mixed(b)) {
         ensc::launch_element_batch_mixed(b->T, ge, st);
+        ensc::launch_node_params_batch(b->T, b->slots, st);
         ensc::launch_node_batch_mixed(b->T, gn, st);
     } else {
         ensc::launch_element_batch_fp64(b->T, ge, st);
+        ensc::launch_node_params_batch(b->T, b->slots, st);
         ensc::launch_node_batch_fp64(b->T, gn, st);
     }
 }
@@ -294,10 +333,12 @@ int ensc_batch_create(const ensc_params* params, int32_t max_instances, int64_t 
     // tables
     auto al = [](size_t x) { return (x + 255) / 256 * 256; };
     const size_t s_desc = al(sizeof(ensc::InstanceDesc) * b->slots), s_et = al(4 * b->max_etiles),
-                 s_nt = al(4 * b->max_ntiles), s_cnt = 256, s_ep = al(8 * 3 * b->max_etiles),
+                 s_nt = al(4 * b->max_ntiles), s_cnt = 256, s_ep = al(8 * 3 * b->max_etiles * (b->etile / 32)),
                  s_np = al(8 * 2 * b->max_ntiles), s_ctl = al(sizeof(Ctl) * b->slots),
-                 s_scr = al(8 * 3 * static_cast<size_t>(b->scratch_blocks));
-    const size_t total = s_desc + 2 * s_et + 2 * s_nt + s_cnt + s_ep + s_np + s_ctl + s_scr;
+                 s_scr = al(8 * 3 * static_cast<size_t>(b->scratch_blocks)),
+                 s_nprm = al(sizeof(ensc::NodeParam) * b->slots), s_sprm = al(sizeof(ensc::StageHdr) * b->slots),
+                 s_esrc = al(sizeof(ensc::ETileSrc) * b->max_etiles);
+    const size_t total = s_desc + 2 * s_et + 2 * s_nt + s_cnt + s_ep + s_np + s_ctl + s_scr + s_nprm + s_sprm + s_esrc;
     e = cudaMalloc(&b->tables, total);
     if (e != cudaSuccess) return fail(bcuda(b, "cudaMalloc(batch tables)", e));
     cudaMemset(b->tables, 0, total);
@@ -321,6 +362,12 @@ int ensc_batch_create(const ensc_params* params, int32_t max_instances, int64_t 
     b->d_ctl = reinterpret_cast<Ctl*>(p);
     p += s_ctl;
     b->d_scratch = reinterpret_cast<double*>(p);
+    p += s_scr;
+    b->d_nparam = reinterpret_cast<ensc::NodeParam*>(p);
+    p += s_nprm;
+    b->d_sparam = reinterpret_cast<ensc::StageHdr*>(p);
+    p += s_sprm;
+    b->d_etile_src = reinterpret_cast<ensc::ETileSrc*>(p);
     e = cudaMallocHost(reinterpret_cast<void**>(&b->h_ctl), sizeof(Ctl) * b->slots);
     if (e != cudaSuccess) return fail(bcuda(b, "cudaMallocHost(ctl)", e));
     std::memset(b->h_ctl, 0, sizeof(Ctl) * b->slots);
@@ -337,6 +384,10 @@ int ensc_batch_create(const ensc_params* params, int32_t max_instances, int64_t 
     b->T.ntile_part = b->d_ntile_part;
     b->T.etile = b->etile;
     b->T.ntile = b->ntile;
+    b->T.exact_count = b->d_counts + 3;
+    b->T.nparam = b->d_nparam;
+    b->T.sparam = b->d_sparam;
+    b->T.etile_src = b->d_etile_src;
     int rc = rebuild_tables(b);
     if (rc) return fail(rc);
     *out = b;

@@ -266,45 +266,103 @@ __global__ void k_aos_to_soa(const double* aos, int64_t n, int64_t pad, int comp
     }
 }
 
-// ---- batched instances: one block per instance slot ------------------------
-// Folds the instance's tile partials of the last cycle in tile order and, in
-// mode 0, begins its next cycle exactly as k_between does for one instance;
-// mode 1 folds and marks instances that have reached their limits as done.
-__global__ void __launch_bounds__(kCtlThreads) k_between_batch(BatchTables T, int mode) {
+// ---- batched instances ---------------------------------------------------------
+// Begins every instance's next cycle exactly as k_between does for one
+// instance (one thread per instance slot), after marking instances that have
+// reached their limits as done, and counts the instances whose cycle needs
+// the edge prepass.  The energy terms stay in the per-tile accumulators
+// until k_fold_batch.  Each slot's element-pass scalars (dt_i_1, live) go to
+// T.sparam; k_begin_exact_batch rewrites them where the prepass decides dt.
+__global__ void k_begin_batch(BatchTables T, int begin) {
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= T.counts[2]) return;
+    const InstanceDesc& d = T.desc[slot];
+    StageHdr h{0.0, 0, 0};
+    if (d.active) {
+        Ctl* ctl = d.ctl;
+        if (!ctl->done) {
+            if (ctl->status || !(ctl->time < ctl->step_end) || ctl->cycles_done >= ctl->cycles_target ||
+                !(ctl->time < ctl->pause_time)) {
+                ctl->done = 1;
+            } else if (begin) {
+                cycle_begin(ctl);
+                if (ctl->need_exact) atomicAdd(T.exact_count, 1);
+                h.dt1 = ctl->dt_i_1;
+                h.live = 1;
+            }
+        }
+    }
+    T.sparam[slot] = h;
+}
+
+// Folds an instance's tile accumulators into its control block (one block
+// per instance slot, tiles in order): the work terms are added and the tile
+// accumulators cleared; the kinetic energy is the sum of the tiles' latest
+// values when cycles ran since the last fold.
+__global__ void __launch_bounds__(kCtlThreads) k_fold_batch(BatchTables T) {
     const int slot = blockIdx.x;
     if (slot >= T.counts[2]) return;
     const InstanceDesc& d = T.desc[slot];
     if (!d.active) return;
     Ctl* ctl = d.ctl;
-    if (ctl->energy_pending) {
-        const double ei = fixed_sum_strided(T.etile_part + 3 * static_cast<int64_t>(d.e_tile0) + 0, d.e_ntiles, 3);
-        const double eh = fixed_sum_strided(T.etile_part + 3 * static_cast<int64_t>(d.e_tile0) + 1, d.e_ntiles, 3);
-        const double ev = fixed_sum_strided(T.etile_part + 3 * static_cast<int64_t>(d.e_tile0) + 2, d.e_ntiles, 3);
-        const double kin = fixed_sum_strided(T.ntile_part + 2 * static_cast<int64_t>(d.n_tile0) + 0, d.n_ntiles, 2);
-        const double wx = fixed_sum_strided(T.ntile_part + 2 * static_cast<int64_t>(d.n_tile0) + 1, d.n_ntiles, 2);
-        if (threadIdx.x == 0) {
-            ctl->energy[0] = kin;
-            ctl->energy[1] += ei;
-            ctl->energy[2] += eh;
-            ctl->energy[3] += ev;
-            ctl->energy[4] += wx;
-            ctl->energy_pending = 0;
+    const int nw = T.etile / 32;  // element-tile partials: one per warp
+    const int ne_part = d.e_ntiles * nw;
+    double* ep = T.etile_part + 3 * static_cast<int64_t>(d.e_tile0) * nw;
+    double* np = T.ntile_part + 2 * static_cast<int64_t>(d.n_tile0);
+    const double ei = fixed_sum_strided(ep + 0, ne_part, 3);
+    const double eh = fixed_sum_strided(ep + 1, ne_part, 3);
+    const double ev = fixed_sum_strided(ep + 2, ne_part, 3);
+    const double kin = fixed_sum_strided(np + 0, d.n_ntiles, 2);
+    const double wx = fixed_sum_strided(np + 1, d.n_ntiles, 2);
+    for (int i = threadIdx.x; i < 3 * ne_part; i += kCtlThreads) ep[i] = 0.0;
+    for (int i = threadIdx.x; i < d.n_ntiles; i += kCtlThreads) np[2 * i + 1] = 0.0;
+    if (threadIdx.x == 0) {
+        if (ctl->energy_pending) ctl->energy[0] = kin;
+        ctl->energy[1] += ei;
+        ctl->energy[2] += eh;
+        ctl->energy[3] += ev;
+        ctl->energy[4] += wx;
+        ctl->energy_pending = 0;
+    }
+}
+
+// The node pass's scalars of every instance (one thread per slot): this
+// cycle's stable dt (update_minVertex_perMaterial_and_dt,
+// exDyna3D.cpp:673-679, as k_node computes it), the previous dt and the
+// gravity amplitude; also the control-block updates k_node makes.
+__global__ void k_node_params_batch(BatchTables T) {
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= T.counts[2]) return;
+    const InstanceDesc& d = T.desc[slot];
+    NodeParam p{0.0, 0.0, 1.0, 0, 0};
+    Ctl* ctl = d.ctl;
+    if (d.active && !ctl->done) {
+        double dt_i;
+        const int dt_final = ctl->dt_final;
+        if (dt_final) {
+            dt_i = ctl->dt_i;
+        } else {
+            double dd = bits_ord(ctl->len_min) / ctl->wos;
+            const double tmp = ctl->dts_cur;
+            dd = dd < tmp ? dd : tmp;
+            dt_i = dd * ctl->factor;
         }
+        if (!(dt_i > 0.0) || !isfinite(dt_i)) atomicOr(&ctl->status, ST_BAD_DT);
+        if (!dt_final) ctl->dt_i = dt_i;
+        ctl->cycles_done += 1;
+        ctl->energy_pending = 1;
+        p.dt_i = dt_i;
+        p.dt_i_1 = ctl->dt_i_1;
+        p.amp = (d.M.gravity_on && d.M.amp_n > 0) ? gravity_amplitude(d.M.amp, d.M.amp_n, ctl->time, dt_i) : 1.0;
+        p.live = 1;
     }
-    if (threadIdx.x != 0 || ctl->done) return;
-    // an instance that has reached its limits is marked done here in both
-    // modes, so that a sync right after its last cycle reports it finished
-    if (ctl->status || !(ctl->time < ctl->step_end) || ctl->cycles_done >= ctl->cycles_target ||
-        !(ctl->time < ctl->pause_time)) {
-        ctl->done = 1;
-        return;
-    }
-    if (mode == 0) cycle_begin(ctl);
+    T.nparam[slot] = p;
 }
 
 // Minimum element edge for the instances whose cycle may hit the total-time
 // clamp (see k_edge_prepass), one warp per element tile of T.etile elements.
 __global__ void __launch_bounds__(128) k_edge_prepass_batch(BatchTables T) {
+    if (*T.exact_count == 0) return;
     const int lane = threadIdx.x & 31;
     const int warp = static_cast<int>((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
     const int nwarps = static_cast<int>((static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5);
@@ -349,6 +407,7 @@ __global__ void __launch_bounds__(128) k_edge_prepass_batch(BatchTables T) {
 }
 
 __global__ void k_begin_exact_batch(BatchTables T) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) *T.exact_count = 0;  // the prepass has read it
     const int slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= T.counts[2]) return;
     const InstanceDesc& d = T.desc[slot];
@@ -356,6 +415,7 @@ __global__ void k_begin_exact_batch(BatchTables T) {
     Ctl* ctl = d.ctl;
     if (ctl->done || !ctl->need_exact) return;
     begin_exact(ctl);
+    T.sparam[slot].dt1 = ctl->dt_i_1;
 }
 
 int grid_for(int64_t work, int threads) {
@@ -366,7 +426,11 @@ int grid_for(int64_t work, int threads) {
 }  // namespace
 
 void launch_between_batch(const BatchTables& T, int slots, int mode, cudaStream_t st) {
-    k_between_batch<<<slots, kCtlThreads, 0, st>>>(T, mode);
+    if (mode == 1) k_fold_batch<<<slots, kCtlThreads, 0, st>>>(T);
+    k_begin_batch<<<(slots + 127) / 128, 128, 0, st>>>(T, mode == 0 ? 1 : 0);
+}
+void launch_node_params_batch(const BatchTables& T, int slots, cudaStream_t st) {
+    k_node_params_batch<<<(slots + 127) / 128, 128, 0, st>>>(T);
 }
 void launch_edge_prepass_batch(const BatchTables& T, int grid, cudaStream_t st) {
     k_edge_prepass_batch<<<grid, 128, 0, st>>>(T);

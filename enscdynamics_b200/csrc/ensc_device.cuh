@@ -25,6 +25,7 @@
 //                                    same slot in more than one element
 #pragma once
 
+#include <cmath>
 #include <cstring>
 
 #include <cstdint>
@@ -63,6 +64,14 @@ struct Ctl {
     double energy[6];          // kinetic, internal, hourglass, viscous, external, kinetic0
 };
 
+// FP32 constants of the mixed-precision element pass, derived once per
+// instance on the host (set_mixed_consts).  lambda and 2G are float pairs
+// (hi + lo); DRc and CRc are the per-element-invariant factors of the
+// hourglass stiffness and damping (Element_HexN8.cpp hourglass terms).
+struct MixedConsts {
+    float G, lam_hi, lam_lo, g2_hi, g2_lo, rho, wos, cvisl, cvisq, y0, H, DRc, CRc, pad[3];
+};
+
 struct Material {
     double E, nu, rho, G, K, lambda, wos;
     double yield0, hardening;
@@ -73,7 +82,28 @@ struct Material {
     // gravity amplitude table: amp_n (time, value) pairs in device memory
     const double* amp;
     int32_t amp_n;
+    MixedConsts mc;
 };
+
+// Fills M.mc from the FP64 material and controls; call after every change
+// of them.
+inline void set_mixed_consts(Material& M) {
+    MixedConsts& c = M.mc;
+    c = MixedConsts{};
+    c.G = static_cast<float>(M.G);
+    c.lam_hi = static_cast<float>(M.lambda);
+    c.lam_lo = static_cast<float>(M.lambda - static_cast<double>(c.lam_hi));
+    c.g2_hi = static_cast<float>(2.0 * M.G);
+    c.g2_lo = static_cast<float>(2.0 * M.G - static_cast<double>(c.g2_hi));
+    c.rho = static_cast<float>(M.rho);
+    c.wos = static_cast<float>(M.wos);
+    c.cvisl = static_cast<float>(M.cvisl);
+    c.cvisq = static_cast<float>(M.cvisq);
+    c.y0 = static_cast<float>(M.yield0);
+    c.H = static_cast<float>(M.hardening);
+    c.DRc = static_cast<float>(M.c_dr * (4.0 / 3.0 * M.G + M.K) * 0.1 / std::sqrt(8.0));
+    c.CRc = static_cast<float>(M.c_cr * M.rho * M.wos / 4.0);
+}
 
 struct ElemArrays {
     int64_t ne, ne_pad;
@@ -127,7 +157,47 @@ struct Partials {
 // clock and reductions are warp-uniform.
 constexpr int kTile = 32;
 
-struct InstanceDesc {
+// The scalars of an instance's node pass in the current cycle (stable dt,
+// previous dt, gravity amplitude), computed once per instance.
+struct NodeParam {
+    double dt_i, dt_i_1, amp;
+    int32_t live, pad;
+};
+
+// The scalars of an instance's element pass in the current cycle (dt_i_1,
+// and whether it runs), written per slot at the start of the cycle and
+// bulk-copied into the stage of each of its element tiles.
+struct StageHdr {
+    double dt1;
+    int32_t live, pad;
+};
+
+// Where the staged batch element passes copy an element tile from: the
+// instance's element rows, each pointer already at the tile's first element.
+// A tile's record travels with the stage of the tile two visits earlier, so
+// the block that copies a tile reads its record from shared memory.
+struct alignas(16) ETileSrc {
+    const void* conn;
+    const void* bt;
+    const void* vol0;
+    const void* cbrt_v0;
+    const void* cbrt_v0sq;
+    const void* sigma;
+    const void* qia;
+    const void* eps_p;
+    int32_t ne_pad;   // row stride in elements
+    int32_t cnt;      // entries copied per row (tile size, or the rest of the padded rows)
+    int32_t slot, base;
+};
+static_assert(sizeof(ETileSrc) == 80, "tile records are bulk-copied");
+
+// Written into each stage by the thread that fills it: the tile's instance
+// slot and first element.
+struct TileInfo {
+    int32_t slot, base, pad0, pad1;
+};
+
+struct alignas(16) InstanceDesc {
     ElemArrays E;
     NodeArrays N;
     Material M;
@@ -145,10 +215,17 @@ struct BatchTables {
     const int32_t* ntile_inst;   // [ntiles]
     const int32_t* ntile_base;
     const int32_t* counts;       // [0] element tiles, [1] node tiles, [2] slots in use
-    double* etile_part;          // [etiles][3] internal / hourglass / viscous work per tile
-    double* ntile_part;          // [ntiles][2] kinetic / external work per tile
+    // per-tile energy terms: work done since the last fold (internal,
+    // hourglass, viscous; external) and the latest kinetic energy
+    double* etile_part;          // [etiles][etile / 32][3] internal / hourglass / viscous work per tile warp
+    double* ntile_part;          // [ntiles][2] kinetic energy / external work per tile
+    int32_t* exact_count;        // instances whose current cycle needs the edge prepass
+    NodeParam* nparam;           // [slots] this cycle's node-pass scalars
+    StageHdr* sparam;            // [slots] this cycle's element-pass scalars
+    const ETileSrc* etile_src;   // [etiles] copy sources of each element tile
     int32_t etile, ntile;        // elements / nodes per tile
 };
+static_assert(sizeof(InstanceDesc) % 16 == 0, "instance descriptors are bulk-copied");
 
 // Amplitude factor of gravity in a cycle at `time` with step dt, as
 // exDyna3D::deal_amp computes it (exDyna3D.cpp:1222-1278), behaviour kept as

@@ -570,19 +570,32 @@ __device__ __forceinline__ const double* f64_stage_row(const ElemArrays& E, int 
 // Thread 0: the tile starting at element `base` into the stage at shared
 // address dst, completing on bar (rows padded to 32 entries and 256-byte
 // aligned: every copy is 16-byte aligned and a multiple of 128 bytes).
-template <bool PLASTIC, bool BT>
-__device__ __forceinline__ void f64_stage_issue(const ElemArrays& E, uint32_t dst, uint32_t bar, int64_t base) {
+__device__ __forceinline__ uint32_t f64_stage_count(const ElemArrays& E, int64_t base) {
     const int64_t left = E.ne_pad - base;
-    const uint32_t cnt = static_cast<uint32_t>(left < kStageTileF64 ? left : kStageTileF64);
+    return static_cast<uint32_t>(left < kStageTileF64 ? left : kStageTileF64);
+}
+template <bool PLASTIC, bool BT>
+__device__ __forceinline__ uint32_t f64_stage_tx_bytes(uint32_t cnt) {
     constexpr int drows = kF64StageRows + (BT ? 24 : 0);
     constexpr int dcopies = PLASTIC ? drows : drows - 1;
-    mbar_arrive_expect_tx(bar, 8u * cnt * 4u + static_cast<uint32_t>(dcopies) * cnt * 8u);
+    return 8u * cnt * 4u + static_cast<uint32_t>(dcopies) * cnt * 8u;
+}
+template <bool PLASTIC, bool BT>
+__device__ __forceinline__ void f64_stage_copies(const ElemArrays& E, uint32_t dst, uint32_t bar, int64_t base,
+                                                 uint32_t cnt) {
+    constexpr int drows = kF64StageRows + (BT ? 24 : 0);
     for (int k = 0; k < 8; ++k) bulk_g2s(dst + k * (kStageTileF64 * 4u), E.conn + k * E.ne_pad + base, cnt * 4u, bar);
     const uint32_t dbase = dst + 8u * kStageTileF64 * 4u;
     for (int r = 0; r < drows; ++r) {
         if (!PLASTIC && r == 21) continue;  // eps_p is read only with J2
         bulk_g2s(dbase + r * (kStageTileF64 * 8u), f64_stage_row(E, r) + base, cnt * 8u, bar);
     }
+}
+template <bool PLASTIC, bool BT>
+__device__ __forceinline__ void f64_stage_issue(const ElemArrays& E, uint32_t dst, uint32_t bar, int64_t base) {
+    const uint32_t cnt = f64_stage_count(E, base);
+    mbar_arrive_expect_tx(bar, f64_stage_tx_bytes<PLASTIC, BT>(cnt));
+    f64_stage_copies<PLASTIC, BT>(E, dst, bar, base, cnt);
 }
 
 template <bool PLASTIC, bool BT>
@@ -792,9 +805,10 @@ __global__ void __launch_bounds__(kNodeThreads, ENSC_NODE_MINB_FP64) k_node(Elem
 // 32 * kNodeGroupFp64 nodes, each inside one instance whose arrays, material
 // and control block come from the instance table.  The element pass runs the
 // staged pipeline over the tile list, one tile per block at a time; the node
-// pass gives each node tile to one warp.  Per-tile work sums are written to a
-// tile-indexed buffer and folded per instance in tile order, so the totals
-// do not depend on scheduling.  Arithmetic per element and node is that of
+// pass gives each node tile to one warp.  Each tile accumulates its work terms across
+// cycles (one owner per tile and pass) and keeps its latest kinetic energy;
+// k_fold_batch folds them per instance in tile order, so the totals do not
+// depend on scheduling.  Arithmetic per element and node is that of
 // the single-instance kernels, so states are bit-identical to them.
 __device__ __forceinline__ double warp_sum_b(double v) {
 #pragma unroll
@@ -811,23 +825,42 @@ __device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v)
     return v;
 }
 
-// Tiles of instances that are done are not copied: their stage's phase is
-// completed by a plain arrival (done cannot change during the pass).
-__device__ __forceinline__ void f64_batch_stage_issue(const BatchTables& T, int64_t t, uint32_t dst, uint32_t bar) {
-    const InstanceDesc& d = T.desc[T.etile_inst[t]];
-    if (d.ctl->done) mbar_arrive(bar);
-    else if (d.M.plastic) f64_stage_issue<true, true>(d.E, dst, bar, T.etile_base[t]);
-    else f64_stage_issue<false, true>(d.E, dst, bar, T.etile_base[t]);
+// A batch stage: the single-instance stage (B0^T included) followed by the
+// tile's instance descriptor, so that the element body reads arrays and
+// material from shared memory.  Tiles of instances that are done get only the
+// descriptor (done cannot change during the pass).
+constexpr uint32_t kF64BatchStageBytes = f64_stage_bytes<true>() + (sizeof(InstanceDesc) + 127) / 128 * 128;
+constexpr size_t kF64BatchStageSmem = 2 * static_cast<size_t>(kF64BatchStageBytes) + 16;
+static_assert(sizeof(InstanceDesc) + sizeof(StageHdr) <= kF64BatchStageBytes - f64_stage_bytes<true>(), "stage tail");
+
+__device__ __forceinline__ StageHdr* f64_stage_hdr(unsigned char* smem, int s) {
+    return reinterpret_cast<StageHdr*>(smem + s * kF64BatchStageBytes + f64_stage_bytes<true>() + sizeof(InstanceDesc));
+}
+
+__device__ __forceinline__ void f64_batch_stage_issue(const BatchTables& T, int64_t t, uint32_t dst, uint32_t bar,
+                                                StageHdr* hdr) {
+    const InstanceDesc* dp = T.desc + T.etile_inst[t];
+    const Ctl* c = dp->ctl;
+    const int32_t done = c->done;
+    hdr->live = done ? 0 : 1;  // visible to the waiters through the arrive below
+    hdr->dt1 = c->dt_i_1;
+    const uint32_t db = static_cast<uint32_t>(sizeof(InstanceDesc));
+    const int64_t base = T.etile_base[t];
+    if (done) {
+        mbar_arrive_expect_tx(bar, db);
+    } else {
+        const uint32_t cnt = f64_stage_count(dp->E, base);
+        mbar_arrive_expect_tx(bar, f64_stage_tx_bytes<true, true>(cnt) + db);
+        f64_stage_copies<true, true>(dp->E, dst, bar, base, cnt);
+    }
+    bulk_g2s(dst + f64_stage_bytes<true>(), dp, db, bar);
 }
 
 __global__ void __launch_bounds__(kStageTileF64, 2) k_element_batch_fp64(BatchTables T) {
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr int TT = kStageTileF64;
     constexpr int NW = TT / 32;
-    constexpr uint32_t SB = f64_stage_bytes<true>();
-    __shared__ double red_e[3][NW];
-    __shared__ unsigned long long red_m[2][NW];
-    __shared__ int red_bad[NW];
+    constexpr uint32_t SB = kF64BatchStageBytes;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const uint32_t stage0 = smem_addr(smem);
     const uint32_t bar0 = stage0 + 2 * SB;
@@ -842,7 +875,7 @@ __global__ void __launch_bounds__(kStageTileF64, 2) k_element_batch_fp64(BatchTa
     if (tid == 0) {
         for (int s = 0; s < 2; ++s) {
             const int64_t t = blockIdx.x + s * gstride;
-            if (t < ntiles) f64_batch_stage_issue(T, t, stage0 + s * SB, bar0 + 8 * s);
+            if (t < ntiles) f64_batch_stage_issue(T, t, stage0 + s * SB, bar0 + 8 * s, f64_stage_hdr(smem, s));
         }
     }
     bool timed_out = false;
@@ -856,61 +889,44 @@ __global__ void __launch_bounds__(kStageTileF64, 2) k_element_batch_fp64(BatchTa
             timed_out = true;
             break;
         }
-        const InstanceDesc& d = T.desc[T.etile_inst[t]];
+        const unsigned char* st = smem + s * SB;
+        const InstanceDesc& d = *reinterpret_cast<const InstanceDesc*>(st + f64_stage_bytes<true>());
+        const StageHdr& h = *f64_stage_hdr(smem, s);
         Ctl* ctl = d.ctl;
-        const bool live = !ctl->done;
+        const bool live = h.live != 0;
         double ei = 0.0, eh = 0.0, ev = 0.0, dts = DBL_MAX, len = DBL_MAX;
         int32_t bad = 0;
         const int64_t e = static_cast<int64_t>(T.etile_base[t]) + tid;
         if (live && e < d.E.ne) {
-            const double dt1 = ctl->dt_i_1;
-            const unsigned char* st = smem + s * SB;
+            const double dt1 = h.dt1;
             const double* dr = reinterpret_cast<const double*>(st + 8 * TT * 4);
             const Fp64Src S{reinterpret_cast<const uint32_t*>(st), dr, dr + 6 * TT, dr + 18 * TT, dr + 19 * TT,
                             dr + 20 * TT, dr + 21 * TT, TT, tid, dr + kF64StageRows * TT, TT, tid};
-            if (d.M.plastic) element_body<true, false, true, true>(d.E, d.N, d.M, S, dt1, e, dts, len, ei, eh, ev, bad);
-            else element_body<false, false, true, true>(d.E, d.N, d.M, S, dt1, e, dts, len, ei, eh, ev, bad);
+            element_body<true, false, true, true>(d.E, d.N, d.M, S, dt1, e, dts, len, ei, eh, ev, bad);
         }
-        // the tile's sums and minima (fixed order: lanes, then warps)
+        // each warp's sums go to its own slot (tile-major, warp-minor; folded
+        // in that order) and its minima to the instance's control block
         ei = warp_sum_b(ei);
         eh = warp_sum_b(eh);
         ev = warp_sum_b(ev);
         const unsigned long long dmin = warp_min_u64(ord_bits(dts));
         const unsigned long long lmin = warp_min_u64(ord_bits(len));
         bad = static_cast<int32_t>(__reduce_or_sync(0xffffffffu, static_cast<unsigned>(bad)));
-        if (lane == 0) {
-            red_e[0][wid] = ei;
-            red_e[1][wid] = eh;
-            red_e[2][wid] = ev;
-            red_m[0][wid] = dmin;
-            red_m[1][wid] = lmin;
-            red_bad[wid] = bad;
+        if (live && lane == 0) {
+            double* part = T.etile_part + 3 * (t * NW + wid);
+            part[0] += ei;
+            part[1] += eh;
+            part[2] += ev;
+            atomicMin(&ctl->dts_next, dmin);
+            atomicMin(&ctl->len_min, lmin);
+            if (bad) atomicOr(&ctl->status, bad);
         }
-        __syncthreads();  // also: the block is done with stage s
+        __syncthreads();  // the block is done with stage s
         if (tid == 0) {
-            double se[3] = {0.0, 0.0, 0.0};
-            unsigned long long md = kInfBits, ml = kInfBits;
-            int32_t b = 0;
-#pragma unroll
-            for (int w = 0; w < NW; ++w) {
-#pragma unroll
-                for (int k = 0; k < 3; ++k) se[k] = se[k] + red_e[k][w];
-                md = red_m[0][w] < md ? red_m[0][w] : md;
-                ml = red_m[1][w] < ml ? red_m[1][w] : ml;
-                b |= red_bad[w];
-            }
-            double* part = T.etile_part + 3 * t;
-#pragma unroll
-            for (int k = 0; k < 3; ++k) part[k] = se[k];
-            if (live) {
-                atomicMin(&ctl->dts_next, md);
-                atomicMin(&ctl->len_min, ml);
-                if (b) atomicOr(&ctl->status, b);
-            }
             const int64_t tn = t + 2 * gstride;
             if (tn < ntiles) {
                 fence_proxy_async_smem();
-                f64_batch_stage_issue(T, tn, stage0 + s * SB, bar);
+                f64_batch_stage_issue(T, tn, stage0 + s * SB, bar, f64_stage_hdr(smem, s));
             }
         }
     }
@@ -933,34 +949,11 @@ __global__ void __launch_bounds__(kNodeThreads, ENSC_NODE_MINB_FP64) k_node_batc
     const int ntiles = T.counts[1];
     for (int t = warp; t < ntiles; t += nwarps) {
         const int slot = T.ntile_inst[t];
+        const NodeParam p = T.nparam[slot];
+        if (!p.live) continue;
         const InstanceDesc& d = T.desc[slot];
-        Ctl* ctl = d.ctl;
         double* part = T.ntile_part + 2 * static_cast<int64_t>(t);
-        if (ctl->done) {
-            if (lane < 2) part[lane] = 0.0;
-            continue;
-        }
-        // stable dt of this cycle, identically on every tile of the instance
-        // (update_minVertex_perMaterial_and_dt, exDyna3D.cpp:673-679)
-        double dt_i;
-        const double dt_i_1 = ctl->dt_i_1;
-        const int dt_final = ctl->dt_final;
-        if (dt_final) {
-            dt_i = ctl->dt_i;
-        } else {
-            double dd = bits_ord(ctl->len_min) / ctl->wos;
-            const double tmp = ctl->dts_cur;
-            dd = dd < tmp ? dd : tmp;
-            dt_i = dd * ctl->factor;
-        }
-        if (t == d.n_tile0 && lane == 0) {
-            if (!(dt_i > 0.0) || !isfinite(dt_i)) atomicOr(&ctl->status, ST_BAD_DT);
-            if (!dt_final) ctl->dt_i = dt_i;
-            ctl->cycles_done += 1;
-            ctl->energy_pending = 1;
-        }
-        const double amp =
-            (d.M.gravity_on && d.M.amp_n > 0) ? gravity_amplitude(d.M.amp, d.M.amp_n, ctl->time, dt_i) : 1.0;
+        const double dt_i = p.dt_i, dt_i_1 = p.dt_i_1, amp = p.amp;
         double kin = 0.0, wext = 0.0;
         int32_t bad = 0;
         const int64_t n0 = static_cast<int64_t>(T.ntile_base[t]) + static_cast<int64_t>(lane) * W;
@@ -977,9 +970,9 @@ __global__ void __launch_bounds__(kNodeThreads, ENSC_NODE_MINB_FP64) k_node_batc
         wext = warp_sum_b(wext);
         bad = static_cast<int32_t>(__reduce_or_sync(0xffffffffu, static_cast<unsigned>(bad)));
         if (lane == 0) {
-            if (bad) atomicOr(&ctl->status, bad);
+            if (bad) atomicOr(&d.ctl->status, bad);
             part[0] = kin;
-            part[1] = wext;
+            part[1] += wext;
         }
     }
 }
@@ -1043,7 +1036,7 @@ int occupancy_node_fp64() {
 
 
 void launch_element_batch_fp64(const BatchTables& T, int grid, cudaStream_t st) {
-    k_element_batch_fp64<<<grid, kStageTileF64, f64_stage_smem<true>(), st>>>(T);
+    k_element_batch_fp64<<<grid, kStageTileF64, kF64BatchStageSmem, st>>>(T);
 }
 void launch_node_batch_fp64(const BatchTables& T, int grid, cudaStream_t st) {
     k_node_batch_fp64<<<grid, kNodeThreads, 0, st>>>(T);
@@ -1053,8 +1046,8 @@ int occupancy_element_batch_fp64() {
     // dynamic shared memory above the default 48 KB: set on the current
     // device before any launch or capture
     cudaFuncSetAttribute(k_element_batch_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         static_cast<int>(f64_stage_smem<true>()));
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_batch_fp64, kStageTileF64, f64_stage_smem<true>());
+                         static_cast<int>(kF64BatchStageSmem));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_batch_fp64, kStageTileF64, kF64BatchStageSmem);
     return nb;
 }
 

@@ -319,6 +319,7 @@ void material_from(const ensc_material* mat, const ensc_params* p, Material& M) 
     M.gravity_on = p->gravity_on;
     M.gravity_value = p->gravity_value;
     for (int i = 0; i < 3; ++i) M.gravity_dir[i] = p->gravity_dir[i];
+    set_mixed_consts(M);
 }
 
 Ctl initial_ctl(const ensc_params* p, const Material& M) {

@@ -41,6 +41,12 @@ constexpr int kNodeUnrollMixed = ENSC_NODE_UNROLL_MIXED;
 #ifndef ENSC_STAGE_MINB_MIXED
 #define ENSC_STAGE_MINB_MIXED 8
 #endif
+#ifndef ENSC_BATCH_MINB_MIXED
+#define ENSC_BATCH_MINB_MIXED 8
+#endif
+#ifndef ENSC_NODE_BATCH_MINB_MIXED
+#define ENSC_NODE_BATCH_MINB_MIXED 3
+#endif
 // FP64 element pass staged the same way: 0 off, 1 staging all streamed
 // inputs except B0^T (read from global memory), 2 staging B0^T too.
 #ifndef ENSC_STAGED_FP64
@@ -97,6 +103,9 @@ int batch_node_tile(bool mixed_precision);
 void launch_between_batch(const BatchTables& T, int slots, int mode, cudaStream_t st);
 void launch_edge_prepass_batch(const BatchTables& T, int grid, cudaStream_t st);
 void launch_begin_exact_batch(const BatchTables& T, int slots, cudaStream_t st);
+// per-instance node-pass scalars (and the control-block updates of the node
+// pass); runs between the element and node passes
+void launch_node_params_batch(const BatchTables& T, int slots, cudaStream_t st);
 
 // control (ensc_control.cu, built with -fmad=false)
 // mode 0: fold energy partials + begin next cycle; 1: fold only; 2: fold as initial KE

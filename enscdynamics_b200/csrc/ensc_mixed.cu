@@ -180,16 +180,13 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
     float* __restrict__ fe = static_cast<float*>(E.fe);
     const double* __restrict__ X = N.x;
     const float* __restrict__ V = static_cast<const float*>(N.v);
-    const float G = static_cast<float>(M.G);
-    const float lam_hi = static_cast<float>(M.lambda);
-    const float lam_lo = static_cast<float>(M.lambda - static_cast<double>(lam_hi));
-    const float g2_hi = static_cast<float>(2.0 * M.G);
-    const float g2_lo = static_cast<float>(2.0 * M.G - static_cast<double>(g2_hi));
-    const float rho = static_cast<float>(M.rho), wos = static_cast<float>(M.wos);
-    const float cvisl = static_cast<float>(M.cvisl), cvisq = static_cast<float>(M.cvisq);
-    const float y0 = static_cast<float>(M.yield0), H = static_cast<float>(M.hardening);
-    const float DRc = static_cast<float>(M.c_dr * (4.0 / 3.0 * M.G + M.K) * 0.1 / sqrt(8.0));
-    const float CRc = static_cast<float>(M.c_cr * M.rho * M.wos / 4.0);
+    const float G = M.mc.G;
+    const float lam_hi = M.mc.lam_hi, lam_lo = M.mc.lam_lo;
+    const float g2_hi = M.mc.g2_hi, g2_lo = M.mc.g2_lo;
+    const float rho = M.mc.rho, wos = M.mc.wos;
+    const float cvisl = M.mc.cvisl, cvisq = M.mc.cvisq;
+    const float y0 = M.mc.y0, H = M.mc.H;
+    const float DRc = M.mc.DRc, CRc = M.mc.CRc;
     // A = sum_j B0_j s_j^T as a float pair (hi + lo); B0 enters every
     // product through A, so no FP32 rounding of the reference geometry is
     // shared by all elements of a uniform mesh
@@ -459,23 +456,7 @@ __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_MIXED)
     if (ctl->done) return;
     const float dt1 = INIT ? 0.f : static_cast<float>(ctl->dt_i_1);
     const double dt1d = INIT ? 0.0 : ctl->dt_i_1;
-    const int64_t ne = E.ne, ep = E.ne_pad, np = N.nn_pad;
-    const uint32_t* __restrict__ conn = E.conn;
-    const float* __restrict__ bt = static_cast<const float*>(E.bt);
-    const float* __restrict__ vol0 = reinterpret_cast<const float*>(E.vol0);
-    const float* __restrict__ cb = reinterpret_cast<const float*>(E.cbrt_v0);
-    float* __restrict__ sig = static_cast<float*>(E.sigma);
-    float* __restrict__ qia = static_cast<float*>(E.qia);
-    float* __restrict__ epsp = static_cast<float*>(E.eps_p);
-    float* __restrict__ fe = static_cast<float*>(E.fe);
-    const double* __restrict__ X = N.x;
-    const float* __restrict__ V = static_cast<const float*>(N.v);
-    const float G = static_cast<float>(M.G), lam = static_cast<float>(M.lambda);
-    const float rho = static_cast<float>(M.rho), wos = static_cast<float>(M.wos);
-    const float cvisl = static_cast<float>(M.cvisl), cvisq = static_cast<float>(M.cvisq);
-    const float y0 = static_cast<float>(M.yield0), H = static_cast<float>(M.hardening);
-    const float DRc = static_cast<float>(M.c_dr * (4.0 / 3.0 * M.G + M.K) * 0.1 / sqrt(8.0));
-    const float CRc = static_cast<float>(M.c_cr * M.rho * M.wos / 4.0);
+    const int64_t ne = E.ne;
     double e_int = 0.0, e_hg = 0.0, e_vis = 0.0;
     double dts_min = DBL_MAX, len_min = DBL_MAX;
     int32_t bad = 0;
@@ -524,18 +505,32 @@ __device__ __forceinline__ const float* stage_row(const ElemArrays& E, int r) {
     return static_cast<const float*>(E.eps_p);
 }
 
-// Thread 0: copies the tile starting at element `base` into the stage at
-// shared address dst, completing on bar.  The rows are padded to a multiple
-// of 32 entries and start 256-byte aligned, so every copy is 16-byte aligned
-// and a multiple of 128 bytes long.
+// Warp 0 copies the tile starting at element `base` into the stage at
+// shared address dst, completing on bar: lane 0 arms the barrier with the
+// byte count, then the lanes start the row copies between them.  The rows
+// are padded to a multiple of 32 entries and start 256-byte aligned, so
+// every copy is 16-byte aligned and a multiple of 128 bytes long.
 template <bool PLASTIC>
-__device__ __forceinline__ void stage_issue(const ElemArrays& E, uint32_t dst, uint32_t bar, int64_t base) {
+__device__ __forceinline__ uint32_t stage_count(const ElemArrays& E, int64_t base) {
     const int64_t left = E.ne_pad - base;
-    const uint32_t cnt = static_cast<uint32_t>(left < kStageTile ? left : kStageTile);
+    return static_cast<uint32_t>(left < kStageTile ? left : kStageTile);
+}
+template <bool PLASTIC>
+__device__ __forceinline__ uint32_t stage_tx_bytes(uint32_t cnt) {
     constexpr int rows = PLASTIC ? kStageWordRows : kStageWordRows - 1;  // eps_p last, J2 only
-    mbar_arrive_expect_tx(bar, rows * cnt * 4u + cnt * 8u);
-    for (int r = 0; r < rows; ++r) bulk_g2s(dst + r * (kStageTile * 4u), stage_row(E, r) + base, cnt * 4u, bar);
-    bulk_g2s(dst + kStageV0Off, E.vol0 + base, cnt * 8u, bar);
+    return rows * cnt * 4u + cnt * 8u;
+}
+template <bool PLASTIC>
+__device__ __forceinline__ void stage_issue(const ElemArrays& E, uint32_t dst, uint32_t bar, int64_t base, int lane) {
+    constexpr int rows = PLASTIC ? kStageWordRows : kStageWordRows - 1;
+    const uint32_t cnt = stage_count<PLASTIC>(E, base);
+    if (lane == 0) mbar_arrive_expect_tx(bar, stage_tx_bytes<PLASTIC>(cnt));
+    __syncwarp();
+    fence_proxy_async_smem();  // the block's reads of this stage come before the copies into it
+    for (int r = lane; r <= rows; r += 32) {
+        if (r < rows) bulk_g2s(dst + r * (kStageTile * 4u), stage_row(E, r) + base, cnt * 4u, bar);
+        else bulk_g2s(dst + kStageV0Off, E.vol0 + base, cnt * 8u, bar);
+    }
 }
 
 template <bool PLASTIC>
@@ -545,7 +540,7 @@ __global__ void __launch_bounds__(kStageTile, ENSC_STAGE_MINB_MIXED)
     extern __shared__ __align__(128) unsigned char smem[];
     const float dt1 = static_cast<float>(ctl->dt_i_1);
     const double dt1d = ctl->dt_i_1;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const uint32_t stage0 = smem_addr(smem);
     const uint32_t bar0 = stage0 + 2 * kStageBytes;
     const int64_t ntiles = (E.ne + kStageTile - 1) / kStageTile;
@@ -556,10 +551,10 @@ __global__ void __launch_bounds__(kStageTile, ENSC_STAGE_MINB_MIXED)
         mbar_init_fence();
     }
     __syncthreads();
-    if (tid == 0) {
+    if (wid == 0) {
         for (int s = 0; s < 2; ++s) {
             const int64_t t = blockIdx.x + s * gstride;
-            if (t < ntiles) stage_issue<PLASTIC>(E, stage0 + s * kStageBytes, bar0 + 8 * s, t * kStageTile);
+            if (t < ntiles) stage_issue<PLASTIC>(E, stage0 + s * kStageBytes, bar0 + 8 * s, t * kStageTile, lane);
         }
     }
     double e_int = 0.0, e_hg = 0.0, e_vis = 0.0;
@@ -594,10 +589,7 @@ __global__ void __launch_bounds__(kStageTile, ENSC_STAGE_MINB_MIXED)
         }
         __syncthreads();  // the block is done with stage s
         const int64_t tn = t + 2 * gstride;
-        if (tid == 0 && tn < ntiles) {
-            fence_proxy_async_smem();
-            stage_issue<PLASTIC>(E, stage0 + s * kStageBytes, bar, tn * kStageTile);
-        }
+        if (wid == 0 && tn < ntiles) stage_issue<PLASTIC>(E, stage0 + s * kStageBytes, bar, tn * kStageTile, lane);
     }
     if (timed_out) {
         // record the failure and let the copies this block started land
@@ -830,9 +822,10 @@ __global__ void __launch_bounds__(kNodeThreads, ENSC_NODE_MINB_MIXED) k_node_mix
 // nodes, each inside one instance whose arrays, material and control block
 // come from the instance table.  The element pass runs the staged pipeline
 // over the tile list, one tile per block at a time; the node pass gives each
-// node tile to one warp.  Per-tile work sums are written to a tile-indexed
-// buffer and folded per instance in tile order, so the totals do not depend
-// on scheduling.
+// node tile to one warp.  Each tile accumulates its work terms across
+// cycles (one owner per tile and pass) and keeps its latest kinetic energy;
+// k_fold_batch folds them per instance in tile order, so the totals do not
+// depend on scheduling.
 __device__ __forceinline__ double warp_sum_b(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -848,24 +841,63 @@ __device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v)
     return v;
 }
 
-// Tiles of instances that are done are not copied: their stage's phase is
-// completed by a plain arrival (done cannot change during the pass).
-__device__ __forceinline__ void batch_stage_issue(const BatchTables& T, int64_t t, uint32_t dst, uint32_t bar) {
-    const InstanceDesc& d = T.desc[T.etile_inst[t]];
-    if (d.ctl->done) mbar_arrive(bar);
-    else if (d.M.plastic) stage_issue<true>(d.E, dst, bar, T.etile_base[t]);
-    else stage_issue<false>(d.E, dst, bar, T.etile_base[t]);
+// A batch stage: the single-instance stage, then the tile's instance
+// descriptor, its element-pass scalars (StageHdr), the TileInfo the filling
+// warp writes, and the ETileSrc record of the tile that uses the stage next.
+// Every tile is copied whole whether or not its instance runs this cycle;
+// the consumer skips the tiles of instances that do not.
+constexpr uint32_t kDescBytes = sizeof(InstanceDesc);
+constexpr uint32_t kBatchDescOff = kStageBytes;
+constexpr uint32_t kBatchHdrOff = kBatchDescOff + kDescBytes;
+constexpr uint32_t kBatchInfoOff = kBatchHdrOff + sizeof(StageHdr);
+constexpr uint32_t kBatchNextOff = kBatchInfoOff + sizeof(TileInfo);
+constexpr uint32_t kBatchStageBytes = (kBatchNextOff + sizeof(ETileSrc) + 127) / 128 * 128;
+constexpr size_t kBatchStageSmem = 2 * static_cast<size_t>(kBatchStageBytes) + 16;
+static_assert(kDescBytes % 16 == 0 && sizeof(StageHdr) == 16 && sizeof(TileInfo) == 16, "16-byte copies");
+
+// word row r of a batch tile in global memory
+__device__ __forceinline__ const void* tile_row(const ETileSrc& src, int r) {
+    const int64_t ep = src.ne_pad;
+    if (r < 8) return static_cast<const uint32_t*>(src.conn) + r * ep;
+    if (r < 26) return static_cast<const float*>(src.bt) + (r - 8) * ep;
+    if (r < 32) return static_cast<const float*>(src.sigma) + (r - 26) * ep;
+    if (r < 44) return static_cast<const float*>(src.qia) + (r - 32) * ep;
+    if (r == 44) return src.cbrt_v0;
+    return src.eps_p;
 }
 
-__global__ void __launch_bounds__(kStageTile, ENSC_STAGE_MINB_MIXED) k_element_batch_mixed(BatchTables T) {
+// Warp 0 fills a stage with the tile `src` describes (and the record of tile
+// t_next, if there is one): lane 0 writes the TileInfo and arms the barrier
+// with the byte count, then the lanes start the copies between them.
+__device__ __forceinline__ void batch_stage_issue(const BatchTables& T, const ETileSrc& src, int64_t t_next,
+                                                  int64_t ntiles, unsigned char* stage, uint32_t dst, uint32_t bar,
+                                                  int lane) {
+    const uint32_t cnt = static_cast<uint32_t>(src.cnt);
+    const bool next = t_next < ntiles;
+    if (lane == 0) {
+        TileInfo* ti = reinterpret_cast<TileInfo*>(stage + kBatchInfoOff);
+        ti->slot = src.slot;
+        ti->base = src.base;
+        mbar_arrive_expect_tx(bar, kStageWordRows * cnt * 4u + cnt * 8u + kDescBytes + sizeof(StageHdr) +
+                                       (next ? sizeof(ETileSrc) : 0u));
+    }
+    __syncwarp();
+    fence_proxy_async_smem();  // the block's reads of this stage come before the copies into it
+    for (int r = lane; r < kStageWordRows + 4; r += 32) {
+        if (r < kStageWordRows) bulk_g2s(dst + r * (kStageTile * 4u), tile_row(src, r), cnt * 4u, bar);
+        else if (r == kStageWordRows) bulk_g2s(dst + kStageV0Off, src.vol0, cnt * 8u, bar);
+        else if (r == kStageWordRows + 1) bulk_g2s(dst + kBatchDescOff, T.desc + src.slot, kDescBytes, bar);
+        else if (r == kStageWordRows + 2) bulk_g2s(dst + kBatchHdrOff, T.sparam + src.slot, sizeof(StageHdr), bar);
+        else if (next) bulk_g2s(dst + kBatchNextOff, T.etile_src + t_next, sizeof(ETileSrc), bar);
+    }
+}
+
+__global__ void __launch_bounds__(kStageTile, ENSC_BATCH_MINB_MIXED) k_element_batch_mixed(BatchTables T) {
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr int NW = kStageTile / 32;
-    __shared__ double red_e[3][NW];
-    __shared__ unsigned long long red_m[2][NW];
-    __shared__ int red_bad[NW];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const uint32_t stage0 = smem_addr(smem);
-    const uint32_t bar0 = stage0 + 2 * kStageBytes;
+    const uint32_t bar0 = stage0 + 2 * kBatchStageBytes;
     const int64_t ntiles = T.counts[0];
     const int64_t gstride = gridDim.x;
     if (tid == 0) {
@@ -874,10 +906,14 @@ __global__ void __launch_bounds__(kStageTile, ENSC_STAGE_MINB_MIXED) k_element_b
         mbar_init_fence();
     }
     __syncthreads();
-    if (tid == 0) {
+    if (wid == 0) {
         for (int s = 0; s < 2; ++s) {
             const int64_t t = blockIdx.x + s * gstride;
-            if (t < ntiles) batch_stage_issue(T, t, stage0 + s * kStageBytes, bar0 + 8 * s);
+            if (t < ntiles) {
+                const ETileSrc src = T.etile_src[t];
+                batch_stage_issue(T, src, t + 2 * gstride, ntiles, smem + s * kBatchStageBytes,
+                                  stage0 + s * kBatchStageBytes, bar0 + 8 * s, lane);
+            }
         }
     }
     bool timed_out = false;
@@ -891,71 +927,58 @@ __global__ void __launch_bounds__(kStageTile, ENSC_STAGE_MINB_MIXED) k_element_b
             timed_out = true;
             break;
         }
-        const InstanceDesc& d = T.desc[T.etile_inst[t]];
-        Ctl* ctl = d.ctl;
-        const bool live = !ctl->done;
+        unsigned char* sb = smem + s * kBatchStageBytes;
+        const InstanceDesc& d = *reinterpret_cast<const InstanceDesc*>(sb + kBatchDescOff);
+        const StageHdr& h = *reinterpret_cast<const StageHdr*>(sb + kBatchHdrOff);
+        const TileInfo& ti = *reinterpret_cast<const TileInfo*>(sb + kBatchInfoOff);
+        const bool live = h.live != 0;
+        Ctl* const ctl = d.ctl;
         double ei = 0.0, eh = 0.0, ev = 0.0, dts = DBL_MAX, len = DBL_MAX;
         int32_t bad = 0;
-        const int64_t e = static_cast<int64_t>(T.etile_base[t]) + tid;
+        const int64_t e = static_cast<int64_t>(ti.base) + tid;
         if (live && e < d.E.ne) {
-            const double dt1d = ctl->dt_i_1;
+            // the instance's arrays and constants, read from the stage once:
+            // the body's stores could alias the stage as far as the compiler
+            // knows, so references into it would be re-read after each store
+            const ElemArrays E = d.E;
+            const NodeArrays N = d.N;
+            const Material M = d.M;
+            const double dt1d = h.dt1;
             const float dt1 = static_cast<float>(dt1d);
-            const float* st = reinterpret_cast<const float*>(smem + s * kStageBytes);
+            const float* st = reinterpret_cast<const float*>(sb);
             const MixedSrc S{reinterpret_cast<const uint32_t*>(st),
                              st + 8 * kStageTile,
-                             reinterpret_cast<const double*>(smem + s * kStageBytes + kStageV0Off),
+                             reinterpret_cast<const double*>(sb + kStageV0Off),
                              st + 44 * kStageTile,
                              st + 26 * kStageTile,
                              st + 32 * kStageTile,
                              st + 45 * kStageTile,
                              kStageTile,
                              tid};
-            if (d.M.plastic)
-                element_body_mixed<true, false, true>(d.E, d.N, d.M, S, dt1, dt1d, e, dts, len, ei, eh, ev, bad);
-            else
-                element_body_mixed<false, false, true>(d.E, d.N, d.M, S, dt1, dt1d, e, dts, len, ei, eh, ev, bad);
+            element_body_mixed<true, false, true>(E, N, M, S, dt1, dt1d, e, dts, len, ei, eh, ev, bad);
         }
-        // the tile's sums and minima (fixed order: lanes, then warps)
+        // each warp's sums go to its own slot (tile-major, warp-minor; folded
+        // in that order) and its minima to the instance's control block
         ei = warp_sum_b(ei);
         eh = warp_sum_b(eh);
         ev = warp_sum_b(ev);
         const unsigned long long dmin = warp_min_u64(ord_bits(dts));
         const unsigned long long lmin = warp_min_u64(ord_bits(len));
         bad = static_cast<int32_t>(__reduce_or_sync(0xffffffffu, static_cast<unsigned>(bad)));
-        if (lane == 0) {
-            red_e[0][wid] = ei;
-            red_e[1][wid] = eh;
-            red_e[2][wid] = ev;
-            red_m[0][wid] = dmin;
-            red_m[1][wid] = lmin;
-            red_bad[wid] = bad;
+        if (live && lane == 0) {
+            double* part = T.etile_part + 3 * (t * NW + wid);
+            part[0] += ei;
+            part[1] += eh;
+            part[2] += ev;
+            atomicMin(&ctl->dts_next, dmin);
+            atomicMin(&ctl->len_min, lmin);
+            if (bad) atomicOr(&ctl->status, bad);
         }
-        __syncthreads();  // also: the block is done with stage s
-        if (tid == 0) {
-            double se[3] = {0.0, 0.0, 0.0};
-            unsigned long long md = kInfBits, ml = kInfBits;
-            int32_t b = 0;
-#pragma unroll
-            for (int w = 0; w < NW; ++w) {
-#pragma unroll
-                for (int k = 0; k < 3; ++k) se[k] = se[k] + red_e[k][w];
-                md = red_m[0][w] < md ? red_m[0][w] : md;
-                ml = red_m[1][w] < ml ? red_m[1][w] : ml;
-                b |= red_bad[w];
-            }
-            double* part = T.etile_part + 3 * t;
-#pragma unroll
-            for (int k = 0; k < 3; ++k) part[k] = se[k];
-            if (live) {
-                atomicMin(&ctl->dts_next, md);
-                atomicMin(&ctl->len_min, ml);
-                if (b) atomicOr(&ctl->status, b);
-            }
-            const int64_t tn = t + 2 * gstride;
-            if (tn < ntiles) {
-                fence_proxy_async_smem();
-                batch_stage_issue(T, tn, stage0 + s * kStageBytes, bar);
-            }
+        __syncthreads();  // the block is done with stage s
+        const int64_t tn = t + 2 * gstride;
+        if (wid == 0 && tn < ntiles) {
+            const ETileSrc src = *reinterpret_cast<const ETileSrc*>(sb + kBatchNextOff);
+            batch_stage_issue(T, src, tn + 2 * gstride, ntiles, sb, stage0 + s * kBatchStageBytes, bar, lane);
         }
     }
     if (timed_out && tid == 0) {
@@ -969,7 +992,7 @@ __global__ void __launch_bounds__(kStageTile, ENSC_STAGE_MINB_MIXED) k_element_b
     }
 }
 
-__global__ void __launch_bounds__(kNodeThreads, ENSC_NODE_MINB_MIXED) k_node_batch_mixed(BatchTables T) {
+__global__ void __launch_bounds__(kNodeThreads, ENSC_NODE_BATCH_MINB_MIXED) k_node_batch_mixed(BatchTables T) {
     constexpr int W = kNodeGroupMixed;
     const int lane = threadIdx.x & 31;
     const int warp = static_cast<int>((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
@@ -977,34 +1000,18 @@ __global__ void __launch_bounds__(kNodeThreads, ENSC_NODE_MINB_MIXED) k_node_bat
     const int ntiles = T.counts[1];
     for (int t = warp; t < ntiles; t += nwarps) {
         const int slot = T.ntile_inst[t];
-        const InstanceDesc& d = T.desc[slot];
-        Ctl* ctl = d.ctl;
+        const NodeParam p = T.nparam[slot];
+        if (!p.live) continue;
+        // the instance's arrays and constants, read once per tile (references
+        // into the table would be re-read after every store)
+        struct {
+            ElemArrays E;
+            NodeArrays N;
+            Material M;
+            Ctl* ctl;
+        } const d{T.desc[slot].E, T.desc[slot].N, T.desc[slot].M, T.desc[slot].ctl};
         double* part = T.ntile_part + 2 * static_cast<int64_t>(t);
-        if (ctl->done) {
-            if (lane < 2) part[lane] = 0.0;
-            continue;
-        }
-        // stable dt of this cycle, identically on every tile of the instance
-        // (update_minVertex_perMaterial_and_dt, exDyna3D.cpp:673-679)
-        double dt_i;
-        const double dt_i_1 = ctl->dt_i_1;
-        const int dt_final = ctl->dt_final;
-        if (dt_final) {
-            dt_i = ctl->dt_i;
-        } else {
-            double dd = bits_ord(ctl->len_min) / ctl->wos;
-            const double tmp = ctl->dts_cur;
-            dd = dd < tmp ? dd : tmp;
-            dt_i = dd * ctl->factor;
-        }
-        if (t == d.n_tile0 && lane == 0) {
-            if (!(dt_i > 0.0) || !isfinite(dt_i)) atomicOr(&ctl->status, ST_BAD_DT);
-            if (!dt_final) ctl->dt_i = dt_i;
-            ctl->cycles_done += 1;
-            ctl->energy_pending = 1;
-        }
-        const double amp =
-            (d.M.gravity_on && d.M.amp_n > 0) ? gravity_amplitude(d.M.amp, d.M.amp_n, ctl->time, dt_i) : 1.0;
+        const double dt_i = p.dt_i, dt_i_1 = p.dt_i_1, amp = p.amp;
         double kin = 0.0, wext = 0.0;
         int32_t bad = 0;
         const int64_t n0 = static_cast<int64_t>(T.ntile_base[t]) + static_cast<int64_t>(lane) * W;
@@ -1021,9 +1028,9 @@ __global__ void __launch_bounds__(kNodeThreads, ENSC_NODE_MINB_MIXED) k_node_bat
         wext = warp_sum_b(wext);
         bad = static_cast<int32_t>(__reduce_or_sync(0xffffffffu, static_cast<unsigned>(bad)));
         if (lane == 0) {
-            if (bad) atomicOr(&ctl->status, bad);
+            if (bad) atomicOr(&d.ctl->status, bad);
             part[0] = kin;
-            part[1] = wext;
+            part[1] += wext;
         }
     }
 }
@@ -1080,7 +1087,7 @@ int occupancy_node_mixed() {
 
 
 void launch_element_batch_mixed(const BatchTables& T, int grid, cudaStream_t st) {
-    k_element_batch_mixed<<<grid, kStageTile, kStageSmem, st>>>(T);
+    k_element_batch_mixed<<<grid, kStageTile, kBatchStageSmem, st>>>(T);
 }
 void launch_node_batch_mixed(const BatchTables& T, int grid, cudaStream_t st) {
     k_node_batch_mixed<<<grid, kNodeThreads, 0, st>>>(T);
@@ -1090,8 +1097,8 @@ int occupancy_element_batch_mixed() {
     // dynamic shared memory above the default 48 KB: set on the current
     // device before any launch or capture
     cudaFuncSetAttribute(k_element_batch_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         static_cast<int>(kStageSmem));
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_batch_mixed, kStageTile, kStageSmem);
+                         static_cast<int>(kBatchStageSmem));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_batch_mixed, kStageTile, kBatchStageSmem);
     return nb;
 }
 

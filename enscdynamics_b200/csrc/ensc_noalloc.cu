@@ -162,6 +162,7 @@ int ensc_step_noalloc(const ensc_device_model* m, const ensc_material* mat, cons
     M.gravity_on = params->gravity_on;
     M.gravity_value = params->gravity_value;
     for (int i = 0; i < 3; ++i) M.gravity_dir[i] = params->gravity_dir[i];
+    ensc::set_mixed_consts(M);
 
     // the shared scratch keeps the previous call's contents: every control
     // field is rewritten here, reductions restart from +inf, sums from zero

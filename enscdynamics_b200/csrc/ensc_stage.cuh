@@ -50,12 +50,6 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity)
     return true;
 }
 
-// plain arrival without transaction bytes (completes a phase whose stage is
-// left unfilled)
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-
 // orders this thread's earlier generic-proxy accesses of shared memory before
 // later bulk-copy (async-proxy) writes to it
 __device__ __forceinline__ void fence_proxy_async_smem() {
