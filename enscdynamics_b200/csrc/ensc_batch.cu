@@ -67,6 +67,7 @@ struct ensc_batch {
     double* d_scratch = nullptr;  // partials for init / kinetic passes of one instance
     ensc::NodeParam* d_nparam = nullptr;
     ensc::StageHdr* d_sparam = nullptr;
+    ensc::NodeView* d_nview = nullptr;
     ensc::ETileSrc* d_etile_src = nullptr;
     int scratch_blocks = 4096;
     Ctl* h_ctl = nullptr;         // pinned mirror of d_ctl
@@ -122,6 +123,7 @@ int rebuild_tables(ensc_batch* b) {
     ensc::launch_between_batch(b->T, b->slots, 1, b->stream);
     BCK(b, cudaGetLastError());
     std::vector<ensc::InstanceDesc> desc(static_cast<size_t>(b->slots));
+    std::vector<ensc::NodeView> views(static_cast<size_t>(b->slots));
     std::vector<int32_t> ei, eb, ni, nb;
     std::vector<ensc::ETileSrc> es;
     const int64_t real = is_mixed(b) ? 4 : 8;
@@ -144,6 +146,7 @@ int rebuild_tables(ensc_batch* b) {
             ensc::set_mixed_consts(d.M);
         }
         d.active = 1;
+        views[s] = ensc::node_view(d.E, d.N, d.M, d.ctl);
         d.e_tile0 = static_cast<int32_t>(ei.size());
         for (int64_t e = 0; e < sl.ne; e += b->etile) {
             ei.push_back(s);
@@ -177,6 +180,8 @@ int rebuild_tables(ensc_batch* b) {
         return berr(b, ENSC_ERR_OOM, "batch tile capacity exceeded");
     const int32_t counts[3] = {static_cast<int32_t>(ei.size()), static_cast<int32_t>(ni.size()), used_slots};
     BCK(b, cudaMemcpyAsync(b->d_desc, desc.data(), desc.size() * sizeof(ensc::InstanceDesc), cudaMemcpyHostToDevice,
+                           b->stream));
+    BCK(b, cudaMemcpyAsync(b->d_nview, views.data(), views.size() * sizeof(ensc::NodeView), cudaMemcpyHostToDevice,
                            b->stream));
     if (!ei.empty()) {
         BCK(b, cudaMemcpyAsync(b->d_etile_inst, ei.data(), ei.size() * 4, cudaMemcpyHostToDevice, b->stream));
@@ -337,8 +342,9 @@ int ensc_batch_create(const ensc_params* params, int32_t max_instances, int64_t 
                  s_np = al(8 * 2 * b->max_ntiles), s_ctl = al(sizeof(Ctl) * b->slots),
                  s_scr = al(8 * 3 * static_cast<size_t>(b->scratch_blocks)),
                  s_nprm = al(sizeof(ensc::NodeParam) * b->slots), s_sprm = al(sizeof(ensc::StageHdr) * b->slots),
-                 s_esrc = al(sizeof(ensc::ETileSrc) * b->max_etiles);
-    const size_t total = s_desc + 2 * s_et + 2 * s_nt + s_cnt + s_ep + s_np + s_ctl + s_scr + s_nprm + s_sprm + s_esrc;
+                 s_esrc = al(sizeof(ensc::ETileSrc) * b->max_etiles), s_nview = al(sizeof(ensc::NodeView) * b->slots);
+    const size_t total =
+        s_desc + 2 * s_et + 2 * s_nt + s_cnt + s_ep + s_np + s_ctl + s_scr + s_nprm + s_sprm + s_esrc + s_nview;
     e = cudaMalloc(&b->tables, total);
     if (e != cudaSuccess) return fail(bcuda(b, "cudaMalloc(batch tables)", e));
     cudaMemset(b->tables, 0, total);
@@ -368,6 +374,8 @@ int ensc_batch_create(const ensc_params* params, int32_t max_instances, int64_t 
     b->d_sparam = reinterpret_cast<ensc::StageHdr*>(p);
     p += s_sprm;
     b->d_etile_src = reinterpret_cast<ensc::ETileSrc*>(p);
+    p += s_esrc;
+    b->d_nview = reinterpret_cast<ensc::NodeView*>(p);
     e = cudaMallocHost(reinterpret_cast<void**>(&b->h_ctl), sizeof(Ctl) * b->slots);
     if (e != cudaSuccess) return fail(bcuda(b, "cudaMallocHost(ctl)", e));
     std::memset(b->h_ctl, 0, sizeof(Ctl) * b->slots);
@@ -388,6 +396,7 @@ int ensc_batch_create(const ensc_params* params, int32_t max_instances, int64_t 
     b->T.nparam = b->d_nparam;
     b->T.sparam = b->d_sparam;
     b->T.etile_src = b->d_etile_src;
+    b->T.nview = b->d_nview;
     int rc = rebuild_tables(b);
     if (rc) return fail(rc);
     *out = b;

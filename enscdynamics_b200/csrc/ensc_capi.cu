@@ -415,6 +415,13 @@ int ensc_step_until(ensc_handle* h, int64_t max_cycles, double step_end_time, do
     return status_code(h, h->ctl_host->status);
 }
 
+// The staging area may be the element force scratch, whose slots no
+// element fills must read as zeros for the node pass: clear what was used.
+static int release_staging(ensc_handle* h, size_t used) {
+    if (!h->staging_owned && used) CK(h, cudaMemsetAsync(h->staging, 0, used, h->stream));
+    return ENSC_OK;
+}
+
 int ensc_download(ensc_handle* h, double* x, double* u, double* v, double* sigma, double* qia, double* eps_p) {
     if (!h) return ENSC_ERR_ARG;
     DevGuard dg(h->device);
@@ -429,6 +436,7 @@ int ensc_download(ensc_handle* h, double* x, double* u, double* v, double* sigma
     const Item items[] = {{x, h->N.x, h->nn, h->nn_pad, 3, false},        {u, h->N.u, h->nn, h->nn_pad, 3, false},
                           {v, h->N.v, h->nn, h->nn_pad, 3, mx},           {sigma, h->E.sigma, h->ne, h->ne_pad, 6, mx},
                           {qia, h->E.qia, h->ne, h->ne_pad, 12, mx},      {eps_p, h->E.eps_p, h->ne, h->ne_pad, 1, mx}};
+    size_t used = 0;
     for (const Item& it : items) {
         if (!it.dst) continue;
         ensc::launch_soa_to_aos(it.src, it.n, it.pad, it.comps, it.f32, h->staging, h->stream);
@@ -436,8 +444,9 @@ int ensc_download(ensc_handle* h, double* x, double* u, double* v, double* sigma
         CK(h, cudaMemcpyAsync(it.dst, h->staging, it.n * it.comps * sizeof(double), cudaMemcpyDeviceToHost,
                               h->stream));
         CK(h, cudaStreamSynchronize(h->stream));
+        used = std::max(used, static_cast<size_t>(it.n * it.comps) * sizeof(double));
     }
-    return ENSC_OK;
+    return release_staging(h, used);
 }
 
 int ensc_download_reactions(ensc_handle* h, double* rf) {
@@ -447,7 +456,7 @@ int ensc_download_reactions(ensc_handle* h, double* rf) {
     CK(h, cudaGetLastError());
     CK(h, cudaMemcpyAsync(rf, h->staging, h->nn * 3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CK(h, cudaStreamSynchronize(h->stream));
-    return ENSC_OK;
+    return release_staging(h, static_cast<size_t>(h->nn * 3) * sizeof(double));
 }
 
 int ensc_upload_state(ensc_handle* h, const double* x, const double* u, const double* v, const double* sigma,
@@ -466,13 +475,16 @@ int ensc_upload_state(ensc_handle* h, const double* x, const double* u, const do
     const Item items[] = {{x, h->N.x, h->nn, h->nn_pad, 3, false},        {u, h->N.u, h->nn, h->nn_pad, 3, false},
                           {v, h->N.v, h->nn, h->nn_pad, 3, mx},           {sigma, h->E.sigma, h->ne, h->ne_pad, 6, mx},
                           {qia, h->E.qia, h->ne, h->ne_pad, 12, mx},      {eps_p, h->E.eps_p, h->ne, h->ne_pad, 1, mx}};
+    size_t used = 0;
     for (const Item& it : items) {
         if (!it.src) continue;
         CK(h, cudaMemcpyAsync(h->staging, it.src, it.n * it.comps * sizeof(double), cudaMemcpyHostToDevice,
                               h->stream));
         ensc::launch_aos_to_soa(h->staging, it.n, it.pad, it.comps, it.dst, it.f32, h->stream);
         CK(h, cudaGetLastError());
+        used = std::max(used, static_cast<size_t>(it.n * it.comps) * sizeof(double));
     }
+    if (int rc0 = release_staging(h, used)) return rc0;
     int rc = read_ctl(h);
     if (rc) return rc;
     h->ctl_host->time = time;

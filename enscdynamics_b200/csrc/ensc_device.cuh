@@ -151,6 +151,47 @@ struct Partials {
     int32_t n_elem_blocks, n_node_blocks;
 };
 
+// The node pass's view of one instance: node arrays, slot-major forces,
+// gravity and the control block.  `grouped` is 1 when the forces are
+// slot-major and the rows tile-aligned, so W consecutive nodes can be read
+// and written as vectors.  In a batch, one 128-byte line per slot.
+struct alignas(128) NodeView {
+    const void* fe;
+    void* v;                   // double (FP64) or float (mixed)
+    double* u;
+    double* x;
+    const double* inv_mass;
+    const uint8_t* bc;
+    const uint8_t* slot_mask;  // bit k: slot k holds an element
+    double* rf;
+    Ctl* ctl;
+    int64_t nn, np;
+    double gravity_value, gravity_dir[3];
+    int32_t gravity_on;
+    int32_t grouped;
+};
+static_assert(sizeof(NodeView) == 128, "one line per slot");
+
+__host__ __device__ inline NodeView node_view(const ElemArrays& E, const NodeArrays& N, const Material& M, Ctl* ctl) {
+    NodeView v{};
+    v.fe = E.fe;
+    v.v = N.v;
+    v.u = N.u;
+    v.x = N.x;
+    v.inv_mass = N.inv_mass;
+    v.bc = N.bc;
+    v.slot_mask = N.slot_mask;
+    v.rf = N.rf;
+    v.ctl = ctl;
+    v.nn = N.nn;
+    v.np = N.nn_pad;
+    v.gravity_value = M.gravity_value;
+    for (int c = 0; c < 3; ++c) v.gravity_dir[c] = M.gravity_dir[c];
+    v.gravity_on = M.gravity_on;
+    v.grouped = (E.slot_major && E.tiles_aligned) ? 1 : 0;
+    return v;
+}
+
 // ---- batched instances ------------------------------------------------------
 // Independent solver instances advanced together: each warp-sized tile (32
 // elements or 32 nodes) belongs to one instance, so instance parameters,
@@ -159,7 +200,7 @@ constexpr int kTile = 32;
 
 // The scalars of an instance's node pass in the current cycle (stable dt,
 // previous dt, gravity amplitude), computed once per instance.
-struct NodeParam {
+struct alignas(16) NodeParam {
     double dt_i, dt_i_1, amp;
     int32_t live, pad;
 };
@@ -222,6 +263,7 @@ struct BatchTables {
     int32_t* exact_count;        // instances whose current cycle needs the edge prepass
     NodeParam* nparam;           // [slots] this cycle's node-pass scalars
     StageHdr* sparam;            // [slots] this cycle's element-pass scalars
+    const NodeView* nview;       // [slots]
     const ETileSrc* etile_src;   // [etiles] copy sources of each element tile
     int32_t etile, ntile;        // elements / nodes per tile
 };
@@ -315,6 +357,28 @@ __device__ __forceinline__ uint32_t ld_bytes(const uint8_t* p) {
     static_assert(W == 2 || W == 4, "2 or 4 bytes");
     if (W == 4) return *reinterpret_cast<const uint32_t*>(p);
     return *reinterpret_cast<const uint16_t*>(p);
+}
+
+// A NodeView of a batch table through the non-coherent (L1-cached) path:
+// the table does not change while a pass runs.
+__device__ __forceinline__ NodeView ld_view(const NodeView* p) {
+    uint4 w[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) w[i] = __ldg(reinterpret_cast<const uint4*>(p) + i);
+    NodeView v;
+    memcpy(&v, w, sizeof(v));
+    return v;
+}
+__device__ __forceinline__ NodeParam ld_param(const NodeParam* p) {
+    uint4 w[2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) w[i] = __ldg(reinterpret_cast<const uint4*>(p) + i);
+    NodeParam v;
+    memcpy(&v, w, sizeof(v));
+    return v;
+}
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
 }
 
 // Read-only input loads: through the non-coherent path from global memory,

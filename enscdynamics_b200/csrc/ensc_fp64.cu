@@ -676,24 +676,24 @@ __global__ void __launch_bounds__(kStageTileF64, BT ? 2 : 3)
 
 // W consecutive nodes of the node pass with 16-byte row accesses: the same
 // arithmetic per node as node_body on the slot-major layout, in the same
-// order.  Nodes at or past nn (row padding) are loaded and stored back
-// unchanged.
-
+// order.  Slots the mask marks empty are skipped, or (ENSC_NODE_ALL_SLOTS)
+// added as the zeros they hold, as the reference adds all 8 slot vectors:
+// the slot-major rows start zeroed and only the slot's element writes them.
+// Nodes at or past nn (row padding) are loaded and stored back unchanged.
 template <int W>
-__device__ __forceinline__ void node_group(const ElemArrays& E, const NodeArrays& N, const Material& M,
-                                           const double dt_i, const double dt_i_1, const double amp, const int64_t n0,
-                                           const int64_t nn, double& kin, double& wext, int32_t& bad) {
-    const int64_t np = N.nn_pad;
-    const double* __restrict__ fe = static_cast<const double*>(E.fe);
+__device__ __forceinline__ void node_group(const NodeView& N, const double dt_i, const double dt_i_1, const double amp,
+                                           const int64_t n0, double& kin, double& wext, int32_t& bad) {
+    const int64_t np = N.np, nn = N.nn;
+    const double* __restrict__ fe = static_cast<const double*>(N.fe);
     double* __restrict__ V = static_cast<double*>(N.v);
     const double half = (dt_i + dt_i_1);
     const double dt_avg = (dt_i + dt_i_1) / 2.0;
-    const uint32_t msk = ld_bytes<W>(N.slot_mask + n0);
     double f[3][W];
 #pragma unroll
     for (int c = 0; c < 3; ++c)
 #pragma unroll
         for (int j = 0; j < W; ++j) f[c][j] = 0.0;
+    const uint32_t msk = ENSC_NODE_ALL_SLOTS ? 0xffffffffu : ld_bytes<W>(N.slot_mask + n0);
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
         uint32_t sel = 0;
@@ -727,8 +727,8 @@ __device__ __forceinline__ void node_group(const ElemArrays& E, const NodeArrays
             if (n0 + j >= nn) continue;
             double a = f[c][j];
             double g = 0.0;
-            if (M.gravity_on) {
-                g = amp * M.gravity_value * M.gravity_dir[c] / im[j];
+            if (N.gravity_on) {
+                g = amp * N.gravity_value * N.gravity_dir[c] / im[j];
                 a = a + g;
             }
             const uint32_t cc = (code >> (8 * j + 2 * c)) & 3u;
@@ -790,7 +790,8 @@ __global__ void __launch_bounds__(kNodeThreads, ENSC_NODE_MINB_FP64) k_node(Elem
     const int64_t t0 = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (E.slot_major && E.tiles_aligned) {
         constexpr int W = kNodeGroupFp64;
-        for (int64_t g = t0; g * W < nn; g += stride) node_group<W>(E, N, M, dt_i, dt_i_1, amp, g * W, nn, kin, wext, bad);
+        const NodeView nv = node_view(E, N, M, ctl);
+        for (int64_t g = t0; g * W < nn; g += stride) node_group<W>(nv, dt_i, dt_i_1, amp, g * W, kin, wext, bad);
     } else {
         for (int64_t n = t0; n < nn; n += stride) node_body(E, N, M, dt_i, dt_i_1, amp, n, kin, wext, bad);
     }
@@ -914,9 +915,11 @@ __global__ void __launch_bounds__(kStageTileF64, 2) k_element_batch_fp64(BatchTa
         bad = static_cast<int32_t>(__reduce_or_sync(0xffffffffu, static_cast<unsigned>(bad)));
         if (live && lane == 0) {
             double* part = T.etile_part + 3 * (t * NW + wid);
-            part[0] += ei;
-            part[1] += eh;
-            part[2] += ev;
+            // one writer per slot and pass: the reductions (no return value)
+            // add in cycle order without a round trip
+            atomicAdd(part + 0, ei);
+            atomicAdd(part + 1, eh);
+            atomicAdd(part + 2, ev);
             atomicMin(&ctl->dts_next, dmin);
             atomicMin(&ctl->len_min, lmin);
             if (bad) atomicOr(&ctl->status, bad);
@@ -941,39 +944,56 @@ __global__ void __launch_bounds__(kStageTileF64, 2) k_element_batch_fp64(BatchTa
     }
 }
 
+// As k_node_batch_mixed: one warp per node tile, slots and first nodes read
+// two tiles ahead, table lines prefetched into L1 one tile ahead.
 __global__ void __launch_bounds__(kNodeThreads, ENSC_NODE_MINB_FP64) k_node_batch_fp64(BatchTables T) {
     constexpr int W = kNodeGroupFp64;
     const int lane = threadIdx.x & 31;
     const int warp = static_cast<int>((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
     const int nwarps = static_cast<int>((static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5);
     const int ntiles = T.counts[1];
+    int slot = warp < ntiles ? __ldg(T.ntile_inst + warp) : 0;
+    int slot_n = warp + nwarps < ntiles ? __ldg(T.ntile_inst + warp + nwarps) : 0;
+    int base = warp < ntiles ? __ldg(T.ntile_base + warp) : 0;
+    int base_n = warp + nwarps < ntiles ? __ldg(T.ntile_base + warp + nwarps) : 0;
     for (int t = warp; t < ntiles; t += nwarps) {
-        const int slot = T.ntile_inst[t];
-        const NodeParam p = T.nparam[slot];
-        if (!p.live) continue;
-        const InstanceDesc& d = T.desc[slot];
-        double* part = T.ntile_part + 2 * static_cast<int64_t>(t);
-        const double dt_i = p.dt_i, dt_i_1 = p.dt_i_1, amp = p.amp;
-        double kin = 0.0, wext = 0.0;
-        int32_t bad = 0;
-        const int64_t n0 = static_cast<int64_t>(T.ntile_base[t]) + static_cast<int64_t>(lane) * W;
-        const int64_t nn = d.N.nn;
-        if (n0 < nn) {
-            if (d.E.slot_major && d.E.tiles_aligned) {
-                node_group<W>(d.E, d.N, d.M, dt_i, dt_i_1, amp, n0, nn, kin, wext, bad);
-            } else {
-                for (int j = 0; j < W && n0 + j < nn; ++j)
-                    node_body(d.E, d.N, d.M, dt_i, dt_i_1, amp, n0 + j, kin, wext, bad);
+        const int t2 = t + 2 * nwarps;
+        const int slot_nn = t2 < ntiles ? __ldg(T.ntile_inst + t2) : 0;
+        const int base_nn = t2 < ntiles ? __ldg(T.ntile_base + t2) : 0;
+        if (lane == 0) {
+            prefetch_l1(T.nview + slot_n);
+            prefetch_l1(T.nparam + slot_n);
+        }
+        const NodeParam p = ld_param(T.nparam + slot);
+        if (p.live) {
+            const NodeView v = ld_view(T.nview + slot);
+            const double dt_i = p.dt_i, dt_i_1 = p.dt_i_1, amp = p.amp;
+            double kin = 0.0, wext = 0.0;
+            int32_t bad = 0;
+            const int64_t n0 = static_cast<int64_t>(base) + static_cast<int64_t>(lane) * W;
+            if (n0 < v.nn) {
+                if (v.grouped) {
+                    node_group<W>(v, dt_i, dt_i_1, amp, n0, kin, wext, bad);
+                } else {
+                    const InstanceDesc& d = T.desc[slot];
+                    for (int j = 0; j < W && n0 + j < v.nn; ++j)
+                        node_body(d.E, d.N, d.M, dt_i, dt_i_1, amp, n0 + j, kin, wext, bad);
+                }
+            }
+            kin = warp_sum_b(kin);
+            wext = warp_sum_b(wext);
+            bad = static_cast<int32_t>(__reduce_or_sync(0xffffffffu, static_cast<unsigned>(bad)));
+            if (lane == 0) {
+                double* part = T.ntile_part + 2 * static_cast<int64_t>(t);
+                if (bad) atomicOr(&v.ctl->status, bad);
+                part[0] = kin;
+                atomicAdd(part + 1, wext);  // one writer per slot and pass
             }
         }
-        kin = warp_sum_b(kin);
-        wext = warp_sum_b(wext);
-        bad = static_cast<int32_t>(__reduce_or_sync(0xffffffffu, static_cast<unsigned>(bad)));
-        if (lane == 0) {
-            if (bad) atomicOr(&d.ctl->status, bad);
-            part[0] = kin;
-            part[1] += wext;
-        }
+        slot = slot_n;
+        slot_n = slot_nn;
+        base = base_n;
+        base_n = base_nn;
     }
 }
 

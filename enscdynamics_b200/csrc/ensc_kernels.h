@@ -44,6 +44,22 @@ constexpr int kNodeUnrollMixed = ENSC_NODE_UNROLL_MIXED;
 #ifndef ENSC_BATCH_MINB_MIXED
 #define ENSC_BATCH_MINB_MIXED 8
 #endif
+// 1: the staged mixed element passes read A and the connectivity from the
+// stage again for the force step instead of keeping them in registers
+#ifndef ENSC_MIXED_REREAD
+#define ENSC_MIXED_REREAD 1
+#endif
+// how the batched mixed element pass reads the staged instance descriptor:
+// 1 all fields copied to registers per tile, 2 arrays copied and material
+// constants read at use, 0 everything read at use
+#ifndef ENSC_BATCH_DESC_MODE
+#define ENSC_BATCH_DESC_MODE 2
+#endif
+// 1: the grouped node passes sum all 8 force slots (empty ones hold zeros)
+// instead of reading the slot mask first
+#ifndef ENSC_NODE_ALL_SLOTS
+#define ENSC_NODE_ALL_SLOTS 1
+#endif
 #ifndef ENSC_NODE_BATCH_MINB_MIXED
 #define ENSC_NODE_BATCH_MINB_MIXED 3
 #endif

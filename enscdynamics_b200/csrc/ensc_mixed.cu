@@ -413,6 +413,18 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
     }
     // nodal forces f_j = -(B0_j Z) - Gamma_j Gq^T with B0_j Z = s_j^T Y / 8,
     // Y = A^T Z
+    // (from a shared-memory stage, A and the connectivity are read again
+    // here rather than kept in registers across the stress update)
+    constexpr bool kReread = SMEM && ENSC_MIXED_REREAD;
+    if (kReread) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int m = 0; m < 3; ++m) {
+                Ah[c][m] = S.a[(3 * c + m) * ss + si];
+                Al[c][m] = S.a[(9 + 3 * c + m) * ss + si];
+            }
+    }
     float Y[3][3];
 #pragma unroll
     for (int m = 0; m < 3; ++m)
@@ -426,6 +438,10 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
             t = fmaf(Ah[2][m], Z[2][i], t);
             Y[m][i] = 0.125f * t;
         }
+    if (kReread) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) nk[k] = S.conn[k * ss + si];
+    }
     // per force component: the node values of -(B0_j Z) - Gamma_j Gq^T from
     // their corner coefficients (-Y on xi, eta, zeta; -Gq on the hourglass
     // vectors, signed as Gamma)
@@ -695,25 +711,27 @@ __device__ __forceinline__ void node_body_mixed(const ElemArrays& E, const NodeA
 
 // W consecutive nodes of the mixed node pass with 16-byte row accesses
 // (float4 force slots and velocities, pairs of doubles for x, u and the
-// inverse mass); per node the arithmetic of node_body_mixed.  Nodes at or
-// past nn (row padding) are loaded and stored back unchanged.
+// inverse mass); per node the arithmetic of node_body_mixed.  Slots the mask
+// marks empty are skipped, or (ENSC_NODE_ALL_SLOTS) summed as the zeros they
+// hold: the slot-major rows start zeroed and only the slot's element writes
+// them.  Nodes at or past nn (row padding) are loaded and stored back
+// unchanged.
 template <int W>
-__device__ __forceinline__ void node_group_mixed(const ElemArrays& E, const NodeArrays& N, const Material& M,
-                                                 const double dt_i, const double dt_i_1, const double amp,
-                                                 const int64_t n0, const int64_t nn, double& kin, double& wext,
+__device__ __forceinline__ void node_group_mixed(const NodeView& N, const double dt_i, const double dt_i_1,
+                                                 const double amp, const int64_t n0, double& kin, double& wext,
                                                  int32_t& bad) {
-    const int64_t np = N.nn_pad;
-    const float* __restrict__ fe = static_cast<const float*>(E.fe);
+    const int64_t np = N.np, nn = N.nn;
+    const float* __restrict__ fe = static_cast<const float*>(N.fe);
     float* __restrict__ V = static_cast<float*>(N.v);
     const float hdt = static_cast<float>(0.5 * (dt_i + dt_i_1));
     const float hdt_lo = static_cast<float>(0.5 * (dt_i + dt_i_1) - static_cast<double>(hdt));
     const double dt_avg = 0.5 * (dt_i + dt_i_1);
-    const uint32_t msk = ld_bytes<W>(N.slot_mask + n0);
     float f[3][W];
 #pragma unroll
     for (int c = 0; c < 3; ++c)
 #pragma unroll
         for (int j = 0; j < W; ++j) f[c][j] = 0.f;
+    const uint32_t msk = ENSC_NODE_ALL_SLOTS ? 0xffffffffu : ld_bytes<W>(N.slot_mask + n0);
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
         uint32_t sel = 0;
@@ -748,8 +766,8 @@ __device__ __forceinline__ void node_group_mixed(const ElemArrays& E, const Node
             if (n0 + j >= nn) continue;
             float a = f[c][j];
             float g = 0.f;
-            if (M.gravity_on) {
-                g = static_cast<float>(amp * M.gravity_value * M.gravity_dir[c] / im[j]);
+            if (N.gravity_on) {
+                g = static_cast<float>(amp * N.gravity_value * N.gravity_dir[c] / im[j]);
                 a += g;
             }
             const uint32_t cc = (code >> (8 * j + 2 * c)) & 3u;
@@ -806,8 +824,8 @@ __global__ void __launch_bounds__(kNodeThreads, ENSC_NODE_MINB_MIXED) k_node_mix
     const int64_t t0 = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (E.slot_major && E.tiles_aligned) {
         constexpr int W = kNodeGroupMixed;
-        for (int64_t g = t0; g * W < nn; g += stride)
-            node_group_mixed<W>(E, N, M, dt_i, dt_i_1, amp, g * W, nn, kin, wext, bad);
+        const NodeView nv = node_view(E, N, M, ctl);
+        for (int64_t g = t0; g * W < nn; g += stride) node_group_mixed<W>(nv, dt_i, dt_i_1, amp, g * W, kin, wext, bad);
     } else {
         for (int64_t n = t0; n < nn; n += stride) node_body_mixed(E, N, M, dt_i, dt_i_1, amp, n, kin, wext, bad);
     }
@@ -937,12 +955,22 @@ __global__ void __launch_bounds__(kStageTile, ENSC_BATCH_MINB_MIXED) k_element_b
         int32_t bad = 0;
         const int64_t e = static_cast<int64_t>(ti.base) + tid;
         if (live && e < d.E.ne) {
+#if ENSC_BATCH_DESC_MODE == 1
             // the instance's arrays and constants, read from the stage once:
             // the body's stores could alias the stage as far as the compiler
             // knows, so references into it would be re-read after each store
             const ElemArrays E = d.E;
             const NodeArrays N = d.N;
             const Material M = d.M;
+#elif ENSC_BATCH_DESC_MODE == 2
+            const ElemArrays E = d.E;
+            const NodeArrays N = d.N;
+            const Material& M = d.M;
+#else
+            const ElemArrays& E = d.E;
+            const NodeArrays& N = d.N;
+            const Material& M = d.M;
+#endif
             const double dt1d = h.dt1;
             const float dt1 = static_cast<float>(dt1d);
             const float* st = reinterpret_cast<const float*>(sb);
@@ -967,9 +995,11 @@ __global__ void __launch_bounds__(kStageTile, ENSC_BATCH_MINB_MIXED) k_element_b
         bad = static_cast<int32_t>(__reduce_or_sync(0xffffffffu, static_cast<unsigned>(bad)));
         if (live && lane == 0) {
             double* part = T.etile_part + 3 * (t * NW + wid);
-            part[0] += ei;
-            part[1] += eh;
-            part[2] += ev;
+            // one writer per slot and pass: the reductions (no return value)
+            // add in cycle order without a round trip
+            atomicAdd(part + 0, ei);
+            atomicAdd(part + 1, eh);
+            atomicAdd(part + 2, ev);
             atomicMin(&ctl->dts_next, dmin);
             atomicMin(&ctl->len_min, lmin);
             if (bad) atomicOr(&ctl->status, bad);
@@ -992,46 +1022,58 @@ __global__ void __launch_bounds__(kStageTile, ENSC_BATCH_MINB_MIXED) k_element_b
     }
 }
 
+// One warp per node tile.  The tile's instance slot and first node are read
+// two tiles ahead and its NodeView and NodeParam lines prefetched into L1 one
+// tile ahead, so a tile starts on its node rows without waiting on the
+// tables.
 __global__ void __launch_bounds__(kNodeThreads, ENSC_NODE_BATCH_MINB_MIXED) k_node_batch_mixed(BatchTables T) {
     constexpr int W = kNodeGroupMixed;
     const int lane = threadIdx.x & 31;
     const int warp = static_cast<int>((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
     const int nwarps = static_cast<int>((static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5);
     const int ntiles = T.counts[1];
+    int slot = warp < ntiles ? __ldg(T.ntile_inst + warp) : 0;
+    int slot_n = warp + nwarps < ntiles ? __ldg(T.ntile_inst + warp + nwarps) : 0;
+    int base = warp < ntiles ? __ldg(T.ntile_base + warp) : 0;
+    int base_n = warp + nwarps < ntiles ? __ldg(T.ntile_base + warp + nwarps) : 0;
     for (int t = warp; t < ntiles; t += nwarps) {
-        const int slot = T.ntile_inst[t];
-        const NodeParam p = T.nparam[slot];
-        if (!p.live) continue;
-        // the instance's arrays and constants, read once per tile (references
-        // into the table would be re-read after every store)
-        struct {
-            ElemArrays E;
-            NodeArrays N;
-            Material M;
-            Ctl* ctl;
-        } const d{T.desc[slot].E, T.desc[slot].N, T.desc[slot].M, T.desc[slot].ctl};
-        double* part = T.ntile_part + 2 * static_cast<int64_t>(t);
-        const double dt_i = p.dt_i, dt_i_1 = p.dt_i_1, amp = p.amp;
-        double kin = 0.0, wext = 0.0;
-        int32_t bad = 0;
-        const int64_t n0 = static_cast<int64_t>(T.ntile_base[t]) + static_cast<int64_t>(lane) * W;
-        const int64_t nn = d.N.nn;
-        if (n0 < nn) {
-            if (d.E.slot_major && d.E.tiles_aligned) {
-                node_group_mixed<W>(d.E, d.N, d.M, dt_i, dt_i_1, amp, n0, nn, kin, wext, bad);
-            } else {
-                for (int j = 0; j < W && n0 + j < nn; ++j)
-                    node_body_mixed(d.E, d.N, d.M, dt_i, dt_i_1, amp, n0 + j, kin, wext, bad);
+        const int t2 = t + 2 * nwarps;
+        const int slot_nn = t2 < ntiles ? __ldg(T.ntile_inst + t2) : 0;
+        const int base_nn = t2 < ntiles ? __ldg(T.ntile_base + t2) : 0;
+        if (lane == 0) {
+            prefetch_l1(T.nview + slot_n);
+            prefetch_l1(T.nparam + slot_n);
+        }
+        const NodeParam p = ld_param(T.nparam + slot);
+        if (p.live) {
+            const NodeView v = ld_view(T.nview + slot);
+            const double dt_i = p.dt_i, dt_i_1 = p.dt_i_1, amp = p.amp;
+            double kin = 0.0, wext = 0.0;
+            int32_t bad = 0;
+            const int64_t n0 = static_cast<int64_t>(base) + static_cast<int64_t>(lane) * W;
+            if (n0 < v.nn) {
+                if (v.grouped) {
+                    node_group_mixed<W>(v, dt_i, dt_i_1, amp, n0, kin, wext, bad);
+                } else {
+                    const InstanceDesc& d = T.desc[slot];
+                    for (int j = 0; j < W && n0 + j < v.nn; ++j)
+                        node_body_mixed(d.E, d.N, d.M, dt_i, dt_i_1, amp, n0 + j, kin, wext, bad);
+                }
+            }
+            kin = warp_sum_b(kin);
+            wext = warp_sum_b(wext);
+            bad = static_cast<int32_t>(__reduce_or_sync(0xffffffffu, static_cast<unsigned>(bad)));
+            if (lane == 0) {
+                double* part = T.ntile_part + 2 * static_cast<int64_t>(t);
+                if (bad) atomicOr(&v.ctl->status, bad);
+                part[0] = kin;
+                atomicAdd(part + 1, wext);  // one writer per slot and pass
             }
         }
-        kin = warp_sum_b(kin);
-        wext = warp_sum_b(wext);
-        bad = static_cast<int32_t>(__reduce_or_sync(0xffffffffu, static_cast<unsigned>(bad)));
-        if (lane == 0) {
-            if (bad) atomicOr(&d.ctl->status, bad);
-            part[0] = kin;
-            part[1] += wext;
-        }
+        slot = slot_n;
+        slot_n = slot_nn;
+        base = base_n;
+        base_n = base_nn;
     }
 }
 
