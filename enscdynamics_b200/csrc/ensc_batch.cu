@@ -206,7 +206,6 @@ int rebuild_tables(ensc_batch* b) {
 void launch_cycle(ensc_batch* b, int ge, int gn, cudaStream_t st) {
     ensc::launch_between_batch(b->T, b->slots, 0, st);
     ensc::launch_edge_prepass_batch(b->T, b->sms * b->occ_pre, st);
-    ensc::launch_begin_exact_batch(b->T, b->slots, st);
     if (is_mixed(b)) {
         ensc::launch_element_batch_mixed(b->T, ge, st);
         ensc::launch_node_params_batch(b->T, b->slots, st);
@@ -393,6 +392,7 @@ int ensc_batch_create(const ensc_params* params, int32_t max_instances, int64_t 
     b->T.etile = b->etile;
     b->T.ntile = b->ntile;
     b->T.exact_count = b->d_counts + 3;
+    b->T.prepass_done = b->d_counts + 4;
     b->T.nparam = b->d_nparam;
     b->T.sparam = b->d_sparam;
     b->T.etile_src = b->d_etile_src;

@@ -161,11 +161,12 @@ __global__ void __launch_bounds__(128) k_edge_prepass(ElemArrays E, NodeArrays N
 
 // Rest of update_minVertex_perMaterial_and_dt and run()'s clamp for a cycle
 // that needed the exact edge minimum.
-__device__ __forceinline__ void begin_exact(Ctl* ctl) {
+// (len_min_bits: the edge minimum of the prepass, ordered bits)
+__device__ __forceinline__ void begin_exact(Ctl* ctl, unsigned long long len_min_bits) {
     const double time = ctl->time;
     double dt_i_1 = ctl->dt_prev;
     const double time_prev = time + dt_i_1;
-    double d = bits_ord(ctl->len_min) / ctl->wos;
+    double d = bits_ord(len_min_bits) / ctl->wos;
     d = d < ctl->dts_cur ? d : ctl->dts_cur;
     double dt_i = d * ctl->factor;
     if ((ctl->total_time - time_prev) < dt_i && (ctl->total_time - time_prev) > 0.0) {
@@ -187,7 +188,7 @@ __device__ __forceinline__ void begin_exact(Ctl* ctl) {
 
 __global__ void k_begin_exact(Ctl* ctl) {
     if (threadIdx.x != 0 || ctl->done || !ctl->need_exact) return;
-    begin_exact(ctl);
+    begin_exact(ctl, ctl->len_min);
 }
 
 __global__ void k_arm(Ctl* ctl, double step_end, long long max_cycles, double pause) {
@@ -272,7 +273,7 @@ __global__ void k_aos_to_soa(const double* aos, int64_t n, int64_t pad, int comp
 // reached their limits as done, and counts the instances whose cycle needs
 // the edge prepass.  The energy terms stay in the per-tile accumulators
 // until k_fold_batch.  Each slot's element-pass scalars (dt_i_1, live) go to
-// T.sparam; k_begin_exact_batch rewrites them where the prepass decides dt.
+// T.sparam; the edge prepass rewrites them where it decides dt.
 __global__ void k_begin_batch(BatchTables T, int begin) {
     const int slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= T.counts[2]) return;
@@ -404,19 +405,30 @@ __global__ void __launch_bounds__(128) k_edge_prepass_batch(BatchTables T) {
         }
         if (lane == 0) atomicMin(&ctl->len_min, b);
     }
+    // the last block to finish begins the exact cycles (k_begin_exact for
+    // each such instance) and clears the counters
+    __shared__ int last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(T.prepass_done, 1) == static_cast<int>(gridDim.x) - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    for (int slot = threadIdx.x; slot < T.counts[2]; slot += blockDim.x) {
+        const InstanceDesc& d = T.desc[slot];
+        if (!d.active) continue;
+        Ctl* ctl = d.ctl;
+        if (ctl->done || !ctl->need_exact) continue;
+        // the edge minimum through L2 (this block may hold an older copy)
+        begin_exact(ctl, atomicOr(&ctl->len_min, 0ull));
+        T.sparam[slot].dt1 = ctl->dt_i_1;
+    }
+    if (threadIdx.x == 0) {
+        *T.prepass_done = 0;
+        *T.exact_count = 0;
+    }
 }
 
-__global__ void k_begin_exact_batch(BatchTables T) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) *T.exact_count = 0;  // the prepass has read it
-    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= T.counts[2]) return;
-    const InstanceDesc& d = T.desc[slot];
-    if (!d.active) return;
-    Ctl* ctl = d.ctl;
-    if (ctl->done || !ctl->need_exact) return;
-    begin_exact(ctl);
-    T.sparam[slot].dt1 = ctl->dt_i_1;
-}
 
 int grid_for(int64_t work, int threads) {
     const int64_t g = (work + threads - 1) / threads;
@@ -434,9 +446,6 @@ void launch_node_params_batch(const BatchTables& T, int slots, cudaStream_t st) 
 }
 void launch_edge_prepass_batch(const BatchTables& T, int grid, cudaStream_t st) {
     k_edge_prepass_batch<<<grid, 128, 0, st>>>(T);
-}
-void launch_begin_exact_batch(const BatchTables& T, int slots, cudaStream_t st) {
-    k_begin_exact_batch<<<(slots + 127) / 128, 128, 0, st>>>(T);
 }
 void launch_between(Ctl* ctl, const Partials& P, int mode, cudaStream_t st) {
     k_between<<<1, kCtlThreads, 0, st>>>(ctl, P, mode);

@@ -261,6 +261,7 @@ struct BatchTables {
     double* etile_part;          // [etiles][etile / 32][3] internal / hourglass / viscous work per tile warp
     double* ntile_part;          // [ntiles][2] kinetic energy / external work per tile
     int32_t* exact_count;        // instances whose current cycle needs the edge prepass
+    int32_t* prepass_done;       // blocks of the edge prepass that have finished
     NodeParam* nparam;           // [slots] this cycle's node-pass scalars
     StageHdr* sparam;            // [slots] this cycle's element-pass scalars
     const NodeView* nview;       // [slots]

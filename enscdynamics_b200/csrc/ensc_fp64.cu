@@ -567,9 +567,10 @@ __device__ __forceinline__ const double* f64_stage_row(const ElemArrays& E, int 
     return static_cast<const double*>(E.bt) + (r - kF64StageRows) * ep;
 }
 
-// Thread 0: the tile starting at element `base` into the stage at shared
+// Warp 0: the tile starting at element `base` into the stage at shared
 // address dst, completing on bar (rows padded to 32 entries and 256-byte
-// aligned: every copy is 16-byte aligned and a multiple of 128 bytes).
+// aligned: every copy is 16-byte aligned and a multiple of 128 bytes); lane
+// 0 arms the barrier, then the lanes start the row copies between them.
 __device__ __forceinline__ uint32_t f64_stage_count(const ElemArrays& E, int64_t base) {
     const int64_t left = E.ne_pad - base;
     return static_cast<uint32_t>(left < kStageTileF64 ? left : kStageTileF64);
@@ -581,21 +582,23 @@ __device__ __forceinline__ uint32_t f64_stage_tx_bytes(uint32_t cnt) {
     return 8u * cnt * 4u + static_cast<uint32_t>(dcopies) * cnt * 8u;
 }
 template <bool PLASTIC, bool BT>
-__device__ __forceinline__ void f64_stage_copies(const ElemArrays& E, uint32_t dst, uint32_t bar, int64_t base,
-                                                 uint32_t cnt) {
+__device__ __forceinline__ void f64_stage_issue(const ElemArrays& E, uint32_t dst, uint32_t bar, int64_t base,
+                                                int lane) {
     constexpr int drows = kF64StageRows + (BT ? 24 : 0);
-    for (int k = 0; k < 8; ++k) bulk_g2s(dst + k * (kStageTileF64 * 4u), E.conn + k * E.ne_pad + base, cnt * 4u, bar);
-    const uint32_t dbase = dst + 8u * kStageTileF64 * 4u;
-    for (int r = 0; r < drows; ++r) {
-        if (!PLASTIC && r == 21) continue;  // eps_p is read only with J2
-        bulk_g2s(dbase + r * (kStageTileF64 * 8u), f64_stage_row(E, r) + base, cnt * 8u, bar);
-    }
-}
-template <bool PLASTIC, bool BT>
-__device__ __forceinline__ void f64_stage_issue(const ElemArrays& E, uint32_t dst, uint32_t bar, int64_t base) {
     const uint32_t cnt = f64_stage_count(E, base);
-    mbar_arrive_expect_tx(bar, f64_stage_tx_bytes<PLASTIC, BT>(cnt));
-    f64_stage_copies<PLASTIC, BT>(E, dst, bar, base, cnt);
+    if (lane == 0) mbar_arrive_expect_tx(bar, f64_stage_tx_bytes<PLASTIC, BT>(cnt));
+    __syncwarp();
+    fence_proxy_async_smem();  // the block's reads of this stage come before the copies into it
+    const uint32_t dbase = dst + 8u * kStageTileF64 * 4u;
+    for (int q = lane; q < 8 + drows; q += 32) {
+        if (q < 8) {
+            bulk_g2s(dst + q * (kStageTileF64 * 4u), E.conn + q * E.ne_pad + base, cnt * 4u, bar);
+        } else {
+            const int r = q - 8;
+            if (PLASTIC || r != 21)  // eps_p is read only with J2
+                bulk_g2s(dbase + r * (kStageTileF64 * 8u), f64_stage_row(E, r) + base, cnt * 8u, bar);
+        }
+    }
 }
 
 template <bool PLASTIC, bool BT>
@@ -606,7 +609,7 @@ __global__ void __launch_bounds__(kStageTileF64, BT ? 2 : 3)
     constexpr uint32_t SB = f64_stage_bytes<BT>();
     constexpr int T = kStageTileF64;
     const double dt1 = ctl->dt_i_1;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const uint32_t stage0 = smem_addr(smem);
     const uint32_t bar0 = stage0 + 2 * SB;
     const int64_t ntiles = (E.ne + T - 1) / T;
@@ -617,10 +620,10 @@ __global__ void __launch_bounds__(kStageTileF64, BT ? 2 : 3)
         mbar_init_fence();
     }
     __syncthreads();
-    if (tid == 0) {
+    if (wid == 0) {
         for (int s = 0; s < 2; ++s) {
             const int64_t t = blockIdx.x + s * gstride;
-            if (t < ntiles) f64_stage_issue<PLASTIC, BT>(E, stage0 + s * SB, bar0 + 8 * s, t * T);
+            if (t < ntiles) f64_stage_issue<PLASTIC, BT>(E, stage0 + s * SB, bar0 + 8 * s, t * T, lane);
         }
     }
     double e_int = 0.0, e_hg = 0.0, e_vis = 0.0;
@@ -651,10 +654,7 @@ __global__ void __launch_bounds__(kStageTileF64, BT ? 2 : 3)
         }
         __syncthreads();  // the block is done with stage s
         const int64_t tn = t + 2 * gstride;
-        if (tid == 0 && tn < ntiles) {
-            fence_proxy_async_smem();
-            f64_stage_issue<PLASTIC, BT>(E, stage0 + s * SB, bar, tn * T);
-        }
+        if (wid == 0 && tn < ntiles) f64_stage_issue<PLASTIC, BT>(E, stage0 + s * SB, bar, tn * T, lane);
     }
     if (timed_out) {
         // record the failure and let the copies this block started land
@@ -826,37 +826,65 @@ __device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v)
     return v;
 }
 
-// A batch stage: the single-instance stage (B0^T included) followed by the
-// tile's instance descriptor, so that the element body reads arrays and
-// material from shared memory.  Tiles of instances that are done get only the
-// descriptor (done cannot change during the pass).
-constexpr uint32_t kF64BatchStageBytes = f64_stage_bytes<true>() + (sizeof(InstanceDesc) + 127) / 128 * 128;
+// A batch stage: the single-instance stage (B0^T included), then the tile's
+// instance descriptor, its element-pass scalars (StageHdr), the TileInfo the
+// filling warp writes, and the ETileSrc record of the tile that uses the
+// stage next (as in the mixed batch pass).
+constexpr uint32_t kF64DescOff = f64_stage_bytes<true>();
+constexpr uint32_t kF64HdrOff = kF64DescOff + sizeof(InstanceDesc);
+constexpr uint32_t kF64InfoOff = kF64HdrOff + sizeof(StageHdr);
+constexpr uint32_t kF64NextOff = kF64InfoOff + sizeof(TileInfo);
+constexpr uint32_t kF64BatchStageBytes = (kF64NextOff + sizeof(ETileSrc) + 127) / 128 * 128;
 constexpr size_t kF64BatchStageSmem = 2 * static_cast<size_t>(kF64BatchStageBytes) + 16;
-static_assert(sizeof(InstanceDesc) + sizeof(StageHdr) <= kF64BatchStageBytes - f64_stage_bytes<true>(), "stage tail");
+static_assert(sizeof(InstanceDesc) % 16 == 0, "16-byte copies");
 
-__device__ __forceinline__ StageHdr* f64_stage_hdr(unsigned char* smem, int s) {
-    return reinterpret_cast<StageHdr*>(smem + s * kF64BatchStageBytes + f64_stage_bytes<true>() + sizeof(InstanceDesc));
+// double row r (as f64_stage_row) of a batch tile in global memory
+__device__ __forceinline__ const double* f64_tile_row(const ETileSrc& src, int r) {
+    const int64_t ep = src.ne_pad;
+    if (r < 6) return static_cast<const double*>(src.sigma) + r * ep;
+    if (r < 18) return static_cast<const double*>(src.qia) + (r - 6) * ep;
+    if (r == 18) return static_cast<const double*>(src.vol0);
+    if (r == 19) return static_cast<const double*>(src.cbrt_v0);
+    if (r == 20) return static_cast<const double*>(src.cbrt_v0sq);
+    if (r == 21) return static_cast<const double*>(src.eps_p);
+    return static_cast<const double*>(src.bt) + (r - kF64StageRows) * ep;
 }
 
-__device__ __forceinline__ void f64_batch_stage_issue(const BatchTables& T, int64_t t, uint32_t dst, uint32_t bar,
-                                                StageHdr* hdr) {
-    const InstanceDesc* dp = T.desc + T.etile_inst[t];
-    const Ctl* c = dp->ctl;
-    const int32_t done = c->done;
-    hdr->live = done ? 0 : 1;  // visible to the waiters through the arrive below
-    hdr->dt1 = c->dt_i_1;
-    const uint32_t db = static_cast<uint32_t>(sizeof(InstanceDesc));
-    const int64_t base = T.etile_base[t];
-    if (done) {
-        mbar_arrive_expect_tx(bar, db);
-    } else {
-        const uint32_t cnt = f64_stage_count(dp->E, base);
-        mbar_arrive_expect_tx(bar, f64_stage_tx_bytes<true, true>(cnt) + db);
-        f64_stage_copies<true, true>(dp->E, dst, bar, base, cnt);
+__device__ __forceinline__ void f64_batch_stage_issue(const BatchTables& T, const ETileSrc& src, int64_t t_next,
+                                                      int64_t ntiles, unsigned char* stage, uint32_t dst, uint32_t bar,
+                                                      int lane) {
+    constexpr int drows = kF64StageRows + 24;
+    const uint32_t cnt = static_cast<uint32_t>(src.cnt);
+    const bool next = t_next < ntiles;
+    if (lane == 0) {
+        TileInfo* ti = reinterpret_cast<TileInfo*>(stage + kF64InfoOff);
+        ti->slot = src.slot;
+        ti->base = src.base;
+        mbar_arrive_expect_tx(bar, f64_stage_tx_bytes<true, true>(cnt) + sizeof(InstanceDesc) + sizeof(StageHdr) +
+                                       (next ? sizeof(ETileSrc) : 0u));
     }
-    bulk_g2s(dst + f64_stage_bytes<true>(), dp, db, bar);
+    __syncwarp();
+    fence_proxy_async_smem();  // the block's reads of this stage come before the copies into it
+    const uint32_t dbase = dst + 8u * kStageTileF64 * 4u;
+    for (int q = lane; q < 8 + drows + 3; q += 32) {
+        if (q < 8)
+            bulk_g2s(dst + q * (kStageTileF64 * 4u), static_cast<const uint32_t*>(src.conn) + q * src.ne_pad,
+                     cnt * 4u, bar);
+        else if (q < 8 + drows)
+            bulk_g2s(dbase + (q - 8) * (kStageTileF64 * 8u), f64_tile_row(src, q - 8), cnt * 8u, bar);
+        else if (q == 8 + drows)
+            bulk_g2s(dst + kF64DescOff, T.desc + src.slot, sizeof(InstanceDesc), bar);
+        else if (q == 8 + drows + 1)
+            bulk_g2s(dst + kF64HdrOff, T.sparam + src.slot, sizeof(StageHdr), bar);
+        else if (next)
+            bulk_g2s(dst + kF64NextOff, T.etile_src + t_next, sizeof(ETileSrc), bar);
+    }
 }
 
+// The batched FP64 element pass: element_body's arithmetic per element, so
+// states are bit-identical to the single-instance pass.  A block's
+// consecutive tiles of one instance form a run whose sums and minima are
+// reduced once, into the partial slot of the run's first tile.
 __global__ void __launch_bounds__(kStageTileF64, 2) k_element_batch_fp64(BatchTables T) {
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr int TT = kStageTileF64;
@@ -873,12 +901,45 @@ __global__ void __launch_bounds__(kStageTileF64, 2) k_element_batch_fp64(BatchTa
         mbar_init_fence();
     }
     __syncthreads();
-    if (tid == 0) {
+    if (wid == 0) {
         for (int s = 0; s < 2; ++s) {
             const int64_t t = blockIdx.x + s * gstride;
-            if (t < ntiles) f64_batch_stage_issue(T, t, stage0 + s * SB, bar0 + 8 * s, f64_stage_hdr(smem, s));
+            if (t < ntiles) {
+                const ETileSrc src = T.etile_src[t];
+                f64_batch_stage_issue(T, src, t + 2 * gstride, ntiles, smem + s * SB, stage0 + s * SB, bar0 + 8 * s,
+                                      lane);
+            }
         }
     }
+    // the current run: instance slot, first tile, control block, liveness
+    int run_slot = -1;
+    int64_t run_tile = 0;
+    Ctl* run_ctl = nullptr;
+    bool run_live = false;
+    double ei = 0.0, eh = 0.0, ev = 0.0, dts = DBL_MAX, len = DBL_MAX;
+    int32_t bad = 0;
+    auto flush = [&]() {
+        ei = warp_sum_b(ei);
+        eh = warp_sum_b(eh);
+        ev = warp_sum_b(ev);
+        const unsigned long long dmin = warp_min_u64(ord_bits(dts));
+        const unsigned long long lmin = warp_min_u64(ord_bits(len));
+        bad = static_cast<int32_t>(__reduce_or_sync(0xffffffffu, static_cast<unsigned>(bad)));
+        if (run_live && lane == 0) {
+            double* part = T.etile_part + 3 * (run_tile * NW + wid);
+            // one writer per slot and pass: the reductions (no return value)
+            // add in cycle order without a round trip
+            atomicAdd(part + 0, ei);
+            atomicAdd(part + 1, eh);
+            atomicAdd(part + 2, ev);
+            atomicMin(&run_ctl->dts_next, dmin);
+            atomicMin(&run_ctl->len_min, lmin);
+            if (bad) atomicOr(&run_ctl->status, bad);
+        }
+        ei = eh = ev = 0.0;
+        dts = len = DBL_MAX;
+        bad = 0;
+    };
     bool timed_out = false;
     int it = 0;
     int64_t t = blockIdx.x;
@@ -890,50 +951,41 @@ __global__ void __launch_bounds__(kStageTileF64, 2) k_element_batch_fp64(BatchTa
             timed_out = true;
             break;
         }
-        const unsigned char* st = smem + s * SB;
-        const InstanceDesc& d = *reinterpret_cast<const InstanceDesc*>(st + f64_stage_bytes<true>());
-        const StageHdr& h = *f64_stage_hdr(smem, s);
-        Ctl* ctl = d.ctl;
-        const bool live = h.live != 0;
-        double ei = 0.0, eh = 0.0, ev = 0.0, dts = DBL_MAX, len = DBL_MAX;
-        int32_t bad = 0;
-        const int64_t e = static_cast<int64_t>(T.etile_base[t]) + tid;
-        if (live && e < d.E.ne) {
+        unsigned char* st = smem + s * SB;
+        const InstanceDesc& d = *reinterpret_cast<const InstanceDesc*>(st + kF64DescOff);
+        const StageHdr& h = *reinterpret_cast<const StageHdr*>(st + kF64HdrOff);
+        const TileInfo& ti = *reinterpret_cast<const TileInfo*>(st + kF64InfoOff);
+        if (ti.slot != run_slot) {
+            flush();
+            run_slot = ti.slot;
+            run_tile = t;
+            run_ctl = d.ctl;
+            run_live = h.live != 0;
+        }
+        const int64_t e = static_cast<int64_t>(ti.base) + tid;
+        if (run_live && e < d.E.ne) {
+            // arrays copied to registers, material read at use
+            const ElemArrays E = d.E;
+            const NodeArrays N = d.N;
             const double dt1 = h.dt1;
             const double* dr = reinterpret_cast<const double*>(st + 8 * TT * 4);
             const Fp64Src S{reinterpret_cast<const uint32_t*>(st), dr, dr + 6 * TT, dr + 18 * TT, dr + 19 * TT,
                             dr + 20 * TT, dr + 21 * TT, TT, tid, dr + kF64StageRows * TT, TT, tid};
-            element_body<true, false, true, true>(d.E, d.N, d.M, S, dt1, e, dts, len, ei, eh, ev, bad);
-        }
-        // each warp's sums go to its own slot (tile-major, warp-minor; folded
-        // in that order) and its minima to the instance's control block
-        ei = warp_sum_b(ei);
-        eh = warp_sum_b(eh);
-        ev = warp_sum_b(ev);
-        const unsigned long long dmin = warp_min_u64(ord_bits(dts));
-        const unsigned long long lmin = warp_min_u64(ord_bits(len));
-        bad = static_cast<int32_t>(__reduce_or_sync(0xffffffffu, static_cast<unsigned>(bad)));
-        if (live && lane == 0) {
-            double* part = T.etile_part + 3 * (t * NW + wid);
-            // one writer per slot and pass: the reductions (no return value)
-            // add in cycle order without a round trip
-            atomicAdd(part + 0, ei);
-            atomicAdd(part + 1, eh);
-            atomicAdd(part + 2, ev);
-            atomicMin(&ctl->dts_next, dmin);
-            atomicMin(&ctl->len_min, lmin);
-            if (bad) atomicOr(&ctl->status, bad);
+            double d1, l1;
+            element_body<true, false, true, true>(E, N, d.M, S, dt1, e, d1, l1, ei, eh, ev, bad);
+            dts = d1 < dts ? d1 : dts;
+            len = l1 < len ? l1 : len;
         }
         __syncthreads();  // the block is done with stage s
-        if (tid == 0) {
-            const int64_t tn = t + 2 * gstride;
-            if (tn < ntiles) {
-                fence_proxy_async_smem();
-                f64_batch_stage_issue(T, tn, stage0 + s * SB, bar, f64_stage_hdr(smem, s));
-            }
+        const int64_t tn = t + 2 * gstride;
+        if (wid == 0 && tn < ntiles) {
+            const ETileSrc src = *reinterpret_cast<const ETileSrc*>(st + kF64NextOff);
+            f64_batch_stage_issue(T, src, tn + 2 * gstride, ntiles, st, stage0 + s * SB, bar, lane);
         }
     }
-    if (timed_out && tid == 0) {
+    if (!timed_out) {
+        flush();
+    } else if (tid == 0) {
         // record the failure on the instance whose tile could not be read and
         // let the copies this block started land (bounded) before exiting
         atomicOr(&T.desc[T.etile_inst[t]].ctl->status, ST_TIMEOUT);

@@ -118,7 +118,6 @@ int batch_element_tile_fp64();
 int batch_node_tile(bool mixed_precision);
 void launch_between_batch(const BatchTables& T, int slots, int mode, cudaStream_t st);
 void launch_edge_prepass_batch(const BatchTables& T, int grid, cudaStream_t st);
-void launch_begin_exact_batch(const BatchTables& T, int slots, cudaStream_t st);
 // per-instance node-pass scalars (and the control-block updates of the node
 // pass); runs between the element and node passes
 void launch_node_params_batch(const BatchTables& T, int slots, cudaStream_t st);

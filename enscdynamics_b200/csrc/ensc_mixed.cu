@@ -934,6 +934,35 @@ __global__ void __launch_bounds__(kStageTile, ENSC_BATCH_MINB_MIXED) k_element_b
             }
         }
     }
+    // the current run: instance slot, first tile, control block, liveness
+    int run_slot = -1;
+    int64_t run_tile = 0;
+    Ctl* run_ctl = nullptr;
+    bool run_live = false;
+    double ei = 0.0, eh = 0.0, ev = 0.0, dts = DBL_MAX, len = DBL_MAX;
+    int32_t bad = 0;
+    auto flush = [&]() {
+        ei = warp_sum_b(ei);
+        eh = warp_sum_b(eh);
+        ev = warp_sum_b(ev);
+        const unsigned long long dmin = warp_min_u64(ord_bits(dts));
+        const unsigned long long lmin = warp_min_u64(ord_bits(len));
+        bad = static_cast<int32_t>(__reduce_or_sync(0xffffffffu, static_cast<unsigned>(bad)));
+        if (run_live && lane == 0) {
+            double* part = T.etile_part + 3 * (run_tile * NW + wid);
+            // one writer per slot and pass: the reductions (no return value)
+            // add in cycle order without a round trip
+            atomicAdd(part + 0, ei);
+            atomicAdd(part + 1, eh);
+            atomicAdd(part + 2, ev);
+            atomicMin(&run_ctl->dts_next, dmin);
+            atomicMin(&run_ctl->len_min, lmin);
+            if (bad) atomicOr(&run_ctl->status, bad);
+        }
+        ei = eh = ev = 0.0;
+        dts = len = DBL_MAX;
+        bad = 0;
+    };
     bool timed_out = false;
     int it = 0;
     int64_t t = blockIdx.x;
@@ -949,12 +978,15 @@ __global__ void __launch_bounds__(kStageTile, ENSC_BATCH_MINB_MIXED) k_element_b
         const InstanceDesc& d = *reinterpret_cast<const InstanceDesc*>(sb + kBatchDescOff);
         const StageHdr& h = *reinterpret_cast<const StageHdr*>(sb + kBatchHdrOff);
         const TileInfo& ti = *reinterpret_cast<const TileInfo*>(sb + kBatchInfoOff);
-        const bool live = h.live != 0;
-        Ctl* const ctl = d.ctl;
-        double ei = 0.0, eh = 0.0, ev = 0.0, dts = DBL_MAX, len = DBL_MAX;
-        int32_t bad = 0;
+        if (ti.slot != run_slot) {
+            flush();
+            run_slot = ti.slot;
+            run_tile = t;
+            run_ctl = d.ctl;
+            run_live = h.live != 0;
+        }
         const int64_t e = static_cast<int64_t>(ti.base) + tid;
-        if (live && e < d.E.ne) {
+        if (run_live && e < d.E.ne) {
 #if ENSC_BATCH_DESC_MODE == 1
             // the instance's arrays and constants, read from the stage once:
             // the body's stores could alias the stage as far as the compiler
@@ -963,6 +995,7 @@ __global__ void __launch_bounds__(kStageTile, ENSC_BATCH_MINB_MIXED) k_element_b
             const NodeArrays N = d.N;
             const Material M = d.M;
 #elif ENSC_BATCH_DESC_MODE == 2
+            // arrays copied to registers, material constants read at use
             const ElemArrays E = d.E;
             const NodeArrays N = d.N;
             const Material& M = d.M;
@@ -983,26 +1016,10 @@ __global__ void __launch_bounds__(kStageTile, ENSC_BATCH_MINB_MIXED) k_element_b
                              st + 45 * kStageTile,
                              kStageTile,
                              tid};
-            element_body_mixed<true, false, true>(E, N, M, S, dt1, dt1d, e, dts, len, ei, eh, ev, bad);
-        }
-        // each warp's sums go to its own slot (tile-major, warp-minor; folded
-        // in that order) and its minima to the instance's control block
-        ei = warp_sum_b(ei);
-        eh = warp_sum_b(eh);
-        ev = warp_sum_b(ev);
-        const unsigned long long dmin = warp_min_u64(ord_bits(dts));
-        const unsigned long long lmin = warp_min_u64(ord_bits(len));
-        bad = static_cast<int32_t>(__reduce_or_sync(0xffffffffu, static_cast<unsigned>(bad)));
-        if (live && lane == 0) {
-            double* part = T.etile_part + 3 * (t * NW + wid);
-            // one writer per slot and pass: the reductions (no return value)
-            // add in cycle order without a round trip
-            atomicAdd(part + 0, ei);
-            atomicAdd(part + 1, eh);
-            atomicAdd(part + 2, ev);
-            atomicMin(&ctl->dts_next, dmin);
-            atomicMin(&ctl->len_min, lmin);
-            if (bad) atomicOr(&ctl->status, bad);
+            double d1, l1;
+            element_body_mixed<true, false, true>(E, N, M, S, dt1, dt1d, e, d1, l1, ei, eh, ev, bad);
+            dts = fmin(dts, d1);
+            len = fmin(len, l1);
         }
         __syncthreads();  // the block is done with stage s
         const int64_t tn = t + 2 * gstride;
@@ -1011,7 +1028,9 @@ __global__ void __launch_bounds__(kStageTile, ENSC_BATCH_MINB_MIXED) k_element_b
             batch_stage_issue(T, src, tn + 2 * gstride, ntiles, sb, stage0 + s * kBatchStageBytes, bar, lane);
         }
     }
-    if (timed_out && tid == 0) {
+    if (!timed_out) {
+        flush();
+    } else if (tid == 0) {
         // record the failure on the instance whose tile could not be read and
         // let the copies this block started land (bounded) before exiting
         atomicOr(&T.desc[T.etile_inst[t]].ctl->status, ST_TIMEOUT);
