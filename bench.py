@@ -270,7 +270,7 @@ def time_block(args, p, precision, stream, local, barrier, max_over_ranks, sum_o
     rep = s.sync()
     assert rep["status"] == 0, rep
     ms_max = max_over_ranks(ms)
-    work = sum_over_ranks(float(ne) * C * args.steps)
+    value = replica_value(float(ne) * C * args.steps, ms, max_over_ranks, sum_over_ranks)
     # per-kernel CUDA-event durations on the launching stream (roofline)
     prof = s.profile(args.profile_cycles)
     el = prof["element"]
@@ -289,7 +289,7 @@ def time_block(args, p, precision, stream, local, barrier, max_over_ranks, sum_o
             traffic = json.load(f).get("bytes_per_launch")
     cb = cycle_bytes(ne, nn, plastic, mixed)
     return s, {
-        "value": work / (ms_max / 1000.0), "ms_max": ms_max, "launches": args.steps * (C * kpc + 1),
+        "value": value, "ms_max": ms_max, "launches": args.steps * (C * kpc + 1),
         "clocks": clocks, "cycles_run": (args.warmup + args.steps) * C + args.profile_cycles,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic,
@@ -334,10 +334,9 @@ def e2e_block(args, s, stream, max_over_ranks, sum_over_ranks, barrier):
         s._check(lib.ensc_download(s.h, None, ptr(outp["u"]), ptr(outp["v"]), ptr(outp["sigma"]), None, None))
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
-    e2e_work = sum_over_ranks(float(s.n_elements) * C * args.e2e_steps)
-    return {"value": e2e_work / (e2e_ms / 1000.0), "unit": METRIC, "h2d_bytes_per_step": h2d,
-            "d2h_bytes_per_step": d2h}
+    value = replica_value(float(s.n_elements) * C * args.e2e_steps, e0.elapsed_time(e1), max_over_ranks,
+                          sum_over_ranks)
+    return {"value": value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
 
 
 def sweep_leg(args, local):
@@ -450,6 +449,39 @@ def serve_leg(args, local):
     return summ
 
 
+def rank_ops(world: int, device):
+    """The collective steps of a replica run: a barrier, and the max and the
+    sum of one float over all ranks (identity at one rank).  Every rank calls
+    them in the same order."""
+    import torch
+    import torch.distributed as dist
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def reduce(x: float, op) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], device=device, dtype=torch.float64)
+        dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    def max_over_ranks(x: float) -> float:
+        return reduce(x, dist.ReduceOp.MAX)
+
+    def sum_over_ranks(x: float) -> float:
+        return reduce(x, dist.ReduceOp.SUM)
+
+    return barrier, max_over_ranks, sum_over_ranks
+
+
+def replica_value(work: float, ms: float, max_over_ranks, sum_over_ranks) -> float:
+    """Whole-job throughput of a replica run: all ranks' units over the
+    slowest rank's device time."""
+    return sum_over_ranks(work) / (max_over_ranks(ms) / 1000.0)
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -462,24 +494,7 @@ def run_ours(args):
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def sum_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+    barrier, max_over_ranks, sum_over_ranks = rank_ops(world, torch.device("cuda", local))
 
     p = build_problem(args.workload, args.block_dims)
     ne, nn = p.mesh.n_elements, p.mesh.n_nodes
