@@ -208,11 +208,9 @@ void launch_cycle(ensc_batch* b, int ge, int gn, cudaStream_t st) {
     ensc::launch_edge_prepass_batch(b->T, b->sms * b->occ_pre, st);
     if (is_mixed(b)) {
         ensc::launch_element_batch_mixed(b->T, ge, st);
-        ensc::launch_node_params_batch(b->T, b->slots, st);
         ensc::launch_node_batch_mixed(b->T, gn, st);
     } else {
         ensc::launch_element_batch_fp64(b->T, ge, st);
-        ensc::launch_node_params_batch(b->T, b->slots, st);
         ensc::launch_node_batch_fp64(b->T, gn, st);
     }
 }
@@ -393,6 +391,7 @@ int ensc_batch_create(const ensc_params* params, int32_t max_instances, int64_t 
     b->T.ntile = b->ntile;
     b->T.exact_count = b->d_counts + 3;
     b->T.prepass_done = b->d_counts + 4;
+    b->T.elem_done = b->d_counts + 5;
     b->T.nparam = b->d_nparam;
     b->T.sparam = b->d_sparam;
     b->T.etile_src = b->d_etile_src;

@@ -116,7 +116,6 @@ int build_graph(ensc_handle* h) {
     for (int c = 0; c < h->chunk; ++c) {
         ensc::launch_between(h->ctl, h->P, 0, h->cap_stream);
         ensc::launch_edge_prepass(h->E, h->N, h->ctl, h->grid_e, h->cap_stream);
-        ensc::launch_begin_exact(h->ctl, h->cap_stream);
         launch_element(h, false, h->cap_stream);
         launch_node(h, h->cap_stream);
     }
@@ -534,8 +533,7 @@ int ensc_profile(ensc_handle* h, int64_t max_cycles, double step_end_time, doubl
         cudaEventRecord(ev[1], h->stream);
         ensc::launch_edge_prepass(h->E, h->N, h->ctl, h->grid_e, h->stream);
         cudaEventRecord(ev[2], h->stream);
-        ensc::launch_begin_exact(h->ctl, h->stream);
-        cudaEventRecord(ev[3], h->stream);
+        cudaEventRecord(ev[3], h->stream);  // begin_exact runs inside the prepass
         launch_element(h, false, h->stream);
         cudaEventRecord(ev[4], h->stream);
         launch_node(h, h->stream);
@@ -563,7 +561,7 @@ int64_t ensc_device_bytes(const ensc_handle* h) {
     return static_cast<int64_t>(h->arena_bytes + (h->staging_owned ? h->staging_bytes : 0));
 }
 
-int32_t ensc_kernels_per_cycle(const ensc_handle* h) { return h ? 5 : 0; }
+int32_t ensc_kernels_per_cycle(const ensc_handle* h) { return h ? 4 : 0; }
 
 void ensc_destroy(ensc_handle* h) {
     if (!h) return;

@@ -77,14 +77,15 @@ __device__ __forceinline__ void cycle_begin(Ctl* ctl) {
     }
 }
 
-// Folds the energy partials of the previous cycle, then performs the first
-// half of update_minVertex_perMaterial_and_dt for the next cycle: rotate
-// dt_i_1 <- dt_i, advance time (computeSate :775-780) and fix dt_i_1 unless
-// the total-time clamp (:682-685) could fire, which needs this cycle's minimum
-// element edge first (edge_prepass + begin_exact).
-// mode 0: fold + begin, 1: fold only, 2: fold as the initial kinetic energy.
+// mode 0: the first half of update_minVertex_perMaterial_and_dt for the
+// next cycle: rotate dt_i_1 <- dt_i, advance time (computeSate :775-780) and
+// fix dt_i_1 unless the total-time clamp (:682-685) could fire, which needs
+// this cycle's minimum element edge first (the edge prepass).
+// mode 1: fold the energy partials into the control block and clear the work
+// partials, which accumulate over cycles between folds (the host folds
+// before it reads energies); 2: fold as the initial kinetic energy.
 __global__ void __launch_bounds__(kCtlThreads) k_between(Ctl* ctl, Partials P, int mode) {
-    if (ctl->energy_pending || mode == 2) {
+    if (mode != 0 && (ctl->energy_pending || mode == 2)) {
         const double ei = fixed_sum(P.elem + 0 * P.n_elem_blocks, P.n_elem_blocks);
         const double eh = fixed_sum(P.elem + 1 * P.n_elem_blocks, P.n_elem_blocks);
         const double ev = fixed_sum(P.elem + 2 * P.n_elem_blocks, P.n_elem_blocks);
@@ -103,6 +104,8 @@ __global__ void __launch_bounds__(kCtlThreads) k_between(Ctl* ctl, Partials P, i
             }
             ctl->energy_pending = 0;
         }
+        for (int i = threadIdx.x; i < 3 * P.n_elem_blocks; i += kCtlThreads) P.elem[i] = 0.0;
+        for (int i = threadIdx.x; i < P.n_node_blocks; i += kCtlThreads) P.node[P.n_node_blocks + i] = 0.0;
     }
     if (mode != 0 || threadIdx.x != 0 || ctl->done) return;
     if (ctl->status || !(ctl->time < ctl->step_end) || ctl->cycles_done >= ctl->cycles_target ||
@@ -113,9 +116,37 @@ __global__ void __launch_bounds__(kCtlThreads) k_between(Ctl* ctl, Partials P, i
     cycle_begin(ctl);
 }
 
+// Rest of update_minVertex_perMaterial_and_dt and run()'s clamp for a cycle
+// that needed the exact edge minimum (len_min_bits: that minimum, as
+// ordered bits).
+__device__ __forceinline__ void begin_exact(Ctl* ctl, unsigned long long len_min_bits) {
+    const double time = ctl->time;
+    double dt_i_1 = ctl->dt_prev;
+    const double time_prev = time + dt_i_1;
+    double d = bits_ord(len_min_bits) / ctl->wos;
+    d = d < ctl->dts_cur ? d : ctl->dts_cur;
+    double dt_i = d * ctl->factor;
+    if ((ctl->total_time - time_prev) < dt_i && (ctl->total_time - time_prev) > 0.0) {
+        dt_i = ctl->total_time - time_prev;
+        dt_i_1 = dt_i;
+    }
+    if (time + dt_i_1 > ctl->step_end) {
+        const double r = ctl->step_end - time;
+        dt_i = r;
+        dt_i_1 = r;
+    }
+    ctl->dt_i = dt_i;
+    ctl->dt_i_1 = dt_i_1;
+    ctl->dt_final = 1;
+    double t = time + dt_i_1;
+    if (t > ctl->total_time) t = ctl->total_time;
+    ctl->time = t;
+}
+
 // Minimum element edge over the current coordinates (min_ele_edge,
 // exDyna3D.cpp:1173-1220), needed before the element pass only in a cycle
-// where the total-time clamp may fire.
+// where the total-time clamp may fire; the last block then applies the clamp
+// (begin_exact).
 __global__ void __launch_bounds__(128) k_edge_prepass(ElemArrays E, NodeArrays N, Ctl* ctl) {
     if (ctl->done || !ctl->need_exact) return;
     __shared__ unsigned long long red[4];
@@ -156,40 +187,17 @@ __global__ void __launch_bounds__(128) k_edge_prepass(ElemArrays E, NodeArrays N
         unsigned long long r = red[0];
         for (int i = 1; i < 4; ++i) r = red[i] < r ? red[i] : r;
         atomicMin(&ctl->len_min, r);
+        // the last block to finish takes the edge minimum (through L2: this
+        // block may hold an older copy) and begins the cycle (begin_exact)
+        __threadfence();
+        if (atomicAdd(&ctl->prepass_done, 1) == static_cast<int>(gridDim.x) - 1) {
+            __threadfence();
+            begin_exact(ctl, atomicOr(&ctl->len_min, 0ull));
+            ctl->prepass_done = 0;
+        }
     }
 }
 
-// Rest of update_minVertex_perMaterial_and_dt and run()'s clamp for a cycle
-// that needed the exact edge minimum.
-// (len_min_bits: the edge minimum of the prepass, ordered bits)
-__device__ __forceinline__ void begin_exact(Ctl* ctl, unsigned long long len_min_bits) {
-    const double time = ctl->time;
-    double dt_i_1 = ctl->dt_prev;
-    const double time_prev = time + dt_i_1;
-    double d = bits_ord(len_min_bits) / ctl->wos;
-    d = d < ctl->dts_cur ? d : ctl->dts_cur;
-    double dt_i = d * ctl->factor;
-    if ((ctl->total_time - time_prev) < dt_i && (ctl->total_time - time_prev) > 0.0) {
-        dt_i = ctl->total_time - time_prev;
-        dt_i_1 = dt_i;
-    }
-    if (time + dt_i_1 > ctl->step_end) {
-        const double r = ctl->step_end - time;
-        dt_i = r;
-        dt_i_1 = r;
-    }
-    ctl->dt_i = dt_i;
-    ctl->dt_i_1 = dt_i_1;
-    ctl->dt_final = 1;
-    double t = time + dt_i_1;
-    if (t > ctl->total_time) t = ctl->total_time;
-    ctl->time = t;
-}
-
-__global__ void k_begin_exact(Ctl* ctl) {
-    if (threadIdx.x != 0 || ctl->done || !ctl->need_exact) return;
-    begin_exact(ctl, ctl->len_min);
-}
 
 __global__ void k_arm(Ctl* ctl, double step_end, long long max_cycles, double pause) {
     ctl->step_end = step_end;
@@ -327,39 +335,6 @@ __global__ void __launch_bounds__(kCtlThreads) k_fold_batch(BatchTables T) {
     }
 }
 
-// The node pass's scalars of every instance (one thread per slot): this
-// cycle's stable dt (update_minVertex_perMaterial_and_dt,
-// exDyna3D.cpp:673-679, as k_node computes it), the previous dt and the
-// gravity amplitude; also the control-block updates k_node makes.
-__global__ void k_node_params_batch(BatchTables T) {
-    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= T.counts[2]) return;
-    const InstanceDesc& d = T.desc[slot];
-    NodeParam p{0.0, 0.0, 1.0, 0, 0};
-    Ctl* ctl = d.ctl;
-    if (d.active && !ctl->done) {
-        double dt_i;
-        const int dt_final = ctl->dt_final;
-        if (dt_final) {
-            dt_i = ctl->dt_i;
-        } else {
-            double dd = bits_ord(ctl->len_min) / ctl->wos;
-            const double tmp = ctl->dts_cur;
-            dd = dd < tmp ? dd : tmp;
-            dt_i = dd * ctl->factor;
-        }
-        if (!(dt_i > 0.0) || !isfinite(dt_i)) atomicOr(&ctl->status, ST_BAD_DT);
-        if (!dt_final) ctl->dt_i = dt_i;
-        ctl->cycles_done += 1;
-        ctl->energy_pending = 1;
-        p.dt_i = dt_i;
-        p.dt_i_1 = ctl->dt_i_1;
-        p.amp = (d.M.gravity_on && d.M.amp_n > 0) ? gravity_amplitude(d.M.amp, d.M.amp_n, ctl->time, dt_i) : 1.0;
-        p.live = 1;
-    }
-    T.nparam[slot] = p;
-}
-
 // Minimum element edge for the instances whose cycle may hit the total-time
 // clamp (see k_edge_prepass), one warp per element tile of T.etile elements.
 __global__ void __launch_bounds__(128) k_edge_prepass_batch(BatchTables T) {
@@ -441,9 +416,6 @@ void launch_between_batch(const BatchTables& T, int slots, int mode, cudaStream_
     if (mode == 1) k_fold_batch<<<slots, kCtlThreads, 0, st>>>(T);
     k_begin_batch<<<(slots + 127) / 128, 128, 0, st>>>(T, mode == 0 ? 1 : 0);
 }
-void launch_node_params_batch(const BatchTables& T, int slots, cudaStream_t st) {
-    k_node_params_batch<<<(slots + 127) / 128, 128, 0, st>>>(T);
-}
 void launch_edge_prepass_batch(const BatchTables& T, int grid, cudaStream_t st) {
     k_edge_prepass_batch<<<grid, 128, 0, st>>>(T);
 }
@@ -453,7 +425,6 @@ void launch_between(Ctl* ctl, const Partials& P, int mode, cudaStream_t st) {
 void launch_edge_prepass(const ElemArrays& E, const NodeArrays& N, Ctl* ctl, int grid, cudaStream_t st) {
     k_edge_prepass<<<grid, 128, 0, st>>>(E, N, ctl);
 }
-void launch_begin_exact(Ctl* ctl, cudaStream_t st) { k_begin_exact<<<1, 32, 0, st>>>(ctl); }
 void launch_arm(Ctl* ctl, double step_end, long long max_cycles, cudaStream_t st, double pause) {
     k_arm<<<1, 1, 0, st>>>(ctl, step_end, max_cycles, pause);
 }

@@ -60,16 +60,17 @@ struct Ctl {
     int32_t dt_final;          // dt_i already fixed for this cycle
     int32_t energy_pending;    // partial energy sums of the last cycle not yet folded
     int32_t status;
-    int32_t pad;
+    int32_t prepass_done;      // blocks of the edge prepass that have finished
     double energy[6];          // kinetic, internal, hourglass, viscous, external, kinetic0
 };
 
-// FP32 constants of the mixed-precision element pass, derived once per
-// instance on the host (set_mixed_consts).  lambda and 2G are float pairs
-// (hi + lo); DRc and CRc are the per-element-invariant factors of the
-// hourglass stiffness and damping (Element_HexN8.cpp hourglass terms).
+// Constants of the mixed-precision element pass, derived once per instance
+// on the host (set_mixed_consts).  lambda and 2G are float pairs (hi + lo);
+// DRc and CRc are the per-element-invariant factors of the hourglass
+// stiffness and damping; the element dt uses 1/wos and cvisq^2/wos in FP64.
 struct MixedConsts {
     float G, lam_hi, lam_lo, g2_hi, g2_lo, rho, wos, cvisl, cvisq, y0, H, DRc, CRc, pad[3];
+    double inv_wos, cq2_wos;
 };
 
 struct Material {
@@ -103,6 +104,8 @@ inline void set_mixed_consts(Material& M) {
     c.H = static_cast<float>(M.hardening);
     c.DRc = static_cast<float>(M.c_dr * (4.0 / 3.0 * M.G + M.K) * 0.1 / std::sqrt(8.0));
     c.CRc = static_cast<float>(M.c_cr * M.rho * M.wos / 4.0);
+    c.inv_wos = 1.0 / M.wos;
+    c.cq2_wos = M.cvisq * M.cvisq / M.wos;
 }
 
 struct ElemArrays {
@@ -262,6 +265,7 @@ struct BatchTables {
     double* ntile_part;          // [ntiles][2] kinetic energy / external work per tile
     int32_t* exact_count;        // instances whose current cycle needs the edge prepass
     int32_t* prepass_done;       // blocks of the edge prepass that have finished
+    int32_t* elem_done;          // blocks of the element pass that have finished
     NodeParam* nparam;           // [slots] this cycle's node-pass scalars
     StageHdr* sparam;            // [slots] this cycle's element-pass scalars
     const NodeView* nview;       // [slots]
@@ -388,6 +392,53 @@ template <bool SMEM, typename T>
 __device__ __forceinline__ T ldin(const T* p) {
     if constexpr (SMEM) return *p;
     else return __ldg(p);
+}
+
+// The node pass's scalars of one batch slot: this cycle's stable dt
+// (update_minVertex_perMaterial_and_dt, exDyna3D.cpp:673-679, as the
+// single-instance node pass computes it), the previous dt and the gravity
+// amplitude; also the control-block updates that pass makes.  Run by the
+// last block of the batched element pass, after every block's minima: the
+// edge minimum is read through L2.
+__device__ inline void node_params_slot(const BatchTables& T, int slot) {
+    const InstanceDesc& d = T.desc[slot];
+    NodeParam p{0.0, 0.0, 1.0, 0, 0};
+    Ctl* ctl = d.ctl;
+    if (d.active && !ctl->done) {
+        double dt_i;
+        const int dt_final = ctl->dt_final;
+        if (dt_final) {
+            dt_i = ctl->dt_i;
+        } else {
+            double dd = __longlong_as_double(static_cast<long long>(__ldcg(&ctl->len_min))) / ctl->wos;
+            const double tmp = ctl->dts_cur;
+            dd = dd < tmp ? dd : tmp;
+            dt_i = dd * ctl->factor;
+        }
+        if (!(dt_i > 0.0) || !isfinite(dt_i)) atomicOr(&ctl->status, ST_BAD_DT);
+        if (!dt_final) ctl->dt_i = dt_i;
+        ctl->cycles_done += 1;
+        ctl->energy_pending = 1;
+        p.dt_i = dt_i;
+        p.dt_i_1 = ctl->dt_i_1;
+        p.amp = (d.M.gravity_on && d.M.amp_n > 0) ? gravity_amplitude(d.M.amp, d.M.amp_n, ctl->time, dt_i) : 1.0;
+        p.live = 1;
+    }
+    T.nparam[slot] = p;
+}
+
+// Called by every block of a batched element pass after its last tile: the
+// last block to finish fills the node pass's scalars of all slots.
+__device__ inline void element_pass_done(const BatchTables& T) {
+    __shared__ int last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(T.elem_done, 1) == static_cast<int>(gridDim.x) - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    for (int slot = threadIdx.x; slot < T.counts[2]; slot += blockDim.x) node_params_slot(T, slot);
+    if (threadIdx.x == 0) *T.elem_done = 0;
 }
 
 // Positive doubles order like their bit patterns; min-reductions over

@@ -75,7 +75,10 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 // Fixed-shape block reduction (warp butterflies, then warp 0 over the
 // warp results): deterministic for a given block size.
-template <int NT, int NV>
+// Block sum of NV values into out_slots[i * stride + slot]; values whose bit
+// is set in ACC are added to the slot (it accumulates over cycles, one writer
+// per slot and pass), the others stored.
+template <int NT, int NV, unsigned ACC = 0u>
 __device__ __forceinline__ void block_sum(double (&v)[NV], double* out_slots, int stride, int slot) {
     __shared__ double red[NV][NT / 32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -90,7 +93,11 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double* out_slots, in
         for (int i = 0; i < NV; ++i) {
             double s = lane < NT / 32 ? red[i][lane] : 0.0;
             s = warp_sum(s);
-            if (lane == 0) out_slots[i * stride + slot] = s;
+            if (lane == 0) {
+                double* o = out_slots + i * stride + slot;
+                if ((ACC >> i) & 1u) atomicAdd(o, s);
+                else *o = s;
+            }
         }
     }
     __syncthreads();
@@ -435,7 +442,7 @@ __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_FP64) k_element(E
     block_min2<kElemThreads>(dts_min, len_min, &ctl->dts_next, &ctl->len_min);
     if (!INIT) {
         double v3[3] = {e_int, e_hg, e_vis};
-        block_sum<kElemThreads, 3>(v3, P.elem, P.n_elem_blocks, blockIdx.x);
+        block_sum<kElemThreads, 3, 7u>(v3, P.elem, P.n_elem_blocks, blockIdx.x);
     }
 }
 
@@ -671,7 +678,7 @@ __global__ void __launch_bounds__(kStageTileF64, BT ? 2 : 3)
     if (bad) atomicOr(&ctl->status, bad);
     block_min2<kStageTileF64>(dts_min, len_min, &ctl->dts_next, &ctl->len_min);
     double v3[3] = {e_int, e_hg, e_vis};
-    block_sum<kStageTileF64, 3>(v3, P.elem, P.n_elem_blocks, blockIdx.x);
+    block_sum<kStageTileF64, 3, 7u>(v3, P.elem, P.n_elem_blocks, blockIdx.x);
 }
 
 // W consecutive nodes of the node pass with 16-byte row accesses: the same
@@ -797,7 +804,7 @@ __global__ void __launch_bounds__(kNodeThreads, ENSC_NODE_MINB_FP64) k_node(Elem
     }
     if (bad) atomicOr(&ctl->status, bad);
     double v2[2] = {kin, wext};
-    block_sum<kNodeThreads, 2>(v2, P.node, P.n_node_blocks, blockIdx.x);
+    block_sum<kNodeThreads, 2, 2u>(v2, P.node, P.n_node_blocks, blockIdx.x);
 }
 
 
@@ -994,6 +1001,7 @@ __global__ void __launch_bounds__(kStageTileF64, 2) k_element_batch_fp64(BatchTa
             if (blockIdx.x + itk * gstride < ntiles) mbar_wait_bounded(bar0 + 8 * (itk & 1), (itk >> 1) & 1);
         }
     }
+    element_pass_done(T);
 }
 
 // As k_node_batch_mixed: one warp per node tile, slots and first nodes read

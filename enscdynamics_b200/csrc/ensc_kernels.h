@@ -120,13 +120,11 @@ void launch_between_batch(const BatchTables& T, int slots, int mode, cudaStream_
 void launch_edge_prepass_batch(const BatchTables& T, int grid, cudaStream_t st);
 // per-instance node-pass scalars (and the control-block updates of the node
 // pass); runs between the element and node passes
-void launch_node_params_batch(const BatchTables& T, int slots, cudaStream_t st);
 
 // control (ensc_control.cu, built with -fmad=false)
 // mode 0: fold energy partials + begin next cycle; 1: fold only; 2: fold as initial KE
 void launch_between(Ctl* ctl, const Partials& P, int mode, cudaStream_t st);
 void launch_edge_prepass(const ElemArrays& E, const NodeArrays& N, Ctl* ctl, int grid, cudaStream_t st);
-void launch_begin_exact(Ctl* ctl, cudaStream_t st);
 // pause: the instance stops after the cycle in which its time reaches pause
 // (dt is not clamped to it)
 void launch_arm(Ctl* ctl, double step_end, long long max_cycles, cudaStream_t st, double pause = HUGE_VAL);

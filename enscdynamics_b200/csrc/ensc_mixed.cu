@@ -37,7 +37,10 @@ __device__ __forceinline__ double warp_sum_d(double v) {
     return v;
 }
 
-template <int NT, int NV>
+// Block sum of NV values into out_slots[i * stride + slot]; values whose bit
+// is set in ACC are added to the slot (it accumulates over cycles, one writer
+// per slot and pass), the others stored.
+template <int NT, int NV, unsigned ACC = 0u>
 __device__ __forceinline__ void block_sum_d(double (&v)[NV], double* out_slots, int stride, int slot) {
     __shared__ double red[NV][NT / 32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -52,7 +55,11 @@ __device__ __forceinline__ void block_sum_d(double (&v)[NV], double* out_slots, 
         for (int i = 0; i < NV; ++i) {
             double s = lane < NT / 32 ? red[i][lane] : 0.0;
             s = warp_sum_d(s);
-            if (lane == 0) out_slots[i * stride + slot] = s;
+            if (lane == 0) {
+                double* o = out_slots + i * stride + slot;
+                if ((ACC >> i) & 1u) atomicAdd(o, s);
+                else *o = s;
+            }
         }
     }
     __syncthreads();
@@ -457,11 +464,12 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
             else fe[(3 * j + i) * ep + e] = f[j];
         }
     }
-    // element dt (compute_dtStable, exDyna3D.cpp:828-834)
+    // element dt (compute_dtStable, exDyna3D.cpp:828-834), with the
+    // divisions by wos as products with its reciprocal
     {
         const double m0 = fmin(static_cast<double>(vr), 0.0);
-        const double xi = M.cvisl - M.cvisq * M.cvisq * len / M.wos * m0;
-        dts = (sqrt(1.0 + xi * xi) - xi) * len / M.wos;
+        const double xi = M.cvisl - M.mc.cq2_wos * len * m0;
+        dts = (sqrt(1.0 + xi * xi) - xi) * len * M.mc.inv_wos;
     }
     if (!isfinite(dts)) bad |= ST_NONFINITE;
 }
@@ -489,7 +497,7 @@ __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_MIXED)
     block_min2_d<kElemThreads>(dts_min, len_min, &ctl->dts_next, &ctl->len_min);
     if (!INIT) {
         double v3[3] = {e_int, e_hg, e_vis};
-        block_sum_d<kElemThreads, 3>(v3, P.elem, P.n_elem_blocks, blockIdx.x);
+        block_sum_d<kElemThreads, 3, 7u>(v3, P.elem, P.n_elem_blocks, blockIdx.x);
     }
 }
 
@@ -622,7 +630,7 @@ __global__ void __launch_bounds__(kStageTile, ENSC_STAGE_MINB_MIXED)
     if (bad) atomicOr(&ctl->status, bad);
     block_min2_d<kStageTile>(dts_min, len_min, &ctl->dts_next, &ctl->len_min);
     double v3[3] = {e_int, e_hg, e_vis};
-    block_sum_d<kStageTile, 3>(v3, P.elem, P.n_elem_blocks, blockIdx.x);
+    block_sum_d<kStageTile, 3, 7u>(v3, P.elem, P.n_elem_blocks, blockIdx.x);
 }
 
 // v + (dt_i + dt_i_1) / 2 * f * M^-1 in FP32 with the half step and the
@@ -831,7 +839,7 @@ __global__ void __launch_bounds__(kNodeThreads, ENSC_NODE_MINB_MIXED) k_node_mix
     }
     if (bad) atomicOr(&ctl->status, bad);
     double v2[2] = {kin, wext};
-    block_sum_d<kNodeThreads, 2>(v2, P.node, P.n_node_blocks, blockIdx.x);
+    block_sum_d<kNodeThreads, 2, 2u>(v2, P.node, P.n_node_blocks, blockIdx.x);
 }
 
 
@@ -1039,6 +1047,7 @@ __global__ void __launch_bounds__(kStageTile, ENSC_BATCH_MINB_MIXED) k_element_b
             if (blockIdx.x + itk * gstride < ntiles) mbar_wait_bounded(bar0 + 8 * (itk & 1), (itk >> 1) & 1);
         }
     }
+    element_pass_done(T);
 }
 
 // One warp per node tile.  The tile's instance slot and first node are read

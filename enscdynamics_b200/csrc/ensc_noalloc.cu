@@ -186,6 +186,9 @@ int ensc_step_noalloc(const ensc_device_model* m, const ensc_material* mat, cons
     if (e != cudaSuccess) return fail(ENSC_ERR_CUDA, std::string("control upload: ") + cudaGetErrorString(e));
 
     const int ge = P.n_elem_blocks, gn = P.n_node_blocks;
+    // the work partials accumulate over the call's cycles
+    e = cudaMemsetAsync(P.elem, 0, kPartialBytes, st);
+    if (e != cudaSuccess) return fail(ENSC_ERR_CUDA, std::string("partials reset: ") + cudaGetErrorString(e));
     // init()'s force pass sees the velocities before any boundary condition
     // (exDyna3D.cpp:124-141); the step's conditions are then applied to the
     // velocity field, as setCurrentStep / computeSate do (:1911, :782)
@@ -194,7 +197,6 @@ int ensc_step_noalloc(const ensc_device_model* m, const ensc_material* mat, cons
     for (int64_t i = 0; i < max_cycles; ++i) {
         ensc::launch_between(ctl, P, 0, st);
         ensc::launch_edge_prepass(E, N, ctl, ge, st);
-        ensc::launch_begin_exact(ctl, st);
         ensc::launch_element_fp64(E, N, M, ctl, P, ge, false, st);
         ensc::launch_node_fp64(E, N, M, ctl, P, gn, st);
     }
