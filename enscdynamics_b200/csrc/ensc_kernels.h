@@ -49,6 +49,13 @@ constexpr int kNodeUnrollMixed = ENSC_NODE_UNROLL_MIXED;
 #ifndef ENSC_MIXED_REREAD
 #define ENSC_MIXED_REREAD 1
 #endif
+// The single-instance staged mixed element pass prefetches an element's node
+// rows into L1 before its coordinate phase: bit 0 the velocities, bit 1 the
+// coordinate components 1 and 2 (the batched pass does not: the addresses
+// cost it registers and spills)
+#ifndef ENSC_MIXED_PREFETCH
+#define ENSC_MIXED_PREFETCH 3
+#endif
 // how the batched mixed element pass reads the staged instance descriptor:
 // 1 all fields copied to registers per tile, 2 arrays copied and material
 // constants read at use, 0 everything read at use

@@ -175,7 +175,9 @@ __device__ __forceinline__ void corner_values(T (&c)[8], T (&a)[8]) {
 // One element of the mixed element pass (see the kernel comment below);
 // shared by the single-instance, staged and batched kernels.  Inputs come
 // from S, outputs go to the instance's arrays at element e.
-template <bool PLASTIC, bool INIT, bool SMEM = false>
+// PF: node rows prefetched into L1 at the start (bit 0 velocities, bit 1
+// coordinate components 1 and 2).
+template <bool PLASTIC, bool INIT, bool SMEM = false, int PF = 0>
 __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const NodeArrays& N, const Material& M,
                                                    const MixedSrc& S, const float dt1, const double dt1d,
                                                    const int64_t e, double& dts, double& len, double& e_int,
@@ -208,6 +210,19 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
     uint32_t nk[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) nk[k] = ldin<SMEM>(S.conn + k * ss + si);
+    // start the node rows the body reads later on their way into L1
+    if (PF & 1) {
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int k = 0; k < 8; ++k) prefetch_l1(V + r * np + nk[k]);
+    }
+    if (PF & 2) {
+#pragma unroll
+        for (int r = 1; r < 3; ++r)
+#pragma unroll
+            for (int k = 0; k < 8; ++k) prefetch_l1(X + r * np + nk[k]);
+    }
     // coordinates relative to node 0, as FP64 differences, one component at a
     // time: hourglass projections TAU x = TAU (x - x0) (the Gamma rows sum to
     // zero) rounded to FP32; the minimum edge and F = sum_j (x_j - x_0) B0_j
@@ -607,7 +622,8 @@ __global__ void __launch_bounds__(kStageTile, ENSC_STAGE_MINB_MIXED)
                              kStageTile,
                              tid};
             double dts, len;
-            element_body_mixed<PLASTIC, false, true>(E, N, M, S, dt1, dt1d, e, dts, len, e_int, e_hg, e_vis, bad);
+            element_body_mixed<PLASTIC, false, true, ENSC_MIXED_PREFETCH>(E, N, M, S, dt1, dt1d, e, dts, len, e_int,
+                                                                          e_hg, e_vis, bad);
             dts_min = fmin(dts_min, dts);
             len_min = fmin(len_min, len);
         }
