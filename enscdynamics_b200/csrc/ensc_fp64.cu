@@ -551,7 +551,10 @@ __device__ __forceinline__ void node_body(const ElemArrays& E, const NodeArrays&
 // cbrt(V0^2), eps_p and, when BT, B0^T -- thread 0 copies into one of two
 // shared-memory stages with bulk copies one tile ahead of the compute.  The
 // arithmetic is element_body's, so results are bit-identical to k_element.
-constexpr int kStageTileF64 = 128;
+constexpr int kStageTileF64 = ENSC_STAGE_TILE_FP64;
+// resident blocks per SM of the staged FP64 passes (same threads per SM for
+// any tile size)
+constexpr int kStageMinbF64 = 256 / kStageTileF64;
 constexpr int kF64StageRows = 22;  // double rows before B0^T: 6 sigma, 12 QIA, V0, cbrt V0, cbrt V0^2, eps_p
 template <bool BT>
 constexpr uint32_t f64_stage_bytes() {
@@ -609,7 +612,7 @@ __device__ __forceinline__ void f64_stage_issue(const ElemArrays& E, uint32_t ds
 }
 
 template <bool PLASTIC, bool BT>
-__global__ void __launch_bounds__(kStageTileF64, BT ? 2 : 3)
+__global__ void __launch_bounds__(kStageTileF64, BT ? kStageMinbF64 : kStageMinbF64 * 3 / 2)
     k_element_staged(ElemArrays E, NodeArrays N, Material M, Ctl* ctl, Partials P) {
     if (ctl->done) return;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -892,7 +895,7 @@ __device__ __forceinline__ void f64_batch_stage_issue(const BatchTables& T, cons
 // states are bit-identical to the single-instance pass.  A block's
 // consecutive tiles of one instance form a run whose sums and minima are
 // reduced once, into the partial slot of the run's first tile.
-__global__ void __launch_bounds__(kStageTileF64, 2) k_element_batch_fp64(BatchTables T) {
+__global__ void __launch_bounds__(kStageTileF64, kStageMinbF64) k_element_batch_fp64(BatchTables T) {
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr int TT = kStageTileF64;
     constexpr int NW = TT / 32;

@@ -75,6 +75,10 @@ constexpr int kNodeUnrollMixed = ENSC_NODE_UNROLL_MIXED;
 #ifndef ENSC_STAGED_FP64
 #define ENSC_STAGED_FP64 2
 #endif
+// elements per stage (= threads per block) of the staged FP64 passes
+#ifndef ENSC_STAGE_TILE_FP64
+#define ENSC_STAGE_TILE_FP64 128
+#endif
 constexpr int kNodeThreads = 256;
 constexpr int kCtlThreads = 256;
 
