@@ -69,7 +69,7 @@ struct Ctl {
 // DRc and CRc are the per-element-invariant factors of the hourglass
 // stiffness and damping; the element dt uses 1/wos and cvisq^2/wos in FP64.
 struct MixedConsts {
-    float G, lam_hi, lam_lo, g2_hi, g2_lo, rho, wos, cvisl, cvisq, y0, H, DRc, CRc, pad[3];
+    float G, lam_hi, lam_lo, g2_hi, g2_lo, rho, wos, cvisl, cvisq, y0, H, DRc, CRc, inv_3gh, pad[2];
     double inv_wos, cq2_wos;
 };
 
@@ -104,6 +104,7 @@ inline void set_mixed_consts(Material& M) {
     c.H = static_cast<float>(M.hardening);
     c.DRc = static_cast<float>(M.c_dr * (4.0 / 3.0 * M.G + M.K) * 0.1 / std::sqrt(8.0));
     c.CRc = static_cast<float>(M.c_cr * M.rho * M.wos / 4.0);
+    c.inv_3gh = static_cast<float>(1.0 / (3.0 * M.G + M.hardening));
     c.inv_wos = 1.0 / M.wos;
     c.cq2_wos = M.cvisq * M.cvisq / M.wos;
 }

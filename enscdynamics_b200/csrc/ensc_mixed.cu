@@ -370,7 +370,7 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
         const float ep_old = S.eps[si];
         const float sy = y0 + H * ep_old;
         if (seq > sy) {
-            const float dl = (seq - sy) / (3.f * G + H);
+            const float dl = (seq - sy) * M.mc.inv_3gh;
             const float r = 1.f - 3.f * G * dl / seq;
             s[0] = d0 * r + pm;
             s[1] = d1 * r + pm;
@@ -394,7 +394,7 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
     }
     const float DR = DRc * nx2 * Vc * dt1;
     const float cbe = S.cb[si];
-    const float CR = CRc / J * (cbe * cbe);  // V0 / Vc = 1 / J
+    const float CR = CRc * invdet * (cbe * cbe);  // V0 / Vc = 1 / J
     float Gq[3][4];
 #pragma unroll
     for (int i = 0; i < 3; ++i)
@@ -408,7 +408,7 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
     float pv = 0.f;
     if (visc) {
         const float m0 = fminf(vr, 0.f);
-        pv = rho / J * cbe * (cvisq * cvisq * cbe * vr * m0 - cvisl * wos * vr);
+        pv = rho * invdet * cbe * (cvisq * cvisq * cbe * vr * m0 - cvisl * wos * vr);
         e_vis += -static_cast<double>(pv * Vc * vr) * dt1d;
     }
     // Z = Vc F^-1 (sigma - p I) - W^T, W = Gq TX
