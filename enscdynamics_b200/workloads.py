@@ -119,7 +119,10 @@ def impact_bar(n_core: int = 12, n_ring: int = 6, n_layers: int = 120, radius: f
     """Taylor-type impact bar: butterfly-meshed copper cylinder (r = 3.2 mm,
     L = 32.4 mm) with J2 (E 117 GPa, nu 0.35, rho 8930, yield 400 MPa,
     tangent 100 MPa), z = 0 face fixed in z only, all nodes at vz = -190 m/s,
-    run to 80 us."""
+    run to 80 us.  The deck writes the z constraint as ZSYMM: the reference
+    reader takes a dof-range line "Set-1, 3, 3" without a fourth field as
+    condition 3, which fixes nothing (dataIn.cpp:978-1003 with
+    exDyna3D.cpp:477-481)."""
     m = M.butterfly_cylinder(radius, length, n_core, n_ring, n_layers)
     bot = M.face_nodes(m, 2, "min")
     allnodes = np.arange(m.n_nodes)
@@ -130,7 +133,7 @@ def impact_bar(n_core: int = 12, n_ring: int = 6, n_layers: int = 120, radius: f
     mat = M.Material(117e9, 0.35, 8930.0, 400e6 if plastic else 0.0, 100e6 if plastic else 0.0)
     ctl = M.Controls(total_time=end_time, **DEFAULT_CONTROLS)
     return Problem("impact_bar", m, v0, code, val, mat, ctl, cycles=0, end_time=end_time,
-                   fixed_sets=[("Set-1", "3, 3")], initial_velocity=[("Set-2", 3, v_impact)])
+                   fixed_sets=[("Set-1", "ZSYMM")], initial_velocity=[("Set-2", 3, v_impact)])
 
 
 # dt factor of the sweep and serving problems (stable over nu in [0.25, 0.4])

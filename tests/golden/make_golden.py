@@ -70,6 +70,11 @@ def cases():
                             gravity_amplitude=[(0.0, 0.0), (3.0e-3, 1.0), (6.0e-3, 0.25), (1.0e-2, 0.8)],
                             **W.DEFAULT_CONTROLS)
     out.append(("gravity_amp_6x2x2", p, "cycles", 600))
+    # 7. the impact bar's butterfly-meshed cylinder (nodes share local slots
+    #    where the core meets the ring), elastic as the reference has no J2,
+    #    z = 0 face fixed in z, all nodes at -190 m/s
+    p = W.impact_bar(4, 2, 8, plastic=False)
+    out.append(("impact_bar_4x2x8", p, "cycles", 300))
     return out
 
 
