@@ -19,7 +19,9 @@
 // requires, exDyna3D.cpp:705):
 //   ensc_ref_harness <deck.inp> cycles <N> <dump.bin>
 //   ensc_ref_harness <deck.inp> full <dump.bin>
-//   ensc_ref_harness <deck.inp> setup <dump.bin>
+//   ensc_ref_harness <deck.inp> setup <dump.bin>  (state after init() and
+//       setCurrentStep(1); the u field carries the velocities init() left,
+//       before the first step's boundary conditions)
 //   ensc_ref_harness <deck.inp> time <N>          (timing JSON on stdout)
 // OMP_NUM_THREADS selects the OpenMP thread count as for the reference.
 #include "exDyna3D.h"
@@ -42,6 +44,7 @@ class RefHarness : public EnSC::exDyna3D {
 public:
     long cycles_done = 0;
     long cycle_cap = -1;  // < 0: unbounded
+    std::vector<double> v_read;  // setup dumps: written in place of u (keep_velocity)
 
     // Counts cycles; the body of a cycle is the reference's own computeSate().
     void computeSate() override {
@@ -78,6 +81,10 @@ public:
     }
 
     void full_run() { EnSC::exDyna3D::run(); }
+
+    // The velocities init() left (the deck's initial conditions, before the
+    // first step's boundary conditions), for the setup dump.
+    void keep_velocity() { v_read.assign(solution_v.data(), solution_v.data() + solution_v.size()); }
 
     std::size_t n_nodes() const { return vertices.size(); }
     std::size_t n_elements() const { return hexahedron_elements.size(); }
@@ -137,8 +144,8 @@ public:
         for (int64_t i = 0; i < nn; ++i)
             for (int c = 0; c < 3; ++c) buf[3 * i + c] = vertices[i][c];
         put(buf);                                                     // x
-        for (int64_t i = 0; i < 3 * nn; ++i) buf[i] = solution_u[i];
-        put(buf);                                                     // u
+        for (int64_t i = 0; i < 3 * nn; ++i) buf[i] = v_read.empty() ? solution_u[i] : v_read[i];
+        put(buf);                                                     // u (setup: v as read)
         for (int64_t i = 0; i < 3 * nn; ++i) buf[i] = solution_v[i];
         put(buf);                                                     // v
         for (int64_t i = 0; i < 3 * nn; ++i) buf[i] = inv_mass_matrix[i];
@@ -206,6 +213,7 @@ int main(int argc, char** argv) {
 
     if (mode == "setup") {
         h.prologue();
+        h.keep_velocity();
         h.setCurrentStep(1);
         h.dump(argv[3]);
         return 0;

@@ -34,6 +34,17 @@ def rel(a, b):
     return float(np.abs(a - b).max() / scale)
 
 
+def sampled(g, key, a):
+    """The part of a computed field that fixture g holds: all of it, or (for
+    a large reference deck) the rows at its sampled nodes / elements."""
+    a = np.asarray(a)
+    idx = "out_elements" if key in ("sigma", "qia") else "out_nodes"
+    if idx not in g:
+        return a.reshape(-1)
+    rows = len(g["conn"]) if idx == "out_elements" else len(g["x0"])
+    return a.reshape(rows, -1)[g[idx]].reshape(-1)
+
+
 def material_controls(meta):
     mat = M.Material(meta["E"], meta["nu"], meta["rho"], meta.get("yield", 0.0), meta.get("tangent", 0.0))
     g = meta.get("gravity")

@@ -9,9 +9,16 @@ Run in a container that has the reference checkout (REF, default
 
 Each fixture stores the model in array form (x0, conn, v0, BC arrays,
 material, controls) and the reference's state after the run (u, v, x, sigma,
-QIA, time, dt_i, dt_i_1, reactions).  Fixtures are small (<= a few hundred
+QIA, time, dt_i, dt_i_1, reactions).  Fixtures are small (<= a few thousand
 elements) so the CPU restatement and the GPU stepper can be checked against
 them anywhere, without the reference.
+
+Two kinds of case:
+  * decks written by enscdynamics_b200.mesh for the model in array form
+    (``cases``);
+  * the reference's own example decks (REF/inp, ``ref_deck_cases``): the
+    model is taken from the reference's state after init() and the first
+    step's setup, run for a bounded number of cycles inside that first step.
 """
 from __future__ import annotations
 
@@ -78,6 +85,80 @@ def cases():
     return out
 
 
+# the reference's example decks (REF/inp) and the cycles run in their first
+# step (each stays inside it)
+REF_DECKS = [("GenVirPa.inp", 200), ("Job-6.inp", 300), ("test_part1.inp", 300), ("test_single2.inp", 300),
+             ("test_step.inp", 300), ("test_trans.inp", 300), ("test.inp", 100)]
+
+
+# decks with more elements than this keep sampled results (SAMPLE_ROWS rows)
+SAMPLE_ABOVE = 2000
+SAMPLE_ROWS = 1000
+
+
+def ref_deck_cases(ref):
+    return [("refdeck_" + os.path.splitext(d)[0], os.path.join(ref, "inp", d), n) for d, n in REF_DECKS]
+
+
+def _first_step(deck_path):
+    """The first step's period and its gravity load (value, direction) or
+    None, read from the deck text as the reference reader reads them
+    (``*Dynamic, Explicit`` data line ``, period``; ``*Dload`` data line
+    ``, GRAV, g, dx, dy, dz``)."""
+    lines = open(deck_path).read().splitlines()
+    period, grav, in_step, k = None, None, False, 0
+    while k < len(lines):
+        u = lines[k].strip().upper()
+        if u.startswith("*STEP"):
+            if in_step:
+                break
+            in_step = True
+        elif in_step and u.startswith("*DYNAMIC"):
+            period = float(lines[k + 1].split(",")[1])
+        elif in_step and u.startswith("*DLOAD"):
+            f = [t.strip() for t in lines[k + 1].split(",")]
+            if len(f) >= 6 and f[1].upper() == "GRAV":
+                grav = (float(f[2]), [float(f[3]), float(f[4]), float(f[5])])
+        k += 1
+    return period, grav
+
+
+def make_ref_deck_fixture(name, deck_path, cycles):
+    """Runs one of the reference's example decks through the harness and
+    writes its fixture; returns the fixture's meta."""
+    import shutil
+    deck = os.path.basename(deck_path)
+    period, grav = _first_step(deck_path)
+    with tempfile.TemporaryDirectory() as d:
+        shutil.copy(deck_path, d)
+        M.write_project(d, deck, M.Controls(total_time=1.0, **W.DEFAULT_CONTROLS))
+        pyoracle.run_reference(d, deck, "setup", dump=os.path.join(d, "s.bin"))
+        s = pyoracle.read_dump(os.path.join(d, "s.bin"))
+        info = pyoracle.run_reference(d, deck, "cycles", cycles, dump=os.path.join(d, "o.bin"))
+        r = pyoracle.read_dump(os.path.join(d, "o.bin"))
+    assert r["cycles"] == cycles and r["time"] <= period, (name, r["cycles"], r["time"], period)
+    meta = dict(E=s["E"], nu=s["nu"], rho=s["rho"], c_dr=s["c_dr"], c_cr=s["c_cr"], factor=s["factor"],
+                cvisl=s["cvisl"], cvisq=s["cvisq"], total_time=s["total_time"], gravity=grav, mode="cycles",
+                cycles=int(r["cycles"]), amplitude=None, step_end=None, deck=deck)
+    arrays = dict(x0=s["x"], conn=s["conn"], v0=s["u"], bc_code=s["bc_code"], bc_value=s["bc_value"],
+                  clock=np.array([r["time"], r["dt_i"], r["dt_i_1"]]), meta=np.array(json.dumps(meta)))
+    ne, nn = s["n_elements"], s["n_nodes"]
+    if ne <= SAMPLE_ABOVE:
+        arrays.update(bt=s["bt"], vol0=s["vol0"], inv_mass=s["inv_mass"], u=r["u"], v=r["v"], x=r["x"],
+                      sigma=r["sigma"], qia=r["qia"], rf=r["rf"])
+    else:
+        # a large deck keeps the model whole but its results at seeded samples
+        # of nodes and elements (out_nodes / out_elements), to stay small
+        rng = np.random.default_rng(2026)
+        on = np.sort(rng.choice(nn, SAMPLE_ROWS, replace=False))
+        oe = np.sort(rng.choice(ne, SAMPLE_ROWS, replace=False))
+        arrays.update(out_nodes=on, out_elements=oe, u=r["u"][on], v=r["v"][on], x=r["x"][on],
+                      sigma=r["sigma"][oe])
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
+    print(name, info)
+    return meta
+
+
 def _rotations():
     """The 24 proper rotations of the reference hexahedron as node permutations."""
     xi = np.array([[-1, -1, -1], [1, -1, -1], [1, 1, -1], [-1, 1, -1],
@@ -142,6 +223,11 @@ def main(only=()):
     if only and os.path.exists(ipath):
         with open(ipath) as f:
             index = json.load(f)
+    ref = os.environ.get("REF", "/root/reference")
+    for name, deck_path, cycles in ref_deck_cases(ref):
+        if only and name not in only:
+            continue
+        index[name] = make_ref_deck_fixture(name, deck_path, cycles)
     for name, p, mode, cycles in cases():
         if only and name not in only:
             continue

@@ -93,7 +93,7 @@ def test_batch_matches_single_instances(precision):
     cases = [golden_case(n) for n in golden_names()]
     cases += [sweep_case(0, 170), sweep_case(1, 230, plastic=False), sweep_case(2, 95), sweep_case(5, 301)]
     refs = [single(c, precision) for c in cases]
-    with make_batch(precision) as b:
+    with make_batch(precision, max_instances=len(cases)) as b:
         slots = [add(b, c) for c in cases]
         for s, c in zip(slots, cases):
             b.arm(s, c.cycles, c.end)

@@ -8,7 +8,7 @@ reference's order depends on data alignment, so agreement is to round-off.
 import numpy as np
 import pytest
 
-from _common import golden_names, load_golden, oracle_for, rel, run_len
+from _common import golden_names, load_golden, oracle_for, rel, run_len, sampled
 
 ORACLE_TOL = 1e-10
 
@@ -17,10 +17,12 @@ ORACLE_TOL = 1e-10
 def test_oracle_matches_reference_golden(name):
     g = load_golden(name)
     o = oracle_for(g)
-    # element constants and lumped mass: same Eigen closed forms
-    assert rel(o.vol0, g["vol0"]) < 1e-15
-    assert rel(o.inv_mass, g["inv_mass"]) < 1e-15
-    assert rel(o.bt, g["bt"]) < 1e-14
+    # element constants and lumped mass: same Eigen closed forms, to a few
+    # ulps (fixtures of large reference decks do not keep them)
+    if "bt" in g:
+        assert rel(o.vol0, g["vol0"]) < 1e-14
+        assert rel(o.inv_mass, g["inv_mass"]) < 1e-14
+        assert rel(o.bt, g["bt"]) < 1e-14
     n, end = run_len(g)
     ran = o.run(n, end)
     assert ran == g["meta"]["cycles"]
@@ -28,7 +30,8 @@ def test_oracle_matches_reference_golden(name):
     assert abs(o.time - t) <= 1e-14 * abs(t)
     assert abs(o.dt[0] - dti) <= 1e-12 * abs(dti)
     for k, a in (("u", o.u), ("v", o.v), ("x", o.x), ("sigma", o.sigma)):
-        assert rel(a, g[k]) < ORACLE_TOL, (k, rel(a, g[k]))
+        err = rel(sampled(g, k, a), g[k])
+        assert err < ORACLE_TOL, (k, err)
 
 
 def test_oracle_clash_mesh_has_clashes():
