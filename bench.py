@@ -532,11 +532,14 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         res = cpu_reference_sample(args.cpu_cycles, threads)
+        one = cpu_reference_sample(max(2, args.cpu_cycles // 10), 1) if res is not None else None
         if res is not None:
             nx, ny, nz = CPU_SAMPLE_DIMS
             cpu = {"value": res["value"], "unit": METRIC, "cores": threads, "kind": "reference",
                    "sample": f"{nx}x{ny}x{nz} slab ({res['elements']} elements) of the block workload, elastic "
-                             f"(the reference has no J2), {args.cpu_cycles} cycles, cycle loop timed by the harness"}
+                             f"(the reference has no J2), {args.cpu_cycles} cycles, cycle loop timed by the harness",
+                   "value_1_thread": one["value"], "sample_1_thread": f"the same slab, {one['cycles']} cycles, "
+                                                                      f"OMP_NUM_THREADS=1"}
 
     if world > 1:
         dist.destroy_process_group()

@@ -109,7 +109,7 @@ def test_mixed_long_run_keeps_phase():
 
 
 def test_mixed_impact_bar_to_40us():
-    """The full plastic impact bar (51,840 elements, J2) run to 40 us, mixed
+    """The full plastic impact bar (195,840 elements, J2) run to 40 us, mixed
     against FP64 on the GPU (the FP64 stepper equals the oracle bit for bit,
     test_gpu_parity), with the same bars as above.  40 us, not the 80 us of
     the bar's deck: near 44 us the reference algorithm itself (the FP64
