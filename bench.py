@@ -31,8 +31,9 @@ Arms:
 One JSON line is printed by rank 0.  Multi-GPU (torchrun): every rank runs
 an independent replica of the block workload (the stepper has no
 cross-instance exchange), so scaling is weak and ``value`` sums all ranks'
-element-cycles over the slowest rank's device time; the sweep and serving
-legs run at one GPU only.
+element-cycles over the slowest rank's device time.  The sweep's instances
+are sharded across the ranks (every world-th instance per rank, no
+collective on the data path); the serving leg runs at one GPU only.
 """
 from __future__ import annotations
 
@@ -339,17 +340,28 @@ def e2e_block(args, s, stream, max_over_ranks, sum_over_ranks, barrier):
     return {"value": value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
 
 
-def sweep_leg(args, local):
+def shard(n: int, world: int, rank: int) -> list:
+    """The instances of an n-instance workload that rank `rank` of `world`
+    runs: every world-th one, so that ranks get similar mixes of sizes."""
+    return list(range(rank, n, world))
+
+
+def sweep_leg(args, local, world=1, rank=0, barrier=lambda: None, max_over_ranks=lambda x: x,
+              sum_over_ranks=lambda x: x):
     """Batched parameter sweep: args.sweep_instances uneven instances, each
     its own material, dt and clock, args.sweep_cycles cycles each, in one
     batch (mixed precision).  Timed with CUDA events from the first run to
     the last instance's completion; the plain FP64 stepper solves a bounded
-    sample of the same instances one after another for comparison."""
+    sample of the same instances one after another for comparison.  With
+    several ranks the instances are sharded across them (shard), each rank
+    runs its share in its own batch, and the rates are the totals over the
+    slowest rank's time."""
     import torch
     from enscdynamics_b200 import capi
     from enscdynamics_b200 import workloads as W
     n, cyc = args.sweep_instances, args.sweep_cycles
-    probs = [W.sweep_instance(i, cycles=cyc) for i in range(n)]
+    mine = shard(n, world, rank)
+    probs = [W.sweep_instance(i, cycles=cyc) for i in mine]
     ne_tot = sum(p.mesh.n_elements for p in probs)
     nn_tot = sum(p.mesh.n_nodes for p in probs)
     stream = torch.cuda.Stream()
@@ -365,6 +377,7 @@ def sweep_leg(args, local):
     admit_s = time.perf_counter() - t0
     dev_bytes = b.device_bytes
     torch.cuda.synchronize()
+    barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -376,8 +389,9 @@ def sweep_leg(args, local):
     assert running == 0
     bad = [i for i, sl in enumerate(slots) if b.report(sl)["status"] != 0 or b.report(sl)["cycles"] != cyc]
     b.close()
+    ms = max_over_ranks(ms)
     # plain FP64 stepper, one solve after another, on a bounded sample
-    k = min(n, args.sweep_fp64_sample)
+    k = min(len(probs), -(-args.sweep_fp64_sample // world))
     seq_ms = 0.0
     seq_work = 0
     for p in probs[:k]:
@@ -392,13 +406,15 @@ def sweep_leg(args, local):
             torch.cuda.synchronize()
             seq_ms += e0.elapsed_time(e1)
             seq_work += p.mesh.n_elements * cyc
+    ne_all = sum_over_ranks(float(ne_tot))
     batched = n / (ms / 1000.0)
-    seq = k / (seq_ms / 1000.0)
-    return {"instances": n, "cycles": cyc, "elements": ne_tot,
+    seq = sum_over_ranks(k / (seq_ms / 1000.0))
+    return {"instances": n, "cycles": cyc, "elements": int(ne_all), "ranks": world,
             "elements_range": [min(p.mesh.n_elements for p in probs), max(p.mesh.n_elements for p in probs)],
-            "precision": "mixed", "solves_per_s": batched, "element_cycles_per_s": ne_tot * cyc / (ms / 1000.0),
-            "ms": ms, "admit_s": admit_s, "device_bytes": dev_bytes, "failed": len(bad),
-            "sequential_fp64": {"sample": k, "solves_per_s": seq, "element_cycles_per_s": seq_work / (seq_ms / 1000.0)},
+            "precision": "mixed", "solves_per_s": batched, "element_cycles_per_s": ne_all * cyc / (ms / 1000.0),
+            "ms": ms, "admit_s": admit_s, "device_bytes": dev_bytes, "failed": int(sum_over_ranks(float(len(bad)))),
+            "sequential_fp64": {"sample": int(sum_over_ranks(float(k))), "solves_per_s": seq,
+                                "element_cycles_per_s": sum_over_ranks(seq_work / (seq_ms / 1000.0))},
             "speedup_vs_sequential_fp64": batched / seq}
 
 
@@ -523,8 +539,8 @@ def run_ours(args):
     s_head.close()
 
     sweep = serve = None
-    if world == 1 and args.sweep_instances > 0:
-        sweep = sweep_leg(args, local)
+    if args.sweep_instances > 0:
+        sweep = sweep_leg(args, local, world, rank, barrier, max_over_ranks, sum_over_ranks)
     if world == 1 and args.serve_requests > 0:
         serve = serve_leg(args, local)
 

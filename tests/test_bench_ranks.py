@@ -84,3 +84,13 @@ def test_reference_arm_runs_on_rank_zero_only():
                         "--steps", "1", "--warmup", "3"], env=env, capture_output=True, text=True, timeout=120)
     assert p.returncode == 0, p.stderr[-2000:]
     assert p.stdout.strip() == ""
+
+
+def test_sweep_shards_partition_the_instances():
+    sys.path.insert(0, ROOT)
+    import bench
+    for world in (1, 2, 3, 8):
+        parts = [bench.shard(256, world, r) for r in range(world)]
+        flat = sorted(i for p in parts for i in p)
+        assert flat == list(range(256))
+        assert max(len(p) for p in parts) - min(len(p) for p in parts) <= 1
