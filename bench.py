@@ -386,6 +386,7 @@ def sweep_leg(args, local, world=1, rank=0, barrier=lambda: None, max_over_ranks
     running = b.sync()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
+    tuning = b.tuning
     assert running == 0
     bad = [i for i, sl in enumerate(slots) if b.report(sl)["status"] != 0 or b.report(sl)["cycles"] != cyc]
     b.close()
@@ -413,6 +414,7 @@ def sweep_leg(args, local, world=1, rank=0, barrier=lambda: None, max_over_ranks
             "elements_range": [min(p.mesh.n_elements for p in probs), max(p.mesh.n_elements for p in probs)],
             "precision": "mixed", "solves_per_s": batched, "element_cycles_per_s": ne_all * cyc / (ms / 1000.0),
             "ms": ms, "admit_s": admit_s, "device_bytes": dev_bytes, "failed": int(sum_over_ranks(float(len(bad)))),
+            "tuning": tuning,
             "sequential_fp64": {"sample": int(sum_over_ranks(float(k))), "solves_per_s": seq,
                                 "element_cycles_per_s": sum_over_ranks(seq_work / (seq_ms / 1000.0))},
             "speedup_vs_sequential_fp64": batched / seq}

@@ -40,8 +40,11 @@ struct Slot {
     double* amp = nullptr;  // gravity amplitude table (from the pool)
 };
 
+// Launch choices of the batched cycle: grid multipliers (over one wave of
+// resident blocks) of the element and node passes, cycles per graph launch,
+// and threads per block of the node pass.
 struct Tune {
-    int mult_e = 1, mult_n = 1, chunk = 32;
+    int mult_e = 1, mult_n = 1, chunk = 32, node_threads = ensc::kNodeThreads;
 };
 
 }  // namespace
@@ -75,12 +78,12 @@ struct ensc_batch {
     ensc::BatchTables T{};
     bool dirty = true;
     int64_t n_etiles = 0, n_ntiles = 0;
-    int sms = 148, occ_e = 1, occ_n = 1, occ_pre = 4;
+    int sms = 148, occ_e = 1, occ_pre = 4;
     Tune tune;
     int fixed_chunk = 0;  // cycles per graph launch given by the caller (0: tuned)
     bool tuned = false;
     cudaGraphExec_t graph = nullptr;
-    int graph_chunk = 0, graph_ge = 0, graph_gn = 0;
+    int graph_chunk = 0, graph_ge = 0, graph_gn = 0, graph_nt = 0;
     std::string err;
 };
 
@@ -203,28 +206,35 @@ int rebuild_tables(ensc_batch* b) {
     return ENSC_OK;
 }
 
-void launch_cycle(ensc_batch* b, int ge, int gn, cudaStream_t st) {
+void launch_cycle(ensc_batch* b, int ge, int gn, int nt, cudaStream_t st) {
     ensc::launch_between_batch(b->T, b->slots, 0, st);
     ensc::launch_edge_prepass_batch(b->T, b->sms * b->occ_pre, st);
     if (is_mixed(b)) {
         ensc::launch_element_batch_mixed(b->T, ge, st);
-        ensc::launch_node_batch_mixed(b->T, gn, st);
+        ensc::launch_node_batch_mixed(b->T, gn, nt, st);
     } else {
         ensc::launch_element_batch_fp64(b->T, ge, st);
-        ensc::launch_node_batch_fp64(b->T, gn, st);
+        ensc::launch_node_batch_fp64(b->T, gn, nt, st);
     }
 }
 
+int occupancy_node(ensc_batch* b, int threads) {
+    return std::max(1, is_mixed(b) ? ensc::occupancy_node_batch_mixed(threads)
+                                    : ensc::occupancy_node_batch_fp64(threads));
+}
+
 int build_graph(ensc_batch* b, const Tune& t) {
-    const int ge = b->sms * b->occ_e * t.mult_e, gn = b->sms * b->occ_n * t.mult_n;
-    if (b->graph && b->graph_chunk == t.chunk && b->graph_ge == ge && b->graph_gn == gn) return ENSC_OK;
+    const int nt = t.node_threads;
+    const int ge = b->sms * b->occ_e * t.mult_e, gn = b->sms * occupancy_node(b, nt) * t.mult_n;
+    if (b->graph && b->graph_chunk == t.chunk && b->graph_ge == ge && b->graph_gn == gn && b->graph_nt == nt)
+        return ENSC_OK;
     if (b->graph) {
         cudaGraphExecDestroy(b->graph);
         b->graph = nullptr;
     }
     cudaGraph_t g = nullptr;
     BCK(b, cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal));
-    for (int c = 0; c < t.chunk; ++c) launch_cycle(b, ge, gn, b->cap_stream);
+    for (int c = 0; c < t.chunk; ++c) launch_cycle(b, ge, gn, nt, b->cap_stream);
     cudaError_t e = cudaStreamEndCapture(b->cap_stream, &g);
     if (e != cudaSuccess) return bcuda(b, "cudaStreamEndCapture", e);
     e = cudaGraphInstantiate(&b->graph, g, 0);
@@ -233,15 +243,18 @@ int build_graph(ensc_batch* b, const Tune& t) {
     b->graph_chunk = t.chunk;
     b->graph_ge = ge;
     b->graph_gn = gn;
+    b->graph_nt = nt;
     return ENSC_OK;
 }
 
-// Picks the launch geometry and graph length with the shortest time per
-// cycle on the batch as loaded.  The candidates differ only in how work is
+// Picks the launch geometry (grid sizes, node-pass block size) and graph
+// length with the shortest time per cycle on the batch as loaded.  The candidates differ only in how work is
 // spread over the GPU, not in arithmetic, so the cycles they run are ordinary
 // cycles of the solve (results are identical whichever wins).
 int autotune(ensc_batch* b, int64_t* cycles_left) {
-    const Tune cand[] = {{1, 1, 32}, {2, 1, 32}, {1, 2, 32}, {2, 2, 32}, {1, 1, 8}};
+    constexpr int kN = ensc::kNodeThreads;
+    const Tune cand[] = {{1, 1, 32, kN},     {2, 1, 32, kN}, {1, 2, 32, kN},     {2, 2, 32, kN},
+                         {1, 1, 32, kN / 2}, {1, 2, 32, kN / 2}, {1, 1, 8, kN}};
     cudaEvent_t e0, e1;
     BCK(b, cudaEventCreate(&e0));
     BCK(b, cudaEventCreate(&e1));
@@ -313,7 +326,6 @@ int ensc_batch_create(const ensc_params* params, int32_t max_instances, int64_t 
     if (cudaGetDeviceProperties(&prop, b->device) != cudaSuccess) return fail(berr(b, ENSC_ERR_CUDA, "device query"));
     b->sms = prop.multiProcessorCount;
     b->occ_e = std::max(1, is_mixed(b) ? ensc::occupancy_element_batch_mixed() : ensc::occupancy_element_batch_fp64());
-    b->occ_n = std::max(1, is_mixed(b) ? ensc::occupancy_node_batch_mixed() : ensc::occupancy_node_batch_fp64());
     // arena: a memory pool that keeps released blocks for reuse
     cudaMemPoolProps pp{};
     pp.allocType = cudaMemAllocationTypePinned;
@@ -648,6 +660,17 @@ int ensc_batch_remove(ensc_batch* b, int32_t slot) {
 }
 
 int64_t ensc_batch_device_bytes(const ensc_batch* b) { return b ? b->used : 0; }
+
+int ensc_batch_tuning(const ensc_batch* b, int32_t* mult_element, int32_t* mult_node, int32_t* graph_cycles,
+                      int32_t* node_threads) {
+    if (!b) return ENSC_ERR_ARG;
+    const bool t = b->tuned;
+    if (mult_element) *mult_element = t ? b->tune.mult_e : 0;
+    if (mult_node) *mult_node = t ? b->tune.mult_n : 0;
+    if (graph_cycles) *graph_cycles = t ? b->tune.chunk : 0;
+    if (node_threads) *node_threads = t ? b->tune.node_threads : 0;
+    return ENSC_OK;
+}
 
 int32_t ensc_batch_instances(const ensc_batch* b) {
     if (!b) return 0;

@@ -1009,7 +1009,8 @@ __global__ void __launch_bounds__(kStageTileF64, kStageMinbF64) k_element_batch_
 
 // As k_node_batch_mixed: one warp per node tile, slots and first nodes read
 // two tiles ahead, table lines prefetched into L1 one tile ahead.
-__global__ void __launch_bounds__(kNodeThreads, ENSC_NODE_MINB_FP64) k_node_batch_fp64(BatchTables T) {
+template <int NT>
+__global__ void __launch_bounds__(NT, ENSC_NODE_MINB_FP64 * kNodeThreads / NT) k_node_batch_fp64(BatchTables T) {
     constexpr int W = kNodeGroupFp64;
     const int lane = threadIdx.x & 31;
     const int warp = static_cast<int>((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
@@ -1121,8 +1122,9 @@ int occupancy_node_fp64() {
 void launch_element_batch_fp64(const BatchTables& T, int grid, cudaStream_t st) {
     k_element_batch_fp64<<<grid, kStageTileF64, kF64BatchStageSmem, st>>>(T);
 }
-void launch_node_batch_fp64(const BatchTables& T, int grid, cudaStream_t st) {
-    k_node_batch_fp64<<<grid, kNodeThreads, 0, st>>>(T);
+void launch_node_batch_fp64(const BatchTables& T, int grid, int threads, cudaStream_t st) {
+    if (threads == kNodeThreads / 2) k_node_batch_fp64<kNodeThreads / 2><<<grid, threads, 0, st>>>(T);
+    else k_node_batch_fp64<kNodeThreads><<<grid, kNodeThreads, 0, st>>>(T);
 }
 int occupancy_element_batch_fp64() {
     int nb = 0;
@@ -1135,9 +1137,12 @@ int occupancy_element_batch_fp64() {
 }
 
 int batch_element_tile_fp64() { return kStageTileF64; }
-int occupancy_node_batch_fp64() {
+int occupancy_node_batch_fp64(int threads) {
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_node_batch_fp64, kNodeThreads, 0);
+    if (threads == kNodeThreads / 2)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_node_batch_fp64<kNodeThreads / 2>, threads, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_node_batch_fp64<kNodeThreads>, kNodeThreads, 0);
     return nb;
 }
 

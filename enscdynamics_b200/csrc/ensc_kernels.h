@@ -115,13 +115,14 @@ int occupancy_node_mixed();
 
 // batched instances (one launch per phase for all instances of a batch)
 void launch_element_batch_fp64(const BatchTables& T, int grid, cudaStream_t st);
-void launch_node_batch_fp64(const BatchTables& T, int grid, cudaStream_t st);
+// threads per block of the batched node passes: kNodeThreads or half of it
+void launch_node_batch_fp64(const BatchTables& T, int grid, int threads, cudaStream_t st);
 int occupancy_element_batch_fp64();
-int occupancy_node_batch_fp64();
+int occupancy_node_batch_fp64(int threads);
 void launch_element_batch_mixed(const BatchTables& T, int grid, cudaStream_t st);
-void launch_node_batch_mixed(const BatchTables& T, int grid, cudaStream_t st);
+void launch_node_batch_mixed(const BatchTables& T, int grid, int threads, cudaStream_t st);
 int occupancy_element_batch_mixed();
-int occupancy_node_batch_mixed();
+int occupancy_node_batch_mixed(int threads);
 // elements and nodes per batch tile (element tiles are the staged passes'
 // tiles; node tiles are one warp of node groups)
 int batch_element_tile(bool mixed_precision);

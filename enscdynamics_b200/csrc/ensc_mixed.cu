@@ -1070,7 +1070,9 @@ __global__ void __launch_bounds__(kStageTile, ENSC_BATCH_MINB_MIXED) k_element_b
 // two tiles ahead and its NodeView and NodeParam lines prefetched into L1 one
 // tile ahead, so a tile starts on its node rows without waiting on the
 // tables.
-__global__ void __launch_bounds__(kNodeThreads, ENSC_NODE_BATCH_MINB_MIXED) k_node_batch_mixed(BatchTables T) {
+// NT threads per block (a tuning choice: the warps are independent).
+template <int NT>
+__global__ void __launch_bounds__(NT, ENSC_NODE_BATCH_MINB_MIXED * kNodeThreads / NT) k_node_batch_mixed(BatchTables T) {
     constexpr int W = kNodeGroupMixed;
     const int lane = threadIdx.x & 31;
     const int warp = static_cast<int>((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
@@ -1175,8 +1177,9 @@ int occupancy_node_mixed() {
 void launch_element_batch_mixed(const BatchTables& T, int grid, cudaStream_t st) {
     k_element_batch_mixed<<<grid, kStageTile, kBatchStageSmem, st>>>(T);
 }
-void launch_node_batch_mixed(const BatchTables& T, int grid, cudaStream_t st) {
-    k_node_batch_mixed<<<grid, kNodeThreads, 0, st>>>(T);
+void launch_node_batch_mixed(const BatchTables& T, int grid, int threads, cudaStream_t st) {
+    if (threads == kNodeThreads / 2) k_node_batch_mixed<kNodeThreads / 2><<<grid, threads, 0, st>>>(T);
+    else k_node_batch_mixed<kNodeThreads><<<grid, kNodeThreads, 0, st>>>(T);
 }
 int occupancy_element_batch_mixed() {
     int nb = 0;
@@ -1190,9 +1193,12 @@ int occupancy_element_batch_mixed() {
 
 int batch_element_tile(bool mixed_precision) { return mixed_precision ? kStageTile : batch_element_tile_fp64(); }
 int batch_node_tile(bool mixed_precision) { return 32 * (mixed_precision ? kNodeGroupMixed : kNodeGroupFp64); }
-int occupancy_node_batch_mixed() {
+int occupancy_node_batch_mixed(int threads) {
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_node_batch_mixed, kNodeThreads, 0);
+    if (threads == kNodeThreads / 2)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_node_batch_mixed<kNodeThreads / 2>, threads, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_node_batch_mixed<kNodeThreads>, kNodeThreads, 0);
     return nb;
 }
 

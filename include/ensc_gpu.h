@@ -267,6 +267,14 @@ int ensc_batch_remove(ensc_batch* b, int32_t slot);
 int64_t ensc_batch_device_bytes(const ensc_batch* b);
 int32_t ensc_batch_instances(const ensc_batch* b);
 
+/* The launch choices the batch's autotuner made on its first run (no
+ * reference counterpart: the reference has no batched stepper): grid
+ * multipliers over one wave of resident blocks of the element and node
+ * passes, cycles per graph launch, threads per block of the node pass.
+ * All zero before the first ensc_batch_run.  Any pointer may be NULL. */
+int ensc_batch_tuning(const ensc_batch* b, int32_t* mult_element, int32_t* mult_node, int32_t* graph_cycles,
+                      int32_t* node_threads);
+
 void ensc_batch_destroy(ensc_batch* b);
 
 /* Message of the last error on b (NULL: as ensc_last_error(NULL)). */

@@ -160,6 +160,27 @@ def test_graph_length_does_not_change_results():
                 assert np.array_equal(r0[k], r1[k]), k
 
 
+@pytest.mark.parametrize("precision", [capi.FP64, capi.MIXED])
+def test_autotuner_tries_every_candidate_without_changing_results(precision):
+    """A first run long enough for every launch candidate of the autotuner
+    (grid sizes, graph lengths, both node-pass block sizes) gives the
+    single-instance results, and the choice it reports is one of them."""
+    cases = [sweep_case(20, 900), sweep_case(21, 900, plastic=False)]
+    refs = [single(c, precision) for c in cases]
+    with make_batch(precision) as b:
+        assert b.tuning == dict(mult_element=0, mult_node=0, graph_cycles=0, node_threads=0)
+        ss = [add(b, c) for c in cases]
+        for s, c in zip(ss, cases):
+            b.arm(s, c.cycles)
+        b.run(900)
+        assert b.sync() == 0
+        t = b.tuning
+        assert t["mult_element"] in (1, 2) and t["mult_node"] in (1, 2)
+        assert t["graph_cycles"] in (8, 32) and t["node_threads"] in (128, 256)
+        for s, c, ref in zip(ss, cases, refs):
+            assert_same(b.download(s), b.report(s), b.energy(s), ref, c.name)
+
+
 def test_budget_and_capacity_are_enforced():
     c = sweep_case(16, 10)
     with make_batch(capi.MIXED, budget_bytes=1 << 16) as b:
