@@ -550,7 +550,7 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         res = cpu_reference_sample(args.cpu_cycles, threads)
-        one = cpu_reference_sample(max(2, args.cpu_cycles // 10), 1) if res is not None else None
+        one = cpu_reference_sample(max(3, args.cpu_cycles // 4), 1) if res is not None else None
         if res is not None:
             nx, ny, nz = CPU_SAMPLE_DIMS
             cpu = {"value": res["value"], "unit": METRIC, "cores": threads, "kind": "reference",
