@@ -3,30 +3,46 @@
 
 Workload (headline): the large elastic-plastic block -- 256x128x64 8-node
 hexahedra (2,097,152 elements, 2,154,945 nodes), J2 plasticity, seeded
-smoothed-Gaussian initial velocities, bottom face fixed.  One bench step is
-``--cycles-per-step`` cycles (default 500) of the stepper on the resident
-model; ten steps make the workload's 5000 cycles.  The per-cycle working set
-(1.3-2.3 GB) is far larger than the 126 MB L2, so no flush is needed between
-timed steps.  ``value`` is the headline precision (default mixed); the other
-precision is timed the same way beside it, and the mixed result's maximum
-displacement error against FP64 after the same cycles is reported.
+smoothed-Gaussian initial velocities, bottom face fixed, 5000 cycles.  One
+bench step is ``--cycles-per-step`` cycles (default 500) of the stepper on
+the resident model.  The per-cycle working set (1.3-2.3 GB) is far larger
+than the 126 MB L2, so no flush is needed between timed steps.  ``value`` is
+the headline precision (default mixed); the other precision is timed the
+same way beside it.
+
+Accuracy (``fp64_vs_mixed``): fresh FP64 and mixed steppers run exactly the
+workload's 5000 cycles (``--accuracy-cycles``) from the same initial state,
+whatever --steps and --warmup are; the mixed result's maximum relative
+displacement error and energy-balance drift against FP64 at that point are
+the headline accuracy figures.  The same two figures after all the cycles
+the timed runs made are reported beside them (``after_timed_cycles``).
+
+End to end (``e2e``, and ``e2e_fp64`` beside the mixed headline): through
+the C ABI with host buffers; every step uploads the state from pinned host
+memory, runs the step's cycles and reads u, v and sigma back, over --steps
+steps.
 
 Further legs of the same run (one GPU):
   batched_sweep  256 uneven cantilever/plate instances (2k-60k elements, own
-                 material, dt and clock), 3000 cycles each, in one batch;
-                 solves/s beside the plain FP64 stepper solving a sample of
-                 them one after another;
-  serving        a seeded Poisson stream (50/s) of 1k-500k-element solves
-                 served with continuous batching under a 150 GB budget;
-                 solves/s and p50/p99 latency beside the plain FP64 stepper
-                 serving the same stream one request at a time.
+                 material, dt and clock), 3000 cycles each, in one mixed
+                 batch and in one FP64 batch (every instance's mixed error
+                 and energy drift against its FP64 run; the maximum is
+                 reported); the plain FP64 stepper solves a sample of them
+                 one after another;
+  serving        a seeded Poisson stream (50/s, 500 requests) of
+                 1k-500k-element solves served with continuous batching
+                 under a 150 GB budget: solves/s and p50/p99 latency; the
+                 first 100 requests also through the plain FP64 stepper one
+                 at a time (latency, and each result's mixed error and
+                 energy drift against FP64).
 
 Arms:
   --impl ours (default)  the sm_100a stepper through the C ABI
                          (enscdynamics_b200/_lib/libensc_b200.so)
   --impl reference       the reference CPU stepper (compiled from its sources
                          into oracle/_ref) on a bounded slab of the same
-                         workload, with all host threads
+                         workload, at the fastest of 1, 2, 4, 8 and all host
+                         threads
 
 One JSON line is printed by rank 0.  Multi-GPU (torchrun): every rank runs
 an independent replica of the block workload (the stepper has no
@@ -67,13 +83,17 @@ def parse():
     ap.add_argument("--cycles-per-step", type=int, default=500)
     ap.add_argument("--block-dims", default="256,128,64", help="block workload cells nx,ny,nz")
     ap.add_argument("--profile-cycles", type=int, default=40)
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--accuracy-cycles", type=int, default=5000,
+                    help="cycles of the fresh FP64-vs-mixed comparison (the block workload's 5000; 0: skip)")
+    ap.add_argument("--e2e-steps", type=int, default=0, help="steps of the end-to-end legs (0: --steps)")
     ap.add_argument("--cpu-cycles", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sweep-instances", type=int, default=256, help="batched sweep leg (0: skip)")
     ap.add_argument("--sweep-cycles", type=int, default=3000)
     ap.add_argument("--sweep-fp64-sample", type=int, default=32)
-    ap.add_argument("--serve-requests", type=int, default=48, help="serving leg (0: skip)")
+    ap.add_argument("--serve-requests", type=int, default=500, help="serving leg (0: skip)")
+    ap.add_argument("--serve-seq-sample", type=int, default=100,
+                    help="requests of the serving stream also served by the plain FP64 stepper one at a time")
     return ap.parse_args()
 
 
@@ -181,52 +201,85 @@ def build_problem(name: str, dims: str = "256,128,64"):
 # --------------------------------------------------------------------------
 # CPU legs (reference stepper compiled from its sources; checker territory)
 
-def cpu_reference_sample(cycles: int, threads: int, repeats: int = 1):
-    """Times the reference CPU stepper on a slab of the block workload."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import pyoracle
-    from enscdynamics_b200 import workloads
-    if not pyoracle.harness_available():
-        return None
-    nx, ny, nz = CPU_SAMPLE_DIMS
-    p = workloads.block(nx, ny, nz, 1.0, 0.5, 0.25 * nz / 64, plastic=False)
-    out = []
-    with tempfile.TemporaryDirectory() as d:
-        deck = p.write_deck(d)
-        for _ in range(repeats):
-            r = pyoracle.run_reference(d, deck, "time", cycles, threads=threads)
-            out.append(r)
-    ne = p.mesh.n_elements
-    return {"elements": ne, "cycles": cycles, "runs": out,
-            "loop_s": [r["loop_s"] for r in out],
-            "value": ne * cycles * len(out) / sum(r["loop_s"] for r in out)}
+def thread_counts() -> list:
+    """Thread counts the CPU legs try: 1, 2, 4, 8 and all host threads."""
+    n = os.cpu_count() or 1
+    return sorted({t for t in (1, 2, 4, 8, n) if t <= n})
+
+
+class CpuReference:
+    """The reference CPU stepper (compiled from its own sources into
+    oracle/_ref) on a slab of the block workload: the deck is written once,
+    each run parses it, sets up and times its cycle loop.  More OpenMP
+    threads are not always faster for the reference (its parallel regions
+    and per-cycle zeroing cost more than they save at this size), so the
+    legs time every count of ``thread_counts`` briefly and use the fastest."""
+
+    def __init__(self):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle
+        from enscdynamics_b200 import workloads
+        self.pyoracle = pyoracle
+        self.ok = pyoracle.harness_available()
+        self.dir = tempfile.mkdtemp(prefix="ensc_ref_")
+        self.deck = None
+        if self.ok:
+            nx, ny, nz = CPU_SAMPLE_DIMS
+            self.p = workloads.block(nx, ny, nz, 1.0, 0.5, 0.25 * nz / 64, plastic=False)
+            self.deck = self.p.write_deck(self.dir)
+            self.elements = self.p.mesh.n_elements
+
+    def run(self, cycles: int, threads: int) -> dict:
+        r = self.pyoracle.run_reference(self.dir, self.deck, "time", cycles, threads=threads)
+        r["value"] = self.elements * cycles / r["loop_s"]
+        return r
+
+    def choose_threads(self, cycles: int = 3):
+        """(fastest thread count, {threads: element-cycles/s}) over a short run each."""
+        rates = {t: self.run(cycles, t)["value"] for t in thread_counts()}
+        return max(rates, key=rates.get), rates
+
+    def sample_text(self, cycles: int, threads: int) -> str:
+        nx, ny, nz = CPU_SAMPLE_DIMS
+        return (f"{nx}x{ny}x{nz} slab ({self.elements} elements) of the block workload, elastic (the reference "
+                f"has no J2), {cycles} cycles per run, cycle loop timed by the harness, OMP_NUM_THREADS={threads} "
+                f"(fastest of {thread_counts()})")
+
+    def close(self):
+        import shutil
+        shutil.rmtree(self.dir, ignore_errors=True)
 
 
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    threads = os.cpu_count() or 1
-    for _ in range(args.warmup):
-        cpu_reference_sample(max(2, args.cpu_cycles // 4), threads)
-    t0 = time.time()
-    res = cpu_reference_sample(args.cpu_cycles, threads, repeats=args.steps)
-    wall = time.time() - t0
-    if res is None:
+    ref = CpuReference()
+    if not ref.ok:
         print(json.dumps({"impl": "reference", "unavailable": "reference harness not built (oracle/_ref)"}))
         return 0
-    nx, ny, nz = CPU_SAMPLE_DIMS
-    sample = (f"{nx}x{ny}x{nz} slab ({res['elements']} elements) of the block workload, elastic (the reference "
-              f"has no J2), {args.cpu_cycles} cycles per step, cycle loop timed by the harness")
-    line = {"impl": "reference", "metric": METRIC, "value": res["value"], "unit": METRIC, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1000.0 * sum(res["loop_s"]) / len(res["loop_s"]),
+    t0 = time.time()
+    try:
+        # warm-up: every thread count once, keep the fastest
+        threads, rates = ref.choose_threads(max(2, args.cpu_cycles // 8))
+        for _ in range(max(0, args.warmup - 1)):
+            ref.run(max(2, args.cpu_cycles // 4), threads)
+        runs = [ref.run(args.cpu_cycles, threads) for _ in range(args.steps)]
+    finally:
+        ref.close()
+    wall = time.time() - t0
+    loop = [r["loop_s"] for r in runs]
+    value = ref.elements * args.cpu_cycles * len(runs) / sum(loop)
+    sample = ref.sample_text(args.cpu_cycles, threads)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sum(loop) / len(loop),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "block 256x128x64 hex8 J2 (reference sample: slab)", "elements": res["elements"],
-                       "cycles_per_step": args.cpu_cycles, "threads": threads},
-            "cpu_baseline": {"value": res["value"], "unit": METRIC, "cores": threads, "kind": "reference",
-                             "sample": sample},
-            "e2e": {"value": res["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "config": {"workload": "block 256x128x64 hex8 J2 (reference sample: elastic slab)",
+                       "elements": ref.elements, "cycles_per_step": args.cpu_cycles, "threads": threads},
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "reference",
+                             "sample": sample, "by_threads": rates},
+            "parse_s": statistics.median(r["parse_s"] for r in runs),
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "wall_s": wall}
     print(json.dumps(line))
     return 0
@@ -307,12 +360,14 @@ def time_block(args, p, precision, stream, local, barrier, max_over_ranks, sum_o
 
 def e2e_block(args, s, stream, max_over_ranks, sum_over_ranks, barrier):
     """End to end through the C ABI with host buffers: each step uploads the
-    step's input state from pinned host memory, runs C cycles, and reads back
-    u, v and sigma into pinned host memory."""
+    step's input state (x, u, v, sigma, QIA, eps_p and the clock) from pinned
+    host memory, runs C cycles, and reads back u, v and sigma into pinned
+    host memory; timed with CUDA events around all steps."""
     import ctypes as C_
     import numpy as np
     import torch
     C = args.cycles_per_step
+    steps = args.e2e_steps or args.steps
     ck = s.download()
     clk = s.step(0)
     pin = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for k, v in ck.items()}
@@ -327,7 +382,7 @@ def e2e_block(args, s, stream, max_over_ranks, sum_over_ranks, barrier):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(args.e2e_steps):
+    for _ in range(steps):
         s._check(lib.ensc_upload_state(s.h, ptr(pin["x"]), ptr(pin["u"]), ptr(pin["v"]), ptr(pin["sigma"]),
                                        ptr(pin["qia"]), ptr(pin["eps_p"]), clk["time"], clk["dt_i"], clk["dt_i_1"],
                                        clk["dt_stable_min"]))
@@ -335,9 +390,56 @@ def e2e_block(args, s, stream, max_over_ranks, sum_over_ranks, barrier):
         s._check(lib.ensc_download(s.h, None, ptr(outp["u"]), ptr(outp["v"]), ptr(outp["sigma"]), None, None))
     e1.record(stream)
     torch.cuda.synchronize()
-    value = replica_value(float(s.n_elements) * C * args.e2e_steps, e0.elapsed_time(e1), max_over_ranks,
-                          sum_over_ranks)
-    return {"value": value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+    ms = e0.elapsed_time(e1)
+    value = replica_value(float(s.n_elements) * C * steps, ms, max_over_ranks, sum_over_ranks)
+    return {"value": value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": steps,
+            "ms_per_step": max_over_ranks(ms) / steps}
+
+
+def energy_balance(e: dict) -> float:
+    """kinetic + internal + hourglass + viscous - external work."""
+    return e["kinetic"] + e["internal"] + e["hourglass"] + e["viscous"] - e["external"]
+
+
+def compare_to_fp64(u_mixed, u_fp64, e_mixed: dict, e_fp64: dict) -> dict:
+    """The accuracy bars of the mixed stepper against FP64 on the same solve:
+    max |u_mixed - u_fp64| / max |u_fp64|, and the energy-balance drift
+    |E_bal(mixed) - E_bal(FP64)| / KE0."""
+    import numpy as np
+    umax = float(np.abs(u_fp64).max())
+    err = float(np.abs(u_mixed - u_fp64).max() / umax) if umax > 0 else float(np.abs(u_mixed).max())
+    ke0 = e_fp64["kinetic0"]
+    drift = abs(energy_balance(e_mixed) - energy_balance(e_fp64)) / ke0 if ke0 > 0 else 0.0
+    return {"max_rel_disp_err": err, "energy_drift": drift}
+
+
+def accuracy_leg(args, p, local, stream) -> dict:
+    """Fresh FP64 and mixed steppers on the block workload, each run exactly
+    ``--accuracy-cycles`` cycles (the workload's 5000) from the same initial
+    state, independent of --steps / --warmup; the mixed result's
+    displacement error and energy drift against FP64 (compare_to_fp64), and
+    how far each run's energy balance moved from its initial kinetic energy
+    (|E_bal - KE0| / KE0)."""
+    import numpy as np
+    from enscdynamics_b200 import capi
+    cyc = args.accuracy_cycles
+    nn = p.mesh.n_nodes
+    out = {}
+    for prec in (capi.FP64, capi.MIXED):
+        with capi.Stepper(p.mesh.x0, p.mesh.conn, p.v0, material=p.material, controls=p.controls, device=local,
+                          stream=stream.cuda_stream, precision=prec) as s:
+            s.set_bcs(p.bc_code, p.bc_value)
+            rep = s.step(cyc)
+            assert rep["status"] == 0 and rep["cycles"] == cyc, rep
+            out[prec] = (s.download({"u": np.empty((nn, 3))})["u"], s.energy(), rep["time"])
+    (u64, e64, t64), (umx, emx, tmx) = out[capi.FP64], out[capi.MIXED]
+    r = compare_to_fp64(umx, u64, emx, e64)
+    r.update({"cycles": cyc, "time_fp64": t64, "time_mixed": tmx,
+              "energy_balance_fp64": abs(energy_balance(e64) - e64["kinetic0"]) / e64["kinetic0"],
+              "energy_balance_mixed": abs(energy_balance(emx) - emx["kinetic0"]) / emx["kinetic0"],
+              "bars": {"max_rel_disp_err": 1e-5, "energy_drift": 5e-3}})
+    r["pass"] = r["max_rel_disp_err"] <= 1e-5 and r["energy_drift"] <= 5e-3
+    return r
 
 
 def shard(n: int, world: int, rank: int) -> list:
@@ -350,12 +452,14 @@ def sweep_leg(args, local, world=1, rank=0, barrier=lambda: None, max_over_ranks
               sum_over_ranks=lambda x: x):
     """Batched parameter sweep: args.sweep_instances uneven instances, each
     its own material, dt and clock, args.sweep_cycles cycles each, in one
-    batch (mixed precision).  Timed with CUDA events from the first run to
-    the last instance's completion; the plain FP64 stepper solves a bounded
-    sample of the same instances one after another for comparison.  With
-    several ranks the instances are sharded across them (shard), each rank
-    runs its share in its own batch, and the rates are the totals over the
-    slowest rank's time."""
+    batch in mixed precision, timed with CUDA events from the first run to
+    the last instance's completion.  The same instances then run as one
+    FP64 batch (timed the same way), which gives every instance's mixed
+    displacement error and energy drift against FP64 (the maximum over
+    instances is reported); and the plain FP64 stepper solves a bounded
+    sample of them one after another.  With several ranks the instances are
+    sharded across them (shard), each rank runs its share in its own
+    batches, and the rates are totals over the slowest rank's time."""
     import torch
     from enscdynamics_b200 import capi
     from enscdynamics_b200 import workloads as W
@@ -365,32 +469,43 @@ def sweep_leg(args, local, world=1, rank=0, barrier=lambda: None, max_over_ranks
     ne_tot = sum(p.mesh.n_elements for p in probs)
     nn_tot = sum(p.mesh.n_nodes for p in probs)
     stream = torch.cuda.Stream()
-    t0 = time.perf_counter()
-    b = capi.Batch(max_instances=n, max_elements=ne_tot, max_nodes=nn_tot, budget_bytes=150 * 10 ** 9,
-                   precision=capi.MIXED, device=local, stream=stream.cuda_stream)
-    slots = []
-    for p in probs:
-        sl = b.add(p.mesh.x0, p.mesh.conn, p.v0, material=p.material, controls=p.controls)
-        b.set_bcs(sl, p.bc_code, p.bc_value)
-        b.arm(sl, cyc)
-        slots.append(sl)
-    admit_s = time.perf_counter() - t0
-    dev_bytes = b.device_bytes
-    torch.cuda.synchronize()
-    barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    b.run(cyc)
-    e1.record(stream)
-    running = b.sync()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    tuning = b.tuning
-    assert running == 0
-    bad = [i for i, sl in enumerate(slots) if b.report(sl)["status"] != 0 or b.report(sl)["cycles"] != cyc]
-    b.close()
-    ms = max_over_ranks(ms)
+
+    def run_batch(precision):
+        t0 = time.perf_counter()
+        b = capi.Batch(max_instances=len(probs), max_elements=ne_tot, max_nodes=nn_tot, budget_bytes=150 * 10 ** 9,
+                       precision=precision, device=local, stream=stream.cuda_stream)
+        slots = []
+        for p in probs:
+            sl = b.add(p.mesh.x0, p.mesh.conn, p.v0, material=p.material, controls=p.controls)
+            b.set_bcs(sl, p.bc_code, p.bc_value)
+            b.arm(sl, cyc)
+            slots.append(sl)
+        admit_s = time.perf_counter() - t0
+        dev_bytes = b.device_bytes
+        torch.cuda.synchronize()
+        barrier()
+        e0.record(stream)
+        b.run(cyc)
+        e1.record(stream)
+        running = b.sync()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        assert running == 0
+        reps = [b.report(sl) for sl in slots]
+        bad = [i for i, r in enumerate(reps) if r["status"] != 0 or r["cycles"] != cyc]
+        res = [(b.download(sl, ("u",))["u"], b.energy(sl)) for sl in slots]
+        tuning = b.tuning
+        b.close()
+        return {"ms": max_over_ranks(ms), "admit_s": admit_s, "device_bytes": dev_bytes, "bad": len(bad),
+                "tuning": tuning, "res": res}
+
+    mx = run_batch(capi.MIXED)
+    f64 = run_batch(capi.FP64)
+    acc = [compare_to_fp64(um, u64, em, e64) for (um, em), (u64, e64) in zip(mx["res"], f64["res"])]
+    worst_err = max_over_ranks(max(a["max_rel_disp_err"] for a in acc))
+    worst_drift = max_over_ranks(max(a["energy_drift"] for a in acc))
     # plain FP64 stepper, one solve after another, on a bounded sample
     k = min(len(probs), -(-args.sweep_fp64_sample // world))
     seq_ms = 0.0
@@ -408,13 +523,22 @@ def sweep_leg(args, local, world=1, rank=0, barrier=lambda: None, max_over_ranks
             seq_ms += e0.elapsed_time(e1)
             seq_work += p.mesh.n_elements * cyc
     ne_all = sum_over_ranks(float(ne_tot))
+    ms = mx["ms"]
     batched = n / (ms / 1000.0)
     seq = sum_over_ranks(k / (seq_ms / 1000.0))
+    rate_mx = ne_all * cyc / (ms / 1000.0)
+    rate_64 = ne_all * cyc / (f64["ms"] / 1000.0)
     return {"instances": n, "cycles": cyc, "elements": int(ne_all), "ranks": world,
             "elements_range": [min(p.mesh.n_elements for p in probs), max(p.mesh.n_elements for p in probs)],
-            "precision": "mixed", "solves_per_s": batched, "element_cycles_per_s": ne_all * cyc / (ms / 1000.0),
-            "ms": ms, "admit_s": admit_s, "device_bytes": dev_bytes, "failed": int(sum_over_ranks(float(len(bad)))),
-            "tuning": tuning,
+            "precision": "mixed", "solves_per_s": batched, "element_cycles_per_s": rate_mx,
+            "ms": ms, "admit_s": mx["admit_s"], "device_bytes": mx["device_bytes"],
+            "failed": int(sum_over_ranks(float(mx["bad"] + f64["bad"]))),
+            "tuning": mx["tuning"],
+            "accuracy_vs_fp64": {"max_rel_disp_err": worst_err, "energy_drift": worst_drift,
+                                 "instances": n, "of": "maximum over instances"},
+            "batched_fp64": {"element_cycles_per_s": rate_64, "solves_per_s": n / (f64["ms"] / 1000.0),
+                             "ms": f64["ms"], "tuning": f64["tuning"]},
+            "mixed_over_batched_fp64": rate_mx / rate_64,
             "sequential_fp64": {"sample": int(sum_over_ranks(float(k))), "solves_per_s": seq,
                                 "element_cycles_per_s": sum_over_ranks(seq_work / (seq_ms / 1000.0))},
             "speedup_vs_sequential_fp64": batched / seq}
@@ -423,9 +547,13 @@ def sweep_leg(args, local, world=1, rank=0, barrier=lambda: None, max_over_ranks
 def serve_leg(args, local):
     """Serving stream: args.serve_requests Poisson arrivals at 50/s, element
     counts log-uniform in 1k-500k, 1000-10000 cycles, elastic or J2, mixed
-    precision, admitted against a 150 GB device budget.  Beside it, the same
-    stream through the plain FP64 stepper one request at a time (each
-    request's solve time measured; its queueing follows from the arrivals)."""
+    precision, admitted against a 150 GB device budget.  Beside it, the first
+    args.serve_seq_sample requests of the same stream through the plain FP64
+    stepper one request at a time (each request's solve time measured; its
+    queueing follows from the arrivals, and the first k requests' latencies
+    in a one-at-a-time server depend only on those k).  The FP64 results of
+    that sample give each sampled request's mixed displacement error and
+    energy drift (maximum over the sample reported)."""
     import numpy as np
     import torch
     from enscdynamics_b200 import capi
@@ -438,13 +566,15 @@ def serve_leg(args, local):
     finally:
         be.close()
     summ = S.summarize(out)
+    k = min(len(reqs), args.serve_seq_sample)
     # sequential FP64: solve times per request, queue by arrival
     stream = torch.cuda.Stream()
     fin = 0.0
     lat = []
     work = 0
+    acc = []
     t_first = reqs[0].arrival
-    for r in reqs:
+    for r, o in zip(reqs[:k], out[:k]):
         p = r.problem
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -452,18 +582,28 @@ def serve_leg(args, local):
                           stream=stream.cuda_stream, precision=capi.FP64) as s:
             s.set_bcs(p.bc_code, p.bc_value)
             s.step(p.cycles)
-            s.download({"u": np.empty((p.mesh.n_nodes, 3))})
+            u64 = s.download({"u": np.empty((p.mesh.n_nodes, 3))})["u"]
+            e64 = s.energy()
         dt = time.perf_counter() - t0
         start = max(r.arrival, fin)
         fin = start + dt
         lat.append(fin - r.arrival)
         work += p.mesh.n_elements * p.cycles
+        if o.status == 0:
+            acc.append(compare_to_fp64(o.result["u"], u64, o.energy, e64))
     span = fin - t_first
-    seq = {"solves_per_s": len(reqs) / span, "p50_latency_s": float(np.percentile(lat, 50)),
+    seq = {"requests": k, "solves_per_s": k / span, "p50_latency_s": float(np.percentile(lat, 50)),
            "p99_latency_s": float(np.percentile(lat, 99)), "element_cycles_per_s": work / span}
+    first = S.summarize(out[:k])
+    first_rate = k / (max(o.finished for o in out[:k]) - t_first)
     summ.update({"rate_per_s": 50.0, "budget_bytes": 150 * 10 ** 9, "precision": "mixed",
+                 "first_k": {"requests": k, "p50_latency_s": first["p50_latency_s"],
+                             "p99_latency_s": first["p99_latency_s"], "solves_per_s": first_rate},
+                 "accuracy_vs_fp64": {"max_rel_disp_err": max(a["max_rel_disp_err"] for a in acc),
+                                      "energy_drift": max(a["energy_drift"] for a in acc),
+                                      "requests": len(acc), "of": f"maximum over the first {k} requests"},
                  "sequential_fp64": seq,
-                 "speedup_vs_sequential_fp64": summ["solves_per_s"] / seq["solves_per_s"]})
+                 "speedup_vs_sequential_fp64": first_rate / seq["solves_per_s"]})
     return summ
 
 
@@ -523,20 +663,31 @@ def run_ours(args):
     other = "fp64" if head == "mixed" else "mixed"
     s_head, m_head = time_block(args, p, head, stream, local, barrier, max_over_ranks, sum_over_ranks)
     cmp = None
+    e2e_other = None
     if not args.single_precision:
         s_other, m_other = time_block(args, p, other, stream, local, barrier, max_over_ranks, sum_over_ranks)
-        # the two steppers ran the same cycles from the same state: the
-        # mixed result's displacement error against FP64
-        u_h = s_head.download({"u": np.empty((nn, 3))})["u"]
-        u_o = s_other.download({"u": np.empty((nn, 3))})["u"]
+        # the two timed steppers ran the same cycles from the same state: the
+        # mixed result's accuracy after all the cycles the timing ran
+        st = {}
+        for name, s in ((head, s_head), (other, s_other)):
+            st[name] = (s.download({"u": np.empty((nn, 3))})["u"], s.energy())
+        after = compare_to_fp64(st["mixed"][0], st["fp64"][0], st["mixed"][1], st["fp64"][1])
+        after["cycles"] = m_head["cycles_run"]
+        e2e_other = e2e_block(args, s_other, stream, max_over_ranks, sum_over_ranks, barrier)
         s_other.close()
-        u64, umx = (u_o, u_h) if head == "mixed" else (u_h, u_o)
-        err = float(np.abs(umx - u64).max() / np.abs(u64).max())
         m64, mmx = (m_other, m_head) if head == "mixed" else (m_head, m_other)
         cmp = {"fp64_value": m64["value"], "mixed_value": mmx["value"],
                "mixed_over_fp64": mmx["value"] / m64["value"],
-               "mixed_max_rel_disp_err": err, "cycles_compared": m_head["cycles_run"],
-               "fp64_roofline_frac": m64["roofline"]["frac"], "mixed_roofline_frac": mmx["roofline"]["frac"]}
+               "fp64_roofline_frac": m64["roofline"]["frac"], "mixed_roofline_frac": mmx["roofline"]["frac"],
+               "fp64_node_roofline_frac": m64["node_roofline"]["frac"],
+               "after_timed_cycles": after}
+        if args.workload == "block" and args.accuracy_cycles > 0:
+            acc = accuracy_leg(args, p, local, stream)
+            cmp["at_workload_cycles"] = acc
+            # the headline accuracy figures: the workload's own cycle count
+            cmp["mixed_max_rel_disp_err"] = acc["max_rel_disp_err"]
+            cmp["mixed_energy_drift"] = acc["energy_drift"]
+            cmp["cycles_compared"] = acc["cycles"]
     e2e = e2e_block(args, s_head, stream, max_over_ranks, sum_over_ranks, barrier)
     s_head.close()
 
@@ -548,29 +699,35 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
-        res = cpu_reference_sample(args.cpu_cycles, threads)
-        one = cpu_reference_sample(max(3, args.cpu_cycles // 4), 1) if res is not None else None
-        if res is not None:
-            nx, ny, nz = CPU_SAMPLE_DIMS
-            cpu = {"value": res["value"], "unit": METRIC, "cores": threads, "kind": "reference",
-                   "sample": f"{nx}x{ny}x{nz} slab ({res['elements']} elements) of the block workload, elastic "
-                             f"(the reference has no J2), {args.cpu_cycles} cycles, cycle loop timed by the harness",
-                   "value_1_thread": one["value"], "sample_1_thread": f"the same slab, {one['cycles']} cycles, "
-                                                                      f"OMP_NUM_THREADS=1"}
+        ref = CpuReference()
+        if ref.ok:
+            try:
+                threads, rates = ref.choose_threads()
+                r = ref.run(args.cpu_cycles, threads)
+            finally:
+                ref.close()
+            cpu = {"value": r["value"], "unit": METRIC, "cores": threads, "kind": "reference",
+                   "sample": ref.sample_text(args.cpu_cycles, threads), "by_threads": rates,
+                   "parse_s": r["parse_s"]}
 
     if world > 1:
         dist.destroy_process_group()
     if rank != 0:
         return 0
     mixed = head == "mixed"
+    steps_text = (f"{C} cycles per step, {args.steps} timed steps after {args.warmup} warm-up steps "
+                  f"({(args.warmup + args.steps) * C} cycles per stepper); accuracy of mixed against FP64 at the "
+                  f"workload's {args.accuracy_cycles} cycles from a fresh start")
+    if args.workload == "block":
+        dims = "x".join(args.block_dims.split(","))
+        workload = f"block {dims} hex8 ({ne:,} el, {nn:,} nodes), J2; {steps_text}"
+    else:
+        workload = p.name
     line = {
         "metric": METRIC, "value": m_head["value"], "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": m_head["ms_max"] / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if mixed else "f64", "data": "synthetic",
-        "config": {"workload": ("block 256x128x64 hex8 (2,097,152 el, 2,154,945 nodes), J2, 5000 cycles = 10 steps"
-                                if args.block_dims == "256,128,64" else p.name) if args.workload == "block" else p.name,
-                   "elements": ne, "nodes": nn, "cycles_per_step": C, "precision": head,
+        "config": {"workload": workload, "elements": ne, "nodes": nn, "cycles_per_step": C, "precision": head,
                    "l2": f"inputs larger than L2 ({cycle_bytes(ne, nn, plastic, mixed) / 1e9:.2f} GB per cycle)",
                    "parallelism": f"replicas x{world}"},
         "roofline": m_head["roofline"],
@@ -582,6 +739,7 @@ def run_ours(args):
         "serving": serve,
         "cpu_baseline": cpu,
         "e2e": e2e,
+        "e2e_" + other: e2e_other,
         "gpu_launches": m_head["launches"],
         "clocks": m_head["clocks"],
     }

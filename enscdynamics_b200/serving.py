@@ -5,10 +5,10 @@ arrive over time.  The loop admits each arrived request into the running
 batch as soon as an instance slot and enough of the device-memory budget are
 free -- the batch itself refuses an instance that would exceed the budget --
 keeps its state resident on the device while it runs beside the others,
-retires it when its cycles are done (downloading what the caller asked for)
-and frees its memory for the next arrivals.  Admission is first come, first
-served, with backfill: a request that does not fit yet does not block later
-ones that do.
+retires it when its cycles are done (downloading what the caller asked for,
+and its energy sums) and frees its memory for the next arrivals.  Admission
+is first come, first served, with backfill: a request that does not fit yet
+does not block later ones that do.
 
 The GPU advances in quanta of graph-captured cycles; between quanta the host
 retires finished instances and admits new ones.  A quantum ends no later
@@ -43,6 +43,7 @@ class Outcome:
     status: int = 0
     elements: int = 0
     result: Optional[Dict[str, np.ndarray]] = None
+    energy: Optional[Dict[str, float]] = None
 
     @property
     def latency(self) -> float:
@@ -91,6 +92,9 @@ class BatchBackend:
 
     def download(self, slot: int) -> Dict[str, np.ndarray]:
         return self.batch.download(slot, self.fields) if self.fields else {}
+
+    def energy(self, slot: int) -> Dict[str, float]:
+        return self.batch.energy(slot)
 
     def remove(self, slot: int) -> None:
         self.batch.remove(slot)
@@ -158,6 +162,9 @@ class FakeBackend:
         return {"cycles": s["done"], "done": int(s["done"] >= s["target"]), "status": 0}
 
     def download(self, slot: int) -> Dict[str, np.ndarray]:
+        return {}
+
+    def energy(self, slot: int) -> Dict[str, float]:
         return {}
 
     def remove(self, slot: int) -> None:
@@ -232,6 +239,7 @@ class Server:
                     o.cycles = int(rep["cycles"])
                     o.status = int(rep["status"])
                     o.result = self.backend.download(slot)
+                    o.energy = self.backend.energy(slot)
                     self.backend.remove(slot)
                     o.finished = now()
                     del running[slot]
