@@ -2,8 +2,8 @@
 CPU stepper (compiled from the reference sources into oracle/_ref by
 oracle/Makefile) on decks written by enscdynamics_b200.mesh.
 
-Run in a container that has the reference checkout (REF, default
-/root/reference):
+Run in a container that has the reference checkout (REF, default: a
+checkout named ``reference`` beside this repository):
 
     make -C oracle && python tests/golden/make_golden.py
 
@@ -198,6 +198,62 @@ def clash_problem():
                      fixed_sets=[("Set-1", "PINNED")], initial_velocity=[("Set-2", 1, 1.5)])
 
 
+# slab of the roofline block workload run through the reference: the block's
+# element size (3.90625 mm cubes), material (elastic: the reference has no
+# J2), controls and seeded smoothed-Gaussian velocity field, at 64x32x16
+BLOCK_CASE = dict(name="block_64x32x16", dims=(64, 32, 16), lengths=(0.25, 0.125, 0.0625), seed=20241203,
+                  cycles=200)
+
+
+def _sha(a):
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def block_problem(dims, lengths, seed):
+    return W.block(*dims, *lengths, seed=seed, plastic=False)
+
+
+def make_block_fixture():
+    """The block workload's slab (BLOCK_CASE) through the reference stepper.
+    The fixture keeps the reference's results at seeded samples of nodes and
+    elements, and instead of the model arrays the parameters that rebuild
+    them (workloads.block) with a SHA-256 of each rebuilt array, which the
+    tests check before use."""
+    c = BLOCK_CASE
+    p = block_problem(c["dims"], c["lengths"], c["seed"])
+    with tempfile.TemporaryDirectory() as d:
+        deck = p.write_deck(d)
+        pyoracle.run_reference(d, deck, "setup", dump=os.path.join(d, "s.bin"))
+        s = pyoracle.read_dump(os.path.join(d, "s.bin"))
+        assert np.array_equal(s["conn"], p.mesh.conn)
+        assert np.array_equal(s["x"], p.mesh.x0)
+        assert np.array_equal(s["bc_code"], p.bc_code)
+        assert np.array_equal(s["bc_value"], p.bc_value)
+        assert np.array_equal(s["u"].reshape(-1, 3), p.v0)  # the setup dump's u holds the initial velocities
+        info = pyoracle.run_reference(d, deck, "cycles", c["cycles"], dump=os.path.join(d, "o.bin"))
+        r = pyoracle.read_dump(os.path.join(d, "o.bin"))
+    assert r["cycles"] == c["cycles"]
+    ctl = p.controls
+    meta = dict(E=p.material.E, nu=p.material.nu, rho=p.material.rho, c_dr=ctl.c_dr, c_cr=ctl.c_cr,
+                factor=ctl.factor, cvisl=ctl.cvisl, cvisq=ctl.cvisq, total_time=ctl.total_time, gravity=None,
+                mode="cycles", cycles=int(r["cycles"]), amplitude=None, step_end=None,
+                regenerate=dict(workload="block", dims=list(c["dims"]), lengths=list(c["lengths"]),
+                                seed=c["seed"],
+                                sha256={k: _sha(a) for k, a in (("x0", p.mesh.x0), ("conn", p.mesh.conn),
+                                                                 ("v0", p.v0), ("bc_code", p.bc_code),
+                                                                 ("bc_value", p.bc_value))}))
+    ne, nn = p.mesh.n_elements, p.mesh.n_nodes
+    rng = np.random.default_rng(2026)
+    on = np.sort(rng.choice(nn, SAMPLE_ROWS, replace=False))
+    oe = np.sort(rng.choice(ne, SAMPLE_ROWS, replace=False))
+    np.savez_compressed(os.path.join(HERE, c["name"] + ".npz"), out_nodes=on, out_elements=oe, u=r["u"][on],
+                        v=r["v"][on], x=r["x"][on], sigma=r["sigma"][oe],
+                        clock=np.array([r["time"], r["dt_i"], r["dt_i_1"]]), meta=np.array(json.dumps(meta)))
+    print(c["name"], info)
+    return meta
+
+
 def write_case_deck(p, d):
     deck = "model.inp"
     per = p.end_time if p.end_time else p.controls.total_time
@@ -223,11 +279,13 @@ def main(only=()):
     if only and os.path.exists(ipath):
         with open(ipath) as f:
             index = json.load(f)
-    ref = os.environ.get("REF", "/root/reference")
+    ref = os.environ.get("REF") or os.path.join(os.path.dirname(ROOT), "reference")
     for name, deck_path, cycles in ref_deck_cases(ref):
         if only and name not in only:
             continue
         index[name] = make_ref_deck_fixture(name, deck_path, cycles)
+    if not only or BLOCK_CASE["name"] in only:
+        index[BLOCK_CASE["name"]] = make_block_fixture()
     for name, p, mode, cycles in cases():
         if only and name not in only:
             continue

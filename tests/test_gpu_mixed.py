@@ -132,3 +132,24 @@ def test_mixed_impact_bar_to_40us():
     drift = abs(energy_balance(emx) - energy_balance(e64)) / e64["kinetic0"]
     assert err <= DISP_TOL, err
     assert drift <= ENERGY_TOL, drift
+
+
+def test_mixed_full_block_at_workload_cycles():
+    """The roofline workload itself -- the 256x128x64 block (2,097,152
+    elements, 2,154,945 nodes, J2) -- for its stated 5000 cycles, mixed
+    against the FP64 stepper from the same initial state, with both bars."""
+    p = W.block()
+    assert p.mesh.n_elements == 256 * 128 * 64 and p.cycles == 5000
+    out = {}
+    for prec in (capi.FP64, capi.MIXED):
+        with capi.Stepper(p.mesh.x0, p.mesh.conn, p.v0, material=p.material, controls=p.controls,
+                          precision=prec) as s:
+            s.set_bcs(p.bc_code, p.bc_value)
+            rep = s.step(p.cycles)
+            assert rep["status"] == 0 and rep["cycles"] == p.cycles
+            out[prec] = (s.download({"u": np.empty((p.mesh.n_nodes, 3))})["u"], s.energy())
+    (u64, e64), (umx, emx) = out[capi.FP64], out[capi.MIXED]
+    err = np.abs(umx - u64).max() / np.abs(u64).max()
+    drift = abs(energy_balance(emx) - energy_balance(e64)) / e64["kinetic0"]
+    assert err <= DISP_TOL, err
+    assert drift <= ENERGY_TOL, drift
