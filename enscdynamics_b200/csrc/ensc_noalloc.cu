@@ -1,13 +1,14 @@
 // ensc_step_noalloc: the FP64 stepper for callers that cannot allocate
 // device memory.
 //
-// Some hosts of this stepper run where cudaMalloc is not available to them:
-// code that executes inside a CUDA stream capture owned by someone else (an
-// allocation would invalidate the capture), plug-ins of an application that
-// owns and pre-plans all device memory through its own pool, or solver loops
-// with a fixed memory budget that must not grow after start-up.  They can
-// hand over device arrays they already own for the model and its state, but
-// they cannot provide the stepper's internal scratch.  This entry point keeps
+// Some hosts of this stepper may not call cudaMalloc: plug-ins of an
+// application that owns and pre-plans all device memory through its own
+// pool (the application accounts for every byte and an allocation behind
+// its back can fail its budget or fragment its pool), and solver loops with
+// a memory budget fixed at start-up (cudaMalloc can synchronise the device
+// and its failure mid-run cannot be handled there).  They can hand over
+// device arrays they already own for the model and its state, but they
+// cannot provide the stepper's internal scratch.  This entry point keeps
 // that scratch -- the per-element force hand-off between the element pass
 // and the node gather, the per-block energy partials and the control block --
 // in one file-scope __device__ array of fixed size, so a call performs no
@@ -24,14 +25,18 @@
 //     threads at the same time) race on it and corrupt each other;
 //   * the first call on a device looks up the array's device address with
 //     cudaGetSymbolAddress (once per device, with that device current); make
-//     that first call before any stream capture that should contain later
-//     calls.
+//     that first call before any stream capture;
+//   * the call launches its cycles in batches of kBatchCycles and reads the
+//     control block back after each batch (it waits for the stream), so it
+//     returns as soon as the step end or a status stops the run, whatever
+//     max_cycles is.
 #include "ensc_gpu.h"
 #include "ensc_device.cuh"
 #include "ensc_kernels.h"
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -40,6 +45,8 @@
 namespace {
 
 constexpr int kMaxDevices = 64;
+// cycles launched between two read-backs of the control block
+constexpr int64_t kBatchCycles = 32;
 constexpr int kMaxElemBlocks = (ENSC_NOALLOC_MAX_ELEMENTS + ensc::kElemThreads - 1) / ensc::kElemThreads;
 constexpr int kMaxNodeBlocks = (ENSC_NOALLOC_MAX_NODES + ensc::kNodeThreads - 1) / ensc::kNodeThreads;
 constexpr size_t kCtlBytes = (sizeof(ensc::Ctl) + 255) / 256 * 256;
@@ -92,6 +99,9 @@ int ensc_step_noalloc(const ensc_device_model* m, const ensc_material* mat, cons
         return fail(ENSC_ERR_ARG, "a device array of the model is NULL");
     if (params->device < 0 || params->device >= kMaxDevices) return fail(ENSC_ERR_ARG, "bad device ordinal");
     if (!(mat->rho > 0.0) || !(mat->E > 0.0) || !(mat->nu < 0.5)) return fail(ENSC_ERR_ARG, "invalid material");
+    if (m->gravity_amp_n < 0 || m->gravity_amp_n > ENSC_MAX_AMPLITUDE_POINTS ||
+        (m->gravity_amp_n > 0 && !m->gravity_amp))
+        return fail(ENSC_ERR_ARG, "bad gravity amplitude table");
 
     int prev = -1;
     cudaGetDevice(&prev);
@@ -162,6 +172,10 @@ int ensc_step_noalloc(const ensc_device_model* m, const ensc_material* mat, cons
     M.gravity_on = params->gravity_on;
     M.gravity_value = params->gravity_value;
     for (int i = 0; i < 3; ++i) M.gravity_dir[i] = params->gravity_dir[i];
+    // the amplitude table stays in the caller's device memory; the node pass
+    // reads it there
+    M.amp = m->gravity_amp_n > 0 ? m->gravity_amp : nullptr;
+    M.amp_n = m->gravity_amp_n;
     ensc::set_mixed_consts(M);
 
     // the shared scratch keeps the previous call's contents: every control
@@ -194,11 +208,24 @@ int ensc_step_noalloc(const ensc_device_model* m, const ensc_material* mat, cons
     // velocity field, as setCurrentStep / computeSate do (:1911, :782)
     if (clk->init_pass) ensc::launch_element_fp64(E, N, M, ctl, P, ge, true, st);
     ensc::launch_apply_bc_v(N, false, st);
-    for (int64_t i = 0; i < max_cycles; ++i) {
-        ensc::launch_between(ctl, P, 0, st);
-        ensc::launch_edge_prepass(E, N, ctl, ge, st);
-        ensc::launch_element_fp64(E, N, M, ctl, P, ge, false, st);
-        ensc::launch_node_fp64(E, N, M, ctl, P, gn, st);
+    // cycles in batches; after each, the control block tells whether the run
+    // stopped (step end reached, cycle budget spent, or a status raised)
+    int64_t launched = 0;
+    while (launched < max_cycles) {
+        const int64_t n = std::min<int64_t>(kBatchCycles, max_cycles - launched);
+        for (int64_t i = 0; i < n; ++i) {
+            ensc::launch_between(ctl, P, 0, st);
+            ensc::launch_edge_prepass(E, N, ctl, ge, st);
+            ensc::launch_element_fp64(E, N, M, ctl, P, ge, false, st);
+            ensc::launch_node_fp64(E, N, M, ctl, P, gn, st);
+        }
+        launched += n;
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return fail(ENSC_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+        e = cudaMemcpyAsync(&c, ctl, sizeof(c), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return fail(ENSC_ERR_CUDA, std::string("control read-back: ") + cudaGetErrorString(e));
+        if (c.status || !(c.time < c.step_end) || c.cycles_done >= max_cycles) break;
     }
     ensc::launch_between(ctl, P, 1, st);
     e = cudaGetLastError();
