@@ -55,13 +55,21 @@ class EnergyReport(C.Structure):
                 ("viscous", C.c_double), ("external", C.c_double), ("kinetic0", C.c_double)]
 
 
+class Snapshot(C.Structure):
+    """ensc_snapshot: host pointers into the library's pinned snapshot buffer."""
+    _fields_ = [("x", _P), ("u", _P), ("v", _P), ("a", _P), ("rf", _P), ("sigma", _P),
+                ("time", C.c_double), ("dt_i", C.c_double), ("dt_i_1", C.c_double),
+                ("total_cycles", C.c_int64), ("status", C.c_int32)]
+
+
 class DeviceModel(C.Structure):
     """ensc_device_model: caller-owned device arrays for ensc_step_noalloc."""
     _fields_ = [("n_nodes", C.c_int64), ("n_elements", C.c_int64), ("conn", C.c_void_p), ("bt", C.c_void_p),
                 ("vol0", C.c_void_p), ("cbrt_v0", C.c_void_p), ("cbrt_v0sq", C.c_void_p),
                 ("inv_mass", C.c_void_p), ("bc", C.c_void_p), ("bc_value", C.c_void_p), ("node_elem", C.c_void_p),
                 ("x", C.c_void_p), ("u", C.c_void_p), ("v", C.c_void_p), ("sigma", C.c_void_p),
-                ("qia", C.c_void_p), ("eps_p", C.c_void_p), ("rf", C.c_void_p)]
+                ("qia", C.c_void_p), ("eps_p", C.c_void_p), ("rf", C.c_void_p),
+                ("gravity_amp", C.c_void_p), ("gravity_amp_n", C.c_int32)]
 
 
 class NoallocClock(C.Structure):
@@ -71,6 +79,26 @@ class NoallocClock(C.Structure):
 
 NOALLOC_MAX_ELEMENTS = 32768
 NOALLOC_MAX_NODES = 262144
+
+
+def noalloc_node_elem(conn: np.ndarray, n_nodes: int) -> np.ndarray:
+    """The ``node_elem`` table of ensc_device_model ([8][n_nodes] uint32:
+    the element holding node n in local slot k, or 0xFFFFFFFF) from the
+    (n_elements, 8) connectivity.  ensc_step_noalloc keeps one element per
+    slot, so a mesh where a node sits in the same local slot of two elements
+    cannot run there: raises ValueError naming the first such node."""
+    conn = np.asarray(conn, dtype=np.int64)
+    ne = conn.shape[0]
+    out = np.full((8, n_nodes), 0xFFFFFFFF, dtype=np.uint32)
+    for k in range(8):
+        col = conn[:, k]
+        counts = np.bincount(col, minlength=n_nodes)
+        if counts.max(initial=0) > 1:
+            node = int(np.argmax(counts > 1))
+            raise ValueError(f"node {node} sits in local slot {k} of {int(counts[node])} elements: "
+                             "ensc_step_noalloc needs one element per node and slot")
+        out[k, col] = np.arange(ne, dtype=np.uint32)
+    return out
 
 
 # every symbol include/ensc_gpu.h declares: (name, restype, argtypes)
@@ -85,6 +113,9 @@ SIGNATURES = [
     ("ensc_step_until", C.c_int, [C.c_void_p, C.c_int64, C.c_double, C.c_double, C.POINTER(StepReport)]),
     ("ensc_step_async", C.c_int, [C.c_void_p, C.c_int64, C.c_double]),
     ("ensc_sync", C.c_int, [C.c_void_p, C.POINTER(StepReport)]),
+    ("ensc_step_until_async", C.c_int, [C.c_void_p, C.c_int64, C.c_double, C.c_double]),
+    ("ensc_snapshot_begin", C.c_int, [C.c_void_p]),
+    ("ensc_snapshot_wait", C.c_int, [C.c_void_p, C.POINTER(Snapshot)]),
     ("ensc_download", C.c_int, [C.c_void_p, _P, _P, _P, _P, _P, _P]),
     ("ensc_upload_state", C.c_int, [C.c_void_p, _P, _P, _P, _P, _P, _P, C.c_double, C.c_double, C.c_double,
                                     C.c_double]),
@@ -248,6 +279,27 @@ class Stepper:
 
     def step_async(self, max_cycles: int, step_end: float = math.inf) -> None:
         self._check(self._lib.ensc_step_async(self.h, int(max_cycles), float(step_end)))
+
+    def step_until_async(self, max_cycles: int, step_end: float, pause: float) -> None:
+        self._check(self._lib.ensc_step_until_async(self.h, int(max_cycles), float(step_end), float(pause)))
+
+    def snapshot_begin(self) -> None:
+        """Captures the output fields now (in stream order) and starts their
+        copy to host memory without waiting."""
+        self._check(self._lib.ensc_snapshot_begin(self.h))
+
+    def snapshot_wait(self) -> Dict[str, np.ndarray]:
+        """Waits for the last snapshot and returns copies of its fields
+        (x, u, v, a, rf: (n_nodes, 3); sigma: (n_elements, 6)) and clock."""
+        sn = Snapshot()
+        self._check(self._lib.ensc_snapshot_wait(self.h, C.byref(sn)))
+        nn, ne = self.n_nodes, self.n_elements
+        out = {k: np.ctypeslib.as_array(getattr(sn, k), shape=(nn * 3,)).reshape(nn, 3).copy()
+               for k in ("x", "u", "v", "a", "rf")}
+        out["sigma"] = np.ctypeslib.as_array(sn.sigma, shape=(ne * 6,)).reshape(ne, 6).copy()
+        for k in ("time", "dt_i", "dt_i_1", "total_cycles", "status"):
+            out[k] = getattr(sn, k)
+        return out
 
     def sync(self) -> Dict[str, float]:
         r = StepReport()

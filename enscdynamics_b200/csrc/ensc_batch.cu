@@ -628,7 +628,8 @@ int ensc_batch_download(ensc_batch* b, int32_t slot, double* x, double* u, doubl
     int rc = ENSC_OK;
     for (const Item& it : items) {
         if (!it.dst) continue;
-        ensc::launch_soa_to_aos(it.src, it.n, it.pad, it.comps, it.f32, stage, b->stream);
+        if (it.src == sl.N.v) ensc::launch_v_to_aos(sl.N, mx, stage, b->stream);
+        else ensc::launch_soa_to_aos(it.src, it.n, it.pad, it.comps, it.f32, stage, b->stream);
         cudaError_t e = cudaMemcpyAsync(it.dst, stage, it.n * it.comps * sizeof(double), cudaMemcpyDeviceToHost,
                                         b->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);

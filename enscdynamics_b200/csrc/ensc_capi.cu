@@ -50,6 +50,17 @@ struct ensc_handle {
     cudaGraphExec_t graph = nullptr;
     bool kinetic0_done = false;
     double* amp = nullptr;         // device gravity amplitude table
+    // output snapshots (ensc_snapshot_begin / ensc_snapshot_wait): a device
+    // buffer of AoS fields and the control block, copied on copy_stream into
+    // two pinned host buffers used in turn
+    double* snap_dev = nullptr;
+    size_t snap_bytes = 0;
+    double* snap_host[2] = {nullptr, nullptr};
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t snap_captured = nullptr;
+    cudaEvent_t snap_landed[2] = {nullptr, nullptr};
+    int64_t snap_count = 0;
+    bool fe_valid = false;         // fe holds the last force pass's element forces
     std::string err;
 };
 
@@ -85,7 +96,6 @@ int cuda_err(ensc_handle* h, const char* what, cudaError_t e) {
         if (_e != cudaSuccess) return cuda_err((h), #call, _e); \
     } while (0)
 
-int64_t pad32(int64_t n) { return (n + 31) / 32 * 32; }
 
 template <typename T>
 int upload(ensc_handle* h, void* dst, const std::vector<T>& src) {
@@ -366,6 +376,21 @@ int ensc_step_async(ensc_handle* h, int64_t max_cycles, double step_end_time) {
     const int64_t launches = (max_cycles + h->chunk - 1) / h->chunk;
     for (int64_t i = 0; i < launches; ++i) CK(h, cudaGraphLaunch(h->graph, h->stream));
     CK(h, cudaGetLastError());
+    h->fe_valid = true;
+    return ENSC_OK;
+}
+
+int ensc_step_until_async(ensc_handle* h, int64_t max_cycles, double step_end_time, double pause_time) {
+    if (!h || max_cycles < 0) return ENSC_ERR_ARG;
+    if (max_cycles > (int64_t(1) << 24))
+        return set_err(h, ENSC_ERR_ARG, "ensc_step_until_async: at most 2^24 cycles per call");
+    if (max_cycles == 0) return ENSC_OK;
+    DevGuard dg(h->device);
+    ensc::launch_arm(h->ctl, step_end_time, max_cycles, h->stream, pause_time);
+    const int64_t launches = (max_cycles + h->chunk - 1) / h->chunk;
+    for (int64_t i = 0; i < launches; ++i) CK(h, cudaGraphLaunch(h->graph, h->stream));
+    CK(h, cudaGetLastError());
+    h->fe_valid = true;
     return ENSC_OK;
 }
 
@@ -401,6 +426,7 @@ int ensc_step_until(ensc_handle* h, int64_t max_cycles, double step_end_time, do
             const int64_t n = std::min(batch, needed - launched);
             for (int64_t i = 0; i < n; ++i) CK(h, cudaGraphLaunch(h->graph, h->stream));
             launched += n;
+            h->fe_valid = true;
             int rc = read_ctl(h);
             if (rc) return rc;
             if (h->ctl_host->done || h->ctl_host->status) break;
@@ -417,7 +443,10 @@ int ensc_step_until(ensc_handle* h, int64_t max_cycles, double step_end_time, do
 // The staging area may be the element force scratch, whose slots no
 // element fills must read as zeros for the node pass: clear what was used.
 static int release_staging(ensc_handle* h, size_t used) {
-    if (!h->staging_owned && used) CK(h, cudaMemsetAsync(h->staging, 0, used, h->stream));
+    if (!h->staging_owned && used) {
+        h->fe_valid = false;
+        CK(h, cudaMemsetAsync(h->staging, 0, used, h->stream));
+    }
     return ENSC_OK;
 }
 
@@ -438,7 +467,8 @@ int ensc_download(ensc_handle* h, double* x, double* u, double* v, double* sigma
     size_t used = 0;
     for (const Item& it : items) {
         if (!it.dst) continue;
-        ensc::launch_soa_to_aos(it.src, it.n, it.pad, it.comps, it.f32, h->staging, h->stream);
+        if (it.src == h->N.v) ensc::launch_v_to_aos(h->N, mx, h->staging, h->stream);
+        else ensc::launch_soa_to_aos(it.src, it.n, it.pad, it.comps, it.f32, h->staging, h->stream);
         CK(h, cudaGetLastError());
         CK(h, cudaMemcpyAsync(it.dst, h->staging, it.n * it.comps * sizeof(double), cudaMemcpyDeviceToHost,
                               h->stream));
@@ -479,7 +509,8 @@ int ensc_upload_state(ensc_handle* h, const double* x, const double* u, const do
         if (!it.src) continue;
         CK(h, cudaMemcpyAsync(h->staging, it.src, it.n * it.comps * sizeof(double), cudaMemcpyHostToDevice,
                               h->stream));
-        ensc::launch_aos_to_soa(h->staging, it.n, it.pad, it.comps, it.dst, it.f32, h->stream);
+        if (it.dst == h->N.v) ensc::launch_aos_to_v(h->staging, h->N, mx, h->stream);
+        else ensc::launch_aos_to_soa(h->staging, it.n, it.pad, it.comps, it.dst, it.f32, h->stream);
         CK(h, cudaGetLastError());
         used = std::max(used, static_cast<size_t>(it.n * it.comps) * sizeof(double));
     }
@@ -496,6 +527,83 @@ int ensc_upload_state(ensc_handle* h, const double* x, const double* u, const do
     }
     CK(h, cudaMemcpyAsync(h->ctl, h->ctl_host, sizeof(Ctl), cudaMemcpyHostToDevice, h->stream));
     CK(h, cudaStreamSynchronize(h->stream));
+    return ENSC_OK;
+}
+
+int ensc_snapshot_begin(ensc_handle* h) {
+    if (!h) return ENSC_ERR_ARG;
+    if (!h->fe_valid)
+        return set_err(h, ENSC_ERR_ARG,
+                       "ensc_snapshot_begin: no force pass since the last download or upload; run a cycle first");
+    DevGuard dg(h->device);
+    const size_t nodes3 = static_cast<size_t>(3 * h->nn), elems6 = static_cast<size_t>(6 * h->ne);
+    const size_t fields = (5 * nodes3 + elems6) * sizeof(double);
+    if (!h->snap_dev) {
+        h->snap_bytes = (fields + 255) / 256 * 256 + sizeof(Ctl);
+        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&h->snap_dev), h->snap_bytes);
+        if (e != cudaSuccess) {
+            h->snap_dev = nullptr;
+            return cuda_err(h, "cudaMalloc(snapshot)", e);
+        }
+        for (int k = 0; k < 2; ++k) {
+            e = cudaMallocHost(reinterpret_cast<void**>(&h->snap_host[k]), h->snap_bytes);
+            if (e != cudaSuccess) {
+                h->snap_host[k] = nullptr;
+                return cuda_err(h, "cudaMallocHost(snapshot)", e);
+            }
+        }
+        CK(h, cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+        CK(h, cudaEventCreateWithFlags(&h->snap_captured, cudaEventDisableTiming));
+        for (int k = 0; k < 2; ++k) CK(h, cudaEventCreateWithFlags(&h->snap_landed[k], cudaEventDisableTiming));
+    }
+    // the previous snapshot's copy to the host reads the device buffer this
+    // one overwrites (the copy before it used the same host buffer and ran
+    // earlier on the same copy stream)
+    if (h->snap_count > 0) CK(h, cudaStreamWaitEvent(h->stream, h->snap_landed[(h->snap_count - 1) % 2], 0));
+    double* d = h->snap_dev;
+    const bool mx = mixed(h);
+    if (mx) ensc::launch_acceleration_mixed(h->E, h->N, h->M, h->ctl, d + 3 * nodes3, h->stream);
+    else ensc::launch_acceleration_fp64(h->E, h->N, h->M, h->ctl, d + 3 * nodes3, h->stream);
+    ensc::launch_soa_to_aos(h->N.x, h->nn, h->nn_pad, 3, false, d, h->stream);
+    ensc::launch_soa_to_aos(h->N.u, h->nn, h->nn_pad, 3, false, d + nodes3, h->stream);
+    ensc::launch_v_to_aos(h->N, mx, d + 2 * nodes3, h->stream);
+    ensc::launch_soa_to_aos(h->N.rf, h->nn, h->nn_pad, 3, false, d + 4 * nodes3, h->stream);
+    ensc::launch_soa_to_aos(h->E.sigma, h->ne, h->ne_pad, 6, mx, d + 5 * nodes3, h->stream);
+    CK(h, cudaGetLastError());
+    char* ctl_copy = reinterpret_cast<char*>(d) + (h->snap_bytes - sizeof(Ctl));
+    CK(h, cudaMemcpyAsync(ctl_copy, h->ctl, sizeof(Ctl), cudaMemcpyDeviceToDevice, h->stream));
+    CK(h, cudaEventRecord(h->snap_captured, h->stream));
+    const int k = static_cast<int>(h->snap_count % 2);
+    CK(h, cudaStreamWaitEvent(h->copy_stream, h->snap_captured, 0));
+    CK(h, cudaMemcpyAsync(h->snap_host[k], h->snap_dev, h->snap_bytes, cudaMemcpyDeviceToHost, h->copy_stream));
+    CK(h, cudaEventRecord(h->snap_landed[k], h->copy_stream));
+    h->snap_count += 1;
+    return ENSC_OK;
+}
+
+int ensc_snapshot_wait(ensc_handle* h, ensc_snapshot* out) {
+    if (!h || !out) return ENSC_ERR_ARG;
+    if (h->snap_count == 0) return set_err(h, ENSC_ERR_ARG, "ensc_snapshot_wait: no snapshot begun");
+    DevGuard dg(h->device);
+    const int k = static_cast<int>((h->snap_count - 1) % 2);
+    CK(h, cudaEventSynchronize(h->snap_landed[k]));
+    const double* b = h->snap_host[k];
+    const size_t nodes3 = static_cast<size_t>(3 * h->nn);
+    out->x = b;
+    out->u = b + nodes3;
+    out->v = b + 2 * nodes3;
+    out->a = b + 3 * nodes3;
+    out->rf = b + 4 * nodes3;
+    out->sigma = b + 5 * nodes3;
+    Ctl c;
+    std::memcpy(&c, reinterpret_cast<const char*>(b) + (h->snap_bytes - sizeof(Ctl)), sizeof(Ctl));
+    out->time = c.time;
+    out->dt_i = c.dt_i;
+    out->dt_i_1 = c.dt_i_1;
+    out->total_cycles = c.cycles_done;
+    out->status = (c.status & ensc::ST_TIMEOUT) ? ENSC_ERR_TIMEOUT
+                  : (c.status & ensc::ST_INVERTED) ? ENSC_ERR_INVERTED
+                  : c.status ? ENSC_ERR_NONFINITE : ENSC_OK;
     return ENSC_OK;
 }
 
@@ -573,6 +681,16 @@ void ensc_destroy(ensc_handle* h) {
     if (h->staging_owned && h->staging) cudaFree(h->staging);
     if (h->arena) cudaFree(h->arena);
     if (h->amp) cudaFree(h->amp);
+    if (h->copy_stream) {
+        cudaStreamSynchronize(h->copy_stream);
+        cudaStreamDestroy(h->copy_stream);
+    }
+    if (h->snap_captured) cudaEventDestroy(h->snap_captured);
+    for (int k = 0; k < 2; ++k) {
+        if (h->snap_landed[k]) cudaEventDestroy(h->snap_landed[k]);
+        if (h->snap_host[k]) cudaFreeHost(h->snap_host[k]);
+    }
+    if (h->snap_dev) cudaFree(h->snap_dev);
     if (h->ctl_host) cudaFreeHost(h->ctl_host);
     delete h;
 }

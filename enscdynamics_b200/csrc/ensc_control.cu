@@ -5,6 +5,7 @@
 #include "ensc_device.cuh"
 #include "ensc_kernels.h"
 
+#include <algorithm>
 #include <cfloat>
 
 namespace ensc {
@@ -215,30 +216,47 @@ __global__ void k_reset_init(Ctl* ctl) {
 
 // apply_boundary_condition_vec (exDyna3D.cpp:379-490): velocity conditions
 // first, fixed DOFs last.
+// One velocity component of a node: FP64, or the mixed stepper's float
+// (with its residual row, ENSC_MIXED_VLO).
+template <typename VT>
+__device__ __forceinline__ double load_v(const NodeArrays& N, int c, int64_t n) {
+    const int64_t i = c * N.nn_pad + n;
+    if constexpr (sizeof(VT) == 4 && ENSC_MIXED_VLO)
+        return v_join(static_cast<const float*>(N.v)[i], v_lo_rows(N.v, N.nn_pad)[i]);
+    else
+        return static_cast<double>(static_cast<const VT*>(N.v)[i]);
+}
+template <typename VT>
+__device__ __forceinline__ void store_v(const NodeArrays& N, int c, int64_t n, double v) {
+    const int64_t i = c * N.nn_pad + n;
+    if constexpr (sizeof(VT) == 4 && ENSC_MIXED_VLO)
+        v_split(v, static_cast<float*>(N.v)[i], v_lo_rows(N.v, N.nn_pad)[i]);
+    else
+        static_cast<VT*>(N.v)[i] = static_cast<VT>(v);
+}
+
 template <typename VT>
 __global__ void k_apply_bc_v(NodeArrays N) {
-    VT* V = static_cast<VT*>(N.v);
     for (int64_t n = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; n < N.nn;
          n += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         const uint32_t code = N.bc[n];
         if (!code) continue;
         for (int c = 0; c < 3; ++c) {
             const uint32_t cc = (code >> (2 * c)) & 3u;
-            if (cc & 2u) V[c * N.nn_pad + n] = static_cast<VT>(N.bcv[c * N.nn_pad + n]);
-            if (cc & 1u) V[c * N.nn_pad + n] = static_cast<VT>(0.0);
+            if (cc & 2u) store_v<VT>(N, c, n, N.bcv[c * N.nn_pad + n]);
+            if (cc & 1u) store_v<VT>(N, c, n, 0.0);
         }
     }
 }
 
 template <typename VT>
 __global__ void __launch_bounds__(kNodeThreads) k_kinetic(NodeArrays N, Partials P) {
-    const VT* V = static_cast<const VT*>(N.v);
     double kin = 0.0;
     for (int64_t n = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; n < N.nn;
          n += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         const double im = N.inv_mass[n];
         for (int c = 0; c < 3; ++c) {
-            const double v = static_cast<double>(V[c * N.nn_pad + n]);
+            const double v = load_v<VT>(N, c, n);
             kin = kin + 0.5 * (v * v) / im;
         }
     }
@@ -263,6 +281,20 @@ __global__ void k_soa_to_aos(const ST* soa, int64_t n, int64_t pad, int comps, d
         const int c = static_cast<int>(i - e * comps);
         aos[i] = static_cast<double>(soa[c * pad + e]);
     }
+}
+
+// Velocities between interleaved xyz doubles and the device rows.
+template <typename VT>
+__global__ void k_v_to_aos(NodeArrays N, double* aos) {
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < 3 * N.nn;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        aos[i] = load_v<VT>(N, static_cast<int>(i % 3), i / 3);
+}
+template <typename VT>
+__global__ void k_aos_to_v(const double* aos, NodeArrays N) {
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < 3 * N.nn;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        store_v<VT>(N, static_cast<int>(i % 3), i / 3, aos[i]);
 }
 
 template <typename DT>
@@ -444,6 +476,16 @@ void launch_soa_to_aos(const void* soa, int64_t n, int64_t pad, int comps, bool 
     const int g = grid_for(n * comps, 256);
     if (src_fp32) k_soa_to_aos<float><<<g, 256, 0, st>>>(static_cast<const float*>(soa), n, pad, comps, aos);
     else k_soa_to_aos<double><<<g, 256, 0, st>>>(static_cast<const double*>(soa), n, pad, comps, aos);
+}
+void launch_v_to_aos(const NodeArrays& N, bool fp32_v, double* aos, cudaStream_t st) {
+    const int g = static_cast<int>(std::min<int64_t>((3 * N.nn + 255) / 256, 65535));
+    if (fp32_v) k_v_to_aos<float><<<g, 256, 0, st>>>(N, aos);
+    else k_v_to_aos<double><<<g, 256, 0, st>>>(N, aos);
+}
+void launch_aos_to_v(const double* aos, const NodeArrays& N, bool fp32_v, cudaStream_t st) {
+    const int g = static_cast<int>(std::min<int64_t>((3 * N.nn + 255) / 256, 65535));
+    if (fp32_v) k_aos_to_v<float><<<g, 256, 0, st>>>(aos, N);
+    else k_aos_to_v<double><<<g, 256, 0, st>>>(aos, N);
 }
 void launch_aos_to_soa(const double* aos, int64_t n, int64_t pad, int comps, void* soa, bool dst_fp32,
                        cudaStream_t st) {

@@ -321,6 +321,53 @@ __host__ __device__ inline double gravity_amplitude(const double* amp, int n, do
     return y;
 }
 
+// ---- mixed-precision velocities ---------------------------------------------
+// The mixed stepper keeps each velocity component as a float `hi` (what the
+// element pass reads) and a 16-bit residual `lo` in units of 2^-16 of hi's
+// spacing: v = hi + lo * ulp(hi) / 2^16, about 40 significant bits.  The node
+// pass updates v in FP64 and splits it again, so the velocity integration
+// does not drop FP32 rounding every cycle.  In memory the residual rows
+// follow the three float rows: [3][nn_pad] float, then [3][nn_pad] int16.
+#ifndef ENSC_MIXED_VLO
+#define ENSC_MIXED_VLO 1
+#endif
+
+// ulp(hi) / 2^16 and its inverse (normal or zero hi; hi's exponent field e
+// gives ulp(hi) = 2^(e - 150), with e = 1 for zero and subnormals)
+__host__ __device__ inline double vlo_unit(float hi) {
+    uint32_t b;
+    memcpy(&b, &hi, sizeof b);
+    int e = static_cast<int>((b >> 23) & 0xFFu);
+    if (e == 0) e = 1;
+    const uint64_t d = static_cast<uint64_t>(e - 166 + 1023) << 52;
+    double r;
+    memcpy(&r, &d, sizeof r);
+    return r;
+}
+__host__ __device__ inline double vlo_inv_unit(float hi) {
+    uint32_t b;
+    memcpy(&b, &hi, sizeof b);
+    int e = static_cast<int>((b >> 23) & 0xFFu);
+    if (e == 0) e = 1;
+    const uint64_t d = static_cast<uint64_t>(166 - e + 1023) << 52;
+    double r;
+    memcpy(&r, &d, sizeof r);
+    return r;
+}
+__host__ __device__ inline double v_join(float hi, int16_t lo) {
+    return static_cast<double>(hi) + static_cast<double>(lo) * vlo_unit(hi);
+}
+__host__ __device__ inline void v_split(double v, float& hi, int16_t& lo) {
+    hi = static_cast<float>(v);
+    double q = rint((v - static_cast<double>(hi)) * vlo_inv_unit(hi));
+    if (!(q >= -32768.0 && q <= 32767.0)) q = q > 0.0 ? 32767.0 : -32768.0;  // |q| <= 2^15; NaN -> bound
+    lo = static_cast<int16_t>(q);
+}
+// the residual rows of a mixed velocity array
+__host__ __device__ inline int16_t* v_lo_rows(void* v, int64_t nn_pad) {
+    return reinterpret_cast<int16_t*>(static_cast<float*>(v) + 3 * nn_pad);
+}
+
 // Vector access to W consecutive entries of a padded SoA row (rows start
 // 256-byte aligned, the row stride is a multiple of 32 entries and the first
 // index a multiple of W): 16-byte chunks, or one 8-byte chunk when the W

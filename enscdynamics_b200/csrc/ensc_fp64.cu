@@ -11,6 +11,7 @@
 #include "ensc_kernels.h"
 #include "ensc_stage.cuh"
 
+#include <algorithm>
 #include <cfloat>
 
 namespace ensc {
@@ -413,17 +414,7 @@ __global__ void __launch_bounds__(kElemThreads, ENSC_ELEM_MINB_FP64) k_element(E
                                                              Partials P) {
     if (ctl->done) return;
     const double dt1 = INIT ? 0.0 : ctl->dt_i_1;
-    const int64_t ne = E.ne, ep = E.ne_pad, np = N.nn_pad;
-    const uint32_t* __restrict__ conn = E.conn;
-    const double* __restrict__ bt = static_cast<const double*>(E.bt);
-    double* __restrict__ sig = static_cast<double*>(E.sigma);
-    double* __restrict__ qia = static_cast<double*>(E.qia);
-    double* __restrict__ epsp = static_cast<double*>(E.eps_p);
-    double* __restrict__ fe = static_cast<double*>(E.fe);
-    const double* __restrict__ X = N.x;
-    const double* __restrict__ U = N.u;
-    const double* __restrict__ V = static_cast<const double*>(N.v);
-    const double G = M.G, lam = M.lambda;
+    const int64_t ne = E.ne;
     double e_int = 0.0, e_hg = 0.0, e_vis = 0.0;
     double dts_min = DBL_MAX, len_min = DBL_MAX;
     int32_t bad = 0;
@@ -682,6 +673,181 @@ __global__ void __launch_bounds__(kStageTileF64, BT ? kStageMinbF64 : kStageMinb
     block_min2<kStageTileF64>(dts_min, len_min, &ctl->dts_next, &ctl->len_min);
     double v3[3] = {e_int, e_hg, e_vis};
     block_sum<kStageTileF64, 3, 7u>(v3, P.elem, P.n_elem_blocks, blockIdx.x);
+}
+
+// ---- output: the last cycle's acceleration --------------------------------
+// solution_a as compute_a leaves it (exDyna3D.cpp:642-644) in the last cycle
+// -- assembled element forces, gravity, the acceleration boundary conditions,
+// times the inverse mass -- which output_results writes (:231).  The node
+// pass does not store it; this pass evaluates it again from the element
+// forces that the last force pass left in fe, with the node pass's
+// arithmetic in the node pass's order (the grouped layout adds all 8 slots,
+// empty ones as the zeros they hold).  Writes interleaved xyz per node.
+__global__ void __launch_bounds__(kNodeThreads) k_acceleration(ElemArrays E, NodeArrays N, Material M, const Ctl* ctl,
+                                                               double* a_out) {
+    const int64_t np = N.nn_pad, ep = E.ne_pad;
+    const double* __restrict__ fe = static_cast<const double*>(E.fe);
+    const bool grouped = E.slot_major && E.tiles_aligned;
+    const double amp = (M.gravity_on && M.amp_n > 0) ? gravity_amplitude(M.amp, M.amp_n, ctl->time, ctl->dt_i) : 1.0;
+    for (int64_t n = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; n < N.nn;
+         n += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        double f[3] = {0.0, 0.0, 0.0};
+        if (E.slot_major) {
+            const uint32_t msk = grouped ? 0xffu : N.slot_mask[n];
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                if ((msk >> k) & 1u) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) f[c] = f[c] + fe[(3 * k + c) * np + n];
+                }
+        } else if (N.csr_ptr == nullptr) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const uint32_t el = N.ell[k * np + n];
+                if (el != ENSC_NONE) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) f[c] = f[c] + fe[(3 * k + c) * ep + el];
+                }
+            }
+        } else {
+            int cur = -1;
+            double sl[3] = {0.0, 0.0, 0.0};
+            for (int64_t i = N.csr_ptr[n]; i < N.csr_ptr[n + 1]; ++i) {
+                const uint32_t ent = N.csr_ent[i];
+                const int k = static_cast<int>(ent & 7u);
+                const uint32_t el = ent >> 3;
+                if (k != cur) {
+                    if (cur >= 0) {
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) f[c] = f[c] + sl[c];
+                    }
+                    cur = k;
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) sl[c] = 0.0 + fe[(3 * k + c) * ep + el];
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) sl[c] = sl[c] + fe[(3 * k + c) * ep + el];
+                }
+            }
+            if (cur >= 0) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) f[c] = f[c] + sl[c];
+            }
+        }
+        const double im = N.inv_mass[n];
+        const uint32_t code = N.bc[n];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            double a = f[c];
+            if (M.gravity_on) a = a + amp * M.gravity_value * M.gravity_dir[c] / im;
+            const uint32_t cc = (code >> (2 * c)) & 3u;
+            if (cc & 2u) a = 0.0;
+            if ((cc & 1u) && a != 0.0) a = 0.0;
+            a_out[3 * n + c] = a * im;
+        }
+    }
+}
+
+// ---- warp-pipelined element pass ---------------------------------------
+// As k_element_staged (B0^T staged too), but every warp runs its own
+// pipeline over tiles of 32 consecutive elements: its own two stages, its
+// own barriers, a stage reused as soon as its 32 lanes are done with it, and
+// no block-wide barrier per tile.  element_body's arithmetic, so results are
+// bit-identical to the other FP64 element passes.
+constexpr int kF64WarpTile = 32;
+constexpr uint32_t kF64WarpStageBytes = 8u * kF64WarpTile * 4u + (kF64StageRows + 24) * kF64WarpTile * 8u;
+constexpr int kF64PipeWarps = ENSC_F64_PIPE_WARPS;
+constexpr size_t kF64WarpPipeSmem = static_cast<size_t>(kF64PipeWarps) * (2 * kF64WarpStageBytes + 16);
+
+template <bool PLASTIC>
+__device__ __forceinline__ void f64_warp_stage_issue(const ElemArrays& E, uint32_t dst, uint32_t bar, int64_t base,
+                                                     int lane) {
+    constexpr int drows = kF64StageRows + 24;
+    // whole 32-entry tiles of rows padded to multiples of 32: 128- and
+    // 256-byte copies
+    if (lane == 0) mbar_arrive_expect_tx(bar, f64_stage_tx_bytes<PLASTIC, true>(kF64WarpTile));
+    __syncwarp();
+    fence_proxy_async_smem();  // the warp's reads of this stage come before the copies into it
+    const uint32_t dbase = dst + 8u * kF64WarpTile * 4u;
+    for (int q = lane; q < 8 + drows; q += 32) {
+        if (q < 8) {
+            bulk_g2s(dst + q * (kF64WarpTile * 4u), E.conn + q * E.ne_pad + base, kF64WarpTile * 4u, bar);
+        } else {
+            const int r = q - 8;
+            if (PLASTIC || r != 21)  // eps_p is read only with J2
+                bulk_g2s(dbase + r * (kF64WarpTile * 8u), f64_stage_row(E, r) + base, kF64WarpTile * 8u, bar);
+        }
+    }
+}
+
+template <bool PLASTIC>
+__global__ void __launch_bounds__(32 * kF64PipeWarps, ENSC_F64_PIPE_MINB)
+    k_element_fp64_warp(ElemArrays E, NodeArrays N, Material M, Ctl* ctl, Partials P) {
+    if (ctl->done) return;
+    extern __shared__ __align__(128) unsigned char smem[];
+    constexpr int T = kF64WarpTile;
+    const double dt1 = ctl->dt_i_1;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    unsigned char* wst = smem + static_cast<size_t>(wid) * 2 * kF64WarpStageBytes;
+    const uint32_t stage0 = smem_addr(wst);
+    const uint32_t bar0 = smem_addr(smem + static_cast<size_t>(kF64PipeWarps) * 2 * kF64WarpStageBytes) + 16u * wid;
+    const int64_t ntiles = (E.ne + T - 1) / T;
+    const int64_t wstride = static_cast<int64_t>(gridDim.x) * kF64PipeWarps;
+    const int64_t w0 = static_cast<int64_t>(blockIdx.x) * kF64PipeWarps + wid;
+    if (lane == 0) {
+        mbar_init(bar0, 1);
+        mbar_init(bar0 + 8, 1);
+        mbar_init_fence();
+    }
+    __syncwarp();
+    for (int s = 0; s < 2; ++s) {
+        const int64_t t = w0 + s * wstride;
+        if (t < ntiles) f64_warp_stage_issue<PLASTIC>(E, stage0 + s * kF64WarpStageBytes, bar0 + 8 * s, t * T, lane);
+    }
+    double e_int = 0.0, e_hg = 0.0, e_vis = 0.0;
+    double dts_min = DBL_MAX, len_min = DBL_MAX;
+    int32_t bad = 0;
+    bool timed_out = false;
+    int it = 0;
+    for (int64_t t = w0; t < ntiles; t += wstride, ++it) {
+        const int s = it & 1;
+        const uint32_t bar = bar0 + 8 * s;
+        const bool ok = mbar_wait_bounded(bar, (it >> 1) & 1);
+        if (__any_sync(0xffffffffu, !ok)) {
+            timed_out = true;
+            break;
+        }
+        const int64_t e = t * T + lane;
+        if (e < E.ne) {
+            const unsigned char* st = wst + s * kF64WarpStageBytes;
+            const double* d = reinterpret_cast<const double*>(st + 8 * T * 4);
+            const Fp64Src S{reinterpret_cast<const uint32_t*>(st), d, d + 6 * T, d + 18 * T, d + 19 * T, d + 20 * T,
+                            d + 21 * T, T, lane, d + kF64StageRows * T, static_cast<int64_t>(T),
+                            static_cast<int64_t>(lane)};
+            double dts, len;
+            element_body<PLASTIC, false, true, true>(E, N, M, S, dt1, e, dts, len, e_int, e_hg, e_vis, bad);
+            dts_min = dts < dts_min ? dts : dts_min;
+            len_min = len < len_min ? len : len_min;
+        }
+        const int64_t tn = t + 2 * wstride;
+        if (tn < ntiles) f64_warp_stage_issue<PLASTIC>(E, stage0 + s * kF64WarpStageBytes, bar, tn * T, lane);
+    }
+    if (timed_out) {
+        // record the failure and let the copies this warp started land
+        // (bounded) before the block's shared memory is released
+        if (lane == 0) {
+            atomicOr(&ctl->status, ST_TIMEOUT);
+            for (int k = 0; k < 2; ++k) {
+                const int itk = it + k;
+                if (w0 + itk * wstride < ntiles) mbar_wait_bounded(bar0 + 8 * (itk & 1), (itk >> 1) & 1);
+            }
+        }
+        __syncwarp();
+    }
+    if (bad) atomicOr(&ctl->status, bad);
+    block_min2<32 * kF64PipeWarps>(dts_min, len_min, &ctl->dts_next, &ctl->len_min);
+    double v3[3] = {e_int, e_hg, e_vis};
+    block_sum<32 * kF64PipeWarps, 3, 7u>(v3, P.elem, P.n_elem_blocks, blockIdx.x);
 }
 
 // W consecutive nodes of the node pass with 16-byte row accesses: the same
@@ -1069,6 +1235,11 @@ constexpr bool kStagedBt = ENSC_STAGED_FP64 == 2;
 
 void launch_element_fp64(const ElemArrays& E, const NodeArrays& N, const Material& M, Ctl* ctl, const Partials& P,
                          int grid, bool init, cudaStream_t st) {
+    if (ENSC_WARP_PIPE_FP64 && !init && E.tiles_aligned) {
+        if (M.plastic) k_element_fp64_warp<true><<<grid, 32 * kF64PipeWarps, kF64WarpPipeSmem, st>>>(E, N, M, ctl, P);
+        else k_element_fp64_warp<false><<<grid, 32 * kF64PipeWarps, kF64WarpPipeSmem, st>>>(E, N, M, ctl, P);
+        return;
+    }
     if (ENSC_STAGED_FP64 && !init && E.tiles_aligned) {
         constexpr size_t smem = f64_stage_smem<kStagedBt>();
         if (M.plastic) k_element_staged<true, kStagedBt><<<grid, kStageTileF64, smem, st>>>(E, N, M, ctl, P);
@@ -1091,6 +1262,19 @@ void launch_node_fp64(const ElemArrays& E, const NodeArrays& N, const Material& 
 
 int occupancy_element_fp64(bool plastic) {
     int nb = 0;
+    if (ENSC_WARP_PIPE_FP64) {
+        cudaFuncSetAttribute(k_element_fp64_warp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(kF64WarpPipeSmem));
+        cudaFuncSetAttribute(k_element_fp64_warp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(kF64WarpPipeSmem));
+        if (plastic)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_fp64_warp<true>, 32 * kF64PipeWarps,
+                                                          kF64WarpPipeSmem);
+        else
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_fp64_warp<false>, 32 * kF64PipeWarps,
+                                                          kF64WarpPipeSmem);
+        return nb;
+    }
     if (ENSC_STAGED_FP64) {
         // more than the default 48 KB of dynamic shared memory: set on the
         // current device, before any launch or capture
@@ -1108,6 +1292,12 @@ int occupancy_element_fp64(bool plastic) {
     if (plastic) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element<true, false>, kElemThreads, 0);
     else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element<false, false>, kElemThreads, 0);
     return nb;
+}
+
+void launch_acceleration_fp64(const ElemArrays& E, const NodeArrays& N, const Material& M, const Ctl* ctl,
+                              double* a_aos, cudaStream_t st) {
+    const int64_t g = std::min<int64_t>((N.nn + kNodeThreads - 1) / kNodeThreads, 65535);
+    k_acceleration<<<static_cast<int>(g), kNodeThreads, 0, st>>>(E, N, M, ctl, a_aos);
 }
 
 int node_group_width(bool mixed_precision) { return mixed_precision ? kNodeGroupMixed : kNodeGroupFp64; }

@@ -190,7 +190,8 @@ int instance_prepare(const ensc_mesh_desc* mesh, const ensc_material* mat, bool 
     h.size[P::FE] = 24 * fe_rows * real;
     h.size[P::X] = 3 * N8 * 8;
     h.size[P::U] = 3 * N8 * 8;
-    h.size[P::V] = 3 * N8 * real;
+    // mixed: float rows, then the 16-bit velocity residual rows (v_lo_rows)
+    h.size[P::V] = 3 * N8 * real + ((mixed && ENSC_MIXED_VLO) ? 3 * N8 * sizeof(int16_t) : 0);
     h.size[P::IM] = N8 * 8;
     h.size[P::BC] = N8;
     h.size[P::BCV] = 3 * N8 * 8;
@@ -251,6 +252,13 @@ int instance_upload(const InstanceHost& h, void* block, cudaStream_t st, ElemArr
     if (h.v0) {
         if (h.mixed) {
             vf = to_soa<float>(h.v0, h.nn, np, 3);
+#if ENSC_MIXED_VLO
+            std::vector<int16_t> vl(static_cast<size_t>(3 * np), 0);
+            for (int64_t n = 0; n < h.nn; ++n)
+                for (int c = 0; c < 3; ++c) v_split(h.v0[3 * n + c], vf[c * np + n], vl[c * np + n]);
+            if (e == cudaSuccess) e = put(block, h.off[P::V] + 3 * np * sizeof(float), vl, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // vl dies here
+#endif
             if (e == cudaSuccess) e = put(block, h.off[P::V], vf, st);
         } else {
             vd = to_soa<double>(h.v0, h.nn, np, 3);

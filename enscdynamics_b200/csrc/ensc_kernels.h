@@ -33,6 +33,24 @@ constexpr int kNodeUnrollMixed = ENSC_NODE_UNROLL_MIXED;
 #ifndef ENSC_STAGED_MIXED
 #define ENSC_STAGED_MIXED 1
 #endif
+// 1: the single-instance mixed element pass runs one bulk-copy pipeline per
+// warp (k_element_mixed_warp: 32-element tiles, two stages per warp, no
+// block-wide barrier per tile) instead of one per block
+#ifndef ENSC_WARP_PIPE_MIXED
+#define ENSC_WARP_PIPE_MIXED 1
+#endif
+// 1: the batched mixed element pass runs one pipeline per warp too
+// (k_element_batch_mixed_warp, 32-element batch tiles)
+#ifndef ENSC_WARP_PIPE_BATCH
+#define ENSC_WARP_PIPE_BATCH 1
+#endif
+// warps per block and resident blocks per SM of the warp-pipelined passes
+#ifndef ENSC_WARP_PIPE_WARPS
+#define ENSC_WARP_PIPE_WARPS 4
+#endif
+#ifndef ENSC_WARP_PIPE_MINB
+#define ENSC_WARP_PIPE_MINB 4
+#endif
 // elements per stage (= threads per block) and resident blocks per SM of
 // the staged mixed pass; tuned on B200
 #ifndef ENSC_STAGE_TILE_MIXED
@@ -75,6 +93,17 @@ constexpr int kNodeUnrollMixed = ENSC_NODE_UNROLL_MIXED;
 #ifndef ENSC_STAGED_FP64
 #define ENSC_STAGED_FP64 2
 #endif
+// 1: the single-instance FP64 element pass runs one bulk-copy pipeline per
+// warp (k_element_fp64_warp), as the mixed one does
+#ifndef ENSC_WARP_PIPE_FP64
+#define ENSC_WARP_PIPE_FP64 1
+#endif
+#ifndef ENSC_F64_PIPE_WARPS
+#define ENSC_F64_PIPE_WARPS 4
+#endif
+#ifndef ENSC_F64_PIPE_MINB
+#define ENSC_F64_PIPE_MINB 2
+#endif
 // elements per stage (= threads per block) of the staged FP64 passes
 #ifndef ENSC_STAGE_TILE_FP64
 #define ENSC_STAGE_TILE_FP64 128
@@ -113,6 +142,13 @@ void launch_node_mixed(const ElemArrays& E, const NodeArrays& N, const Material&
 int occupancy_element_mixed(bool plastic);
 int occupancy_node_mixed();
 
+// the last cycle's acceleration (compute_a), interleaved xyz per node, from
+// the element forces the last force pass left in E.fe
+void launch_acceleration_fp64(const ElemArrays& E, const NodeArrays& N, const Material& M, const Ctl* ctl,
+                              double* a_aos, cudaStream_t st);
+void launch_acceleration_mixed(const ElemArrays& E, const NodeArrays& N, const Material& M, const Ctl* ctl,
+                               double* a_aos, cudaStream_t st);
+
 // batched instances (one launch per phase for all instances of a batch)
 void launch_element_batch_fp64(const BatchTables& T, int grid, cudaStream_t st);
 // threads per block of the batched node passes: kNodeThreads or half of it
@@ -148,6 +184,10 @@ void launch_soa_to_aos(const void* soa, int64_t n, int64_t pad, int comps, bool 
                        cudaStream_t st);
 void launch_aos_to_soa(const double* aos, int64_t n, int64_t pad, int comps, void* soa, bool dst_fp32,
                        cudaStream_t st);
+// velocities (FP64 rows, or the mixed stepper's float rows and residual rows)
+// to and from interleaved xyz doubles
+void launch_v_to_aos(const NodeArrays& N, bool fp32_v, double* aos, cudaStream_t st);
+void launch_aos_to_v(const double* aos, const NodeArrays& N, bool fp32_v, cudaStream_t st);
 
 // thread-local message returned by ensc_last_error(NULL) (ensc_capi.cu)
 void set_thread_error(const std::string& msg);

@@ -649,6 +649,110 @@ __global__ void __launch_bounds__(kStageTile, ENSC_STAGE_MINB_MIXED)
     block_sum_d<kStageTile, 3, 7u>(v3, P.elem, P.n_elem_blocks, blockIdx.x);
 }
 
+// ---- warp-pipelined element pass ---------------------------------------
+// As k_element_mixed_staged, but every warp runs its own pipeline: it walks
+// tiles of 32 consecutive elements (one per lane), fills its own two stages
+// with bulk copies that complete on its own barriers, and reuses a stage as
+// soon as its 32 lanes are done with it.  No warp waits for another warp
+// until the block's final reductions, so a warp held up by its gathers does
+// not stall the others of its block at a per-tile barrier.
+constexpr int kWarpTile = 32;
+constexpr uint32_t kWarpV0Off = kStageWordRows * kWarpTile * 4;
+constexpr uint32_t kWarpStageBytes = kWarpV0Off + kWarpTile * 8;  // 6 KB
+constexpr int kPipeWarps = ENSC_WARP_PIPE_WARPS;
+constexpr size_t kWarpPipeSmem = static_cast<size_t>(kPipeWarps) * (2 * kWarpStageBytes + 16);
+
+template <bool PLASTIC>
+__device__ __forceinline__ void warp_stage_issue(const ElemArrays& E, uint32_t dst, uint32_t bar, int64_t base,
+                                                 int lane) {
+    constexpr int rows = PLASTIC ? kStageWordRows : kStageWordRows - 1;  // eps_p last, J2 only
+    // rows are padded to whole 32-entry tiles: every copy is 128 or 256 bytes
+    if (lane == 0) mbar_arrive_expect_tx(bar, rows * kWarpTile * 4u + kWarpTile * 8u);
+    __syncwarp();
+    fence_proxy_async_smem();  // the warp's reads of this stage come before the copies into it
+    for (int r = lane; r <= rows; r += 32) {
+        if (r < rows) bulk_g2s(dst + r * (kWarpTile * 4u), stage_row(E, r) + base, kWarpTile * 4u, bar);
+        else bulk_g2s(dst + kWarpV0Off, E.vol0 + base, kWarpTile * 8u, bar);
+    }
+}
+
+template <bool PLASTIC>
+__global__ void __launch_bounds__(32 * kPipeWarps, ENSC_WARP_PIPE_MINB)
+    k_element_mixed_warp(ElemArrays E, NodeArrays N, Material M, Ctl* ctl, Partials P) {
+    if (ctl->done) return;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const float dt1 = static_cast<float>(ctl->dt_i_1);
+    const double dt1d = ctl->dt_i_1;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    // this warp's two stages, then the block's barriers (two per warp)
+    unsigned char* wst = smem + static_cast<size_t>(wid) * 2 * kWarpStageBytes;
+    const uint32_t stage0 = smem_addr(wst);
+    const uint32_t bar0 = smem_addr(smem + static_cast<size_t>(kPipeWarps) * 2 * kWarpStageBytes) + 16u * wid;
+    const int64_t ntiles = (E.ne + kWarpTile - 1) / kWarpTile;
+    const int64_t wstride = static_cast<int64_t>(gridDim.x) * kPipeWarps;
+    const int64_t w0 = static_cast<int64_t>(blockIdx.x) * kPipeWarps + wid;
+    if (lane == 0) {
+        mbar_init(bar0, 1);
+        mbar_init(bar0 + 8, 1);
+        mbar_init_fence();
+    }
+    __syncwarp();
+    for (int s = 0; s < 2; ++s) {
+        const int64_t t = w0 + s * wstride;
+        if (t < ntiles) warp_stage_issue<PLASTIC>(E, stage0 + s * kWarpStageBytes, bar0 + 8 * s, t * kWarpTile, lane);
+    }
+    double e_int = 0.0, e_hg = 0.0, e_vis = 0.0;
+    double dts_min = DBL_MAX, len_min = DBL_MAX;
+    int32_t bad = 0;
+    bool timed_out = false;
+    int it = 0;
+    for (int64_t t = w0; t < ntiles; t += wstride, ++it) {
+        const int s = it & 1;
+        const uint32_t bar = bar0 + 8 * s;
+        const bool ok = mbar_wait_bounded(bar, (it >> 1) & 1);
+        if (__any_sync(0xffffffffu, !ok)) {
+            timed_out = true;
+            break;
+        }
+        const int64_t e = t * kWarpTile + lane;
+        if (e < E.ne) {
+            const float* st = reinterpret_cast<const float*>(wst + s * kWarpStageBytes);
+            const MixedSrc S{reinterpret_cast<const uint32_t*>(st),
+                             st + 8 * kWarpTile,
+                             reinterpret_cast<const double*>(wst + s * kWarpStageBytes + kWarpV0Off),
+                             st + 44 * kWarpTile,
+                             st + 26 * kWarpTile,
+                             st + 32 * kWarpTile,
+                             st + 45 * kWarpTile,
+                             kWarpTile,
+                             lane};
+            double dts, len;
+            element_body_mixed<PLASTIC, false, true, ENSC_MIXED_PREFETCH>(E, N, M, S, dt1, dt1d, e, dts, len, e_int,
+                                                                          e_hg, e_vis, bad);
+            dts_min = fmin(dts_min, dts);
+            len_min = fmin(len_min, len);
+        }
+        const int64_t tn = t + 2 * wstride;
+        if (tn < ntiles) warp_stage_issue<PLASTIC>(E, stage0 + s * kWarpStageBytes, bar, tn * kWarpTile, lane);
+    }
+    if (timed_out) {
+        // record the failure and let the copies this warp started land
+        // (bounded) before the block's shared memory is released
+        if (lane == 0) {
+            atomicOr(&ctl->status, ST_TIMEOUT);
+            for (int k = 0; k < 2; ++k) {
+                const int itk = it + k;
+                if (w0 + itk * wstride < ntiles) mbar_wait_bounded(bar0 + 8 * (itk & 1), (itk >> 1) & 1);
+            }
+        }
+        __syncwarp();
+    }
+    if (bad) atomicOr(&ctl->status, bad);
+    block_min2_d<32 * kPipeWarps>(dts_min, len_min, &ctl->dts_next, &ctl->len_min);
+    double v3[3] = {e_int, e_hg, e_vis};
+    block_sum_d<32 * kPipeWarps, 3, 7u>(v3, P.elem, P.n_elem_blocks, blockIdx.x);
+}
+
 // v + (dt_i + dt_i_1) / 2 * f * M^-1 in FP32 with the half step and the
 // inverse mass as float pairs: both are the same for many nodes and cycles,
 // so their FP32 rounding would scale all accelerations alike.
@@ -659,6 +763,20 @@ __device__ __forceinline__ float velocity_update(float vo, float f, double im, f
     return fmaf(hdt, acc, fmaf(hdt_lo, acc, vo));
 }
 
+// The velocity update in FP64 on the split velocity (hi float + 16-bit
+// residual, v_join / v_split): v + (dt_i + dt_i_1) / 2 * a with the FP32
+// acceleration a = f M^-1 (inverse mass as a float pair); returns the new
+// velocity as a double and its split form.
+__device__ __forceinline__ double velocity_update_split(double vo, float f, double im, double hdt, float& hi,
+                                                        int16_t& lo) {
+    const float im_hi = static_cast<float>(im);
+    const float im_lo = static_cast<float>(im - static_cast<double>(im_hi));
+    const float acc = fmaf(f, im_hi, f * im_lo);
+    const double vn = fma(hdt, static_cast<double>(acc), vo);
+    v_split(vn, hi, lo);
+    return vn;
+}
+
 // One node of the mixed node pass; shared by the single-instance and
 // batched kernels.
 __device__ __forceinline__ void node_body_mixed(const ElemArrays& E, const NodeArrays& N, const Material& M,
@@ -667,8 +785,8 @@ __device__ __forceinline__ void node_body_mixed(const ElemArrays& E, const NodeA
     const int64_t np = N.nn_pad, ep = E.ne_pad;
     const float* __restrict__ fe = static_cast<const float*>(E.fe);
     float* __restrict__ V = static_cast<float*>(N.v);
-    const float hdt = static_cast<float>(0.5 * (dt_i + dt_i_1));
-    const float hdt_lo = static_cast<float>(0.5 * (dt_i + dt_i_1) - static_cast<double>(hdt));
+    [[maybe_unused]] const float hdt = static_cast<float>(0.5 * (dt_i + dt_i_1));
+    [[maybe_unused]] const float hdt_lo = static_cast<float>(0.5 * (dt_i + dt_i_1) - static_cast<double>(hdt));
     const double dt_avg = 0.5 * (dt_i + dt_i_1);
 
     float f[3] = {0.f, 0.f, 0.f};
@@ -721,15 +839,26 @@ __device__ __forceinline__ void node_body_mixed(const ElemArrays& E, const NodeA
             a = 0.f;
         }
         if (cc) N.rf[c * np + n] = static_cast<double>(rf);
+#if ENSC_MIXED_VLO
+        int16_t* VL = v_lo_rows(N.v, np);
+        const double vod = v_join(V[c * np + n], VL[c * np + n]);
+        float vn;
+        int16_t vl;
+        const double vnd = velocity_update_split(vod, a, im, dt_avg, vn, vl);
+        V[c * np + n] = vn;
+        VL[c * np + n] = vl;
+#else
         const float vo = V[c * np + n];
         const float vn = velocity_update(vo, a, im, hdt, hdt_lo);
         V[c * np + n] = vn;
         const double vnd = static_cast<double>(vn);
+        const double vod = static_cast<double>(vo);
+#endif
         N.u[c * np + n] += dt_i * vnd;
         N.x[c * np + n] += dt_i * vnd;
-        wext += static_cast<double>(g + r) * dt_avg * 0.5 * (static_cast<double>(vo) + vnd);
+        wext += static_cast<double>(g + r) * dt_avg * 0.5 * (vod + vnd);
         kin += 0.5 * (vnd * vnd) / im;
-        if (!isfinite(vn)) bad |= ST_NONFINITE;
+        if (!isfinite(vnd)) bad |= ST_NONFINITE;
     }
 }
 
@@ -747,8 +876,8 @@ __device__ __forceinline__ void node_group_mixed(const NodeView& N, const double
     const int64_t np = N.np, nn = N.nn;
     const float* __restrict__ fe = static_cast<const float*>(N.fe);
     float* __restrict__ V = static_cast<float*>(N.v);
-    const float hdt = static_cast<float>(0.5 * (dt_i + dt_i_1));
-    const float hdt_lo = static_cast<float>(0.5 * (dt_i + dt_i_1) - static_cast<double>(hdt));
+    [[maybe_unused]] const float hdt = static_cast<float>(0.5 * (dt_i + dt_i_1));
+    [[maybe_unused]] const float hdt_lo = static_cast<float>(0.5 * (dt_i + dt_i_1) - static_cast<double>(hdt));
     const double dt_avg = 0.5 * (dt_i + dt_i_1);
     float f[3][W];
 #pragma unroll
@@ -782,9 +911,17 @@ __device__ __forceinline__ void node_group_mixed(const NodeView& N, const double
         ld_row<W>(V + c * np + n0, vo);
         ld_row<W>(N.u + c * np + n0, uo);
         ld_row<W>(N.x + c * np + n0, xo);
+#if ENSC_MIXED_VLO
+        int16_t* VL = v_lo_rows(N.v, np);
+        int16_t lo[W], ln[W];
+        ld_row<W>(VL + c * np + n0, lo);
+#endif
 #pragma unroll
         for (int j = 0; j < W; ++j) {
             vn[j] = vo[j];
+#if ENSC_MIXED_VLO
+            ln[j] = lo[j];
+#endif
             un[j] = uo[j];
             xn[j] = xo[j];
             if (n0 + j >= nn) continue;
@@ -806,15 +943,24 @@ __device__ __forceinline__ void node_group_mixed(const NodeView& N, const double
                 a = 0.f;
             }
             if (cc) N.rf[c * np + n0 + j] = static_cast<double>(rf);
+#if ENSC_MIXED_VLO
+            const double vod = v_join(vo[j], lo[j]);
+            const double vnd = velocity_update_split(vod, a, im[j], dt_avg, vn[j], ln[j]);
+#else
             vn[j] = velocity_update(vo[j], a, im[j], hdt, hdt_lo);
             const double vnd = static_cast<double>(vn[j]);
+            const double vod = static_cast<double>(vo[j]);
+#endif
             un[j] = uo[j] + dt_i * vnd;
             xn[j] = xo[j] + dt_i * vnd;
-            wext += static_cast<double>(g + r) * dt_avg * 0.5 * (static_cast<double>(vo[j]) + vnd);
+            wext += static_cast<double>(g + r) * dt_avg * 0.5 * (vod + vnd);
             kin += 0.5 * (vnd * vnd) / im[j];
-            if (!isfinite(vn[j])) bad |= ST_NONFINITE;
+            if (!isfinite(vnd)) bad |= ST_NONFINITE;
         }
         st_row<W>(V + c * np + n0, vn);
+#if ENSC_MIXED_VLO
+        st_row<W>(VL + c * np + n0, ln);
+#endif
         st_row<W>(N.u + c * np + n0, un);
         st_row<W>(N.x + c * np + n0, xn);
     }
@@ -858,6 +1004,61 @@ __global__ void __launch_bounds__(kNodeThreads, ENSC_NODE_MINB_MIXED) k_node_mix
     block_sum_d<kNodeThreads, 2, 2u>(v2, P.node, P.n_node_blocks, blockIdx.x);
 }
 
+
+// The last cycle's acceleration in mixed precision (see k_acceleration in
+// the FP64 stepper): the FP32 force sum, gravity and the FP32 acceleration
+// f M^-1 that the mixed node pass feeds into the velocity update, written
+// as doubles, interleaved xyz per node.
+__global__ void __launch_bounds__(kNodeThreads) k_acceleration_mixed(ElemArrays E, NodeArrays N, Material M,
+                                                                     const Ctl* ctl, double* a_out) {
+    const int64_t np = N.nn_pad, ep = E.ne_pad;
+    const float* __restrict__ fe = static_cast<const float*>(E.fe);
+    const bool grouped = E.slot_major && E.tiles_aligned;
+    const double amp = (M.gravity_on && M.amp_n > 0) ? gravity_amplitude(M.amp, M.amp_n, ctl->time, ctl->dt_i) : 1.0;
+    for (int64_t n = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; n < N.nn;
+         n += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        float f[3] = {0.f, 0.f, 0.f};
+        if (E.slot_major) {
+            const uint32_t msk = grouped ? 0xffu : N.slot_mask[n];
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                if ((msk >> k) & 1u) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) f[c] += fe[(3 * k + c) * np + n];
+                }
+        } else if (N.csr_ptr == nullptr) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const uint32_t el = N.ell[k * np + n];
+                if (el != ENSC_NONE) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) f[c] += fe[(3 * k + c) * ep + el];
+                }
+            }
+        } else {
+            for (int64_t i = N.csr_ptr[n]; i < N.csr_ptr[n + 1]; ++i) {
+                const uint32_t ent = N.csr_ent[i];
+                const int k = static_cast<int>(ent & 7u);
+                const uint32_t el = ent >> 3;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) f[c] += fe[(3 * k + c) * ep + el];
+            }
+        }
+        const double im = N.inv_mass[n];
+        const float im_hi = static_cast<float>(im);
+        const float im_lo = static_cast<float>(im - static_cast<double>(im_hi));
+        const uint32_t code = N.bc[n];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            float a = f[c];
+            if (M.gravity_on) a += static_cast<float>(amp * M.gravity_value * M.gravity_dir[c] / im);
+            const uint32_t cc = (code >> (2 * c)) & 3u;
+            if (cc & 2u) a = 0.f;
+            if ((cc & 1u) && a != 0.f) a = 0.f;
+            a_out[3 * n + c] = static_cast<double>(fmaf(a, im_hi, a * im_lo));
+        }
+    }
+}
 
 // ---- batched instances --------------------------------------------------------
 // Element tiles of kStageTile elements and node tiles of 32 * kNodeGroupMixed
@@ -1066,6 +1267,161 @@ __global__ void __launch_bounds__(kStageTile, ENSC_BATCH_MINB_MIXED) k_element_b
     element_pass_done(T);
 }
 
+// The batched pass with one pipeline per warp (as k_element_mixed_warp):
+// element tiles of 32, each warp filling and consuming its own two stages.
+// A stage holds the tile's rows, its instance descriptor, its StageHdr, the
+// TileInfo the warp writes and the ETileSrc record of the tile the warp
+// visits two tiles later.  A warp's consecutive tiles of one instance form a
+// run whose sums are reduced once into the partial slot of the run's first
+// tile.
+constexpr uint32_t kBWDescOff = kWarpStageBytes;
+constexpr uint32_t kBWHdrOff = kBWDescOff + kDescBytes;
+constexpr uint32_t kBWInfoOff = kBWHdrOff + sizeof(StageHdr);
+constexpr uint32_t kBWNextOff = kBWInfoOff + sizeof(TileInfo);
+constexpr uint32_t kBWStageBytes = (kBWNextOff + sizeof(ETileSrc) + 127) / 128 * 128;
+constexpr int kBatchPipeWarps = ENSC_WARP_PIPE_WARPS;
+constexpr size_t kBWPipeSmem = static_cast<size_t>(kBatchPipeWarps) * (2 * kBWStageBytes + 16);
+
+__device__ __forceinline__ void batch_warp_stage_issue(const BatchTables& T, const ETileSrc& src, int64_t t_next,
+                                                       int64_t ntiles, unsigned char* stage, uint32_t dst,
+                                                       uint32_t bar, int lane) {
+    const bool next = t_next < ntiles;
+    if (lane == 0) {
+        TileInfo* ti = reinterpret_cast<TileInfo*>(stage + kBWInfoOff);
+        ti->slot = src.slot;
+        ti->base = src.base;
+        mbar_arrive_expect_tx(bar, kStageWordRows * kWarpTile * 4u + kWarpTile * 8u + kDescBytes + sizeof(StageHdr) +
+                                       (next ? sizeof(ETileSrc) : 0u));
+    }
+    __syncwarp();
+    fence_proxy_async_smem();  // the warp's reads of this stage come before the copies into it
+    for (int r = lane; r < kStageWordRows + 4; r += 32) {
+        if (r < kStageWordRows) bulk_g2s(dst + r * (kWarpTile * 4u), tile_row(src, r), kWarpTile * 4u, bar);
+        else if (r == kStageWordRows) bulk_g2s(dst + kWarpV0Off, src.vol0, kWarpTile * 8u, bar);
+        else if (r == kStageWordRows + 1) bulk_g2s(dst + kBWDescOff, T.desc + src.slot, kDescBytes, bar);
+        else if (r == kStageWordRows + 2) bulk_g2s(dst + kBWHdrOff, T.sparam + src.slot, sizeof(StageHdr), bar);
+        else if (next) bulk_g2s(dst + kBWNextOff, T.etile_src + t_next, sizeof(ETileSrc), bar);
+    }
+}
+
+__global__ void __launch_bounds__(32 * kBatchPipeWarps, ENSC_WARP_PIPE_MINB) k_element_batch_mixed_warp(BatchTables T) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    unsigned char* wst = smem + static_cast<size_t>(wid) * 2 * kBWStageBytes;
+    const uint32_t stage0 = smem_addr(wst);
+    const uint32_t bar0 = smem_addr(smem + static_cast<size_t>(kBatchPipeWarps) * 2 * kBWStageBytes) + 16u * wid;
+    const int64_t ntiles = T.counts[0];
+    const int64_t wstride = static_cast<int64_t>(gridDim.x) * kBatchPipeWarps;
+    const int64_t w0 = static_cast<int64_t>(blockIdx.x) * kBatchPipeWarps + wid;
+    if (lane == 0) {
+        mbar_init(bar0, 1);
+        mbar_init(bar0 + 8, 1);
+        mbar_init_fence();
+    }
+    __syncwarp();
+    for (int s = 0; s < 2; ++s) {
+        const int64_t t = w0 + s * wstride;
+        if (t < ntiles) {
+            const ETileSrc src = T.etile_src[t];
+            batch_warp_stage_issue(T, src, t + 2 * wstride, ntiles, wst + s * kBWStageBytes,
+                                   stage0 + s * kBWStageBytes, bar0 + 8 * s, lane);
+        }
+    }
+    int run_slot = -1;
+    int64_t run_tile = 0;
+    Ctl* run_ctl = nullptr;
+    bool run_live = false;
+    double ei = 0.0, eh = 0.0, ev = 0.0, dts = DBL_MAX, len = DBL_MAX;
+    int32_t bad = 0;
+    auto flush = [&]() {
+        ei = warp_sum_b(ei);
+        eh = warp_sum_b(eh);
+        ev = warp_sum_b(ev);
+        const unsigned long long dmin = warp_min_u64(ord_bits(dts));
+        const unsigned long long lmin = warp_min_u64(ord_bits(len));
+        bad = static_cast<int32_t>(__reduce_or_sync(0xffffffffu, static_cast<unsigned>(bad)));
+        if (run_live && lane == 0) {
+            double* part = T.etile_part + 3 * run_tile;  // one warp per 32-element tile
+            // one writer per slot and pass: reductions add in cycle order
+            atomicAdd(part + 0, ei);
+            atomicAdd(part + 1, eh);
+            atomicAdd(part + 2, ev);
+            atomicMin(&run_ctl->dts_next, dmin);
+            atomicMin(&run_ctl->len_min, lmin);
+            if (bad) atomicOr(&run_ctl->status, bad);
+        }
+        ei = eh = ev = 0.0;
+        dts = len = DBL_MAX;
+        bad = 0;
+    };
+    bool timed_out = false;
+    int it = 0;
+    int64_t t = w0;
+    for (; t < ntiles; t += wstride, ++it) {
+        const int s = it & 1;
+        const uint32_t bar = bar0 + 8 * s;
+        const bool ok = mbar_wait_bounded(bar, (it >> 1) & 1);
+        if (__any_sync(0xffffffffu, !ok)) {
+            timed_out = true;
+            break;
+        }
+        unsigned char* sb = wst + s * kBWStageBytes;
+        const InstanceDesc& d = *reinterpret_cast<const InstanceDesc*>(sb + kBWDescOff);
+        const StageHdr& h = *reinterpret_cast<const StageHdr*>(sb + kBWHdrOff);
+        const TileInfo& ti = *reinterpret_cast<const TileInfo*>(sb + kBWInfoOff);
+        if (ti.slot != run_slot) {
+            flush();
+            run_slot = ti.slot;
+            run_tile = t;
+            run_ctl = d.ctl;
+            run_live = h.live != 0;
+        }
+        const int64_t e = static_cast<int64_t>(ti.base) + lane;
+        if (run_live && e < d.E.ne) {
+            // arrays copied to registers, material constants read at use
+            const ElemArrays E = d.E;
+            const NodeArrays N = d.N;
+            const Material& M = d.M;
+            const double dt1d = h.dt1;
+            const float dt1 = static_cast<float>(dt1d);
+            const float* st = reinterpret_cast<const float*>(sb);
+            const MixedSrc S{reinterpret_cast<const uint32_t*>(st),
+                             st + 8 * kWarpTile,
+                             reinterpret_cast<const double*>(sb + kWarpV0Off),
+                             st + 44 * kWarpTile,
+                             st + 26 * kWarpTile,
+                             st + 32 * kWarpTile,
+                             st + 45 * kWarpTile,
+                             kWarpTile,
+                             lane};
+            double d1, l1;
+            element_body_mixed<true, false, true>(E, N, M, S, dt1, dt1d, e, d1, l1, ei, eh, ev, bad);
+            dts = fmin(dts, d1);
+            len = fmin(len, l1);
+        }
+        const int64_t tn = t + 2 * wstride;
+        if (tn < ntiles) {
+            const ETileSrc src = *reinterpret_cast<const ETileSrc*>(sb + kBWNextOff);
+            batch_warp_stage_issue(T, src, tn + 2 * wstride, ntiles, sb, stage0 + s * kBWStageBytes, bar, lane);
+        }
+    }
+    if (!timed_out) {
+        flush();
+    } else {
+        // record the failure on the instance whose tile could not be read and
+        // let the copies this warp started land (bounded) before exiting
+        if (lane == 0) {
+            atomicOr(&T.desc[T.etile_inst[t]].ctl->status, ST_TIMEOUT);
+            for (int k = 0; k < 2; ++k) {
+                const int itk = it + k;
+                if (w0 + itk * wstride < ntiles) mbar_wait_bounded(bar0 + 8 * (itk & 1), (itk >> 1) & 1);
+            }
+        }
+        __syncwarp();
+    }
+    element_pass_done(T);
+}
+
 // One warp per node tile.  The tile's instance slot and first node are read
 // two tiles ahead and its NodeView and NodeParam lines prefetched into L1 one
 // tile ahead, so a tile starts on its node rows without waiting on the
@@ -1127,6 +1483,11 @@ __global__ void __launch_bounds__(NT, ENSC_NODE_BATCH_MINB_MIXED * kNodeThreads 
 
 void launch_element_mixed(const ElemArrays& E, const NodeArrays& N, const Material& M, Ctl* ctl, const Partials& P,
                           int grid, bool init, cudaStream_t st) {
+    if (ENSC_WARP_PIPE_MIXED && !init && E.tiles_aligned) {
+        if (M.plastic) k_element_mixed_warp<true><<<grid, 32 * kPipeWarps, kWarpPipeSmem, st>>>(E, N, M, ctl, P);
+        else k_element_mixed_warp<false><<<grid, 32 * kPipeWarps, kWarpPipeSmem, st>>>(E, N, M, ctl, P);
+        return;
+    }
     if (ENSC_STAGED_MIXED && !init && E.tiles_aligned) {
         if (M.plastic) k_element_mixed_staged<true><<<grid, kStageTile, kStageSmem, st>>>(E, N, M, ctl, P);
         else k_element_mixed_staged<false><<<grid, kStageTile, kStageSmem, st>>>(E, N, M, ctl, P);
@@ -1141,6 +1502,12 @@ void launch_element_mixed(const ElemArrays& E, const NodeArrays& N, const Materi
     }
 }
 
+void launch_acceleration_mixed(const ElemArrays& E, const NodeArrays& N, const Material& M, const Ctl* ctl,
+                               double* a_aos, cudaStream_t st) {
+    const int64_t g = (N.nn + kNodeThreads - 1) / kNodeThreads;
+    k_acceleration_mixed<<<static_cast<int>(g < 65535 ? g : 65535), kNodeThreads, 0, st>>>(E, N, M, ctl, a_aos);
+}
+
 void launch_node_mixed(const ElemArrays& E, const NodeArrays& N, const Material& M, Ctl* ctl, const Partials& P,
                        int grid, cudaStream_t st) {
     k_node_mixed<<<grid, kNodeThreads, 0, st>>>(E, N, M, ctl, P);
@@ -1148,6 +1515,19 @@ void launch_node_mixed(const ElemArrays& E, const NodeArrays& N, const Material&
 
 int occupancy_element_mixed(bool plastic) {
     int nb = 0;
+    if (ENSC_WARP_PIPE_MIXED) {
+        cudaFuncSetAttribute(k_element_mixed_warp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(kWarpPipeSmem));
+        cudaFuncSetAttribute(k_element_mixed_warp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(kWarpPipeSmem));
+        if (plastic)
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_mixed_warp<true>, 32 * kPipeWarps,
+                                                          kWarpPipeSmem);
+        else
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_mixed_warp<false>, 32 * kPipeWarps,
+                                                          kWarpPipeSmem);
+        return nb;
+    }
     if (ENSC_STAGED_MIXED) {
         // the staged pass needs more than the default 48 KB of dynamic shared
         // memory; the attribute is set here, on the current device, before
@@ -1175,7 +1555,8 @@ int occupancy_node_mixed() {
 
 
 void launch_element_batch_mixed(const BatchTables& T, int grid, cudaStream_t st) {
-    k_element_batch_mixed<<<grid, kStageTile, kBatchStageSmem, st>>>(T);
+    if (ENSC_WARP_PIPE_BATCH) k_element_batch_mixed_warp<<<grid, 32 * kBatchPipeWarps, kBWPipeSmem, st>>>(T);
+    else k_element_batch_mixed<<<grid, kStageTile, kBatchStageSmem, st>>>(T);
 }
 void launch_node_batch_mixed(const BatchTables& T, int grid, int threads, cudaStream_t st) {
     if (threads == kNodeThreads / 2) k_node_batch_mixed<kNodeThreads / 2><<<grid, threads, 0, st>>>(T);
@@ -1183,6 +1564,13 @@ void launch_node_batch_mixed(const BatchTables& T, int grid, int threads, cudaSt
 }
 int occupancy_element_batch_mixed() {
     int nb = 0;
+    if (ENSC_WARP_PIPE_BATCH) {
+        cudaFuncSetAttribute(k_element_batch_mixed_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(kBWPipeSmem));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_batch_mixed_warp, 32 * kBatchPipeWarps,
+                                                      kBWPipeSmem);
+        return nb;
+    }
     // dynamic shared memory above the default 48 KB: set on the current
     // device before any launch or capture
     cudaFuncSetAttribute(k_element_batch_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1191,7 +1579,10 @@ int occupancy_element_batch_mixed() {
     return nb;
 }
 
-int batch_element_tile(bool mixed_precision) { return mixed_precision ? kStageTile : batch_element_tile_fp64(); }
+int batch_element_tile(bool mixed_precision) {
+    if (mixed_precision) return ENSC_WARP_PIPE_BATCH ? kWarpTile : kStageTile;
+    return batch_element_tile_fp64();
+}
 int batch_node_tile(bool mixed_precision) { return 32 * (mixed_precision ? kNodeGroupMixed : kNodeGroupFp64); }
 int occupancy_node_batch_mixed(int threads) {
     int nb = 0;

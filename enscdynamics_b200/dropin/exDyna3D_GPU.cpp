@@ -1,6 +1,7 @@
 // exDyna3D_GPU: see exDyna3D_GPU.h.
 #include "exDyna3D_GPU.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <stdexcept>
@@ -13,6 +14,9 @@ namespace {
 // Upper bound on the cycles one ensc_step_until call may run; the call
 // returns earlier at the step end, the pause time or an error.
 constexpr int64_t kCycleBound = int64_t(1) << 40;
+// Most cycles enqueued ahead of an output write (ensc_step_until_async's
+// limit is 2^24); the rest of the way runs after the write.
+constexpr int64_t kAheadCycles = int64_t(1) << 20;
 
 }  // namespace
 
@@ -197,6 +201,36 @@ void exDyna3D_GPU::update_strain_measure() {
     }
 }
 
+// The fields of a snapshot into the reference's arrays, then the
+// reference's own output_results() (exDyna3D.cpp:207-336) at the snapshot's
+// time.
+void exDyna3D_GPU::write_snapshot(const ensc_snapshot& sn) {
+    const std::size_t nn = vertices.size(), ne = hexahedron_elements.size();
+    for (std::size_t n = 0; n < nn; ++n)
+        for (int c = 0; c < 3; ++c) vertices[n][c] = sn.x[3 * n + c];
+    std::copy(sn.u, sn.u + 3 * nn, solution_u.data());
+    std::copy(sn.v, sn.v + 3 * nn, solution_v.data());
+    std::copy(sn.a, sn.a + 3 * nn, solution_a.data());
+    std::copy(sn.rf, sn.rf + 3 * nn, solution_rf.data());
+    std::copy(sn.sigma, sn.sigma + 6 * ne, reinterpret_cast<double*>(all_sigma.data()));
+    const Types::Real t = time, d0 = dt_i, d1 = dt_i_1;
+    time = sn.time;
+    dt_i = sn.dt_i;
+    dt_i_1 = sn.dt_i_1;
+    update_strain_measure();
+    output_results();
+    time = t;
+    dt_i = d0;
+    dt_i_1 = d1;
+}
+
+void exDyna3D_GPU::take_report(const ensc_step_report& r) {
+    time = r.time;
+    dt_i = r.dt_i;
+    dt_i_1 = r.dt_i_1;
+    cycles_ += r.cycles;
+}
+
 void exDyna3D_GPU::run() {
     // exDyna3D::run()'s prologue (exDyna3D.cpp:55-67), on the host as there
     init();
@@ -204,35 +238,59 @@ void exDyna3D_GPU::run() {
     calculate_time_interval();
     get_fsiSph_virtualParticles_and_vel(0, 1.0 / 10.0);
     create_device();
+    if (solution_a.size() != static_cast<Eigen::Index>(3 * vertices.size())) solution_a.resize(3 * vertices.size());
     for (std::size_t s = 1; s < steps.size(); ++s) {
         if (s > 1) download_state();  // the step switch acts on the current state
         setCurrentStep(s);
         upload_step_conditions();
         const Types::Real stepEnd = time + steps[s].timePeriod;
+        bool run_cycles = true;
         while (time < stepEnd && time < totalTime) {
-            int64_t max_cycles = kCycleBound;
-            double pause = HUGE_VAL;
-            if (opt_.write_output) {
-                // output is due in the cycle in which time reaches time_output;
-                // when it is due already, that is the next cycle
-                if (!(time < time_output))
-                    max_cycles = 1;
-                else
-                    pause = time_output;
+            if (run_cycles) {
+                int64_t max_cycles = kCycleBound;
+                double pause = HUGE_VAL;
+                if (opt_.write_output) {
+                    // output is due in the cycle in which time reaches time_output;
+                    // when it is due already, that is the next cycle
+                    if (!(time < time_output))
+                        max_cycles = 1;
+                    else
+                        pause = time_output;
+                }
+                ensc_step_report r{};
+                const int rc = ensc_step_until(h_, max_cycles, stepEnd, pause, &r);
+                take_report(r);
+                check(rc, "ensc_step_until");
+                if (r.cycles == 0) break;
             }
-            ensc_step_report r{};
-            const int rc = ensc_step_until(h_, max_cycles, stepEnd, pause, &r);
-            time = r.time;
-            dt_i = r.dt_i;
-            dt_i_1 = r.dt_i_1;
-            cycles_ += r.cycles;
-            check(rc, "ensc_step_until");
+            run_cycles = true;
             if (opt_.write_output && (time >= time_output || time >= totalTime)) {
-                download_state();
-                update_strain_measure();
-                output_results();
+                // capture the fields on the device, let the cycles up to the
+                // next output time run while the copy and the file writing
+                // proceed on the host, then take their report
+                check(ensc_snapshot_begin(h_), "ensc_snapshot_begin");
+                const Types::Real next = time_output + time_interval;  // output_results advances it so
+                bool ahead = false;
+                if (time < stepEnd && time < totalTime && next > time && dt_i > 0.0) {
+                    const double span = std::min<double>(next, stepEnd) - time;
+                    const double est = std::ceil(span / dt_i * 1.02) + 2.0;
+                    const int64_t n = static_cast<int64_t>(std::min(est, static_cast<double>(kAheadCycles)));
+                    check(ensc_step_until_async(h_, n, stepEnd, next), "ensc_step_until_async");
+                    ahead = true;
+                }
+                ensc_snapshot sn{};
+                check(ensc_snapshot_wait(h_, &sn), "ensc_snapshot_wait");
+                write_snapshot(sn);
+                if (ahead) {
+                    ensc_step_report r{};
+                    const int rc = ensc_sync(h_, &r);
+                    take_report(r);
+                    check(rc, "ensc_sync");
+                    // the cycles ran up to the next output time: that output
+                    // is due now, before any further cycle
+                    run_cycles = !(time >= time_output || time >= totalTime);
+                }
             }
-            if (r.cycles == 0) break;
         }
     }
     download_state();

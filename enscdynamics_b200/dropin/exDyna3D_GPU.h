@@ -13,13 +13,20 @@
 // arrays (vertices, solution_u, solution_v, solution_rf, all_sigma, all_QIA,
 // time, dt_i, dt_i_1) at every output time and step end.
 //
+// Output: at an output time the fields are captured on the device
+// (ensc_snapshot_begin) and the cycles up to the next output time are
+// enqueued (ensc_step_until_async) before the host copies and writes them,
+// so the file writing overlaps the stepping.
+//
 // Differences from exDyna3D::run():
 //   * results are written after the cycle in which time reaches the next
 //     output time; the reference writes them from inside that cycle, before
 //     its velocity update (computeSate :788), so the written velocities and
-//     positions are those at the end of the same cycle;
-//   * the written acceleration and nodal-force fields are zero (they stay on
-//     the device); the strain field is recomputed on the host from u;
+//     positions are those at the end of the same cycle (the acceleration is
+//     that cycle's, as the reference writes it);
+//   * the strain field is recomputed on the host from u; the nodal-force
+//     field is zero, as the reference's own solution_f, which it never fills
+//     (exDyna3D.cpp:157,179);
 //   * FSI virtual-particle forces are not applied (none exist unless a
 //     coupled SPH solver provides them);
 //   * a step whose end lies beyond totalTime ends at totalTime (the reference
@@ -70,6 +77,8 @@ protected:
     void upload_step_conditions();
     void download_state();
     void update_strain_measure();
+    void write_snapshot(const ensc_snapshot& sn);
+    void take_report(const ensc_step_report& r);
     void check(int rc, const char* what) const;
 
     Options opt_;

@@ -168,6 +168,43 @@ int ensc_step_until(ensc_handle* h, int64_t max_cycles, double step_end_time, do
 int ensc_step_async(ensc_handle* h, int64_t max_cycles, double step_end_time);
 int ensc_sync(ensc_handle* h, ensc_step_report* report);
 
+/* ensc_step_until without waiting: enqueues up to max_cycles cycles (at most
+ * 2^24) that stop after the cycle in which time reaches pause_time, and
+ * returns at once, so the host can write output while the device steps.
+ * Cycles past the stop are no-ops; ensc_sync (or a later ensc_step_until
+ * with the same limits) completes the call and reports. */
+int ensc_step_until_async(ensc_handle* h, int64_t max_cycles, double step_end_time, double pause_time);
+
+/* ---- output snapshots ----------------------------------------------------
+ * The fields output_results writes at an output time (exDyna3D.cpp:207-336):
+ * vertices, solution_u, solution_v and solution_a (the last cycle's
+ * acceleration, compute_a :642-644: assembled force and gravity with the
+ * acceleration conditions applied, times the inverse mass), the reactions
+ * solution_rf and all_sigma, plus the clock.  ensc_snapshot_begin captures
+ * them on the device in stream order (after the cycles already enqueued)
+ * and copies them to pinned host memory on a second stream, without
+ * waiting: stepping can continue while the copy runs.  ensc_snapshot_wait
+ * waits for the last snapshot begun and points `out` at its host copy, which
+ * stays valid until the second ensc_snapshot_begin after it (two host
+ * buffers are used in turn).  The acceleration is evaluated from the last
+ * force pass's element forces, which ensc_download and ensc_upload_state
+ * overwrite: begin fails with ENSC_ERR_ARG when no cycle ran since them.
+ * (The reference also writes a "force" field, solution_f, which it never
+ * fills, exDyna3D.cpp:157,179,232: it is zero there.) */
+typedef struct {
+    const double* x;        /* [n_nodes*3] vertices */
+    const double* u;        /* [n_nodes*3] solution_u */
+    const double* v;        /* [n_nodes*3] solution_v */
+    const double* a;        /* [n_nodes*3] solution_a of the last cycle */
+    const double* rf;       /* [n_nodes*3] solution_rf */
+    const double* sigma;    /* [n_elements*6] all_sigma */
+    double time, dt_i, dt_i_1;
+    int64_t total_cycles;
+    int32_t status;         /* 0 or the ENSC_ERR_* the device had raised */
+} ensc_snapshot;
+int ensc_snapshot_begin(ensc_handle* h);
+int ensc_snapshot_wait(ensc_handle* h, ensc_snapshot* out);
+
 /* Copies state to host arrays (any pointer may be NULL): x = vertices,
  * u = solution_u, v = solution_v ([n_nodes*3]), sigma = all_sigma
  * ([n_elements*6]), qia = all_QIA ([n_elements*12]), eps_p = equivalent
@@ -282,20 +319,22 @@ const char* ensc_batch_last_error(const ensc_batch* b);
 
 /* ---- stepping without device allocation --------------------------------
  * No counterpart in the reference: the reference stepper never allocates on
- * a GPU.  For callers that cannot call cudaMalloc -- code running inside a
- * stream capture it does not own, plug-ins whose host application owns all
- * device memory, loops with a budget fixed at start-up -- ensc_step_noalloc
- * runs the FP64 cycle on device arrays the caller already owns and keeps its
- * scratch (element-force hand-off, energy partials, control block) in one
- * fixed file-scope device array of about 6.3 MiB that every GPU loading this
- * library holds until exit.  It allocates nothing.  Meshes above the limits
- * below are rejected with ENSC_ERR_ARG; meshes where a node sits in the same
- * local slot of two elements are not supported (node_elem holds one element
- * per slot).  All calls share the scratch and it keeps the last call's
- * contents: each call re-initialises it, but calls that overlap on the GPU
- * race on it.  The first call on a device looks up the scratch address
- * (once per device); make it before any stream capture that should contain
- * later calls.  Messages: ensc_last_error(NULL). */
+ * a GPU.  For callers that may not call cudaMalloc -- plug-ins inside a host
+ * application that owns and budgets all device memory through its own pool,
+ * solver loops whose device memory is fixed at start-up (an allocation can
+ * synchronise the device, and its failure mid-run has no recovery there) --
+ * ensc_step_noalloc runs the FP64 cycle on device arrays the caller already
+ * owns and keeps its scratch (element-force hand-off, energy partials,
+ * control block) in one fixed file-scope device array of about 6.3 MiB that
+ * every GPU loading this library holds until exit.  It allocates nothing.
+ * Meshes above the limits below are rejected with ENSC_ERR_ARG; meshes where
+ * a node sits in the same local slot of two elements are not supported
+ * (node_elem holds one element per slot; build it with a check for such
+ * clashes, as capi.noalloc_node_elem does).  All calls share the scratch and
+ * it keeps the last call's contents: each call re-initialises it, but calls
+ * that overlap on the GPU race on it.  The first call on a device looks up
+ * the scratch address (once per device); make it before any stream capture.
+ * Messages: ensc_last_error(NULL). */
 #define ENSC_NOALLOC_MAX_ELEMENTS 32768
 #define ENSC_NOALLOC_MAX_NODES 262144
 
@@ -319,6 +358,11 @@ typedef struct {
     double* qia;                /* [12][n_elements] in/out */
     double* eps_p;              /* [n_elements] in/out */
     double* rf;                 /* [3][n_nodes] reactions, out */
+    /* gravity amplitude of the step (as ensc_set_gravity_amplitude): in
+     * device memory, gravity_amp_n (time, value) pairs interleaved, or NULL
+     * with gravity_amp_n = 0 for none (factor 1) */
+    const double* gravity_amp;
+    int32_t gravity_amp_n;
 } ensc_device_model;
 
 /* Clock carried between calls (in/out). */
@@ -331,7 +375,11 @@ typedef struct {
 
 /* Runs up to max_cycles FP64 cycles while time < step_end_time, on
  * params->stream (NULL: the legacy default stream) of params->device, and
- * waits for them.  params->precision must be ENSC_FP64. */
+ * waits for them: cycles are launched in batches of 32 and the call returns
+ * after the batch in which the step end is reached or a status stops the run
+ * (so max_cycles may be INT64_MAX with a finite step_end_time).
+ * params->precision must be ENSC_FP64; gravity comes from params and the
+ * model's amplitude table. */
 int ensc_step_noalloc(const ensc_device_model* m, const ensc_material* mat, const ensc_params* params,
                       ensc_noalloc_clock* clk, int64_t max_cycles, double step_end_time);
 

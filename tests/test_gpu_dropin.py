@@ -107,7 +107,25 @@ def test_dropin_writes_results_at_output_times(reference_run):
     import xml.etree.ElementTree as ET
     root = ET.parse(os.path.join(d, files[-1])).getroot()
     piece = root.find("UnstructuredGrid/Piece")
-    assert int(piece.get("NumberOfPoints")) == ref["x"].size // 3
-    assert int(piece.get("NumberOfCells")) == ref["conn"].size // 8
-    names = {a.get("Name") for a in piece.iter("DataArray")}
-    assert {"u", "v", "Stress", "connectivity", "offsets", "types"} <= names
+    nn, ne = ref["x"].size // 3, ref["conn"].size // 8
+    assert int(piece.get("NumberOfPoints")) == nn
+    assert int(piece.get("NumberOfCells")) == ne
+    arrays = {a.get("Name"): a for a in piece.iter("DataArray")}
+    assert {"a", "force", "u", "v", "Stress", "connectivity", "offsets", "types"} <= set(arrays)
+    # the acceleration written is the output cycle's (zero on constrained
+    # DOFs); its bit-exactness is tested through the C ABI (test_gpu_output)
+    assert np.all(np.isfinite(vtu_array(arrays["u"], np.float64)))
+    assert np.array_equal(vtu_array(arrays["connectivity"], np.int64), gpu["conn"].astype(np.int64))
+    a = vtu_array(arrays["a"], np.float64).reshape(nn, 3)
+    code = gpu["bc_code"].reshape(nn, 3)
+    assert np.all(np.isfinite(a)) and np.all(a[code != 0] == 0.0)
+    assert np.abs(a[code == 0]).max() > 0.0
+    assert not np.any(vtu_array(arrays["force"], np.float64))  # the reference never fills solution_f
+
+
+def vtu_array(el, dtype):
+    """Values of an inline base64 DataArray (UInt64 byte-count header)."""
+    import base64
+    raw = base64.b64decode("".join(el.text.split()))
+    n = int(np.frombuffer(raw[:8], dtype=np.uint64)[0])
+    return np.frombuffer(raw[8:8 + n], dtype=dtype)
