@@ -544,6 +544,28 @@ def sweep_leg(args, local, world=1, rank=0, barrier=lambda: None, max_over_ranks
             "speedup_vs_sequential_fp64": batched / seq}
 
 
+def deck_read_leg(elements_per_side=(100, 100, 50)) -> dict:
+    """Deck reading time at the serving stream's largest request size: a
+    500,000-element block deck with per-node initial velocities, read by the
+    reference's DataIn and by DataInFast (ensc_reader_bench, built with the
+    drop-in), which must fill the solver identically."""
+    exe = os.path.join(ROOT, "enscdynamics_b200", "_lib", "ensc_reader_bench")
+    if not os.path.exists(exe):
+        return {"unavailable": "ensc_reader_bench not built (needs the reference sources)"}
+    from enscdynamics_b200 import workloads as W
+    nx, ny, nz = elements_per_side
+    p = W.block(nx, ny, nz, 0.004 * nx, 0.004 * ny, 0.004 * nz, plastic=False)
+    with tempfile.TemporaryDirectory() as d:
+        deck = p.write_deck(d)
+        r = subprocess.run([exe, os.path.join(d, deck), "2"], cwd=d, capture_output=True, text=True, timeout=600)
+    if r.returncode not in (0, 3):
+        return {"unavailable": "ensc_reader_bench failed: " + r.stderr[-300:]}
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    out.pop("deck", None)
+    out["deck"] = f"block {nx}x{ny}x{nz} with per-node initial velocities (best of 2 reads each)"
+    return out
+
+
 def serve_leg(args, local):
     """Serving stream: args.serve_requests Poisson arrivals at 50/s, element
     counts log-uniform in 1k-500k, 1000-10000 cycles, elastic or J2, mixed
@@ -696,6 +718,8 @@ def run_ours(args):
         sweep = sweep_leg(args, local, world, rank, barrier, max_over_ranks, sum_over_ranks)
     if world == 1 and args.serve_requests > 0:
         serve = serve_leg(args, local)
+        if rank == 0:
+            serve["deck_read"] = deck_read_leg()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -33,24 +33,6 @@ constexpr int kNodeUnrollMixed = ENSC_NODE_UNROLL_MIXED;
 #ifndef ENSC_STAGED_MIXED
 #define ENSC_STAGED_MIXED 1
 #endif
-// 1: the single-instance mixed element pass runs one bulk-copy pipeline per
-// warp (k_element_mixed_warp: 32-element tiles, two stages per warp, no
-// block-wide barrier per tile) instead of one per block
-#ifndef ENSC_WARP_PIPE_MIXED
-#define ENSC_WARP_PIPE_MIXED 1
-#endif
-// 1: the batched mixed element pass runs one pipeline per warp too
-// (k_element_batch_mixed_warp, 32-element batch tiles)
-#ifndef ENSC_WARP_PIPE_BATCH
-#define ENSC_WARP_PIPE_BATCH 1
-#endif
-// warps per block and resident blocks per SM of the warp-pipelined passes
-#ifndef ENSC_WARP_PIPE_WARPS
-#define ENSC_WARP_PIPE_WARPS 4
-#endif
-#ifndef ENSC_WARP_PIPE_MINB
-#define ENSC_WARP_PIPE_MINB 4
-#endif
 // elements per stage (= threads per block) and resident blocks per SM of
 // the staged mixed pass; tuned on B200
 #ifndef ENSC_STAGE_TILE_MIXED
@@ -86,7 +68,7 @@ constexpr int kNodeUnrollMixed = ENSC_NODE_UNROLL_MIXED;
 #define ENSC_NODE_ALL_SLOTS 1
 #endif
 #ifndef ENSC_NODE_BATCH_MINB_MIXED
-#define ENSC_NODE_BATCH_MINB_MIXED 3
+#define ENSC_NODE_BATCH_MINB_MIXED 2
 #endif
 // FP64 element pass staged the same way: 0 off, 1 staging all streamed
 // inputs except B0^T (read from global memory), 2 staging B0^T too.
@@ -94,7 +76,10 @@ constexpr int kNodeUnrollMixed = ENSC_NODE_UNROLL_MIXED;
 #define ENSC_STAGED_FP64 2
 #endif
 // 1: the single-instance FP64 element pass runs one bulk-copy pipeline per
-// warp (k_element_fp64_warp), as the mixed one does
+// warp (k_element_fp64_warp: 32-element tiles, two stages per warp, no
+// block-wide barrier per tile) instead of one per block (measured on B200
+// on the block workload: 0.6% faster; the same structure for the mixed
+// passes was 1-3% slower than their per-block pipelines)
 #ifndef ENSC_WARP_PIPE_FP64
 #define ENSC_WARP_PIPE_FP64 1
 #endif
@@ -124,7 +109,7 @@ int occupancy_element_fp64(bool plastic);
 // resident blocks per SM requested for the node passes (register budget
 // 65536 / (256 * minb)); tuned on B200
 #ifndef ENSC_NODE_MINB_MIXED
-#define ENSC_NODE_MINB_MIXED 3
+#define ENSC_NODE_MINB_MIXED 2
 #endif
 #ifndef ENSC_NODE_MINB_FP64
 #define ENSC_NODE_MINB_FP64 4

@@ -649,110 +649,6 @@ __global__ void __launch_bounds__(kStageTile, ENSC_STAGE_MINB_MIXED)
     block_sum_d<kStageTile, 3, 7u>(v3, P.elem, P.n_elem_blocks, blockIdx.x);
 }
 
-// ---- warp-pipelined element pass ---------------------------------------
-// As k_element_mixed_staged, but every warp runs its own pipeline: it walks
-// tiles of 32 consecutive elements (one per lane), fills its own two stages
-// with bulk copies that complete on its own barriers, and reuses a stage as
-// soon as its 32 lanes are done with it.  No warp waits for another warp
-// until the block's final reductions, so a warp held up by its gathers does
-// not stall the others of its block at a per-tile barrier.
-constexpr int kWarpTile = 32;
-constexpr uint32_t kWarpV0Off = kStageWordRows * kWarpTile * 4;
-constexpr uint32_t kWarpStageBytes = kWarpV0Off + kWarpTile * 8;  // 6 KB
-constexpr int kPipeWarps = ENSC_WARP_PIPE_WARPS;
-constexpr size_t kWarpPipeSmem = static_cast<size_t>(kPipeWarps) * (2 * kWarpStageBytes + 16);
-
-template <bool PLASTIC>
-__device__ __forceinline__ void warp_stage_issue(const ElemArrays& E, uint32_t dst, uint32_t bar, int64_t base,
-                                                 int lane) {
-    constexpr int rows = PLASTIC ? kStageWordRows : kStageWordRows - 1;  // eps_p last, J2 only
-    // rows are padded to whole 32-entry tiles: every copy is 128 or 256 bytes
-    if (lane == 0) mbar_arrive_expect_tx(bar, rows * kWarpTile * 4u + kWarpTile * 8u);
-    __syncwarp();
-    fence_proxy_async_smem();  // the warp's reads of this stage come before the copies into it
-    for (int r = lane; r <= rows; r += 32) {
-        if (r < rows) bulk_g2s(dst + r * (kWarpTile * 4u), stage_row(E, r) + base, kWarpTile * 4u, bar);
-        else bulk_g2s(dst + kWarpV0Off, E.vol0 + base, kWarpTile * 8u, bar);
-    }
-}
-
-template <bool PLASTIC>
-__global__ void __launch_bounds__(32 * kPipeWarps, ENSC_WARP_PIPE_MINB)
-    k_element_mixed_warp(ElemArrays E, NodeArrays N, Material M, Ctl* ctl, Partials P) {
-    if (ctl->done) return;
-    extern __shared__ __align__(128) unsigned char smem[];
-    const float dt1 = static_cast<float>(ctl->dt_i_1);
-    const double dt1d = ctl->dt_i_1;
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    // this warp's two stages, then the block's barriers (two per warp)
-    unsigned char* wst = smem + static_cast<size_t>(wid) * 2 * kWarpStageBytes;
-    const uint32_t stage0 = smem_addr(wst);
-    const uint32_t bar0 = smem_addr(smem + static_cast<size_t>(kPipeWarps) * 2 * kWarpStageBytes) + 16u * wid;
-    const int64_t ntiles = (E.ne + kWarpTile - 1) / kWarpTile;
-    const int64_t wstride = static_cast<int64_t>(gridDim.x) * kPipeWarps;
-    const int64_t w0 = static_cast<int64_t>(blockIdx.x) * kPipeWarps + wid;
-    if (lane == 0) {
-        mbar_init(bar0, 1);
-        mbar_init(bar0 + 8, 1);
-        mbar_init_fence();
-    }
-    __syncwarp();
-    for (int s = 0; s < 2; ++s) {
-        const int64_t t = w0 + s * wstride;
-        if (t < ntiles) warp_stage_issue<PLASTIC>(E, stage0 + s * kWarpStageBytes, bar0 + 8 * s, t * kWarpTile, lane);
-    }
-    double e_int = 0.0, e_hg = 0.0, e_vis = 0.0;
-    double dts_min = DBL_MAX, len_min = DBL_MAX;
-    int32_t bad = 0;
-    bool timed_out = false;
-    int it = 0;
-    for (int64_t t = w0; t < ntiles; t += wstride, ++it) {
-        const int s = it & 1;
-        const uint32_t bar = bar0 + 8 * s;
-        const bool ok = mbar_wait_bounded(bar, (it >> 1) & 1);
-        if (__any_sync(0xffffffffu, !ok)) {
-            timed_out = true;
-            break;
-        }
-        const int64_t e = t * kWarpTile + lane;
-        if (e < E.ne) {
-            const float* st = reinterpret_cast<const float*>(wst + s * kWarpStageBytes);
-            const MixedSrc S{reinterpret_cast<const uint32_t*>(st),
-                             st + 8 * kWarpTile,
-                             reinterpret_cast<const double*>(wst + s * kWarpStageBytes + kWarpV0Off),
-                             st + 44 * kWarpTile,
-                             st + 26 * kWarpTile,
-                             st + 32 * kWarpTile,
-                             st + 45 * kWarpTile,
-                             kWarpTile,
-                             lane};
-            double dts, len;
-            element_body_mixed<PLASTIC, false, true, ENSC_MIXED_PREFETCH>(E, N, M, S, dt1, dt1d, e, dts, len, e_int,
-                                                                          e_hg, e_vis, bad);
-            dts_min = fmin(dts_min, dts);
-            len_min = fmin(len_min, len);
-        }
-        const int64_t tn = t + 2 * wstride;
-        if (tn < ntiles) warp_stage_issue<PLASTIC>(E, stage0 + s * kWarpStageBytes, bar, tn * kWarpTile, lane);
-    }
-    if (timed_out) {
-        // record the failure and let the copies this warp started land
-        // (bounded) before the block's shared memory is released
-        if (lane == 0) {
-            atomicOr(&ctl->status, ST_TIMEOUT);
-            for (int k = 0; k < 2; ++k) {
-                const int itk = it + k;
-                if (w0 + itk * wstride < ntiles) mbar_wait_bounded(bar0 + 8 * (itk & 1), (itk >> 1) & 1);
-            }
-        }
-        __syncwarp();
-    }
-    if (bad) atomicOr(&ctl->status, bad);
-    block_min2_d<32 * kPipeWarps>(dts_min, len_min, &ctl->dts_next, &ctl->len_min);
-    double v3[3] = {e_int, e_hg, e_vis};
-    block_sum_d<32 * kPipeWarps, 3, 7u>(v3, P.elem, P.n_elem_blocks, blockIdx.x);
-}
-
 // v + (dt_i + dt_i_1) / 2 * f * M^-1 in FP32 with the half step and the
 // inverse mass as float pairs: both are the same for many nodes and cycles,
 // so their FP32 rounding would scale all accelerations alike.
@@ -1267,161 +1163,6 @@ __global__ void __launch_bounds__(kStageTile, ENSC_BATCH_MINB_MIXED) k_element_b
     element_pass_done(T);
 }
 
-// The batched pass with one pipeline per warp (as k_element_mixed_warp):
-// element tiles of 32, each warp filling and consuming its own two stages.
-// A stage holds the tile's rows, its instance descriptor, its StageHdr, the
-// TileInfo the warp writes and the ETileSrc record of the tile the warp
-// visits two tiles later.  A warp's consecutive tiles of one instance form a
-// run whose sums are reduced once into the partial slot of the run's first
-// tile.
-constexpr uint32_t kBWDescOff = kWarpStageBytes;
-constexpr uint32_t kBWHdrOff = kBWDescOff + kDescBytes;
-constexpr uint32_t kBWInfoOff = kBWHdrOff + sizeof(StageHdr);
-constexpr uint32_t kBWNextOff = kBWInfoOff + sizeof(TileInfo);
-constexpr uint32_t kBWStageBytes = (kBWNextOff + sizeof(ETileSrc) + 127) / 128 * 128;
-constexpr int kBatchPipeWarps = ENSC_WARP_PIPE_WARPS;
-constexpr size_t kBWPipeSmem = static_cast<size_t>(kBatchPipeWarps) * (2 * kBWStageBytes + 16);
-
-__device__ __forceinline__ void batch_warp_stage_issue(const BatchTables& T, const ETileSrc& src, int64_t t_next,
-                                                       int64_t ntiles, unsigned char* stage, uint32_t dst,
-                                                       uint32_t bar, int lane) {
-    const bool next = t_next < ntiles;
-    if (lane == 0) {
-        TileInfo* ti = reinterpret_cast<TileInfo*>(stage + kBWInfoOff);
-        ti->slot = src.slot;
-        ti->base = src.base;
-        mbar_arrive_expect_tx(bar, kStageWordRows * kWarpTile * 4u + kWarpTile * 8u + kDescBytes + sizeof(StageHdr) +
-                                       (next ? sizeof(ETileSrc) : 0u));
-    }
-    __syncwarp();
-    fence_proxy_async_smem();  // the warp's reads of this stage come before the copies into it
-    for (int r = lane; r < kStageWordRows + 4; r += 32) {
-        if (r < kStageWordRows) bulk_g2s(dst + r * (kWarpTile * 4u), tile_row(src, r), kWarpTile * 4u, bar);
-        else if (r == kStageWordRows) bulk_g2s(dst + kWarpV0Off, src.vol0, kWarpTile * 8u, bar);
-        else if (r == kStageWordRows + 1) bulk_g2s(dst + kBWDescOff, T.desc + src.slot, kDescBytes, bar);
-        else if (r == kStageWordRows + 2) bulk_g2s(dst + kBWHdrOff, T.sparam + src.slot, sizeof(StageHdr), bar);
-        else if (next) bulk_g2s(dst + kBWNextOff, T.etile_src + t_next, sizeof(ETileSrc), bar);
-    }
-}
-
-__global__ void __launch_bounds__(32 * kBatchPipeWarps, ENSC_WARP_PIPE_MINB) k_element_batch_mixed_warp(BatchTables T) {
-    extern __shared__ __align__(128) unsigned char smem[];
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    unsigned char* wst = smem + static_cast<size_t>(wid) * 2 * kBWStageBytes;
-    const uint32_t stage0 = smem_addr(wst);
-    const uint32_t bar0 = smem_addr(smem + static_cast<size_t>(kBatchPipeWarps) * 2 * kBWStageBytes) + 16u * wid;
-    const int64_t ntiles = T.counts[0];
-    const int64_t wstride = static_cast<int64_t>(gridDim.x) * kBatchPipeWarps;
-    const int64_t w0 = static_cast<int64_t>(blockIdx.x) * kBatchPipeWarps + wid;
-    if (lane == 0) {
-        mbar_init(bar0, 1);
-        mbar_init(bar0 + 8, 1);
-        mbar_init_fence();
-    }
-    __syncwarp();
-    for (int s = 0; s < 2; ++s) {
-        const int64_t t = w0 + s * wstride;
-        if (t < ntiles) {
-            const ETileSrc src = T.etile_src[t];
-            batch_warp_stage_issue(T, src, t + 2 * wstride, ntiles, wst + s * kBWStageBytes,
-                                   stage0 + s * kBWStageBytes, bar0 + 8 * s, lane);
-        }
-    }
-    int run_slot = -1;
-    int64_t run_tile = 0;
-    Ctl* run_ctl = nullptr;
-    bool run_live = false;
-    double ei = 0.0, eh = 0.0, ev = 0.0, dts = DBL_MAX, len = DBL_MAX;
-    int32_t bad = 0;
-    auto flush = [&]() {
-        ei = warp_sum_b(ei);
-        eh = warp_sum_b(eh);
-        ev = warp_sum_b(ev);
-        const unsigned long long dmin = warp_min_u64(ord_bits(dts));
-        const unsigned long long lmin = warp_min_u64(ord_bits(len));
-        bad = static_cast<int32_t>(__reduce_or_sync(0xffffffffu, static_cast<unsigned>(bad)));
-        if (run_live && lane == 0) {
-            double* part = T.etile_part + 3 * run_tile;  // one warp per 32-element tile
-            // one writer per slot and pass: reductions add in cycle order
-            atomicAdd(part + 0, ei);
-            atomicAdd(part + 1, eh);
-            atomicAdd(part + 2, ev);
-            atomicMin(&run_ctl->dts_next, dmin);
-            atomicMin(&run_ctl->len_min, lmin);
-            if (bad) atomicOr(&run_ctl->status, bad);
-        }
-        ei = eh = ev = 0.0;
-        dts = len = DBL_MAX;
-        bad = 0;
-    };
-    bool timed_out = false;
-    int it = 0;
-    int64_t t = w0;
-    for (; t < ntiles; t += wstride, ++it) {
-        const int s = it & 1;
-        const uint32_t bar = bar0 + 8 * s;
-        const bool ok = mbar_wait_bounded(bar, (it >> 1) & 1);
-        if (__any_sync(0xffffffffu, !ok)) {
-            timed_out = true;
-            break;
-        }
-        unsigned char* sb = wst + s * kBWStageBytes;
-        const InstanceDesc& d = *reinterpret_cast<const InstanceDesc*>(sb + kBWDescOff);
-        const StageHdr& h = *reinterpret_cast<const StageHdr*>(sb + kBWHdrOff);
-        const TileInfo& ti = *reinterpret_cast<const TileInfo*>(sb + kBWInfoOff);
-        if (ti.slot != run_slot) {
-            flush();
-            run_slot = ti.slot;
-            run_tile = t;
-            run_ctl = d.ctl;
-            run_live = h.live != 0;
-        }
-        const int64_t e = static_cast<int64_t>(ti.base) + lane;
-        if (run_live && e < d.E.ne) {
-            // arrays copied to registers, material constants read at use
-            const ElemArrays E = d.E;
-            const NodeArrays N = d.N;
-            const Material& M = d.M;
-            const double dt1d = h.dt1;
-            const float dt1 = static_cast<float>(dt1d);
-            const float* st = reinterpret_cast<const float*>(sb);
-            const MixedSrc S{reinterpret_cast<const uint32_t*>(st),
-                             st + 8 * kWarpTile,
-                             reinterpret_cast<const double*>(sb + kWarpV0Off),
-                             st + 44 * kWarpTile,
-                             st + 26 * kWarpTile,
-                             st + 32 * kWarpTile,
-                             st + 45 * kWarpTile,
-                             kWarpTile,
-                             lane};
-            double d1, l1;
-            element_body_mixed<true, false, true>(E, N, M, S, dt1, dt1d, e, d1, l1, ei, eh, ev, bad);
-            dts = fmin(dts, d1);
-            len = fmin(len, l1);
-        }
-        const int64_t tn = t + 2 * wstride;
-        if (tn < ntiles) {
-            const ETileSrc src = *reinterpret_cast<const ETileSrc*>(sb + kBWNextOff);
-            batch_warp_stage_issue(T, src, tn + 2 * wstride, ntiles, sb, stage0 + s * kBWStageBytes, bar, lane);
-        }
-    }
-    if (!timed_out) {
-        flush();
-    } else {
-        // record the failure on the instance whose tile could not be read and
-        // let the copies this warp started land (bounded) before exiting
-        if (lane == 0) {
-            atomicOr(&T.desc[T.etile_inst[t]].ctl->status, ST_TIMEOUT);
-            for (int k = 0; k < 2; ++k) {
-                const int itk = it + k;
-                if (w0 + itk * wstride < ntiles) mbar_wait_bounded(bar0 + 8 * (itk & 1), (itk >> 1) & 1);
-            }
-        }
-        __syncwarp();
-    }
-    element_pass_done(T);
-}
-
 // One warp per node tile.  The tile's instance slot and first node are read
 // two tiles ahead and its NodeView and NodeParam lines prefetched into L1 one
 // tile ahead, so a tile starts on its node rows without waiting on the
@@ -1483,11 +1224,6 @@ __global__ void __launch_bounds__(NT, ENSC_NODE_BATCH_MINB_MIXED * kNodeThreads 
 
 void launch_element_mixed(const ElemArrays& E, const NodeArrays& N, const Material& M, Ctl* ctl, const Partials& P,
                           int grid, bool init, cudaStream_t st) {
-    if (ENSC_WARP_PIPE_MIXED && !init && E.tiles_aligned) {
-        if (M.plastic) k_element_mixed_warp<true><<<grid, 32 * kPipeWarps, kWarpPipeSmem, st>>>(E, N, M, ctl, P);
-        else k_element_mixed_warp<false><<<grid, 32 * kPipeWarps, kWarpPipeSmem, st>>>(E, N, M, ctl, P);
-        return;
-    }
     if (ENSC_STAGED_MIXED && !init && E.tiles_aligned) {
         if (M.plastic) k_element_mixed_staged<true><<<grid, kStageTile, kStageSmem, st>>>(E, N, M, ctl, P);
         else k_element_mixed_staged<false><<<grid, kStageTile, kStageSmem, st>>>(E, N, M, ctl, P);
@@ -1515,19 +1251,6 @@ void launch_node_mixed(const ElemArrays& E, const NodeArrays& N, const Material&
 
 int occupancy_element_mixed(bool plastic) {
     int nb = 0;
-    if (ENSC_WARP_PIPE_MIXED) {
-        cudaFuncSetAttribute(k_element_mixed_warp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(kWarpPipeSmem));
-        cudaFuncSetAttribute(k_element_mixed_warp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(kWarpPipeSmem));
-        if (plastic)
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_mixed_warp<true>, 32 * kPipeWarps,
-                                                          kWarpPipeSmem);
-        else
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_mixed_warp<false>, 32 * kPipeWarps,
-                                                          kWarpPipeSmem);
-        return nb;
-    }
     if (ENSC_STAGED_MIXED) {
         // the staged pass needs more than the default 48 KB of dynamic shared
         // memory; the attribute is set here, on the current device, before
@@ -1555,8 +1278,7 @@ int occupancy_node_mixed() {
 
 
 void launch_element_batch_mixed(const BatchTables& T, int grid, cudaStream_t st) {
-    if (ENSC_WARP_PIPE_BATCH) k_element_batch_mixed_warp<<<grid, 32 * kBatchPipeWarps, kBWPipeSmem, st>>>(T);
-    else k_element_batch_mixed<<<grid, kStageTile, kBatchStageSmem, st>>>(T);
+    k_element_batch_mixed<<<grid, kStageTile, kBatchStageSmem, st>>>(T);
 }
 void launch_node_batch_mixed(const BatchTables& T, int grid, int threads, cudaStream_t st) {
     if (threads == kNodeThreads / 2) k_node_batch_mixed<kNodeThreads / 2><<<grid, threads, 0, st>>>(T);
@@ -1564,13 +1286,6 @@ void launch_node_batch_mixed(const BatchTables& T, int grid, int threads, cudaSt
 }
 int occupancy_element_batch_mixed() {
     int nb = 0;
-    if (ENSC_WARP_PIPE_BATCH) {
-        cudaFuncSetAttribute(k_element_batch_mixed_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(kBWPipeSmem));
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_batch_mixed_warp, 32 * kBatchPipeWarps,
-                                                      kBWPipeSmem);
-        return nb;
-    }
     // dynamic shared memory above the default 48 KB: set on the current
     // device before any launch or capture
     cudaFuncSetAttribute(k_element_batch_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1579,10 +1294,7 @@ int occupancy_element_batch_mixed() {
     return nb;
 }
 
-int batch_element_tile(bool mixed_precision) {
-    if (mixed_precision) return ENSC_WARP_PIPE_BATCH ? kWarpTile : kStageTile;
-    return batch_element_tile_fp64();
-}
+int batch_element_tile(bool mixed_precision) { return mixed_precision ? kStageTile : batch_element_tile_fp64(); }
 int batch_node_tile(bool mixed_precision) { return 32 * (mixed_precision ? kNodeGroupMixed : kNodeGroupFp64); }
 int occupancy_node_batch_mixed(int threads) {
     int nb = 0;

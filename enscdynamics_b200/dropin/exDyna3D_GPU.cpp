@@ -296,6 +296,105 @@ void exDyna3D_GPU::run() {
     download_state();
 }
 
+namespace {
+
+struct Record {
+    std::string bytes;
+    template <typename T>
+    void pod(const T& v) {
+        bytes.append(reinterpret_cast<const char*>(&v), sizeof(T));
+    }
+    void str(const std::string& s) {
+        pod(static_cast<uint64_t>(s.size()));
+        bytes.append(s);
+    }
+    void sizes(const std::vector<std::size_t>& v) {
+        pod(static_cast<uint64_t>(v.size()));
+        for (std::size_t x : v) pod(static_cast<uint64_t>(x));
+    }
+};
+
+}  // namespace
+
+std::string exDyna3D_GPU::model_record() {
+    Record r;
+    r.pod(static_cast<uint64_t>(vertices.size()));
+    for (const auto& x : vertices) r.pod(x);
+    r.pod(static_cast<uint64_t>(hexahedron_elements.size()));
+    for (auto& el : hexahedron_elements) {
+        r.pod(el.get_PID());
+        r.pod(el.get_MID());
+        const auto& vi = el.get_verticesIndex();
+        r.pod(static_cast<uint64_t>(vi.size()));
+        for (auto v : vi) r.pod(v);
+    }
+    for (const auto* sets : {&map_set_node_list, &map_set_ele_list}) {
+        r.pod(static_cast<uint64_t>(sets->size()));
+        for (const auto& s : *sets) {
+            r.str(s.first);
+            r.sizes(s.second);
+        }
+    }
+    r.pod(static_cast<uint64_t>(map_set_surface_list.size()));
+    for (const auto& s : map_set_surface_list) {
+        r.str(s.first);
+        r.str(s.second.first);
+        r.str(s.second.second);
+    }
+    r.pod(static_cast<uint64_t>(steps.size()));
+    for (const auto& st : steps) {
+        r.str(st.name);
+        r.pod(st.timePeriod);
+        r.pod(st.resetSpcBoundary);
+        r.pod(st.resetVelBoundary);
+        r.pod(st.resetDload);
+        r.pod(st.resetDsload);
+        r.pod(static_cast<uint64_t>(st.boundary.spc_nodes.size()));
+        for (const auto& b : st.boundary.spc_nodes) {
+            r.str(b.first);
+            for (auto v : b.second) r.pod(static_cast<uint64_t>(v));
+        }
+        r.pod(static_cast<uint64_t>(st.boundary.vel_nodes.size()));
+        for (const auto& b : st.boundary.vel_nodes) {
+            r.str(b.first);
+            for (auto v : b.second.first) r.pod(static_cast<uint64_t>(v));
+            r.pod(b.second.second);
+        }
+        r.pod(std::get<0>(st.gravity));
+        if (std::get<0>(st.gravity)) {  // the other fields are set only with gravity on
+            r.str(std::get<1>(st.gravity));
+            r.pod(std::get<2>(st.gravity));
+            r.pod(std::get<3>(st.gravity));
+            r.pod(std::get<4>(st.gravity));
+            r.pod(std::get<5>(st.gravity));
+        }
+        r.pod(static_cast<uint64_t>(st.dsload.size()));
+        for (const auto& d : st.dsload) {
+            r.str(std::get<0>(d));
+            r.str(std::get<1>(d));
+            r.str(std::get<2>(d));
+            r.pod(std::get<3>(d));
+        }
+    }
+    r.pod(static_cast<uint64_t>(ini_vel_generation.size()));
+    for (const auto& iv : ini_vel_generation) {
+        r.str(iv.first);
+        r.pod(static_cast<uint64_t>(iv.second.first));
+        r.pod(iv.second.second);
+    }
+    r.pod(static_cast<uint64_t>(map_amp_list.size()));
+    for (const auto& a : map_amp_list) {
+        r.str(a.first);
+        r.pod(static_cast<uint64_t>(a.second.size()));
+        for (const auto& pt : a.second) r.pod(pt);
+    }
+    for (double v : {mMatElastic.E, mMatElastic.rho, mMatElastic.v, mMatElastic.G, mMatElastic.K, mMatElastic.lambda,
+                     mMatElastic.WOS, Cvisl, Cvisq, totalTime, time_interval})
+        r.pod(v);
+    r.pod(time_interval_set);
+    return r.bytes;
+}
+
 void exDyna3D_GPU::dump_state(const std::string& path) const {
     FILE* f = std::fopen(path.c_str(), "wb");
     if (!f) throw std::runtime_error("cannot open " + path);

@@ -42,6 +42,8 @@
 namespace EnSC {
 
 class exDyna3D_GPU : public exDyna3D {
+    friend class DataInFast;  // the fast deck reader fills the model as DataIn does
+
 public:
     struct Options {
         int32_t precision = ENSC_FP64;   // ENSC_FP64 or ENSC_MIXED
@@ -66,6 +68,14 @@ public:
     void run() override;
 
     int64_t cycles() const { return cycles_; }
+    std::size_t n_vertices() const { return vertices.size(); }
+    std::size_t n_elements() const { return hexahedron_elements.size(); }
+
+    // Everything a deck reader fills in the solver (nodes, elements, sets,
+    // surfaces, steps with their conditions and loads, initial velocities,
+    // amplitudes, material, bulk viscosity, total time, output interval) as
+    // one byte string, for comparing two readers on the same deck.
+    std::string model_record();
 
     // Writes the solver state in the ENSCDMP1 layout (counts, clock and
     // controls, then x, u, v, inverse mass, reactions, sigma, QIA, B0^T, V0,

@@ -6,11 +6,15 @@
 //
 //   ensc_dropin [--precision fp64|mixed] [--device N] [--graph-chunk N]
 //               [--yield S --hardening H] [--no-output] [--dump FILE]
-//               [--log-level LEVEL] [deck.inp]
+//               [--reference-reader] [--log-level LEVEL] [deck.inp]
+//
+// The deck is read with DataInFast (deck_reader.h), which fills the solver
+// as the reference's DataIn does; --reference-reader uses DataIn itself.
 //
 // On success it prints one JSON line: cycles run, final time, dt, and the
 // wall time of run().
 #include "dataIn.h"
+#include "deck_reader.h"
 #include "exDyna3D_GPU.h"
 #include "spdlog/spdlog.h"
 
@@ -37,7 +41,7 @@ std::string deck_from_project() {
 int usage(const char* argv0) {
     std::fprintf(stderr,
                  "usage: %s [--precision fp64|mixed] [--device N] [--graph-chunk N] [--yield S --hardening H] "
-                 "[--no-output] [--dump FILE] [--log-level LEVEL] [deck.inp]\n",
+                 "[--no-output] [--dump FILE] [--reference-reader] [--log-level LEVEL] [deck.inp]\n",
                  argv0);
     return 2;
 }
@@ -48,6 +52,7 @@ int main(int argc, char** argv) {
     EnSC::exDyna3D_GPU::Options opt;
     std::string deck, dump;
     std::string level = "warn";
+    bool reference_reader = false;
     for (int i = 1; i < argc; ++i) {
         const std::string a = argv[i];
         auto next = [&]() -> const char* { return i + 1 < argc ? argv[++i] : nullptr; };
@@ -64,6 +69,8 @@ int main(int argc, char** argv) {
             opt.yield_stress = std::atof(v);
         } else if (a == "--hardening" && (v = next())) {
             opt.hardening_modulus = std::atof(v);
+        } else if (a == "--reference-reader") {
+            reference_reader = true;
         } else if (a == "--no-output") {
             opt.write_output = false;
         } else if (a == "--dump" && (v = next())) {
@@ -84,13 +91,16 @@ int main(int argc, char** argv) {
     }
     try {
         EnSC::exDyna3D_GPU solver(opt);
-        EnSC::DataIn reader(solver);
-        reader.read_inp(deck);
+        const auto tr = std::chrono::steady_clock::now();
+        if (reference_reader) EnSC::DataIn(solver).read_inp(deck);
+        else EnSC::DataInFast(solver).read_inp(deck);
+        const double read_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - tr).count();
         const auto t0 = std::chrono::steady_clock::now();
         solver.run();
         const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         if (!dump.empty()) solver.dump_state(dump);
-        std::printf("{\"cycles\": %lld, \"run_s\": %.6f}\n", static_cast<long long>(solver.cycles()), secs);
+        std::printf("{\"cycles\": %lld, \"read_s\": %.6f, \"run_s\": %.6f}\n", static_cast<long long>(solver.cycles()),
+                    read_s, secs);
     } catch (const std::exception& e) {
         std::fprintf(stderr, "ensc_dropin: %s\n", e.what());
         return 1;

@@ -6,6 +6,7 @@ import os
 import numpy as np
 
 from enscdynamics_b200 import mesh as M
+from enscdynamics_b200 import workloads as W
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
@@ -90,3 +91,25 @@ def run_len(g):
     if meta["mode"] == "full":
         return 10 ** 6, meta["step_end"]
     return meta["cycles"], float("inf")
+
+
+# the two-step deck of the drop-in tests: step periods
+STEP1, STEP2 = 1.2e-3, 0.9e-3
+
+
+def write_two_step_deck(d):
+    p = W.cantilever(8, 2, 2, 0.8, 0.2, 0.2, vz=1.0)
+    tip = M.face_nodes(p.mesh, 0, "max")
+    p.mesh.node_sets["Set-3"] = tip
+    deck = "model.inp"
+    path = os.path.join(d, deck)
+    M.write_deck(path, p.mesh, p.material, period=STEP1, fixed_sets=p.fixed_sets,
+                 initial_velocity=p.initial_velocity, bulk_viscosity=(p.controls.cvisl, p.controls.cvisq),
+                 gravity=(2.0e3, (0.0, 0.0, -1.0)), amplitude=[(0.0, 0.2), (6.0e-4, 1.0), (2.0e-3, 0.5)])
+    with open(path, "a") as f:
+        f.write("*Step, name=Step-2, nlgeom=YES\n*Dynamic, Explicit\n")
+        f.write(f", {STEP2!r}\n")
+        f.write("*Boundary, type=VELOCITY\nSet-3, 3, 3, -0.5\n")
+        f.write("*End Step\n")
+    M.write_project(d, deck, p.controls)
+    return deck

@@ -22,9 +22,7 @@ import sys
 import numpy as np
 import pytest
 
-from _common import REL_TOL_REFERENCE, rel
-from enscdynamics_b200 import mesh as M
-from enscdynamics_b200 import workloads as W
+from _common import REL_TOL_REFERENCE, STEP1, STEP2, rel, write_two_step_deck
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -35,27 +33,6 @@ DROPIN = os.path.join(ROOT, "enscdynamics_b200", "_lib", "ensc_dropin")
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not (os.path.exists(DROPIN) and pyoracle.harness_available()),
                                  reason="drop-in or reference harness not built (needs the reference sources)")]
-
-STEP1, STEP2 = 1.2e-3, 0.9e-3
-
-
-def write_two_step_deck(d):
-    p = W.cantilever(8, 2, 2, 0.8, 0.2, 0.2, vz=1.0)
-    tip = M.face_nodes(p.mesh, 0, "max")
-    p.mesh.node_sets["Set-3"] = tip
-    deck = "model.inp"
-    path = os.path.join(d, deck)
-    M.write_deck(path, p.mesh, p.material, period=STEP1, fixed_sets=p.fixed_sets,
-                 initial_velocity=p.initial_velocity, bulk_viscosity=(p.controls.cvisl, p.controls.cvisq),
-                 gravity=(2.0e3, (0.0, 0.0, -1.0)), amplitude=[(0.0, 0.2), (6.0e-4, 1.0), (2.0e-3, 0.5)])
-    with open(path, "a") as f:
-        f.write("*Step, name=Step-2, nlgeom=YES\n*Dynamic, Explicit\n")
-        f.write(f", {STEP2!r}\n")
-        f.write("*Boundary, type=VELOCITY\nSet-3, 3, 3, -0.5\n")
-        f.write("*End Step\n")
-    M.write_project(d, deck, p.controls)
-    return deck
-
 
 def run_dropin(d, deck, *args):
     out = subprocess.run([DROPIN, *args, "--dump", os.path.join(d, "gpu.bin"), deck], cwd=d,
@@ -115,7 +92,7 @@ def test_dropin_writes_results_at_output_times(reference_run):
     # the acceleration written is the output cycle's (zero on constrained
     # DOFs); its bit-exactness is tested through the C ABI (test_gpu_output)
     assert np.all(np.isfinite(vtu_array(arrays["u"], np.float64)))
-    assert np.array_equal(vtu_array(arrays["connectivity"], np.int64), gpu["conn"].astype(np.int64))
+    assert np.array_equal(vtu_array(arrays["connectivity"], np.int64), gpu["conn"].astype(np.int64).reshape(-1))
     a = vtu_array(arrays["a"], np.float64).reshape(nn, 3)
     code = gpu["bc_code"].reshape(nn, 3)
     assert np.all(np.isfinite(a)) and np.all(a[code != 0] == 0.0)
