@@ -175,18 +175,19 @@ def node_pass_bytes(ne: int, nn: int, mixed: bool = False) -> int:
     """Algorithmic bytes of one node-pass launch: the element forces (24
     components per element, each read once: 192 B FP64, 96 B mixed), and per
     node the inverse mass 8, BC code 1, x and u read and write 96, v read and
-    write (48 FP64, 24 mixed).  Reactions and prescribed velocities are
-    touched only at constrained nodes and not counted; force slots that no
-    element fills (boundary nodes) are read as zeros but not counted."""
+    write (48 FP64; mixed: 24 for the float rows and 12 for their 16-bit
+    residual rows).  Reactions and prescribed velocities are touched only at
+    constrained nodes and not counted; force slots that no element fills
+    (boundary nodes) are read as zeros but not counted."""
     if mixed:
-        return ne * 96 + nn * (8 + 1 + 96 + 24)
+        return ne * 96 + nn * (8 + 1 + 96 + 24 + 12)
     return ne * 192 + nn * (8 + 1 + 96 + 48)
 
 
 def cycle_bytes(ne: int, nn: int, plastic: bool, mixed: bool = False) -> int:
     """Canonical algorithmic bytes of one cycle (element pass + node pass):
     FP64 904 B per element (+16 with J2) and 225 B per node; mixed 452 B per
-    element (+8) and 165 B per node."""
+    element (+8) and 177 B per node."""
     return element_pass_bytes(ne, nn, plastic, mixed) + node_pass_bytes(ne, nn, mixed)
 
 

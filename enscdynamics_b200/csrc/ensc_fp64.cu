@@ -755,17 +755,21 @@ __global__ void __launch_bounds__(kNodeThreads) k_acceleration(ElemArrays E, Nod
 // no block-wide barrier per tile.  element_body's arithmetic, so results are
 // bit-identical to the other FP64 element passes.
 constexpr int kF64WarpTile = 32;
-constexpr uint32_t kF64WarpStageBytes = 8u * kF64WarpTile * 4u + (kF64StageRows + 24) * kF64WarpTile * 8u;
+// B0^T staged with the other rows (1) or read from global memory through L1
+// (0, a smaller stage: more warps fit in shared memory)
+constexpr bool kF64WarpBt = ENSC_F64_WARP_BT != 0;
+constexpr uint32_t kF64WarpStageBytes =
+    8u * kF64WarpTile * 4u + (kF64StageRows + (kF64WarpBt ? 24 : 0)) * kF64WarpTile * 8u;
 constexpr int kF64PipeWarps = ENSC_F64_PIPE_WARPS;
 constexpr size_t kF64WarpPipeSmem = static_cast<size_t>(kF64PipeWarps) * (2 * kF64WarpStageBytes + 16);
 
 template <bool PLASTIC>
 __device__ __forceinline__ void f64_warp_stage_issue(const ElemArrays& E, uint32_t dst, uint32_t bar, int64_t base,
                                                      int lane) {
-    constexpr int drows = kF64StageRows + 24;
+    constexpr int drows = kF64StageRows + (kF64WarpBt ? 24 : 0);
     // whole 32-entry tiles of rows padded to multiples of 32: 128- and
     // 256-byte copies
-    if (lane == 0) mbar_arrive_expect_tx(bar, f64_stage_tx_bytes<PLASTIC, true>(kF64WarpTile));
+    if (lane == 0) mbar_arrive_expect_tx(bar, f64_stage_tx_bytes<PLASTIC, kF64WarpBt>(kF64WarpTile));
     __syncwarp();
     fence_proxy_async_smem();  // the warp's reads of this stage come before the copies into it
     const uint32_t dbase = dst + 8u * kF64WarpTile * 4u;
@@ -822,10 +826,12 @@ __global__ void __launch_bounds__(32 * kF64PipeWarps, ENSC_F64_PIPE_MINB)
             const unsigned char* st = wst + s * kF64WarpStageBytes;
             const double* d = reinterpret_cast<const double*>(st + 8 * T * 4);
             const Fp64Src S{reinterpret_cast<const uint32_t*>(st), d, d + 6 * T, d + 18 * T, d + 19 * T, d + 20 * T,
-                            d + 21 * T, T, lane, d + kF64StageRows * T, static_cast<int64_t>(T),
-                            static_cast<int64_t>(lane)};
+                            d + 21 * T, T, lane,
+                            kF64WarpBt ? d + kF64StageRows * T : static_cast<const double*>(E.bt),
+                            kF64WarpBt ? static_cast<int64_t>(T) : E.ne_pad,
+                            kF64WarpBt ? static_cast<int64_t>(lane) : e};
             double dts, len;
-            element_body<PLASTIC, false, true, true>(E, N, M, S, dt1, e, dts, len, e_int, e_hg, e_vis, bad);
+            element_body<PLASTIC, false, true, kF64WarpBt>(E, N, M, S, dt1, e, dts, len, e_int, e_hg, e_vis, bad);
             dts_min = dts < dts_min ? dts : dts_min;
             len_min = len < len_min ? len : len_min;
         }

@@ -86,6 +86,10 @@ constexpr int kNodeUnrollMixed = ENSC_NODE_UNROLL_MIXED;
 #ifndef ENSC_F64_PIPE_WARPS
 #define ENSC_F64_PIPE_WARPS 4
 #endif
+// 1: the warp-pipelined FP64 pass stages B0^T too; 0: reads it through L1
+#ifndef ENSC_F64_WARP_BT
+#define ENSC_F64_WARP_BT 1
+#endif
 #ifndef ENSC_F64_PIPE_MINB
 #define ENSC_F64_PIPE_MINB 2
 #endif
