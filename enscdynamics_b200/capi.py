@@ -132,6 +132,11 @@ SIGNATURES = [
                                     C.POINTER(C.c_void_p)]),
     ("ensc_batch_add", C.c_int, [C.c_void_p, C.POINTER(MeshDesc), C.POINTER(MaterialDesc), C.POINTER(Params),
                                  C.POINTER(C.c_int32)]),
+    ("ensc_batch_prepare", C.c_int, [C.POINTER(MeshDesc), C.POINTER(MaterialDesc), C.c_int32,
+                                     C.POINTER(C.c_void_p)]),
+    ("ensc_batch_add_prepared", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(Params), C.POINTER(C.c_int32)]),
+    ("ensc_prepared_bytes", C.c_int64, [C.c_void_p]),
+    ("ensc_prepared_destroy", None, [C.c_void_p]),
     ("ensc_batch_set_bcs", C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int8), _P]),
     ("ensc_batch_set_gravity_amplitude", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, _P]),
     ("ensc_batch_arm", C.c_int, [C.c_void_p, C.c_int32, C.c_int64, C.c_double]),
@@ -351,6 +356,45 @@ class Stepper:
         return int(self._lib.ensc_kernels_per_cycle(self.h))
 
 
+class Prepared:
+    """An instance prepared on the host for Batch.add_prepared
+    (ensc_batch_prepare): element constants, lumped mass and node tables.
+    Holds the arrays the device part reads again.  The work runs in the C
+    library without the interpreter lock, so several requests can be
+    prepared on threads while a batch steps."""
+
+    def __init__(self, x0: np.ndarray, conn: np.ndarray, v0: Optional[np.ndarray] = None, *,
+                 material: _mesh.Material, controls: _mesh.Controls, precision: int = MIXED):
+        lib = load()
+        self._lib = lib
+        self.h = C.c_void_p()
+        keep, m, mt, p = _descriptors(x0, conn, v0, material, controls)
+        rc = lib.ensc_batch_prepare(C.byref(m), C.byref(mt), int(precision), C.byref(self.h))
+        if rc != 0:
+            raise EnscError(rc, lib.ensc_last_error(None).decode())
+        self._keep = keep
+        self.controls = controls
+        self._params = p
+        self.precision = precision
+        self.sizes = (int(x0.shape[0]), int(conn.shape[0]))
+
+    @property
+    def device_bytes(self) -> int:
+        return int(self._lib.ensc_prepared_bytes(self.h))
+
+    def close(self) -> None:
+        if self.h:
+            self._lib.ensc_prepared_destroy(self.h)
+            self.h = C.c_void_p()
+            self._keep = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Batch:
     """Many independent solver instances stepped together (ensc_batch_* ABI).
 
@@ -406,6 +450,16 @@ class Batch:
         self.sizes[slot.value] = (int(x0.shape[0]), int(conn.shape[0]))
         if controls.gravity_amplitude:
             self.set_gravity_amplitude(slot.value, controls.gravity_amplitude)
+        return slot.value
+
+    def add_prepared(self, prep: Prepared) -> int:
+        """Adds an instance prepared by Prepared (ensc_batch_add_prepared);
+        the Prepared object may be closed afterwards."""
+        slot = C.c_int32(-1)
+        self._check(self._lib.ensc_batch_add_prepared(self.h, prep.h, C.byref(prep._params), C.byref(slot)))
+        self.sizes[slot.value] = prep.sizes
+        if prep.controls.gravity_amplitude:
+            self.set_gravity_amplitude(slot.value, prep.controls.gravity_amplitude)
         return slot.value
 
     def set_gravity_amplitude(self, slot: int, points) -> None:

@@ -20,6 +20,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -77,14 +78,29 @@ struct ensc_batch {
     std::vector<Slot> inst;
     ensc::BatchTables T{};
     bool dirty = true;
+    ensc::InstanceDesc h_desc_off{};  // host copy of a removed slot's table entry
     int64_t n_etiles = 0, n_ntiles = 0;
     int sms = 148, occ_e = 1, occ_pre = 4;
     Tune tune;
     int fixed_chunk = 0;  // cycles per graph launch given by the caller (0: tuned)
     bool tuned = false;
+    // tuning in progress: next candidate, best time per cycle and its choice;
+    // element tiles of the batch the last tuning measured
+    int tune_next = 0;
+    float tune_best = 1e30f;
+    Tune tune_pick;
+    int64_t tune_etiles = 0;
+    int tunings = 0;  // completed tunings
     cudaGraphExec_t graph = nullptr;
     int graph_chunk = 0, graph_ge = 0, graph_gn = 0, graph_nt = 0;
     std::string err;
+};
+
+// An instance prepared on the host (ensc_batch_prepare).
+struct ensc_prepared {
+    ensc::InstanceHost ih;
+    int32_t precision = ENSC_MIXED;
+    ensc_material mat{};
 };
 
 namespace {
@@ -248,43 +264,73 @@ int build_graph(ensc_batch* b, const Tune& t) {
 }
 
 // Picks the launch geometry (grid sizes, node-pass block size) and graph
-// length with the shortest time per cycle on the batch as loaded.  The candidates differ only in how work is
-// spread over the GPU, not in arithmetic, so the cycles they run are ordinary
-// cycles of the solve (results are identical whichever wins).
-int autotune(ensc_batch* b, int64_t* cycles_left) {
+// length with the shortest time per cycle on the batch as loaded.  The
+// candidates differ only in how work is spread over the GPU, not in
+// arithmetic, so the cycles they run are ordinary cycles of the solve
+// (results are identical whichever wins).  Each candidate runs one warm-up
+// graph launch and one timed launch; a run too short for the next candidate
+// continues with the best so far, and the next run goes on from there.
+constexpr int kTuneCands = 7;
+Tune tune_candidate(int i) {
     constexpr int kN = ensc::kNodeThreads;
-    const Tune cand[] = {{1, 1, 32, kN},     {2, 1, 32, kN}, {1, 2, 32, kN},     {2, 2, 32, kN},
-                         {1, 1, 32, kN / 2}, {1, 2, 32, kN / 2}, {1, 1, 8, kN}};
+    const Tune cand[kTuneCands] = {{1, 1, 32, kN},     {2, 1, 32, kN},     {1, 2, 32, kN}, {2, 2, 32, kN},
+                                   {1, 1, 32, kN / 2}, {1, 2, 32, kN / 2}, {1, 1, 8, kN}};
+    return cand[i];
+}
+
+int autotune(ensc_batch* b, int64_t* cycles_left) {
     cudaEvent_t e0, e1;
     BCK(b, cudaEventCreate(&e0));
     BCK(b, cudaEventCreate(&e1));
-    float best = 1e30f;
-    Tune bt = b->tune;
-    for (Tune t : cand) {
+    int rc = ENSC_OK;
+    for (; b->tune_next < kTuneCands; ++b->tune_next) {
+        Tune t = tune_candidate(b->tune_next);
         if (b->fixed_chunk > 0) t.chunk = b->fixed_chunk;
-        if (*cycles_left < 3 * t.chunk) break;
-        int rc = build_graph(b, t);
-        if (rc) return rc;
-        BCK(b, cudaGraphLaunch(b->graph, b->stream));  // warm-up
-        BCK(b, cudaEventRecord(e0, b->stream));
-        BCK(b, cudaGraphLaunch(b->graph, b->stream));
-        BCK(b, cudaGraphLaunch(b->graph, b->stream));
-        BCK(b, cudaEventRecord(e1, b->stream));
-        BCK(b, cudaEventSynchronize(e1));
+        if (*cycles_left < 2 * t.chunk) break;
+        rc = build_graph(b, t);
+        if (rc) break;
+        cudaError_t e = cudaGraphLaunch(b->graph, b->stream);  // warm-up
+        if (e == cudaSuccess) e = cudaEventRecord(e0, b->stream);
+        if (e == cudaSuccess) e = cudaGraphLaunch(b->graph, b->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(e1, b->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) {
+            rc = bcuda(b, "autotune", e);
+            break;
+        }
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e0, e1);
-        const float per = ms / (2.f * t.chunk);
-        if (per < best) {
-            best = per;
-            bt = t;
+        const float per = ms / static_cast<float>(t.chunk);
+        if (per < b->tune_best) {
+            b->tune_best = per;
+            b->tune_pick = t;
         }
-        *cycles_left -= 3 * t.chunk;
+        *cycles_left -= 2 * t.chunk;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    b->tune = bt;
-    b->tuned = true;
-    return build_graph(b, bt);
+    if (rc) return rc;
+    if (b->tune_next == kTuneCands) {
+        b->tune = b->tune_pick;
+        b->tuned = true;
+        b->tunings += 1;
+        b->tune_etiles = b->n_etiles;
+    } else if (b->tune_best < 1e30f) {
+        b->tune = b->tune_pick;
+    }
+    if (b->fixed_chunk > 0) b->tune.chunk = b->fixed_chunk;
+    return build_graph(b, b->tune);
+}
+
+// Starts a new tuning when the batch's element tiles have grown or shrunk
+// four-fold since the last one (a stream of arrivals and retirements).
+void retune_if_reshaped(ensc_batch* b) {
+    if (!b->tuned || b->tune_etiles <= 0) return;
+    if (b->n_etiles > 4 * b->tune_etiles || 4 * b->n_etiles < b->tune_etiles) {
+        b->tuned = false;
+        b->tune_next = 0;
+        b->tune_best = 1e30f;
+    }
 }
 
 }  // namespace
@@ -414,10 +460,50 @@ int ensc_batch_create(const ensc_params* params, int32_t max_instances, int64_t 
     return ENSC_OK;
 }
 
+int ensc_batch_prepare(const ensc_mesh_desc* mesh, const ensc_material* mat, int32_t precision, ensc_prepared** out) {
+    if (!out) return berr(nullptr, ENSC_ERR_ARG, "out is required");
+    *out = nullptr;
+    if (precision != ENSC_FP64 && precision != ENSC_MIXED) return berr(nullptr, ENSC_ERR_ARG, "unknown precision");
+    if (!mesh || !mat) return berr(nullptr, ENSC_ERR_ARG, "mesh and material are required");
+    ensc_prepared* p = new (std::nothrow) ensc_prepared;
+    if (!p) return berr(nullptr, ENSC_ERR_OOM, "host allocation failed");
+    std::string perr;
+    int rc;
+    try {
+        rc = ensc::instance_prepare(mesh, mat, precision == ENSC_MIXED, p->ih, perr);
+    } catch (const std::bad_alloc&) {
+        rc = ENSC_ERR_OOM;
+        perr = "host allocation failed";
+    }
+    if (rc) {
+        delete p;
+        return berr(nullptr, rc, perr);
+    }
+    p->precision = precision;
+    p->mat = *mat;
+    *out = p;
+    return ENSC_OK;
+}
+
+int64_t ensc_prepared_bytes(const ensc_prepared* prep) { return prep ? static_cast<int64_t>(prep->ih.bytes) : 0; }
+
+void ensc_prepared_destroy(ensc_prepared* prep) { delete prep; }
+
 int ensc_batch_add(ensc_batch* b, const ensc_mesh_desc* mesh, const ensc_material* mat, const ensc_params* controls,
                    int32_t* slot_out) {
     if (!b || !mesh || !mat || !controls || !slot_out) return berr(b, ENSC_ERR_ARG, "missing argument");
+    ensc_prepared* p = nullptr;
+    int rc = ensc_batch_prepare(mesh, mat, b->precision, &p);
+    if (rc) return berr(b, rc, ensc_last_error(nullptr));
+    rc = ensc_batch_add_prepared(b, p, controls, slot_out);
+    ensc_prepared_destroy(p);
+    return rc;
+}
+
+int ensc_batch_add_prepared(ensc_batch* b, const ensc_prepared* prep, const ensc_params* controls, int32_t* slot_out) {
+    if (!b || !prep || !controls || !slot_out) return berr(b, ENSC_ERR_ARG, "missing argument");
     if (!(controls->factor_timestep > 0.0)) return berr(b, ENSC_ERR_ARG, "factor_timestep must be > 0");
+    if (prep->precision != b->precision) return berr(b, ENSC_ERR_ARG, "instance prepared for another precision");
     DevGuard dg(b->device);
     int s = -1;
     for (int i = 0; i < b->slots; ++i)
@@ -426,10 +512,9 @@ int ensc_batch_add(ensc_batch* b, const ensc_mesh_desc* mesh, const ensc_materia
             break;
         }
     if (s < 0) return berr(b, ENSC_ERR_OOM, "no free instance slot");
-    ensc::InstanceHost ih;
-    std::string perr;
-    int rc = ensc::instance_prepare(mesh, mat, is_mixed(b), ih, perr);
-    if (rc) return berr(b, rc, perr);
+    const ensc::InstanceHost& ih = prep->ih;
+    const ensc_material* mat = &prep->mat;
+    int rc;
     if (b->used + static_cast<int64_t>(ih.bytes) > b->budget)
         return berr(b, ENSC_ERR_OOM, "instance does not fit the batch's memory budget");
     const int64_t et = (ih.ne + b->etile - 1) / b->etile, nt = (ih.nn + b->ntile - 1) / b->ntile;
@@ -438,6 +523,7 @@ int ensc_batch_add(ensc_batch* b, const ensc_mesh_desc* mesh, const ensc_materia
     Slot& sl = b->inst[s];
     void* block = nullptr;
     BCK(b, cudaMallocFromPoolAsync(&block, ih.bytes, b->pool, b->stream));
+    std::string perr;
     rc = ensc::instance_upload(ih, block, b->stream, sl.E, sl.N, perr);
     if (rc) {
         cudaFreeAsync(block, b->stream);
@@ -474,8 +560,7 @@ int ensc_batch_add(ensc_batch* b, const ensc_mesh_desc* mesh, const ensc_materia
     BCK(b, cudaMemcpyAsync(b->d_ctl + s, b->h_ctl + s, sizeof(Ctl), cudaMemcpyHostToDevice, b->stream));
     sl.used = true;
     b->used += static_cast<int64_t>(ih.bytes);
-    rc = rebuild_tables(b);
-    if (rc) return rc;
+    b->dirty = true;  // the tables are rewritten before the next run
     *slot_out = s;
     return ENSC_OK;
 }
@@ -531,7 +616,8 @@ int ensc_batch_set_gravity_amplitude(ensc_batch* b, int32_t slot, int32_t n_poin
                                b->stream));
     sl.M.amp = n_points > 0 ? sl.amp : nullptr;
     sl.M.amp_n = n_points;
-    return rebuild_tables(b);  // the instance table carries the material by value
+    b->dirty = true;  // the instance table carries the material by value
+    return ENSC_OK;
 }
 
 int ensc_batch_arm(ensc_batch* b, int32_t slot, int64_t max_cycles, double step_end_time) {
@@ -551,6 +637,7 @@ int ensc_batch_run(ensc_batch* b, int64_t cycles) {
         int rc = rebuild_tables(b);
         if (rc) return rc;
     }
+    retune_if_reshaped(b);
     int64_t left = cycles;
     if (!b->tuned) {
         int rc = autotune(b, &left);
@@ -647,12 +734,23 @@ int ensc_batch_remove(ensc_batch* b, int32_t slot) {
     if (!b || slot < 0 || slot >= b->slots || !b->inst[slot].used) return berr(b, ENSC_ERR_ARG, "bad slot");
     DevGuard dg(b->device);
     Slot& sl = b->inst[slot];
+    // fold what the instance's tiles still hold (the tables list them until
+    // the next run rewrites them), then take it out of the device table so
+    // that folds before that rewrite skip the slot, whoever takes it next
+    ensc::launch_between_batch(b->T, b->slots, 1, b->stream);
+    BCK(b, cudaGetLastError());
+    b->h_desc_off = ensc::InstanceDesc{};
+    b->h_desc_off.ctl = b->d_ctl + slot;
+    BCK(b, cudaMemcpyAsync(b->d_desc + slot, &b->h_desc_off, sizeof(ensc::InstanceDesc), cudaMemcpyHostToDevice,
+                           b->stream));
     // the slot idles from now on; its block returns to the pool in stream order
     b->h_ctl[slot] = Ctl{};
     b->h_ctl[slot].done = 1;
     BCK(b, cudaMemcpyAsync(b->d_ctl + slot, b->h_ctl + slot, sizeof(Ctl), cudaMemcpyHostToDevice, b->stream));
+    BCK(b, cudaStreamSynchronize(b->stream));  // the copies above read host memory
     sl.used = false;
-    int rc = rebuild_tables(b);
+    b->dirty = true;
+    const int rc = ENSC_OK;
     if (sl.amp) BCK(b, cudaFreeAsync(sl.amp, b->stream));
     BCK(b, cudaFreeAsync(sl.block, b->stream));
     b->used -= static_cast<int64_t>(sl.bytes);
@@ -665,7 +763,7 @@ int64_t ensc_batch_device_bytes(const ensc_batch* b) { return b ? b->used : 0; }
 int ensc_batch_tuning(const ensc_batch* b, int32_t* mult_element, int32_t* mult_node, int32_t* graph_cycles,
                       int32_t* node_threads) {
     if (!b) return ENSC_ERR_ARG;
-    const bool t = b->tuned;
+    const bool t = b->tunings > 0;
     if (mult_element) *mult_element = t ? b->tune.mult_e : 0;
     if (mult_node) *mult_node = t ? b->tune.mult_n : 0;
     if (graph_cycles) *graph_cycles = t ? b->tune.chunk : 0;

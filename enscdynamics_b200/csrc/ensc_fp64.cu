@@ -154,8 +154,10 @@ __device__ __forceinline__ Fp64Src fp64_src_global(const ElemArrays& E, int64_t 
 // reference mapping), shared by the single-instance, staged and batched
 // kernels; inputs come from S, outputs go to the instance's arrays at
 // element e.  SMEM / BT_SMEM: S's rows / B0^T rows
-// are in shared memory.
-template <bool PLASTIC, bool INIT, bool SMEM = false, bool BT_SMEM = false>
+// are in shared memory.  PF: node rows the body reads later are prefetched
+// into L1 once the connectivity is known (bit 0 the velocities, bit 1 the
+// displacements).
+template <bool PLASTIC, bool INIT, bool SMEM = false, bool BT_SMEM = false, int PF = 0>
 __device__ __forceinline__ void element_body(const ElemArrays& E, const NodeArrays& N, const Material& M,
                                              const Fp64Src& S, const double dt1, const int64_t e, double& dts,
                                              double& len, double& e_int, double& e_hg, double& e_vis,
@@ -175,6 +177,18 @@ __device__ __forceinline__ void element_body(const ElemArrays& E, const NodeArra
     uint32_t n[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) n[k] = ldin<SMEM>(S.conn + k * ss + si);
+    if (PF & 1) {
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int k = 0; k < 8; ++k) prefetch_l1(V + r * np + n[k]);
+    }
+    if (PF & 2) {
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int k = 0; k < 8; ++k) prefetch_l1(U + r * np + n[k]);
+    }
     // current coordinates: hourglass projections TAU x (exact, the
     // Gamma entries are +-1) and the minimum edge (min_ele_edge :1173-1220)
     double TX[4][3];
@@ -831,7 +845,8 @@ __global__ void __launch_bounds__(32 * kF64PipeWarps, ENSC_F64_PIPE_MINB)
                             kF64WarpBt ? static_cast<int64_t>(T) : E.ne_pad,
                             kF64WarpBt ? static_cast<int64_t>(lane) : e};
             double dts, len;
-            element_body<PLASTIC, false, true, kF64WarpBt>(E, N, M, S, dt1, e, dts, len, e_int, e_hg, e_vis, bad);
+            element_body<PLASTIC, false, true, kF64WarpBt, ENSC_F64_PREFETCH>(E, N, M, S, dt1, e, dts, len, e_int,
+                                                                              e_hg, e_vis, bad);
             dts_min = dts < dts_min ? dts : dts_min;
             len_min = len < len_min ? len : len_min;
         }
@@ -1154,7 +1169,7 @@ __global__ void __launch_bounds__(kStageTileF64, kStageMinbF64) k_element_batch_
             const Fp64Src S{reinterpret_cast<const uint32_t*>(st), dr, dr + 6 * TT, dr + 18 * TT, dr + 19 * TT,
                             dr + 20 * TT, dr + 21 * TT, TT, tid, dr + kF64StageRows * TT, TT, tid};
             double d1, l1;
-            element_body<true, false, true, true>(E, N, d.M, S, dt1, e, d1, l1, ei, eh, ev, bad);
+            element_body<true, false, true, true, ENSC_F64_PREFETCH>(E, N, d.M, S, dt1, e, d1, l1, ei, eh, ev, bad);
             dts = d1 < dts ? d1 : dts;
             len = l1 < len ? l1 : len;
         }

@@ -90,6 +90,12 @@ constexpr int kNodeUnrollMixed = ENSC_NODE_UNROLL_MIXED;
 #ifndef ENSC_F64_WARP_BT
 #define ENSC_F64_WARP_BT 1
 #endif
+// The FP64 warp-pipelined element pass prefetches an element's node rows
+// into L1 once its connectivity is staged: bit 0 the velocities, bit 1 the
+// displacements
+#ifndef ENSC_F64_PREFETCH
+#define ENSC_F64_PREFETCH 3
+#endif
 #ifndef ENSC_F64_PIPE_MINB
 #define ENSC_F64_PIPE_MINB 2
 #endif

@@ -28,6 +28,7 @@ from typing import Callable, Dict, List, Optional, Sequence
 
 import numpy as np
 
+ERR_ARG = -1
 ERR_OOM = -2
 
 
@@ -77,6 +78,24 @@ class BatchBackend:
             raise
         self.batch.set_bcs(slot, p.bc_code, p.bc_value)
         return slot
+
+    def prepare(self, problem):
+        p = problem
+        return self._capi.Prepared(p.mesh.x0, p.mesh.conn, p.v0, material=p.material, controls=p.controls,
+                                   precision=self.batch.precision)
+
+    def add_prepared(self, token, problem) -> int:
+        try:
+            slot = self.batch.add_prepared(token)
+        except self._capi.EnscError as e:
+            if e.code == ERR_OOM:
+                raise AdmissionError(str(e)) from None
+            raise
+        self.batch.set_bcs(slot, problem.bc_code, problem.bc_value)
+        return slot
+
+    def release(self, token) -> None:
+        token.close()
 
     def arm(self, slot: int, cycles: int) -> None:
         self.batch.arm(slot, cycles)
@@ -135,6 +154,17 @@ class FakeBackend:
         self.peak_instances = max(self.peak_instances, len(self.slots))
         return slot
 
+    def prepare(self, problem):
+        if problem.mesh.n_elements <= 0:
+            raise ValueError("empty mesh")
+        return problem
+
+    def add_prepared(self, token, problem) -> int:
+        return self.add(token)
+
+    def release(self, token) -> None:
+        pass
+
     def arm(self, slot: int, cycles: int) -> None:
         s = self.slots[slot]
         s["target"] = s["done"] + cycles
@@ -181,70 +211,161 @@ class FakeBackend:
 class Server:
     """The request loop.  ``requests`` carry ``index``, ``arrival`` (seconds
     after the start of the stream) and ``problem`` (a workloads.Problem whose
-    ``cycles`` is the requested cycle count)."""
+    ``cycles`` is the requested cycle count).
+
+    Admission has a host part (``backend.prepare``: element constants,
+    lumped mass, node tables) and a device part (``backend.add_prepared``).
+    The host part of the next arrivals runs while the GPU steps the current
+    quantum: on ``prepare_workers`` threads, or with ``prepare_workers=0`` on
+    the loop's own thread between enqueueing the quantum and waiting for it.
+    At most ``prepare_ahead`` requests are prepared and not yet admitted, which
+    bounds the host memory they hold.  ``stats`` accumulates where the loop's
+    time went."""
 
     def __init__(self, backend, *, min_quantum: int = 64, max_quantum: int = 1024,
-                 clock: Callable[[], float] = time.perf_counter, sleep: Callable[[float], None] = time.sleep):
+                 clock: Callable[[], float] = time.perf_counter, sleep: Callable[[float], None] = time.sleep,
+                 prepare_workers: int = 0, prepare_ahead: int = 8):
         self.backend = backend
         self.min_quantum = min_quantum
         self.max_quantum = max_quantum
         self.clock = clock
         self.sleep = sleep
+        self.prepare_workers = prepare_workers
+        self.prepare_ahead = max(1, prepare_ahead)
+        self.stats: Dict[str, float] = {}
 
     def serve(self, requests: Sequence) -> List[Outcome]:
         pending = sorted(requests, key=lambda r: r.arrival)
         out = {r.index: Outcome(r.index, r.arrival, elements=r.problem.mesh.n_elements) for r in pending}
         waiting: List = []          # arrived, not admitted (arrival order)
+        prep: Dict[int, object] = {}  # request index -> future / (token, error) of its host part
         running: Dict[int, tuple] = {}   # slot -> (request, cycles left estimate)
+        st = dict(prepare_s=0.0, admit_s=0.0, run_s=0.0, wait_s=0.0, retire_s=0.0, idle_s=0.0, quanta=0,
+                  cycles=0)
+        self.stats = st
+        be = self.backend
+        pool = None
+        if self.prepare_workers > 0:
+            from concurrent.futures import ThreadPoolExecutor
+            pool = ThreadPoolExecutor(self.prepare_workers)
         t0 = self.clock()
         now = lambda: self.clock() - t0  # noqa: E731
-        nxt = 0
-        while nxt < len(pending) or waiting or running:
-            t = now()
-            if not running and not waiting and nxt < len(pending) and pending[nxt].arrival > t:
-                self.sleep(pending[nxt].arrival - t)  # idle until the next arrival
-                t = now()
-            while nxt < len(pending) and pending[nxt].arrival <= t:
-                waiting.append(pending[nxt])
-                nxt += 1
-            # admit: first come, first served, with backfill
-            still = []
-            for r in waiting:
-                try:
-                    slot = self.backend.add(r.problem)
-                except AdmissionError:
-                    still.append(r)
+
+        def host_part(r):
+            try:
+                return be.prepare(r.problem), None
+            except Exception as e:  # noqa: BLE001 - reported as the request's status
+                return None, e
+
+        def start_prepares():
+            # the host part of the first prepare_ahead waiting requests
+            for r in waiting[:self.prepare_ahead]:
+                if r.index in prep:
                     continue
-                self.backend.arm(slot, r.problem.cycles)
-                running[slot] = (r, r.problem.cycles)
-                out[r.index].admitted = now()
-            waiting = still
-            if not running:
-                # an empty batch that cannot take a request never will: reject it
-                for r in waiting:
-                    o = out[r.index]
-                    o.status = ERR_OOM
-                    o.finished = now()
-                waiting = []
-                continue
-            q = min(left for _, left in running.values())
-            q = int(min(self.max_quantum, max(self.min_quantum, q)))
-            self.backend.run(q)
-            self.backend.sync()
-            for slot in list(running):
-                r, left = running[slot]
-                rep = self.backend.report(slot)
-                if rep["done"] or rep["status"]:
-                    o = out[r.index]
-                    o.cycles = int(rep["cycles"])
-                    o.status = int(rep["status"])
-                    o.result = self.backend.download(slot)
-                    o.energy = self.backend.energy(slot)
-                    self.backend.remove(slot)
-                    o.finished = now()
-                    del running[slot]
+                if pool is not None:
+                    prep[r.index] = pool.submit(host_part, r)
                 else:
-                    running[slot] = (r, max(0, left - q))
+                    c = self.clock()
+                    prep[r.index] = host_part(r)
+                    st["prepare_s"] += self.clock() - c
+
+        def prepared(r, block: bool):
+            f = prep.get(r.index)
+            if f is None:
+                return None
+            if pool is None:
+                return f
+            if not block and not f.done():
+                return None
+            return f.result()
+
+        def fail(r, code: int):
+            o = out[r.index]
+            o.status = code
+            o.finished = now()
+
+        try:
+            nxt = 0
+            while nxt < len(pending) or waiting or running:
+                t = now()
+                if not running and not waiting and nxt < len(pending) and pending[nxt].arrival > t:
+                    c = self.clock()
+                    self.sleep(pending[nxt].arrival - t)  # idle until the next arrival
+                    st["idle_s"] += self.clock() - c
+                    t = now()
+                while nxt < len(pending) and pending[nxt].arrival <= t:
+                    waiting.append(pending[nxt])
+                    nxt += 1
+                start_prepares()
+                # admit the prepared: first come, first served, with backfill
+                c = self.clock()
+                still, refused = [], []
+                for i, r in enumerate(waiting):
+                    # with nothing on the device, wait for the first request's host part
+                    res = prepared(r, block=not running and i == 0)
+                    if res is None:
+                        still.append(r)
+                        continue
+                    token, err = res
+                    if err is not None:
+                        del prep[r.index]
+                        fail(r, getattr(err, "code", ERR_ARG))
+                        continue
+                    try:
+                        slot = be.add_prepared(token, r.problem)
+                    except AdmissionError:
+                        still.append(r)
+                        refused.append(r)
+                        continue
+                    del prep[r.index]
+                    be.release(token)
+                    be.arm(slot, r.problem.cycles)
+                    running[slot] = (r, r.problem.cycles)
+                    out[r.index].admitted = now()
+                waiting = still
+                st["admit_s"] += self.clock() - c
+                if not running:
+                    # an empty batch that cannot take a request never will: reject it
+                    for r in refused:
+                        be.release(prepared(r, block=True)[0])
+                        del prep[r.index]
+                        fail(r, ERR_OOM)
+                    waiting = [r for r in waiting if out[r.index].status == 0]
+                    continue
+                q = min(left for _, left in running.values())
+                q = int(min(self.max_quantum, max(self.min_quantum, q)))
+                c = self.clock()
+                be.run(q)
+                st["run_s"] += self.clock() - c
+                st["quanta"] += 1
+                st["cycles"] += q
+                start_prepares()  # host work while the quantum runs
+                c = self.clock()
+                be.sync()
+                st["wait_s"] += self.clock() - c
+                c = self.clock()
+                for slot in list(running):
+                    r, left = running[slot]
+                    rep = be.report(slot)
+                    if rep["done"] or rep["status"]:
+                        o = out[r.index]
+                        o.cycles = int(rep["cycles"])
+                        o.status = int(rep["status"])
+                        o.result = be.download(slot)
+                        o.energy = be.energy(slot)
+                        be.remove(slot)
+                        o.finished = now()
+                        del running[slot]
+                    else:
+                        running[slot] = (r, max(0, left - q))
+                st["retire_s"] += self.clock() - c
+        finally:
+            for f in prep.values():
+                res = f.result() if pool is not None else f
+                if res[0] is not None:
+                    be.release(res[0])
+            if pool is not None:
+                pool.shutdown()
         return [out[r.index] for r in pending]
 
 

@@ -271,6 +271,23 @@ int ensc_batch_create(const ensc_params* params, int32_t max_instances, int64_t 
 int ensc_batch_add(ensc_batch* b, const ensc_mesh_desc* mesh, const ensc_material* mat, const ensc_params* controls,
                    int32_t* slot);
 
+/* ensc_batch_add in two parts, so that the host work of an arriving solve
+ * can overlap the batch's running cycles.  ensc_batch_prepare does the host
+ * part -- checks the mesh and material and computes the element constants,
+ * lumped mass and node tables for `precision` -- on the calling thread and
+ * makes no CUDA call, so it may run on any thread while a batch steps;
+ * errors are reported through ensc_last_error(NULL) of that thread.  The
+ * mesh's x0 and v0 arrays are read again by ensc_batch_add_prepared and must
+ * stay valid until then.  ensc_batch_add_prepared does the device part
+ * (ENSC_ERR_OOM as ensc_batch_add; ENSC_ERR_ARG when the precision is not the
+ * batch's) and leaves `prep` to the caller, who frees it with
+ * ensc_prepared_destroy; the instance is the one ensc_batch_add would add. */
+typedef struct ensc_prepared ensc_prepared;
+int ensc_batch_prepare(const ensc_mesh_desc* mesh, const ensc_material* mat, int32_t precision, ensc_prepared** out);
+int ensc_batch_add_prepared(ensc_batch* b, const ensc_prepared* prep, const ensc_params* controls, int32_t* slot);
+int64_t ensc_prepared_bytes(const ensc_prepared* prep);  /* device bytes the instance will take */
+void ensc_prepared_destroy(ensc_prepared* prep);
+
 /* ensc_set_bcs for one instance. */
 int ensc_batch_set_bcs(ensc_batch* b, int32_t slot, const int8_t* dof_code, const double* dof_value);
 

@@ -103,3 +103,23 @@ def _load_missing(path):
         capi.load(path)
     finally:
         capi._lib = saved
+
+
+def test_batch_prepare_runs_on_the_host_only(lib):
+    """ensc_batch_prepare makes no CUDA call: it works here, without a GPU,
+    sizes the instance's device block and reports bad input through
+    ensc_last_error(NULL)."""
+    from enscdynamics_b200 import workloads as W
+    p = W.block(6, 4, 3, 0.6, 0.4, 0.3)
+    sizes = {}
+    for prec in (capi.FP64, capi.MIXED):
+        pr = capi.Prepared(p.mesh.x0, p.mesh.conn, p.v0, material=p.material, controls=p.controls, precision=prec)
+        sizes[prec] = pr.device_bytes
+        pr.close()
+    assert sizes[capi.FP64] > sizes[capi.MIXED] > 0
+    with pytest.raises(capi.EnscError, match="out of range"):
+        bad = p.mesh.conn.copy()
+        bad[0, 7] = p.mesh.n_nodes
+        capi.Prepared(p.mesh.x0, bad, p.v0, material=p.material, controls=p.controls)
+    with pytest.raises(capi.EnscError, match="precision"):
+        capi.Prepared(p.mesh.x0, p.mesh.conn, p.v0, material=p.material, controls=p.controls, precision=5)

@@ -207,3 +207,47 @@ def test_instance_reports_done_right_after_its_last_cycle():
         assert b.sync() == 0
         rep = b.report(s)
         assert rep["done"] == 1 and rep["cycles"] == 100
+
+
+@pytest.mark.parametrize("precision", [capi.FP64, capi.MIXED])
+def test_churn_with_short_runs_and_prepared_instances(precision):
+    """The serving pattern: runs of 70 cycles (the autotuner then
+    spreads its candidates over several runs), instances prepared on the
+    host beforehand (ensc_batch_prepare / ensc_batch_add_prepared), and
+    instances removed and added between runs, slots reused before the tables
+    are rewritten.  Every instance still ends with its single-instance
+    results and energies."""
+    cases = [sweep_case(40 + i, 120 + 45 * i, plastic=i % 2 == 0) for i in range(6)]
+    refs = [single(c, precision) for c in cases]
+    got = {}
+    with make_batch(precision, max_instances=4) as b:
+        todo = list(range(len(cases)))
+        live = {}
+
+        def admit():
+            while todo and len(live) < 3:
+                i = todo.pop(0)
+                c = cases[i]
+                pr = capi.Prepared(c.x0, c.conn, c.v0, material=c.mat, controls=c.ctl, precision=precision)
+                s = b.add_prepared(pr)
+                pr.close()
+                b.set_bcs(s, c.code, c.val)
+                b.arm(s, c.cycles)
+                live[s] = i
+        admit()
+        runs = 0
+        while live:
+            b.run(70)
+            runs += 1
+            b.sync()
+            for s in list(live):
+                if b.report(s)["done"]:
+                    i = live.pop(s)
+                    got[i] = (b.download(s), b.report(s), b.energy(s))
+                    b.remove(s)
+            admit()
+            assert runs < 1000
+        t = b.tuning
+        assert t["graph_cycles"] in (8, 32)
+    for i, c in enumerate(cases):
+        assert_same(*got[i], refs[i], c.name)

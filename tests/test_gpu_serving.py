@@ -26,7 +26,7 @@ def test_results_in_the_mix_equal_results_alone():
     be = S.BatchBackend(budget_bytes=1 << 30, max_instances=8, max_elements=1 << 20, max_nodes=1 << 21,
                         fields=FIELDS)
     try:
-        out = S.Server(be, min_quantum=32).serve(reqs)
+        out = S.Server(be, min_quantum=32, prepare_workers=2, prepare_ahead=3).serve(reqs)
     finally:
         be.close()
     assert all(o.status == 0 for o in out)

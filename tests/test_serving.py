@@ -76,3 +76,29 @@ def test_quantum_follows_the_earliest_finishing_instance():
     # the short request retires after one 70-cycle quantum, not after 1024
     assert out[1].finished <= out[0].finished
     assert be.cycles_run < 1000 + 64
+
+
+def test_prepare_on_threads_matches_inline_prepare():
+    reqs = stream(120, seed=9)
+    budget = 200_000 * 400 * 3
+    outs = []
+    for workers in (0, 3):
+        be = S.FakeBackend(budget_bytes=budget, max_instances=16)
+        srv = S.Server(be, clock=be.now, sleep=be.sleep, prepare_workers=workers, prepare_ahead=4)
+        out = srv.serve(reqs)
+        assert all(o.status == 0 for o in out) and be.used == 0
+        assert srv.stats["quanta"] > 0 and srv.stats["cycles"] >= max(r.problem.cycles for r in reqs)
+        outs.append(out)
+    # threads change only when a request's host part is ready, not what runs
+    for a, b in zip(*outs):
+        assert a.cycles == b.cycles and a.arrival <= a.admitted <= a.finished and b.arrival <= b.admitted
+
+
+def test_a_request_whose_host_part_fails_is_reported_and_others_finish():
+    reqs = [W.Request(0, 0.0, _Problem(500, 300)), W.Request(1, 0.1, _Problem(0, 100)),
+            W.Request(2, 0.2, _Problem(300, 200))]
+    for workers in (0, 2):
+        be = S.FakeBackend(budget_bytes=10 ** 9, max_instances=8)
+        out = S.Server(be, clock=be.now, sleep=be.sleep, prepare_workers=workers).serve(reqs)
+        assert out[1].status == S.ERR_ARG and out[1].finished >= out[1].arrival
+        assert out[0].status == 0 and out[2].status == 0 and out[2].cycles == 200
