@@ -157,38 +157,53 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def element_pass_bytes(ne: int, nn: int, plastic: bool, mixed: bool = False) -> int:
+def element_pass_bytes(ne: int, nn: int, plastic: bool, mixed: bool = False, patches: int = 0,
+                       partials: int = 0) -> int:
     """Algorithmic bytes of one element-pass launch.
     FP64: connectivity 32, sigma r/w 96, QIA r/w 192, B0^T 192, V0 8,
     element-force write 192 per element (+16 eps_p r/w with J2); x, u, v
     gathered once per node (72 B).
     Mixed: connectivity 32, sigma r/w 48, QIA r/w 96, the B0 matrix A as a
-    float pair 72, V0 8, cbrt(V0) 4, force write 96 (+8 eps_p); x FP64 and
-    v FP32 per node (36 B: the mixed pass forms F from current coordinates
-    and does not read u)."""
+    float pair 72, V0 8, cbrt(V0) 4 (+8 eps_p) per element; x FP64 and v
+    FP32 per node (36 B: the mixed pass forms F from current coordinates and
+    does not read u).  Slot assembly: force write 96 per element.  Patch
+    assembly (partials > 0): the incidence list 16 per element, per
+    (patch, node) partial its incidence offset 4 and its three FP32 sums 12,
+    and 4 per patch for the partial range -- instead of the force write."""
     if mixed:
-        return ne * (32 + 48 + 96 + 72 + 8 + 4 + 96 + (8 if plastic else 0)) + nn * 36
+        base = ne * (32 + 48 + 96 + 72 + 8 + 4 + (8 if plastic else 0)) + nn * 36
+        if partials:
+            return base + ne * 16 + partials * (4 + 12) + (patches + 1) * 4
+        return base + ne * 96
     return ne * (32 + 96 + 192 + 192 + 8 + 192 + (16 if plastic else 0)) + nn * 72
 
 
-def node_pass_bytes(ne: int, nn: int, mixed: bool = False) -> int:
-    """Algorithmic bytes of one node-pass launch: the element forces (24
-    components per element, each read once: 192 B FP64, 96 B mixed), and per
-    node the inverse mass 8, BC code 1, x and u read and write 96, v read and
-    write (48 FP64; mixed: 24 for the float rows and 12 for their 16-bit
-    residual rows).  Reactions and prescribed velocities are touched only at
-    constrained nodes and not counted; force slots that no element fills
+def node_pass_bytes(ne: int, nn: int, mixed: bool = False, partials: int = 0) -> int:
+    """Algorithmic bytes of one node-pass launch: the element forces, and
+    per node the inverse mass 8, BC code 1, x and u read and write 96, v read
+    and write (48 FP64; mixed: 24 for the float rows and 12 for their 16-bit
+    residual rows).  Slot assembly: the 24 force components of every element,
+    each read once (192 B FP64, 96 B mixed).  Patch assembly (partials > 0):
+    per node its partial range 4, per partial its index 4 and its three sums
+    12.  Reactions and prescribed velocities are touched only at constrained
+    nodes and not counted; slot-major force slots that no element fills
     (boundary nodes) are read as zeros but not counted."""
     if mixed:
-        return ne * 96 + nn * (8 + 1 + 96 + 24 + 12)
+        per_node = nn * (8 + 1 + 96 + 24 + 12)
+        if partials:
+            return per_node + nn * 4 + partials * (4 + 12)
+        return ne * 96 + per_node
     return ne * 192 + nn * (8 + 1 + 96 + 48)
 
 
-def cycle_bytes(ne: int, nn: int, plastic: bool, mixed: bool = False) -> int:
+def cycle_bytes(ne: int, nn: int, plastic: bool, mixed: bool = False, patches: int = 0, partials: int = 0) -> int:
     """Canonical algorithmic bytes of one cycle (element pass + node pass):
-    FP64 904 B per element (+16 with J2) and 225 B per node; mixed 452 B per
-    element (+8) and 177 B per node."""
-    return element_pass_bytes(ne, nn, plastic, mixed) + node_pass_bytes(ne, nn, mixed)
+    FP64 904 B per element (+16 with J2) and 225 B per node; mixed with the
+    slot assembly 452 B per element (+8) and 177 B per node; mixed with the
+    patch assembly 276 B per element (+8), 181 B per node and 32 B per
+    partial (about 1.5-1.8 partials per node)."""
+    return (element_pass_bytes(ne, nn, plastic, mixed, patches, partials)
+            + node_pass_bytes(ne, nn, mixed, partials))
 
 
 def build_problem(name: str, dims: str = "256,128,64"):
@@ -302,6 +317,8 @@ def time_block(args, p, precision, stream, local, barrier, max_over_ranks, sum_o
                      stream=stream.cuda_stream, precision=capi.MIXED if mixed else capi.FP64)
     s.set_bcs(p.bc_code, p.bc_value)
     kpc = s.kernels_per_cycle
+    asm = s.assembly
+    pt, pq = asm["patches"], asm["partials"]
     for _ in range(args.warmup):
         s.step_async(C)
     s.sync()
@@ -333,8 +350,8 @@ def time_block(args, p, precision, stream, local, barrier, max_over_ranks, sum_o
     nd = prof["node"]
     nd_ms = nd["ms"] / max(nd["launches"], 1)
     peak, peak_kind = measured_peaks()
-    el_bytes = element_pass_bytes(ne, nn, plastic, mixed)
-    nd_bytes = node_pass_bytes(ne, nn, mixed)
+    el_bytes = element_pass_bytes(ne, nn, plastic, mixed, pt, pq)
+    nd_bytes = node_pass_bytes(ne, nn, mixed, pq)
     achieved = el_bytes / (el_ms / 1000.0) / 1e9
     total_ms = sum(v["ms"] for v in prof.values())
     traffic = None
@@ -342,13 +359,15 @@ def time_block(args, p, precision, stream, local, barrier, max_over_ranks, sum_o
     if os.path.exists(tp):
         with open(tp) as f:
             traffic = json.load(f).get("bytes_per_launch")
-    cb = cycle_bytes(ne, nn, plastic, mixed)
+    cb = cycle_bytes(ne, nn, plastic, mixed, pt, pq)
+    kernel = ("k_element_mixed_patch" if pq else "k_element_mixed_staged") if mixed else "k_element_fp64_warp"
     return s, {
+        "assembly": {"kind": "patch" if pq else "slot", "patches": pt, "partials": pq},
         "value": value, "ms_max": ms_max, "launches": args.steps * (C * kpc + 1),
         "clocks": clocks, "cycles_run": (args.warmup + args.steps) * C + args.profile_cycles,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic,
-                     "kernel": "element pass (%s)" % ("k_element_mixed_staged" if mixed else "k_element_staged, FP64"),
+                     "kernel": "element pass (%s)" % kernel,
                      "peak_source": peak_kind, "kernel_ms": el_ms, "bytes_per_launch": el_bytes},
         "node_roofline": {"achieved": nd_bytes / (nd_ms / 1000.0) / 1e9, "frac": nd_bytes / (nd_ms / 1000.0) / 1e9 / peak,
                           "kernel_ms": nd_ms, "bytes_per_launch": nd_bytes},
@@ -770,8 +789,10 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": m_head["ms_max"] / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if mixed else "f64", "data": "synthetic",
         "config": {"workload": workload, "elements": ne, "nodes": nn, "cycles_per_step": C, "precision": head,
-                   "l2": f"inputs larger than L2 ({cycle_bytes(ne, nn, plastic, mixed) / 1e9:.2f} GB per cycle)",
+                   "l2": f"inputs larger than L2 ({m_head['cycle_roofline']['bytes_per_cycle'] / 1e9:.2f} GB "
+                         "per cycle)",
                    "parallelism": f"replicas x{world}"},
+        "assembly": m_head["assembly"],
         "roofline": m_head["roofline"],
         "node_roofline": m_head["node_roofline"],
         "cycle_roofline": m_head["cycle_roofline"],

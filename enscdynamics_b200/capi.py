@@ -19,6 +19,10 @@ LIB_PATH = os.path.join(_PKG, "_lib", "libensc_b200.so")
 
 FP64 = 0
 MIXED = 1
+# force assembly (ensc_params.assembly)
+ASSEMBLY_AUTO = 0
+ASSEMBLY_SLOT = 1
+ASSEMBLY_PATCH = 2
 
 _ERR = {-1: "ENSC_ERR_ARG", -2: "ENSC_ERR_OOM", -3: "ENSC_ERR_CUDA", -4: "ENSC_ERR_NONFINITE",
         -5: "ENSC_ERR_INVERTED", -6: "ENSC_ERR_TIMEOUT", -7: "ENSC_ERR_NODEVICE"}
@@ -41,7 +45,15 @@ class Params(C.Structure):
                 ("cvisl", C.c_double), ("cvisq", C.c_double), ("total_time", C.c_double),
                 ("gravity_on", C.c_int32), ("gravity_value", C.c_double), ("gravity_dir", C.c_double * 3),
                 ("precision", C.c_int32), ("device", C.c_int32), ("stream", C.c_void_p),
-                ("graph_chunk", C.c_int32)]
+                ("graph_chunk", C.c_int32), ("assembly", C.c_int32)]
+
+
+class PatchTables(C.Structure):
+    _fields_ = [("n_elements", C.c_int64), ("n_nodes", C.c_int64), ("n_patches", C.c_int64),
+                ("n_partials", C.c_int64), ("stored", C.POINTER(C.c_int32)),
+                ("patch_first", C.POINTER(C.c_uint32)), ("inc_first", C.POINTER(C.c_uint32)),
+                ("inc", C.POINTER(C.c_uint16)), ("node_first", C.POINTER(C.c_uint32)),
+                ("node_partials", C.POINTER(C.c_uint32))]
 
 
 class StepReport(C.Structure):
@@ -124,6 +136,7 @@ SIGNATURES = [
     ("ensc_profile", C.c_int, [C.c_void_p, C.c_int64, C.c_double, _P, C.POINTER(C.c_int64)]),
     ("ensc_device_bytes", C.c_int64, [C.c_void_p]),
     ("ensc_kernels_per_cycle", C.c_int32, [C.c_void_p]),
+    ("ensc_assembly", C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     ("ensc_destroy", None, [C.c_void_p]),
     ("ensc_step_noalloc", C.c_int, [C.POINTER(DeviceModel), C.POINTER(MaterialDesc), C.POINTER(Params),
                                     C.POINTER(NoallocClock), C.c_int64, C.c_double]),
@@ -132,8 +145,11 @@ SIGNATURES = [
                                     C.POINTER(C.c_void_p)]),
     ("ensc_batch_add", C.c_int, [C.c_void_p, C.POINTER(MeshDesc), C.POINTER(MaterialDesc), C.POINTER(Params),
                                  C.POINTER(C.c_int32)]),
-    ("ensc_batch_prepare", C.c_int, [C.POINTER(MeshDesc), C.POINTER(MaterialDesc), C.c_int32,
+    ("ensc_batch_prepare", C.c_int, [C.POINTER(MeshDesc), C.POINTER(MaterialDesc), C.POINTER(Params),
                                      C.POINTER(C.c_void_p)]),
+    ("ensc_prepared_assembly", C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int64),
+                                         C.POINTER(C.c_int64)]),
+    ("ensc_prepared_patch_tables", C.c_int, [C.c_void_p, C.POINTER(PatchTables)]),
     ("ensc_batch_add_prepared", C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(Params), C.POINTER(C.c_int32)]),
     ("ensc_prepared_bytes", C.c_int64, [C.c_void_p]),
     ("ensc_prepared_destroy", None, [C.c_void_p]),
@@ -216,7 +232,7 @@ class Stepper:
                  material: _mesh.Material, controls: _mesh.Controls, precision: int = FP64,
                  bt: Optional[np.ndarray] = None, vol0: Optional[np.ndarray] = None,
                  inv_mass: Optional[np.ndarray] = None, device: int = 0, stream: Optional[int] = None,
-                 graph_chunk: int = 0):
+                 graph_chunk: int = 0, assembly: int = ASSEMBLY_AUTO):
         lib = load()
         self._lib = lib
         self.h = C.c_void_p()
@@ -227,6 +243,7 @@ class Stepper:
         p.device = device
         p.stream = stream
         p.graph_chunk = graph_chunk
+        p.assembly = assembly
         rc = lib.ensc_create(C.byref(m), C.byref(mt), C.byref(p), C.byref(self.h))
         if rc != 0:
             raise EnscError(rc, lib.ensc_last_error(None).decode())
@@ -355,6 +372,13 @@ class Stepper:
     def kernels_per_cycle(self) -> int:
         return int(self._lib.ensc_kernels_per_cycle(self.h))
 
+    @property
+    def assembly(self) -> Dict[str, int]:
+        """The force assembly in use (ensc_assembly), its patches and partials."""
+        a, np_, nq = C.c_int32(), C.c_int64(), C.c_int64()
+        self._check(self._lib.ensc_assembly(self.h, C.byref(a), C.byref(np_), C.byref(nq)))
+        return {"assembly": int(a.value), "patches": int(np_.value), "partials": int(nq.value)}
+
 
 class Prepared:
     """An instance prepared on the host for Batch.add_prepared
@@ -364,12 +388,15 @@ class Prepared:
     prepared on threads while a batch steps."""
 
     def __init__(self, x0: np.ndarray, conn: np.ndarray, v0: Optional[np.ndarray] = None, *,
-                 material: _mesh.Material, controls: _mesh.Controls, precision: int = MIXED):
+                 material: _mesh.Material, controls: _mesh.Controls, precision: int = MIXED,
+                 assembly: int = ASSEMBLY_AUTO):
         lib = load()
         self._lib = lib
         self.h = C.c_void_p()
         keep, m, mt, p = _descriptors(x0, conn, v0, material, controls)
-        rc = lib.ensc_batch_prepare(C.byref(m), C.byref(mt), int(precision), C.byref(self.h))
+        p.precision = int(precision)
+        p.assembly = int(assembly)
+        rc = lib.ensc_batch_prepare(C.byref(m), C.byref(mt), C.byref(p), C.byref(self.h))
         if rc != 0:
             raise EnscError(rc, lib.ensc_last_error(None).decode())
         self._keep = keep
@@ -381,6 +408,29 @@ class Prepared:
     @property
     def device_bytes(self) -> int:
         return int(self._lib.ensc_prepared_bytes(self.h))
+
+    @property
+    def assembly(self) -> Dict[str, int]:
+        """The force assembly the instance uses, its patches and partials."""
+        a, np_, nq = C.c_int32(), C.c_int64(), C.c_int64()
+        rc = self._lib.ensc_prepared_assembly(self.h, C.byref(a), C.byref(np_), C.byref(nq))
+        if rc != 0:
+            raise EnscError(rc, self._lib.ensc_last_error(None).decode())
+        return {"assembly": int(a.value), "patches": int(np_.value), "partials": int(nq.value)}
+
+    def patch_tables(self) -> Dict[str, np.ndarray]:
+        """Copies of the patch tables (ensc_prepared_patch_tables)."""
+        t = PatchTables()
+        rc = self._lib.ensc_prepared_patch_tables(self.h, C.byref(t))
+        if rc != 0:
+            raise EnscError(rc, self._lib.ensc_last_error(None).decode())
+        ne, nn, npch, nq = int(t.n_elements), int(t.n_nodes), int(t.n_patches), int(t.n_partials)
+
+        def arr(ptr, n):
+            return np.ctypeslib.as_array(ptr, shape=(n,)).copy()
+        return {"stored": arr(t.stored, ne), "patch_first": arr(t.patch_first, npch + 1),
+                "inc_first": arr(t.inc_first, nq + 1), "inc": arr(t.inc, 8 * ne),
+                "node_first": arr(t.node_first, nn + 1), "node_partials": arr(t.node_partials, nq)}
 
     def close(self) -> None:
         if self.h:
@@ -402,7 +452,8 @@ class Batch:
     batch runs one launch per cycle phase for all of them."""
 
     def __init__(self, *, max_instances: int, max_elements: int, max_nodes: int, budget_bytes: int,
-                 precision: int = MIXED, device: int = 0, stream: Optional[int] = None, graph_chunk: int = 0):
+                 precision: int = MIXED, device: int = 0, stream: Optional[int] = None, graph_chunk: int = 0,
+                 assembly: int = ASSEMBLY_AUTO):
         lib = load()
         self._lib = lib
         self.h = C.c_void_p()
@@ -411,12 +462,14 @@ class Batch:
         p.device = device
         p.stream = stream
         p.graph_chunk = graph_chunk
+        p.assembly = assembly
         p.factor_timestep = 1.0
         rc = lib.ensc_batch_create(C.byref(p), int(max_instances), int(max_elements), int(max_nodes),
                                    int(budget_bytes), C.byref(self.h))
         if rc != 0:
             raise EnscError(rc, lib.ensc_last_error(None).decode())
         self.precision = precision
+        self.assembly = assembly
         self.sizes: Dict[int, tuple] = {}
 
     def _check(self, rc: int) -> None:

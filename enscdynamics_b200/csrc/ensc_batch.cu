@@ -53,6 +53,7 @@ struct Tune {
 struct ensc_batch {
     int device = 0;
     int precision = ENSC_MIXED;
+    int assembly = ENSC_ASSEMBLY_AUTO;  // for ensc_batch_add
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     cudaStream_t cap_stream = nullptr;
@@ -351,6 +352,7 @@ int ensc_batch_create(const ensc_params* params, int32_t max_instances, int64_t 
     ensc_batch* b = new ensc_batch();
     b->device = params->device;
     b->precision = params->precision;
+    b->assembly = params->assembly;
     b->budget = budget_bytes;
     b->slots = max_instances;
     // tiles: every instance rounds its element and node counts up to tiles
@@ -460,17 +462,19 @@ int ensc_batch_create(const ensc_params* params, int32_t max_instances, int64_t 
     return ENSC_OK;
 }
 
-int ensc_batch_prepare(const ensc_mesh_desc* mesh, const ensc_material* mat, int32_t precision, ensc_prepared** out) {
+int ensc_batch_prepare(const ensc_mesh_desc* mesh, const ensc_material* mat, const ensc_params* params,
+                       ensc_prepared** out) {
     if (!out) return berr(nullptr, ENSC_ERR_ARG, "out is required");
     *out = nullptr;
+    if (!mesh || !mat || !params) return berr(nullptr, ENSC_ERR_ARG, "mesh, material and params are required");
+    const int32_t precision = params->precision;
     if (precision != ENSC_FP64 && precision != ENSC_MIXED) return berr(nullptr, ENSC_ERR_ARG, "unknown precision");
-    if (!mesh || !mat) return berr(nullptr, ENSC_ERR_ARG, "mesh and material are required");
     ensc_prepared* p = new (std::nothrow) ensc_prepared;
     if (!p) return berr(nullptr, ENSC_ERR_OOM, "host allocation failed");
     std::string perr;
     int rc;
     try {
-        rc = ensc::instance_prepare(mesh, mat, precision == ENSC_MIXED, p->ih, perr);
+        rc = ensc::instance_prepare(mesh, mat, precision == ENSC_MIXED, params->assembly, p->ih, perr);
     } catch (const std::bad_alloc&) {
         rc = ENSC_ERR_OOM;
         perr = "host allocation failed";
@@ -487,13 +491,41 @@ int ensc_batch_prepare(const ensc_mesh_desc* mesh, const ensc_material* mat, int
 
 int64_t ensc_prepared_bytes(const ensc_prepared* prep) { return prep ? static_cast<int64_t>(prep->ih.bytes) : 0; }
 
+int ensc_prepared_assembly(const ensc_prepared* prep, int32_t* assembly, int64_t* patches, int64_t* partials) {
+    if (!prep) return berr(nullptr, ENSC_ERR_ARG, "prep is NULL");
+    if (assembly) *assembly = prep->ih.patch ? ENSC_ASSEMBLY_PATCH : ENSC_ASSEMBLY_SLOT;
+    if (patches) *patches = prep->ih.n_patches;
+    if (partials) *partials = prep->ih.n_pnodes;
+    return ENSC_OK;
+}
+
+int ensc_prepared_patch_tables(const ensc_prepared* prep, ensc_patch_tables* out) {
+    if (!prep || !out) return berr(nullptr, ENSC_ERR_ARG, "prep and out are required");
+    const ensc::InstanceHost& h = prep->ih;
+    if (!h.patch) return berr(nullptr, ENSC_ERR_ARG, "the instance uses the slot assembly");
+    out->n_elements = h.ne;
+    out->n_nodes = h.nn;
+    out->n_patches = h.n_patches;
+    out->n_partials = h.n_pnodes;
+    out->stored = h.iperm.data();
+    out->patch_first = h.pf_off.data();
+    out->inc_first = h.pinc_off.data();
+    out->inc = h.pinc.data();
+    out->node_first = h.nptr.data();
+    out->node_partials = h.nent.data();
+    return ENSC_OK;
+}
+
 void ensc_prepared_destroy(ensc_prepared* prep) { delete prep; }
 
 int ensc_batch_add(ensc_batch* b, const ensc_mesh_desc* mesh, const ensc_material* mat, const ensc_params* controls,
                    int32_t* slot_out) {
     if (!b || !mesh || !mat || !controls || !slot_out) return berr(b, ENSC_ERR_ARG, "missing argument");
     ensc_prepared* p = nullptr;
-    int rc = ensc_batch_prepare(mesh, mat, b->precision, &p);
+    ensc_params pp{};
+    pp.precision = b->precision;
+    pp.assembly = b->assembly;
+    int rc = ensc_batch_prepare(mesh, mat, &pp, &p);
     if (rc) return berr(b, rc, ensc_last_error(nullptr));
     rc = ensc_batch_add_prepared(b, p, controls, slot_out);
     ensc_prepared_destroy(p);
@@ -705,10 +737,15 @@ int ensc_batch_download(ensc_batch* b, int32_t slot, double* x, double* u, doubl
         int64_t n, pad;
         int comps;
         bool f32;
+        const int32_t* at;
     };
-    const Item items[] = {{x, sl.N.x, sl.nn, sl.nn_pad, 3, false},       {u, sl.N.u, sl.nn, sl.nn_pad, 3, false},
-                          {v, sl.N.v, sl.nn, sl.nn_pad, 3, mx},          {sigma, sl.E.sigma, sl.ne, sl.ne_pad, 6, mx},
-                          {qia, sl.E.qia, sl.ne, sl.ne_pad, 12, mx},     {eps_p, sl.E.eps_p, sl.ne, sl.ne_pad, 1, mx}};
+    const int32_t* ep = sl.E.iperm;  // element fields: stored positions
+    const Item items[] = {{x, sl.N.x, sl.nn, sl.nn_pad, 3, false, nullptr},
+                          {u, sl.N.u, sl.nn, sl.nn_pad, 3, false, nullptr},
+                          {v, sl.N.v, sl.nn, sl.nn_pad, 3, mx, nullptr},
+                          {sigma, sl.E.sigma, sl.ne, sl.ne_pad, 6, mx, ep},
+                          {qia, sl.E.qia, sl.ne, sl.ne_pad, 12, mx, ep},
+                          {eps_p, sl.E.eps_p, sl.ne, sl.ne_pad, 1, mx, ep}};
     const size_t need = static_cast<size_t>(std::max<int64_t>(12 * sl.ne, 3 * sl.nn)) * sizeof(double);
     double* stage = nullptr;
     BCK(b, cudaMallocFromPoolAsync(reinterpret_cast<void**>(&stage), need, b->pool, b->stream));
@@ -716,7 +753,7 @@ int ensc_batch_download(ensc_batch* b, int32_t slot, double* x, double* u, doubl
     for (const Item& it : items) {
         if (!it.dst) continue;
         if (it.src == sl.N.v) ensc::launch_v_to_aos(sl.N, mx, stage, b->stream);
-        else ensc::launch_soa_to_aos(it.src, it.n, it.pad, it.comps, it.f32, stage, b->stream);
+        else ensc::launch_soa_to_aos(it.src, it.n, it.pad, it.comps, it.f32, stage, b->stream, it.at);
         cudaError_t e = cudaMemcpyAsync(it.dst, stage, it.n * it.comps * sizeof(double), cudaMemcpyDeviceToHost,
                                         b->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);

@@ -61,6 +61,7 @@ struct ensc_handle {
     cudaEvent_t snap_landed[2] = {nullptr, nullptr};
     int64_t snap_count = 0;
     bool fe_valid = false;         // fe holds the last force pass's element forces
+    int64_t n_patches = 0, n_partials = 0;  // patch assembly
     std::string err;
 };
 
@@ -189,7 +190,7 @@ int ensc_create(const ensc_mesh_desc* mesh, const ensc_material* mat, const ensc
     const bool mx = params->precision == ENSC_MIXED;
     ensc::InstanceHost ih;
     std::string perr;
-    int rc = ensc::instance_prepare(mesh, mat, mx, ih, perr);
+    int rc = ensc::instance_prepare(mesh, mat, mx, params->assembly, ih, perr);
     if (rc) return set_err(nullptr, rc, perr);
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= params->device || params->device < 0)
@@ -258,6 +259,8 @@ int ensc_create(const ensc_mesh_desc* mesh, const ensc_material* mat, const ensc
         set_err(h, rc, perr);
         return fail(rc);
     }
+    h->n_patches = ih.n_patches;
+    h->n_partials = ih.n_pnodes;
     char* tail = static_cast<char*>(h->arena) + ih.bytes;
     h->P.elem = reinterpret_cast<double*>(tail);
     h->P.node = h->P.elem + 3 * h->grid_e;
@@ -459,16 +462,21 @@ int ensc_download(ensc_handle* h, double* x, double* u, double* v, double* sigma
         int64_t n, pad;
         int comps;
         bool f32;
+        const int32_t* at;
     };
     const bool mx = mixed(h);
-    const Item items[] = {{x, h->N.x, h->nn, h->nn_pad, 3, false},        {u, h->N.u, h->nn, h->nn_pad, 3, false},
-                          {v, h->N.v, h->nn, h->nn_pad, 3, mx},           {sigma, h->E.sigma, h->ne, h->ne_pad, 6, mx},
-                          {qia, h->E.qia, h->ne, h->ne_pad, 12, mx},      {eps_p, h->E.eps_p, h->ne, h->ne_pad, 1, mx}};
+    const int32_t* ep = h->E.iperm;  // element fields: stored positions
+    const Item items[] = {{x, h->N.x, h->nn, h->nn_pad, 3, false, nullptr},
+                          {u, h->N.u, h->nn, h->nn_pad, 3, false, nullptr},
+                          {v, h->N.v, h->nn, h->nn_pad, 3, mx, nullptr},
+                          {sigma, h->E.sigma, h->ne, h->ne_pad, 6, mx, ep},
+                          {qia, h->E.qia, h->ne, h->ne_pad, 12, mx, ep},
+                          {eps_p, h->E.eps_p, h->ne, h->ne_pad, 1, mx, ep}};
     size_t used = 0;
     for (const Item& it : items) {
         if (!it.dst) continue;
         if (it.src == h->N.v) ensc::launch_v_to_aos(h->N, mx, h->staging, h->stream);
-        else ensc::launch_soa_to_aos(it.src, it.n, it.pad, it.comps, it.f32, h->staging, h->stream);
+        else ensc::launch_soa_to_aos(it.src, it.n, it.pad, it.comps, it.f32, h->staging, h->stream, it.at);
         CK(h, cudaGetLastError());
         CK(h, cudaMemcpyAsync(it.dst, h->staging, it.n * it.comps * sizeof(double), cudaMemcpyDeviceToHost,
                               h->stream));
@@ -499,18 +507,23 @@ int ensc_upload_state(ensc_handle* h, const double* x, const double* u, const do
         int64_t n, pad;
         int comps;
         bool f32;
+        const int32_t* at;
     };
     const bool mx = mixed(h);
-    const Item items[] = {{x, h->N.x, h->nn, h->nn_pad, 3, false},        {u, h->N.u, h->nn, h->nn_pad, 3, false},
-                          {v, h->N.v, h->nn, h->nn_pad, 3, mx},           {sigma, h->E.sigma, h->ne, h->ne_pad, 6, mx},
-                          {qia, h->E.qia, h->ne, h->ne_pad, 12, mx},      {eps_p, h->E.eps_p, h->ne, h->ne_pad, 1, mx}};
+    const int32_t* ep = h->E.iperm;  // element fields: stored positions
+    const Item items[] = {{x, h->N.x, h->nn, h->nn_pad, 3, false, nullptr},
+                          {u, h->N.u, h->nn, h->nn_pad, 3, false, nullptr},
+                          {v, h->N.v, h->nn, h->nn_pad, 3, mx, nullptr},
+                          {sigma, h->E.sigma, h->ne, h->ne_pad, 6, mx, ep},
+                          {qia, h->E.qia, h->ne, h->ne_pad, 12, mx, ep},
+                          {eps_p, h->E.eps_p, h->ne, h->ne_pad, 1, mx, ep}};
     size_t used = 0;
     for (const Item& it : items) {
         if (!it.src) continue;
         CK(h, cudaMemcpyAsync(h->staging, it.src, it.n * it.comps * sizeof(double), cudaMemcpyHostToDevice,
                               h->stream));
         if (it.dst == h->N.v) ensc::launch_aos_to_v(h->staging, h->N, mx, h->stream);
-        else ensc::launch_aos_to_soa(h->staging, it.n, it.pad, it.comps, it.dst, it.f32, h->stream);
+        else ensc::launch_aos_to_soa(h->staging, it.n, it.pad, it.comps, it.dst, it.f32, h->stream, it.at);
         CK(h, cudaGetLastError());
         used = std::max(used, static_cast<size_t>(it.n * it.comps) * sizeof(double));
     }
@@ -568,7 +581,7 @@ int ensc_snapshot_begin(ensc_handle* h) {
     ensc::launch_soa_to_aos(h->N.u, h->nn, h->nn_pad, 3, false, d + nodes3, h->stream);
     ensc::launch_v_to_aos(h->N, mx, d + 2 * nodes3, h->stream);
     ensc::launch_soa_to_aos(h->N.rf, h->nn, h->nn_pad, 3, false, d + 4 * nodes3, h->stream);
-    ensc::launch_soa_to_aos(h->E.sigma, h->ne, h->ne_pad, 6, mx, d + 5 * nodes3, h->stream);
+    ensc::launch_soa_to_aos(h->E.sigma, h->ne, h->ne_pad, 6, mx, d + 5 * nodes3, h->stream, h->E.iperm);
     CK(h, cudaGetLastError());
     char* ctl_copy = reinterpret_cast<char*>(d) + (h->snap_bytes - sizeof(Ctl));
     CK(h, cudaMemcpyAsync(ctl_copy, h->ctl, sizeof(Ctl), cudaMemcpyDeviceToDevice, h->stream));
@@ -670,6 +683,14 @@ int64_t ensc_device_bytes(const ensc_handle* h) {
 }
 
 int32_t ensc_kernels_per_cycle(const ensc_handle* h) { return h ? 4 : 0; }
+
+int ensc_assembly(const ensc_handle* h, int32_t* assembly, int64_t* patches, int64_t* partials) {
+    if (!h) return ENSC_ERR_ARG;
+    if (assembly) *assembly = h->E.patch ? ENSC_ASSEMBLY_PATCH : ENSC_ASSEMBLY_SLOT;
+    if (patches) *patches = h->n_patches;
+    if (partials) *partials = h->n_partials;
+    return ENSC_OK;
+}
 
 void ensc_destroy(ensc_handle* h) {
     if (!h) return;

@@ -273,13 +273,15 @@ __global__ void __launch_bounds__(kNodeThreads) k_kinetic(NodeArrays N, Partials
     }
 }
 
+// Entry e of the interleaved array is row position at[e] of the SoA rows
+// (at null: e).
 template <typename ST>
-__global__ void k_soa_to_aos(const ST* soa, int64_t n, int64_t pad, int comps, double* aos) {
+__global__ void k_soa_to_aos(const ST* soa, int64_t n, int64_t pad, int comps, const int32_t* at, double* aos) {
     for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n * comps;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         const int64_t e = i / comps;
         const int c = static_cast<int>(i - e * comps);
-        aos[i] = static_cast<double>(soa[c * pad + e]);
+        aos[i] = static_cast<double>(soa[c * pad + (at ? at[e] : e)]);
     }
 }
 
@@ -298,12 +300,12 @@ __global__ void k_aos_to_v(const double* aos, NodeArrays N) {
 }
 
 template <typename DT>
-__global__ void k_aos_to_soa(const double* aos, int64_t n, int64_t pad, int comps, DT* soa) {
+__global__ void k_aos_to_soa(const double* aos, int64_t n, int64_t pad, int comps, const int32_t* at, DT* soa) {
     for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n * comps;
          i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         const int64_t e = i / comps;
         const int c = static_cast<int>(i - e * comps);
-        soa[c * pad + e] = static_cast<DT>(aos[i]);
+        soa[c * pad + (at ? at[e] : e)] = static_cast<DT>(aos[i]);
     }
 }
 
@@ -472,10 +474,10 @@ void launch_kinetic0(const NodeArrays& N, const Partials& P, Ctl* ctl, bool fp32
     k_between<<<1, kCtlThreads, 0, st>>>(ctl, P, 2);
 }
 void launch_soa_to_aos(const void* soa, int64_t n, int64_t pad, int comps, bool src_fp32, double* aos,
-                       cudaStream_t st) {
+                       cudaStream_t st, const int32_t* at) {
     const int g = grid_for(n * comps, 256);
-    if (src_fp32) k_soa_to_aos<float><<<g, 256, 0, st>>>(static_cast<const float*>(soa), n, pad, comps, aos);
-    else k_soa_to_aos<double><<<g, 256, 0, st>>>(static_cast<const double*>(soa), n, pad, comps, aos);
+    if (src_fp32) k_soa_to_aos<float><<<g, 256, 0, st>>>(static_cast<const float*>(soa), n, pad, comps, at, aos);
+    else k_soa_to_aos<double><<<g, 256, 0, st>>>(static_cast<const double*>(soa), n, pad, comps, at, aos);
 }
 void launch_v_to_aos(const NodeArrays& N, bool fp32_v, double* aos, cudaStream_t st) {
     const int g = static_cast<int>(std::min<int64_t>((3 * N.nn + 255) / 256, 65535));
@@ -488,10 +490,10 @@ void launch_aos_to_v(const double* aos, const NodeArrays& N, bool fp32_v, cudaSt
     else k_aos_to_v<double><<<g, 256, 0, st>>>(aos, N);
 }
 void launch_aos_to_soa(const double* aos, int64_t n, int64_t pad, int comps, void* soa, bool dst_fp32,
-                       cudaStream_t st) {
+                       cudaStream_t st, const int32_t* at) {
     const int g = grid_for(n * comps, 256);
-    if (dst_fp32) k_aos_to_soa<float><<<g, 256, 0, st>>>(aos, n, pad, comps, static_cast<float*>(soa));
-    else k_aos_to_soa<double><<<g, 256, 0, st>>>(aos, n, pad, comps, static_cast<double*>(soa));
+    if (dst_fp32) k_aos_to_soa<float><<<g, 256, 0, st>>>(aos, n, pad, comps, at, static_cast<float*>(soa));
+    else k_aos_to_soa<double><<<g, 256, 0, st>>>(aos, n, pad, comps, at, static_cast<double*>(soa));
 }
 
 }  // namespace ensc

@@ -131,7 +131,26 @@ struct ElemArrays {
     // 0: fe is element-major, fe[(3k + c) * ne_pad + e], gathered through
     // ell / csr by the node pass
     int32_t slot_major;
+    // Patch assembly (mixed precision, patch = 1): elements are stored in
+    // patches of kPatchElems consecutive elements.  The element pass sums a
+    // patch's element forces per patch node in shared memory and writes one
+    // partial per (patch, node): patch p's nodes are the partial entries
+    // pf_off[p] .. pf_off[p + 1] - 1, entry q's incidences are
+    // pinc[pinc_off[q] .. pinc_off[q + 1]) as (element in patch << 3 | slot),
+    // in slot order, and its partial goes to pf[c * pf_pad + q].  fe is not
+    // used.  iperm maps an element of the caller's numbering to its stored
+    // position (null: the caller's order is kept).
+    int32_t patch;
+    const uint32_t* pf_off;
+    const uint32_t* pinc_off;
+    const uint16_t* pinc;
+    float* pf;
+    int64_t pf_pad;
+    const int32_t* iperm;
 };
+
+// Elements per patch of the mixed patch assembly: one staged tile.
+constexpr int kPatchElems = 64;
 
 struct NodeArrays {
     int64_t nn, nn_pad;
@@ -146,6 +165,10 @@ struct NodeArrays {
     const uint32_t* csr_ent;   // (e << 3) | slot
     const uint8_t* slot_mask;  // slot-major forces: bit k set if slot k holds an element
     double* rf;                // reactions, [3][nn_pad]
+    // patch assembly: node n's partials are pf entries nent[nptr[n] ..
+    // nptr[n + 1]), in patch order
+    const uint32_t* nptr;
+    const uint32_t* nent;
 };
 
 // Partial sums written by each block of a pass, folded in fixed block order.
@@ -158,7 +181,9 @@ struct Partials {
 // The node pass's view of one instance: node arrays, slot-major forces,
 // gravity and the control block.  `grouped` is 1 when the forces are
 // slot-major and the rows tile-aligned, so W consecutive nodes can be read
-// and written as vectors.  In a batch, one 128-byte line per slot.
+// and written as vectors, and 2 for the same under the patch assembly.  In
+// a batch, two 128-byte lines per slot; the second is read only under the
+// patch assembly.
 struct alignas(128) NodeView {
     const void* fe;
     void* v;                   // double (FP64) or float (mixed)
@@ -173,8 +198,14 @@ struct alignas(128) NodeView {
     double gravity_value, gravity_dir[3];
     int32_t gravity_on;
     int32_t grouped;
+    // patch assembly (pf non-null): node n's force is the sum of
+    // pf[c * pf_pad + nent[i]] over i in [nptr[n], nptr[n + 1])
+    const float* pf;
+    const uint32_t* nptr;
+    const uint32_t* nent;
+    int64_t pf_pad;
 };
-static_assert(sizeof(NodeView) == 128, "one line per slot");
+static_assert(sizeof(NodeView) == 256, "two lines per slot");
 
 __host__ __device__ inline NodeView node_view(const ElemArrays& E, const NodeArrays& N, const Material& M, Ctl* ctl) {
     NodeView v{};
@@ -192,7 +223,11 @@ __host__ __device__ inline NodeView node_view(const ElemArrays& E, const NodeArr
     v.gravity_value = M.gravity_value;
     for (int c = 0; c < 3; ++c) v.gravity_dir[c] = M.gravity_dir[c];
     v.gravity_on = M.gravity_on;
-    v.grouped = (E.slot_major && E.tiles_aligned) ? 1 : 0;
+    v.grouped = (E.slot_major && E.tiles_aligned) ? (E.patch ? 2 : 1) : 0;
+    v.pf = E.patch ? E.pf : nullptr;
+    v.nptr = N.nptr;
+    v.nent = N.nent;
+    v.pf_pad = E.pf_pad;
     return v;
 }
 
@@ -415,9 +450,10 @@ __device__ __forceinline__ uint32_t ld_bytes(const uint8_t* p) {
 // A NodeView of a batch table through the non-coherent (L1-cached) path:
 // the table does not change while a pass runs.
 __device__ __forceinline__ NodeView ld_view(const NodeView* p) {
-    uint4 w[8];
+    constexpr int kW = sizeof(NodeView) / sizeof(uint4);
+    uint4 w[kW];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) w[i] = __ldg(reinterpret_cast<const uint4*>(p) + i);
+    for (int i = 0; i < kW; ++i) w[i] = __ldg(reinterpret_cast<const uint4*>(p) + i);
     NodeView v;
     memcpy(&v, w, sizeof(v));
     return v;

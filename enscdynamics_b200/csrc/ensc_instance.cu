@@ -1,8 +1,10 @@
 // Host-side preparation and device layout of one solver instance.
 #include "ensc_instance.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <limits>
 
 namespace ensc {
 namespace {
@@ -87,8 +89,104 @@ cudaError_t put(void* block, size_t off, const std::vector<T>& v, cudaStream_t s
 
 }  // namespace
 
-int instance_prepare(const ensc_mesh_desc* mesh, const ensc_material* mat, bool mixed, InstanceHost& h,
-                     std::string& err) {
+std::vector<int32_t> patch_order(int64_t ne, const uint32_t* conn, const double* x0) {
+    std::vector<double> cen(static_cast<size_t>(3 * ne));
+    double lo[3], hi[3], ext[3];
+    for (int c = 0; c < 3; ++c) {
+        lo[c] = std::numeric_limits<double>::infinity();
+        hi[c] = -lo[c];
+        ext[c] = lo[c];
+    }
+    for (int64_t e = 0; e < ne; ++e)
+        for (int c = 0; c < 3; ++c) {
+            double sum = 0.0, mn = std::numeric_limits<double>::infinity(), mx = -mn;
+            for (int k = 0; k < 8; ++k) {
+                const double v = x0[3 * static_cast<int64_t>(conn[8 * e + k]) + c];
+                sum += v;
+                mn = std::min(mn, v);
+                mx = std::max(mx, v);
+            }
+            const double m = sum / 8.0;
+            cen[3 * e + c] = m;
+            lo[c] = std::min(lo[c], m);
+            hi[c] = std::max(hi[c], m);
+            if (mx - mn > 0.0) ext[c] = std::min(ext[c], mx - mn);
+        }
+    // cell size per axis: the smallest element extent, widened so that the
+    // cell indices fit 21 bits; centroids of a structured grid land on whole
+    // cells
+    constexpr double kMaxCell = (1 << 21) - 1;
+    double hc[3];
+    for (int c = 0; c < 3; ++c) {
+        const double range = hi[c] - lo[c];
+        hc[c] = std::isfinite(ext[c]) ? ext[c] : 1.0;
+        if (range / hc[c] > kMaxCell) hc[c] = range / kMaxCell;
+    }
+    std::vector<std::pair<uint64_t, int32_t>> key(static_cast<size_t>(ne));
+    for (int64_t e = 0; e < ne; ++e) {
+        uint64_t cell[3];
+        for (int c = 0; c < 3; ++c) {
+            const double t = std::floor((cen[3 * e + c] - lo[c]) / hc[c] + 0.5);
+            cell[c] = static_cast<uint64_t>(std::min(std::max(t, 0.0), kMaxCell));
+        }
+        uint64_t m = 0;
+        for (int b = 0; b < 21; ++b)
+            for (int c = 0; c < 3; ++c) m |= ((cell[c] >> b) & 1u) << (3 * b + c);
+        key[e] = {m, static_cast<int32_t>(e)};
+    }
+    std::sort(key.begin(), key.end());
+    std::vector<int32_t> perm(static_cast<size_t>(ne));
+    for (int64_t s = 0; s < ne; ++s) perm[s] = key[s].second;
+    return perm;
+}
+
+void build_patches(int64_t nn, int64_t ne, const uint32_t* conn, InstanceHost& h) {
+    const int64_t npatch = (ne + kPatchElems - 1) / kPatchElems;
+    h.n_patches = npatch;
+    h.pf_off.assign(static_cast<size_t>(npatch + 1), 0);
+    h.pinc.assign(static_cast<size_t>(8 * ne), 0);
+    h.pinc_off.clear();
+    h.pinc_off.reserve(static_cast<size_t>(2 * nn + npatch + 1));
+    std::vector<uint32_t> pnode;
+    pnode.reserve(static_cast<size_t>(2 * nn + npatch));
+    std::vector<uint64_t> trip;
+    trip.reserve(8 * kPatchElems);
+    uint32_t pos = 0;
+    for (int64_t p = 0; p < npatch; ++p) {
+        const int64_t e0 = p * kPatchElems, e1 = std::min(ne, e0 + kPatchElems);
+        trip.clear();
+        // (node, slot, element in patch), sorted: each node's incidences in
+        // slot order
+        for (int64_t e = e0; e < e1; ++e)
+            for (int k = 0; k < 8; ++k)
+                trip.push_back((static_cast<uint64_t>(conn[8 * e + k]) << 32) | (static_cast<uint64_t>(k) << 8) |
+                               static_cast<uint64_t>(e - e0));
+        std::sort(trip.begin(), trip.end());
+        h.pf_off[p] = static_cast<uint32_t>(pnode.size());
+        for (size_t i = 0; i < trip.size(); ++i) {
+            const uint32_t node = static_cast<uint32_t>(trip[i] >> 32);
+            if (i == 0 || node != static_cast<uint32_t>(trip[i - 1] >> 32)) {
+                pnode.push_back(node);
+                h.pinc_off.push_back(pos);
+            }
+            const uint32_t k = static_cast<uint32_t>((trip[i] >> 8) & 7u), el = static_cast<uint32_t>(trip[i] & 0xffu);
+            h.pinc[pos++] = static_cast<uint16_t>((el << 3) | k);
+        }
+    }
+    h.pf_off[npatch] = static_cast<uint32_t>(pnode.size());
+    h.pinc_off.push_back(pos);
+    h.n_pnodes = static_cast<int64_t>(pnode.size());
+    // node -> its partials, in patch order
+    h.nptr.assign(static_cast<size_t>(nn + 1), 0);
+    for (uint32_t g : pnode) h.nptr[g + 1] += 1;
+    for (int64_t n = 0; n < nn; ++n) h.nptr[n + 1] += h.nptr[n];
+    h.nent.resize(pnode.size());
+    std::vector<uint32_t> fill(h.nptr.begin(), h.nptr.end() - 1);
+    for (size_t q = 0; q < pnode.size(); ++q) h.nent[fill[pnode[q]]++] = static_cast<uint32_t>(q);
+}
+
+int instance_prepare(const ensc_mesh_desc* mesh, const ensc_material* mat, bool mixed, int assembly,
+                     InstanceHost& h, std::string& err) {
     if (!mesh || !mat) {
         err = "mesh and material are required";
         return ENSC_ERR_ARG;
@@ -121,7 +219,8 @@ int instance_prepare(const ensc_mesh_desc* mesh, const ensc_material* mat, bool 
     h.v0 = mesh->v0;
     const int64_t ep = h.ne_pad, np = h.nn_pad;
 
-    // element constants and lumped mass
+    // element constants and lumped mass, in the caller's element order (the
+    // mass sums follow it)
     std::vector<double> inv_mass_dof;
     if (mesh->bt && mesh->vol0 && mesh->inv_mass) {
         h.bt.assign(mesh->bt, mesh->bt + 24 * ne);
@@ -130,6 +229,52 @@ int instance_prepare(const ensc_mesh_desc* mesh, const ensc_material* mat, bool 
     } else {
         element_constants(nn, ne, mesh->conn, mesh->x0, mat->rho, h.bt, h.vol0, inv_mass_dof);
     }
+
+    // no node repeating a local slot: slot-major forces, and patches allowed
+    h.clash = false;
+    {
+        std::vector<uint8_t> seen(static_cast<size_t>(nn), 0);
+        for (int64_t e = 0; e < ne && !h.clash; ++e)
+            for (int k = 0; k < 8; ++k) {
+                uint8_t& m = seen[mesh->conn[8 * e + k]];
+                if ((m >> k) & 1u) {
+                    h.clash = true;
+                    break;
+                }
+                m = static_cast<uint8_t>(m | (1u << k));
+            }
+    }
+    if (assembly != ENSC_ASSEMBLY_AUTO && assembly != ENSC_ASSEMBLY_SLOT && assembly != ENSC_ASSEMBLY_PATCH) {
+        err = "unknown force assembly";
+        return ENSC_ERR_ARG;
+    }
+    if (assembly == ENSC_ASSEMBLY_PATCH && (!mixed || h.clash)) {
+        err = "patch assembly needs mixed precision and a mesh where no node repeats a local slot";
+        return ENSC_ERR_ARG;
+    }
+    h.patch = assembly == ENSC_ASSEMBLY_PATCH;
+
+    // stored element order: the caller's, or patch order
+    const uint32_t* conn = mesh->conn;
+    std::vector<uint32_t> pconn;
+    if (h.patch) {
+        const std::vector<int32_t> perm = patch_order(ne, mesh->conn, mesh->x0);
+        pconn.resize(static_cast<size_t>(8 * ne));
+        std::vector<double> bt(static_cast<size_t>(24 * ne)), vol0(static_cast<size_t>(ne));
+        h.iperm.resize(static_cast<size_t>(ne));
+        for (int64_t sidx = 0; sidx < ne; ++sidx) {
+            const int64_t e = perm[sidx];
+            h.iperm[e] = static_cast<int32_t>(sidx);
+            std::memcpy(&pconn[8 * sidx], &mesh->conn[8 * e], 8 * sizeof(uint32_t));
+            std::memcpy(&bt[24 * sidx], &h.bt[24 * e], 24 * sizeof(double));
+            vol0[sidx] = h.vol0[e];
+        }
+        h.bt.swap(bt);
+        h.vol0.swap(vol0);
+        conn = pconn.data();
+        build_patches(nn, ne, conn, h);
+    }
+
     h.cb.resize(ne);
     h.cb2.resize(ne);
     for (int64_t e = 0; e < ne; ++e) {
@@ -140,34 +285,33 @@ int instance_prepare(const ensc_mesh_desc* mesh, const ensc_material* mat, bool 
     for (int64_t n = 0; n < nn; ++n) h.im[n] = inv_mass_dof[3 * n];
     h.conn_soa.assign(static_cast<size_t>(8 * ep), 0);
     for (int64_t e = 0; e < ne; ++e)
-        for (int k = 0; k < 8; ++k) h.conn_soa[k * ep + e] = mesh->conn[8 * e + k];
+        for (int k = 0; k < 8; ++k) h.conn_soa[k * ep + e] = conn[8 * e + k];
 
-    // node-to-element tables: slot-major when no node repeats a local slot
+    // node-to-element tables
     h.ell.assign(static_cast<size_t>(8 * np), ENSC_NONE);
-    h.clash = false;
-    for (int k = 0; k < 8 && !h.clash; ++k)
-        for (int64_t e = 0; e < ne; ++e) {
-            uint32_t& slot = h.ell[k * np + mesh->conn[8 * e + k]];
-            if (slot != ENSC_NONE) {
-                h.clash = true;
-                break;
-            }
-            slot = static_cast<uint32_t>(e);
-        }
     if (!h.clash) {
+        for (int k = 0; k < 8; ++k)
+            for (int64_t e = 0; e < ne; ++e) h.ell[k * np + conn[8 * e + k]] = static_cast<uint32_t>(e);
         h.slot_mask.assign(static_cast<size_t>(np), 0);
         for (int k = 0; k < 8; ++k)
             for (int64_t n = 0; n < nn; ++n)
                 if (h.ell[k * np + n] != ENSC_NONE) h.slot_mask[n] |= static_cast<uint8_t>(1u << k);
     } else {
+        // ell keeps the first element per (slot, node) as before; the lists
+        // carry all of them
+        for (int k = 0; k < 8; ++k)
+            for (int64_t e = 0; e < ne; ++e) {
+                uint32_t& slot = h.ell[k * np + conn[8 * e + k]];
+                if (slot == ENSC_NONE) slot = static_cast<uint32_t>(e);
+            }
         h.csr_ptr.assign(static_cast<size_t>(nn + 1), 0);
-        for (int64_t i = 0; i < 8 * ne; ++i) h.csr_ptr[mesh->conn[i] + 1] += 1;
+        for (int64_t i = 0; i < 8 * ne; ++i) h.csr_ptr[conn[i] + 1] += 1;
         for (int64_t n = 0; n < nn; ++n) h.csr_ptr[n + 1] += h.csr_ptr[n];
         h.csr_ent.resize(static_cast<size_t>(8 * ne));
         std::vector<int64_t> fill(h.csr_ptr.begin(), h.csr_ptr.end() - 1);
         for (int k = 0; k < 8; ++k)
             for (int64_t e = 0; e < ne; ++e) {
-                const uint32_t n = mesh->conn[8 * e + k];
+                const uint32_t n = conn[8 * e + k];
                 h.csr_ent[fill[n]++] = (static_cast<uint32_t>(e) << 3) | static_cast<uint32_t>(k);
             }
     }
@@ -200,6 +344,16 @@ int instance_prepare(const ensc_mesh_desc* mesh, const ensc_material* mat, bool 
     h.size[P::CPTR] = h.clash ? static_cast<size_t>(nn + 1) * sizeof(int64_t) : 0;
     h.size[P::CENT] = h.clash ? static_cast<size_t>(8 * ne) * sizeof(uint32_t) : 0;
     h.size[P::MASK] = h.clash ? 0 : N8;
+    if (h.patch) {
+        h.size[P::IPERM] = static_cast<size_t>(ne) * sizeof(int32_t);
+        h.size[P::PFOFF] = static_cast<size_t>(h.n_patches + 1) * sizeof(uint32_t);
+        h.size[P::PINCOFF] = static_cast<size_t>(h.n_pnodes + 1) * sizeof(uint32_t);
+        h.size[P::PINC] = static_cast<size_t>(8 * ne) * sizeof(uint16_t);
+        h.size[P::PF] = 3 * static_cast<size_t>(pad32(h.n_pnodes)) * sizeof(float);
+        // node groups read nptr[n0 .. n0 + W] with n0 + W <= nn_pad
+        h.size[P::NPTR] = (N8 + 1) * sizeof(uint32_t);
+        h.size[P::NENT] = static_cast<size_t>(h.n_pnodes) * sizeof(uint32_t);
+    }
     size_t total = 0;
     for (int i = 0; i < P::NPIECE; ++i) {
         h.off[i] = total;
@@ -272,6 +426,18 @@ int instance_upload(const InstanceHost& h, void* block, cudaStream_t st, ElemArr
     } else {
         if (e == cudaSuccess) e = put(block, h.off[P::MASK], h.slot_mask, st);
     }
+    std::vector<uint32_t> nptr_pad;
+    if (h.patch) {
+        // padding nodes have no partials: nptr stays at the total past nn
+        nptr_pad.assign(static_cast<size_t>(np + 1), h.nptr.empty() ? 0u : h.nptr.back());
+        std::copy(h.nptr.begin(), h.nptr.end(), nptr_pad.begin());
+        if (e == cudaSuccess) e = put(block, h.off[P::IPERM], h.iperm, st);
+        if (e == cudaSuccess) e = put(block, h.off[P::PFOFF], h.pf_off, st);
+        if (e == cudaSuccess) e = put(block, h.off[P::PINCOFF], h.pinc_off, st);
+        if (e == cudaSuccess) e = put(block, h.off[P::PINC], h.pinc, st);
+        if (e == cudaSuccess) e = put(block, h.off[P::NPTR], nptr_pad, st);
+        if (e == cudaSuccess) e = put(block, h.off[P::NENT], h.nent, st);
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
         err = std::string("instance upload: ") + cudaGetErrorString(e);
@@ -291,6 +457,15 @@ int instance_upload(const InstanceHost& h, void* block, cudaStream_t st, ElemArr
     E.fe = b + h.off[P::FE];
     E.tiles_aligned = 1;  // pieces are 256-byte aligned, ne_pad % 32 == 0
     E.slot_major = h.clash ? 0 : 1;
+    if (h.patch) {
+        E.patch = 1;
+        E.pf_off = reinterpret_cast<uint32_t*>(b + h.off[P::PFOFF]);
+        E.pinc_off = reinterpret_cast<uint32_t*>(b + h.off[P::PINCOFF]);
+        E.pinc = reinterpret_cast<uint16_t*>(b + h.off[P::PINC]);
+        E.pf = reinterpret_cast<float*>(b + h.off[P::PF]);
+        E.pf_pad = pad32(h.n_pnodes);
+        E.iperm = reinterpret_cast<int32_t*>(b + h.off[P::IPERM]);
+    }
     N = NodeArrays{};
     N.nn = h.nn;
     N.nn_pad = np;
@@ -305,6 +480,10 @@ int instance_upload(const InstanceHost& h, void* block, cudaStream_t st, ElemArr
     N.csr_ent = h.clash ? reinterpret_cast<uint32_t*>(b + h.off[P::CENT]) : nullptr;
     N.rf = reinterpret_cast<double*>(b + h.off[P::RF]);
     N.slot_mask = h.clash ? nullptr : reinterpret_cast<uint8_t*>(b + h.off[P::MASK]);
+    if (h.patch) {
+        N.nptr = reinterpret_cast<uint32_t*>(b + h.off[P::NPTR]);
+        N.nent = reinterpret_cast<uint32_t*>(b + h.off[P::NENT]);
+    }
     return ENSC_OK;
 }
 

@@ -29,8 +29,21 @@ struct InstanceHost {
     std::vector<uint32_t> csr_ent;
     const double* x0 = nullptr;       // caller arrays, read during upload
     const double* v0 = nullptr;
+    // patch assembly (ElemArrays::patch): the stored order of the elements
+    // and the patch tables; all element arrays above are in stored order
+    bool patch = false;
+    std::vector<int32_t> iperm;       // [ne] element of the caller's numbering -> stored position
+    std::vector<uint32_t> pf_off;     // [n_patches + 1]
+    std::vector<uint32_t> pinc_off;   // [n_pnodes + 1]
+    std::vector<uint16_t> pinc;       // [8 ne]
+    std::vector<uint32_t> nptr;       // [nn + 1]
+    std::vector<uint32_t> nent;       // [n_pnodes]
+    int64_t n_patches = 0, n_pnodes = 0;
     // device layout: byte offsets of the pieces in one 256-byte-aligned block
-    enum Piece { CONN, BT, VOL0, CB, CB2, SIG, QIA, EPS, FE, X, U, V, IM, BC, BCV, ELL, RF, CPTR, CENT, MASK, NPIECE };
+    enum Piece {
+        CONN, BT, VOL0, CB, CB2, SIG, QIA, EPS, FE, X, U, V, IM, BC, BCV, ELL, RF, CPTR, CENT, MASK,
+        IPERM, PFOFF, PINCOFF, PINC, PF, NPTR, NENT, NPIECE
+    };
     size_t off[NPIECE] = {};
     size_t size[NPIECE] = {};
     size_t bytes = 0;
@@ -38,8 +51,18 @@ struct InstanceHost {
 
 // Validates the mesh and fills `h` (element constants computed as
 // compute_invMassMatrix does unless the caller supplies them).
-int instance_prepare(const ensc_mesh_desc* mesh, const ensc_material* mat, bool mixed, InstanceHost& h,
-                     std::string& err);
+int instance_prepare(const ensc_mesh_desc* mesh, const ensc_material* mat, bool mixed, int assembly,
+                     InstanceHost& h, std::string& err);
+
+// Stored order of the patch assembly: elements sorted by the Morton key of
+// their centroid's cell on a grid of the smallest element extent per axis,
+// so that runs of kPatchElems stored elements are compact clusters.  Returns
+// perm[stored position] = element of the caller's numbering.
+std::vector<int32_t> patch_order(int64_t ne, const uint32_t* conn, const double* x0);
+
+// Builds the patch tables of h (pf_off, pinc_off, pinc, nptr, nent) for the
+// stored connectivity conn [ne][8].
+void build_patches(int64_t nn, int64_t ne, const uint32_t* conn, InstanceHost& h);
 
 // Copies the instance into `block` (h.bytes bytes, 256-byte aligned) on
 // stream `st`, waits for the copies, and fills the array descriptors.

@@ -175,10 +175,12 @@ void launch_apply_bc_v(const NodeArrays& N, bool fp32_v, cudaStream_t st);
 void launch_reset_init(Ctl* ctl, cudaStream_t st);
 void launch_kinetic0(const NodeArrays& N, const Partials& P, Ctl* ctl, bool fp32_v, int grid, cudaStream_t st);
 // layout conversion between caller AoS arrays and device SoA arrays
+// `at` (may be null): entry e of the interleaved array is SoA row position
+// at[e] -- an element's stored position under the patch order
 void launch_soa_to_aos(const void* soa, int64_t n, int64_t pad, int comps, bool src_fp32, double* aos,
-                       cudaStream_t st);
+                       cudaStream_t st, const int32_t* at = nullptr);
 void launch_aos_to_soa(const double* aos, int64_t n, int64_t pad, int comps, void* soa, bool dst_fp32,
-                       cudaStream_t st);
+                       cudaStream_t st, const int32_t* at = nullptr);
 // velocities (FP64 rows, or the mixed stepper's float rows and residual rows)
 // to and from interleaved xyz doubles
 void launch_v_to_aos(const NodeArrays& N, bool fp32_v, double* aos, cudaStream_t st);

@@ -177,11 +177,14 @@ __device__ __forceinline__ void corner_values(T (&c)[8], T (&a)[8]) {
 // from S, outputs go to the instance's arrays at element e.
 // PF: node rows prefetched into L1 at the start (bit 0 velocities, bit 1
 // coordinate components 1 and 2).
-template <bool PLASTIC, bool INIT, bool SMEM = false, int PF = 0>
+// FOUT: the 24 nodal forces go to fout[3 * 8] (component-major) instead of
+// the instance's force array, for the patch assembly.
+template <bool PLASTIC, bool INIT, bool SMEM = false, int PF = 0, bool FOUT = false>
 __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const NodeArrays& N, const Material& M,
                                                    const MixedSrc& S, const float dt1, const double dt1d,
                                                    const int64_t e, double& dts, double& len, double& e_int,
-                                                   double& e_hg, double& e_vis, int32_t& bad) {
+                                                   double& e_hg, double& e_vis, int32_t& bad,
+                                                   float* fout = nullptr) {
     const int64_t ep = E.ne_pad, np = N.nn_pad, ss = S.stride, si = S.i;
     float* sig = static_cast<float*>(E.sigma);
     float* qia = static_cast<float*>(E.qia);
@@ -475,7 +478,8 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
         corner_values(c, f);
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
-            if (E.slot_major) fe[(3 * j + i) * np + nk[j]] = f[j];
+            if (FOUT) fout[8 * i + j] = f[j];
+            else if (E.slot_major) fe[(3 * j + i) * np + nk[j]] = f[j];
             else fe[(3 * j + i) * ep + e] = f[j];
         }
     }
@@ -649,6 +653,134 @@ __global__ void __launch_bounds__(kStageTile, ENSC_STAGE_MINB_MIXED)
     block_sum_d<kStageTile, 3, 7u>(v3, P.elem, P.n_elem_blocks, blockIdx.x);
 }
 
+// ---- staged element pass with patch assembly ----------------------------
+// k_element_mixed_staged with one patch per tile.  After its element body a
+// thread holds its element's 24 nodal forces; once the whole block is done
+// with the stage's inputs, the forces go into the stage's memory as
+// [3][8 slots][kStageTile elements], and the block sums each of the patch's
+// nodes over its incidences in slot order (starting from zero) and writes the
+// node's partial to E.pf.  INIT: the init force pass (dt = 0, no state
+// written, no energy).
+static_assert(kStageTile == kPatchElems, "one patch per staged tile");
+static_assert(3u * 8u * kStageTile * 4u <= kStageBytes, "the element forces fit in a stage");
+
+__device__ __forceinline__ void patch_partials(const ElemArrays& E, const float* sf, int64_t t, int tid) {
+    const uint32_t q0 = __ldg(E.pf_off + t), q1 = __ldg(E.pf_off + t + 1);
+    for (uint32_t q = q0 + tid; q < q1; q += kStageTile) {
+        const uint32_t a = __ldg(E.pinc_off + q), b = __ldg(E.pinc_off + q + 1);
+        float f0 = 0.f, f1 = 0.f, f2 = 0.f;
+        for (uint32_t r = a; r < b; ++r) {
+            const uint32_t u = __ldg(E.pinc + r);
+            const uint32_t col = (u & 7u) * kStageTile + (u >> 3);
+            f0 += sf[col];
+            f1 += sf[8 * kStageTile + col];
+            f2 += sf[16 * kStageTile + col];
+        }
+        E.pf[q] = f0;
+        E.pf[E.pf_pad + q] = f1;
+        E.pf[2 * E.pf_pad + q] = f2;
+    }
+}
+
+template <bool PLASTIC, bool INIT>
+__global__ void __launch_bounds__(kStageTile, ENSC_STAGE_MINB_MIXED)
+    k_element_mixed_patch(ElemArrays E, NodeArrays N, Material M, Ctl* ctl, Partials P) {
+    if (ctl->done) return;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const float dt1 = INIT ? 0.f : static_cast<float>(ctl->dt_i_1);
+    const double dt1d = INIT ? 0.0 : ctl->dt_i_1;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const uint32_t stage0 = smem_addr(smem);
+    const uint32_t bar0 = stage0 + 2 * kStageBytes;
+    const int64_t ntiles = (E.ne + kStageTile - 1) / kStageTile;
+    const int64_t gstride = gridDim.x;
+    if (tid == 0) {
+        mbar_init(bar0, 1);
+        mbar_init(bar0 + 8, 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    if (wid == 0) {
+        for (int s = 0; s < 2; ++s) {
+            const int64_t t = blockIdx.x + s * gstride;
+            if (t < ntiles) stage_issue<PLASTIC>(E, stage0 + s * kStageBytes, bar0 + 8 * s, t * kStageTile, lane);
+        }
+    }
+    double e_int = 0.0, e_hg = 0.0, e_vis = 0.0;
+    double dts_min = DBL_MAX, len_min = DBL_MAX;
+    int32_t bad = 0;
+    bool timed_out = false;
+    int it = 0;
+    for (int64_t t = blockIdx.x; t < ntiles; t += gstride, ++it) {
+        const int s = it & 1;
+        const uint32_t bar = bar0 + 8 * s;
+        const bool ok = mbar_wait_bounded(bar, (it >> 1) & 1);
+        if (__syncthreads_or(!ok)) {
+            timed_out = true;
+            break;
+        }
+        const int64_t e = t * kStageTile + tid;
+        const bool live = e < E.ne;
+        float fo[24];
+        if (live) {
+            const float* st = reinterpret_cast<const float*>(smem + s * kStageBytes);
+            const MixedSrc S{reinterpret_cast<const uint32_t*>(st),
+                             st + 8 * kStageTile,
+                             reinterpret_cast<const double*>(smem + s * kStageBytes + kStageV0Off),
+                             st + 44 * kStageTile,
+                             st + 26 * kStageTile,
+                             st + 32 * kStageTile,
+                             st + 45 * kStageTile,
+                             kStageTile,
+                             tid};
+            double dts, len;
+            element_body_mixed<PLASTIC, INIT, true, ENSC_MIXED_PREFETCH, true>(E, N, M, S, dt1, dt1d, e, dts, len,
+                                                                               e_int, e_hg, e_vis, bad, fo);
+            dts_min = fmin(dts_min, dts);
+            len_min = fmin(len_min, len);
+        }
+        __syncthreads();  // the stage's inputs are consumed
+        float* sf = reinterpret_cast<float*>(smem + s * kStageBytes);
+        if (live) {
+#pragma unroll
+            for (int i = 0; i < 24; ++i) sf[i * kStageTile + tid] = fo[i];
+        }
+        __syncthreads();
+        patch_partials(E, sf, t, tid);
+        __syncthreads();  // the block is done with stage s
+        const int64_t tn = t + 2 * gstride;
+        if (wid == 0 && tn < ntiles) stage_issue<PLASTIC>(E, stage0 + s * kStageBytes, bar, tn * kStageTile, lane);
+    }
+    if (timed_out) {
+        if (tid == 0) {
+            atomicOr(&ctl->status, ST_TIMEOUT);
+            for (int k = 0; k < 2; ++k) {
+                const int itk = it + k;
+                if (blockIdx.x + itk * gstride < ntiles) mbar_wait_bounded(bar0 + 8 * (itk & 1), (itk >> 1) & 1);
+            }
+        }
+        __syncthreads();
+    }
+    if (bad) atomicOr(&ctl->status, bad);
+    block_min2_d<kStageTile>(dts_min, len_min, &ctl->dts_next, &ctl->len_min);
+    if (!INIT) {
+        double v3[3] = {e_int, e_hg, e_vis};
+        block_sum_d<kStageTile, 3, 7u>(v3, P.elem, P.n_elem_blocks, blockIdx.x);
+    }
+}
+
+// One node's force under the patch assembly: its partials in patch order,
+// from zero.
+__device__ __forceinline__ void patch_gather(const ElemArrays& E, const NodeArrays& N, int64_t n, float (&f)[3]) {
+    const int64_t pp = E.pf_pad;
+    for (uint32_t r = __ldg(N.nptr + n), b = __ldg(N.nptr + n + 1); r < b; ++r) {
+        const uint32_t q = __ldg(N.nent + r);
+        f[0] += __ldg(E.pf + q);
+        f[1] += __ldg(E.pf + pp + q);
+        f[2] += __ldg(E.pf + 2 * pp + q);
+    }
+}
+
 // v + (dt_i + dt_i_1) / 2 * f * M^-1 in FP32 with the half step and the
 // inverse mass as float pairs: both are the same for many nodes and cycles,
 // so their FP32 rounding would scale all accelerations alike.
@@ -686,7 +818,9 @@ __device__ __forceinline__ void node_body_mixed(const ElemArrays& E, const NodeA
     const double dt_avg = 0.5 * (dt_i + dt_i_1);
 
     float f[3] = {0.f, 0.f, 0.f};
-    if (E.slot_major) {
+    if (E.patch) {
+        patch_gather(E, N, n, f);
+    } else if (E.slot_major) {
         const uint32_t msk = N.slot_mask[n];
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
@@ -765,7 +899,7 @@ __device__ __forceinline__ void node_body_mixed(const ElemArrays& E, const NodeA
 // hold: the slot-major rows start zeroed and only the slot's element writes
 // them.  Nodes at or past nn (row padding) are loaded and stored back
 // unchanged.
-template <int W>
+template <int W, bool PATCH>
 __device__ __forceinline__ void node_group_mixed(const NodeView& N, const double dt_i, const double dt_i_1,
                                                  const double amp, const int64_t n0, double& kin, double& wext,
                                                  int32_t& bad) {
@@ -780,20 +914,39 @@ __device__ __forceinline__ void node_group_mixed(const NodeView& N, const double
     for (int c = 0; c < 3; ++c)
 #pragma unroll
         for (int j = 0; j < W; ++j) f[c][j] = 0.f;
-    const uint32_t msk = ENSC_NODE_ALL_SLOTS ? 0xffffffffu : ld_bytes<W>(N.slot_mask + n0);
+    if constexpr (PATCH) {
+        // patch assembly: the node's partials in patch order
+        uint32_t lo[W], bnd[W + 1];
+        ld_row<W>(N.nptr + n0, lo);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        uint32_t sel = 0;
+        for (int j = 0; j < W; ++j) bnd[j] = lo[j];
+        bnd[W] = __ldg(N.nptr + n0 + W);
+        const int64_t pp = N.pf_pad;
 #pragma unroll
-        for (int j = 0; j < W; ++j) sel |= ((msk >> (8 * j + k)) & 1u) << j;
-        if (sel) {
+        for (int j = 0; j < W; ++j) {
+            for (uint32_t r = bnd[j]; r < bnd[j + 1]; ++r) {
+                const uint32_t q = __ldg(N.nent + r);
+                f[0][j] += __ldg(N.pf + q);
+                f[1][j] += __ldg(N.pf + pp + q);
+                f[2][j] += __ldg(N.pf + 2 * pp + q);
+            }
+        }
+    } else {
+        const uint32_t msk = ENSC_NODE_ALL_SLOTS ? 0xffffffffu : ld_bytes<W>(N.slot_mask + n0);
 #pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                float r[W];
-                ld_row<W>(fe + (3 * k + c) * np + n0, r);
+        for (int k = 0; k < 8; ++k) {
+            uint32_t sel = 0;
 #pragma unroll
-                for (int j = 0; j < W; ++j)
-                    if ((sel >> j) & 1u) f[c][j] += r[j];
+            for (int j = 0; j < W; ++j) sel |= ((msk >> (8 * j + k)) & 1u) << j;
+            if (sel) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    float r[W];
+                    ld_row<W>(fe + (3 * k + c) * np + n0, r);
+#pragma unroll
+                    for (int j = 0; j < W; ++j)
+                        if ((sel >> j) & 1u) f[c][j] += r[j];
+                }
             }
         }
     }
@@ -891,7 +1044,13 @@ __global__ void __launch_bounds__(kNodeThreads, ENSC_NODE_MINB_MIXED) k_node_mix
     if (E.slot_major && E.tiles_aligned) {
         constexpr int W = kNodeGroupMixed;
         const NodeView nv = node_view(E, N, M, ctl);
-        for (int64_t g = t0; g * W < nn; g += stride) node_group_mixed<W>(nv, dt_i, dt_i_1, amp, g * W, kin, wext, bad);
+        if (E.patch) {
+            for (int64_t g = t0; g * W < nn; g += stride)
+                node_group_mixed<W, true>(nv, dt_i, dt_i_1, amp, g * W, kin, wext, bad);
+        } else {
+            for (int64_t g = t0; g * W < nn; g += stride)
+                node_group_mixed<W, false>(nv, dt_i, dt_i_1, amp, g * W, kin, wext, bad);
+        }
     } else {
         for (int64_t n = t0; n < nn; n += stride) node_body_mixed(E, N, M, dt_i, dt_i_1, amp, n, kin, wext, bad);
     }
@@ -914,7 +1073,9 @@ __global__ void __launch_bounds__(kNodeThreads) k_acceleration_mixed(ElemArrays 
     for (int64_t n = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; n < N.nn;
          n += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         float f[3] = {0.f, 0.f, 0.f};
-        if (E.slot_major) {
+        if (E.patch) {
+            patch_gather(E, N, n, f);
+        } else if (E.slot_major) {
             const uint32_t msk = grouped ? 0xffu : N.slot_mask[n];
 #pragma unroll
             for (int k = 0; k < 8; ++k)
@@ -1107,6 +1268,9 @@ __global__ void __launch_bounds__(kStageTile, ENSC_BATCH_MINB_MIXED) k_element_b
             run_live = h.live != 0;
         }
         const int64_t e = static_cast<int64_t>(ti.base) + tid;
+        const bool patch = d.E.patch != 0;  // uniform over the tile
+        const ElemArrays* pe = patch ? &d.E : nullptr;
+        float fo[24];
         if (run_live && e < d.E.ne) {
 #if ENSC_BATCH_DESC_MODE == 1
             // the instance's arrays and constants, read from the stage once:
@@ -1138,9 +1302,36 @@ __global__ void __launch_bounds__(kStageTile, ENSC_BATCH_MINB_MIXED) k_element_b
                              kStageTile,
                              tid};
             double d1, l1;
-            element_body_mixed<true, false, true>(E, N, M, S, dt1, dt1d, e, d1, l1, ei, eh, ev, bad);
+            element_body_mixed<true, false, true, 0, true>(E, N, M, S, dt1, dt1d, e, d1, l1, ei, eh, ev, bad, fo);
             dts = fmin(dts, d1);
             len = fmin(len, l1);
+            if (!patch) {
+                // slot assembly: the forces to the instance's force array
+                float* __restrict__ fe = static_cast<float*>(E.fe);
+                const int64_t np = N.nn_pad, ep = E.ne_pad;
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const uint32_t nj = S.conn[j * kStageTile + tid];
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+                        if (E.slot_major) fe[(3 * j + i) * np + nj] = fo[8 * i + j];
+                        else fe[(3 * j + i) * ep + e] = fo[8 * i + j];
+                    }
+                }
+            }
+        }
+        if (patch && run_live) {
+            // the tile's patch: its forces summed per patch node (see
+            // k_element_mixed_patch); the stage's element rows hold them
+            const ElemArrays PE = *pe;
+            __syncthreads();  // the stage's inputs are consumed
+            float* sf = reinterpret_cast<float*>(sb);
+            if (e < PE.ne) {
+#pragma unroll
+                for (int i = 0; i < 24; ++i) sf[i * kStageTile + tid] = fo[i];
+            }
+            __syncthreads();
+            patch_partials(PE, sf, static_cast<int64_t>(ti.base) / kPatchElems, tid);
         }
         __syncthreads();  // the block is done with stage s
         const int64_t tn = t + 2 * gstride;
@@ -1195,8 +1386,10 @@ __global__ void __launch_bounds__(NT, ENSC_NODE_BATCH_MINB_MIXED * kNodeThreads 
             int32_t bad = 0;
             const int64_t n0 = static_cast<int64_t>(base) + static_cast<int64_t>(lane) * W;
             if (n0 < v.nn) {
-                if (v.grouped) {
-                    node_group_mixed<W>(v, dt_i, dt_i_1, amp, n0, kin, wext, bad);
+                if (v.grouped == 2) {
+                    node_group_mixed<W, true>(v, dt_i, dt_i_1, amp, n0, kin, wext, bad);
+                } else if (v.grouped) {
+                    node_group_mixed<W, false>(v, dt_i, dt_i_1, amp, n0, kin, wext, bad);
                 } else {
                     const InstanceDesc& d = T.desc[slot];
                     for (int j = 0; j < W && n0 + j < v.nn; ++j)
@@ -1224,6 +1417,16 @@ __global__ void __launch_bounds__(NT, ENSC_NODE_BATCH_MINB_MIXED * kNodeThreads 
 
 void launch_element_mixed(const ElemArrays& E, const NodeArrays& N, const Material& M, Ctl* ctl, const Partials& P,
                           int grid, bool init, cudaStream_t st) {
+    if (E.patch) {
+        if (M.plastic) {
+            if (init) k_element_mixed_patch<true, true><<<grid, kStageTile, kStageSmem, st>>>(E, N, M, ctl, P);
+            else k_element_mixed_patch<true, false><<<grid, kStageTile, kStageSmem, st>>>(E, N, M, ctl, P);
+        } else {
+            if (init) k_element_mixed_patch<false, true><<<grid, kStageTile, kStageSmem, st>>>(E, N, M, ctl, P);
+            else k_element_mixed_patch<false, false><<<grid, kStageTile, kStageSmem, st>>>(E, N, M, ctl, P);
+        }
+        return;
+    }
     if (ENSC_STAGED_MIXED && !init && E.tiles_aligned) {
         if (M.plastic) k_element_mixed_staged<true><<<grid, kStageTile, kStageSmem, st>>>(E, N, M, ctl, P);
         else k_element_mixed_staged<false><<<grid, kStageTile, kStageSmem, st>>>(E, N, M, ctl, P);
@@ -1249,8 +1452,27 @@ void launch_node_mixed(const ElemArrays& E, const NodeArrays& N, const Material&
     k_node_mixed<<<grid, kNodeThreads, 0, st>>>(E, N, M, ctl, P);
 }
 
+// The staged passes need more than the default 48 KB of dynamic shared
+// memory; the attribute is set on the current device before any launch or
+// capture.
+void set_element_mixed_attributes() {
+    cudaFuncSetAttribute(k_element_mixed_staged<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(kStageSmem));
+    cudaFuncSetAttribute(k_element_mixed_staged<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(kStageSmem));
+    cudaFuncSetAttribute(k_element_mixed_patch<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(kStageSmem));
+    cudaFuncSetAttribute(k_element_mixed_patch<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(kStageSmem));
+    cudaFuncSetAttribute(k_element_mixed_patch<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(kStageSmem));
+    cudaFuncSetAttribute(k_element_mixed_patch<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(kStageSmem));
+}
+
 int occupancy_element_mixed(bool plastic) {
     int nb = 0;
+    set_element_mixed_attributes();
     if (ENSC_STAGED_MIXED) {
         // the staged pass needs more than the default 48 KB of dynamic shared
         // memory; the attribute is set here, on the current device, before
@@ -1286,6 +1508,7 @@ void launch_node_batch_mixed(const BatchTables& T, int grid, int threads, cudaSt
 }
 int occupancy_element_batch_mixed() {
     int nb = 0;
+    set_element_mixed_attributes();  // the batch's init passes run the single-instance kernels
     // dynamic shared memory above the default 48 KB: set on the current
     // device before any launch or capture
     cudaFuncSetAttribute(k_element_batch_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -60,12 +60,12 @@ class BatchBackend:
 
     def __init__(self, *, budget_bytes: int, max_instances: int = 1024, max_elements: int = 64 << 20,
                  max_nodes: int = 72 << 20, precision: Optional[int] = None, device: int = 0,
-                 fields: Sequence[str] = ("u",)):
+                 fields: Sequence[str] = ("u",), assembly: int = 0):
         from . import capi
         self._capi = capi
         self.batch = capi.Batch(max_instances=max_instances, max_elements=max_elements, max_nodes=max_nodes,
                                 budget_bytes=budget_bytes, precision=capi.MIXED if precision is None else precision,
-                                device=device)
+                                device=device, assembly=assembly)
         self.fields = tuple(fields)
 
     def add(self, problem) -> int:
@@ -82,7 +82,7 @@ class BatchBackend:
     def prepare(self, problem):
         p = problem
         return self._capi.Prepared(p.mesh.x0, p.mesh.conn, p.v0, material=p.material, controls=p.controls,
-                                   precision=self.batch.precision)
+                                   precision=self.batch.precision, assembly=self.batch.assembly)
 
     def add_prepared(self, token, problem) -> int:
         try:

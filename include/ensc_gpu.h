@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define ENSC_ABI_VERSION 1
+#define ENSC_ABI_VERSION 2
 
 /* return codes */
 #define ENSC_OK 0
@@ -49,6 +49,21 @@ extern "C" {
 /* precision of the stepper */
 #define ENSC_FP64 0     /* plain FP64, operation order of the reference */
 #define ENSC_MIXED 1    /* FP32 element work and gather; FP64 x, u, time, dt, energy */
+
+/* Force assembly (ensc_params.assembly).  SLOT: every element writes its 8
+ * nodal forces to the reference's per-local-slot nodal vectors and the node
+ * pass adds the 8 slots in order, ((a0 + a1) + ...) + a7, as the reference
+ * does (exDyna3D.cpp:589-639).  PATCH (mixed precision, meshes where no node
+ * repeats a local slot): elements are stored in spatially compact patches
+ * of 64 (Morton order of their centroids); the element pass sums each
+ * patch's forces per patch node in shared memory and the node pass adds the
+ * ~1.5-1.8 patch partials of each node in patch order -- 30% fewer bytes per
+ * cycle, different FP32 rounding, but on B200 a slower element pass (the
+ * per-patch sums serialise each tile behind two more block barriers and
+ * dependent table reads).  AUTO: SLOT. */
+#define ENSC_ASSEMBLY_AUTO 0
+#define ENSC_ASSEMBLY_SLOT 1
+#define ENSC_ASSEMBLY_PATCH 2
 
 /* BC code bits per DOF, as resolved by apply_boundary_condition_vec /
  * apply_boundary_condition_a (exDyna3D.cpp:379-490, 2029-2145) */
@@ -98,6 +113,7 @@ typedef struct {
     int32_t device;         /* CUDA device ordinal */
     void* stream;           /* cudaStream_t to run on, or NULL for a private stream */
     int32_t graph_chunk;    /* cycles per captured CUDA graph; 0 = default */
+    int32_t assembly;       /* ENSC_ASSEMBLY_*; 0 = AUTO */
 } ensc_params;
 
 typedef struct {
@@ -241,6 +257,11 @@ int64_t ensc_device_bytes(const ensc_handle* h);
 /* Number of kernel launches one cycle issues (for launch accounting). */
 int32_t ensc_kernels_per_cycle(const ensc_handle* h);
 
+/* The force assembly the instance uses (ENSC_ASSEMBLY_SLOT or _PATCH), and
+ * for PATCH its number of patches and of (patch, node) partials; any
+ * pointer may be NULL. */
+int ensc_assembly(const ensc_handle* h, int32_t* assembly, int64_t* patches, int64_t* partials);
+
 void ensc_destroy(ensc_handle* h);
 
 /* ---- batches of independent solves --------------------------------------
@@ -274,7 +295,8 @@ int ensc_batch_add(ensc_batch* b, const ensc_mesh_desc* mesh, const ensc_materia
 /* ensc_batch_add in two parts, so that the host work of an arriving solve
  * can overlap the batch's running cycles.  ensc_batch_prepare does the host
  * part -- checks the mesh and material and computes the element constants,
- * lumped mass and node tables for `precision` -- on the calling thread and
+ * lumped mass and node tables for params->precision and params->assembly
+ * (the other fields are not read) -- on the calling thread and
  * makes no CUDA call, so it may run on any thread while a batch steps;
  * errors are reported through ensc_last_error(NULL) of that thread.  The
  * mesh's x0 and v0 arrays are read again by ensc_batch_add_prepared and must
@@ -283,9 +305,32 @@ int ensc_batch_add(ensc_batch* b, const ensc_mesh_desc* mesh, const ensc_materia
  * batch's) and leaves `prep` to the caller, who frees it with
  * ensc_prepared_destroy; the instance is the one ensc_batch_add would add. */
 typedef struct ensc_prepared ensc_prepared;
-int ensc_batch_prepare(const ensc_mesh_desc* mesh, const ensc_material* mat, int32_t precision, ensc_prepared** out);
+int ensc_batch_prepare(const ensc_mesh_desc* mesh, const ensc_material* mat, const ensc_params* params,
+                       ensc_prepared** out);
 int ensc_batch_add_prepared(ensc_batch* b, const ensc_prepared* prep, const ensc_params* controls, int32_t* slot);
 int64_t ensc_prepared_bytes(const ensc_prepared* prep);  /* device bytes the instance will take */
+/* The force assembly the instance uses (ENSC_ASSEMBLY_SLOT or _PATCH), and
+ * for PATCH its number of patches and of (patch, node) partials; any
+ * pointer may be NULL. */
+int ensc_prepared_assembly(const ensc_prepared* prep, int32_t* assembly, int64_t* patches, int64_t* partials);
+
+/* The host tables of a PATCH instance, for inspection; the pointers stay
+ * valid until ensc_prepared_destroy.  Patch p holds the elements stored at
+ * positions 64 p .. 64 p + 63 and the partials patch_first[p] ..
+ * patch_first[p + 1] - 1; partial q sums the incidences inc[inc_first[q] ..
+ * inc_first[q + 1]), each (element position in the patch << 3 | local slot);
+ * node n adds the partials node_partials[node_first[n] .. node_first[n + 1]).
+ * ENSC_ERR_ARG for a SLOT instance. */
+typedef struct {
+    int64_t n_elements, n_nodes, n_patches, n_partials;
+    const int32_t* stored;          /* [n_elements] element of the caller's numbering -> stored position */
+    const uint32_t* patch_first;    /* [n_patches + 1] */
+    const uint32_t* inc_first;      /* [n_partials + 1] */
+    const uint16_t* inc;            /* [8 n_elements] */
+    const uint32_t* node_first;     /* [n_nodes + 1] */
+    const uint32_t* node_partials;  /* [n_partials] */
+} ensc_patch_tables;
+int ensc_prepared_patch_tables(const ensc_prepared* prep, ensc_patch_tables* out);
 void ensc_prepared_destroy(ensc_prepared* prep);
 
 /* ensc_set_bcs for one instance. */

@@ -42,7 +42,7 @@ def test_binding_covers_every_declared_symbol():
 
 
 def test_abi_version(lib):
-    assert lib.ensc_abi_version() == 1
+    assert lib.ensc_abi_version() == 2
 
 
 def _desc(nn, ne, conn, x0):

@@ -251,3 +251,22 @@ def test_churn_with_short_runs_and_prepared_instances(precision):
         assert t["graph_cycles"] in (8, 32)
     for i, c in enumerate(cases):
         assert_same(*got[i], refs[i], c.name)
+
+
+@pytest.mark.parametrize("assembly", [capi.ASSEMBLY_SLOT, capi.ASSEMBLY_PATCH])
+def test_mixed_batch_matches_single_under_each_assembly(assembly):
+    cases = [sweep_case(50, 260), sweep_case(51, 190, plastic=False), sweep_case(52, 330)]
+    refs = []
+    for c in cases:
+        with capi.Stepper(c.x0, c.conn, c.v0, material=c.mat, controls=c.ctl, precision=capi.MIXED,
+                          assembly=assembly) as s:
+            s.set_bcs(c.code, c.val)
+            rep = s.step(c.cycles)
+            refs.append((s.download(), rep, s.energy()))
+    with make_batch(capi.MIXED, assembly=assembly) as b:
+        ss = [add(b, c) for c in cases]
+        for s, c in zip(ss, cases):
+            b.arm(s, c.cycles)
+        drain(b)
+        for s, c, ref in zip(ss, cases, refs):
+            assert_same(b.download(s), b.report(s), b.energy(s), ref, c.name)

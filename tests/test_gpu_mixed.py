@@ -153,3 +153,66 @@ def test_mixed_full_block_at_workload_cycles():
     drift = abs(energy_balance(emx) - energy_balance(e64)) / e64["kinetic0"]
     assert err <= DISP_TOL, err
     assert drift <= ENERGY_TOL, drift
+
+
+def _run_mixed(p, cycles, assembly, precision=capi.MIXED):
+    with capi.Stepper(p.mesh.x0, p.mesh.conn, p.v0, material=p.material, controls=p.controls,
+                      precision=precision, assembly=assembly) as s:
+        s.set_bcs(p.bc_code, p.bc_value)
+        rep = s.step(cycles)
+        assert rep["status"] == 0 and rep["cycles"] == cycles
+        return s.download(), s.energy()
+
+
+def test_patch_and_slot_assembly_agree():
+    """The mixed stepper's two force assemblies -- PATCH (per-patch sums in
+    shared memory, elements stored in patch order) and SLOT (the reference's
+    per-slot nodal vectors) -- differ only in the FP32 order of the force
+    sums.  After 500 cycles of a J2 block with uneven sides both meet the FP64
+    bar, they agree with each other well inside it, and the element fields
+    come back in the caller's numbering (a wrong order would differ by the
+    whole field)."""
+    p = W.block(21, 11, 7, 0.21, 0.11, 0.07, plastic=True)
+    st64, e64 = _run_mixed(p, 500, capi.ASSEMBLY_AUTO, capi.FP64)
+    stp, ep = _run_mixed(p, 500, capi.ASSEMBLY_PATCH)
+    sts, es = _run_mixed(p, 500, capi.ASSEMBLY_SLOT)
+    scale = np.abs(st64["u"]).max()
+    for st, e in ((stp, ep), (sts, es)):
+        assert np.abs(st["u"] - st64["u"]).max() / scale <= DISP_TOL
+        drift = abs(energy_balance(e) - energy_balance(e64)) / e64["kinetic0"]
+        assert drift <= ENERGY_TOL, drift
+    assert np.abs(stp["u"] - sts["u"]).max() / scale <= 1e-6
+    for k in ("sigma", "qia"):
+        ref = np.abs(st64[k]).max()
+        assert np.abs(stp[k] - st64[k]).max() <= 1e-3 * ref, k
+        assert np.abs(stp[k] - sts[k]).max() <= 1e-3 * ref, k
+    assert not np.array_equal(stp["u"], sts["u"])  # the assemblies really differ
+
+
+def test_patch_assembly_restarts_and_chunks_bit_exactly():
+    """Under the patch assembly, stepping in pieces and restarting a fresh
+    instance from a downloaded state reproduce one uninterrupted run bit for
+    bit (element state goes through the stored order both ways)."""
+    p = W.block(20, 9, 6, 0.2, 0.09, 0.06, plastic=True)
+
+    def stepper():
+        s = capi.Stepper(p.mesh.x0, p.mesh.conn, p.v0, material=p.material, controls=p.controls,
+                         precision=capi.MIXED, assembly=capi.ASSEMBLY_PATCH)
+        s.set_bcs(p.bc_code, p.bc_value)
+        return s
+    with stepper() as a:
+        a.step(400)
+        ref = a.download()
+    with stepper() as b:
+        b.step(150)
+        mid = b.download()
+        c1 = b.step(0)
+        b.step(250)
+        got = b.download()
+    with stepper() as c:
+        c.upload_state(mid, c1["time"], c1["dt_i"], c1["dt_i_1"], c1["dt_stable_min"])
+        c.step(250)
+        got2 = c.download()
+    for k in ("u", "v", "x", "sigma", "qia", "eps_p"):
+        assert np.array_equal(got[k], ref[k]), k
+        assert np.array_equal(got2[k], ref[k]), k

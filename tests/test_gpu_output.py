@@ -63,12 +63,14 @@ def test_snapshot_fields_and_acceleration_fp64(name):
     assert np.array_equal(sn["a"].reshape(-1), oracle_acceleration(o, g))
 
 
-def test_snapshot_acceleration_mixed():
+@pytest.mark.parametrize("assembly", [capi.ASSEMBLY_SLOT, capi.ASSEMBLY_PATCH])
+def test_snapshot_acceleration_mixed(assembly):
     g = load_golden("gravity_6x2x2")
     mat, ctl = material_controls(g["meta"])
     o = oracle_for(g)
     o.run(200)
-    with capi.Stepper(g["x0"], g["conn"], g["v0"], material=mat, controls=ctl, precision=capi.MIXED) as s:
+    with capi.Stepper(g["x0"], g["conn"], g["v0"], material=mat, controls=ctl, precision=capi.MIXED,
+                      assembly=assembly) as s:
         s.set_bcs(g["bc_code"], g["bc_value"])
         s.step(200)
         s.snapshot_begin()
