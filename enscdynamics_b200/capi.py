@@ -164,7 +164,7 @@ SIGNATURES = [
     ("ensc_batch_remove", C.c_int, [C.c_void_p, C.c_int32]),
     ("ensc_batch_device_bytes", C.c_int64, [C.c_void_p]),
     ("ensc_batch_instances", C.c_int32, [C.c_void_p]),
-    ("ensc_batch_tuning", C.c_int, [C.c_void_p] + [C.POINTER(C.c_int32)] * 4),
+    ("ensc_batch_tuning", C.c_int, [C.c_void_p] + [C.POINTER(C.c_int32)] * 6),
     ("ensc_batch_destroy", None, [C.c_void_p]),
     ("ensc_batch_last_error", C.c_char_p, [C.c_void_p]),
 ]
@@ -570,7 +570,9 @@ class Batch:
 
     @property
     def tuning(self) -> Dict[str, int]:
-        """The autotuner's launch choices (all 0 before the first run)."""
-        v = [C.c_int32() for _ in range(4)]
+        """The autotuner's launch choices (0 until its first tuning completes)
+        and the batch's force assembly."""
+        v = [C.c_int32() for _ in range(6)]
         self._check(self._lib.ensc_batch_tuning(self.h, *[C.byref(x) for x in v]))
-        return dict(zip(("mult_element", "mult_node", "graph_cycles", "node_threads"), (x.value for x in v)))
+        return dict(zip(("mult_element", "mult_node", "graph_cycles", "node_threads", "elements_per_thread",
+                         "assembly"), (x.value for x in v)))

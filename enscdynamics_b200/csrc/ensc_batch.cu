@@ -46,6 +46,7 @@ struct Slot {
 // and threads per block of the node pass.
 struct Tune {
     int mult_e = 1, mult_n = 1, chunk = 32, node_threads = ensc::kNodeThreads;
+    int ept = 1;  // elements per thread of the element pass
 };
 
 }  // namespace
@@ -93,7 +94,8 @@ struct ensc_batch {
     int64_t tune_etiles = 0;
     int tunings = 0;  // completed tunings
     cudaGraphExec_t graph = nullptr;
-    int graph_chunk = 0, graph_ge = 0, graph_gn = 0, graph_nt = 0;
+    int graph_chunk = 0, graph_ge = 0, graph_gn = 0, graph_nt = 0, graph_ept = 0;
+    int occ_e2 = 1;  // resident element-pass blocks per SM at 2 elements per thread (mixed)
     std::string err;
 };
 
@@ -223,11 +225,11 @@ int rebuild_tables(ensc_batch* b) {
     return ENSC_OK;
 }
 
-void launch_cycle(ensc_batch* b, int ge, int gn, int nt, cudaStream_t st) {
+void launch_cycle(ensc_batch* b, int ge, int gn, int nt, int ept, cudaStream_t st) {
     ensc::launch_between_batch(b->T, b->slots, 0, st);
     ensc::launch_edge_prepass_batch(b->T, b->sms * b->occ_pre, st);
     if (is_mixed(b)) {
-        ensc::launch_element_batch_mixed(b->T, ge, st);
+        ensc::launch_element_batch_mixed(b->T, ge, ept, st);
         ensc::launch_node_batch_mixed(b->T, gn, nt, st);
     } else {
         ensc::launch_element_batch_fp64(b->T, ge, st);
@@ -242,8 +244,10 @@ int occupancy_node(ensc_batch* b, int threads) {
 
 int build_graph(ensc_batch* b, const Tune& t) {
     const int nt = t.node_threads;
-    const int ge = b->sms * b->occ_e * t.mult_e, gn = b->sms * occupancy_node(b, nt) * t.mult_n;
-    if (b->graph && b->graph_chunk == t.chunk && b->graph_ge == ge && b->graph_gn == gn && b->graph_nt == nt)
+    const int ge = b->sms * (t.ept == 2 ? b->occ_e2 : b->occ_e) * t.mult_e;
+    const int gn = b->sms * occupancy_node(b, nt) * t.mult_n;
+    if (b->graph && b->graph_chunk == t.chunk && b->graph_ge == ge && b->graph_gn == gn && b->graph_nt == nt &&
+        b->graph_ept == t.ept)
         return ENSC_OK;
     if (b->graph) {
         cudaGraphExecDestroy(b->graph);
@@ -251,7 +255,7 @@ int build_graph(ensc_batch* b, const Tune& t) {
     }
     cudaGraph_t g = nullptr;
     BCK(b, cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal));
-    for (int c = 0; c < t.chunk; ++c) launch_cycle(b, ge, gn, nt, b->cap_stream);
+    for (int c = 0; c < t.chunk; ++c) launch_cycle(b, ge, gn, nt, t.ept, b->cap_stream);
     cudaError_t e = cudaStreamEndCapture(b->cap_stream, &g);
     if (e != cudaSuccess) return bcuda(b, "cudaStreamEndCapture", e);
     e = cudaGraphInstantiate(&b->graph, g, 0);
@@ -261,22 +265,32 @@ int build_graph(ensc_batch* b, const Tune& t) {
     b->graph_ge = ge;
     b->graph_gn = gn;
     b->graph_nt = nt;
+    b->graph_ept = t.ept;
     return ENSC_OK;
 }
 
-// Picks the launch geometry (grid sizes, node-pass block size) and graph
-// length with the shortest time per cycle on the batch as loaded.  The
-// candidates differ only in how work is spread over the GPU, not in
-// arithmetic, so the cycles they run are ordinary cycles of the solve
-// (results are identical whichever wins).  Each candidate runs one warm-up
+// Picks the launch geometry (grid sizes, node-pass block size, elements per
+// thread of the mixed element pass) and graph length with the shortest time
+// per cycle on the batch as loaded.  The candidates differ only in how work
+// is spread over the GPU, not in arithmetic, so the cycles they run are
+// ordinary cycles of the solve (the state is identical whichever wins; the
+// energy sums are grouped per warp, so with 2 elements per thread they may
+// differ in the last bits).  Each candidate runs one warm-up
 // graph launch and one timed launch; a run too short for the next candidate
 // continues with the best so far, and the next run goes on from there.
-constexpr int kTuneCands = 7;
+constexpr int kTuneCands = 9;
 Tune tune_candidate(int i) {
     constexpr int kN = ensc::kNodeThreads;
-    const Tune cand[kTuneCands] = {{1, 1, 32, kN},     {2, 1, 32, kN},     {1, 2, 32, kN}, {2, 2, 32, kN},
-                                   {1, 1, 32, kN / 2}, {1, 2, 32, kN / 2}, {1, 1, 8, kN}};
+    const Tune cand[kTuneCands] = {{1, 1, 32, kN, 1},     {2, 1, 32, kN, 1},     {1, 2, 32, kN, 1},
+                                   {2, 2, 32, kN, 1},     {1, 1, 32, kN / 2, 1}, {1, 2, 32, kN / 2, 1},
+                                   {1, 1, 8, kN, 1},      {1, 1, 32, kN, 2},     {2, 1, 32, kN, 2}};
     return cand[i];
+}
+
+// 2 elements per thread: mixed precision, slot assembly (the patch sums take
+// one element per thread)
+bool candidate_applies(const ensc_batch* b, const Tune& t) {
+    return t.ept == 1 || (is_mixed(b) && b->assembly != ENSC_ASSEMBLY_PATCH);
 }
 
 int autotune(ensc_batch* b, int64_t* cycles_left) {
@@ -286,6 +300,7 @@ int autotune(ensc_batch* b, int64_t* cycles_left) {
     int rc = ENSC_OK;
     for (; b->tune_next < kTuneCands; ++b->tune_next) {
         Tune t = tune_candidate(b->tune_next);
+        if (!candidate_applies(b, t)) continue;
         if (b->fixed_chunk > 0) t.chunk = b->fixed_chunk;
         if (*cycles_left < 2 * t.chunk) break;
         rc = build_graph(b, t);
@@ -373,7 +388,8 @@ int ensc_batch_create(const ensc_params* params, int32_t max_instances, int64_t 
     cudaDeviceProp prop{};
     if (cudaGetDeviceProperties(&prop, b->device) != cudaSuccess) return fail(berr(b, ENSC_ERR_CUDA, "device query"));
     b->sms = prop.multiProcessorCount;
-    b->occ_e = std::max(1, is_mixed(b) ? ensc::occupancy_element_batch_mixed() : ensc::occupancy_element_batch_fp64());
+    b->occ_e = std::max(1, is_mixed(b) ? ensc::occupancy_element_batch_mixed(1) : ensc::occupancy_element_batch_fp64());
+    b->occ_e2 = std::max(1, is_mixed(b) ? ensc::occupancy_element_batch_mixed(2) : 1);
     // arena: a memory pool that keeps released blocks for reuse
     cudaMemPoolProps pp{};
     pp.allocType = cudaMemAllocationTypePinned;
@@ -798,13 +814,15 @@ int ensc_batch_remove(ensc_batch* b, int32_t slot) {
 int64_t ensc_batch_device_bytes(const ensc_batch* b) { return b ? b->used : 0; }
 
 int ensc_batch_tuning(const ensc_batch* b, int32_t* mult_element, int32_t* mult_node, int32_t* graph_cycles,
-                      int32_t* node_threads) {
+                      int32_t* node_threads, int32_t* elements_per_thread, int32_t* assembly) {
     if (!b) return ENSC_ERR_ARG;
     const bool t = b->tunings > 0;
     if (mult_element) *mult_element = t ? b->tune.mult_e : 0;
     if (mult_node) *mult_node = t ? b->tune.mult_n : 0;
     if (graph_cycles) *graph_cycles = t ? b->tune.chunk : 0;
     if (node_threads) *node_threads = t ? b->tune.node_threads : 0;
+    if (elements_per_thread) *elements_per_thread = t ? b->tune.ept : 0;
+    if (assembly) *assembly = b->assembly == ENSC_ASSEMBLY_PATCH ? ENSC_ASSEMBLY_PATCH : ENSC_ASSEMBLY_SLOT;
     return ENSC_OK;
 }
 

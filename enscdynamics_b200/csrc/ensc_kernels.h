@@ -150,9 +150,9 @@ void launch_element_batch_fp64(const BatchTables& T, int grid, cudaStream_t st);
 void launch_node_batch_fp64(const BatchTables& T, int grid, int threads, cudaStream_t st);
 int occupancy_element_batch_fp64();
 int occupancy_node_batch_fp64(int threads);
-void launch_element_batch_mixed(const BatchTables& T, int grid, cudaStream_t st);
+void launch_element_batch_mixed(const BatchTables& T, int grid, int ept, cudaStream_t st);
 void launch_node_batch_mixed(const BatchTables& T, int grid, int threads, cudaStream_t st);
-int occupancy_element_batch_mixed();
+int occupancy_element_batch_mixed(int ept);
 int occupancy_node_batch_mixed(int threads);
 // elements and nodes per batch tile (element tiles are the staged passes'
 // tiles; node tiles are one warp of node groups)

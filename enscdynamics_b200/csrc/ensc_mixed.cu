@@ -1192,9 +1192,14 @@ __device__ __forceinline__ void batch_stage_issue(const BatchTables& T, const ET
     }
 }
 
-__global__ void __launch_bounds__(kStageTile, ENSC_BATCH_MINB_MIXED) k_element_batch_mixed(BatchTables T) {
+// EPT elements per thread: the block has kStageTile / EPT threads, and each
+// thread evaluates elements tid, tid + kStageTile / EPT, ... of a tile in
+// turn (a tuning choice; EPT > 1 only under the slot assembly).
+template <int EPT>
+__global__ void __launch_bounds__(kStageTile / EPT, ENSC_BATCH_MINB_MIXED) k_element_batch_mixed(BatchTables T) {
     extern __shared__ __align__(128) unsigned char smem[];
-    constexpr int NW = kStageTile / 32;
+    constexpr int NW = kStageTile / 32;  // energy partial slots per tile
+    constexpr int NT = kStageTile / EPT;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const uint32_t stage0 = smem_addr(smem);
     const uint32_t bar0 = stage0 + 2 * kBatchStageBytes;
@@ -1267,55 +1272,60 @@ __global__ void __launch_bounds__(kStageTile, ENSC_BATCH_MINB_MIXED) k_element_b
             run_ctl = d.ctl;
             run_live = h.live != 0;
         }
-        const int64_t e = static_cast<int64_t>(ti.base) + tid;
-        const bool patch = d.E.patch != 0;  // uniform over the tile
+        const bool patch = EPT == 1 && d.E.patch != 0;  // uniform over the tile
         const ElemArrays* pe = patch ? &d.E : nullptr;
         float fo[24];
-        if (run_live && e < d.E.ne) {
+        int64_t e = 0;
+#pragma unroll 1
+        for (int k = 0; k < EPT; ++k) {
+            const int li = tid + k * NT;
+            e = static_cast<int64_t>(ti.base) + li;
+            if (run_live && e < d.E.ne) {
 #if ENSC_BATCH_DESC_MODE == 1
-            // the instance's arrays and constants, read from the stage once:
-            // the body's stores could alias the stage as far as the compiler
-            // knows, so references into it would be re-read after each store
-            const ElemArrays E = d.E;
-            const NodeArrays N = d.N;
-            const Material M = d.M;
+                // the instance's arrays and constants, read from the stage once:
+                // the body's stores could alias the stage as far as the compiler
+                // knows, so references into it would be re-read after each store
+                const ElemArrays E = d.E;
+                const NodeArrays N = d.N;
+                const Material M = d.M;
 #elif ENSC_BATCH_DESC_MODE == 2
-            // arrays copied to registers, material constants read at use
-            const ElemArrays E = d.E;
-            const NodeArrays N = d.N;
-            const Material& M = d.M;
+                // arrays copied to registers, material constants read at use
+                const ElemArrays E = d.E;
+                const NodeArrays N = d.N;
+                const Material& M = d.M;
 #else
-            const ElemArrays& E = d.E;
-            const NodeArrays& N = d.N;
-            const Material& M = d.M;
+                const ElemArrays& E = d.E;
+                const NodeArrays& N = d.N;
+                const Material& M = d.M;
 #endif
-            const double dt1d = h.dt1;
-            const float dt1 = static_cast<float>(dt1d);
-            const float* st = reinterpret_cast<const float*>(sb);
-            const MixedSrc S{reinterpret_cast<const uint32_t*>(st),
-                             st + 8 * kStageTile,
-                             reinterpret_cast<const double*>(sb + kStageV0Off),
-                             st + 44 * kStageTile,
-                             st + 26 * kStageTile,
-                             st + 32 * kStageTile,
-                             st + 45 * kStageTile,
-                             kStageTile,
-                             tid};
-            double d1, l1;
-            element_body_mixed<true, false, true, 0, true>(E, N, M, S, dt1, dt1d, e, d1, l1, ei, eh, ev, bad, fo);
-            dts = fmin(dts, d1);
-            len = fmin(len, l1);
-            if (!patch) {
-                // slot assembly: the forces to the instance's force array
-                float* __restrict__ fe = static_cast<float*>(E.fe);
-                const int64_t np = N.nn_pad, ep = E.ne_pad;
+                const double dt1d = h.dt1;
+                const float dt1 = static_cast<float>(dt1d);
+                const float* st = reinterpret_cast<const float*>(sb);
+                const MixedSrc S{reinterpret_cast<const uint32_t*>(st),
+                                 st + 8 * kStageTile,
+                                 reinterpret_cast<const double*>(sb + kStageV0Off),
+                                 st + 44 * kStageTile,
+                                 st + 26 * kStageTile,
+                                 st + 32 * kStageTile,
+                                 st + 45 * kStageTile,
+                                 kStageTile,
+                                 li};
+                double d1, l1;
+                element_body_mixed<true, false, true, 0, true>(E, N, M, S, dt1, dt1d, e, d1, l1, ei, eh, ev, bad, fo);
+                dts = fmin(dts, d1);
+                len = fmin(len, l1);
+                if (!patch) {
+                    // slot assembly: the forces to the instance's force array
+                    float* __restrict__ fe = static_cast<float*>(E.fe);
+                    const int64_t np = N.nn_pad, ep = E.ne_pad;
 #pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    const uint32_t nj = S.conn[j * kStageTile + tid];
+                    for (int j = 0; j < 8; ++j) {
+                        const uint32_t nj = S.conn[j * kStageTile + li];
 #pragma unroll
-                    for (int i = 0; i < 3; ++i) {
-                        if (E.slot_major) fe[(3 * j + i) * np + nj] = fo[8 * i + j];
-                        else fe[(3 * j + i) * ep + e] = fo[8 * i + j];
+                        for (int i = 0; i < 3; ++i) {
+                            if (E.slot_major) fe[(3 * j + i) * np + nj] = fo[8 * i + j];
+                            else fe[(3 * j + i) * ep + e] = fo[8 * i + j];
+                        }
                     }
                 }
             }
@@ -1499,21 +1509,27 @@ int occupancy_node_mixed() {
 }
 
 
-void launch_element_batch_mixed(const BatchTables& T, int grid, cudaStream_t st) {
-    k_element_batch_mixed<<<grid, kStageTile, kBatchStageSmem, st>>>(T);
+void launch_element_batch_mixed(const BatchTables& T, int grid, int ept, cudaStream_t st) {
+    if (ept == 2) k_element_batch_mixed<2><<<grid, kStageTile / 2, kBatchStageSmem, st>>>(T);
+    else k_element_batch_mixed<1><<<grid, kStageTile, kBatchStageSmem, st>>>(T);
 }
 void launch_node_batch_mixed(const BatchTables& T, int grid, int threads, cudaStream_t st) {
     if (threads == kNodeThreads / 2) k_node_batch_mixed<kNodeThreads / 2><<<grid, threads, 0, st>>>(T);
     else k_node_batch_mixed<kNodeThreads><<<grid, kNodeThreads, 0, st>>>(T);
 }
-int occupancy_element_batch_mixed() {
+int occupancy_element_batch_mixed(int ept) {
     int nb = 0;
     set_element_mixed_attributes();  // the batch's init passes run the single-instance kernels
     // dynamic shared memory above the default 48 KB: set on the current
     // device before any launch or capture
-    cudaFuncSetAttribute(k_element_batch_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_element_batch_mixed<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          static_cast<int>(kBatchStageSmem));
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_batch_mixed, kStageTile, kBatchStageSmem);
+    cudaFuncSetAttribute(k_element_batch_mixed<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(kBatchStageSmem));
+    if (ept == 2)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_batch_mixed<2>, kStageTile / 2, kBatchStageSmem);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_batch_mixed<1>, kStageTile, kBatchStageSmem);
     return nb;
 }
 

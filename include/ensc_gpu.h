@@ -366,13 +366,18 @@ int ensc_batch_remove(ensc_batch* b, int32_t slot);
 int64_t ensc_batch_device_bytes(const ensc_batch* b);
 int32_t ensc_batch_instances(const ensc_batch* b);
 
-/* The launch choices the batch's autotuner made on its first run (no
- * reference counterpart: the reference has no batched stepper): grid
- * multipliers over one wave of resident blocks of the element and node
- * passes, cycles per graph launch, threads per block of the node pass.
- * All zero before the first ensc_batch_run.  Any pointer may be NULL. */
+/* The launch choices of the batch's autotuner (no reference counterpart:
+ * the reference has no batched stepper): grid multipliers over one wave of
+ * resident blocks of the element and node passes, cycles per graph launch,
+ * threads per block of the node pass and elements per thread of the element
+ * pass -- zero until the first tuning completes; the autotuner spreads its
+ * candidates over the first runs and tunes again when the batch's element
+ * count changes four-fold -- and the force assembly of the batch's
+ * instances (ENSC_ASSEMBLY_SLOT or _PATCH, fixed at ensc_batch_create:
+ * the assemblies round differently, so they are not timed against each
+ * other mid-solve).  Any pointer may be NULL. */
 int ensc_batch_tuning(const ensc_batch* b, int32_t* mult_element, int32_t* mult_node, int32_t* graph_cycles,
-                      int32_t* node_threads);
+                      int32_t* node_threads, int32_t* elements_per_thread, int32_t* assembly);
 
 void ensc_batch_destroy(ensc_batch* b);
 

@@ -163,12 +163,14 @@ def test_graph_length_does_not_change_results():
 @pytest.mark.parametrize("precision", [capi.FP64, capi.MIXED])
 def test_autotuner_tries_every_candidate_without_changing_results(precision):
     """A first run long enough for every launch candidate of the autotuner
-    (grid sizes, graph lengths, both node-pass block sizes) gives the
-    single-instance results, and the choice it reports is one of them."""
+    (grid sizes, graph lengths, both node-pass block sizes, 1 and 2 elements
+    per thread in mixed precision) gives the single-instance results, and
+    the choice it reports is one of them."""
     cases = [sweep_case(20, 900), sweep_case(21, 900, plastic=False)]
     refs = [single(c, precision) for c in cases]
     with make_batch(precision) as b:
-        assert b.tuning == dict(mult_element=0, mult_node=0, graph_cycles=0, node_threads=0)
+        assert b.tuning == dict(mult_element=0, mult_node=0, graph_cycles=0, node_threads=0, elements_per_thread=0,
+                                assembly=capi.ASSEMBLY_SLOT)
         ss = [add(b, c) for c in cases]
         for s, c in zip(ss, cases):
             b.arm(s, c.cycles)
@@ -177,6 +179,7 @@ def test_autotuner_tries_every_candidate_without_changing_results(precision):
         t = b.tuning
         assert t["mult_element"] in (1, 2) and t["mult_node"] in (1, 2)
         assert t["graph_cycles"] in (8, 32) and t["node_threads"] in (128, 256)
+        assert t["elements_per_thread"] in ((1, 2) if precision == capi.MIXED else (1,))
         for s, c, ref in zip(ss, cases, refs):
             assert_same(b.download(s), b.report(s), b.energy(s), ref, c.name)
 
