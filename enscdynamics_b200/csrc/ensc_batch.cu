@@ -36,6 +36,7 @@ struct Slot {
     bool plastic = false;
     ensc::ElemArrays E{};
     ensc::NodeArrays N{};
+    ensc::PatchArrays PA{};
     ensc::Material M{};
     bool kinetic0_done = false;
     double* amp = nullptr;  // gravity amplitude table (from the pool)
@@ -168,7 +169,9 @@ int rebuild_tables(ensc_batch* b) {
             ensc::set_mixed_consts(d.M);
         }
         d.active = 1;
-        views[s] = ensc::node_view(d.E, d.N, d.M, d.ctl);
+        d.patch = sl.PA.pf ? 1 : 0;
+        d.pa = sl.PA;
+        views[s] = ensc::node_view(d.E, d.N, d.M, d.ctl, &sl.PA);
         d.e_tile0 = static_cast<int32_t>(ei.size());
         for (int64_t e = 0; e < sl.ne; e += b->etile) {
             ei.push_back(s);
@@ -572,7 +575,7 @@ int ensc_batch_add_prepared(ensc_batch* b, const ensc_prepared* prep, const ensc
     void* block = nullptr;
     BCK(b, cudaMallocFromPoolAsync(&block, ih.bytes, b->pool, b->stream));
     std::string perr;
-    rc = ensc::instance_upload(ih, block, b->stream, sl.E, sl.N, perr);
+    rc = ensc::instance_upload(ih, block, b->stream, sl.E, sl.N, sl.PA, perr);
     if (rc) {
         cudaFreeAsync(block, b->stream);
         return berr(b, rc, perr);
@@ -599,7 +602,7 @@ int ensc_batch_add_prepared(ensc_batch* b, const ensc_prepared* prep, const ensc
     const int g = static_cast<int>(std::min<int64_t>((ih.ne + ensc::kElemThreads - 1) / ensc::kElemThreads,
                                                      b->scratch_blocks));
     P.n_elem_blocks = g;
-    if (is_mixed(b)) ensc::launch_element_mixed(sl.E, sl.N, sl.M, b->d_ctl + s, P, g, true, b->stream);
+    if (is_mixed(b)) ensc::launch_element_mixed(sl.E, sl.N, sl.M, b->d_ctl + s, P, g, true, b->stream, sl.PA);
     else ensc::launch_element_fp64(sl.E, sl.N, sl.M, b->d_ctl + s, P, g, true, b->stream);
     BCK(b, cudaGetLastError());
     BCK(b, cudaMemcpyAsync(b->h_ctl + s, b->d_ctl + s, sizeof(Ctl), cudaMemcpyDeviceToHost, b->stream));
@@ -755,7 +758,7 @@ int ensc_batch_download(ensc_batch* b, int32_t slot, double* x, double* u, doubl
         bool f32;
         const int32_t* at;
     };
-    const int32_t* ep = sl.E.iperm;  // element fields: stored positions
+    const int32_t* ep = sl.PA.iperm;  // element fields: stored positions
     const Item items[] = {{x, sl.N.x, sl.nn, sl.nn_pad, 3, false, nullptr},
                           {u, sl.N.u, sl.nn, sl.nn_pad, 3, false, nullptr},
                           {v, sl.N.v, sl.nn, sl.nn_pad, 3, mx, nullptr},

@@ -41,6 +41,7 @@ struct ensc_handle {
     size_t staging_bytes = 0;
     ensc::ElemArrays E{};
     ensc::NodeArrays N{};
+    ensc::PatchArrays PA{};        // patch assembly tables (null: slot assembly)
     ensc::Material M{};
     ensc::Partials P{};
     Ctl* ctl = nullptr;            // device
@@ -108,12 +109,12 @@ int upload(ensc_handle* h, void* dst, const std::vector<T>& src) {
 bool mixed(const ensc_handle* h) { return h->precision == ENSC_MIXED; }
 
 void launch_element(ensc_handle* h, bool init, cudaStream_t st) {
-    if (mixed(h)) ensc::launch_element_mixed(h->E, h->N, h->M, h->ctl, h->P, h->grid_e, init, st);
+    if (mixed(h)) ensc::launch_element_mixed(h->E, h->N, h->M, h->ctl, h->P, h->grid_e, init, st, h->PA);
     else ensc::launch_element_fp64(h->E, h->N, h->M, h->ctl, h->P, h->grid_e, init, st);
 }
 
 void launch_node(ensc_handle* h, cudaStream_t st) {
-    if (mixed(h)) ensc::launch_node_mixed(h->E, h->N, h->M, h->ctl, h->P, h->grid_n, st);
+    if (mixed(h)) ensc::launch_node_mixed(h->E, h->N, h->M, h->ctl, h->P, h->grid_n, st, h->PA);
     else ensc::launch_node_fp64(h->E, h->N, h->M, h->ctl, h->P, h->grid_n, st);
 }
 
@@ -254,7 +255,7 @@ int ensc_create(const ensc_mesh_desc* mesh, const ensc_material* mat, const ensc
         cuda_err(h, "cudaStreamCreate(capture)", ce);
         return fail(ENSC_ERR_CUDA);
     }
-    rc = ensc::instance_upload(ih, h->arena, h->stream, h->E, h->N, perr);
+    rc = ensc::instance_upload(ih, h->arena, h->stream, h->E, h->N, h->PA, perr);
     if (rc) {
         set_err(h, rc, perr);
         return fail(rc);
@@ -465,7 +466,7 @@ int ensc_download(ensc_handle* h, double* x, double* u, double* v, double* sigma
         const int32_t* at;
     };
     const bool mx = mixed(h);
-    const int32_t* ep = h->E.iperm;  // element fields: stored positions
+    const int32_t* ep = h->PA.iperm;  // element fields: stored positions
     const Item items[] = {{x, h->N.x, h->nn, h->nn_pad, 3, false, nullptr},
                           {u, h->N.u, h->nn, h->nn_pad, 3, false, nullptr},
                           {v, h->N.v, h->nn, h->nn_pad, 3, mx, nullptr},
@@ -510,7 +511,7 @@ int ensc_upload_state(ensc_handle* h, const double* x, const double* u, const do
         const int32_t* at;
     };
     const bool mx = mixed(h);
-    const int32_t* ep = h->E.iperm;  // element fields: stored positions
+    const int32_t* ep = h->PA.iperm;  // element fields: stored positions
     const Item items[] = {{x, h->N.x, h->nn, h->nn_pad, 3, false, nullptr},
                           {u, h->N.u, h->nn, h->nn_pad, 3, false, nullptr},
                           {v, h->N.v, h->nn, h->nn_pad, 3, mx, nullptr},
@@ -575,13 +576,13 @@ int ensc_snapshot_begin(ensc_handle* h) {
     if (h->snap_count > 0) CK(h, cudaStreamWaitEvent(h->stream, h->snap_landed[(h->snap_count - 1) % 2], 0));
     double* d = h->snap_dev;
     const bool mx = mixed(h);
-    if (mx) ensc::launch_acceleration_mixed(h->E, h->N, h->M, h->ctl, d + 3 * nodes3, h->stream);
+    if (mx) ensc::launch_acceleration_mixed(h->E, h->N, h->M, h->ctl, d + 3 * nodes3, h->stream, h->PA);
     else ensc::launch_acceleration_fp64(h->E, h->N, h->M, h->ctl, d + 3 * nodes3, h->stream);
     ensc::launch_soa_to_aos(h->N.x, h->nn, h->nn_pad, 3, false, d, h->stream);
     ensc::launch_soa_to_aos(h->N.u, h->nn, h->nn_pad, 3, false, d + nodes3, h->stream);
     ensc::launch_v_to_aos(h->N, mx, d + 2 * nodes3, h->stream);
     ensc::launch_soa_to_aos(h->N.rf, h->nn, h->nn_pad, 3, false, d + 4 * nodes3, h->stream);
-    ensc::launch_soa_to_aos(h->E.sigma, h->ne, h->ne_pad, 6, mx, d + 5 * nodes3, h->stream, h->E.iperm);
+    ensc::launch_soa_to_aos(h->E.sigma, h->ne, h->ne_pad, 6, mx, d + 5 * nodes3, h->stream, h->PA.iperm);
     CK(h, cudaGetLastError());
     char* ctl_copy = reinterpret_cast<char*>(d) + (h->snap_bytes - sizeof(Ctl));
     CK(h, cudaMemcpyAsync(ctl_copy, h->ctl, sizeof(Ctl), cudaMemcpyDeviceToDevice, h->stream));
@@ -686,7 +687,7 @@ int32_t ensc_kernels_per_cycle(const ensc_handle* h) { return h ? 4 : 0; }
 
 int ensc_assembly(const ensc_handle* h, int32_t* assembly, int64_t* patches, int64_t* partials) {
     if (!h) return ENSC_ERR_ARG;
-    if (assembly) *assembly = h->E.patch ? ENSC_ASSEMBLY_PATCH : ENSC_ASSEMBLY_SLOT;
+    if (assembly) *assembly = h->PA.pf ? ENSC_ASSEMBLY_PATCH : ENSC_ASSEMBLY_SLOT;
     if (patches) *patches = h->n_patches;
     if (partials) *partials = h->n_partials;
     return ENSC_OK;

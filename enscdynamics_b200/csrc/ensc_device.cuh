@@ -131,26 +131,33 @@ struct ElemArrays {
     // 0: fe is element-major, fe[(3k + c) * ne_pad + e], gathered through
     // ell / csr by the node pass
     int32_t slot_major;
-    // Patch assembly (mixed precision, patch = 1): elements are stored in
-    // patches of kPatchElems consecutive elements.  The element pass sums a
-    // patch's element forces per patch node in shared memory and writes one
-    // partial per (patch, node): patch p's nodes are the partial entries
-    // pf_off[p] .. pf_off[p + 1] - 1, entry q's incidences are
-    // pinc[pinc_off[q] .. pinc_off[q + 1]) as (element in patch << 3 | slot),
-    // in slot order, and its partial goes to pf[c * pf_pad + q].  fe is not
-    // used.  iperm maps an element of the caller's numbering to its stored
-    // position (null: the caller's order is kept).
-    int32_t patch;
+};
+
+// Elements per patch of the mixed patch assembly: one staged tile.
+constexpr int kPatchElems = 64;
+
+// The tables of the patch assembly (mixed precision), kept apart from the
+// element and node arrays so that kernels of the slot assembly see the same
+// argument layout either way; all null for an instance on the slot
+// assembly.  Elements are stored in patches of kPatchElems consecutive
+// elements.  The element pass sums a patch's element forces per patch node
+// in shared memory and writes one partial per (patch, node): patch p's
+// nodes are the partial entries pf_off[p] .. pf_off[p + 1] - 1, entry q's
+// incidences are pinc[pinc_off[q] .. pinc_off[q + 1]) as (element in patch
+// << 3 | slot), in slot order, and its partial goes to pf[c * pf_pad + q].
+// Node n's force is the sum of its partials nent[nptr[n] .. nptr[n + 1]),
+// in patch order.  iperm maps an element of the caller's numbering to its
+// stored position.
+struct PatchArrays {
     const uint32_t* pf_off;
     const uint32_t* pinc_off;
     const uint16_t* pinc;
     float* pf;
     int64_t pf_pad;
+    const uint32_t* nptr;
+    const uint32_t* nent;
     const int32_t* iperm;
 };
-
-// Elements per patch of the mixed patch assembly: one staged tile.
-constexpr int kPatchElems = 64;
 
 struct NodeArrays {
     int64_t nn, nn_pad;
@@ -165,10 +172,6 @@ struct NodeArrays {
     const uint32_t* csr_ent;   // (e << 3) | slot
     const uint8_t* slot_mask;  // slot-major forces: bit k set if slot k holds an element
     double* rf;                // reactions, [3][nn_pad]
-    // patch assembly: node n's partials are pf entries nent[nptr[n] ..
-    // nptr[n + 1]), in patch order
-    const uint32_t* nptr;
-    const uint32_t* nent;
 };
 
 // Partial sums written by each block of a pass, folded in fixed block order.
@@ -207,7 +210,8 @@ struct alignas(128) NodeView {
 };
 static_assert(sizeof(NodeView) == 256, "two lines per slot");
 
-__host__ __device__ inline NodeView node_view(const ElemArrays& E, const NodeArrays& N, const Material& M, Ctl* ctl) {
+__host__ __device__ inline NodeView node_view(const ElemArrays& E, const NodeArrays& N, const Material& M, Ctl* ctl,
+                                              const PatchArrays* pa = nullptr) {
     NodeView v{};
     v.fe = E.fe;
     v.v = N.v;
@@ -223,11 +227,14 @@ __host__ __device__ inline NodeView node_view(const ElemArrays& E, const NodeArr
     v.gravity_value = M.gravity_value;
     for (int c = 0; c < 3; ++c) v.gravity_dir[c] = M.gravity_dir[c];
     v.gravity_on = M.gravity_on;
-    v.grouped = (E.slot_major && E.tiles_aligned) ? (E.patch ? 2 : 1) : 0;
-    v.pf = E.patch ? E.pf : nullptr;
-    v.nptr = N.nptr;
-    v.nent = N.nent;
-    v.pf_pad = E.pf_pad;
+    const bool patch = pa && pa->pf;
+    v.grouped = (E.slot_major && E.tiles_aligned) ? (patch ? 2 : 1) : 0;
+    if (patch) {
+        v.pf = pa->pf;
+        v.nptr = pa->nptr;
+        v.nent = pa->nent;
+        v.pf_pad = pa->pf_pad;
+    }
     return v;
 }
 
@@ -285,7 +292,8 @@ struct alignas(16) InstanceDesc {
     int32_t e_tile0, e_ntiles;   // range in the element-tile list
     int32_t n_tile0, n_ntiles;   // range in the node-tile list
     int32_t active;
-    int32_t pad;
+    int32_t patch;               // 1: the patch assembly, tables in pa
+    PatchArrays pa;
 };
 
 struct BatchTables {

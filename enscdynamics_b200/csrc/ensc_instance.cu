@@ -364,7 +364,7 @@ int instance_prepare(const ensc_mesh_desc* mesh, const ensc_material* mat, bool 
 }
 
 int instance_upload(const InstanceHost& h, void* block, cudaStream_t st, ElemArrays& E, NodeArrays& N,
-                    std::string& err) {
+                    PatchArrays& PA, std::string& err) {
     using P = InstanceHost::Piece;
     const int64_t ep = h.ne_pad, np = h.nn_pad;
     char* b = static_cast<char*>(block);
@@ -457,14 +457,16 @@ int instance_upload(const InstanceHost& h, void* block, cudaStream_t st, ElemArr
     E.fe = b + h.off[P::FE];
     E.tiles_aligned = 1;  // pieces are 256-byte aligned, ne_pad % 32 == 0
     E.slot_major = h.clash ? 0 : 1;
+    PA = PatchArrays{};
     if (h.patch) {
-        E.patch = 1;
-        E.pf_off = reinterpret_cast<uint32_t*>(b + h.off[P::PFOFF]);
-        E.pinc_off = reinterpret_cast<uint32_t*>(b + h.off[P::PINCOFF]);
-        E.pinc = reinterpret_cast<uint16_t*>(b + h.off[P::PINC]);
-        E.pf = reinterpret_cast<float*>(b + h.off[P::PF]);
-        E.pf_pad = pad32(h.n_pnodes);
-        E.iperm = reinterpret_cast<int32_t*>(b + h.off[P::IPERM]);
+        PA.pf_off = reinterpret_cast<uint32_t*>(b + h.off[P::PFOFF]);
+        PA.pinc_off = reinterpret_cast<uint32_t*>(b + h.off[P::PINCOFF]);
+        PA.pinc = reinterpret_cast<uint16_t*>(b + h.off[P::PINC]);
+        PA.pf = reinterpret_cast<float*>(b + h.off[P::PF]);
+        PA.pf_pad = pad32(h.n_pnodes);
+        PA.nptr = reinterpret_cast<uint32_t*>(b + h.off[P::NPTR]);
+        PA.nent = reinterpret_cast<uint32_t*>(b + h.off[P::NENT]);
+        PA.iperm = reinterpret_cast<int32_t*>(b + h.off[P::IPERM]);
     }
     N = NodeArrays{};
     N.nn = h.nn;
@@ -480,10 +482,6 @@ int instance_upload(const InstanceHost& h, void* block, cudaStream_t st, ElemArr
     N.csr_ent = h.clash ? reinterpret_cast<uint32_t*>(b + h.off[P::CENT]) : nullptr;
     N.rf = reinterpret_cast<double*>(b + h.off[P::RF]);
     N.slot_mask = h.clash ? nullptr : reinterpret_cast<uint8_t*>(b + h.off[P::MASK]);
-    if (h.patch) {
-        N.nptr = reinterpret_cast<uint32_t*>(b + h.off[P::NPTR]);
-        N.nent = reinterpret_cast<uint32_t*>(b + h.off[P::NENT]);
-    }
     return ENSC_OK;
 }
 

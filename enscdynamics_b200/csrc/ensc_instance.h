@@ -65,9 +65,10 @@ std::vector<int32_t> patch_order(int64_t ne, const uint32_t* conn, const double*
 void build_patches(int64_t nn, int64_t ne, const uint32_t* conn, InstanceHost& h);
 
 // Copies the instance into `block` (h.bytes bytes, 256-byte aligned) on
-// stream `st`, waits for the copies, and fills the array descriptors.
+// stream `st`, waits for the copies, and fills the array descriptors (PA
+// all null under the slot assembly).
 int instance_upload(const InstanceHost& h, void* block, cudaStream_t st, ElemArrays& E, NodeArrays& N,
-                    std::string& err);
+                    PatchArrays& PA, std::string& err);
 
 // Material_elastic::update (Material_elastic.cpp:9-14) plus the controls.
 void material_from(const ensc_material* mat, const ensc_params* p, Material& M);

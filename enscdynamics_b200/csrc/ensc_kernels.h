@@ -131,9 +131,9 @@ int occupancy_node_fp64();
 
 // mixed precision (ensc_mixed.cu)
 void launch_element_mixed(const ElemArrays& E, const NodeArrays& N, const Material& M, Ctl* ctl, const Partials& P,
-                          int grid, bool init, cudaStream_t st);
+                          int grid, bool init, cudaStream_t st, const PatchArrays& PA = PatchArrays{});
 void launch_node_mixed(const ElemArrays& E, const NodeArrays& N, const Material& M, Ctl* ctl, const Partials& P,
-                       int grid, cudaStream_t st);
+                       int grid, cudaStream_t st, const PatchArrays& PA = PatchArrays{});
 int occupancy_element_mixed(bool plastic);
 int occupancy_node_mixed();
 
@@ -142,7 +142,7 @@ int occupancy_node_mixed();
 void launch_acceleration_fp64(const ElemArrays& E, const NodeArrays& N, const Material& M, const Ctl* ctl,
                               double* a_aos, cudaStream_t st);
 void launch_acceleration_mixed(const ElemArrays& E, const NodeArrays& N, const Material& M, const Ctl* ctl,
-                               double* a_aos, cudaStream_t st);
+                               double* a_aos, cudaStream_t st, const PatchArrays& PA = PatchArrays{});
 
 // batched instances (one launch per phase for all instances of a batch)
 void launch_element_batch_fp64(const BatchTables& T, int grid, cudaStream_t st);

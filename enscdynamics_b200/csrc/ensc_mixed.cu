@@ -659,12 +659,12 @@ __global__ void __launch_bounds__(kStageTile, ENSC_STAGE_MINB_MIXED)
 // with the stage's inputs, the forces go into the stage's memory as
 // [3][8 slots][kStageTile elements], and the block sums each of the patch's
 // nodes over its incidences in slot order (starting from zero) and writes the
-// node's partial to E.pf.  INIT: the init force pass (dt = 0, no state
+// node's partial to PA.pf.  INIT: the init force pass (dt = 0, no state
 // written, no energy).
 static_assert(kStageTile == kPatchElems, "one patch per staged tile");
 static_assert(3u * 8u * kStageTile * 4u <= kStageBytes, "the element forces fit in a stage");
 
-__device__ __forceinline__ void patch_partials(const ElemArrays& E, const float* sf, int64_t t, int tid) {
+__device__ __forceinline__ void patch_partials(const PatchArrays& E, const float* sf, int64_t t, int tid) {
     const uint32_t q0 = __ldg(E.pf_off + t), q1 = __ldg(E.pf_off + t + 1);
     for (uint32_t q = q0 + tid; q < q1; q += kStageTile) {
         const uint32_t a = __ldg(E.pinc_off + q), b = __ldg(E.pinc_off + q + 1);
@@ -684,7 +684,7 @@ __device__ __forceinline__ void patch_partials(const ElemArrays& E, const float*
 
 template <bool PLASTIC, bool INIT>
 __global__ void __launch_bounds__(kStageTile, ENSC_STAGE_MINB_MIXED)
-    k_element_mixed_patch(ElemArrays E, NodeArrays N, Material M, Ctl* ctl, Partials P) {
+    k_element_mixed_patch(ElemArrays E, NodeArrays N, Material M, Ctl* ctl, Partials P, PatchArrays PA) {
     if (ctl->done) return;
     extern __shared__ __align__(128) unsigned char smem[];
     const float dt1 = INIT ? 0.f : static_cast<float>(ctl->dt_i_1);
@@ -746,7 +746,7 @@ __global__ void __launch_bounds__(kStageTile, ENSC_STAGE_MINB_MIXED)
             for (int i = 0; i < 24; ++i) sf[i * kStageTile + tid] = fo[i];
         }
         __syncthreads();
-        patch_partials(E, sf, t, tid);
+        patch_partials(PA, sf, t, tid);
         __syncthreads();  // the block is done with stage s
         const int64_t tn = t + 2 * gstride;
         if (wid == 0 && tn < ntiles) stage_issue<PLASTIC>(E, stage0 + s * kStageBytes, bar, tn * kStageTile, lane);
@@ -771,13 +771,13 @@ __global__ void __launch_bounds__(kStageTile, ENSC_STAGE_MINB_MIXED)
 
 // One node's force under the patch assembly: its partials in patch order,
 // from zero.
-__device__ __forceinline__ void patch_gather(const ElemArrays& E, const NodeArrays& N, int64_t n, float (&f)[3]) {
-    const int64_t pp = E.pf_pad;
-    for (uint32_t r = __ldg(N.nptr + n), b = __ldg(N.nptr + n + 1); r < b; ++r) {
-        const uint32_t q = __ldg(N.nent + r);
-        f[0] += __ldg(E.pf + q);
-        f[1] += __ldg(E.pf + pp + q);
-        f[2] += __ldg(E.pf + 2 * pp + q);
+__device__ __forceinline__ void patch_gather(const PatchArrays& PA, int64_t n, float (&f)[3]) {
+    const int64_t pp = PA.pf_pad;
+    for (uint32_t r = __ldg(PA.nptr + n), b = __ldg(PA.nptr + n + 1); r < b; ++r) {
+        const uint32_t q = __ldg(PA.nent + r);
+        f[0] += __ldg(PA.pf + q);
+        f[1] += __ldg(PA.pf + pp + q);
+        f[2] += __ldg(PA.pf + 2 * pp + q);
     }
 }
 
@@ -818,9 +818,7 @@ __device__ __forceinline__ void node_body_mixed(const ElemArrays& E, const NodeA
     const double dt_avg = 0.5 * (dt_i + dt_i_1);
 
     float f[3] = {0.f, 0.f, 0.f};
-    if (E.patch) {
-        patch_gather(E, N, n, f);
-    } else if (E.slot_major) {
+    if (E.slot_major) {
         const uint32_t msk = N.slot_mask[n];
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
@@ -1017,8 +1015,11 @@ __device__ __forceinline__ void node_group_mixed(const NodeView& N, const double
 
 // Node pass in mixed precision: FP32 slot-ordered gather and acceleration,
 // FP32 velocity, FP64 displacement / position accumulation and energy.
+// PATCH: the instance uses the patch assembly (one instantiation each, so
+// the slot-assembly pass carries no code of the other).
+template <bool PATCH>
 __global__ void __launch_bounds__(kNodeThreads, ENSC_NODE_MINB_MIXED) k_node_mixed(ElemArrays E, NodeArrays N, Material M, Ctl* ctl,
-                                                             Partials P) {
+                                                             Partials P, PatchArrays PA) {
     if (ctl->done) return;
     double dt_i;
     const double dt_i_1 = ctl->dt_i_1;
@@ -1043,14 +1044,9 @@ __global__ void __launch_bounds__(kNodeThreads, ENSC_NODE_MINB_MIXED) k_node_mix
     const int64_t t0 = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (E.slot_major && E.tiles_aligned) {
         constexpr int W = kNodeGroupMixed;
-        const NodeView nv = node_view(E, N, M, ctl);
-        if (E.patch) {
-            for (int64_t g = t0; g * W < nn; g += stride)
-                node_group_mixed<W, true>(nv, dt_i, dt_i_1, amp, g * W, kin, wext, bad);
-        } else {
-            for (int64_t g = t0; g * W < nn; g += stride)
-                node_group_mixed<W, false>(nv, dt_i, dt_i_1, amp, g * W, kin, wext, bad);
-        }
+        const NodeView nv = node_view(E, N, M, ctl, &PA);
+        for (int64_t g = t0; g * W < nn; g += stride)
+            node_group_mixed<W, PATCH>(nv, dt_i, dt_i_1, amp, g * W, kin, wext, bad);
     } else {
         for (int64_t n = t0; n < nn; n += stride) node_body_mixed(E, N, M, dt_i, dt_i_1, amp, n, kin, wext, bad);
     }
@@ -1064,7 +1060,7 @@ __global__ void __launch_bounds__(kNodeThreads, ENSC_NODE_MINB_MIXED) k_node_mix
 // the FP64 stepper): the FP32 force sum, gravity and the FP32 acceleration
 // f M^-1 that the mixed node pass feeds into the velocity update, written
 // as doubles, interleaved xyz per node.
-__global__ void __launch_bounds__(kNodeThreads) k_acceleration_mixed(ElemArrays E, NodeArrays N, Material M,
+__global__ void __launch_bounds__(kNodeThreads) k_acceleration_mixed(PatchArrays PA, ElemArrays E, NodeArrays N, Material M,
                                                                      const Ctl* ctl, double* a_out) {
     const int64_t np = N.nn_pad, ep = E.ne_pad;
     const float* __restrict__ fe = static_cast<const float*>(E.fe);
@@ -1073,8 +1069,8 @@ __global__ void __launch_bounds__(kNodeThreads) k_acceleration_mixed(ElemArrays 
     for (int64_t n = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; n < N.nn;
          n += static_cast<int64_t>(gridDim.x) * blockDim.x) {
         float f[3] = {0.f, 0.f, 0.f};
-        if (E.patch) {
-            patch_gather(E, N, n, f);
+        if (PA.pf) {
+            patch_gather(PA, n, f);
         } else if (E.slot_major) {
             const uint32_t msk = grouped ? 0xffu : N.slot_mask[n];
 #pragma unroll
@@ -1272,8 +1268,8 @@ __global__ void __launch_bounds__(kStageTile / EPT, ENSC_BATCH_MINB_MIXED) k_ele
             run_ctl = d.ctl;
             run_live = h.live != 0;
         }
-        const bool patch = EPT == 1 && d.E.patch != 0;  // uniform over the tile
-        const ElemArrays* pe = patch ? &d.E : nullptr;
+        const bool patch = EPT == 1 && d.patch != 0;  // uniform over the tile
+        const PatchArrays* pe = patch ? &d.pa : nullptr;
         float fo[24];
         int64_t e = 0;
 #pragma unroll 1
@@ -1333,10 +1329,11 @@ __global__ void __launch_bounds__(kStageTile / EPT, ENSC_BATCH_MINB_MIXED) k_ele
         if (patch && run_live) {
             // the tile's patch: its forces summed per patch node (see
             // k_element_mixed_patch); the stage's element rows hold them
-            const ElemArrays PE = *pe;
+            const PatchArrays PE = *pe;
+            const int64_t ne = d.E.ne;
             __syncthreads();  // the stage's inputs are consumed
             float* sf = reinterpret_cast<float*>(sb);
-            if (e < PE.ne) {
+            if (e < ne) {
 #pragma unroll
                 for (int i = 0; i < 24; ++i) sf[i * kStageTile + tid] = fo[i];
             }
@@ -1426,14 +1423,14 @@ __global__ void __launch_bounds__(NT, ENSC_NODE_BATCH_MINB_MIXED * kNodeThreads 
 }  // namespace
 
 void launch_element_mixed(const ElemArrays& E, const NodeArrays& N, const Material& M, Ctl* ctl, const Partials& P,
-                          int grid, bool init, cudaStream_t st) {
-    if (E.patch) {
+                          int grid, bool init, cudaStream_t st, const PatchArrays& PA) {
+    if (PA.pf) {
         if (M.plastic) {
-            if (init) k_element_mixed_patch<true, true><<<grid, kStageTile, kStageSmem, st>>>(E, N, M, ctl, P);
-            else k_element_mixed_patch<true, false><<<grid, kStageTile, kStageSmem, st>>>(E, N, M, ctl, P);
+            if (init) k_element_mixed_patch<true, true><<<grid, kStageTile, kStageSmem, st>>>(E, N, M, ctl, P, PA);
+            else k_element_mixed_patch<true, false><<<grid, kStageTile, kStageSmem, st>>>(E, N, M, ctl, P, PA);
         } else {
-            if (init) k_element_mixed_patch<false, true><<<grid, kStageTile, kStageSmem, st>>>(E, N, M, ctl, P);
-            else k_element_mixed_patch<false, false><<<grid, kStageTile, kStageSmem, st>>>(E, N, M, ctl, P);
+            if (init) k_element_mixed_patch<false, true><<<grid, kStageTile, kStageSmem, st>>>(E, N, M, ctl, P, PA);
+            else k_element_mixed_patch<false, false><<<grid, kStageTile, kStageSmem, st>>>(E, N, M, ctl, P, PA);
         }
         return;
     }
@@ -1452,14 +1449,15 @@ void launch_element_mixed(const ElemArrays& E, const NodeArrays& N, const Materi
 }
 
 void launch_acceleration_mixed(const ElemArrays& E, const NodeArrays& N, const Material& M, const Ctl* ctl,
-                               double* a_aos, cudaStream_t st) {
+                               double* a_aos, cudaStream_t st, const PatchArrays& PA) {
     const int64_t g = (N.nn + kNodeThreads - 1) / kNodeThreads;
-    k_acceleration_mixed<<<static_cast<int>(g < 65535 ? g : 65535), kNodeThreads, 0, st>>>(E, N, M, ctl, a_aos);
+    k_acceleration_mixed<<<static_cast<int>(g < 65535 ? g : 65535), kNodeThreads, 0, st>>>(PA, E, N, M, ctl, a_aos);
 }
 
 void launch_node_mixed(const ElemArrays& E, const NodeArrays& N, const Material& M, Ctl* ctl, const Partials& P,
-                       int grid, cudaStream_t st) {
-    k_node_mixed<<<grid, kNodeThreads, 0, st>>>(E, N, M, ctl, P);
+                       int grid, cudaStream_t st, const PatchArrays& PA) {
+    if (PA.pf) k_node_mixed<true><<<grid, kNodeThreads, 0, st>>>(E, N, M, ctl, P, PA);
+    else k_node_mixed<false><<<grid, kNodeThreads, 0, st>>>(E, N, M, ctl, P, PA);
 }
 
 // The staged passes need more than the default 48 KB of dynamic shared
@@ -1504,7 +1502,7 @@ int occupancy_element_mixed(bool plastic) {
 
 int occupancy_node_mixed() {
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_node_mixed, kNodeThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_node_mixed<false>, kNodeThreads, 0);
     return nb;
 }
 
