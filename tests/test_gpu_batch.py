@@ -220,7 +220,7 @@ def test_churn_with_short_runs_and_prepared_instances(precision):
     instances removed and added between runs, slots reused before the tables
     are rewritten.  Every instance still ends with its single-instance
     results and energies."""
-    cases = [sweep_case(40 + i, 120 + 45 * i, plastic=i % 2 == 0) for i in range(6)]
+    cases = [sweep_case(40 + i, 260 + 45 * i, plastic=i % 2 == 0) for i in range(6)]
     refs = [single(c, precision) for c in cases]
     got = {}
     with make_batch(precision, max_instances=4) as b:
