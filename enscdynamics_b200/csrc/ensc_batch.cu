@@ -232,8 +232,9 @@ void launch_cycle(ensc_batch* b, int ge, int gn, int nt, int ept, cudaStream_t s
     ensc::launch_between_batch(b->T, b->slots, 0, st);
     ensc::launch_edge_prepass_batch(b->T, b->sms * b->occ_pre, st);
     if (is_mixed(b)) {
-        ensc::launch_element_batch_mixed(b->T, ge, ept, st);
-        ensc::launch_node_batch_mixed(b->T, gn, nt, st);
+        const bool patch = b->assembly == ENSC_ASSEMBLY_PATCH;
+        ensc::launch_element_batch_mixed(b->T, ge, ept, patch, st);
+        ensc::launch_node_batch_mixed(b->T, gn, nt, patch, st);
     } else {
         ensc::launch_element_batch_fp64(b->T, ge, st);
         ensc::launch_node_batch_fp64(b->T, gn, nt, st);
@@ -555,6 +556,8 @@ int ensc_batch_add_prepared(ensc_batch* b, const ensc_prepared* prep, const ensc
     if (!b || !prep || !controls || !slot_out) return berr(b, ENSC_ERR_ARG, "missing argument");
     if (!(controls->factor_timestep > 0.0)) return berr(b, ENSC_ERR_ARG, "factor_timestep must be > 0");
     if (prep->precision != b->precision) return berr(b, ENSC_ERR_ARG, "instance prepared for another precision");
+    if (prep->ih.patch != (b->assembly == ENSC_ASSEMBLY_PATCH))
+        return berr(b, ENSC_ERR_ARG, "instance prepared for another force assembly");
     DevGuard dg(b->device);
     int s = -1;
     for (int i = 0; i < b->slots; ++i)

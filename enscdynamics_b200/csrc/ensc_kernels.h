@@ -53,6 +53,10 @@ constexpr int kNodeUnrollMixed = ENSC_NODE_UNROLL_MIXED;
 // rows into L1 before its coordinate phase: bit 0 the velocities, bit 1 the
 // coordinate components 1 and 2 (the batched pass does not: the addresses
 // cost it registers and spills)
+// The same for the batched mixed element pass
+#ifndef ENSC_BATCH_MIXED_PREFETCH
+#define ENSC_BATCH_MIXED_PREFETCH 0
+#endif
 #ifndef ENSC_MIXED_PREFETCH
 #define ENSC_MIXED_PREFETCH 3
 #endif
@@ -150,8 +154,8 @@ void launch_element_batch_fp64(const BatchTables& T, int grid, cudaStream_t st);
 void launch_node_batch_fp64(const BatchTables& T, int grid, int threads, cudaStream_t st);
 int occupancy_element_batch_fp64();
 int occupancy_node_batch_fp64(int threads);
-void launch_element_batch_mixed(const BatchTables& T, int grid, int ept, cudaStream_t st);
-void launch_node_batch_mixed(const BatchTables& T, int grid, int threads, cudaStream_t st);
+void launch_element_batch_mixed(const BatchTables& T, int grid, int ept, bool patch, cudaStream_t st);
+void launch_node_batch_mixed(const BatchTables& T, int grid, int threads, bool patch, cudaStream_t st);
 int occupancy_element_batch_mixed(int ept);
 int occupancy_node_batch_mixed(int threads);
 // elements and nodes per batch tile (element tiles are the staged passes'

@@ -781,6 +781,7 @@ __device__ __forceinline__ void patch_gather(const PatchArrays& PA, int64_t n, f
     }
 }
 
+#if !ENSC_MIXED_VLO
 // v + (dt_i + dt_i_1) / 2 * f * M^-1 in FP32 with the half step and the
 // inverse mass as float pairs: both are the same for many nodes and cycles,
 // so their FP32 rounding would scale all accelerations alike.
@@ -790,6 +791,7 @@ __device__ __forceinline__ float velocity_update(float vo, float f, double im, f
     const float acc = fmaf(f, im_hi, f * im_lo);
     return fmaf(hdt, acc, fmaf(hdt_lo, acc, vo));
 }
+#endif
 
 // The velocity update in FP64 on the split velocity (hi float + 16-bit
 // residual, v_join / v_split): v + (dt_i + dt_i_1) / 2 * a with the FP32
@@ -1190,9 +1192,11 @@ __device__ __forceinline__ void batch_stage_issue(const BatchTables& T, const ET
 
 // EPT elements per thread: the block has kStageTile / EPT threads, and each
 // thread evaluates elements tid, tid + kStageTile / EPT, ... of a tile in
-// turn (a tuning choice; EPT > 1 only under the slot assembly).
-template <int EPT>
+// turn (a tuning choice; EPT > 1 only under the slot assembly).  PATCH: the
+// batch's instances use the patch assembly (a batch has one assembly).
+template <int EPT, bool PATCH>
 __global__ void __launch_bounds__(kStageTile / EPT, ENSC_BATCH_MINB_MIXED) k_element_batch_mixed(BatchTables T) {
+    static_assert(EPT == 1 || !PATCH, "the patch sums take one element per thread");
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr int NW = kStageTile / 32;  // energy partial slots per tile
     constexpr int NT = kStageTile / EPT;
@@ -1268,8 +1272,8 @@ __global__ void __launch_bounds__(kStageTile / EPT, ENSC_BATCH_MINB_MIXED) k_ele
             run_ctl = d.ctl;
             run_live = h.live != 0;
         }
-        const bool patch = EPT == 1 && d.patch != 0;  // uniform over the tile
-        const PatchArrays* pe = patch ? &d.pa : nullptr;
+        constexpr bool patch = PATCH;
+        const PatchArrays* pe = &d.pa;
         float fo[24];
         int64_t e = 0;
 #pragma unroll 1
@@ -1307,7 +1311,8 @@ __global__ void __launch_bounds__(kStageTile / EPT, ENSC_BATCH_MINB_MIXED) k_ele
                                  kStageTile,
                                  li};
                 double d1, l1;
-                element_body_mixed<true, false, true, 0, true>(E, N, M, S, dt1, dt1d, e, d1, l1, ei, eh, ev, bad, fo);
+                element_body_mixed<true, false, true, ENSC_BATCH_MIXED_PREFETCH, true>(E, N, M, S, dt1, dt1d, e, d1, l1,
+                                                                                      ei, eh, ev, bad, fo);
                 dts = fmin(dts, d1);
                 len = fmin(len, l1);
                 if (!patch) {
@@ -1366,7 +1371,7 @@ __global__ void __launch_bounds__(kStageTile / EPT, ENSC_BATCH_MINB_MIXED) k_ele
 // tile ahead, so a tile starts on its node rows without waiting on the
 // tables.
 // NT threads per block (a tuning choice: the warps are independent).
-template <int NT>
+template <int NT, bool PATCH>
 __global__ void __launch_bounds__(NT, ENSC_NODE_BATCH_MINB_MIXED * kNodeThreads / NT) k_node_batch_mixed(BatchTables T) {
     constexpr int W = kNodeGroupMixed;
     const int lane = threadIdx.x & 31;
@@ -1393,7 +1398,7 @@ __global__ void __launch_bounds__(NT, ENSC_NODE_BATCH_MINB_MIXED * kNodeThreads 
             int32_t bad = 0;
             const int64_t n0 = static_cast<int64_t>(base) + static_cast<int64_t>(lane) * W;
             if (n0 < v.nn) {
-                if (v.grouped == 2) {
+                if (PATCH) {
                     node_group_mixed<W, true>(v, dt_i, dt_i_1, amp, n0, kin, wext, bad);
                 } else if (v.grouped) {
                     node_group_mixed<W, false>(v, dt_i, dt_i_1, amp, n0, kin, wext, bad);
@@ -1507,27 +1512,36 @@ int occupancy_node_mixed() {
 }
 
 
-void launch_element_batch_mixed(const BatchTables& T, int grid, int ept, cudaStream_t st) {
-    if (ept == 2) k_element_batch_mixed<2><<<grid, kStageTile / 2, kBatchStageSmem, st>>>(T);
-    else k_element_batch_mixed<1><<<grid, kStageTile, kBatchStageSmem, st>>>(T);
+void launch_element_batch_mixed(const BatchTables& T, int grid, int ept, bool patch, cudaStream_t st) {
+    if (patch) k_element_batch_mixed<1, true><<<grid, kStageTile, kBatchStageSmem, st>>>(T);
+    else if (ept == 2) k_element_batch_mixed<2, false><<<grid, kStageTile / 2, kBatchStageSmem, st>>>(T);
+    else k_element_batch_mixed<1, false><<<grid, kStageTile, kBatchStageSmem, st>>>(T);
 }
-void launch_node_batch_mixed(const BatchTables& T, int grid, int threads, cudaStream_t st) {
-    if (threads == kNodeThreads / 2) k_node_batch_mixed<kNodeThreads / 2><<<grid, threads, 0, st>>>(T);
-    else k_node_batch_mixed<kNodeThreads><<<grid, kNodeThreads, 0, st>>>(T);
+void launch_node_batch_mixed(const BatchTables& T, int grid, int threads, bool patch, cudaStream_t st) {
+    if (patch) {
+        if (threads == kNodeThreads / 2) k_node_batch_mixed<kNodeThreads / 2, true><<<grid, threads, 0, st>>>(T);
+        else k_node_batch_mixed<kNodeThreads, true><<<grid, kNodeThreads, 0, st>>>(T);
+    } else {
+        if (threads == kNodeThreads / 2) k_node_batch_mixed<kNodeThreads / 2, false><<<grid, threads, 0, st>>>(T);
+        else k_node_batch_mixed<kNodeThreads, false><<<grid, kNodeThreads, 0, st>>>(T);
+    }
 }
 int occupancy_element_batch_mixed(int ept) {
     int nb = 0;
     set_element_mixed_attributes();  // the batch's init passes run the single-instance kernels
     // dynamic shared memory above the default 48 KB: set on the current
     // device before any launch or capture
-    cudaFuncSetAttribute(k_element_batch_mixed<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_element_batch_mixed<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          static_cast<int>(kBatchStageSmem));
-    cudaFuncSetAttribute(k_element_batch_mixed<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_element_batch_mixed<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(kBatchStageSmem));
+    cudaFuncSetAttribute(k_element_batch_mixed<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          static_cast<int>(kBatchStageSmem));
     if (ept == 2)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_batch_mixed<2>, kStageTile / 2, kBatchStageSmem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_batch_mixed<2, false>, kStageTile / 2,
+                                                      kBatchStageSmem);
     else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_batch_mixed<1>, kStageTile, kBatchStageSmem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_batch_mixed<1, false>, kStageTile, kBatchStageSmem);
     return nb;
 }
 
@@ -1536,9 +1550,9 @@ int batch_node_tile(bool mixed_precision) { return 32 * (mixed_precision ? kNode
 int occupancy_node_batch_mixed(int threads) {
     int nb = 0;
     if (threads == kNodeThreads / 2)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_node_batch_mixed<kNodeThreads / 2>, threads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_node_batch_mixed<kNodeThreads / 2, false>, threads, 0);
     else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_node_batch_mixed<kNodeThreads>, kNodeThreads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_node_batch_mixed<kNodeThreads, false>, kNodeThreads, 0);
     return nb;
 }
 

@@ -273,3 +273,14 @@ def test_mixed_batch_matches_single_under_each_assembly(assembly):
         drain(b)
         for s, c, ref in zip(ss, cases, refs):
             assert_same(b.download(s), b.report(s), b.energy(s), ref, c.name)
+
+
+def test_prepared_instance_must_match_the_batch():
+    c = sweep_case(60, 10)
+    with make_batch(capi.MIXED) as b:
+        for prec, asm in ((capi.FP64, capi.ASSEMBLY_AUTO), (capi.MIXED, capi.ASSEMBLY_PATCH)):
+            pr = capi.Prepared(c.x0, c.conn, c.v0, material=c.mat, controls=c.ctl, precision=prec, assembly=asm)
+            with pytest.raises(capi.EnscError, match="ENSC_ERR_ARG"):
+                b.add_prepared(pr)
+            pr.close()
+        assert b.instances == 0
