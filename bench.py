@@ -34,7 +34,11 @@ Further legs of the same run (one GPU):
                  under a 150 GB budget: solves/s and p50/p99 latency; the
                  first 100 requests also through the plain FP64 stepper one
                  at a time (latency, and each result's mixed error and
-                 energy drift against FP64).
+                 energy drift against FP64), and alone through the same
+                 server; attached to it, the deck-reading time of the
+                 reference reader and DataInFast on a 500,000-element deck
+                 (``deck_read``) and output written while the device steps
+                 against output written synchronously (``output_overlap``).
 
 Arms:
   --impl ours (default)  the sm_100a stepper through the C ABI
@@ -586,6 +590,65 @@ def deck_read_leg(elements_per_side=(100, 100, 50)) -> dict:
     return out
 
 
+def output_leg(local, frames: int = 6, interval: int = 1000, dims=(128, 64, 32)) -> dict:
+    """Output written while the device steps (ensc_snapshot_begin /
+    ensc_step_until_async / ensc_snapshot_wait, the drop-in's output
+    pattern), mixed precision on a 128x64x32 block (262,144 elements):
+    `frames` output intervals of `interval` cycles, at each output time the
+    fields x, u, v, a, reactions and sigma are encoded as base64, as the .vtu
+    writer does.  (a) no output; (b) output overlapped: begin the snapshot,
+    enqueue the next interval, then take and encode the snapshot while it
+    runs; (c) output written synchronously: run the interval, download,
+    encode.  Wall times; hidden = (c - b) / (c - a), the share of the output
+    cost that overlapping takes off the critical path."""
+    import base64
+    import numpy as np
+    import torch
+    from enscdynamics_b200 import capi
+    from enscdynamics_b200 import workloads as W
+    nx, ny, nz = dims
+    p = W.block(nx, ny, nz, 1.0 * nx / 256, 0.5 * ny / 128, 0.25 * nz / 64)
+    stream = torch.cuda.Stream()
+
+    def encode(fields):
+        return sum(len(base64.b64encode(np.ascontiguousarray(v).tobytes())) for v in fields.values()
+                   if isinstance(v, np.ndarray))
+
+    times = {}
+    with capi.Stepper(p.mesh.x0, p.mesh.conn, p.v0, material=p.material, controls=p.controls, device=local,
+                      stream=stream.cuda_stream, precision=capi.MIXED) as s:
+        s.set_bcs(p.bc_code, p.bc_value)
+        s.step(interval)
+        enc = 0
+        for mode in ("none", "overlapped", "synchronous", "none_again"):
+            s.step(1)  # a force pass since the last download
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(frames):
+                if mode.startswith("none"):
+                    s.step_async(interval)
+                    s.sync()
+                elif mode == "overlapped":
+                    s.snapshot_begin()
+                    s.step_until_async(interval, math.inf, math.inf)
+                    enc += encode(s.snapshot_wait())
+                    s.sync()
+                else:
+                    s.step_async(interval)
+                    s.sync()
+                    enc += encode(s.download({"x": np.empty((p.mesh.n_nodes, 3)), "u": np.empty((p.mesh.n_nodes, 3)),
+                                              "v": np.empty((p.mesh.n_nodes, 3)),
+                                              "sigma": np.empty((p.mesh.n_elements, 6))}))
+            torch.cuda.synchronize()
+            times[mode] = time.perf_counter() - t0
+    a = min(times["none"], times["none_again"])
+    b, c = times["overlapped"], times["synchronous"]
+    return {"elements": p.mesh.n_elements, "frames": frames, "cycles_per_frame": interval,
+            "no_output_s": a, "overlapped_s": b, "synchronous_s": c,
+            "hidden": (c - b) / (c - a) if c > a else None, "encoded_bytes": enc,
+            "note": "synchronous output downloads x, u, v, sigma; overlapped snapshots also carry a and reactions"}
+
+
 def serve_leg(args, local):
     """Serving stream: args.serve_requests Poisson arrivals at 50/s, element
     counts log-uniform in 1k-500k, 1000-10000 cycles, elastic or J2, mixed
@@ -757,6 +820,7 @@ def run_ours(args):
         serve = serve_leg(args, local)
         if rank == 0:
             serve["deck_read"] = deck_read_leg()
+            serve["output_overlap"] = output_leg(local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
