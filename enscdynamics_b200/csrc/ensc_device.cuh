@@ -418,8 +418,11 @@ __host__ __device__ inline int16_t* v_lo_rows(void* v, int64_t nn_pad) {
 template <int W, typename T>
 __device__ __forceinline__ void ld_row(const T* p, T (&o)[W]) {
     constexpr int kBytes = W * static_cast<int>(sizeof(T));
-    static_assert(kBytes % 16 == 0 || kBytes == 8, "16-byte chunks or one 8-byte chunk");
-    if constexpr (kBytes == 8) {
+    static_assert(kBytes % 16 == 0 || kBytes == 8 || kBytes == 4, "16-byte chunks or one 8- or 4-byte chunk");
+    if constexpr (kBytes == 4) {
+        const uint32_t q = *reinterpret_cast<const uint32_t*>(p);
+        memcpy(o, &q, 4);
+    } else if constexpr (kBytes == 8) {
         const uint2 q = *reinterpret_cast<const uint2*>(p);
         memcpy(o, &q, 8);
     } else {
@@ -433,8 +436,12 @@ __device__ __forceinline__ void ld_row(const T* p, T (&o)[W]) {
 template <int W, typename T>
 __device__ __forceinline__ void st_row(T* p, const T (&v)[W]) {
     constexpr int kBytes = W * static_cast<int>(sizeof(T));
-    static_assert(kBytes % 16 == 0 || kBytes == 8, "16-byte chunks or one 8-byte chunk");
-    if constexpr (kBytes == 8) {
+    static_assert(kBytes % 16 == 0 || kBytes == 8 || kBytes == 4, "16-byte chunks or one 8- or 4-byte chunk");
+    if constexpr (kBytes == 4) {
+        uint32_t q;
+        memcpy(&q, v, 4);
+        *reinterpret_cast<uint32_t*>(p) = q;
+    } else if constexpr (kBytes == 8) {
         uint2 q;
         memcpy(&q, v, 8);
         *reinterpret_cast<uint2*>(p) = q;
