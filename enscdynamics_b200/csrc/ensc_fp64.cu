@@ -1023,11 +1023,15 @@ __device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v)
     return v;
 }
 
-// A batch stage: the single-instance stage (B0^T included), then the tile's
-// instance descriptor, its element-pass scalars (StageHdr), the TileInfo the
-// filling warp writes, and the ETileSrc record of the tile that uses the
-// stage next (as in the mixed batch pass).
-constexpr uint32_t kF64DescOff = f64_stage_bytes<true>();
+// A batch stage: the element rows of a tile of kF64BatchTile elements (as the
+// single-instance stage, B0^T included), then the tile's instance
+// descriptor, its element-pass scalars (StageHdr), the TileInfo the filling
+// warp writes, and the ETileSrc record of the tile that uses the stage next
+// (as in the mixed batch pass).
+constexpr int kF64BatchTile = ENSC_F64_BATCH_TILE;
+static_assert(kF64BatchTile % 32 == 0, "whole warps per tile");
+constexpr uint32_t kF64DescOff =
+    8u * kF64BatchTile * 4u + static_cast<uint32_t>(kF64StageRows + 24) * kF64BatchTile * 8u;
 constexpr uint32_t kF64HdrOff = kF64DescOff + sizeof(InstanceDesc);
 constexpr uint32_t kF64InfoOff = kF64HdrOff + sizeof(StageHdr);
 constexpr uint32_t kF64NextOff = kF64InfoOff + sizeof(TileInfo);
@@ -1062,13 +1066,13 @@ __device__ __forceinline__ void f64_batch_stage_issue(const BatchTables& T, cons
     }
     __syncwarp();
     fence_proxy_async_smem();  // the block's reads of this stage come before the copies into it
-    const uint32_t dbase = dst + 8u * kStageTileF64 * 4u;
+    const uint32_t dbase = dst + 8u * kF64BatchTile * 4u;
     for (int q = lane; q < 8 + drows + 3; q += 32) {
         if (q < 8)
-            bulk_g2s(dst + q * (kStageTileF64 * 4u), static_cast<const uint32_t*>(src.conn) + q * src.ne_pad,
+            bulk_g2s(dst + q * (kF64BatchTile * 4u), static_cast<const uint32_t*>(src.conn) + q * src.ne_pad,
                      cnt * 4u, bar);
         else if (q < 8 + drows)
-            bulk_g2s(dbase + (q - 8) * (kStageTileF64 * 8u), f64_tile_row(src, q - 8), cnt * 8u, bar);
+            bulk_g2s(dbase + (q - 8) * (kF64BatchTile * 8u), f64_tile_row(src, q - 8), cnt * 8u, bar);
         else if (q == 8 + drows)
             bulk_g2s(dst + kF64DescOff, T.desc + src.slot, sizeof(InstanceDesc), bar);
         else if (q == 8 + drows + 1)
@@ -1082,9 +1086,9 @@ __device__ __forceinline__ void f64_batch_stage_issue(const BatchTables& T, cons
 // states are bit-identical to the single-instance pass.  A block's
 // consecutive tiles of one instance form a run whose sums and minima are
 // reduced once, into the partial slot of the run's first tile.
-__global__ void __launch_bounds__(kStageTileF64, kStageMinbF64) k_element_batch_fp64(BatchTables T) {
+__global__ void __launch_bounds__(kF64BatchTile, 256 / kF64BatchTile) k_element_batch_fp64(BatchTables T) {
     extern __shared__ __align__(128) unsigned char smem[];
-    constexpr int TT = kStageTileF64;
+    constexpr int TT = kF64BatchTile;
     constexpr int NW = TT / 32;
     constexpr uint32_t SB = kF64BatchStageBytes;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
@@ -1331,7 +1335,7 @@ int occupancy_node_fp64() {
 
 
 void launch_element_batch_fp64(const BatchTables& T, int grid, cudaStream_t st) {
-    k_element_batch_fp64<<<grid, kStageTileF64, kF64BatchStageSmem, st>>>(T);
+    k_element_batch_fp64<<<grid, kF64BatchTile, kF64BatchStageSmem, st>>>(T);
 }
 void launch_node_batch_fp64(const BatchTables& T, int grid, int threads, cudaStream_t st) {
     if (threads == kNodeThreads / 2) k_node_batch_fp64<kNodeThreads / 2><<<grid, threads, 0, st>>>(T);
@@ -1343,11 +1347,11 @@ int occupancy_element_batch_fp64() {
     // device before any launch or capture
     cudaFuncSetAttribute(k_element_batch_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          static_cast<int>(kF64BatchStageSmem));
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_batch_fp64, kStageTileF64, kF64BatchStageSmem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_element_batch_fp64, kF64BatchTile, kF64BatchStageSmem);
     return nb;
 }
 
-int batch_element_tile_fp64() { return kStageTileF64; }
+int batch_element_tile_fp64() { return kF64BatchTile; }
 int occupancy_node_batch_fp64(int threads) {
     int nb = 0;
     if (threads == kNodeThreads / 2)
