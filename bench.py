@@ -23,6 +23,8 @@ memory, runs the step's cycles and reads u, v and sigma back, over --steps
 steps.
 
 Further legs of the same run (one GPU):
+  batched_block  the block workload as a one-instance batch, mixed and FP64
+                 (the batched engine's own rate on the headline mesh);
   batched_sweep  256 uneven cantilever/plate instances (2k-60k elements, own
                  material, dt and clock), 3000 cycles each, in one mixed
                  batch and in one FP64 batch (every instance's mixed error
@@ -96,6 +98,8 @@ def parse():
     ap.add_argument("--sweep-cycles", type=int, default=3000)
     ap.add_argument("--sweep-fp64-sample", type=int, default=32)
     ap.add_argument("--serve-requests", type=int, default=500, help="serving leg (0: skip)")
+    ap.add_argument("--batched-block-cycles", type=int, default=1024,
+                    help="timed cycles of the block as a one-instance batch, each precision (0: skip)")
     ap.add_argument("--serve-seq-sample", type=int, default=100,
                     help="requests of the serving stream also served by the plain FP64 stepper one at a time")
     return ap.parse_args()
@@ -472,6 +476,43 @@ def shard(n: int, world: int, rank: int) -> list:
     return list(range(rank, n, world))
 
 
+def batched_block_leg(args, local, p) -> dict:
+    """The block workload through the batched engine, one instance per
+    batch, mixed and FP64: after the autotuner's runs (700 cycles),
+    args.batched_block_cycles cycles timed with CUDA events; then 64 more
+    cycles inside an NVTX range named batched_block_<precision>, for a
+    kernel launch list of the batched passes."""
+    import torch
+    from enscdynamics_b200 import capi
+    stream = torch.cuda.Stream()
+    out = {}
+    for prec, name in ((capi.MIXED, "mixed"), (capi.FP64, "fp64")):
+        with capi.Batch(max_instances=1, max_elements=p.mesh.n_elements, max_nodes=p.mesh.n_nodes,
+                        budget_bytes=100 * 10 ** 9, precision=prec, device=local, stream=stream.cuda_stream) as b:
+            sl = b.add(p.mesh.x0, p.mesh.conn, p.v0, material=p.material, controls=p.controls)
+            b.set_bcs(sl, p.bc_code, p.bc_value)
+            b.arm(sl, 10 ** 9)
+            b.run(700)
+            b.sync()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            b.run(args.batched_block_cycles)
+            e1.record(stream)
+            b.sync()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / args.batched_block_cycles
+            torch.cuda.nvtx.range_push(f"batched_block_{name}")
+            b.run(64)
+            b.sync()
+            torch.cuda.nvtx.range_pop()
+            out[name] = {"element_cycles_per_s": p.mesh.n_elements / (ms / 1000.0), "ms_per_cycle": ms,
+                         "tuning": b.tuning}
+    out["mixed_over_batched_fp64"] = out["mixed"]["element_cycles_per_s"] / out["fp64"]["element_cycles_per_s"]
+    return out
+
+
 def sweep_leg(args, local, world=1, rank=0, barrier=lambda: None, max_over_ranks=lambda x: x,
               sum_over_ranks=lambda x: x):
     """Batched parameter sweep: args.sweep_instances uneven instances, each
@@ -815,7 +856,11 @@ def run_ours(args):
     e2e = e2e_block(args, s_head, stream, max_over_ranks, sum_over_ranks, barrier)
     s_head.close()
 
-    sweep = serve = None
+    sweep = serve = bblock = None
+    if rank == 0 and world == 1 and args.batched_block_cycles > 0 and args.workload == "block":
+        bblock = batched_block_leg(args, local, p)
+        if cmp is not None:
+            bblock["mixed_over_plain_fp64"] = bblock["mixed"]["element_cycles_per_s"] / cmp["fp64_value"]
     if args.sweep_instances > 0:
         sweep = sweep_leg(args, local, world, rank, barrier, max_over_ranks, sum_over_ranks)
     if world == 1 and args.serve_requests > 0:
@@ -864,6 +909,7 @@ def run_ours(args):
         "cycle_roofline": m_head["cycle_roofline"],
         "kernel_share": m_head["kernel_share"],
         "fp64_vs_mixed": cmp,
+        "batched_block": bblock,
         "batched_sweep": sweep,
         "serving": serve,
         "cpu_baseline": cpu,
