@@ -30,7 +30,9 @@ Further legs of the same run (one GPU):
                  batch and in one FP64 batch (every instance's mixed error
                  and energy drift against its FP64 run; the maximum is
                  reported); the plain FP64 stepper solves a sample of them
-                 one after another;
+                 one after another; the reference CPU stepper solves a
+                 sample as one process per instance on all host cores
+                 (``cpu_reference``);
   serving        a seeded Poisson stream (50/s, 500 requests) of
                  1k-500k-element solves served with continuous batching
                  under a 150 GB budget: solves/s and p50/p99 latency; the
@@ -272,6 +274,42 @@ class CpuReference:
     def close(self):
         import shutil
         shutil.rmtree(self.dir, ignore_errors=True)
+
+
+def cpu_sweep_leg(sweep_cycles: int, sample: int = 16, cycles: int = 40) -> dict:
+    """The reference CPU stepper on the batched sweep, solved the way the
+    reference can solve many instances at once: one process per instance
+    (its solver state is process-wide), one OpenMP thread each, as many
+    concurrent processes as host cores.  A bounded sample: the first `sample`
+    instances of the sweep (elastic: the reference has no J2), `cycles`
+    cycles each, all started together; solves/s extrapolates each instance's
+    cycle loop to the sweep's cycle count and adds its parse and setup."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from concurrent.futures import ThreadPoolExecutor
+    from enscdynamics_b200 import workloads as W
+    if not pyoracle.harness_available():
+        return {"unavailable": "reference harness not built (oracle/_ref)"}
+    cores = os.cpu_count() or 1
+    n = max(1, min(sample, cores))
+    probs = [W.sweep_instance(i, cycles=sweep_cycles) for i in range(n)]
+    dirs = [tempfile.mkdtemp(prefix="ensc_sweep_ref_") for _ in probs]
+    try:
+        decks = [q.write_deck(d) for q, d in zip(probs, dirs)]
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(n) as pool:
+            runs = list(pool.map(lambda a: pyoracle.run_reference(a[0], a[1], "time", cycles, threads=1),
+                                 zip(dirs, decks)))
+        wall = time.perf_counter() - t0
+    finally:
+        import shutil
+        for d in dirs:
+            shutil.rmtree(d, ignore_errors=True)
+    solve_s = [r["parse_s"] + r["loop_s"] * sweep_cycles / cycles for r in runs]
+    work = sum(q.mesh.n_elements for q in probs) * cycles
+    return {"processes": n, "cores": cores, "sample": f"first {n} sweep instances, elastic, {cycles} cycles each",
+            "solves_per_s": n / statistics.mean(solve_s) if n else 0.0,
+            "element_cycles_per_s": work / max(r["loop_s"] for r in runs), "wall_s": wall}
 
 
 def run_reference_arm(args):
@@ -869,6 +907,10 @@ def run_ours(args):
             serve["deck_read"] = deck_read_leg()
             serve["output_overlap"] = output_leg(local)
 
+    if sweep is not None and rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sweep["cpu_reference"] = cpu_sweep_leg(args.sweep_cycles)
+        if sweep["cpu_reference"].get("solves_per_s"):
+            sweep["speedup_vs_cpu_reference"] = sweep["solves_per_s"] / sweep["cpu_reference"]["solves_per_s"]
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         ref = CpuReference()
