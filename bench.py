@@ -57,7 +57,10 @@ an independent replica of the block workload (the stepper has no
 cross-instance exchange), so scaling is weak and ``value`` sums all ranks'
 element-cycles over the slowest rank's device time.  The sweep's instances
 are sharded across the ranks (every world-th instance per rank, no
-collective on the data path); the serving leg runs at one GPU only.
+collective on the data path); the serving stream is sharded the same way
+by request (every rank serves every world-th request on its own GPU; the
+outcomes are gathered for the stream's percentiles), and its comparisons
+with the sequential FP64 stepper run at one GPU only.
 """
 from __future__ import annotations
 
@@ -730,6 +733,44 @@ def output_leg(local, frames: int = 6, interval: int = 1000, dims=(128, 64, 32))
             "fields": "x, u, v, a, reactions, sigma"}
 
 
+def gather_outcomes(outcomes, world: int) -> list:
+    """Every rank's serving outcomes on every rank (all_gather of plain
+    tuples; identity at one rank), rebuilt as Outcome objects."""
+    from enscdynamics_b200 import serving as S
+    rows = [(o.index, o.arrival, o.admitted, o.finished, o.cycles, o.status, o.elements) for o in outcomes]
+    if world > 1:
+        import torch.distributed as dist
+        parts = [None] * world
+        dist.all_gather_object(parts, rows)
+        rows = [r for part in parts for r in part]
+    out = [S.Outcome(i, a, admitted=ad, finished=f, cycles=c, status=st, elements=e) for i, a, ad, f, c, st, e in rows]
+    return sorted(out, key=lambda o: o.index)
+
+
+def serve_leg_ranks(args, local, world: int, rank: int, barrier) -> dict:
+    """The serving stream over several GPUs: the same seeded stream, every
+    world-th request served by this rank's own loop and batch on its own GPU
+    (instances are independent, so no collective on the data path); the
+    outcomes are gathered for the whole stream's solves/s and latency
+    percentiles."""
+    from enscdynamics_b200 import serving as S
+    from enscdynamics_b200 import workloads as W
+    reqs = W.serving_requests(args.serve_requests, rate=50.0, seed=11)
+    mine = [r for r in reqs if r.index % world == rank]
+    workers = max(1, min(4, (os.cpu_count() or 2) // max(1, world) - 1))
+    be = S.BatchBackend(budget_bytes=150 * 10 ** 9, max_instances=1024, device=local, fields=())
+    srv = S.Server(be, prepare_workers=workers)
+    barrier()  # the ranks start the stream together
+    try:
+        out = srv.serve(mine)
+    finally:
+        be.close()
+    summ = S.summarize(gather_outcomes(out, world))
+    summ.update({"rate_per_s": 50.0, "budget_bytes_per_gpu": 150 * 10 ** 9, "precision": "mixed", "ranks": world,
+                 "sharding": "request i on rank i mod world"})
+    return summ
+
+
 def serve_leg(args, local):
     """Serving stream: args.serve_requests Poisson arrivals at 50/s, element
     counts log-uniform in 1k-500k, 1000-10000 cycles, elastic or J2, mixed
@@ -901,8 +942,8 @@ def run_ours(args):
             bblock["mixed_over_plain_fp64"] = bblock["mixed"]["element_cycles_per_s"] / cmp["fp64_value"]
     if args.sweep_instances > 0:
         sweep = sweep_leg(args, local, world, rank, barrier, max_over_ranks, sum_over_ranks)
-    if world == 1 and args.serve_requests > 0:
-        serve = serve_leg(args, local)
+    if args.serve_requests > 0:
+        serve = serve_leg(args, local) if world == 1 else serve_leg_ranks(args, local, world, rank, barrier)
         if rank == 0:
             serve["deck_read"] = deck_read_leg()
             serve["output_overlap"] = output_leg(local)

@@ -94,3 +94,32 @@ def test_sweep_shards_partition_the_instances():
         flat = sorted(i for p in parts for i in p)
         assert flat == list(range(256))
         assert max(len(p) for p in parts) - min(len(p) for p in parts) <= 1
+
+
+_GATHER_WORKER = r"""
+import json, os, sys
+sys.path.insert(0, {root!r})
+import torch.distributed as dist
+import bench
+from enscdynamics_b200 import serving as S
+rank = int(os.environ["RANK"]); world = int(os.environ["WORLD_SIZE"])
+dist.init_process_group("gloo", init_method="env://", rank=rank, world_size=world)
+# rank r served requests r, r + world, ...: arrival i / 10 s, latency 1 + i s
+mine = [S.Outcome(i, i / 10.0, admitted=i / 10.0, finished=i / 10.0 + 1.0 + i, cycles=100, elements=1000)
+        for i in range(rank, 10, world)]
+allo = bench.gather_outcomes(mine, world)
+summ = S.summarize(allo)
+dist.destroy_process_group()
+print(json.dumps({{"indices": [o.index for o in allo], "requests": summ["requests"],
+                   "p50": summ["p50_latency_s"], "makespan": summ["makespan_s"]}}))
+"""
+
+
+def test_serving_outcomes_are_gathered_over_ranks():
+    """The multi-GPU serving leg shards the stream by request index; every
+    rank ends with the whole stream's outcomes for its percentiles."""
+    outs = [json.loads(o.strip().splitlines()[-1]) for o in _run_ranks(_GATHER_WORKER.format(root=ROOT))]
+    for o in outs:
+        assert o["indices"] == list(range(10)) and o["requests"] == 10
+        assert o["p50"] == pytest.approx(5.5)          # latencies 1..10 s
+        assert o["makespan"] == pytest.approx(10.9)    # first arrival 0, last finish 0.9 + 10
