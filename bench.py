@@ -548,8 +548,9 @@ def batched_block_leg(args, local, p) -> dict:
             b.run(64)
             b.sync()
             torch.cuda.nvtx.range_pop()
+            cb = cycle_bytes(p.mesh.n_elements, p.mesh.n_nodes, True, prec == capi.MIXED)
             out[name] = {"element_cycles_per_s": p.mesh.n_elements / (ms / 1000.0), "ms_per_cycle": ms,
-                         "tuning": b.tuning}
+                         "cycle_frac": cb / (ms / 1000.0) / 1e9 / measured_peaks()[0], "tuning": b.tuning}
     out["mixed_over_batched_fp64"] = out["mixed"]["element_cycles_per_s"] / out["fp64"]["element_cycles_per_s"]
     return out
 
@@ -634,6 +635,13 @@ def sweep_leg(args, local, world=1, rank=0, barrier=lambda: None, max_over_ranks
     seq = sum_over_ranks(k / (seq_ms / 1000.0))
     rate_mx = ne_all * cyc / (ms / 1000.0)
     rate_64 = ne_all * cyc / (f64["ms"] / 1000.0)
+    # the cycle bytes of all instances (the batched passes run the J2 update
+    # for every instance), over the batch's time, against the copy peak
+    peak, peak_kind = measured_peaks()
+    bytes_mx = sum_over_ranks(float(sum(cycle_bytes(p.mesh.n_elements, p.mesh.n_nodes, True, True) for p in probs)))
+    bytes_64 = sum_over_ranks(float(sum(cycle_bytes(p.mesh.n_elements, p.mesh.n_nodes, True) for p in probs)))
+    gbs_mx = bytes_mx * cyc / (ms / 1000.0) / 1e9
+    gbs_64 = bytes_64 * cyc / (f64["ms"] / 1000.0) / 1e9
     return {"instances": n, "cycles": cyc, "elements": int(ne_all), "ranks": world,
             "elements_range": [min(p.mesh.n_elements for p in probs), max(p.mesh.n_elements for p in probs)],
             "precision": "mixed", "solves_per_s": batched, "element_cycles_per_s": rate_mx,
@@ -645,6 +653,9 @@ def sweep_leg(args, local, world=1, rank=0, barrier=lambda: None, max_over_ranks
             "batched_fp64": {"element_cycles_per_s": rate_64, "solves_per_s": n / (f64["ms"] / 1000.0),
                              "ms": f64["ms"], "tuning": f64["tuning"]},
             "mixed_over_batched_fp64": rate_mx / rate_64,
+            "cycle_roofline": {"mixed_gbs": gbs_mx, "mixed_frac": gbs_mx / peak, "fp64_gbs": gbs_64,
+                               "fp64_frac": gbs_64 / peak, "peak": peak, "peak_source": peak_kind,
+                               "nodes_per_element": float(sum_over_ranks(float(nn_tot))) / ne_all},
             "sequential_fp64": {"sample": int(sum_over_ranks(float(k))), "solves_per_s": seq,
                                 "element_cycles_per_s": sum_over_ranks(seq_work / (seq_ms / 1000.0))},
             "speedup_vs_sequential_fp64": batched / seq}

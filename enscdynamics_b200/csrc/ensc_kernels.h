@@ -60,6 +60,11 @@ constexpr int kNodeUnrollMixed = ENSC_NODE_UNROLL_MIXED;
 #ifndef ENSC_MIXED_PREFETCH
 #define ENSC_MIXED_PREFETCH 3
 #endif
+// 1: the mixed passes' L1 prefetches form their addresses inside the asm
+// statement (prefetch_l1_at), so that no address stays live until the load
+#ifndef ENSC_PF_OPAQUE
+#define ENSC_PF_OPAQUE 0
+#endif
 // how the batched mixed element pass reads the staged instance descriptor:
 // 1 all fields copied to registers per tile, 2 arrays copied and material
 // constants read at use, 0 everything read at use
