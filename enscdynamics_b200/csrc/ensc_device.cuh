@@ -484,17 +484,6 @@ __device__ __forceinline__ NodeParam ld_param(const NodeParam* p) {
 __device__ __forceinline__ void prefetch_l1(const void* p) {
     asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
 }
-// The same for row[i], the address formed inside the asm statement: the
-// compiler cannot share it with the later loads of row[i], so prefetching a
-// row entry keeps no 64-bit address live until that load.
-template <typename T>
-__device__ __forceinline__ void prefetch_l1_at(const T* row, uint32_t i) {
-    asm volatile(
-        "{\n\t.reg .u64 a;\n\t"
-        "mad.wide.u32 a, %1, %2, %0;\n\t"
-        "prefetch.global.L1 [a];\n\t}" ::"l"(row),
-        "r"(i), "n"(static_cast<int>(sizeof(T))));
-}
 
 // Read-only input loads: through the non-coherent path from global memory,
 // plain loads from a shared-memory stage.

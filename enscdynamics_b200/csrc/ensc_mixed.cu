@@ -218,19 +218,13 @@ __device__ __forceinline__ void element_body_mixed(const ElemArrays& E, const No
 #pragma unroll
         for (int r = 0; r < 3; ++r)
 #pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                if (ENSC_PF_OPAQUE) prefetch_l1_at(V + r * np, nk[k]);
-                else prefetch_l1(V + r * np + nk[k]);
-            }
+            for (int k = 0; k < 8; ++k) prefetch_l1(V + r * np + nk[k]);
     }
     if (PF & 2) {
 #pragma unroll
         for (int r = 1; r < 3; ++r)
 #pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                if (ENSC_PF_OPAQUE) prefetch_l1_at(X + r * np, nk[k]);
-                else prefetch_l1(X + r * np + nk[k]);
-            }
+            for (int k = 0; k < 8; ++k) prefetch_l1(X + r * np + nk[k]);
     }
     // coordinates relative to node 0, as FP64 differences, one component at a
     // time: hourglass projections TAU x = TAU (x - x0) (the Gamma rows sum to
