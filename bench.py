@@ -193,16 +193,17 @@ def element_pass_bytes(ne: int, nn: int, plastic: bool, mixed: bool = False, pat
 
 def node_pass_bytes(ne: int, nn: int, mixed: bool = False, partials: int = 0) -> int:
     """Algorithmic bytes of one node-pass launch: the element forces, and
-    per node the inverse mass 8, BC code 1, x and u read and write 96, v read
-    and write (48 FP64; mixed: 24 for the float rows and 12 for their 16-bit
-    residual rows).  Slot assembly: the 24 force components of every element,
+    per node the inverse mass 8, BC code 1, x and u read and write 96 (mixed:
+    x only, 48 -- the mixed stepper keeps x - u in the u rows and forms u
+    when the state is read), v read and write (48 FP64; mixed: 24 for the
+    float rows and 12 for their 16-bit residual rows).  Slot assembly: the 24 force components of every element,
     each read once (192 B FP64, 96 B mixed).  Patch assembly (partials > 0):
     per node its partial range 4, per partial its index 4 and its three sums
     12.  Reactions and prescribed velocities are touched only at constrained
     nodes and not counted; slot-major force slots that no element fills
     (boundary nodes) are read as zeros but not counted."""
     if mixed:
-        per_node = nn * (8 + 1 + 96 + 24 + 12)
+        per_node = nn * (8 + 1 + 48 + 24 + 12)
         if partials:
             return per_node + nn * 4 + partials * (4 + 12)
         return ne * 96 + per_node
@@ -212,8 +213,8 @@ def node_pass_bytes(ne: int, nn: int, mixed: bool = False, partials: int = 0) ->
 def cycle_bytes(ne: int, nn: int, plastic: bool, mixed: bool = False, patches: int = 0, partials: int = 0) -> int:
     """Canonical algorithmic bytes of one cycle (element pass + node pass):
     FP64 904 B per element (+16 with J2) and 225 B per node; mixed with the
-    slot assembly 452 B per element (+8) and 177 B per node; mixed with the
-    patch assembly 276 B per element (+8), 181 B per node and 32 B per
+    slot assembly 452 B per element (+8) and 129 B per node; mixed with the
+    patch assembly 276 B per element (+8), 133 B per node and 32 B per
     partial (about 1.5-1.8 partials per node)."""
     return (element_pass_bytes(ne, nn, plastic, mixed, patches, partials)
             + node_pass_bytes(ne, nn, mixed, partials))

@@ -775,6 +775,8 @@ int ensc_batch_download(ensc_batch* b, int32_t slot, double* x, double* u, doubl
     for (const Item& it : items) {
         if (!it.dst) continue;
         if (it.src == sl.N.v) ensc::launch_v_to_aos(sl.N, mx, stage, b->stream);
+        else if (it.src == sl.N.u && mx && ENSC_MIXED_UREF)
+            ensc::launch_disp_to_aos(sl.N.x, sl.N.u, sl.nn, sl.nn_pad, stage, b->stream);
         else ensc::launch_soa_to_aos(it.src, it.n, it.pad, it.comps, it.f32, stage, b->stream, it.at);
         cudaError_t e = cudaMemcpyAsync(it.dst, stage, it.n * it.comps * sizeof(double), cudaMemcpyDeviceToHost,
                                         b->stream);

@@ -477,6 +477,8 @@ int ensc_download(ensc_handle* h, double* x, double* u, double* v, double* sigma
     for (const Item& it : items) {
         if (!it.dst) continue;
         if (it.src == h->N.v) ensc::launch_v_to_aos(h->N, mx, h->staging, h->stream);
+        else if (it.src == h->N.u && mx && ENSC_MIXED_UREF)
+            ensc::launch_disp_to_aos(h->N.x, h->N.u, h->nn, h->nn_pad, h->staging, h->stream);
         else ensc::launch_soa_to_aos(it.src, it.n, it.pad, it.comps, it.f32, h->staging, h->stream, it.at);
         CK(h, cudaGetLastError());
         CK(h, cudaMemcpyAsync(it.dst, h->staging, it.n * it.comps * sizeof(double), cudaMemcpyDeviceToHost,
@@ -519,6 +521,9 @@ int ensc_upload_state(ensc_handle* h, const double* x, const double* u, const do
                           {qia, h->E.qia, h->ne, h->ne_pad, 12, mx, ep},
                           {eps_p, h->E.eps_p, h->ne, h->ne_pad, 1, mx, ep}};
     size_t used = 0;
+    // mixed: the u rows hold x - u; they hold u while x and u are replaced
+    const bool uref = mx && ENSC_MIXED_UREF && (x || u);
+    if (uref) ensc::launch_reflect_rows(h->N.x, h->N.u, h->nn, h->nn_pad, h->stream);
     for (const Item& it : items) {
         if (!it.src) continue;
         CK(h, cudaMemcpyAsync(h->staging, it.src, it.n * it.comps * sizeof(double), cudaMemcpyHostToDevice,
@@ -528,6 +533,8 @@ int ensc_upload_state(ensc_handle* h, const double* x, const double* u, const do
         CK(h, cudaGetLastError());
         used = std::max(used, static_cast<size_t>(it.n * it.comps) * sizeof(double));
     }
+    if (uref) ensc::launch_reflect_rows(h->N.x, h->N.u, h->nn, h->nn_pad, h->stream);
+    CK(h, cudaGetLastError());
     if (int rc0 = release_staging(h, used)) return rc0;
     int rc = read_ctl(h);
     if (rc) return rc;
@@ -579,7 +586,8 @@ int ensc_snapshot_begin(ensc_handle* h) {
     if (mx) ensc::launch_acceleration_mixed(h->E, h->N, h->M, h->ctl, d + 3 * nodes3, h->stream, h->PA);
     else ensc::launch_acceleration_fp64(h->E, h->N, h->M, h->ctl, d + 3 * nodes3, h->stream);
     ensc::launch_soa_to_aos(h->N.x, h->nn, h->nn_pad, 3, false, d, h->stream);
-    ensc::launch_soa_to_aos(h->N.u, h->nn, h->nn_pad, 3, false, d + nodes3, h->stream);
+    if (mx && ENSC_MIXED_UREF) ensc::launch_disp_to_aos(h->N.x, h->N.u, h->nn, h->nn_pad, d + nodes3, h->stream);
+    else ensc::launch_soa_to_aos(h->N.u, h->nn, h->nn_pad, 3, false, d + nodes3, h->stream);
     ensc::launch_v_to_aos(h->N, mx, d + 2 * nodes3, h->stream);
     ensc::launch_soa_to_aos(h->N.rf, h->nn, h->nn_pad, 3, false, d + 4 * nodes3, h->stream);
     ensc::launch_soa_to_aos(h->E.sigma, h->ne, h->ne_pad, 6, mx, d + 5 * nodes3, h->stream, h->PA.iperm);

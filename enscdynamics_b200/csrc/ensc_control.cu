@@ -285,6 +285,28 @@ __global__ void k_soa_to_aos(const ST* soa, int64_t n, int64_t pad, int comps, c
     }
 }
 
+// Displacements of a mixed instance, whose u rows hold the reference
+// position xr = x - u: interleaved u = x - xr.
+__global__ void k_disp_to_aos(const double* x, const double* xr, int64_t n, int64_t pad, double* aos) {
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < 3 * n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t e = i / 3;
+        const int64_t k = (i - 3 * e) * pad + e;
+        aos[i] = x[k] - xr[k];
+    }
+}
+
+// a <- x - a over the three node rows: turns the reference position rows of
+// a mixed instance into displacement rows and back
+__global__ void k_reflect_rows(const double* x, double* a, int64_t n, int64_t pad) {
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < 3 * n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t c = i / n;
+        const int64_t k = c * pad + (i - c * n);
+        a[k] = x[k] - a[k];
+    }
+}
+
 // Velocities between interleaved xyz doubles and the device rows.
 template <typename VT>
 __global__ void k_v_to_aos(NodeArrays N, double* aos) {
@@ -478,6 +500,12 @@ void launch_soa_to_aos(const void* soa, int64_t n, int64_t pad, int comps, bool 
     const int g = grid_for(n * comps, 256);
     if (src_fp32) k_soa_to_aos<float><<<g, 256, 0, st>>>(static_cast<const float*>(soa), n, pad, comps, at, aos);
     else k_soa_to_aos<double><<<g, 256, 0, st>>>(static_cast<const double*>(soa), n, pad, comps, at, aos);
+}
+void launch_disp_to_aos(const double* x, const double* xr, int64_t n, int64_t pad, double* aos, cudaStream_t st) {
+    k_disp_to_aos<<<grid_for(3 * n, 256), 256, 0, st>>>(x, xr, n, pad, aos);
+}
+void launch_reflect_rows(const double* x, double* a, int64_t n, int64_t pad, cudaStream_t st) {
+    k_reflect_rows<<<grid_for(3 * n, 256), 256, 0, st>>>(x, a, n, pad);
 }
 void launch_v_to_aos(const NodeArrays& N, bool fp32_v, double* aos, cudaStream_t st) {
     const int g = static_cast<int>(std::min<int64_t>((3 * N.nn + 255) / 256, 65535));

@@ -375,6 +375,16 @@ __host__ __device__ inline double gravity_amplitude(const double* amp, int n, do
 #define ENSC_MIXED_VLO 1
 #endif
 
+// The mixed stepper's element pass forms F from the current coordinates and
+// never reads the displacement, so it keeps the reference position
+// xr = x - u in the u rows instead of u, and the node pass updates x alone:
+// u = x - xr is formed where the state is read (ensc_download, snapshots),
+// and an upload of x or u sets xr = x - u.  Both are FP64: u = x - xr is
+// within a rounding of x's magnitude of the separately accumulated u.
+#ifndef ENSC_MIXED_UREF
+#define ENSC_MIXED_UREF 1
+#endif
+
 // ulp(hi) / 2^16 and its inverse (normal or zero hi; hi's exponent field e
 // gives ulp(hi) = 2^(e - 150), with e = 1 for zero and subnormals)
 __host__ __device__ inline double vlo_unit(float hi) {

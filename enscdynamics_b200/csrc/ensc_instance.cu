@@ -401,6 +401,8 @@ int instance_upload(const InstanceHost& h, void* block, cudaStream_t st, ElemArr
     if (e == cudaSuccess) e = put(block, h.off[P::IM], h.im, st);
     std::vector<double> xs = to_soa<double>(h.x0, h.nn, np, 3);
     if (e == cudaSuccess) e = put(block, h.off[P::X], xs, st);
+    // mixed: the u rows hold the reference position x - u, x0 at the start
+    if (h.mixed && ENSC_MIXED_UREF && e == cudaSuccess) e = put(block, h.off[P::U], xs, st);
     std::vector<double> vd;
     std::vector<float> vf;
     if (h.v0) {

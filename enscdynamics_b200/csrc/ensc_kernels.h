@@ -195,6 +195,10 @@ void launch_soa_to_aos(const void* soa, int64_t n, int64_t pad, int comps, bool 
                        cudaStream_t st, const int32_t* at = nullptr);
 void launch_aos_to_soa(const double* aos, int64_t n, int64_t pad, int comps, void* soa, bool dst_fp32,
                        cudaStream_t st, const int32_t* at = nullptr);
+// displacements of a mixed instance (u rows holding xr = x - u) to
+// interleaved xyz doubles; and a <- x - a over three node rows
+void launch_disp_to_aos(const double* x, const double* xr, int64_t n, int64_t pad, double* aos, cudaStream_t st);
+void launch_reflect_rows(const double* x, double* a, int64_t n, int64_t pad, cudaStream_t st);
 // velocities (FP64 rows, or the mixed stepper's float rows and residual rows)
 // to and from interleaved xyz doubles
 void launch_v_to_aos(const NodeArrays& N, bool fp32_v, double* aos, cudaStream_t st);

@@ -11,7 +11,8 @@
 // rows are A s_j / 8, s_j the node's reference-corner signs) as a float pair,
 // 9 hi then 9 lo rows; sigma, qia, eps_p and fe are float; vol0 is double;
 // cbrt_v0 is a float copy (in the first ne words of its FP64 storage).
-// Node arrays: x, u double; v float.
+// Node arrays: x double; the u rows hold the reference position x - u
+// (double, ENSC_MIXED_UREF); v float with 16-bit residual rows.
 #include "ensc_device.cuh"
 #include "ensc_kernels.h"
 #include "ensc_stage.cuh"
@@ -884,7 +885,7 @@ __device__ __forceinline__ void node_body_mixed(const ElemArrays& E, const NodeA
         const double vnd = static_cast<double>(vn);
         const double vod = static_cast<double>(vo);
 #endif
-        N.u[c * np + n] += dt_i * vnd;
+        if (!ENSC_MIXED_UREF) N.u[c * np + n] += dt_i * vnd;
         N.x[c * np + n] += dt_i * vnd;
         wext += static_cast<double>(g + r) * dt_avg * 0.5 * (vod + vnd);
         kin += 0.5 * (vnd * vnd) / im;
@@ -958,7 +959,7 @@ __device__ __forceinline__ void node_group_mixed(const NodeView& N, const double
         float vo[W], vn[W];
         double uo[W], xo[W], un[W], xn[W];
         ld_row<W>(V + c * np + n0, vo);
-        ld_row<W>(N.u + c * np + n0, uo);
+        if (!ENSC_MIXED_UREF) ld_row<W>(N.u + c * np + n0, uo);
         ld_row<W>(N.x + c * np + n0, xo);
 #if ENSC_MIXED_VLO
         int16_t* VL = v_lo_rows(N.v, np);
@@ -971,7 +972,7 @@ __device__ __forceinline__ void node_group_mixed(const NodeView& N, const double
 #if ENSC_MIXED_VLO
             ln[j] = lo[j];
 #endif
-            un[j] = uo[j];
+            if (!ENSC_MIXED_UREF) un[j] = uo[j];
             xn[j] = xo[j];
             if (n0 + j >= nn) continue;
             float a = f[c][j];
@@ -1000,7 +1001,7 @@ __device__ __forceinline__ void node_group_mixed(const NodeView& N, const double
             const double vnd = static_cast<double>(vn[j]);
             const double vod = static_cast<double>(vo[j]);
 #endif
-            un[j] = uo[j] + dt_i * vnd;
+            if (!ENSC_MIXED_UREF) un[j] = uo[j] + dt_i * vnd;
             xn[j] = xo[j] + dt_i * vnd;
             wext += static_cast<double>(g + r) * dt_avg * 0.5 * (vod + vnd);
             kin += 0.5 * (vnd * vnd) / im[j];
@@ -1010,13 +1011,14 @@ __device__ __forceinline__ void node_group_mixed(const NodeView& N, const double
 #if ENSC_MIXED_VLO
         st_row<W>(VL + c * np + n0, ln);
 #endif
-        st_row<W>(N.u + c * np + n0, un);
+        if (!ENSC_MIXED_UREF) st_row<W>(N.u + c * np + n0, un);
         st_row<W>(N.x + c * np + n0, xn);
     }
 }
 
 // Node pass in mixed precision: FP32 slot-ordered gather and acceleration,
-// FP32 velocity, FP64 displacement / position accumulation and energy.
+// FP32 velocity, FP64 position accumulation and energy (the u rows hold the
+// reference position x - u and are not touched: ENSC_MIXED_UREF).
 // PATCH: the instance uses the patch assembly (one instantiation each, so
 // the slot-assembly pass carries no code of the other).
 template <bool PATCH>

@@ -48,7 +48,7 @@ extern "C" {
 
 /* precision of the stepper */
 #define ENSC_FP64 0     /* plain FP64, operation order of the reference */
-#define ENSC_MIXED 1    /* FP32 element work and gather; FP64 x, u, time, dt, energy */
+#define ENSC_MIXED 1    /* FP32 element work and gather; FP64 x, u (= x - x_ref), time, dt, energy */
 
 /* Force assembly (ensc_params.assembly).  SLOT: every element writes its 8
  * nodal forces to the reference's per-local-slot nodal vectors and the node
