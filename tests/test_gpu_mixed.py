@@ -216,3 +216,38 @@ def test_patch_assembly_restarts_and_chunks_bit_exactly():
     for k in ("u", "v", "x", "sigma", "qia", "eps_p"):
         assert np.array_equal(got[k], ref[k]), k
         assert np.array_equal(got2[k], ref[k]), k
+
+
+def test_mixed_displacement_follows_uploads_of_x_or_u_alone():
+    """The mixed stepper stores x minus a reference position in place of u:
+    uploading x alone leaves u as it was, uploading u alone leaves x as it
+    was, and u follows x's motion over later cycles as a separately
+    accumulated u would (within a rounding of x's magnitude per cycle)."""
+    p = W.block(12, 6, 4, 0.12, 0.06, 0.04, plastic=False)
+    with capi.Stepper(p.mesh.x0, p.mesh.conn, p.v0, material=p.material, controls=p.controls,
+                      precision=capi.MIXED) as s, \
+            capi.Stepper(p.mesh.x0, p.mesh.conn, p.v0, material=p.material, controls=p.controls,
+                         precision=capi.FP64) as f:
+        for st in (s, f):
+            st.set_bcs(p.bc_code, p.bc_value)
+            st.step(200)
+        a = s.download()
+        b = f.download()
+        # u equals x - x0 to the rounding of x, as FP64's accumulated u does
+        scale = np.abs(a["x"]).max()
+        assert np.abs(a["u"] - (a["x"] - p.mesh.x0)).max() <= 1e-14 * scale
+        assert np.abs(b["u"] - (b["x"] - p.mesh.x0)).max() <= 1e-12 * scale
+        clk = s.step(0)
+        shift = np.full_like(a["x"], 1e-4)
+        s.upload_state({"x": a["x"] + shift}, clk["time"], clk["dt_i"], clk["dt_i_1"], clk["dt_stable_min"])
+        c = s.download()
+        assert np.array_equal(c["x"], a["x"] + shift)
+        assert np.abs(c["u"] - a["u"]).max() <= 1e-15 * scale
+        s.upload_state({"u": a["u"] + shift}, clk["time"], clk["dt_i"], clk["dt_i_1"], clk["dt_stable_min"])
+        d = s.download()
+        assert np.array_equal(d["x"], c["x"])
+        assert np.abs(d["u"] - (a["u"] + shift)).max() <= 1e-15 * scale
+        # later motion moves u with x
+        s.step(50)
+        e = s.download()
+        assert np.abs((e["u"] - d["u"]) - (e["x"] - d["x"])).max() <= 1e-14 * scale
