@@ -70,7 +70,10 @@ constexpr int kNodeUnrollMixed = ENSC_NODE_UNROLL_MIXED;
 #define ENSC_BATCH_DESC_MODE 2
 #endif
 // 1: the grouped node passes sum all 8 force slots (empty ones hold zeros)
-// instead of reading the slot mask first
+// instead of reading the slot mask first (measured on B200, mixed: reading
+// the mask made the node pass 22% slower on the block and the batched
+// 64-instance sweep of plates and cantilevers, whose many boundary nodes have
+// empty slots, 5% slower)
 #ifndef ENSC_NODE_ALL_SLOTS
 #define ENSC_NODE_ALL_SLOTS 1
 #endif
