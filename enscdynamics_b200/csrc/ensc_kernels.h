@@ -51,17 +51,17 @@ constexpr int kNodeUnrollMixed = ENSC_NODE_UNROLL_MIXED;
 #endif
 // The single-instance staged mixed element pass prefetches an element's node
 // rows into L1 before its coordinate phase: bit 0 the velocities, bit 1 the
-// coordinate components 1 and 2 (the batched pass does not: the addresses
-// cost it registers and spills)
-// The same for the batched mixed element pass (measured on B200: the
+// coordinate components 1 and 2
+#ifndef ENSC_MIXED_PREFETCH
+#define ENSC_MIXED_PREFETCH 3
+#endif
+// The same for the batched mixed element pass, off: with the instance's
+// arrays in registers the prefetch addresses spill (measured on B200: the
 // velocity rows there spill 216 B per thread and cost 6%; with the
 // addresses formed inside the prefetch instruction the spill is 36 B and the
 // cost 4-6% on the block and on a 64-instance sweep)
 #ifndef ENSC_BATCH_MIXED_PREFETCH
 #define ENSC_BATCH_MIXED_PREFETCH 0
-#endif
-#ifndef ENSC_MIXED_PREFETCH
-#define ENSC_MIXED_PREFETCH 3
 #endif
 // how the batched mixed element pass reads the staged instance descriptor:
 // 1 all fields copied to registers per tile, 2 arrays copied and material
