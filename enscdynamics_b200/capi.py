@@ -382,10 +382,10 @@ class Stepper:
 
 class Prepared:
     """An instance prepared on the host for Batch.add_prepared
-    (ensc_batch_prepare): element constants, lumped mass and node tables.
-    Holds the arrays the device part reads again.  The work runs in the C
-    library without the interpreter lock, so several requests can be
-    prepared on threads while a batch steps."""
+    (ensc_batch_prepare): element constants, lumped mass, node tables and
+    the device rows, all held by the library (the mesh arrays are not read
+    again).  The work runs in the C library without the interpreter lock, so
+    several requests can be prepared on threads while a batch steps."""
 
     def __init__(self, x0: np.ndarray, conn: np.ndarray, v0: Optional[np.ndarray] = None, *,
                  material: _mesh.Material, controls: _mesh.Controls, precision: int = MIXED,
@@ -399,7 +399,7 @@ class Prepared:
         rc = lib.ensc_batch_prepare(C.byref(m), C.byref(mt), C.byref(p), C.byref(self.h))
         if rc != 0:
             raise EnscError(rc, lib.ensc_last_error(None).decode())
-        self._keep = keep
+        del keep
         self.controls = controls
         self._params = p
         self.precision = precision

@@ -80,6 +80,47 @@ std::vector<T> to_soa(const double* aos, int64_t n, int64_t pad, int comps) {
     return out;
 }
 
+// The rows the upload copies as they are (InstanceHost::a_rows ...): the
+// element geometry in the precision's device form, x0 and v0 as SoA rows.
+// The caller's x0 and v0 are not read after this.
+void form_device_rows(InstanceHost& h) {
+    const int64_t ep = h.ne_pad, np = h.nn_pad;
+    if (h.mixed) {
+        // corner signs s_j of the reference hexahedron (Element_HexN8.cpp:49-91)
+        static const double kCorner[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
+                                             {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
+        h.a_rows.assign(static_cast<size_t>(18 * ep), 0.f);
+        for (int64_t el = 0; el < h.ne; ++el)
+            for (int c = 0; c < 3; ++c)
+                for (int m = 0; m < 3; ++m) {
+                    double v = 0.0;
+                    for (int j = 0; j < 8; ++j) v += h.bt[24 * el + 3 * j + c] * kCorner[j][m];
+                    const float hi = static_cast<float>(v);
+                    h.a_rows[(3 * c + m) * ep + el] = hi;
+                    h.a_rows[(9 + 3 * c + m) * ep + el] = static_cast<float>(v - static_cast<double>(hi));
+                }
+        h.cb_f.assign(h.cb.begin(), h.cb.end());
+    } else {
+        h.bt_rows = to_soa<double>(h.bt.data(), h.ne, ep, 24);
+    }
+    std::vector<double>().swap(h.bt);  // the device form replaces it
+    h.x_rows = to_soa<double>(h.x0, h.nn, np, 3);
+    if (h.v0) {
+        if (h.mixed) {
+            h.v_rows_f = to_soa<float>(h.v0, h.nn, np, 3);
+#if ENSC_MIXED_VLO
+            h.v_lo_rows.assign(static_cast<size_t>(3 * np), 0);
+            for (int64_t n = 0; n < h.nn; ++n)
+                for (int c = 0; c < 3; ++c) v_split(h.v0[3 * n + c], h.v_rows_f[c * np + n], h.v_lo_rows[c * np + n]);
+#endif
+        } else {
+            h.v_rows_d = to_soa<double>(h.v0, h.nn, np, 3);
+        }
+    }
+    h.x0 = nullptr;
+    h.v0 = nullptr;
+}
+
 template <typename T>
 cudaError_t put(void* block, size_t off, const std::vector<T>& v, cudaStream_t st) {
     if (v.empty()) return cudaSuccess;
@@ -360,6 +401,7 @@ int instance_prepare(const ensc_mesh_desc* mesh, const ensc_material* mat, bool 
         total += (h.size[i] + 255) / 256 * 256;
     }
     h.bytes = total;
+    form_device_rows(h);
     return ENSC_OK;
 }
 
@@ -369,57 +411,28 @@ int instance_upload(const InstanceHost& h, void* block, cudaStream_t st, ElemArr
     const int64_t ep = h.ne_pad, np = h.nn_pad;
     char* b = static_cast<char*>(block);
     cudaError_t e = cudaMemsetAsync(block, 0, h.bytes, st);
-    std::vector<uint8_t> bc(static_cast<size_t>(np), 0);
     if (h.mixed) {
-        // corner signs s_j of the reference hexahedron (Element_HexN8.cpp:49-91)
-        static const double kCorner[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
-                                             {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
-        std::vector<float> a(static_cast<size_t>(18 * ep), 0.f);
-        for (int64_t el = 0; el < h.ne; ++el)
-            for (int c = 0; c < 3; ++c)
-                for (int m = 0; m < 3; ++m) {
-                    double v = 0.0;
-                    for (int j = 0; j < 8; ++j) v += h.bt[24 * el + 3 * j + c] * kCorner[j][m];
-                    const float hi = static_cast<float>(v);
-                    a[(3 * c + m) * ep + el] = hi;
-                    a[(9 + 3 * c + m) * ep + el] = static_cast<float>(v - static_cast<double>(hi));
-                }
-        if (e == cudaSuccess) e = put(block, h.off[P::BT], a, st);
-        std::vector<float> cbf(h.cb.begin(), h.cb.end());
+        if (e == cudaSuccess) e = put(block, h.off[P::BT], h.a_rows, st);
         if (e == cudaSuccess) e = put(block, h.off[P::VOL0], h.vol0, st);
-        if (e == cudaSuccess) e = put(block, h.off[P::CB], cbf, st);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // temporaries above die here
+        if (e == cudaSuccess) e = put(block, h.off[P::CB], h.cb_f, st);
     } else {
-        std::vector<double> btsoa = to_soa<double>(h.bt.data(), h.ne, ep, 24);
-        if (e == cudaSuccess) e = put(block, h.off[P::BT], btsoa, st);
+        if (e == cudaSuccess) e = put(block, h.off[P::BT], h.bt_rows, st);
         if (e == cudaSuccess) e = put(block, h.off[P::VOL0], h.vol0, st);
         if (e == cudaSuccess) e = put(block, h.off[P::CB], h.cb, st);
         if (e == cudaSuccess) e = put(block, h.off[P::CB2], h.cb2, st);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     }
     if (e == cudaSuccess) e = put(block, h.off[P::CONN], h.conn_soa, st);
     if (e == cudaSuccess) e = put(block, h.off[P::IM], h.im, st);
-    std::vector<double> xs = to_soa<double>(h.x0, h.nn, np, 3);
-    if (e == cudaSuccess) e = put(block, h.off[P::X], xs, st);
+    if (e == cudaSuccess) e = put(block, h.off[P::X], h.x_rows, st);
     // mixed: the u rows hold the reference position x - u, x0 at the start
-    if (h.mixed && ENSC_MIXED_UREF && e == cudaSuccess) e = put(block, h.off[P::U], xs, st);
-    std::vector<double> vd;
-    std::vector<float> vf;
-    if (h.v0) {
-        if (h.mixed) {
-            vf = to_soa<float>(h.v0, h.nn, np, 3);
+    if (h.mixed && ENSC_MIXED_UREF && e == cudaSuccess) e = put(block, h.off[P::U], h.x_rows, st);
+    if (h.mixed) {
+        if (e == cudaSuccess) e = put(block, h.off[P::V], h.v_rows_f, st);
 #if ENSC_MIXED_VLO
-            std::vector<int16_t> vl(static_cast<size_t>(3 * np), 0);
-            for (int64_t n = 0; n < h.nn; ++n)
-                for (int c = 0; c < 3; ++c) v_split(h.v0[3 * n + c], vf[c * np + n], vl[c * np + n]);
-            if (e == cudaSuccess) e = put(block, h.off[P::V] + 3 * np * sizeof(float), vl, st);
-            if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // vl dies here
+        if (e == cudaSuccess) e = put(block, h.off[P::V] + 3 * np * sizeof(float), h.v_lo_rows, st);
 #endif
-            if (e == cudaSuccess) e = put(block, h.off[P::V], vf, st);
-        } else {
-            vd = to_soa<double>(h.v0, h.nn, np, 3);
-            if (e == cudaSuccess) e = put(block, h.off[P::V], vd, st);
-        }
+    } else {
+        if (e == cudaSuccess) e = put(block, h.off[P::V], h.v_rows_d, st);
     }
     if (e == cudaSuccess) e = put(block, h.off[P::ELL], h.ell, st);
     if (h.clash) {

@@ -27,8 +27,17 @@ struct InstanceHost {
     std::vector<uint8_t> slot_mask;   // [nn_pad] occupied slots (clash-free meshes)
     std::vector<int64_t> csr_ptr;     // clash meshes: (slot, element)-sorted lists
     std::vector<uint32_t> csr_ent;
-    const double* x0 = nullptr;       // caller arrays, read during upload
+    const double* x0 = nullptr;       // caller arrays, read by instance_prepare only
     const double* v0 = nullptr;
+    // the rows the upload copies as they are, formed by instance_prepare (so
+    // that a prepared instance's host work is done before its device part):
+    // mixed: A float pairs [18][ne_pad], cbrt(V0) as float [ne], v float
+    // rows [3][nn_pad] and their 16-bit residual rows [3][nn_pad]; FP64:
+    // B0^T [24][ne_pad], v [3][nn_pad]; both: x0 [3][nn_pad] (v rows empty
+    // when the mesh has no initial velocities)
+    std::vector<float> a_rows, cb_f, v_rows_f;
+    std::vector<int16_t> v_lo_rows;
+    std::vector<double> bt_rows, x_rows, v_rows_d;
     // patch assembly (ElemArrays::patch): the stored order of the elements
     // and the patch tables; all element arrays above are in stored order
     bool patch = false;

@@ -298,9 +298,10 @@ int ensc_batch_add(ensc_batch* b, const ensc_mesh_desc* mesh, const ensc_materia
  * lumped mass and node tables for params->precision and params->assembly
  * (the other fields are not read) -- on the calling thread and
  * makes no CUDA call, so it may run on any thread while a batch steps;
- * errors are reported through ensc_last_error(NULL) of that thread.  The
- * mesh's x0 and v0 arrays are read again by ensc_batch_add_prepared and must
- * stay valid until then.  ensc_batch_add_prepared does the device part
+ * errors are reported through ensc_last_error(NULL) of that thread.  It
+ * also forms the rows the device part copies as they are, and keeps no
+ * pointer into the mesh: its arrays may be freed when it returns.
+ * ensc_batch_add_prepared does the device part
  * (ENSC_ERR_OOM as ensc_batch_add; ENSC_ERR_ARG when the precision is not the
  * batch's) and leaves `prep` to the caller, who frees it with
  * ensc_prepared_destroy; the instance is the one ensc_batch_add would add. */
