@@ -910,6 +910,22 @@ __device__ __forceinline__ void node_group_mixed(const NodeView& N, const double
     [[maybe_unused]] const float hdt = static_cast<float>(0.5 * (dt_i + dt_i_1));
     [[maybe_unused]] const float hdt_lo = static_cast<float>(0.5 * (dt_i + dt_i_1) - static_cast<double>(hdt));
     const double dt_avg = 0.5 * (dt_i + dt_i_1);
+#if ENSC_NODE_LOAD_FIRST
+    // the nodes' own rows first, so that their loads are in flight with the
+    // force slots'
+    double im[W];
+    ld_row<W>(N.inv_mass + n0, im);
+    const uint32_t code = ld_bytes<W>(N.bc + n0);
+    float vo3[3][W];
+    double xo3[3][W];
+    int16_t lo3[3][W];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        ld_row<W>(V + c * np + n0, vo3[c]);
+        ld_row<W>(N.x + c * np + n0, xo3[c]);
+        ld_row<W>(v_lo_rows(N.v, np) + c * np + n0, lo3[c]);
+    }
+#endif
     float f[3][W];
 #pragma unroll
     for (int c = 0; c < 3; ++c)
@@ -951,21 +967,34 @@ __device__ __forceinline__ void node_group_mixed(const NodeView& N, const double
             }
         }
     }
+#if !ENSC_NODE_LOAD_FIRST
     double im[W];
     ld_row<W>(N.inv_mass + n0, im);
     const uint32_t code = ld_bytes<W>(N.bc + n0);
+#endif
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         float vo[W], vn[W];
         double uo[W], xo[W], un[W], xn[W];
-        ld_row<W>(V + c * np + n0, vo);
-        if (!ENSC_MIXED_UREF) ld_row<W>(N.u + c * np + n0, uo);
-        ld_row<W>(N.x + c * np + n0, xo);
 #if ENSC_MIXED_VLO
         int16_t* VL = v_lo_rows(N.v, np);
         int16_t lo[W], ln[W];
+#endif
+#if ENSC_NODE_LOAD_FIRST
+#pragma unroll
+        for (int j = 0; j < W; ++j) {
+            vo[j] = vo3[c][j];
+            xo[j] = xo3[c][j];
+            lo[j] = lo3[c][j];
+        }
+#else
+        ld_row<W>(V + c * np + n0, vo);
+        ld_row<W>(N.x + c * np + n0, xo);
+#if ENSC_MIXED_VLO
         ld_row<W>(VL + c * np + n0, lo);
 #endif
+#endif
+        if (!ENSC_MIXED_UREF) ld_row<W>(N.u + c * np + n0, uo);
 #pragma unroll
         for (int j = 0; j < W; ++j) {
             vn[j] = vo[j];
@@ -1118,7 +1147,7 @@ __global__ void __launch_bounds__(kNodeThreads) k_acceleration_mixed(PatchArrays
 }
 
 // ---- batched instances --------------------------------------------------------
-// Element tiles of kStageTile elements and node tiles of 32 * kNodeGroupMixed
+// Element tiles of kStageTile elements and node tiles of 32 * kNodeGroupBatchMixed
 // nodes, each inside one instance whose arrays, material and control block
 // come from the instance table.  The element pass runs the staged pipeline
 // over the tile list, one tile per block at a time; the node pass gives each
@@ -1375,7 +1404,7 @@ __global__ void __launch_bounds__(kStageTile / EPT, ENSC_BATCH_MINB_MIXED) k_ele
 // NT threads per block (a tuning choice: the warps are independent).
 template <int NT, bool PATCH>
 __global__ void __launch_bounds__(NT, ENSC_NODE_BATCH_MINB_MIXED * kNodeThreads / NT) k_node_batch_mixed(BatchTables T) {
-    constexpr int W = kNodeGroupMixed;
+    constexpr int W = kNodeGroupBatchMixed;
     const int lane = threadIdx.x & 31;
     const int warp = static_cast<int>((static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
     const int nwarps = static_cast<int>((static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5);
@@ -1548,7 +1577,7 @@ int occupancy_element_batch_mixed(int ept) {
 }
 
 int batch_element_tile(bool mixed_precision) { return mixed_precision ? kStageTile : batch_element_tile_fp64(); }
-int batch_node_tile(bool mixed_precision) { return 32 * (mixed_precision ? kNodeGroupMixed : kNodeGroupFp64); }
+int batch_node_tile(bool mixed_precision) { return 32 * (mixed_precision ? kNodeGroupBatchMixed : kNodeGroupFp64); }
 int occupancy_node_batch_mixed(int threads) {
     int nb = 0;
     if (threads == kNodeThreads / 2)
