@@ -5,7 +5,7 @@ Workload (headline): the large elastic-plastic block -- 256x128x64 8-node
 hexahedra (2,097,152 elements, 2,154,945 nodes), J2 plasticity, seeded
 smoothed-Gaussian initial velocities, bottom face fixed, 5000 cycles.  One
 bench step is ``--cycles-per-step`` cycles (default 500) of the stepper on
-the resident model.  The per-cycle working set (1.3-2.3 GB) is far larger
+the resident model.  The per-cycle working set (1.2-2.4 GB) is far larger
 than the 126 MB L2, so no flush is needed between timed steps.  ``value`` is
 the headline precision (default mixed); the other precision is timed the
 same way beside it.
@@ -29,10 +29,11 @@ Further legs of the same run (one GPU):
                  material, dt and clock), 3000 cycles each, in one mixed
                  batch and in one FP64 batch (every instance's mixed error
                  and energy drift against its FP64 run; the maximum is
-                 reported); the plain FP64 stepper solves a sample of them
-                 one after another; the reference CPU stepper solves a
-                 sample as one process per instance on all host cores
-                 (``cpu_reference``);
+                 reported), with both batches' cycle bytes against the
+                 copy peak (``cycle_roofline``); the plain FP64 stepper
+                 solves a sample of them one after another; the reference
+                 CPU stepper solves a sample as one process per instance on
+                 all host cores (``cpu_reference``);
   serving        a seeded Poisson stream (50/s, 500 requests) of
                  1k-500k-element solves served with continuous batching
                  under a 150 GB budget: solves/s and p50/p99 latency; the
