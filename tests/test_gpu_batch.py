@@ -284,3 +284,28 @@ def test_prepared_instance_must_match_the_batch():
                 b.add_prepared(pr)
             pr.close()
         assert b.instances == 0
+
+
+@pytest.mark.parametrize("precision", [capi.FP64, capi.MIXED])
+def test_prepared_instance_outlives_its_mesh_arrays(precision):
+    """A prepared instance holds everything the device part copies: its mesh
+    arrays can be overwritten and freed before ensc_batch_add_prepared, and
+    the instance still runs as one added directly."""
+    c = sweep_case(7, 60)
+    x0, conn, v0 = c.x0.copy(), c.conn.copy(), c.v0.copy()
+    pr = capi.Prepared(x0, conn, v0, material=c.mat, controls=c.ctl, precision=precision)
+    x0[:] = np.nan
+    v0[:] = np.nan
+    conn[:] = 0
+    del x0, conn, v0
+    with make_batch(precision) as b:
+        s = b.add_prepared(pr)
+        pr.close()
+        b.set_bcs(s, c.code, c.val)
+        t = add(b, c)
+        for slot in (s, t):
+            b.arm(slot, c.cycles)
+        drain(b)
+        got, ref = b.download(s), b.download(t)
+        for k in ("x", "u", "v", "sigma"):
+            assert np.array_equal(got[k], ref[k]), k
