@@ -524,17 +524,28 @@ int ensc_upload_state(ensc_handle* h, const double* x, const double* u, const do
     // mixed: the u rows hold x - u; they hold u while x and u are replaced
     const bool uref = mx && ENSC_MIXED_UREF && (x || u);
     if (uref) ensc::launch_reflect_rows(h->N.x, h->N.u, h->nn, h->nn_pad, h->stream);
+    cudaError_t ue = cudaGetLastError();
+    const char* what = "ensc_upload_state";
     for (const Item& it : items) {
-        if (!it.src) continue;
-        CK(h, cudaMemcpyAsync(h->staging, it.src, it.n * it.comps * sizeof(double), cudaMemcpyHostToDevice,
-                              h->stream));
+        if (!it.src || ue != cudaSuccess) continue;
+        ue = cudaMemcpyAsync(h->staging, it.src, it.n * it.comps * sizeof(double), cudaMemcpyHostToDevice,
+                             h->stream);
+        if (ue != cudaSuccess) {
+            what = "cudaMemcpyAsync(state upload)";
+            break;
+        }
         if (it.dst == h->N.v) ensc::launch_aos_to_v(h->staging, h->N, mx, h->stream);
         else ensc::launch_aos_to_soa(h->staging, it.n, it.pad, it.comps, it.dst, it.f32, h->stream, it.at);
-        CK(h, cudaGetLastError());
+        ue = cudaGetLastError();
         used = std::max(used, static_cast<size_t>(it.n * it.comps) * sizeof(double));
     }
+    // back to x - u in the u rows, also when an upload above failed
     if (uref) ensc::launch_reflect_rows(h->N.x, h->N.u, h->nn, h->nn_pad, h->stream);
-    CK(h, cudaGetLastError());
+    if (ue == cudaSuccess) ue = cudaGetLastError();
+    if (ue != cudaSuccess) {
+        release_staging(h, used);
+        return cuda_err(h, what, ue);
+    }
     if (int rc0 = release_staging(h, used)) return rc0;
     int rc = read_ctl(h);
     if (rc) return rc;
