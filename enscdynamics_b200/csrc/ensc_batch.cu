@@ -40,6 +40,9 @@ struct Slot {
     ensc::Material M{};
     bool kinetic0_done = false;
     double* amp = nullptr;  // gravity amplitude table (from the pool)
+    // added, with its device work on the admission stream, and not yet
+    // joined by the batch stream
+    bool pending = false;
 };
 
 // Launch choices of the batched cycle: grid multipliers (over one wave of
@@ -59,6 +62,13 @@ struct ensc_batch {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     cudaStream_t cap_stream = nullptr;
+    // admission stream: the device work of adding an instance (upload, init
+    // pass, its boundary conditions and arming until the batch stream joins)
+    // runs here, so that it overlaps the cycles the batch stream runs;
+    // side_done marks the end of the work enqueued on it so far
+    cudaStream_t side = nullptr;
+    cudaEvent_t side_done = nullptr;
+    bool side_work = false;   // side work enqueued since the batch stream last joined
     cudaMemPool_t pool = nullptr;
     int64_t budget = 0, used = 0;
     int slots = 0;
@@ -138,6 +148,28 @@ struct DevGuard {
 };
 
 bool is_mixed(const ensc_batch* b) { return b->precision == ENSC_MIXED; }
+
+// Marks the end of the admission work enqueued so far.
+int side_mark(ensc_batch* b) {
+    BCK(b, cudaEventRecord(b->side_done, b->side));
+    b->side_work = true;
+    return ENSC_OK;
+}
+
+// The batch stream waits for the admission work enqueued so far (no host
+// wait); added instances stop being pending.  Every entry point that puts
+// work on the batch stream joins first.
+int side_join(ensc_batch* b) {
+    if (!b->side_work) return ENSC_OK;
+    BCK(b, cudaStreamWaitEvent(b->stream, b->side_done, 0));
+    b->side_work = false;
+    for (Slot& sl : b->inst) sl.pending = false;
+    return ENSC_OK;
+}
+
+// The stream for a slot's own device work: the admission stream while it is
+// pending, else the batch stream (after the cycles already enqueued there).
+cudaStream_t slot_stream(const ensc_batch* b, const Slot& sl) { return sl.pending ? b->side : b->stream; }
 
 // Rewrites the instance table and tile lists from the live slots.  The tile
 // energy accumulators are folded into the instances first (tile indices
@@ -412,6 +444,10 @@ int ensc_batch_create(const ensc_params* params, int32_t max_instances, int64_t 
     }
     e = cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return fail(bcuda(b, "cudaStreamCreate", e));
+    e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return fail(bcuda(b, "cudaStreamCreate", e));
+    e = cudaEventCreateWithFlags(&b->side_done, cudaEventDisableTiming);
+    if (e != cudaSuccess) return fail(bcuda(b, "cudaEventCreate", e));
     // tables
     auto al = [](size_t x) { return (x + 255) / 256 * 256; };
     const size_t s_desc = al(sizeof(ensc::InstanceDesc) * b->slots), s_et = al(4 * b->max_etiles),
@@ -575,12 +611,15 @@ int ensc_batch_add_prepared(ensc_batch* b, const ensc_prepared* prep, const ensc
     if (b->n_etiles + et > b->max_etiles || b->n_ntiles + nt > b->max_ntiles)
         return berr(b, ENSC_ERR_OOM, "batch tile capacity exceeded");
     Slot& sl = b->inst[s];
+    // all on the admission stream: the slot is in no table the batch stream
+    // runs until that stream joins it
+    cudaStream_t st = b->side;
     void* block = nullptr;
-    BCK(b, cudaMallocFromPoolAsync(&block, ih.bytes, b->pool, b->stream));
+    BCK(b, cudaMallocFromPoolAsync(&block, ih.bytes, b->pool, st));
     std::string perr;
-    rc = ensc::instance_upload(ih, block, b->stream, sl.E, sl.N, sl.PA, perr);
+    rc = ensc::instance_upload(ih, block, st, sl.E, sl.N, sl.PA, perr);
     if (rc) {
-        cudaFreeAsync(block, b->stream);
+        cudaFreeAsync(block, st);
         return berr(b, rc, perr);
     }
     sl.block = block;
@@ -594,24 +633,25 @@ int ensc_batch_add_prepared(ensc_batch* b, const ensc_prepared* prep, const ensc
     ensc::material_from(mat, controls, sl.M);
     b->h_ctl[s] = ensc::initial_ctl(controls, sl.M);
     b->h_ctl[s].done = 1;  // idle until armed
-    BCK(b, cudaMemcpyAsync(b->d_ctl + s, b->h_ctl + s, sizeof(Ctl), cudaMemcpyHostToDevice, b->stream));
     // init(): force pass with dt = 0 on the unconstrained velocities
     Ctl c0 = b->h_ctl[s];
     c0.done = 0;
-    BCK(b, cudaMemcpyAsync(b->d_ctl + s, &c0, sizeof(Ctl), cudaMemcpyHostToDevice, b->stream));
+    BCK(b, cudaMemcpyAsync(b->d_ctl + s, &c0, sizeof(Ctl), cudaMemcpyHostToDevice, st));
     ensc::Partials P{};
     P.elem = b->d_scratch;
     P.node = b->d_scratch;
     const int g = static_cast<int>(std::min<int64_t>((ih.ne + ensc::kElemThreads - 1) / ensc::kElemThreads,
                                                      b->scratch_blocks));
     P.n_elem_blocks = g;
-    if (is_mixed(b)) ensc::launch_element_mixed(sl.E, sl.N, sl.M, b->d_ctl + s, P, g, true, b->stream, sl.PA);
-    else ensc::launch_element_fp64(sl.E, sl.N, sl.M, b->d_ctl + s, P, g, true, b->stream);
+    if (is_mixed(b)) ensc::launch_element_mixed(sl.E, sl.N, sl.M, b->d_ctl + s, P, g, true, st, sl.PA);
+    else ensc::launch_element_fp64(sl.E, sl.N, sl.M, b->d_ctl + s, P, g, true, st);
     BCK(b, cudaGetLastError());
-    BCK(b, cudaMemcpyAsync(b->h_ctl + s, b->d_ctl + s, sizeof(Ctl), cudaMemcpyDeviceToHost, b->stream));
-    BCK(b, cudaStreamSynchronize(b->stream));
-    b->h_ctl[s].done = 1;
-    BCK(b, cudaMemcpyAsync(b->d_ctl + s, b->h_ctl + s, sizeof(Ctl), cudaMemcpyHostToDevice, b->stream));
+    BCK(b, cudaMemcpyAsync(b->h_ctl + s, b->d_ctl + s, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+    BCK(b, cudaStreamSynchronize(st));
+    b->h_ctl[s].done = 1;  // idle until armed
+    BCK(b, cudaMemcpyAsync(b->d_ctl + s, b->h_ctl + s, sizeof(Ctl), cudaMemcpyHostToDevice, st));
+    if (int rcm = side_mark(b)) return rcm;
+    sl.pending = true;
     sl.used = true;
     b->used += static_cast<int64_t>(ih.bytes);
     b->dirty = true;  // the tables are rewritten before the next run
@@ -623,6 +663,7 @@ int ensc_batch_set_bcs(ensc_batch* b, int32_t slot, const int8_t* dof_code, cons
     if (!b || slot < 0 || slot >= b->slots || !b->inst[slot].used) return berr(b, ENSC_ERR_ARG, "bad slot");
     DevGuard dg(b->device);
     Slot& sl = b->inst[slot];
+    cudaStream_t st = slot_stream(b, sl);
     std::vector<uint8_t> bc(static_cast<size_t>(sl.nn_pad), 0);
     std::vector<double> bcv(static_cast<size_t>(3 * sl.nn_pad), 0.0);
     if (dof_code) {
@@ -636,10 +677,9 @@ int ensc_batch_set_bcs(ensc_batch* b, int32_t slot, const int8_t* dof_code, cons
             bc[n] = static_cast<uint8_t>(packed);
         }
     }
-    BCK(b, cudaMemcpyAsync(const_cast<uint8_t*>(sl.N.bc), bc.data(), bc.size(), cudaMemcpyHostToDevice, b->stream));
-    BCK(b, cudaMemcpyAsync(const_cast<double*>(sl.N.bcv), bcv.data(), bcv.size() * 8, cudaMemcpyHostToDevice,
-                           b->stream));
-    ensc::launch_apply_bc_v(sl.N, is_mixed(b), b->stream);
+    BCK(b, cudaMemcpyAsync(const_cast<uint8_t*>(sl.N.bc), bc.data(), bc.size(), cudaMemcpyHostToDevice, st));
+    BCK(b, cudaMemcpyAsync(const_cast<double*>(sl.N.bcv), bcv.data(), bcv.size() * 8, cudaMemcpyHostToDevice, st));
+    ensc::launch_apply_bc_v(sl.N, is_mixed(b), st);
     if (!sl.kinetic0_done) {
         ensc::Partials P{};
         const int g = static_cast<int>(std::min<int64_t>((sl.nn + ensc::kNodeThreads - 1) / ensc::kNodeThreads,
@@ -648,11 +688,12 @@ int ensc_batch_set_bcs(ensc_batch* b, int32_t slot, const int8_t* dof_code, cons
         P.node = b->d_scratch;
         P.n_elem_blocks = 0;
         P.n_node_blocks = g;
-        ensc::launch_kinetic0(sl.N, P, b->d_ctl + slot, is_mixed(b), g, b->stream);
+        ensc::launch_kinetic0(sl.N, P, b->d_ctl + slot, is_mixed(b), g, st);
         sl.kinetic0_done = true;
     }
     BCK(b, cudaGetLastError());
-    BCK(b, cudaStreamSynchronize(b->stream));
+    BCK(b, cudaStreamSynchronize(st));
+    if (st == b->side) return side_mark(b);
     return ENSC_OK;
 }
 
@@ -661,6 +702,7 @@ int ensc_batch_set_gravity_amplitude(ensc_batch* b, int32_t slot, int32_t n_poin
     if (n_points < 0 || n_points > ENSC_MAX_AMPLITUDE_POINTS || (n_points > 0 && !time_value))
         return berr(b, ENSC_ERR_ARG, "amplitude: 0 to ENSC_MAX_AMPLITUDE_POINTS (time, value) pairs");
     DevGuard dg(b->device);
+    if (int rcj = side_join(b)) return rcj;
     Slot& sl = b->inst[slot];
     if (n_points > 0 && !sl.amp)
         BCK(b, cudaMallocFromPoolAsync(reinterpret_cast<void**>(&sl.amp),
@@ -678,8 +720,10 @@ int ensc_batch_arm(ensc_batch* b, int32_t slot, int64_t max_cycles, double step_
     if (!b || slot < 0 || slot >= b->slots || !b->inst[slot].used || max_cycles < 0)
         return berr(b, ENSC_ERR_ARG, "bad slot or cycle count");
     DevGuard dg(b->device);
-    ensc::launch_arm(b->d_ctl + slot, step_end_time, max_cycles, b->stream);
+    cudaStream_t st = slot_stream(b, b->inst[slot]);
+    ensc::launch_arm(b->d_ctl + slot, step_end_time, max_cycles, st);
     BCK(b, cudaGetLastError());
+    if (st == b->side) return side_mark(b);
     return ENSC_OK;
 }
 
@@ -687,6 +731,7 @@ int ensc_batch_run(ensc_batch* b, int64_t cycles) {
     if (!b || cycles < 0) return berr(b, ENSC_ERR_ARG, "bad cycle count");
     if (cycles == 0) return ENSC_OK;
     DevGuard dg(b->device);
+    if (int rcj = side_join(b)) return rcj;
     if (b->dirty) {
         int rc = rebuild_tables(b);
         if (rc) return rc;
@@ -708,6 +753,7 @@ int ensc_batch_run(ensc_batch* b, int64_t cycles) {
 int ensc_batch_sync(ensc_batch* b, int32_t* n_running) {
     if (!b) return berr(b, ENSC_ERR_ARG, "batch is NULL");
     DevGuard dg(b->device);
+    if (int rcj = side_join(b)) return rcj;
     ensc::launch_between_batch(b->T, b->slots, 1, b->stream);  // fold the last cycle's energy
     BCK(b, cudaGetLastError());
     BCK(b, cudaMemcpyAsync(b->h_ctl, b->d_ctl, sizeof(Ctl) * b->slots, cudaMemcpyDeviceToHost, b->stream));
@@ -751,6 +797,7 @@ int ensc_batch_download(ensc_batch* b, int32_t slot, double* x, double* u, doubl
                         double* eps_p) {
     if (!b || slot < 0 || slot >= b->slots || !b->inst[slot].used) return berr(b, ENSC_ERR_ARG, "bad slot");
     DevGuard dg(b->device);
+    if (int rcj = side_join(b)) return rcj;
     const Slot& sl = b->inst[slot];
     const bool mx = is_mixed(b);
     struct Item {
@@ -794,6 +841,7 @@ int ensc_batch_download(ensc_batch* b, int32_t slot, double* x, double* u, doubl
 int ensc_batch_remove(ensc_batch* b, int32_t slot) {
     if (!b || slot < 0 || slot >= b->slots || !b->inst[slot].used) return berr(b, ENSC_ERR_ARG, "bad slot");
     DevGuard dg(b->device);
+    if (int rcj = side_join(b)) return rcj;
     Slot& sl = b->inst[slot];
     // fold what the instance's tiles still hold (the tables list them until
     // the next run rewrites them), then take it out of the device table so
@@ -844,6 +892,8 @@ int32_t ensc_batch_instances(const ensc_batch* b) {
 void ensc_batch_destroy(ensc_batch* b) {
     if (!b) return;
     DevGuard dg(b->device);
+    if (b->side) cudaStreamSynchronize(b->side);
+    side_join(b);
     if (b->stream) cudaStreamSynchronize(b->stream);
     if (b->graph) cudaGraphExecDestroy(b->graph);
     for (Slot& s : b->inst) {
@@ -852,6 +902,8 @@ void ensc_batch_destroy(ensc_batch* b) {
     }
     if (b->stream) cudaStreamSynchronize(b->stream);
     if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
+    if (b->side) cudaStreamDestroy(b->side);
+    if (b->side_done) cudaEventDestroy(b->side_done);
     if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
     if (b->pool) cudaMemPoolDestroy(b->pool);
     if (b->tables) cudaFree(b->tables);

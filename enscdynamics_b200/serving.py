@@ -218,6 +218,10 @@ class Server:
     The host part of the next arrivals runs while the GPU steps the current
     quantum: on ``prepare_workers`` threads, or with ``prepare_workers=0`` on
     the loop's own thread between enqueueing the quantum and waiting for it.
+    The device part of requests already prepared also runs during the
+    quantum (the batch does it on its own admission stream); they join the
+    next quantum.  Between quanta the loop admits again, after retiring the
+    finished instances, whatever their memory now lets in.
     At most ``prepare_ahead`` requests are prepared and not yet admitted, which
     bounds the host memory they hold.  ``stats`` accumulates where the loop's
     time went."""
@@ -284,46 +288,59 @@ class Server:
             o.status = code
             o.finished = now()
 
+        def intake():
+            # arrivals so far join the waiting list
+            t = now()
+            while state["next"] < len(pending) and pending[state["next"]].arrival <= t:
+                waiting.append(pending[state["next"]])
+                state["next"] += 1
+
+        def admit(block_first: bool, fresh: Optional[set] = None) -> List:
+            # admit the prepared: first come, first served, with backfill;
+            # returns the requests the batch refused
+            nonlocal waiting
+            c = self.clock()
+            still, refused = [], []
+            for i, r in enumerate(waiting):
+                # with nothing on the device, wait for the first request's host part
+                res = prepared(r, block=block_first and not running and i == 0)
+                if res is None:
+                    still.append(r)
+                    continue
+                token, err = res
+                if err is not None:
+                    del prep[r.index]
+                    fail(r, getattr(err, "code", ERR_ARG))
+                    continue
+                try:
+                    slot = be.add_prepared(token, r.problem)
+                except AdmissionError:
+                    still.append(r)
+                    refused.append(r)
+                    continue
+                del prep[r.index]
+                be.release(token)
+                be.arm(slot, r.problem.cycles)
+                running[slot] = (r, r.problem.cycles)
+                if fresh is not None:
+                    fresh.add(slot)
+                out[r.index].admitted = now()
+            waiting = still
+            st["admit_s"] += self.clock() - c
+            return refused
+
+        state = {"next": 0}
         try:
-            nxt = 0
-            while nxt < len(pending) or waiting or running:
+            while state["next"] < len(pending) or waiting or running:
                 t = now()
+                nxt = state["next"]
                 if not running and not waiting and nxt < len(pending) and pending[nxt].arrival > t:
                     c = self.clock()
                     self.sleep(pending[nxt].arrival - t)  # idle until the next arrival
                     st["idle_s"] += self.clock() - c
-                    t = now()
-                while nxt < len(pending) and pending[nxt].arrival <= t:
-                    waiting.append(pending[nxt])
-                    nxt += 1
+                intake()
                 start_prepares()
-                # admit the prepared: first come, first served, with backfill
-                c = self.clock()
-                still, refused = [], []
-                for i, r in enumerate(waiting):
-                    # with nothing on the device, wait for the first request's host part
-                    res = prepared(r, block=not running and i == 0)
-                    if res is None:
-                        still.append(r)
-                        continue
-                    token, err = res
-                    if err is not None:
-                        del prep[r.index]
-                        fail(r, getattr(err, "code", ERR_ARG))
-                        continue
-                    try:
-                        slot = be.add_prepared(token, r.problem)
-                    except AdmissionError:
-                        still.append(r)
-                        refused.append(r)
-                        continue
-                    del prep[r.index]
-                    be.release(token)
-                    be.arm(slot, r.problem.cycles)
-                    running[slot] = (r, r.problem.cycles)
-                    out[r.index].admitted = now()
-                waiting = still
-                st["admit_s"] += self.clock() - c
+                refused = admit(block_first=True)
                 if not running:
                     # an empty batch that cannot take a request never will: reject it
                     for r in refused:
@@ -339,13 +356,22 @@ class Server:
                 st["run_s"] += self.clock() - c
                 st["quanta"] += 1
                 st["cycles"] += q
-                start_prepares()  # host work while the quantum runs
+                # while the quantum runs: host parts of the next arrivals, and
+                # the device part of those already prepared (the backend puts
+                # it beside the running cycles); they join the next quantum
+                intake()
+                start_prepares()
+                fresh: set = set()
+                admit(block_first=False, fresh=fresh)
+                start_prepares()
                 c = self.clock()
                 be.sync()
                 st["wait_s"] += self.clock() - c
                 c = self.clock()
                 for slot in list(running):
                     r, left = running[slot]
+                    if slot in fresh:
+                        continue  # added after the quantum was enqueued: it has not run yet
                     rep = be.report(slot)
                     if rep["done"] or rep["status"]:
                         o = out[r.index]

@@ -288,7 +288,11 @@ int ensc_batch_create(const ensc_params* params, int32_t max_instances, int64_t 
 
 /* Adds an instance (ensc_create's work for it, controls from `controls`);
  * *slot receives its index.  ENSC_ERR_OOM when the budget, the slots or the
- * tile capacity would be exceeded. */
+ * tile capacity would be exceeded.  The device work of adding an instance,
+ * and of its ensc_batch_set_bcs and ensc_batch_arm until the batch next
+ * runs, syncs, downloads or removes, goes on the batch's own admission
+ * stream: it overlaps cycles already enqueued by ensc_batch_run, which the
+ * new instance does not take part in; the next ensc_batch_run includes it. */
 int ensc_batch_add(ensc_batch* b, const ensc_mesh_desc* mesh, const ensc_material* mat, const ensc_params* controls,
                    int32_t* slot);
 
