@@ -99,10 +99,15 @@ int cuda_err(ensc_handle* h, const char* what, cudaError_t e) {
     } while (0)
 
 
+// Copies a host vector to the device on the handle's stream, so that the
+// kernels launched there after it see the data: a plain cudaMemcpy from
+// pageable memory may return before its DMA lands, and it is not ordered
+// with the handle's non-blocking stream.  (A pageable source is staged
+// before the call returns, so the vector may go away after it.)
 template <typename T>
 int upload(ensc_handle* h, void* dst, const std::vector<T>& src) {
     if (src.empty()) return ENSC_OK;
-    CK(h, cudaMemcpy(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, h->stream));
     return ENSC_OK;
 }
 
