@@ -309,3 +309,30 @@ def test_prepared_instance_outlives_its_mesh_arrays(precision):
         got, ref = b.download(s), b.download(t)
         for k in ("x", "u", "v", "sigma"):
             assert np.array_equal(got[k], ref[k]), k
+
+
+@pytest.mark.parametrize("precision", [capi.FP64, capi.MIXED])
+def test_instance_added_while_cycles_run(precision):
+    """An instance added (upload, init pass, boundary conditions, arming on
+    the batch's admission stream) while cycles enqueued for the others are
+    still running joins at the next run, and every result equals the same
+    instance alone."""
+    first, late = sweep_case(3, 2000, ne_max=20000), sweep_case(11, 400)
+    alone = {}
+    for c in (first, late):
+        with make_batch(precision) as b:
+            s = add(b, c)
+            b.arm(s, c.cycles)
+            drain(b)
+            alone[c.name] = (b.download(s), b.report(s), b.energy(s))
+    with make_batch(precision) as b:
+        a = add(b, first)
+        b.arm(a, first.cycles)
+        b.run(700)  # the launch geometry is tuned during the first runs
+        b.sync()
+        b.run(512)  # enqueued; the add below overlaps these cycles
+        s = add(b, late)
+        b.arm(s, late.cycles)
+        drain(b)
+        assert_same(b.download(a), b.report(a), b.energy(a), alone[first.name], first.name)
+        assert_same(b.download(s), b.report(s), b.energy(s), alone[late.name], late.name)
