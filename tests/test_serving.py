@@ -102,3 +102,17 @@ def test_a_request_whose_host_part_fails_is_reported_and_others_finish():
         out = S.Server(be, clock=be.now, sleep=be.sleep, prepare_workers=workers).serve(reqs)
         assert out[1].status == S.ERR_ARG and out[1].finished >= out[1].arrival
         assert out[0].status == 0 and out[2].status == 0 and out[2].cycles == 200
+
+
+def test_request_admitted_during_a_quantum_joins_the_next_with_all_its_cycles():
+    # request 1 arrives while the first quantum runs: it is admitted then (the
+    # device part beside the running cycles), takes no part in that quantum,
+    # and the next quantum is sized by its full cycle count
+    reqs = [W.Request(0, 0.0, _Problem(1000, 1000)), W.Request(1, 1e-6, _Problem(1000, 300))]
+    be = S.FakeBackend(budget_bytes=10 ** 9, max_instances=8)
+    srv = S.Server(be, clock=be.now, sleep=be.sleep)
+    out = srv.serve(reqs)
+    assert [o.status for o in out] == [0, 0]
+    assert out[1].cycles == 300 and out[0].cycles == 1000
+    assert out[1].admitted <= out[0].finished
+    assert srv.stats["quanta"] == 2 and be.cycles_run == 1300
