@@ -707,9 +707,13 @@ int ensc_batch_set_gravity_amplitude(ensc_batch* b, int32_t slot, int32_t n_poin
     if (n_points > 0 && !sl.amp)
         BCK(b, cudaMallocFromPoolAsync(reinterpret_cast<void**>(&sl.amp),
                                        2 * sizeof(double) * ENSC_MAX_AMPLITUDE_POINTS, b->pool, b->stream));
-    if (n_points > 0)
+    if (n_points > 0) {
         BCK(b, cudaMemcpyAsync(sl.amp, time_value, 2 * sizeof(double) * n_points, cudaMemcpyHostToDevice,
                                b->stream));
+        // the caller's table may be pinned memory, which the copy reads in
+        // stream order: done before it is handed back
+        BCK(b, cudaStreamSynchronize(b->stream));
+    }
     sl.M.amp = n_points > 0 ? sl.amp : nullptr;
     sl.M.amp_n = n_points;
     b->dirty = true;  // the instance table carries the material by value
