@@ -116,3 +116,16 @@ def test_request_admitted_during_a_quantum_joins_the_next_with_all_its_cycles():
     assert out[1].cycles == 300 and out[0].cycles == 1000
     assert out[1].admitted <= out[0].finished
     assert srv.stats["quanta"] == 2 and be.cycles_run == 1300
+
+
+def test_request_refused_during_a_quantum_is_admitted_after_the_retire():
+    # request 1 arrives while request 0 holds the whole budget: the admission
+    # tried during the quantum is refused, and the one after request 0
+    # retires takes it
+    reqs = [W.Request(0, 0.0, _Problem(1000, 200)), W.Request(1, 1e-6, _Problem(1000, 100))]
+    be = S.FakeBackend(budget_bytes=1000 * 400, max_instances=8)
+    srv = S.Server(be, clock=be.now, sleep=be.sleep)
+    out = srv.serve(reqs)
+    assert [o.status for o in out] == [0, 0]
+    assert out[1].cycles == 100 and out[1].admitted >= out[0].finished
+    assert be.peak <= 1000 * 400 and be.used == 0
