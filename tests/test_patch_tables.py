@@ -104,3 +104,30 @@ def test_slot_assembly_where_patches_do_not_apply():
         tables(p, precision=capi.FP64, assembly=capi.ASSEMBLY_PATCH)
     with pytest.raises(capi.EnscError, match="assembly"):
         tables(p, assembly=7)
+
+
+def test_prepared_tables_do_not_depend_on_the_mesh_arrays_afterwards():
+    # the prepared instance copies what it needs: overwriting and dropping the
+    # mesh arrays after ensc_batch_prepare leaves its tables unchanged
+    p = W.block(8, 8, 8, 0.08, 0.08, 0.08, plastic=True)
+    x0, conn, v0 = p.mesh.x0.copy(), p.mesh.conn.copy(), p.v0.copy()
+    pr = capi.Prepared(x0, conn, v0, material=p.material, controls=p.controls, precision=capi.MIXED,
+                       assembly=capi.ASSEMBLY_PATCH)
+    try:
+        x0[:] = np.nan
+        conn[:] = 0
+        v0[:] = np.nan
+        del x0, conn, v0
+        got = pr.patch_tables()
+        nbytes = pr.device_bytes
+    finally:
+        pr.close()
+    _, ref = tables(p)
+    for k in ref:
+        assert np.array_equal(got[k], ref[k]), k
+    ref_pr = capi.Prepared(p.mesh.x0, p.mesh.conn, p.v0, material=p.material, controls=p.controls,
+                           precision=capi.MIXED, assembly=capi.ASSEMBLY_PATCH)
+    try:
+        assert ref_pr.device_bytes == nbytes
+    finally:
+        ref_pr.close()
