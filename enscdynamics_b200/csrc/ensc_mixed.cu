@@ -1,7 +1,8 @@
 // Mixed-precision stepper kernels: the element pass (kinematics, Jaumann /
 // J2 stress, hourglass, bulk viscosity) and the force gather run in FP32;
-// nodal position and displacement accumulation (x += dt v, u += dt v), the
-// clock, the stable-dt reduction and the energy sums stay FP64.
+// nodal position accumulation (x += dt v; the displacement is x minus a
+// stored reference position), the clock, the stable-dt reduction and the
+// energy sums stay FP64.
 //
 // Same algorithm and data flow as the FP64 path (ensc_fp64.cu); operation
 // order is free here (FMA contraction on), accuracy is checked against the
@@ -894,7 +895,7 @@ __device__ __forceinline__ void node_body_mixed(const ElemArrays& E, const NodeA
 }
 
 // W consecutive nodes of the mixed node pass with 16-byte row accesses
-// (float4 force slots and velocities, pairs of doubles for x, u and the
+// (float4 force slots and velocities, pairs of doubles for x and the
 // inverse mass); per node the arithmetic of node_body_mixed.  Slots the mask
 // marks empty are skipped, or (ENSC_NODE_ALL_SLOTS) summed as the zeros they
 // hold: the slot-major rows start zeroed and only the slot's element writes
